@@ -1,0 +1,328 @@
+"""artss_b200 -- the ARTSS fractional-step timestep on NVIDIA B200.
+
+Python access to the two native libraries of this package:
+
+* ``libartss_host.so``: C++ host runtime (ARTSS XML reader, geometry and index
+  lists, plugin classes, SolverController / TimeIntegration), ``include/artss_host.h``;
+* ``libartss_cuda.so``: the sm_100a kernels behind the plugin interfaces,
+  ``include/artss_cuda.h``.
+
+There is no CPU implementation of the timestep: a missing library raises
+:class:`NativeLibraryMissing`, and a machine without a CUDA device makes
+:class:`Simulation` raise.  :class:`Geometry` (index lists and boundary
+assignments) runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+__all__ = ["Geometry", "Simulation", "NativeLibraryMissing", "ArtssError", "library_path", "FIELD_TYPES",
+           "PATCHES", "load_cuda", "load_host"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIELD_TYPES = {"rho": 0, "u": 1, "v": 2, "w": 3, "p": 4, "T": 5, "nu": 6}
+PATCHES = ["left", "right", "bottom", "top", "front", "back"]
+MAX_LEVEL = 8
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+class ArtssError(RuntimeError):
+    pass
+
+
+def library_path(name: str) -> str:
+    return os.path.join(HERE, name)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("n_levels", C.c_int32), ("reserved", C.c_int32)] + [
+        (f, C.c_int64 * (MAX_LEVEL + 1)) for f in ("Nx", "Ny", "Nz", "i1", "i2", "j1", "j2", "k1", "k2")
+    ] + [(f, C.c_double * (MAX_LEVEL + 1)) for f in ("dx", "dy", "dz")]
+
+
+class BcAssign(C.Structure):
+    _fields_ = [("target", C.c_int64), ("source", C.c_int64), ("value", C.c_double), ("sign", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class IterCfg(C.Structure):
+    _fields_ = [("max_iter", C.c_int64), ("tol_res", C.c_double), ("w", C.c_double)]
+
+
+class IterStats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("residual", C.c_double)]
+
+
+class MgCfg(C.Structure):
+    _fields_ = [("n_level", C.c_int32), ("n_cycle", C.c_int32), ("max_cycle", C.c_int32), ("n_relax", C.c_int32),
+                ("tol_res", C.c_double), ("smoother", C.c_int32), ("reserved", C.c_int32),
+                ("smoother_max_iter", C.c_int64), ("smoother_tol_res", C.c_double), ("smoother_w", C.c_double)]
+
+
+class MgStats(C.Structure):
+    _fields_ = [("cycles", C.c_int64), ("coarse_iterations", C.c_int64), ("residual", C.c_double)]
+
+
+BC_DTYPE = np.dtype([("target", "<i8"), ("source", "<i8"), ("value", "<f8"), ("sign", "<i4"), ("reserved", "<i4")])
+
+_cuda: Optional[C.CDLL] = None
+_host: Optional[C.CDLL] = None
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I64P = C.POINTER(C.c_int64)
+
+
+def _load(name: str) -> C.CDLL:
+    path = library_path(name)
+    if not os.path.exists(path):
+        raise NativeLibraryMissing(f"{path} is not built; run `make -C {HERE}` or __graft_entry__.build()")
+    return C.CDLL(path, mode=C.RTLD_GLOBAL)
+
+
+def load_cuda() -> C.CDLL:
+    """libartss_cuda.so with argument types of include/artss_cuda.h."""
+    global _cuda
+    if _cuda is None:
+        lib = _load("libartss_cuda.so")
+        sig = {
+            "artss_ctx_create": ([C.POINTER(GridDesc), C.c_int, C.POINTER(_P)], C.c_int),
+            "artss_ctx_destroy": ([_P], C.c_int),
+            "artss_ctx_stream": ([_P], _P),
+            "artss_ctx_sync": ([_P], C.c_int),
+            "artss_last_error": ([], C.c_char_p),
+            "artss_ctx_kernel_launches": ([_P], C.c_int64),
+            "artss_field_alloc": ([_P, C.c_int, C.POINTER(_D)], C.c_int),
+            "artss_field_free": ([_P, _D], C.c_int),
+            "artss_field_size": ([_P, C.c_int], C.c_int64),
+            "artss_upload": ([_P, _D, _D, C.c_int64], C.c_int),
+            "artss_download": ([_P, _D, _D, C.c_int64], C.c_int),
+            "artss_set_cell_lists": ([_P, C.c_int, _I64P, C.c_int64, _I64P, C.c_int64], C.c_int),
+            "artss_get_cell_flags": ([_P, C.c_int, C.POINTER(C.c_uint8), C.c_int64], C.c_int),
+            "artss_set_boundary_program": ([_P, C.c_int, C.c_int, C.POINTER(BcAssign), C.c_int64], C.c_int),
+            "artss_boundary_program_waves": ([_P, C.c_int, C.c_int], C.c_int),
+            "artss_apply_boundary": ([_P, _D, C.c_int, C.c_int], C.c_int),
+            "artss_fill": ([_P, _D, C.c_int, C.c_double], C.c_int),
+            "artss_copy": ([_P, _D, _D, C.c_int], C.c_int),
+            "artss_add_field": ([_P, _D, _D, C.c_int], C.c_int),
+            "artss_add_scalar": ([_P, _D, C.c_double, C.c_int], C.c_int),
+            "artss_scale": ([_P, _D, C.c_double, C.c_int], C.c_int),
+            "artss_scale_copy": ([_P, _D, _D, C.c_double, C.c_int], C.c_int),
+            "artss_couple": ([_P] + [_D] * 9, C.c_int),
+            "artss_advect_sl": ([_P, _D, _D, _D, _D, _D, C.c_double, C.c_int], C.c_int),
+            "artss_advect_sl_uvw": ([_P] + [_D] * 9 + [C.c_double], C.c_int),
+            "artss_turb_const_smagorinsky": ([_P, _D, _D, _D, _D, C.c_double], C.c_int),
+            "artss_diffuse_cgs": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg), C.c_int,
+                                   C.POINTER(IterStats)], C.c_int),
+            "artss_diffuse_jacobi": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg),
+                                      C.POINTER(IterStats)], C.c_int),
+            "artss_divergence": ([_P, _D, _D, _D, _D], C.c_int),
+            "artss_projection": ([_P] + [_D] * 7, C.c_int),
+            "artss_buoyancy_force": ([_P, _D, _D, _D, C.c_double, C.c_double], C.c_int),
+            "artss_add_source": ([_P, _D, _D, C.c_double, C.c_int], C.c_int),
+            "artss_mg_create": ([_P, C.POINTER(MgCfg), C.POINTER(_P)], C.c_int),
+            "artss_mg_destroy": ([_P], C.c_int),
+            "artss_mg_pressure": ([_P, _D, _D, C.c_int, C.POINTER(MgStats)], C.c_int),
+            "artss_mg_set_rhs": ([_P, _D, _D], C.c_int),
+            "artss_mg_vcycle": ([_P, _D], C.c_int),
+            "artss_residual_norm": ([_P, _D, _D, _D, _D], C.c_int),
+        }
+        for fn, (args, res) in sig.items():
+            f = getattr(lib, fn)
+            f.argtypes = args
+            f.restype = res
+        _cuda = lib
+    return _cuda
+
+
+def load_host() -> C.CDLL:
+    """libartss_host.so with argument types of include/artss_host.h."""
+    global _host
+    if _host is None:
+        load_cuda()
+        lib = _load("libartss_host.so")
+        sig = {
+            "artss_host_last_error": ([], C.c_char_p),
+            "artss_geom_create": ([C.c_char_p, C.POINTER(_P)], C.c_int),
+            "artss_geom_destroy": ([_P], None),
+            "artss_geom_levels": ([_P], C.c_int),
+            "artss_geom_obstacles": ([_P], C.c_int),
+            "artss_geom_list": ([_P, C.c_char_p, C.c_int, C.POINTER(_I64P), _I64P], C.c_int),
+            "artss_geom_dims": ([_P, C.c_int, _I64P], C.c_int),
+            "artss_geom_boundary_program": ([_P, C.c_int, C.c_int, C.POINTER(C.POINTER(BcAssign)), _I64P], C.c_int),
+            "artss_geom_grid_desc": ([_P, C.POINTER(GridDesc)], C.c_int),
+            "artss_sim_create": ([C.c_char_p, C.c_int, C.POINTER(_P)], C.c_int),
+            "artss_sim_destroy": ([_P], None),
+            "artss_sim_run": ([_P, C.c_int64, _I64P], C.c_int),
+            "artss_sim_finished": ([_P], C.c_int),
+            "artss_sim_time": ([_P], C.c_double),
+            "artss_sim_step_index": ([_P], C.c_int64),
+            "artss_sim_inner_cells": ([_P], C.c_int64),
+            "artss_sim_get_field": ([_P, C.c_char_p, _D, C.c_int64], C.c_int),
+            "artss_sim_set_field": ([_P, C.c_char_p, _D, C.c_int64], C.c_int),
+            "artss_sim_field_size": ([_P], C.c_int64),
+            "artss_sim_field_device": ([_P, C.c_char_p], _D),
+            "artss_sim_context": ([_P], _P),
+            "artss_sim_last_stats": ([_P, _I64P, _I64P, _D], C.c_int),
+            "artss_sim_pressure": ([_P, C.c_int, _I64P, _D], C.c_int),
+            "artss_sim_mg": ([_P], _P),
+        }
+        for fn, (args, res) in sig.items():
+            f = getattr(lib, fn)
+            f.argtypes = args
+            f.restype = res
+        _host = lib
+    return _host
+
+
+def _host_check(st: int, what: str) -> None:
+    if st != 0:
+        msg = load_host().artss_host_last_error().decode(errors="replace")
+        raise ArtssError(f"{what}: {msg} (status {st})")
+
+
+def cuda_check(st: int, what: str) -> None:
+    if st != 0:
+        msg = load_cuda().artss_last_error().decode(errors="replace")
+        raise ArtssError(f"{what}: {msg} (status {st})")
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+class Geometry:
+    """Index lists and boundary assignments of an ARTSS XML scene (CPU)."""
+
+    def __init__(self, xml_path: str):
+        self._lib = load_host()
+        self._h = _P()
+        _host_check(self._lib.artss_geom_create(os.fsencode(xml_path), C.byref(self._h)), "geometry")
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.artss_geom_destroy(self._h)
+            self._h = _P()
+
+    __del__ = close
+
+    @property
+    def levels(self) -> int:
+        return self._lib.artss_geom_levels(self._h)
+
+    @property
+    def obstacles(self) -> int:
+        return self._lib.artss_geom_obstacles(self._h)
+
+    def dims(self, level: int = 0):
+        d = (C.c_int64 * 3)()
+        _host_check(self._lib.artss_geom_dims(self._h, level, d), "dims")
+        return tuple(int(x) for x in d)
+
+    def list(self, name: str, level: int = 0) -> np.ndarray:
+        p = _I64P()
+        n = C.c_int64()
+        _host_check(self._lib.artss_geom_list(self._h, name.encode(), level, C.byref(p), C.byref(n)), name)
+        if n.value == 0:
+            return np.zeros(0, np.int64)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def boundary_program(self, level: int, field_type) -> np.ndarray:
+        ft = FIELD_TYPES[field_type] if isinstance(field_type, str) else int(field_type)
+        p = C.POINTER(BcAssign)()
+        n = C.c_int64()
+        _host_check(self._lib.artss_geom_boundary_program(self._h, level, ft, C.byref(p), C.byref(n)), "program")
+        if n.value == 0:
+            return np.zeros(0, BC_DTYPE)
+        raw = C.string_at(C.cast(p, C.c_void_p), n.value * C.sizeof(BcAssign))
+        return np.frombuffer(raw, dtype=BC_DTYPE).copy()
+
+    def grid_desc(self) -> GridDesc:
+        d = GridDesc()
+        _host_check(self._lib.artss_geom_grid_desc(self._h, C.byref(d)), "grid")
+        return d
+
+
+class Simulation:
+    """One ARTSS scene on a B200: ``Simulation(xml).run(steps)``."""
+
+    def __init__(self, xml_path: str, device: int = 0):
+        self._lib = load_host()
+        self._h = _P()
+        _host_check(self._lib.artss_sim_create(os.fsencode(xml_path), device, C.byref(self._h)), "simulation")
+        self.size = int(self._lib.artss_sim_field_size(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.artss_sim_destroy(self._h)
+            self._h = _P()
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, steps: int = -1) -> int:
+        done = C.c_int64()
+        _host_check(self._lib.artss_sim_run(self._h, steps, C.byref(done)), "run")
+        return done.value
+
+    @property
+    def finished(self) -> bool:
+        return bool(self._lib.artss_sim_finished(self._h))
+
+    @property
+    def time(self) -> float:
+        return self._lib.artss_sim_time(self._h)
+
+    @property
+    def step_index(self) -> int:
+        return self._lib.artss_sim_step_index(self._h)
+
+    @property
+    def inner_cells(self) -> int:
+        return self._lib.artss_sim_inner_cells(self._h)
+
+    @property
+    def context(self):
+        return self._lib.artss_sim_context(self._h)
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self.size, np.float64)
+        _host_check(self._lib.artss_sim_get_field(self._h, name.encode(), dptr(out), self.size), name)
+        return out
+
+    def set_field(self, name: str, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _host_check(self._lib.artss_sim_set_field(self._h, name.encode(), dptr(v), v.size), name)
+
+    def device_pointer(self, name: str) -> int:
+        p = self._lib.artss_sim_field_device(self._h, name.encode())
+        return C.cast(p, C.c_void_p).value or 0
+
+    def stats(self) -> Dict[str, object]:
+        it = (C.c_int64 * 4)()
+        cyc = C.c_int64()
+        res = C.c_double()
+        _host_check(self._lib.artss_sim_last_stats(self._h, it, C.byref(cyc), C.byref(res)), "stats")
+        return {"diffusion_iterations": list(it), "mg_cycles": cyc.value, "mg_residual": res.value}
+
+    def pressure(self, first_step: bool = True):
+        cyc = C.c_int64()
+        res = C.c_double()
+        _host_check(self._lib.artss_sim_pressure(self._h, 1 if first_step else 0, C.byref(cyc), C.byref(res)),
+                    "pressure")
+        return cyc.value, res.value
+
+    def kernel_launches(self) -> int:
+        return int(load_cuda().artss_ctx_kernel_launches(self.context))

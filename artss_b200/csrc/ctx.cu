@@ -1,0 +1,322 @@
+// Context, device memory, cell flags and whole-array field operations.
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+namespace artss {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t e, const char *what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? ARTSS_ERR_NOMEM
+         : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? ARTSS_ERR_NO_DEVICE
+         : ARTSS_ERR_CUDA;
+}
+
+int check_level(const artss_ctx *ctx, int level) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    if (level < 0 || level > ctx->grid.n_levels) {
+        set_error("level " + std::to_string(level) + " outside 0.." + std::to_string(ctx->grid.n_levels));
+        return ARTSS_ERR_ARG;
+    }
+    return ARTSS_OK;
+}
+
+int check_field_type(int ft) {
+    if (ft < 0 || ft >= kFieldTypes) { set_error("unknown field type " + std::to_string(ft)); return ARTSS_ERR_ARG; }
+    return ARTSS_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+
+__global__ void k_fill(double *__restrict__ f, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        f[i] = v;
+}
+
+__global__ void k_copy(double *__restrict__ d, const double *__restrict__ s, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        d[i] = s[i];
+}
+
+__global__ void k_add_field(double *__restrict__ d, const double *__restrict__ s, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        d[i] += s[i];
+}
+
+__global__ void k_add_scalar(double *__restrict__ d, double x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        d[i] += x;
+}
+
+__global__ void k_scale(double *__restrict__ d, double x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        d[i] *= x;
+}
+
+__global__ void k_scale_copy(double *__restrict__ d, const double *__restrict__ s, double x, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        d[i] = s[i] * x;
+}
+
+// a0 = a, a_tmp = a for up to three vectors in one pass (couple_vector).
+__global__ void k_couple3(const double *__restrict__ a, double *__restrict__ a0, double *__restrict__ at,
+                          const double *__restrict__ b, double *__restrict__ b0, double *__restrict__ bt,
+                          const double *__restrict__ c, double *__restrict__ c0, double *__restrict__ ct,
+                          int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        if (a) { const double x = a[i]; a0[i] = x; at[i] = x; }
+        if (b) { const double x = b[i]; b0[i] = x; bt[i] = x; }
+        if (c) { const double x = c[i]; c0[i] = x; ct[i] = x; }
+    }
+}
+
+// Mark the cells of a sorted index list with `bit`.
+__global__ void k_mark(uint8_t *__restrict__ flags, const int64_t *__restrict__ list, int64_t n, uint8_t bit) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        flags[list[i]] |= bit;
+}
+
+}  // namespace artss
+
+using namespace artss;
+
+extern "C" {
+
+const char *artss_last_error(void) { return g_last_error.c_str(); }
+
+int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
+    if (!grid || !out) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    *out = nullptr;
+    if (grid->n_levels < 0 || grid->n_levels > kMaxLevel) {
+        set_error("n_levels " + std::to_string(grid->n_levels) + " outside 0.." + std::to_string(kMaxLevel));
+        return ARTSS_ERR_LIMIT;
+    }
+    for (int l = 0; l <= grid->n_levels; l++) {
+        if (grid->Nx[l] < 3 || grid->Ny[l] < 3 || grid->Nz[l] < 3 ||
+            grid->i1[l] < 1 || grid->i2[l] > grid->Nx[l] - 2 || grid->i1[l] > grid->i2[l] ||
+            grid->j1[l] < 1 || grid->j2[l] > grid->Ny[l] - 2 || grid->j1[l] > grid->j2[l] ||
+            grid->k1[l] < 1 || grid->k2[l] > grid->Nz[l] - 2 || grid->k1[l] > grid->k2[l]) {
+            set_error("inconsistent grid description at level " + std::to_string(l));
+            return ARTSS_ERR_ARG;
+        }
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        set_error(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count 0"));
+        return ARTSS_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) { set_error("device ordinal out of range"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaSetDevice(device));
+    auto *ctx = new artss_ctx();
+    ctx->device = device;
+    ctx->grid = *grid;
+    for (int l = 0; l <= grid->n_levels; l++) {
+        ctx->lvl[l] = Level{grid->Nx[l], grid->Ny[l], grid->Nz[l], grid->i1[l], grid->i2[l],
+                            grid->j1[l], grid->j2[l], grid->k1[l], grid->k2[l]};
+    }
+    auto fail = [&](cudaError_t err, const char *what) {
+        int st = cuda_fail(err, what);
+        artss_ctx_destroy(ctx);
+        return st;
+    };
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaMalloc(&ctx->d_partials, kMaxPartials * sizeof(double))) != cudaSuccess) return fail(e, "partials");
+    if ((e = cudaMalloc(&ctx->d_loop, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "loop state");
+    if ((e = cudaMemset(ctx->d_loop, 0, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "loop state");
+    if ((e = cudaMallocHost(&ctx->h_loop, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "pinned loop state");
+    for (int l = 0; l <= grid->n_levels; l++) {
+        const int64_t n = ctx->lvl[l].size();
+        if ((e = cudaMalloc(&ctx->d_flags[l], n)) != cudaSuccess) return fail(e, "cell flags");
+        if ((e = cudaMemset(ctx->d_flags[l], 0, n)) != cudaSuccess) return fail(e, "cell flags");
+    }
+    *out = ctx;
+    return ARTSS_OK;
+}
+
+int artss_ctx_destroy(artss_ctx *ctx) {
+    if (!ctx) return ARTSS_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (double *f : ctx->fields) cudaFree(f);
+    for (int l = 0; l <= kMaxLevel; l++) {
+        if (ctx->d_flags[l]) cudaFree(ctx->d_flags[l]);
+        for (int t = 0; t < kFieldTypes; t++) {
+            BcProgram &p = ctx->bc[l][t];
+            cudaFree(p.d_target); cudaFree(p.d_root); cudaFree(p.d_depth); cudaFree(p.d_neg); cudaFree(p.d_value);
+        }
+    }
+    cudaFree(ctx->d_partials);
+    cudaFree(ctx->d_loop);
+    if (ctx->h_loop) cudaFreeHost(ctx->h_loop);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ARTSS_OK;
+}
+
+void *artss_ctx_stream(artss_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+int artss_ctx_sync(artss_ctx *ctx) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    return ARTSS_OK;
+}
+
+int64_t artss_ctx_kernel_launches(artss_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int64_t artss_field_size(artss_ctx *ctx, int level) {
+    if (check_level(ctx, level) != ARTSS_OK) return -1;
+    return ctx->lvl[level].size();
+}
+
+int artss_field_alloc(artss_ctx *ctx, int level, double **out) {
+    int st = check_level(ctx, level);
+    if (st) return st;
+    if (!out) { set_error("null output pointer"); return ARTSS_ERR_ARG; }
+    const int64_t n = ctx->lvl[level].size();
+    double *p = nullptr;
+    ARTSS_CK(cudaMalloc(&p, n * sizeof(double)));
+    cudaError_t e = cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+    if (e != cudaSuccess) { cudaFree(p); return cuda_fail(e, "field zero fill"); }
+    ctx->fields.insert(p);
+    *out = p;
+    return ARTSS_OK;
+}
+
+int artss_field_free(artss_ctx *ctx, double *field) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    auto it = ctx->fields.find(field);
+    if (it == ctx->fields.end()) { set_error("pointer is not a field of this context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    ARTSS_CK(cudaFree(field));
+    ctx->fields.erase(it);
+    return ARTSS_OK;
+}
+
+int artss_upload(artss_ctx *ctx, double *dst, const double *host, int64_t n) {
+    if (!ctx || !dst || !host || n < 0) { set_error("bad upload arguments"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    return ARTSS_OK;
+}
+
+int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n) {
+    if (!ctx || !src || !host || n < 0) { set_error("bad download arguments"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    return ARTSS_OK;
+}
+
+int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_t n_inner,
+                         const int64_t *domain, int64_t n_domain) {
+    int st = check_level(ctx, level);
+    if (st) return st;
+    if ((n_inner && !inner) || (n_domain && !domain) || n_inner < 0 || n_domain < 0) {
+        set_error("bad list arguments"); return ARTSS_ERR_ARG;
+    }
+    const Level &L = ctx->lvl[level];
+    // every inner cell must lie in the computational domain, every domain-list
+    // cell in the box one layer larger; lists are strictly ascending
+    auto check = [&](const int64_t *list, int64_t n, int64_t grow, const char *name) -> bool {
+        for (int64_t q = 0; q < n; q++) {
+            const int64_t idx = list[q];
+            if (idx < 0 || idx >= L.size() || (q && list[q - 1] >= idx)) {
+                set_error(std::string(name) + " list not ascending or out of range"); return false;
+            }
+            const int64_t k = idx / L.nxy(), j = (idx - k * L.nxy()) / L.Nx, i = idx - k * L.nxy() - j * L.Nx;
+            if (i < L.i1 - grow || i > L.i2 + grow || j < L.j1 - grow || j > L.j2 + grow ||
+                k < L.k1 - grow || k > L.k2 + grow) {
+                set_error(std::string(name) + " list cell outside its box"); return false;
+            }
+        }
+        return true;
+    };
+    if (!check(inner, n_inner, 0, "inner") || !check(domain, n_domain, 1, "domain")) return ARTSS_ERR_ARG;
+    int64_t *d_list = nullptr;
+    const int64_t nmax = std::max<int64_t>(std::max(n_inner, n_domain), 1);
+    ARTSS_CK(cudaMalloc(&d_list, nmax * sizeof(int64_t)));
+    cudaError_t e = cudaMemsetAsync(ctx->d_flags[level], 0, L.size(), ctx->stream);
+    if (e == cudaSuccess && n_inner) e = cudaMemcpyAsync(d_list, inner, n_inner * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && n_inner) {
+        k_mark<<<flat_blocks(n_inner), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_inner, kInner);
+        ctx->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && n_domain) e = cudaMemcpyAsync(d_list, domain, n_domain * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && n_domain) {
+        k_mark<<<flat_blocks(n_domain), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_domain, kDomain);
+        ctx->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_list);
+    if (e != cudaSuccess) return cuda_fail(e, "cell flags");
+    return ARTSS_OK;
+}
+
+int artss_get_cell_flags(artss_ctx *ctx, int level, uint8_t *host_out, int64_t n) {
+    int st = check_level(ctx, level);
+    if (st) return st;
+    if (!host_out || n != ctx->lvl[level].size()) { set_error("flag buffer size mismatch"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaMemcpyAsync(host_out, ctx->d_flags[level], n, cudaMemcpyDeviceToHost, ctx->stream));
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    return ARTSS_OK;
+}
+
+#define ARTSS_FIELD_OP(launch)                                        \
+    int st = check_level(ctx, level);                                 \
+    if (st) return st;                                                \
+    const int64_t n = ctx->lvl[level].size();                         \
+    launch;                                                           \
+    ARTSS_LAUNCH_CK(ctx);                                             \
+    return ARTSS_OK;
+
+int artss_fill(artss_ctx *ctx, double *f, int level, double value) {
+    if (!f) { set_error("null field"); return ARTSS_ERR_ARG; }
+    ARTSS_FIELD_OP((k_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(f, n, value)))
+}
+
+int artss_copy(artss_ctx *ctx, double *dst, const double *src, int level) {
+    if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
+    if (dst == src) return check_level(ctx, level);
+    ARTSS_FIELD_OP((k_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+}
+
+int artss_add_field(artss_ctx *ctx, double *dst, const double *src, int level) {
+    if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
+    ARTSS_FIELD_OP((k_add_field<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+}
+
+int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level) {
+    if (!dst) { set_error("null field"); return ARTSS_ERR_ARG; }
+    ARTSS_FIELD_OP((k_add_scalar<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
+}
+
+int artss_scale(artss_ctx *ctx, double *dst, double x, int level) {
+    if (!dst) { set_error("null field"); return ARTSS_ERR_ARG; }
+    ARTSS_FIELD_OP((k_scale<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
+}
+
+int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, int level) {
+    if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
+    ARTSS_FIELD_OP((k_scale_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, x, n)))
+}
+
+int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
+                 const double *b, double *b0, double *b_tmp,
+                 const double *c, double *c0, double *c_tmp) {
+    if ((a && (!a0 || !a_tmp)) || (b && (!b0 || !b_tmp)) || (c && (!c0 || !c_tmp))) {
+        set_error("couple: incomplete triple"); return ARTSS_ERR_ARG;
+    }
+    const int level = 0;
+    ARTSS_FIELD_OP((k_couple3<<<flat_blocks(n), 256, 0, ctx->stream>>>(a, a0, a_tmp, b, b0, b_tmp, c, c0, c_tmp, n)))
+}
+
+}  // extern "C"

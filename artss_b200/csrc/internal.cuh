@@ -1,0 +1,145 @@
+// Internal declarations shared by the translation units of libartss_cuda.so.
+// The arithmetic of every kernel reproduces the reference expression order
+// operation by operation; the library is compiled with --fmad=false so each
+// a*b+c rounds twice, as the reference serial build does.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <set>
+
+#include "../../include/artss_cuda.h"
+
+namespace artss {
+
+constexpr int kMaxLevel = ARTSS_MAX_LEVEL;
+constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
+constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
+constexpr int kReduceThreads = 256;
+constexpr int kMaxPartials = 4096;      // blocks of a reduction pass
+
+enum CellFlag : uint8_t { kInner = 1, kDomain = 2 };
+
+// Geometry of one multigrid level, passed to kernels by value.
+struct Level {
+    int64_t Nx, Ny, Nz;
+    int64_t i1, i2, j1, j2, k1, k2;  // computational-domain inner cells, inclusive
+    __host__ __device__ int64_t nxy() const { return Nx * Ny; }
+    __host__ __device__ int64_t size() const { return Nx * Ny * Nz; }
+};
+
+// Compiled boundary program of one (level, field type): `waves` groups of
+// assignments; within a group no assignment reads a cell another one writes.
+struct BcProgram {
+    bool present = false;
+    int waves = 0;
+    std::vector<int64_t> wave_begin;  // waves+1 offsets
+    int64_t n = 0;
+    int64_t *d_target = nullptr;
+    int64_t *d_root = nullptr;
+    uint8_t *d_depth = nullptr;
+    uint8_t *d_neg = nullptr;          // bit d: step d negates
+    double *d_value = nullptr;         // [kBcMaxDepth][n]
+};
+
+// Device-resident control block of one bounded iteration loop.
+struct LoopState {
+    double sum;        // reduction result of the last pass
+    double residual;   // sqrt(sum) (or caller-defined)
+    long long it;      // iterations done
+    int cond;          // loop continues
+    int pad;
+};
+
+}  // namespace artss
+
+struct artss_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    artss_grid_desc grid{};
+    artss::Level lvl[artss::kMaxLevel + 1]{};
+    uint8_t *d_flags[artss::kMaxLevel + 1]{};
+    artss::BcProgram bc[artss::kMaxLevel + 1][artss::kFieldTypes];
+    double *d_partials = nullptr;       // kMaxPartials doubles
+    artss::LoopState *d_loop = nullptr; // device loop blocks (16)
+    artss::LoopState *h_loop = nullptr; // pinned mirror
+    int64_t launches = 0;
+    std::set<double *> fields;
+};
+
+namespace artss {
+
+// thread-local error message of the last failing call
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define ARTSS_CK(call)                                                   \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) return artss::cuda_fail(e_, #call);       \
+    } while (0)
+
+#define ARTSS_LAUNCH_CK(ctx)                                             \
+    do {                                                                 \
+        (ctx)->launches++;                                               \
+        cudaError_t e_ = cudaGetLastError();                             \
+        if (e_ != cudaSuccess) return artss::cuda_fail(e_, "kernel launch"); \
+    } while (0)
+
+int check_level(const artss_ctx *ctx, int level);
+int check_field_type(int ft);
+
+// 3-D launch shape over an index box [x0..x1] x [y0..y1] x [z0..z1].
+struct Box3 {
+    int64_t x0, x1, y0, y1, z0, z1;
+    __host__ __device__ int64_t nx() const { return x1 - x0 + 1; }
+    __host__ __device__ int64_t ny() const { return y1 - y0 + 1; }
+    __host__ __device__ int64_t nz() const { return z1 - z0 + 1; }
+};
+constexpr int kBx = 64, kBy = 4;
+inline dim3 box_grid(const Box3 &b) {
+    return dim3((unsigned) ((b.nx() + kBx - 1) / kBx), (unsigned) ((b.ny() + kBy - 1) / kBy), (unsigned) b.nz());
+}
+inline dim3 box_block() { return dim3(kBx, kBy, 1); }
+inline Box3 inner_box(const Level &L) { return {L.i1, L.i2, L.j1, L.j2, L.k1, L.k2}; }
+inline Box3 domain_box(const Level &L) { return {L.i1 - 1, L.i2 + 1, L.j1 - 1, L.j2 + 1, L.k1 - 1, L.k2 + 1}; }
+
+// Grid-size helper for flat (1-D) loops over n elements.
+inline unsigned flat_blocks(int64_t n, int threads = 256) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return (unsigned) b;
+}
+
+// Boundary program execution (bc.cu).
+int apply_bc(artss_ctx *ctx, double *f, int level, int field_type);
+
+// Reductions (reduce.cu): sum of per-block partials -> loop state `slot`.
+//   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it
+int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it);
+int init_loop(artss_ctx *ctx, int slot, double residual0, long long it0, int cond0);
+int read_loop(artss_ctx *ctx, int slot, LoopState *out);
+// Plain sum of partials into loop slot (no iteration bookkeeping).
+int finalize_sum(artss_ctx *ctx, int slot, int nblocks);
+
+}  // namespace artss
+
+// Block-wide sum of one double per thread; result valid in thread 0.
+__device__ __forceinline__ double artss_block_sum(double v, double *smem) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int nwarps = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+    if (lane == 0) smem[warp] = v;
+    __syncthreads();
+    v = 0.0;
+    if (tid < 32) {
+        v = (tid < nwarps) ? smem[tid] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}

@@ -1,0 +1,63 @@
+// Deterministic two-pass reductions and the device-side loop-control block.
+//
+// Pass 1 (inside the stencil kernels): every block writes one partial sum to
+// ctx->d_partials[block].  Pass 2 (here, one block): partials are summed in a
+// fixed order, so a residual is reproducible run to run for a given launch
+// shape.  The loop block then holds what the reference keeps in host scalars
+// (`res`, `it`, the while-condition) of its bounded iteration loops, e.g.
+// ARTSS src/diffusion/ColoredGaussSeidelDiffuse.cpp:69-88.
+#include "internal.cuh"
+
+namespace artss {
+
+__global__ void k_finalize_loop(const double *__restrict__ partials, int nblocks, LoopState *__restrict__ st,
+                                double tol, long long max_it, int mode) {
+    __shared__ double smem[32];
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[b];
+    v = artss_block_sum(v, smem);
+    if (threadIdx.x == 0) {
+        st->sum = v;
+        if (mode == 0) {
+            const double r = sqrt(v);
+            st->residual = r;
+            st->it += 1;
+            st->cond = (r > tol && st->it < max_it) ? 1 : 0;
+        }
+    }
+}
+
+__global__ void k_init_loop(LoopState *st, double r0, long long it0, int cond0) {
+    st->sum = 0.0;
+    st->residual = r0;
+    st->it = it0;
+    st->cond = cond0;
+}
+
+int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it) {
+    k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, tol, max_it, 0);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int finalize_sum(artss_ctx *ctx, int slot, int nblocks) {
+    k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int init_loop(artss_ctx *ctx, int slot, double r0, long long it0, int cond0) {
+    k_init_loop<<<1, 1, 0, ctx->stream>>>(ctx->d_loop + slot, r0, it0, cond0);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int read_loop(artss_ctx *ctx, int slot, LoopState *out) {
+    ARTSS_CK(cudaMemcpyAsync(ctx->h_loop + slot, ctx->d_loop + slot, sizeof(LoopState), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    *out = ctx->h_loop[slot];
+    return ARTSS_OK;
+}
+
+}  // namespace artss

@@ -1,0 +1,527 @@
+// Level-0 plugin kernels: semi-Lagrangian advection, constant Smagorinsky,
+// divergence / projection, buoyancy and explicit-Euler sources, and the
+// colored Gauss-Seidel and Jacobi diffusion solvers.
+//
+// Iteration space: the reference loops over index lists (domain inner list,
+// domain list).  Here every kernel sweeps the computational-domain box of the
+// level in x-fastest order and tests the per-cell flags built from those same
+// lists, so the set of cells and the per-cell arithmetic are identical while
+// loads along x stay coalesced.  Threads own one (i, j) column and walk z in
+// strides of gridDim.z.
+#include "internal.cuh"
+
+namespace artss {
+
+// launch shape of box kernels: at most ~2048 blocks so that per-block partial
+// sums of a reduction fit ctx->d_partials
+inline dim3 zgrid(const Box3 &b) {
+    dim3 g = box_grid(b);
+    const int64_t xy = (int64_t) g.x * g.y;
+    int64_t gz = b.nz();
+    const int64_t cap = std::max<int64_t>(1, 2048 / std::max<int64_t>(xy, 1));
+    if (gz > cap) gz = cap;
+    g.z = (unsigned) std::max<int64_t>(gz, 1);
+    return g;
+}
+inline int nblocks(const dim3 &g) { return (int) (g.x * g.y * g.z); }
+
+#define ARTSS_COLUMN(box)                                                  \
+    const int64_t i = (box).x0 + (int64_t) blockIdx.x * blockDim.x + threadIdx.x; \
+    const int64_t j = (box).y0 + (int64_t) blockIdx.y * blockDim.y + threadIdx.y; \
+    const bool col = (i <= (box).x1) && (j <= (box).y1)
+
+__device__ __forceinline__ int block_linear() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
+
+// ------------------------------------------------------------ advection
+
+struct AdvCoef {
+    double dtx, dty, dtz;                 // dt/dx, dt/dy, dt/dz (SLAdvect.cpp:53-55)
+    int64_t is, ie, js, je, ks, ke;       // computational-domain inner index range
+};
+
+// Backtrace of SLAdvect.cpp:79-126 for one axis.
+__device__ __forceinline__ void sl_axis(double C, int64_t c, int64_t cs, int64_t ce,
+                                        int64_t &c0, int64_t &c1, double &r) {
+    const double eps = 1e-6;
+    c0 = c; c1 = c; r = 1.0;
+    if (C > eps) {
+        const int64_t t = c - (int64_t) C;
+        c0 = t > cs ? t : cs;
+        c1 = c0 - 1;
+        r = fmod(C, 1.0);
+    } else if (C < -eps) {
+        const int64_t t = c - (int64_t) C;
+        c0 = t < ce ? t : ce;
+        c1 = c0 + 1;
+        r = fmod(-C, 1.0);
+    }
+}
+
+// Trilinear blend of SLAdvect.cpp:131-162, same operation order.
+__device__ __forceinline__ double sl_interp(const double *__restrict__ in, int64_t Nx, int64_t nxy,
+                                            int64_t i0, int64_t i1, int64_t j0, int64_t j1, int64_t k0, int64_t k1,
+                                            double r, double s, double t) {
+    const double d000 = in[i0 + Nx * j0 + nxy * k0];
+    const double d100 = in[i1 + Nx * j0 + nxy * k0];
+    const double d010 = in[i0 + Nx * j1 + nxy * k0];
+    const double d110 = in[i1 + Nx * j1 + nxy * k0];
+    const double d001 = in[i0 + Nx * j0 + nxy * k1];
+    const double d101 = in[i1 + Nx * j0 + nxy * k1];
+    const double d011 = in[i0 + Nx * j1 + nxy * k1];
+    const double d111 = in[i1 + Nx * j1 + nxy * k1];
+    const double r100 = d000 + r * (d100 - d000);
+    const double r110 = d010 + r * (d110 - d010);
+    const double r101 = d001 + r * (d101 - d001);
+    const double r111 = d011 + r * (d111 - d011);
+    const double s110 = r100 + s * (r110 - r100);
+    const double s111 = r101 + s * (r111 - r101);
+    return s110 + t * (s111 - s110);
+}
+
+template <int NF>
+__global__ void k_advect(double *__restrict__ o0, double *__restrict__ o1, double *__restrict__ o2,
+                         const double *__restrict__ n0, const double *__restrict__ n1, const double *__restrict__ n2,
+                         const double *__restrict__ u, const double *__restrict__ v, const double *__restrict__ w,
+                         const uint8_t *__restrict__ flags, Level L, Box3 box, AdvCoef c) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int64_t nxy = L.nxy();
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t idx = i + L.Nx * j + nxy * k;
+        if (!(flags[idx] & kInner)) continue;
+        int64_t i0, i1, j0, j1, k0, k1;
+        double r, s, t;
+        sl_axis(c.dtx * u[idx], i, c.is, c.ie, i0, i1, r);
+        sl_axis(c.dty * v[idx], j, c.js, c.je, j0, j1, s);
+        sl_axis(c.dtz * w[idx], k, c.ks, c.ke, k0, k1, t);
+        o0[idx] = sl_interp(n0, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+        if (NF == 3) {
+            o1[idx] = sl_interp(n1, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+            o2[idx] = sl_interp(n2, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+        }
+    }
+}
+
+// ------------------------------------------------------------ turbulence
+
+// ConstSmagorinsky.cpp:60-80; cs2d2 = Cs * Cs * delta_s * delta_s (host).
+__global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict__ u, const double *__restrict__ v,
+                              const double *__restrict__ w, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                              double rdx, double rdy, double rdz, double cs2d2) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int64_t ni = 1, nj = L.Nx, nk = L.nxy();
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        const double S11 = (u[q + ni] - u[q - ni]) * 0.5 * rdx;
+        const double S22 = (v[q + nj] - v[q - nj]) * 0.5 * rdy;
+        const double S33 = (w[q + nk] - w[q - nk]) * 0.5 * rdz;
+        const double S12 = 0.5 * ((u[q + nj] - u[q - nj]) * 0.5 * rdy + (v[q + ni] - v[q - ni]) * 0.5 * rdx);
+        const double S13 = 0.5 * ((u[q + nk] - u[q - nk]) * 0.5 * rdz + (w[q + ni] - w[q - ni]) * 0.5 * rdx);
+        const double S23 = 0.5 * ((v[q + nk] - v[q - nk]) * 0.5 * rdz + (w[q + nj] - w[q - nj]) * 0.5 * rdy);
+        const double S_bar = sqrt(2. * (S11 * S11 + S22 * S22 + S33 * S33
+                                        + 2. * (S12 * S12) + 2. * (S13 * S13) + 2. * (S23 * S23)));
+        ev[q] = cs2d2 * S_bar;
+    }
+}
+
+// ------------------------------------------------------------ pressure coupling
+
+// IPressure.cpp:58-66; h* = 0.5 * (1/d*) (host)
+__global__ void k_divergence(double *__restrict__ out, const double *__restrict__ u, const double *__restrict__ v,
+                             const double *__restrict__ w, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                             double hx, double hy, double hz) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int64_t nj = L.Nx, nk = L.nxy();
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        const double a = hx * (u[q + 1] - u[q - 1]);
+        const double b = hy * (v[q + nj] - v[q - nj]);
+        const double c = hz * (w[q + nk] - w[q - nk]);
+        out[q] = a + b + c;
+    }
+}
+
+// zero the ghost ring of the computational domain (IPressure.cpp:69-104)
+__global__ void k_ghost_ring_zero(double *__restrict__ out, Level L, Box3 ring) {
+    ARTSS_COLUMN(ring);
+    if (!col) return;
+    for (int64_t k = ring.z0 + blockIdx.z; k <= ring.z1; k += gridDim.z) {
+        if (i == ring.x0 || i == ring.x1 || j == ring.y0 || j == ring.y1 || k == ring.z0 || k == ring.z1)
+            out[i + L.Nx * j + L.nxy() * k] = 0.0;
+    }
+}
+
+// IPressure.cpp:154-161
+__global__ void k_projection(double *__restrict__ ou, double *__restrict__ ov, double *__restrict__ ow,
+                             const double *__restrict__ us, const double *__restrict__ vs,
+                             const double *__restrict__ ws, const double *__restrict__ p,
+                             const uint8_t *__restrict__ flags, Level L, Box3 box, double hx, double hy, double hz) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int64_t nj = L.Nx, nk = L.nxy();
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        ou[q] = us[q] - hx * (p[q + 1] - p[q - 1]);
+        ov[q] = vs[q] - hy * (p[q + nj] - p[q - nj]);
+        ow[q] = ws[q] - hz * (p[q + nk] - p[q - nk]);
+    }
+}
+
+// ------------------------------------------------------------ sources
+
+// ISource.cpp:41-46 on the domain list; nbeta = -beta (host)
+__global__ void k_buoyancy(double *__restrict__ f, const double *__restrict__ T, const double *__restrict__ Ta,
+                           const uint8_t *__restrict__ flags, Level L, Box3 box, double nbeta, double g) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + L.nxy() * k;
+        if (!(flags[q] & kDomain)) continue;
+        f[q] = nbeta * (T[q] - Ta[q]) * g;
+    }
+}
+
+// ExplicitEulerSource.cpp:92-96
+__global__ void k_add_source(double *__restrict__ out, const double *__restrict__ S,
+                             const uint8_t *__restrict__ flags, Level L, Box3 box, double dt) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + L.nxy() * k;
+        if (!(flags[q] & kInner)) continue;
+        out[q] += dt * S[q];
+    }
+}
+
+// ------------------------------------------------------------ diffusion
+
+struct DiffCoef {
+    double ax, ay, az;         // laminar alphas  D*dt/dx^2 ... (ColoredGaussSeidelDiffuse.cpp:56-58)
+    double beta;               // 1/(1 + 2 sum alpha)
+    double rbeta;              // 1 + 2 sum alpha
+    double dsign, w, omw;      // sign of b, relaxation weight, (1 - w)
+    double D, dt, rdx, rdy, rdz;  // turbulent variant: alphas from D + EV per cell
+};
+
+// alpha / beta of the turbulent variant (ColoredGaussSeidelDiffuse.cpp:248-253)
+__device__ __forceinline__ void turb_alpha(const DiffCoef &c, double ev, double &ax, double &ay, double &az,
+                                           double &rb) {
+    ax = (c.D + ev) * c.dt * c.rdx * c.rdx;
+    ay = (c.D + ev) * c.dt * c.rdy * c.rdy;
+    az = (c.D + ev) * c.dt * c.rdz * c.rdz;
+    rb = (1. + 2. * (ax + ay + az));
+}
+
+// One colour of a colored Gauss-Seidel sweep (stencil at
+// ColoredGaussSeidelDiffuse.cpp:316-341), in place on `out`; also writes the
+// block partial of sum (rbeta * (new - old))^2, the convergence measure of
+// ColoredGaussSeidelDiffuse.cpp:77-85.
+template <bool TURB>
+__global__ void k_cgs_color(double *__restrict__ out, const double *__restrict__ b, const double *__restrict__ ev,
+                            const uint8_t *__restrict__ flags, Level L, Box3 box, int color, DiffCoef c,
+                            double *__restrict__ partials) {
+    __shared__ double smem[32];
+    ARTSS_COLUMN(box);
+    const int64_t nj = L.Nx, nk = L.nxy();
+    double acc = 0.0;
+    if (col) {
+        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+            if (((i + j + k) & 1) != color) continue;
+            const int64_t q = i + L.Nx * j + nk * k;
+            if (!(flags[q] & kInner)) continue;
+            double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+            if (TURB) {
+                turb_alpha(c, ev[q], ax, ay, az, rb);
+                beta = 1. / rb;
+            }
+            const double xp = out[q + 1], xm = out[q - 1];
+            const double yp = out[q + nj], ym = out[q - nj];
+            const double zp = out[q + nk], zm = out[q - nk];
+            const double old = out[q];
+            const double out_h = beta * (c.dsign * b[q] + ax * (xp + xm) + ay * (yp + ym) + az * (zp + zm));
+            const double nw = c.omw * old + c.w * out_h;
+            out[q] = nw;
+            const double res = rb * (nw - old);
+            acc += res * res;
+        }
+    }
+    acc = artss_block_sum(acc, smem);
+    if (partials && threadIdx.x == 0 && threadIdx.y == 0) partials[block_linear()] = acc;
+}
+
+// One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
+// the division by reciprocal_beta; turbulent: :345-362) + residual partials
+// of sum (rbeta * (out - in))^2 (:72-79).
+template <bool TURB>
+__global__ void k_jacobi_diffuse(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
+                                 const double *__restrict__ ev, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                                 DiffCoef c, double *__restrict__ partials) {
+    __shared__ double smem[32];
+    ARTSS_COLUMN(box);
+    const int64_t nj = L.Nx, nk = L.nxy();
+    double acc = 0.0;
+    if (col) {
+        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+            const int64_t q = i + L.Nx * j + nk * k;
+            if (!(flags[q] & kInner)) continue;
+            double out_h, rb;
+            if (TURB) {
+                double ax, ay, az;
+                turb_alpha(c, ev[q], ax, ay, az, rb);
+                const double bb = 1. / rb;
+                const double d_ax = ax * (in[q + 1] + in[q - 1]);
+                const double d_ay = ay * (in[q + nj] + in[q - nj]);
+                const double d_az = az * (in[q + nk] + in[q - nk]);
+                out_h = bb * (c.dsign * b[q] + d_ax + d_ay + d_az);
+            } else {
+                rb = c.rbeta;
+                out_h = (c.dsign * b[q] + c.ax * (in[q + 1] + in[q - 1]) + c.ay * (in[q + nj] + in[q - nj])
+                         + c.az * (in[q + nk] + in[q - nk])) / c.rbeta;
+            }
+            const double nw = c.omw * in[q] + c.w * out_h;
+            out[q] = nw;
+            const double res = rb * (nw - in[q]);
+            acc += res * res;
+        }
+    }
+    acc = artss_block_sum(acc, smem);
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[block_linear()] = acc;
+}
+
+// in = out over the domain list (JacobiDiffuse.cpp:85-89)
+__global__ void k_copy_domain(double *__restrict__ dst, const double *__restrict__ src,
+                              const uint8_t *__restrict__ flags, Level L, Box3 box) {
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t q = i + L.Nx * j + L.nxy() * k;
+        if (flags[q] & kDomain) dst[q] = src[q];
+    }
+}
+
+int check_field_args(artss_ctx *ctx, std::initializer_list<const void *> ptrs) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    for (const void *p : ptrs)
+        if (!p) { set_error("null field pointer"); return ARTSS_ERR_ARG; }
+    return ARTSS_OK;
+}
+
+DiffCoef diff_coef(const artss_ctx *ctx, double D, double dt, double w, double dsign) {
+    // ColoredGaussSeidelDiffuse.cpp:49-62 / JacobiDiffuse.cpp:46-60, level 0
+    DiffCoef c{};
+    const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
+    c.rdx = 1. / dx;
+    c.rdy = 1. / dy;
+    c.rdz = 1. / dz;
+    c.ax = D * dt * c.rdx * c.rdx;
+    c.ay = D * dt * c.rdy * c.rdy;
+    c.az = D * dt * c.rdz * c.rdz;
+    c.rbeta = (1. + 2. * (c.ax + c.ay + c.az));
+    c.beta = 1. / c.rbeta;
+    c.dsign = dsign;
+    c.w = w;
+    c.omw = 1 - w;
+    c.D = D;
+    c.dt = dt;
+    return c;
+}
+
+}  // namespace artss
+
+using namespace artss;
+
+extern "C" {
+
+int artss_advect_sl(artss_ctx *ctx, double *out, const double *in, const double *u, const double *v,
+                    const double *w, double dt, int out_field_type) {
+    int st = check_field_args(ctx, {out, in, u, v, w});
+    if (st || (st = check_field_type(out_field_type))) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
+    const dim3 g = zgrid(box);
+    k_advect<1><<<g, box_block(), 0, ctx->stream>>>(out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
+                                                    ctx->d_flags[0], L, box, c);
+    ARTSS_LAUNCH_CK(ctx);
+    return apply_bc(ctx, out, 0, out_field_type);
+}
+
+int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *out_w, const double *in_u,
+                        const double *in_v, const double *in_w, const double *u, const double *v, const double *w,
+                        double dt) {
+    int st = check_field_args(ctx, {out_u, out_v, out_w, in_u, in_v, in_w, u, v, w});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
+    const dim3 g = zgrid(box);
+    k_advect<3><<<g, box_block(), 0, ctx->stream>>>(out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
+                                                    ctx->d_flags[0], L, box, c);
+    ARTSS_LAUNCH_CK(ctx);
+    if ((st = apply_bc(ctx, out_u, 0, ARTSS_FIELD_U))) return st;
+    if ((st = apply_bc(ctx, out_v, 0, ARTSS_FIELD_V))) return st;
+    return apply_bc(ctx, out_w, 0, ARTSS_FIELD_W);
+}
+
+int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t, const double *u, const double *v, const double *w,
+                                 double cs) {
+    int st = check_field_args(ctx, {nu_t, u, v, w});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
+    const double delta_s = cbrt(dx * dy * dz);
+    const double cs2d2 = cs * cs * delta_s * delta_s;
+    k_smagorinsky<<<zgrid(box), box_block(), 0, ctx->stream>>>(nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
+                                                               1. / dy, 1. / dz, cs2d2);
+    ARTSS_LAUNCH_CK(ctx);
+    return apply_bc(ctx, nu_t, 0, ARTSS_FIELD_NU);
+}
+
+int artss_divergence(artss_ctx *ctx, double *rhs, const double *u, const double *v, const double *w) {
+    int st = check_field_args(ctx, {rhs, u, v, w});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const double hx = 0.5 * (1. / ctx->grid.dx[0]);
+    const double hy = 0.5 * (1. / ctx->grid.dy[0]);
+    const double hz = 0.5 * (1. / ctx->grid.dz[0]);
+    k_divergence<<<zgrid(box), box_block(), 0, ctx->stream>>>(rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz);
+    ARTSS_LAUNCH_CK(ctx);
+    const Box3 ring = domain_box(L);
+    k_ghost_ring_zero<<<zgrid(ring), box_block(), 0, ctx->stream>>>(rhs, L, ring);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int artss_projection(artss_ctx *ctx, double *u, double *v, double *w, const double *us, const double *vs,
+                     const double *ws, const double *p) {
+    int st = check_field_args(ctx, {u, v, w, us, vs, ws, p});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const double hx = 0.5 * (1. / ctx->grid.dx[0]);
+    const double hy = 0.5 * (1. / ctx->grid.dy[0]);
+    const double hz = 0.5 * (1. / ctx->grid.dz[0]);
+    k_projection<<<zgrid(box), box_block(), 0, ctx->stream>>>(u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
+                                                              hy, hz);
+    ARTSS_LAUNCH_CK(ctx);
+    if ((st = apply_bc(ctx, u, 0, ARTSS_FIELD_U))) return st;
+    if ((st = apply_bc(ctx, v, 0, ARTSS_FIELD_V))) return st;
+    return apply_bc(ctx, w, 0, ARTSS_FIELD_W);
+}
+
+int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const double *Ta, double beta, double g) {
+    int st = check_field_args(ctx, {force, T, Ta});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = domain_box(L);
+    k_buoyancy<<<zgrid(box), box_block(), 0, ctx->stream>>>(force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, int field_type) {
+    int st = check_field_args(ctx, {out, S});
+    if (st || (st = check_field_type(field_type))) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    k_add_source<<<zgrid(box), box_block(), 0, ctx->stream>>>(out, S, ctx->d_flags[0], L, box, dt);
+    ARTSS_LAUNCH_CK(ctx);
+    return apply_bc(ctx, out, 0, field_type);
+}
+
+int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
+                      double dt, int field_type, const artss_iter_cfg *cfg, int in_is_scratch,
+                      artss_iter_stats *stats) {
+    int st = check_field_args(ctx, {out, in, b, cfg});
+    if (st || (st = check_field_type(field_type))) return st;
+    if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const dim3 g = zgrid(box);
+    const int nb = nblocks(g);
+    const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
+    // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
+    if ((st = artss_copy(ctx, out, in, 0))) return st;
+    const int slot = 0;
+    // while (res > tol_res && it < max_iter), res starts at 1
+    long long it = 0;
+    double res = 1.;
+    bool cond = res > cfg->tol_res && it < cfg->max_iter;
+    if ((st = init_loop(ctx, slot, res, 0, cond ? 1 : 0))) return st;
+    LoopState ls{};
+    while (cond) {
+        if (!in_is_scratch && (st = artss_copy(ctx, in, out, 0))) return st;
+        if (ev) {
+            k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 0, c,
+                                                                  ctx->d_partials);
+            ARTSS_LAUNCH_CK(ctx);
+            k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 1, c,
+                                                                  ctx->d_partials + nb);
+        } else {
+            k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 0, c,
+                                                                   ctx->d_partials);
+            ARTSS_LAUNCH_CK(ctx);
+            k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 1, c,
+                                                                   ctx->d_partials + nb);
+        }
+        ARTSS_LAUNCH_CK(ctx);
+        if ((st = apply_bc(ctx, out, 0, field_type))) return st;
+        if ((st = finalize_loop(ctx, slot, 2 * nb, cfg->tol_res, cfg->max_iter))) return st;
+        if ((st = read_loop(ctx, slot, &ls))) return st;
+        it = ls.it;
+        res = ls.residual;
+        cond = ls.cond != 0;
+    }
+    if (stats) { stats->iterations = it; stats->residual = res; }
+    return ARTSS_OK;
+}
+
+int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
+                         double dt, int field_type, const artss_iter_cfg *cfg, artss_iter_stats *stats) {
+    int st = check_field_args(ctx, {out, in, b, cfg});
+    if (st || (st = check_field_type(field_type))) return st;
+    if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const Box3 dbox = domain_box(L);
+    const dim3 g = zgrid(box);
+    const int nb = nblocks(g);
+    const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
+    const int slot = 0;
+    long long it = 0;
+    double res = 1.;
+    bool cond = res > cfg->tol_res && it < cfg->max_iter;
+    if ((st = init_loop(ctx, slot, res, 0, cond ? 1 : 0))) return st;
+    LoopState ls{};
+    while (cond) {
+        if (ev) {
+            k_jacobi_diffuse<true><<<g, box_block(), 0, ctx->stream>>>(out, in, b, ev, ctx->d_flags[0], L, box, c,
+                                                                       ctx->d_partials);
+        } else {
+            k_jacobi_diffuse<false><<<g, box_block(), 0, ctx->stream>>>(out, in, b, nullptr, ctx->d_flags[0], L, box,
+                                                                        c, ctx->d_partials);
+        }
+        ARTSS_LAUNCH_CK(ctx);
+        if ((st = apply_bc(ctx, out, 0, field_type))) return st;
+        if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
+        k_copy_domain<<<zgrid(dbox), box_block(), 0, ctx->stream>>>(in, out, ctx->d_flags[0], L, dbox);
+        ARTSS_LAUNCH_CK(ctx);
+        if ((st = read_loop(ctx, slot, &ls))) return st;
+        it = ls.it;
+        res = ls.residual;
+        cond = ls.cond != 0;
+    }
+    // the final odd-count copy of JacobiDiffuse.cpp:92-99 repeats the last
+    // in = out over the domain list and changes nothing
+    if (stats) { stats->iterations = it; stats->residual = res; }
+    return ARTSS_OK;
+}
+
+}  // extern "C"

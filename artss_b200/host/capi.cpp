@@ -1,0 +1,228 @@
+// extern "C" surface of the host runtime (include/artss_host.h).
+#include "../../include/artss_host.h"
+
+#include <map>
+#include <memory>
+#include <string>
+
+#include "solvers.h"
+
+using namespace artss;
+
+struct artss_geom {
+    settings::Settings settings;
+    std::unique_ptr<Geometry> geo;
+    std::map<std::pair<int, int>, std::vector<BcAssign>> programs;
+};
+
+struct artss_sim {
+    std::unique_ptr<Runtime> rt;
+    std::unique_ptr<SolverController> sc;
+    std::unique_ptr<TimeIntegration> ti;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const config_error &e) {
+        g_err = std::string("config error: ") + e.what();
+        return ARTSS_ERR_ARG;
+    } catch (const cuda_error &e) {
+        g_err = e.what();
+        return ARTSS_ERR_CUDA;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return ARTSS_ERR_STATE;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *artss_host_last_error(void) { return g_err.c_str(); }
+
+int artss_geom_create(const char *xml_path, artss_geom **out) {
+    return guarded([&] {
+        if (!xml_path || !out) throw std::invalid_argument("null argument");
+        auto g = std::make_unique<artss_geom>();
+        g->settings = settings::parse_settings_file(xml_path);
+        g->geo = std::make_unique<Geometry>(g->settings);
+        *out = g.release();
+        return ARTSS_OK;
+    });
+}
+
+void artss_geom_destroy(artss_geom *g) { delete g; }
+
+int artss_geom_levels(artss_geom *g) { return g ? (int) g->geo->levels() : -1; }
+
+int artss_geom_obstacles(artss_geom *g) { return g ? (int) g->geo->obstacle_count() : -1; }
+
+int artss_geom_list(artss_geom *g, const char *name, int level, const int64_t **data, int64_t *n) {
+    return guarded([&] {
+        if (!g || !name || !data || !n) throw std::invalid_argument("null argument");
+        if (level < 0 || (size_t) level > g->geo->levels()) throw std::invalid_argument("level out of range");
+        const std::string s(name);
+        const IdxList *L = nullptr;
+        if (s == "inner") L = &g->geo->inner(level);
+        else if (s == "domain") L = &g->geo->domain(level);
+        else if (s == "obst") L = &g->geo->obstacle_cells(level);
+        else {
+            for (int p = 0; p < kPatches && !L; p++) {
+                if (s == std::string("bnd_") + kPatchNames[p]) L = &g->geo->boundary(level, p);
+                for (size_t id = 0; id < g->geo->obstacle_count() && !L; id++)
+                    if (s == "obst" + std::to_string(id) + "_" + kPatchNames[p]) L = &g->geo->obstacle(level, id).patch[p];
+            }
+        }
+        if (!L) throw std::invalid_argument("unknown list '" + s + "'");
+        *data = L->data();
+        *n = (int64_t) L->size();
+        return ARTSS_OK;
+    });
+}
+
+int artss_geom_dims(artss_geom *g, int level, int64_t *dims3) {
+    return guarded([&] {
+        if (!g || !dims3 || level < 0 || (size_t) level > g->geo->levels()) throw std::invalid_argument("bad argument");
+        const GridLevel &L = g->geo->grid().level(level);
+        for (int a = 0; a < 3; a++) dims3[a] = (int64_t) L.N[a];
+        return ARTSS_OK;
+    });
+}
+
+int artss_geom_boundary_program(artss_geom *g, int level, int field_type, const artss_bc_assign **ops, int64_t *n) {
+    return guarded([&] {
+        if (!g || !ops || !n || level < 0 || (size_t) level > g->geo->levels() || field_type < 0 ||
+            field_type >= kFieldTypesHost)
+            throw std::invalid_argument("bad argument");
+        auto key = std::make_pair(level, field_type);
+        auto it = g->programs.find(key);
+        if (it == g->programs.end())
+            it = g->programs.emplace(key, g->geo->has_boundary(field_type)
+                                              ? g->geo->boundary_program((size_t) level, field_type)
+                                              : std::vector<BcAssign>{}).first;
+        *ops = reinterpret_cast<const artss_bc_assign *>(it->second.data());
+        *n = (int64_t) it->second.size();
+        return ARTSS_OK;
+    });
+}
+
+int artss_geom_grid_desc(artss_geom *g, artss_grid_desc *out) {
+    return guarded([&] {
+        if (!g || !out) throw std::invalid_argument("null argument");
+        *out = grid_descriptor(*g->geo);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_create(const char *xml_path, int device, artss_sim **out) {
+    return guarded([&] {
+        if (!xml_path || !out) throw std::invalid_argument("null argument");
+        auto s = std::make_unique<artss_sim>();
+        settings::Settings st = settings::parse_settings_file(xml_path);
+        s->rt = std::make_unique<Runtime>(st, device);
+        s->sc = std::make_unique<SolverController>(*s->rt);
+        s->ti = std::make_unique<TimeIntegration>(*s->rt, *s->sc);
+        check(artss_ctx_sync(s->rt->ctx()), "set-up");
+        *out = s.release();
+        return ARTSS_OK;
+    });
+}
+
+void artss_sim_destroy(artss_sim *s) {
+    if (!s) return;
+    try {
+        s->ti.reset();
+        s->sc.reset();
+        s->rt.reset();
+    } catch (...) {
+    }
+    delete s;
+}
+
+int artss_sim_run(artss_sim *s, int64_t steps, int64_t *done) {
+    return guarded([&] {
+        if (!s) throw std::invalid_argument("null simulation");
+        int64_t d = s->ti->run(steps);
+        check(artss_ctx_sync(s->rt->ctx()), "run");
+        if (done) *done = d;
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_finished(artss_sim *s) { return s ? (s->ti->finished() ? 1 : 0) : -1; }
+double artss_sim_time(artss_sim *s) { return s ? s->ti->time() : -1.0; }
+int64_t artss_sim_step_index(artss_sim *s) { return s ? s->ti->step_index() : -1; }
+int64_t artss_sim_inner_cells(artss_sim *s) { return s ? (int64_t) s->rt->geometry().inner(0).size() : -1; }
+int64_t artss_sim_field_size(artss_sim *s) { return s ? (int64_t) s->rt->level(0).size() : -1; }
+artss_ctx *artss_sim_context(artss_sim *s) { return s ? s->rt->ctx() : nullptr; }
+
+double *artss_sim_field_device(artss_sim *s, const char *name) {
+    if (!s || !name) return nullptr;
+    Field *f = s->sc->fields().by_name(name);
+    return f ? f->data : nullptr;
+}
+
+int artss_sim_get_field(artss_sim *s, const char *name, double *host, int64_t n) {
+    return guarded([&] {
+        if (!s || !name || !host) throw std::invalid_argument("null argument");
+        Field *f = s->sc->fields().by_name(name);
+        if (!f) throw std::invalid_argument(std::string("unknown field ") + name);
+        if ((size_t) n != f->get_size()) throw std::invalid_argument("size mismatch");
+        check(artss_download(s->rt->ctx(), host, f->data, n), "get_field");
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_set_field(artss_sim *s, const char *name, const double *host, int64_t n) {
+    return guarded([&] {
+        if (!s || !name || !host) throw std::invalid_argument("null argument");
+        Field *f = s->sc->fields().by_name(name);
+        if (!f) throw std::invalid_argument(std::string("unknown field ") + name);
+        if ((size_t) n != f->get_size()) throw std::invalid_argument("size mismatch");
+        check(artss_upload(s->rt->ctx(), f->data, host, n), "set_field");
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_last_stats(artss_sim *s, int64_t *diff_iters4, int64_t *mg_cycles, double *mg_residual) {
+    return guarded([&] {
+        if (!s) throw std::invalid_argument("null simulation");
+        auto *ns = dynamic_cast<NSTempTurbSolver *>(&s->sc->solver());
+        if (!ns) throw std::invalid_argument("statistics are kept by NSTempTurbSolver scenes");
+        if (diff_iters4)
+            for (int k = 0; k < 4; k++) diff_iters4[k] = ns->stats.diffusion_iterations[k];
+        if (mg_cycles) *mg_cycles = ns->stats.pressure_cycles;
+        if (mg_residual) *mg_residual = ns->stats.pressure_residual;
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_pressure(artss_sim *s, int first_step, int64_t *cycles, double *residual) {
+    return guarded([&] {
+        if (!s) throw std::invalid_argument("null simulation");
+        auto *ps = dynamic_cast<PressureSolver *>(&s->sc->solver());
+        if (!ps) throw std::invalid_argument("not a PressureSolver scene");
+        const real dt = s->rt->dt();
+        ps->pressure().pressure(s->sc->fields().p, s->sc->fields().rhs, first_step ? dt : 2 * dt, false);
+        check(artss_ctx_sync(s->rt->ctx()), "pressure");
+        if (cycles) *cycles = ps->pressure().last_cycles;
+        if (residual) *residual = ps->pressure().last_residual;
+        return ARTSS_OK;
+    });
+}
+
+artss_mg *artss_sim_mg(artss_sim *s) {
+    if (!s) return nullptr;
+    if (auto *ps = dynamic_cast<PressureSolver *>(&s->sc->solver()))
+        if (auto *mg = dynamic_cast<VCycleMG *>(&ps->pressure())) return mg->handle();
+    return nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,381 @@
+#include "solvers.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace artss {
+
+// ---------------------------------------------------------------- factory
+
+std::unique_ptr<IAdvection> make_advection(Runtime &rt, const settings::Advection &s) {
+    if (s.type == "SemiLagrangian") return std::make_unique<SLAdvect>(rt);
+    throw config_error("advection method '" + s.type + "' is not implemented");
+}
+
+std::unique_ptr<IDiffusion> make_diffusion(Runtime &rt, const settings::Diffusion &s) {
+    if (s.type == "ColoredGaussSeidel") return std::make_unique<ColoredGaussSeidelDiffuse>(rt, s);
+    if (s.type == "Jacobi") return std::make_unique<JacobiDiffuse>(rt, s);
+    throw config_error("diffusion method '" + s.type + "' is not implemented");
+}
+
+std::unique_ptr<ITurbulence> make_turbulence(Runtime &rt, const settings::Turbulence &s) {
+    if (s.type == "ConstSmagorinsky") return std::make_unique<ConstSmagorinsky>(rt, s.cs);
+    throw config_error("turbulence method '" + s.type + "' is not implemented");
+}
+
+std::unique_ptr<IPressure> make_pressure(Runtime &rt, const settings::Pressure &s) {
+    if (s.type == "VCycleMG") return std::make_unique<VCycleMG>(rt, s);
+    throw config_error("pressure method '" + s.type + "' is not implemented");
+}
+
+std::unique_ptr<ISource> make_source(Runtime &rt, const std::string &type, const std::vector<int> &dir) {
+    if (type == "ExplicitEuler") return std::make_unique<ExplicitEulerSource>(rt, dir);
+    throw config_error("source method '" + type + "' is not implemented");
+}
+
+static std::unique_ptr<ISourceFunction> make_temperature_source_function(Runtime &rt,
+                                                                          const settings::TemperatureSource &s) {
+    // SolverSelection::set_temperature_source_function (src/solver/SolverSelection.cpp:165-212)
+    if (s.temp_fct == "Gauss") {
+        auto g = std::make_unique<GaussFunction>(rt, s.gauss);
+        if (s.random) {
+            const auto &r = s.random_parameters;
+            if (!r.custom_seed)
+                throw config_error("a temperature-source noise without custom_seed is not reproducible");
+            g->set_noise(std::make_unique<UniformRandom>(r.range, r.step_size, r.seed), r.absolute);
+        }
+        return g;
+    }
+    if (s.temp_fct == "Zero") return std::make_unique<ZeroSource>();
+    throw config_error("temperature source function '" + s.temp_fct + "' is not implemented");
+}
+
+// ---------------------------------------------------------------- fields
+
+FieldController::FieldController(Runtime &rt)
+    : u(rt, F_U), v(rt, F_V), w(rt, F_W), u0(rt, F_U), v0(rt, F_V), w0(rt, F_W), u_tmp(rt, F_U), v_tmp(rt, F_V),
+      w_tmp(rt, F_W), nu_t(rt, F_NU), kappa_t(rt, F_T), p(rt, F_P), p0(rt, F_P), rhs(rt, F_P), T(rt, F_T),
+      T0(rt, F_T), T_tmp(rt, F_T), T_ambient(rt, F_T), f_x(rt, F_U), f_y(rt, F_V), f_z(rt, F_W), S_T(rt, F_T),
+      m_rt(rt) {}
+
+void FieldController::set_up_boundary() {
+    // FieldController::set_up_boundary (src/field/FieldController.cpp:102-112); the
+    // concentration field is all zero on this path and carries no boundary data
+    m_rt.apply_boundary(u);
+    m_rt.apply_boundary(v);
+    m_rt.apply_boundary(w);
+    m_rt.apply_boundary(p);
+    m_rt.apply_boundary(T);
+    m_rt.apply_boundary(T_ambient);
+}
+
+void FieldController::update_data() {
+    // FieldController::update_data (src/field/FieldController.cpp:119-135)
+    couple_vector(u, u0, u_tmp, v, v0, v_tmp, w, w0, w_tmp);
+    p0.copy_data(p);
+    couple_scalar(T, T0, T_tmp);
+}
+
+void FieldController::couple_vector(const Field &a, Field &a0, Field &a_tmp, const Field &b, Field &b0, Field &b_tmp,
+                                    const Field &c, Field &c0, Field &c_tmp) {
+    check(artss_couple(a.runtime().ctx(), a.data, a0.data, a_tmp.data, b.data, b0.data, b_tmp.data, c.data, c0.data,
+                       c_tmp.data),
+          "couple_vector");
+}
+
+void FieldController::couple_scalar(const Field &a, Field &a0, Field &a_tmp) {
+    check(artss_couple(a.runtime().ctx(), a.data, a0.data, a_tmp.data, nullptr, nullptr, nullptr, nullptr, nullptr,
+                       nullptr),
+          "couple_scalar");
+}
+
+Field *FieldController::by_name(const std::string &n) {
+    if (n == "u") return &u;
+    if (n == "v") return &v;
+    if (n == "w") return &w;
+    if (n == "u0") return &u0;
+    if (n == "v0") return &v0;
+    if (n == "w0") return &w0;
+    if (n == "u_tmp") return &u_tmp;
+    if (n == "v_tmp") return &v_tmp;
+    if (n == "w_tmp") return &w_tmp;
+    if (n == "nu_t") return &nu_t;
+    if (n == "kappa_t") return &kappa_t;
+    if (n == "p") return &p;
+    if (n == "p0") return &p0;
+    if (n == "rhs") return &rhs;
+    if (n == "T") return &T;
+    if (n == "T0") return &T0;
+    if (n == "T_tmp") return &T_tmp;
+    if (n == "T_a") return &T_ambient;
+    if (n == "f_x") return &f_x;
+    if (n == "f_y") return &f_y;
+    if (n == "f_z") return &f_z;
+    if (n == "S_T") return &S_T;
+    return nullptr;
+}
+
+// ---------------------------------------------------------------- NSTempTurbSolver
+
+NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc) : m_rt(rt), m_fc(fc) {
+    const settings::Solver &s = rt.settings().solver;
+    adv_vel = make_advection(rt, s.advection);
+    adv_temp = make_advection(rt, s.temperature.advection);
+    dif_vel = make_diffusion(rt, s.diffusion);
+    mu_tub = make_turbulence(rt, s.turbulence);
+    dif_temp = make_diffusion(rt, s.diffusion);  // NSTempTurbSolver.cpp:45: the velocity settings
+    pres = make_pressure(rt, s.pressure);
+    sou_vel = make_source(rt, s.source.type, s.source.dir);
+    sou_temp = make_source(rt, s.temperature.source.type, s.temperature.source.dir);
+    m_source_function_temperature = make_temperature_source_function(rt, s.temperature.source);
+    m_add_source = s.source.force_fct != "Zero";
+    m_add_temp_source = s.temperature.source.temp_fct != "Zero";
+    // NSTempTurbSolver::control (:254-298)
+    auto sorted = [](std::vector<int> v) { std::sort(v.begin(), v.end()); return v; };
+    if (sorted(s.advection.fields) != std::vector<int>{F_U, F_V, F_W} ||
+        sorted(s.diffusion.fields) != std::vector<int>{F_U, F_V, F_W} ||
+        s.temperature.advection.fields != std::vector<int>{F_T} ||
+        s.temperature.diffusion.fields != std::vector<int>{F_T} || s.pressure.field != F_P)
+        throw config_error("Fields not specified correctly!");
+    if (s.temperature.source.dissipation)
+        throw config_error("temperature dissipation is not part of the fractional-step path implemented here");
+    // `in` of every diffuse() call below is re-coupled before it is read again
+    dif_vel->in_is_scratch = true;
+    dif_temp->in_is_scratch = true;
+}
+
+void NSTempTurbSolver::do_step(real t, bool sync) {
+    FieldController &f = m_fc;
+    const auto &phys = m_rt.settings().physical;
+    const real nu = phys.nu.value();
+    const real kappa = phys.kappa.value();
+
+    // 1. advection of velocity with the old velocity (:129-131)
+    if (auto *sl = dynamic_cast<SLAdvect *>(adv_vel.get())) {
+        sl->advect_vector(f.u, f.v, f.w, f.u0, f.v0, f.w0, f.u0, f.v0, f.w0);
+    } else {
+        adv_vel->advect(f.u, f.u0, f.u0, f.v0, f.w0, sync);
+        adv_vel->advect(f.v, f.v0, f.u0, f.v0, f.w0, sync);
+        adv_vel->advect(f.w, f.w0, f.u0, f.v0, f.w0, sync);
+    }
+    FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+
+    // 2. turbulent viscosity and diffusion (:140-152)
+    mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
+    dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
+    stats.diffusion_iterations[0] = dif_vel->last_iterations;
+    dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
+    stats.diffusion_iterations[1] = dif_vel->last_iterations;
+    dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
+    stats.diffusion_iterations[2] = dif_vel->last_iterations;
+    FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+
+    // 3. momentum source (:155-163)
+    if (m_add_source) {
+        sou_vel->add_source(f.u, f.v, f.w, f.f_x, f.f_y, f.f_z, sync);
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    }
+
+    // 4. pressure and projection (:167-176)
+    pres->divergence(f.rhs, f.u_tmp, f.v_tmp, f.w_tmp, sync);
+    pres->pressure(f.p, f.rhs, t, sync);
+    stats.pressure_cycles = pres->last_cycles;
+    stats.pressure_residual = pres->last_residual;
+    pres->projection(f.u, f.v, f.w, f.u_tmp, f.v_tmp, f.w_tmp, f.p, sync);
+
+    // 5. temperature (:184-240)
+    adv_temp->advect(f.T, f.T0, f.u, f.v, f.w, sync);
+    FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
+    const auto &ts = m_rt.settings().solver.temperature;
+    if (ts.has_turbulence) {
+        const real rPr_T = 1. / ts.prandtl_number.value();
+        check(artss_scale_copy(m_rt.ctx(), f.kappa_t.data, f.nu_t.data, rPr_T, 0), "kappa_t");
+        dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, f.kappa_t, sync);
+        stats.diffusion_iterations[3] = dif_temp->last_iterations;
+        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
+    } else if (kappa != 0.) {
+        dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, sync);
+        stats.diffusion_iterations[3] = dif_temp->last_iterations;
+        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
+    }
+    if (m_add_temp_source) {
+        sou_temp->add_source(f.T, f.S_T, sync);
+        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
+    }
+}
+
+void NSTempTurbSolver::update_source(real t_cur) { m_source_function_temperature->update_source(m_fc.S_T, t_cur); }
+
+void NSTempTurbSolver::update_obstacle_change() { m_source_function_temperature->update_obstacle_change(); }
+
+// ---------------------------------------------------------------- NSSolver / NSTurbSolver
+
+NSSolver::NSSolver(Runtime &rt, FieldController &fc, bool turbulent) : m_rt(rt), m_fc(fc), m_turb(turbulent) {
+    const settings::Solver &s = rt.settings().solver;
+    adv_vel = make_advection(rt, s.advection);
+    dif_vel = make_diffusion(rt, s.diffusion);
+    if (turbulent) mu_tub = make_turbulence(rt, s.turbulence);
+    pres = make_pressure(rt, s.pressure);
+    sou_vel = make_source(rt, s.source.type, s.source.dir);
+    m_add_source = s.source.force_fct != "Zero";
+    dif_vel->in_is_scratch = true;
+}
+
+void NSSolver::do_step(real t, bool sync) {
+    FieldController &f = m_fc;
+    const real nu = m_rt.settings().physical.nu.value();
+    if (auto *sl = dynamic_cast<SLAdvect *>(adv_vel.get())) {
+        sl->advect_vector(f.u, f.v, f.w, f.u0, f.v0, f.w0, f.u0, f.v0, f.w0);
+    } else {
+        adv_vel->advect(f.u, f.u0, f.u0, f.v0, f.w0, sync);
+        adv_vel->advect(f.v, f.v0, f.u0, f.v0, f.w0, sync);
+        adv_vel->advect(f.w, f.w0, f.u0, f.v0, f.w0, sync);
+    }
+    FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    if (m_turb) {
+        // NSTurbSolver.cpp: turbulent viscosity, then turbulent diffusion
+        mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
+        dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
+        dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
+        dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    } else if (nu != 0.) {
+        dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
+        dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, sync);
+        dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    }
+    if (m_add_source) {
+        sou_vel->add_source(f.u, f.v, f.w, f.f_x, f.f_y, f.f_z, sync);
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    }
+    pres->divergence(f.rhs, f.u_tmp, f.v_tmp, f.w_tmp, sync);
+    pres->pressure(f.p, f.rhs, t, sync);
+    pres->projection(f.u, f.v, f.w, f.u_tmp, f.v_tmp, f.w_tmp, f.p, sync);
+}
+
+// ---------------------------------------------------------------- PressureSolver
+
+PressureSolver::PressureSolver(Runtime &rt, FieldController &fc) : m_fc(fc) {
+    if (rt.settings().solver.pressure.field != F_P) throw config_error("Fields not specified correctly!");
+    pres = make_pressure(rt, rt.settings().solver.pressure);
+}
+
+void PressureSolver::do_step(real t, bool sync) { pres->pressure(m_fc.p, m_fc.rhs, t, sync); }
+
+// ---------------------------------------------------------------- SolverController
+
+SolverController::SolverController(Runtime &rt) : m_rt(rt) {
+    m_fc = std::make_unique<FieldController>(rt);
+    const std::string &d = rt.settings().solver.description;
+    if (d == "NSTempTurbSolver") {
+        m_solver = std::make_unique<NSTempTurbSolver>(rt, *m_fc);
+        m_has_momentum_source = true;
+    } else if (d == "NSSolver" || d == "NSTurbSolver") {
+        m_solver = std::make_unique<NSSolver>(rt, *m_fc, d == "NSTurbSolver");
+        m_has_momentum_source = true;
+    } else if (d == "PressureSolver") {
+        m_solver = std::make_unique<PressureSolver>(rt, *m_fc);
+    } else {
+        throw config_error("Solver " + d + " not yet implemented on this path");
+    }
+    set_up_fields();
+    m_fc->set_up_boundary();
+    update_sources(0, true);
+    m_fc->update_data();
+}
+
+void SolverController::set_up_fields() {
+    // SolverController::set_up_fields (src/solver/SolverController.cpp:84-218), the
+    // initial conditions of the fractional-step path
+    const auto &ic = m_rt.settings().ic;
+    const Geometry &geo = m_rt.geometry();
+    const IdxList &inner = geo.inner(0);
+    if (ic.usr_fct == "Uniform") {
+        std::vector<real> T = m_fc->T.to_host();
+        for (Idx idx : inner) T[(size_t) idx] = ic.uniform_value;
+        if (ic.random) {
+            // Functions::random (src/Functions.cpp:738-774); the draws cover
+            // all Nx*Ny*Nz cells in linear order, applied to inner cells
+            const auto &r = ic.random_parameters;
+            if (!r.custom_seed) throw config_error("initial noise without custom_seed is not reproducible");
+            if (!r.absolute && (r.range > 1 || r.range < 0))
+                throw config_error("range for relative noise has to be between [0:1]");
+            UniformRandom noise(r.range, r.step_size, r.seed);
+            std::vector<real> n = noise.random_field(T.size());
+            for (Idx idx : inner) {
+                if (r.absolute) T[(size_t) idx] += n[(size_t) idx];
+                else T[(size_t) idx] *= (1 + n[(size_t) idx]);
+            }
+        }
+        m_fc->T.from_host(T);
+    } else if (ic.usr_fct == "SinSinSin") {
+        // Functions::sin_sin_sin (src/Functions.cpp:782-812)
+        m_fc->p.set_value(0.);
+        const GridLevel &g = geo.grid().level(0);
+        const auto &X1 = geo.grid().start_pd;
+        std::vector<real> rhs = m_fc->rhs.to_host();
+        const size_t Nx = g.N[0], Nxy = g.N[0] * g.N[1];
+        const double l = ic.sin_l;
+        for (Idx idx : inner) {
+            const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx, i = (size_t) idx - k * Nxy - j * Nx;
+            const double xi = X1[0] + ((double) i - 0.5) * g.spacing[0];
+            const double yj = X1[1] + ((double) j - 0.5) * g.spacing[1];
+            const double zk = X1[2] + ((double) k - 0.5) * g.spacing[2];
+            rhs[(size_t) idx] = std::sin(l * M_PI * xi) * std::sin(l * M_PI * yj) * std::sin(l * M_PI * zk);
+        }
+        m_fc->rhs.from_host(rhs);
+    } else if (ic.usr_fct != "Zero") {
+        throw config_error("initial condition '" + ic.usr_fct +
+                           "' is not one of Uniform, SinSinSin, Zero (the initial conditions of the "
+                           "fractional-step path this library runs)");
+    }
+    const std::string &d = m_rt.settings().solver.description;
+    if (d == "NSTempTurbSolver") force_source();
+}
+
+void SolverController::force_source() {
+    // SolverController::force_source (src/solver/SolverController.cpp:228-258)
+    const auto &src = m_rt.settings().solver.source;
+    if (src.force_fct == "Buoyancy") {
+        if (!src.use_init_values) m_fc->T_ambient.set_value(src.ambient_temperature.value());
+    } else if (src.force_fct == "Uniform") {
+        throw config_error("a uniform momentum force is not part of the fractional-step path implemented here");
+    }
+}
+
+void SolverController::momentum_source() {
+    // SolverController::momentum_source (src/solver/SolverController.cpp:263-284)
+    const auto &dir = m_rt.settings().solver.source.dir;
+    auto has = [&](int a) { return std::find(dir.begin(), dir.end(), a) != dir.end(); };
+    if (has(AXIS_X)) ISource::buoyancy_force(m_fc->f_x, m_fc->T, m_fc->T_ambient);
+    if (has(AXIS_Y)) ISource::buoyancy_force(m_fc->f_y, m_fc->T, m_fc->T_ambient);
+    if (has(AXIS_Z)) ISource::buoyancy_force(m_fc->f_z, m_fc->T, m_fc->T_ambient);
+}
+
+void SolverController::update_sources(real t_cur, bool) {
+    if (m_has_momentum_source && m_rt.settings().solver.source.force_fct == "Buoyancy") momentum_source();
+    m_solver->update_source(t_cur);
+}
+
+// ---------------------------------------------------------------- TimeIntegration
+
+TimeIntegration::TimeIntegration(Runtime &rt, SolverController &sc)
+    : m_rt(rt), m_sc(sc), m_dt(rt.settings().physical.dt), m_t_end(rt.settings().physical.t_end), m_t_cur(m_dt) {}
+
+bool TimeIntegration::finished() const { return !(m_t_cur < m_t_end + m_dt / 2); }
+
+int64_t TimeIntegration::run(int64_t steps) {
+    int64_t done = 0;
+    while (!finished() && (steps < 0 || done < steps)) {
+        m_sc.solver_do_step(m_t_cur, false);
+        m_sc.update_sources(m_t_cur, false);
+        m_sc.fields().update_data();
+        m_step++;
+        m_t_cur = (real) m_step * m_dt;
+        done++;
+    }
+    return done;
+}
+
+}  // namespace artss

@@ -1,0 +1,150 @@
+// Field storage, solver compositions, the solver controller and the time
+// loop of ARTSS (src/field/FieldController.*, src/solver/*, src/TimeIntegration.*).
+#pragma once
+
+#include <chrono>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "plugins.h"
+
+namespace artss {
+
+// FieldController (src/field/FieldController.h:15-137): the named fields of
+// the fractional-step path, all device resident.
+class FieldController {
+ public:
+    explicit FieldController(Runtime &rt);
+    Field u, v, w, u0, v0, w0, u_tmp, v_tmp, w_tmp;
+    Field nu_t, kappa_t;
+    Field p, p0, rhs;
+    Field T, T0, T_tmp, T_ambient;
+    Field f_x, f_y, f_z;
+    Field S_T;
+
+    void set_up_boundary();
+    void update_data();
+    static void couple_vector(const Field &a, Field &a0, Field &a_tmp, const Field &b, Field &b0, Field &b_tmp,
+                              const Field &c, Field &c0, Field &c_tmp);
+    static void couple_scalar(const Field &a, Field &a0, Field &a_tmp);
+    Field *by_name(const std::string &name);
+
+ private:
+    Runtime &m_rt;
+};
+
+// ISolver (src/interfaces/ISolver.h:31-38)
+class ISolver {
+ public:
+    virtual ~ISolver() = default;
+    virtual void do_step(real t, bool sync) = 0;
+    virtual void update_source(real t_cur) = 0;
+    virtual void update_obstacle_change() = 0;
+};
+
+struct StepStats {
+    int64_t diffusion_iterations[4] = {0, 0, 0, 0};  // u, v, w, T
+    int64_t pressure_cycles = 0;
+    double pressure_residual = -1;
+};
+
+// NSTempTurbSolver (src/solver/NSTempTurbSolver.cpp:94-248)
+class NSTempTurbSolver : public ISolver {
+ public:
+    NSTempTurbSolver(Runtime &rt, FieldController &fc);
+    void do_step(real t, bool sync) override;
+    void update_source(real t_cur) override;
+    void update_obstacle_change() override;
+    StepStats stats;
+
+ private:
+    Runtime &m_rt;
+    FieldController &m_fc;
+    std::unique_ptr<IAdvection> adv_vel, adv_temp;
+    std::unique_ptr<IDiffusion> dif_vel, dif_temp;
+    std::unique_ptr<ITurbulence> mu_tub;
+    std::unique_ptr<IPressure> pres;
+    std::unique_ptr<ISource> sou_vel, sou_temp;
+    std::unique_ptr<ISourceFunction> m_source_function_temperature;
+    bool m_add_source = false, m_add_temp_source = false;
+};
+
+// NSSolver / NSTurbSolver (src/solver/NSSolver.cpp, NSTurbSolver.cpp)
+class NSSolver : public ISolver {
+ public:
+    NSSolver(Runtime &rt, FieldController &fc, bool turbulent);
+    void do_step(real t, bool sync) override;
+    void update_source(real) override {}
+    void update_obstacle_change() override {}
+
+ private:
+    Runtime &m_rt;
+    FieldController &m_fc;
+    bool m_turb;
+    std::unique_ptr<IAdvection> adv_vel;
+    std::unique_ptr<IDiffusion> dif_vel;
+    std::unique_ptr<ITurbulence> mu_tub;
+    std::unique_ptr<IPressure> pres;
+    std::unique_ptr<ISource> sou_vel;
+    bool m_add_source = false;
+};
+
+// PressureSolver (src/solver/PressureSolver.cpp:30-43)
+class PressureSolver : public ISolver {
+ public:
+    PressureSolver(Runtime &rt, FieldController &fc);
+    void do_step(real t, bool sync) override;
+    void update_source(real) override {}
+    void update_obstacle_change() override {}
+    IPressure &pressure() { return *pres; }
+
+ private:
+    FieldController &m_fc;
+    std::unique_ptr<IPressure> pres;
+};
+
+// SolverController (src/solver/SolverController.cpp:26-311)
+class SolverController {
+ public:
+    SolverController(Runtime &rt);
+    void solver_do_step(real t, bool sync) { m_solver->do_step(t, sync); }
+    void update_sources(real t_cur, bool sync);
+    FieldController &fields() { return *m_fc; }
+    ISolver &solver() { return *m_solver; }
+
+ private:
+    void set_up_fields();
+    void force_source();
+    void momentum_source();
+    Runtime &m_rt;
+    std::unique_ptr<FieldController> m_fc;
+    std::unique_ptr<ISolver> m_solver;
+    bool m_has_momentum_source = false;
+};
+
+// TimeIntegration (src/TimeIntegration.cpp:46-186), benchmark branch.
+class TimeIntegration {
+ public:
+    TimeIntegration(Runtime &rt, SolverController &sc);
+    // runs until t_end (steps < 0) or for `steps` steps; returns steps run
+    int64_t run(int64_t steps = -1);
+    real time() const { return m_t_cur; }
+    int64_t step_index() const { return m_step; }
+    bool finished() const;
+
+ private:
+    Runtime &m_rt;
+    SolverController &m_sc;
+    real m_dt, m_t_end, m_t_cur;
+    int64_t m_step = 1;
+};
+
+// Plugin factory of src/solver/SolverSelection.cpp:33-212.
+std::unique_ptr<IAdvection> make_advection(Runtime &rt, const settings::Advection &s);
+std::unique_ptr<IDiffusion> make_diffusion(Runtime &rt, const settings::Diffusion &s);
+std::unique_ptr<ITurbulence> make_turbulence(Runtime &rt, const settings::Turbulence &s);
+std::unique_ptr<IPressure> make_pressure(Runtime &rt, const settings::Pressure &s);
+std::unique_ptr<ISource> make_source(Runtime &rt, const std::string &type, const std::vector<int> &dir);
+
+}  // namespace artss

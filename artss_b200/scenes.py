@@ -1,0 +1,327 @@
+"""XML scene writers in the ARTSS input format (ARTSS src/utility/settings/Settings.cpp).
+
+Every scene the benchmarks and tests use is produced here, as an ordinary ARTSS
+XML file that both this package and the reference binary read.  Parameters not
+fixed by the workload descriptions (Gauss time constant tau, heat capacity cp,
+turbulent Prandtl number, noise step) follow the reference's own Steckler test
+XML (tests/navierStokesTempTurb/steckler/Test_NavierStokesTempTurb_Steckler.xml).
+"""
+from __future__ import annotations
+
+import os
+import random
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+
+def _f(x: float) -> str:
+    return repr(float(x))
+
+
+@dataclass
+class Box:
+    """Axis-aligned obstacle in physical coordinates (ox1..oz2)."""
+    x1: float
+    x2: float
+    y1: float
+    y2: float
+    z1: float
+    z2: float
+    name: str = "box"
+
+
+@dataclass
+class Scene:
+    """One NSTempTurb / Pressure scene.  Field names follow ARTSS XML keys."""
+    solver: str = "NSTempTurbSolver"
+    nx: int = 64
+    ny: int = 64
+    nz: int = 64
+    X: Tuple[float, float] = (0.0, 2.4)
+    Y: Tuple[float, float] = (0.0, 2.4)
+    Z: Tuple[float, float] = (0.0, 2.4)
+    dt: float = 0.005
+    steps: int = 200
+    nu: float = 3.1e-5
+    kappa: float = 4.2e-5
+    beta: float = 3.34e-3
+    g: float = -9.81
+    diffusion: str = "ColoredGaussSeidel"
+    diff_max_iter: int = 100
+    diff_tol: float = 1e-7
+    cs: float = 0.2
+    buoyancy_dir: str = "z"
+    t_ambient: float = 299.15
+    n_level: int = 4
+    n_cycle: int = 2
+    max_cycle: int = 100
+    mg_tol: float = 1e-8
+    n_relax: int = 2
+    smoother: str = "Jacobi"
+    smoother_max_iter: int = 100
+    smoother_tol: float = 1e-8
+    smoother_w: float = 0.6666666667
+    hrr: float = 25.0
+    cp: float = 1.0
+    source_pos: Tuple[float, float, float] = (1.2, 1.2, 0.3)
+    sigma: Tuple[float, float, float] = (0.1, 0.1, 0.1)
+    tau: float = 5.0
+    pr_t: float = 0.5
+    T0: float = 299.15
+    noise: bool = True
+    noise_range: float = 0.01
+    noise_step: float = 0.001
+    seed: int = 0
+    boundaries: List[Tuple[str, str, str, float]] = field(default_factory=list)
+    obstacles: List[Box] = field(default_factory=list)
+    obstacle_bcs: List[Tuple[str, str, str, float]] = field(default_factory=list)
+    ic: str = "Uniform"
+
+    @property
+    def t_end(self) -> float:
+        return self.steps * self.dt
+
+    def inner_cells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+
+def closed_box_bcs(T_type: str = "neumann", T_value: float = 0.0):
+    return [
+        ("u,v,w", "front,back,bottom,top,left,right", "dirichlet", 0.0),
+        ("p", "front,back,bottom,top,left,right", "neumann", 0.0),
+        ("T", "front,back,bottom,top,left,right", T_type, T_value),
+    ]
+
+
+def solid_obstacle_bcs():
+    return [
+        ("u,v,w", "front,back,left,right,top,bottom", "dirichlet", 0.0),
+        ("p,T", "front,back,left,right,top,bottom", "neumann", 0.0),
+    ]
+
+
+def plume_box(n: int = 64, steps: int = 200, n_level: int = 4, **kw) -> Scene:
+    """Closed 2.4 m box, uniform n^3 grid, 25 kW Gaussian source at (1.2,1.2,0.3):
+    the plain FP64 NSTempTurb workload on a 64^3 grid (n=64, 200 steps)."""
+    s = Scene(nx=n, ny=n, nz=n, steps=steps, n_level=n_level, boundaries=closed_box_bcs(), **kw)
+    return s
+
+
+def channel_with_cube(nx: int = 256, ny: int = 128, nz: int = 128, steps: int = 500,
+                      n_level: int = 4, **kw) -> Scene:
+    """6.4 x 3.2 x 3.2 m channel, one 0.4 m cube with its lower corner at
+    (1.6, 1.6, 0.2) m, Dirichlet inflow u = 0.5 m/s at x = 0, Neumann outflow at
+    x = 6.4 m, 100 kW Gaussian source 0.4 m behind the cube, T0 = 293.15 K."""
+    bcs = [
+        ("u", "left", "dirichlet", 0.5),
+        ("v,w", "left", "dirichlet", 0.0),
+        ("u,v,w", "right", "neumann", 0.0),
+        ("u,v,w", "front,back,bottom,top", "dirichlet", 0.0),
+        ("p", "left,front,back,bottom,top", "neumann", 0.0),
+        ("p", "right", "dirichlet", 0.0),
+        ("T", "left", "dirichlet", 293.15),
+        ("T", "right,front,back,bottom,top", "neumann", 0.0),
+    ]
+    cube = Box(1.6, 2.0, 1.6, 2.0, 0.2, 0.6, name="cube")
+    base = dict(nx=nx, ny=ny, nz=nz, X=(0.0, 6.4), Y=(0.0, 3.2), Z=(0.0, 3.2), dt=0.002,
+                steps=steps, n_level=n_level, hrr=100.0, source_pos=(2.4, 1.8, 0.4),
+                sigma=(0.2, 0.2, 0.2), T0=293.15, t_ambient=293.15, boundaries=bcs,
+                obstacles=[cube], obstacle_bcs=solid_obstacle_bcs())
+    base.update(kw)
+    return Scene(**base)
+
+
+def room_with_door(n: int = 32, steps: int = 10, n_level: int = 2, diffusion: str = "Jacobi", **kw) -> Scene:
+    """A closed room built from seven touching wall obstacles with a door in
+    one wall, heated at the floor centre: the obstacle layout of the
+    reference's Steckler test (touching walls exercise the neighbouring-obstacle
+    handling of src/domain/Obstacle.cpp:539-858), on a 3.2 m cube of n^3 cells."""
+    h = 3.2 / n
+    c = lambda k: round(k * h, 12)  # noqa: E731  cell-aligned coordinate
+    q = n // 16  # wall thickness in cells
+    lo, hi = n // 8, n - n // 8
+    x0 = -1.6
+    X = lambda k: round(x0 + k * h, 12)  # noqa: E731
+    top = (5 * n) // 8
+    door_lo, door_hi = (3 * n) // 8, (5 * n) // 8
+    door_top = n // 2
+    walls = [
+        Box(X(lo), X(lo + q), c(0), c(top), X(lo + q), X(hi - q), "left wall"),
+        Box(X(lo), X(hi), c(top), c(top + q), X(lo), X(hi), "ceiling"),
+        Box(X(lo), X(hi), c(0), c(top), X(hi - q), X(hi), "back wall"),
+        Box(X(lo), X(hi), c(0), c(top), X(lo), X(lo + q), "front wall"),
+        Box(X(hi - q), X(hi), c(0), c(top), X(lo + q), X(door_lo), "right wall left from door"),
+        Box(X(hi - q), X(hi), c(door_top), c(top), X(door_lo), X(door_hi), "right wall above door"),
+        Box(X(hi - q), X(hi), c(0), c(top), X(door_hi), X(hi - q), "right wall right from door"),
+    ]
+    bcs = [
+        ("u,v,w", "front,back,bottom,top,left,right", "dirichlet", 0.0),
+        ("p", "front,back,bottom,top,left,right", "neumann", 0.0),
+        ("T", "front,back,top,left,right", "dirichlet", 299.14),
+        ("T", "bottom", "neumann", 0.0),
+    ]
+    base = dict(nx=n, ny=n, nz=n, X=(-1.6, 1.6), Y=(0.0, 3.2), Z=(-1.6, 1.6), dt=0.01, steps=steps,
+                n_level=n_level, diffusion=diffusion, buoyancy_dir="y", hrr=50.3, source_pos=(0.0, 0.2, 0.0),
+                sigma=(0.25, 0.6, 0.25), T0=299.14, t_ambient=299.14, boundaries=bcs, obstacles=walls,
+                obstacle_bcs=solid_obstacle_bcs(), n_relax=4, mg_tol=1e-7, smoother_tol=1e-7, noise_step=0.1,
+                noise_range=1.0)
+    base.update(kw)
+    return Scene(**base)
+
+
+def random_boxes(n_cells: Tuple[int, int, int], lo: int, hi: int, count: int, seed: int,
+                 spacing: Tuple[float, float, float], origin=(0.0, 0.0, 0.0),
+                 levels: int = 0, max_tries: int = 10000) -> List[Box]:
+    """Axis-aligned boxes with edges uniform in [lo, hi] cells at uniform
+    positions, rejected when they touch or overlap (with a one-cell gap at every
+    multigrid level), since the reference's list construction is only well
+    defined for obstacles that stay apart after restriction
+    (src/domain/Multigrid.cpp:495-512 keeps duplicates)."""
+    rng = random.Random(seed)
+    boxes_idx: List[Tuple[int, int, int, int, int, int]] = []
+    gap = 2 ** (levels + 1)
+    tries = 0
+    while len(boxes_idx) < count and tries < max_tries:
+        tries += 1
+        e = [rng.randint(lo, hi) for _ in range(3)]
+        if any(e[a] > n_cells[a] - 2 * gap for a in range(3)):
+            continue
+        s = [rng.randint(gap, n_cells[a] - e[a] - gap) for a in range(3)]
+        # snap to multiples of 2^levels so coarse boxes keep their shape
+        q = 2 ** levels
+        s = [(s[a] // q) * q for a in range(3)]
+        e = [max(q, (e[a] // q) * q) for a in range(3)]
+        cand = (s[0], s[0] + e[0], s[1], s[1] + e[1], s[2], s[2] + e[2])
+        ok = True
+        for b in boxes_idx:
+            if all(cand[2 * a] < b[2 * a + 1] + gap and b[2 * a] < cand[2 * a + 1] + gap for a in range(3)):
+                ok = False
+                break
+        if ok:
+            boxes_idx.append(cand)
+    out = []
+    for n, b in enumerate(boxes_idx):
+        out.append(Box(origin[0] + b[0] * spacing[0], origin[0] + b[1] * spacing[0],
+                       origin[1] + b[2] * spacing[1], origin[1] + b[3] * spacing[1],
+                       origin[2] + b[4] * spacing[2], origin[2] + b[5] * spacing[2], name=f"box{n}"))
+    return out
+
+
+def to_xml(s: Scene) -> str:
+    L = []
+    a = L.append
+    a('<?xml version="1.0" encoding="UTF-8" ?>')
+    a("<ARTSS>")
+    a("  <physical_parameters>")
+    a(f"    <t_end> {_f(s.t_end)} </t_end>")
+    a(f"    <dt> {_f(s.dt)} </dt>")
+    if s.solver != "PressureSolver":
+        a(f"    <nu> {_f(s.nu)} </nu>")
+        a(f"    <beta> {_f(s.beta)} </beta>")
+        a(f"    <g> {_f(s.g)} </g>")
+        a("    <rhoa> 1 </rhoa>")
+        a(f"    <kappa> {_f(s.kappa)} </kappa>")
+    a("  </physical_parameters>")
+    a(f'  <solver description="{s.solver}" >')
+
+    def diffusion_block(tag_field: str, indent: str, typ: str, max_iter: int, tol: float, w: float):
+        a(f'{indent}<diffusion type="{typ}" field="{tag_field}">')
+        a(f"{indent}  <max_iter> {max_iter} </max_iter>")
+        a(f"{indent}  <tol_res> {_f(tol)} </tol_res>")
+        a(f"{indent}  <w> {_f(w)} </w>")
+        a(f"{indent}</diffusion>")
+
+    if s.solver != "PressureSolver":
+        a('    <advection type="SemiLagrangian" field="u,v,w">')
+        a("    </advection>")
+        diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
+        a('    <turbulence type="ConstSmagorinsky">')
+        a(f"      <Cs> {_f(s.cs)} </Cs>")
+        a("    </turbulence>")
+        a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
+        a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
+        a("    </source>")
+    a('    <pressure type="VCycleMG" field="p">')
+    a(f"      <n_level> {s.n_level} </n_level>")
+    a(f"      <n_cycle> {s.n_cycle} </n_cycle>")
+    a(f"      <max_cycle> {s.max_cycle} </max_cycle>")
+    a(f"      <tol_res> {_f(s.mg_tol)} </tol_res>")
+    a(f"      <n_relax> {s.n_relax} </n_relax>")
+    diffusion_block("p", "      ", s.smoother, s.smoother_max_iter, s.smoother_tol, s.smoother_w)
+    a("    </pressure>")
+    if s.solver != "PressureSolver":
+        a("    <temperature>")
+        a('      <advection type="SemiLagrangian" field="T">')
+        a("      </advection>")
+        diffusion_block("T", "      ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
+        a('      <turbulence include="Yes">')
+        a(f"        <Pr_T> {_f(s.pr_t)} </Pr_T>")
+        a("      </turbulence>")
+        a(f'      <source type="ExplicitEuler" dir="{s.buoyancy_dir}" temp_fct="Gauss" dissipation="No" random="No">')
+        a(f"        <HRR> {_f(s.hrr)} </HRR>")
+        a(f"        <cp> {_f(s.cp)} </cp>")
+        a(f"        <x0> {_f(s.source_pos[0])} </x0>")
+        a(f"        <y0> {_f(s.source_pos[1])} </y0>")
+        a(f"        <z0> {_f(s.source_pos[2])} </z0>")
+        a(f"        <sigma_x> {_f(s.sigma[0])} </sigma_x>")
+        a(f"        <sigma_y> {_f(s.sigma[1])} </sigma_y>")
+        a(f"        <sigma_z> {_f(s.sigma[2])} </sigma_z>")
+        a(f"        <tau> {_f(s.tau)} </tau>")
+        a("      </source>")
+        a("    </temperature>")
+    a('    <solution available="No">')
+    a("    </solution>")
+    a("  </solver>")
+    a('  <domain_parameters enable_computational_domain="No">')
+    for ax, (lo, hi) in zip("XYZ", (s.X, s.Y, s.Z)):
+        a(f"    <{ax}1> {_f(lo)} </{ax}1>")
+        a(f"    <{ax}2> {_f(hi)} </{ax}2>")
+    a(f"    <nx> {s.nx} </nx>")
+    a(f"    <ny> {s.ny} </ny>")
+    a(f"    <nz> {s.nz} </nz>")
+    a("  </domain_parameters>")
+    a('  <adaption dynamic="No" data_extraction="No"> </adaption>')
+    a('  <data_assimilation enabled="No" />')
+    a("  <boundaries>")
+    for fld, patch, typ, val in s.boundaries:
+        a(f'    <boundary field="{fld}" patch="{patch}" type="{typ}" value="{_f(val)}" />')
+    a("  </boundaries>")
+    if s.obstacles:
+        a('  <obstacles enabled="Yes">')
+        for b in s.obstacles:
+            a(f'    <obstacle name="{b.name}">')
+            a(f'      <geometry ox1="{_f(b.x1)}" ox2="{_f(b.x2)}" oy1="{_f(b.y1)}" oy2="{_f(b.y2)}"'
+              f' oz1="{_f(b.z1)}" oz2="{_f(b.z2)}"/>')
+            for fld, patch, typ, val in (s.obstacle_bcs or solid_obstacle_bcs()):
+                a(f'      <boundary field="{fld}" patch="{patch}" type="{typ}" value="{_f(val)}"/>')
+            a("    </obstacle>")
+        a("  </obstacles>")
+    else:
+        a('  <obstacles enabled="No"/>')
+    a('  <surfaces enabled="No"/>')
+    if s.ic == "Uniform":
+        a(f'  <initial_conditions usr_fct="Uniform" random="{"Yes" if s.noise else "No"}">')
+        a(f"    <val> {_f(s.T0)} </val>")
+        if s.noise:
+            a('    <random absolute="Yes" custom_seed="Yes" custom_steps="Yes">')
+            a(f"      <seed> {s.seed} </seed>")
+            a(f"      <step_size> {_f(s.noise_step)} </step_size>")
+            a(f"      <range> {_f(s.noise_range)} </range>")
+            a("    </random>")
+        a("  </initial_conditions>")
+    else:
+        a(f'  <initial_conditions usr_fct="{s.ic}" random="No">')
+        a("  </initial_conditions>")
+    a('  <visualisation save_vtk="No" save_csv="No">')
+    a("  </visualisation>")
+    a('  <logging file="artss.log" level="info">')
+    a("  </logging>")
+    a("</ARTSS>")
+    return "\n".join(L) + "\n"
+
+
+def write(s: Scene, path: str) -> str:
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        f.write(to_xml(s))
+    return path

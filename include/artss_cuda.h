@@ -1,0 +1,245 @@
+/* artss_cuda.h -- C ABI of the B200 kernels behind the ARTSS plugin interfaces.
+ *
+ * One entry point per plugin method of the fractional-step timestep
+ * (ARTSS src/solver/NSTempTurbSolver.cpp:94-248).  Everything crosses the
+ * boundary as plain pointers, sizes and POD structs; device memory is owned by
+ * a context and all work of a context is enqueued on its own CUDA stream.
+ *
+ * Conventions
+ *  - Every function returns ARTSS_OK (0) or a negative status; the message of
+ *    the last failure on the calling thread is returned by artss_last_error().
+ *  - Arrays use the reference layout IX(i,j,k) = i + Nx*j + Nx*Ny*k with one
+ *    ghost layer (ARTSS src/utility/GlobalMacrosTypes.h:70), FP64 unless noted.
+ *  - "level" is the multigrid level (0 = finest), "field_type" the reference
+ *    FieldType (ARTSS src/utility/Mapping.h:55-58) that selects boundary
+ *    conditions.
+ *  - Iterative solvers never hang: each loop is bounded by its max_iter and
+ *    reports the iterations it took.
+ *  - A context is not thread-safe; distinct contexts are independent.
+ */
+#ifndef ARTSS_CUDA_H
+#define ARTSS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARTSS_MAX_LEVEL 8 /* multigrid levels 0..ARTSS_MAX_LEVEL */
+
+enum artss_status {
+    ARTSS_OK = 0,
+    ARTSS_ERR_ARG = -1,       /* invalid argument / size / pointer */
+    ARTSS_ERR_CUDA = -2,      /* CUDA runtime error */
+    ARTSS_ERR_NOMEM = -3,     /* device allocation failed */
+    ARTSS_ERR_STATE = -4,     /* call not valid in the context's state */
+    ARTSS_ERR_NO_DEVICE = -5, /* no CUDA device / extension unusable */
+    ARTSS_ERR_LIMIT = -6      /* a size exceeds a documented maximum */
+};
+
+/* ARTSS FieldType (src/utility/Mapping.h:55-58) */
+enum artss_field_type {
+    ARTSS_FIELD_RHO = 0, ARTSS_FIELD_U = 1, ARTSS_FIELD_V = 2, ARTSS_FIELD_W = 3,
+    ARTSS_FIELD_P = 4, ARTSS_FIELD_T = 5, ARTSS_FIELD_NU = 6, ARTSS_NUM_FIELD_TYPES = 7
+};
+
+typedef struct artss_ctx artss_ctx;
+
+/* Per-level grid geometry, as DomainData computes it
+ * (ARTSS src/domain/DomainData.cpp:12-56, DomainData.h:181-190). */
+typedef struct {
+    int32_t n_levels;                    /* coarse levels (reference n_level); levels 0..n_levels */
+    int32_t reserved;
+    int64_t Nx[ARTSS_MAX_LEVEL + 1];     /* cells incl. ghost layer */
+    int64_t Ny[ARTSS_MAX_LEVEL + 1];
+    int64_t Nz[ARTSS_MAX_LEVEL + 1];
+    int64_t i1[ARTSS_MAX_LEVEL + 1];     /* computational-domain inner index range, inclusive */
+    int64_t i2[ARTSS_MAX_LEVEL + 1];
+    int64_t j1[ARTSS_MAX_LEVEL + 1];
+    int64_t j2[ARTSS_MAX_LEVEL + 1];
+    int64_t k1[ARTSS_MAX_LEVEL + 1];
+    int64_t k2[ARTSS_MAX_LEVEL + 1];
+    double dx[ARTSS_MAX_LEVEL + 1];      /* spacing per level */
+    double dy[ARTSS_MAX_LEVEL + 1];
+    double dz[ARTSS_MAX_LEVEL + 1];
+} artss_grid_desc;
+
+/* One boundary assignment x[target] = sign * x[source] + value, the loop body
+ * of DomainBoundary/ObstacleBoundary::apply_boundary_condition
+ * (ARTSS src/boundaryCondition/DomainBoundary.cpp:42-46,
+ *  src/boundaryCondition/ObstacleBoundary.cpp:42-48). */
+typedef struct {
+    int64_t target;
+    int64_t source;
+    double value;
+    int32_t sign;   /* +1 or -1 */
+    int32_t reserved;
+} artss_bc_assign;
+
+/* Iteration control of the diffusion solvers
+ * (Settings::solver::diffusion_solvers::{jacobi,colored_gauss_seidel}). */
+typedef struct {
+    int64_t max_iter;
+    double tol_res;
+    double w;
+} artss_iter_cfg;
+
+typedef struct {
+    int64_t iterations;
+    double residual;
+} artss_iter_stats;
+
+/* VCycleMG settings (Settings::solver::pressure_solvers::vcycle_mg). */
+enum artss_smoother { ARTSS_SMOOTHER_JACOBI = 0, ARTSS_SMOOTHER_CGS = 1 };
+typedef struct {
+    int32_t n_level;
+    int32_t n_cycle;
+    int32_t max_cycle;
+    int32_t n_relax;
+    double tol_res;           /* first-step absolute residual tolerance */
+    int32_t smoother;         /* enum artss_smoother */
+    int32_t reserved;
+    int64_t smoother_max_iter;
+    double smoother_tol_res;
+    double smoother_w;
+} artss_mg_cfg;
+
+typedef struct {
+    int64_t cycles;             /* V-cycles run by the call */
+    int64_t coarse_iterations;  /* Jacobi/CGS sweeps of the last coarse solve */
+    double residual;            /* first-step loop: final absolute ||b - A p||_2, else -1 */
+} artss_mg_stats;
+
+typedef struct artss_mg artss_mg;
+
+/* ------------------------------------------------------------------ */
+/* context and memory                                                 */
+/* ------------------------------------------------------------------ */
+
+/* Replaces DomainData::init + the OpenACC device set-up (src/main.cpp:62-78). */
+int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out);
+int artss_ctx_destroy(artss_ctx *ctx);
+/* cudaStream_t of the context (all work of the context runs on it). */
+void *artss_ctx_stream(artss_ctx *ctx);
+int artss_ctx_sync(artss_ctx *ctx);
+const char *artss_last_error(void);
+/* Number of kernels this context has launched so far. */
+int64_t artss_ctx_kernel_launches(artss_ctx *ctx);
+
+/* Replaces Field's `new real[]` + `acc enter data` (src/field/Field.cpp:12-53):
+ * a zero-filled device array of Nx*Ny*Nz doubles of `level`. */
+int artss_field_alloc(artss_ctx *ctx, int level, double **out);
+int artss_field_free(artss_ctx *ctx, double *field);
+int64_t artss_field_size(artss_ctx *ctx, int level);
+/* Field::update_dev / update_host (src/field/Field.h:41-49). */
+int artss_upload(artss_ctx *ctx, double *dst, const double *host, int64_t n);
+int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
+
+/* ------------------------------------------------------------------ */
+/* geometry: GPU lists -> device cell flags and boundary programs     */
+/* ------------------------------------------------------------------ */
+
+/* Replaces Multigrid::send_domain_lists_to_GPU (src/domain/Multigrid.cpp:520-526):
+ * the level's domain-inner list and domain list (inner + boundary cells),
+ * sorted ascending as the reference builds them, become per-cell flags. */
+int artss_set_cell_lists(artss_ctx *ctx, int level,
+                         const int64_t *inner, int64_t n_inner,
+                         const int64_t *domain, int64_t n_domain);
+/* Device copy of the level's cell flags (bit0 inner, bit1 domain list). */
+int artss_get_cell_flags(artss_ctx *ctx, int level, uint8_t *host_out, int64_t n);
+
+/* Replaces Multigrid::apply_boundary_condition's per-patch loops
+ * (src/domain/Multigrid.cpp:555-572): the ordered assignments for one field
+ * type on one level (obstacles in id order, then domain patches
+ * left..back).  The library compiles them into dependency-free waves. */
+int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type,
+                               const artss_bc_assign *ops, int64_t n_ops);
+/* Number of kernel waves the compiled program of (level, field_type) needs. */
+int artss_boundary_program_waves(artss_ctx *ctx, int level, int field_type);
+
+/* DomainController::apply_boundary (src/domain/DomainController.cpp:139-141). */
+int artss_apply_boundary(artss_ctx *ctx, double *field, int level, int field_type);
+
+/* ------------------------------------------------------------------ */
+/* whole-array field operations (src/field/Field.h:64-135)            */
+/* ------------------------------------------------------------------ */
+int artss_fill(artss_ctx *ctx, double *field, int level, double value);
+int artss_copy(artss_ctx *ctx, double *dst, const double *src, int level);
+int artss_add_field(artss_ctx *ctx, double *dst, const double *src, int level);   /* dst += src */
+int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level);         /* dst += x */
+int artss_scale(artss_ctx *ctx, double *dst, double x, int level);              /* dst *= x */
+int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, int level); /* dst = src * x */
+/* FieldController::couple_vector / couple_scalar (src/field/FieldController.cpp:151-186):
+ * a0 = a and a_tmp = a for each non-null triple, one pass over memory. */
+int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
+                 const double *b, double *b0, double *b_tmp,
+                 const double *c, double *c0, double *c_tmp);
+
+/* ------------------------------------------------------------------ */
+/* plugins                                                            */
+/* ------------------------------------------------------------------ */
+
+/* IAdvection::advect, SLAdvect (src/advection/SLAdvect.cpp:34-170), with the
+ * closing apply_boundary(out).  dt is the physical time step. */
+int artss_advect_sl(artss_ctx *ctx, double *out, const double *in,
+                    const double *u, const double *v, const double *w,
+                    double dt, int out_field_type);
+/* Three SLAdvect calls sharing one backtrace: out_u <- in_u, out_v <- in_v,
+ * out_w <- in_w, all advected with (u, v, w) (NSTempTurbSolver.cpp:129-131). */
+int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *out_w,
+                        const double *in_u, const double *in_v, const double *in_w,
+                        const double *u, const double *v, const double *w, double dt);
+
+/* ITurbulence::calc_turbulent_viscosity, ConstSmagorinsky
+ * (src/turbulence/ConstSmagorinsky.cpp:30-87), including apply_boundary(ev). */
+int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t,
+                                 const double *u, const double *v, const double *w, double cs);
+
+/* IDiffusion::diffuse, ColoredGaussSeidelDiffuse (src/diffusion/ColoredGaussSeidelDiffuse.cpp:38-173).
+ * ev == NULL selects the laminar variant.  `in` is overwritten as in the
+ * reference (it holds the state before the last sweep) unless
+ * in_is_scratch != 0, in which case its final contents are unspecified. */
+int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
+                      double D, const double *ev, double dt, int field_type,
+                      const artss_iter_cfg *cfg, int in_is_scratch, artss_iter_stats *stats);
+/* IDiffusion::diffuse, JacobiDiffuse (src/diffusion/JacobiDiffuse.cpp:31-203). */
+int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b,
+                         double D, const double *ev, double dt, int field_type,
+                         const artss_iter_cfg *cfg, artss_iter_stats *stats);
+
+/* IPressure::divergence (src/interfaces/IPressure.cpp:20-110): rhs on inner
+ * cells and zero on the computational domain's ghost ring. */
+int artss_divergence(artss_ctx *ctx, double *rhs, const double *u, const double *v, const double *w);
+/* IPressure::projection (src/interfaces/IPressure.cpp:125-172) + BCs of u, v, w. */
+int artss_projection(artss_ctx *ctx, double *u, double *v, double *w,
+                     const double *u_star, const double *v_star, const double *w_star,
+                     const double *p);
+
+/* ISource::buoyancy_force (src/interfaces/ISource.cpp:26-52) on the domain list. */
+int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const double *T_ambient,
+                         double beta, double g);
+/* ExplicitEulerSource::add_source (src/source/ExplicitEulerSource.cpp:25-104):
+ * out += dt * S on inner cells, then apply_boundary(out). */
+int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, int field_type);
+
+/* IPressure::pressure, VCycleMG (src/pressure/VCycleMG.cpp:17-798).
+ * The solver owns its level hierarchy (residuals, errors, temporaries). */
+int artss_mg_create(artss_ctx *ctx, const artss_mg_cfg *cfg, artss_mg **out);
+int artss_mg_destroy(artss_mg *mg);
+/* One VCycleMG::pressure call: first_step != 0 reproduces the Nt == 1 branch
+ * (cycles until the absolute residual reaches tol_res, max_cycle, or the
+ * smoother budget), otherwise n_cycle V-cycles. */
+int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step, artss_mg_stats *stats);
+/* One VCycleMG::VCycleMultigrid on p with the right-hand side last given to
+ * artss_mg_pressure / artss_mg_set_rhs. */
+int artss_mg_set_rhs(artss_mg *mg, const double *p, const double *rhs);
+int artss_mg_vcycle(artss_mg *mg, double *p);
+/* ||b - A p||_2 over level-0 inner cells (VCycleMG.cpp:186-194) and ||b||_2. */
+int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ARTSS_CUDA_H */

@@ -1,0 +1,73 @@
+/* artss_host.h -- C API of the host runtime (libartss_host.so).
+ *
+ * The host runtime reads an ARTSS XML file, builds the geometry (multigrid
+ * levels, index lists, boundary programs) and drives the timestep of
+ * SolverController / TimeIntegration (ARTSS src/solver/SolverController.cpp,
+ * src/TimeIntegration.cpp) through the kernels of artss_cuda.h.
+ *
+ * The artss_geom_* functions need no GPU: they expose the index lists and
+ * boundary assignments the host builds, for bit-exact comparison with the
+ * reference's lists (ARTSS src/domain/Multigrid.cpp:313-374).
+ */
+#ifndef ARTSS_HOST_H
+#define ARTSS_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "artss_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct artss_geom artss_geom;
+typedef struct artss_sim artss_sim;
+
+/* last error of the calling thread (config errors, CUDA errors) */
+const char *artss_host_last_error(void);
+
+/* ---- geometry (CPU only) ---- */
+int artss_geom_create(const char *xml_path, artss_geom **out);
+void artss_geom_destroy(artss_geom *g);
+int artss_geom_levels(artss_geom *g);
+int artss_geom_obstacles(artss_geom *g);
+/* name: "inner", "domain", "obst", "bnd_<patch>", "obst<id>_<patch>" with
+ * <patch> in left,right,bottom,top,front,back.  The pointer stays valid until
+ * artss_geom_destroy. */
+int artss_geom_list(artss_geom *g, const char *name, int level, const int64_t **data, int64_t *n);
+/* Nx, Ny, Nz of a level */
+int artss_geom_dims(artss_geom *g, int level, int64_t *dims3);
+/* ordered boundary assignments of (level, field type); *n == 0 when the
+ * field type has no boundary conditions */
+int artss_geom_boundary_program(artss_geom *g, int level, int field_type, const artss_bc_assign **ops, int64_t *n);
+int artss_geom_grid_desc(artss_geom *g, artss_grid_desc *out);
+
+/* ---- simulation (GPU) ---- */
+int artss_sim_create(const char *xml_path, int device, artss_sim **out);
+void artss_sim_destroy(artss_sim *s);
+/* runs up to `steps` timesteps (all remaining when steps < 0); *done = steps run */
+int artss_sim_run(artss_sim *s, int64_t steps, int64_t *done);
+int artss_sim_finished(artss_sim *s);
+double artss_sim_time(artss_sim *s);
+int64_t artss_sim_step_index(artss_sim *s);
+int64_t artss_sim_inner_cells(artss_sim *s);
+/* field names: u v w u0 v0 w0 u_tmp v_tmp w_tmp nu_t kappa_t p p0 rhs T T0 T_tmp
+ * T_a f_x f_y f_z S_T; n must equal the level-0 array size */
+int artss_sim_get_field(artss_sim *s, const char *name, double *host, int64_t n);
+int artss_sim_set_field(artss_sim *s, const char *name, const double *host, int64_t n);
+int64_t artss_sim_field_size(artss_sim *s);
+/* device pointer of a field (for timing or zero-copy use) */
+double *artss_sim_field_device(artss_sim *s, const char *name);
+artss_ctx *artss_sim_context(artss_sim *s);
+/* per-step statistics of the last step: iterations of the u, v, w, T
+ * diffusion solves, V-cycles and (first step) residual of the pressure solve */
+int artss_sim_last_stats(artss_sim *s, int64_t *diff_iters4, int64_t *mg_cycles, double *mg_residual);
+/* one pressure solve of a PressureSolver scene with the current p and rhs */
+int artss_sim_pressure(artss_sim *s, int first_step, int64_t *cycles, double *residual);
+/* the multigrid solver of a PressureSolver scene, or NULL */
+artss_mg *artss_sim_mg(artss_sim *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,86 @@
+"""Full-timestep parity of the B200 path with the reference serial build.
+
+Each scene is an ARTSS XML written by artss_b200.scenes and run both by the
+reference (oracle/_ref/artss_ref_driver: the unmodified ARTSS sources compiled
+by oracle/Makefile) and by artss_b200.Simulation.  After every checked step
+the fields u, v, w, p, T, nu_t (and rhs, S_T, buoyancy force) must agree to a
+relative max-norm of 1e-10; in practice they agree bit for bit, because every
+kernel evaluates the reference's expression with the same roundings and only
+residual sums (which decide iteration counts, not values) are reduced in a
+different order.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import artss_b200 as A
+from artss_b200 import scenes
+from tests import refdriver
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+CHECK = ["u", "v", "w", "p", "T", "nu_t", "rhs", "S_T", "f_x", "f_y", "f_z"]
+
+
+def _scenes():
+    return {
+        "box16_cgs": scenes.plume_box(n=16, steps=8, n_level=2),
+        "box32_cgs": scenes.plume_box(n=32, steps=4, n_level=3),
+        "channel_cube": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=4, n_level=3),
+        "room_jacobi": scenes.room_with_door(n=32, steps=4, n_level=2),
+        "room_cgs": scenes.room_with_door(n=32, steps=3, n_level=2, diffusion="ColoredGaussSeidel"),
+    }
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory):
+    if not refdriver.available():
+        pytest.skip("reference oracle not built (oracle/Makefile)")
+    base = tmp_path_factory.mktemp("parity")
+    out = {}
+    for name, sc in _scenes().items():
+        xml = scenes.write(sc, str(base / f"{name}.xml"))
+        dump = refdriver.run(xml, str(base / f"{name}_ref"), steps=sc.steps)
+        out[name] = (xml, dump, sc)
+    return out
+
+
+@pytest.mark.parametrize("name", list(_scenes().keys()))
+def test_timestep_parity(cases, name):
+    xml, dump, sc = cases[name]
+    with A.Simulation(xml) as sim:
+        # set-up state (SolverController constructor)
+        for f in CHECK:
+            ref = refdriver.field(dump, 0, f)
+            assert refdriver.rel_max_err(sim.field(f), ref) <= TOL, f"step 0 field {f}"
+        worst = 0.0
+        for step in range(1, sc.steps + 1):
+            assert sim.run(1) == 1
+            for f in CHECK:
+                ref = refdriver.field(dump, step, f)
+                err = refdriver.rel_max_err(sim.field(f), ref)
+                worst = max(worst, err)
+                assert err <= TOL, f"step {step} field {f}: relative max error {err:.3e}"
+        print(f"{name}: worst relative error over {sc.steps} steps {worst:.3e}")
+
+
+def test_cell_flags_match_reference_lists(cases):
+    """The device cell flags are built from the host lists; they must mark
+    exactly the reference's inner and domain lists on every level."""
+    xml, dump, sc = cases["channel_cube"]
+    ref_dir = refdriver.run(xml, dump + "_lists", steps=0, lists=True)
+    g = A.Geometry(xml)
+    cuda = A.load_cuda()
+    with A.Simulation(xml) as sim:
+        for level in range(g.levels + 1):
+            dims = g.dims(level)
+            n = dims[0] * dims[1] * dims[2]
+            flags = np.zeros(n, np.uint8)
+            A.cuda_check(cuda.artss_get_cell_flags(sim.context, level, flags.ctypes.data_as(
+                __import__("ctypes").POINTER(__import__("ctypes").c_uint8)), n), "flags")
+            inner = np.flatnonzero(flags & 1)
+            domain = np.flatnonzero(flags & 2)
+            assert np.array_equal(inner, refdriver.ref_list(ref_dir, "inner", level))
+            assert np.array_equal(domain, refdriver.ref_list(ref_dir, "domain", level))

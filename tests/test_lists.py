@@ -1,0 +1,96 @@
+"""Bit-exact index lists ("GPU lists") of the host geometry against the
+reference's Multigrid/Domain/Obstacle construction.
+
+The golden fixture pins the room scene (seven touching walls: boundary-patch
+trimming and neighbouring-obstacle constraint removal); with the reference
+oracle built, every list of several more scenes is compared directly."""
+import os
+
+import numpy as np
+import pytest
+
+import artss_b200 as A
+from artss_b200 import scenes
+from tests import refdriver
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATCHES = A.PATCHES
+
+
+def all_names(g):
+    names = ["inner", "domain"] + ["bnd_" + p for p in PATCHES]
+    if g.obstacles:
+        names += ["obst"] + [f"obst{i}_{p}" for i in range(g.obstacles) for p in PATCHES]
+    return names
+
+
+def test_room_lists_match_golden(tmp_path):
+    gold = np.load(os.path.join(HERE, "golden", "lists_room32.npz"))
+    xml = scenes.write(scenes.room_with_door(n=32, steps=0, n_level=2), str(tmp_path / "room.xml"))
+    g = A.Geometry(xml)
+    assert g.levels == 2 and g.obstacles == 7
+    for level in range(3):
+        for n in all_names(g):
+            np.testing.assert_array_equal(g.list(n, level), gold[f"{n}_L{level}"], err_msg=f"{n} level {level}")
+
+
+def _scene_set():
+    return {
+        "box16": scenes.plume_box(n=16, steps=0, n_level=2),
+        "box64": scenes.plume_box(n=64, steps=0, n_level=4),
+        "channel": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=0, n_level=3),
+        "room64": scenes.room_with_door(n=64, steps=0, n_level=3),
+        "odd_sizes": scenes.plume_box(n=24, steps=0, n_level=3),
+    }
+
+
+@pytest.mark.parametrize("name", list(_scene_set().keys()))
+def test_lists_match_reference(tmp_path, name):
+    if not refdriver.available():
+        pytest.skip("reference oracle not built")
+    xml = scenes.write(_scene_set()[name], str(tmp_path / f"{name}.xml"))
+    d = refdriver.run(xml, str(tmp_path / "ref"), steps=0, lists=True)
+    g = A.Geometry(xml)
+    for level in range(g.levels + 1):
+        for n in all_names(g):
+            np.testing.assert_array_equal(g.list(n, level), refdriver.ref_list(d, n, level),
+                                          err_msg=f"{name}: {n} level {level}")
+
+
+def test_random_obstacle_scenes_match_reference(tmp_path):
+    """Seeded scenes of 1-6 separated boxes (edges 4-12 cells)."""
+    if not refdriver.available():
+        pytest.skip("reference oracle not built")
+    for seed in range(4):
+        n = 32
+        boxes = scenes.random_boxes((n, n, n), 4, 12, 1 + seed % 6, seed, (2.4 / n,) * 3, levels=2)
+        sc = scenes.plume_box(n=n, steps=0, n_level=2, obstacles=boxes, obstacle_bcs=scenes.solid_obstacle_bcs())
+        xml = scenes.write(sc, str(tmp_path / f"r{seed}.xml"))
+        d = refdriver.run(xml, str(tmp_path / f"r{seed}"), steps=0, lists=True)
+        g = A.Geometry(xml)
+        for level in range(g.levels + 1):
+            for nm in all_names(g):
+                np.testing.assert_array_equal(g.list(nm, level), refdriver.ref_list(d, nm, level),
+                                              err_msg=f"seed {seed}: {nm} level {level}")
+
+
+def test_overlapping_obstacles_rejected(tmp_path):
+    sc = scenes.plume_box(n=16, steps=0, n_level=1, obstacles=[
+        scenes.Box(0.3, 0.9, 0.3, 0.9, 0.3, 0.9, "a"), scenes.Box(0.6, 1.2, 0.6, 1.2, 0.6, 1.2, "b")],
+        obstacle_bcs=scenes.solid_obstacle_bcs())
+    xml = scenes.write(sc, str(tmp_path / "ov.xml"))
+    with pytest.raises(A.ArtssError, match="overlap"):
+        A.Geometry(xml)
+
+
+def test_multigrid_kat_8x12x4():
+    """Known-answer sizes of ARTSS gtests/domain/Multigrid.cpp:30-97 (8x12x4
+    cells, 2 levels): domain-inner list 384/48/6 cells."""
+    import tempfile
+    sc = scenes.Scene(solver="PressureSolver", nx=8, ny=12, nz=4, X=(0, 8), Y=(0, 12), Z=(0, 4), n_level=2,
+                      boundaries=[("p", "front,back,bottom,top,left,right", "dirichlet", 0.0)], ic="Zero",
+                      noise=False, steps=1)
+    with tempfile.TemporaryDirectory() as tmp:
+        g = A.Geometry(scenes.write(sc, os.path.join(tmp, "kat.xml")))
+        assert [g.list("inner", l).size for l in range(3)] == [384, 48, 6]
+        assert g.list("domain", 0).size == 10 * 14 * 6
