@@ -189,11 +189,13 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
     ARTSS_CK(cudaMalloc(&p.d_depth, n));
     ARTSS_CK(cudaMalloc(&p.d_neg, n));
     ARTSS_CK(cudaMalloc(&p.d_value, kBcMaxDepth * n * sizeof(double)));
-    ARTSS_CK(cudaMemcpy(p.d_target, tgt.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    ARTSS_CK(cudaMemcpy(p.d_root, root.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
-    ARTSS_CK(cudaMemcpy(p.d_depth, depth.data(), n, cudaMemcpyHostToDevice));
-    ARTSS_CK(cudaMemcpy(p.d_neg, neg.data(), n, cudaMemcpyHostToDevice));
-    ARTSS_CK(cudaMemcpy(p.d_value, val.data(), kBcMaxDepth * n * sizeof(double), cudaMemcpyHostToDevice));
+    ARTSS_CK(cudaMemcpyAsync(p.d_target, tgt.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    ARTSS_CK(cudaMemcpyAsync(p.d_root, root.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    ARTSS_CK(cudaMemcpyAsync(p.d_depth, depth.data(), n, cudaMemcpyHostToDevice, ctx->stream));
+    ARTSS_CK(cudaMemcpyAsync(p.d_neg, neg.data(), n, cudaMemcpyHostToDevice, ctx->stream));
+    ARTSS_CK(cudaMemcpyAsync(p.d_value, val.data(), kBcMaxDepth * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    // the host vectors die with this call
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
     return ARTSS_OK;
 }
 

@@ -136,6 +136,9 @@ int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
         if ((e = cudaMalloc(&ctx->d_flags[l], n)) != cudaSuccess) return fail(e, "cell flags");
         if ((e = cudaMemset(ctx->d_flags[l], 0, n)) != cudaSuccess) return fail(e, "cell flags");
     }
+    // the memsets above ran on the legacy stream, which the context's
+    // non-blocking stream does not order against
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "set-up");
     *out = ctx;
     return ARTSS_OK;
 }

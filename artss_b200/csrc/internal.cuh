@@ -18,7 +18,7 @@ constexpr int kMaxLevel = ARTSS_MAX_LEVEL;
 constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
 constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
 constexpr int kReduceThreads = 256;
-constexpr int kMaxPartials = 4096;      // blocks of a reduction pass
+constexpr int kMaxPartials = 1 << 16;   // per-block partial sums of up to two reduction passes
 
 enum CellFlag : uint8_t { kInner = 1, kDomain = 2 };
 
@@ -112,6 +112,15 @@ inline unsigned flat_blocks(int64_t n, int threads = 256) {
     if (b < 1) b = 1;
     if (b > 148 * 16) b = 148 * 16;
     return (unsigned) b;
+}
+
+// A reduction pass writes one partial per block; two passes share d_partials.
+inline int check_reduce_blocks(const dim3 &g) {
+    if (2 * (int64_t) g.x * g.y * g.z > kMaxPartials) {
+        set_error("x-y plane too large for the reduction buffer");
+        return ARTSS_ERR_LIMIT;
+    }
+    return ARTSS_OK;
 }
 
 // Boundary program execution (bc.cu).

@@ -211,6 +211,8 @@ int mg_resnorm(artss_mg *mg, const double *x, const double *b, int level, int sl
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
     const dim3 grid = mg_grid(box);
+    int st = check_reduce_blocks(grid);
+    if (st) return st;
     k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(x, b, ctx->d_flags[level], L, box,
                                                         1. / (g.dx[level] * g.dx[level]),
                                                         1. / (g.dy[level] * g.dy[level]),
@@ -458,6 +460,7 @@ int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
     const dim3 grid = mg_grid(box);
+    if (int st0 = check_reduce_blocks(grid)) return st0;
     const int nb = (int) (grid.x * grid.y * grid.z);
     k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(p, b, ctx->d_flags[0], L, box, 1. / (g.dx[0] * g.dx[0]),
                                                         1. / (g.dy[0] * g.dy[0]), 1. / (g.dz[0] * g.dz[0]),

@@ -445,6 +445,7 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     const Level &L = ctx->lvl[0];
     const Box3 box = inner_box(L);
     const dim3 g = zgrid(box);
+    if ((st = check_reduce_blocks(g))) return st;
     const int nb = nblocks(g);
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
@@ -492,6 +493,7 @@ int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *
     const Box3 box = inner_box(L);
     const Box3 dbox = domain_box(L);
     const dim3 g = zgrid(box);
+    if ((st = check_reduce_blocks(g))) return st;
     const int nb = nblocks(g);
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     const int slot = 0;
