@@ -133,6 +133,10 @@ def load_cuda() -> C.CDLL:
             "artss_mg_set_rhs": ([_P, _D, _D], C.c_int),
             "artss_mg_vcycle": ([_P, _D], C.c_int),
             "artss_residual_norm": ([_P, _D, _D, _D, _D], C.c_int),
+            "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
+            "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),
+            "artss_ctx_profile_reset": ([_P], C.c_int),
+            "artss_kernel_family_name": ([C.c_int], C.c_char_p),
         }
         for fn, (args, res) in sig.items():
             f = getattr(lib, fn)

@@ -47,8 +47,8 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type) {
     for (int w = 0; w < p.waves; w++) {
         const int64_t b = p.wave_begin[w], e = p.wave_begin[w + 1];
         if (e <= b) continue;
-        k_bc_wave<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(f, p.d_target, p.d_root, p.d_depth, p.d_neg,
-                                                               p.d_value, b, e, p.n);
+        ARTSS_LAUNCH(ctx, FAM_BC, k_bc_wave<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(f, p.d_target, p.d_root, p.d_depth, p.d_neg,
+                                                               p.d_value, b, e, p.n));
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;

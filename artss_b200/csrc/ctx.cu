@@ -82,6 +82,23 @@ __global__ void k_mark(uint8_t *__restrict__ flags, const int64_t *__restrict__ 
         flags[list[i]] |= bit;
 }
 
+cudaEvent_t prof_event(artss_ctx *ctx) {
+    Profile &p = ctx->prof;
+    if (!p.pool.empty()) {
+        cudaEvent_t e = p.pool.back();
+        p.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+
+static const char *const kFamilyNames[FAM_COUNT] = {
+    "advect", "smagorinsky", "divergence", "projection", "buoyancy", "add_source", "cgs_color",
+    "jacobi_diffuse", "copy_domain", "bc_wave", "field_op", "couple", "mg_jacobi", "mg_cgs", "mg_residuum",
+    "mg_restrict", "mg_prolongate", "mg_resnorm", "reduce", "mg_coarse"};
+
 }  // namespace artss
 
 using namespace artss;
@@ -89,6 +106,48 @@ using namespace artss;
 extern "C" {
 
 const char *artss_last_error(void) { return g_last_error.c_str(); }
+
+const char *artss_kernel_family_name(int family) {
+    return family >= 0 && family < FAM_COUNT ? kFamilyNames[family] : "";
+}
+
+int artss_ctx_profile(artss_ctx *ctx, uint64_t mask) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ctx->prof.mask = mask;
+    return ARTSS_OK;
+}
+
+int artss_ctx_profile_reset(artss_ctx *ctx) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    Profile &p = ctx->prof;
+    for (auto &pe : p.pending) p.pool.push_back(pe.first);
+    for (auto e : p.events) p.pool.push_back(e);
+    p.pending.clear();
+    p.events.clear();
+    for (int f = 0; f < FAM_COUNT; f++) { p.launches[f] = 0; p.ms[f] = 0.0; }
+    return ARTSS_OK;
+}
+
+int artss_ctx_profile_read(artss_ctx *ctx, int64_t *launches, double *ms, int n_families) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    Profile &p = ctx->prof;
+    for (size_t q = 0; q < p.pending.size(); q++) {
+        float t = 0.f;
+        ARTSS_CK(cudaEventElapsedTime(&t, p.pending[q].first, p.events[q]));
+        p.ms[p.pending[q].second] += t;
+        p.pool.push_back(p.pending[q].first);
+        p.pool.push_back(p.events[q]);
+    }
+    p.pending.clear();
+    p.events.clear();
+    for (int f = 0; f < n_families && f < FAM_COUNT; f++) {
+        if (launches) launches[f] = p.launches[f];
+        if (ms) ms[f] = p.ms[f];
+    }
+    return ARTSS_OK;
+}
 
 int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
     if (!grid || !out) { set_error("null argument"); return ARTSS_ERR_ARG; }
@@ -155,6 +214,9 @@ int artss_ctx_destroy(artss_ctx *ctx) {
             cudaFree(p.d_target); cudaFree(p.d_root); cudaFree(p.d_depth); cudaFree(p.d_neg); cudaFree(p.d_value);
         }
     }
+    for (auto &pe : ctx->prof.pending) cudaEventDestroy(pe.first);
+    for (auto e : ctx->prof.events) cudaEventDestroy(e);
+    for (auto e : ctx->prof.pool) cudaEventDestroy(e);
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_loop);
     if (ctx->h_loop) cudaFreeHost(ctx->h_loop);
@@ -247,14 +309,14 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
     cudaError_t e = cudaMemsetAsync(ctx->d_flags[level], 0, L.size(), ctx->stream);
     if (e == cudaSuccess && n_inner) e = cudaMemcpyAsync(d_list, inner, n_inner * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess && n_inner) {
-        k_mark<<<flat_blocks(n_inner), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_inner, kInner);
+        ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mark<<<flat_blocks(n_inner), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_inner, kInner));
         ctx->launches++;
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess && n_domain) e = cudaMemcpyAsync(d_list, domain, n_domain * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess && n_domain) {
-        k_mark<<<flat_blocks(n_domain), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_domain, kDomain);
+        ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mark<<<flat_blocks(n_domain), 256, 0, ctx->stream>>>(ctx->d_flags[level], d_list, n_domain, kDomain));
         ctx->launches++;
         e = cudaGetLastError();
     }
@@ -273,43 +335,43 @@ int artss_get_cell_flags(artss_ctx *ctx, int level, uint8_t *host_out, int64_t n
     return ARTSS_OK;
 }
 
-#define ARTSS_FIELD_OP(launch)                                        \
+#define ARTSS_FIELD_OP(...)                                           \
     int st = check_level(ctx, level);                                 \
     if (st) return st;                                                \
     const int64_t n = ctx->lvl[level].size();                         \
-    launch;                                                           \
+    __VA_ARGS__;                                                      \
     ARTSS_LAUNCH_CK(ctx);                                             \
     return ARTSS_OK;
 
 int artss_fill(artss_ctx *ctx, double *f, int level, double value) {
     if (!f) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP((k_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(f, n, value)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(f, n, value)))
 }
 
 int artss_copy(artss_ctx *ctx, double *dst, const double *src, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
     if (dst == src) return check_level(ctx, level);
-    ARTSS_FIELD_OP((k_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
 }
 
 int artss_add_field(artss_ctx *ctx, double *dst, const double *src, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP((k_add_field<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_add_field<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
 }
 
 int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level) {
     if (!dst) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP((k_add_scalar<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_add_scalar<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
 }
 
 int artss_scale(artss_ctx *ctx, double *dst, double x, int level) {
     if (!dst) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP((k_scale<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_scale<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
 }
 
 int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP((k_scale_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, x, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_scale_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, x, n)))
 }
 
 int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
@@ -319,7 +381,7 @@ int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
         set_error("couple: incomplete triple"); return ARTSS_ERR_ARG;
     }
     const int level = 0;
-    ARTSS_FIELD_OP((k_couple3<<<flat_blocks(n), 256, 0, ctx->stream>>>(a, a0, a_tmp, b, b0, b_tmp, c, c0, c_tmp, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_COUPLE, k_couple3<<<flat_blocks(n), 256, 0, ctx->stream>>>(a, a0, a_tmp, b, b0, b_tmp, c, c0, c_tmp, n)))
 }
 
 }  // extern "C"

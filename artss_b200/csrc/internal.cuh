@@ -53,6 +53,24 @@ struct LoopState {
     int pad;
 };
 
+// Kernel families for launch counting and event timing (artss_ctx_profile).
+enum Family : int {
+    FAM_ADVECT = 0, FAM_SMAGORINSKY, FAM_DIVERGENCE, FAM_PROJECTION, FAM_BUOYANCY, FAM_ADD_SOURCE,
+    FAM_CGS, FAM_JACOBI, FAM_COPY_DOMAIN, FAM_BC, FAM_FIELD_OP, FAM_COUPLE, FAM_MG_JACOBI, FAM_MG_CGS,
+    FAM_MG_RESIDUUM, FAM_MG_RESTRICT, FAM_MG_PROLONGATE, FAM_MG_RESNORM, FAM_REDUCE, FAM_MG_COARSE,
+    FAM_COUNT
+};
+static_assert(FAM_COUNT == ARTSS_KERNEL_FAMILIES, "family table");
+
+struct Profile {
+    uint64_t mask = 0;
+    int64_t launches[FAM_COUNT] = {};
+    double ms[FAM_COUNT] = {};
+    std::vector<std::pair<cudaEvent_t, int>> pending;  // start event (end = next) + family
+    std::vector<cudaEvent_t> events;                    // recorded, in order
+    std::vector<cudaEvent_t> pool;                      // free events
+};
+
 }  // namespace artss
 
 struct artss_ctx {
@@ -67,7 +85,36 @@ struct artss_ctx {
     artss::LoopState *h_loop = nullptr; // pinned mirror
     int64_t launches = 0;
     std::set<double *> fields;
+    artss::Profile prof;
 };
+
+namespace artss {
+cudaEvent_t prof_event(artss_ctx *ctx);
+// Brackets one kernel launch: counts it under its family and, when the
+// family is profiled, records an event pair around it on the context stream.
+struct ProfScope {
+    artss_ctx *ctx;
+    int fam;
+    cudaEvent_t start = nullptr;
+    ProfScope(artss_ctx *c, int f) : ctx(c), fam(f) {
+        if (ctx->prof.mask >> fam & 1) {
+            start = prof_event(ctx);
+            if (start) cudaEventRecord(start, ctx->stream);
+        }
+    }
+    ~ProfScope() {
+        ctx->prof.launches[fam]++;
+        if (start) {
+            cudaEvent_t stop = prof_event(ctx);
+            if (stop) {
+                cudaEventRecord(stop, ctx->stream);
+                ctx->prof.pending.push_back({start, fam});
+                ctx->prof.events.push_back(stop);
+            }
+        }
+    }
+};
+}  // namespace artss
 
 namespace artss {
 
@@ -152,3 +199,10 @@ __device__ __forceinline__ double artss_block_sum(double v, double *smem) {
     }
     return v;
 }
+
+// Launches a kernel inside a ProfScope of the given family.
+#define ARTSS_LAUNCH(ctx, fam, ...)                 \
+    do {                                            \
+        artss::ProfScope ps_((ctx), (fam));         \
+        __VA_ARGS__;                                \
+    } while (0)

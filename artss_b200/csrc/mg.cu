@@ -185,8 +185,8 @@ int mg_jacobi_step(artss_mg *mg, double *out, const double *in, const double *b,
     artss_ctx *ctx = mg->ctx;
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
-    k_mg_jacobi<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
-                                                               mg_coef(mg, level));
+    ARTSS_LAUNCH(ctx, FAM_MG_JACOBI, k_mg_jacobi<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
+                                                               mg_coef(mg, level)));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -197,7 +197,7 @@ int mg_cgs_step(artss_mg *mg, double *out, const double *b, int level) {
     const Box3 box = inner_box(L);
     const MgCoef c = mg_coef(mg, level);
     for (int color = 0; color < 2; color++) {
-        k_mg_cgs_color<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, b, ctx->d_flags[level], L, box, color, c);
+        ARTSS_LAUNCH(ctx, FAM_MG_CGS, k_mg_cgs_color<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, b, ctx->d_flags[level], L, box, color, c));
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;
@@ -213,10 +213,10 @@ int mg_resnorm(artss_mg *mg, const double *x, const double *b, int level, int sl
     const dim3 grid = mg_grid(box);
     int st = check_reduce_blocks(grid);
     if (st) return st;
-    k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(x, b, ctx->d_flags[level], L, box,
+    ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(x, b, ctx->d_flags[level], L, box,
                                                         1. / (g.dx[level] * g.dx[level]),
                                                         1. / (g.dy[level] * g.dy[level]),
-                                                        1. / (g.dz[level] * g.dz[level]), ctx->d_partials, nullptr);
+                                                        1. / (g.dz[level] * g.dz[level]), ctx->d_partials, nullptr));
     ARTSS_LAUNCH_CK(ctx);
     const int nb = (int) (grid.x * grid.y * grid.z);
     if (iterate) return finalize_loop(ctx, slot, nb, tol, max_it);
@@ -293,8 +293,8 @@ int mg_restrict(artss_mg *mg, double *coarse, const double *fine, int coarse_lev
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    k_mg_restrict<<<mg_grid(box), box_block(), 0, ctx->stream>>>(coarse, fine, ctx->d_flags[coarse_level], C,
-                                                                 ctx->lvl[coarse_level - 1], box);
+    ARTSS_LAUNCH(ctx, FAM_MG_RESTRICT, k_mg_restrict<<<mg_grid(box), box_block(), 0, ctx->stream>>>(coarse, fine, ctx->d_flags[coarse_level], C,
+                                                                 ctx->lvl[coarse_level - 1], box));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -303,8 +303,8 @@ int mg_prolongate(artss_mg *mg, double *fine, const double *coarse, int coarse_l
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    k_mg_prolongate<<<mg_grid(box), box_block(), 0, ctx->stream>>>(fine, coarse, ctx->d_flags[coarse_level], C,
-                                                                   ctx->lvl[coarse_level - 1], box);
+    ARTSS_LAUNCH(ctx, FAM_MG_PROLONGATE, k_mg_prolongate<<<mg_grid(box), box_block(), 0, ctx->stream>>>(fine, coarse, ctx->d_flags[coarse_level], C,
+                                                                   ctx->lvl[coarse_level - 1], box));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -314,10 +314,10 @@ int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, in
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
-    k_mg_residuum<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
+    ARTSS_LAUNCH(ctx, FAM_MG_RESIDUUM, k_mg_residuum<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
                                                                  1. / (g.dx[level] * g.dx[level]),
                                                                  1. / (g.dy[level] * g.dy[level]),
-                                                                 1. / (g.dz[level] * g.dz[level]));
+                                                                 1. / (g.dz[level] * g.dz[level])));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -462,9 +462,9 @@ int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double
     const dim3 grid = mg_grid(box);
     if (int st0 = check_reduce_blocks(grid)) return st0;
     const int nb = (int) (grid.x * grid.y * grid.z);
-    k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(p, b, ctx->d_flags[0], L, box, 1. / (g.dx[0] * g.dx[0]),
+    ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mg_resnorm<<<grid, box_block(), 0, ctx->stream>>>(p, b, ctx->d_flags[0], L, box, 1. / (g.dx[0] * g.dx[0]),
                                                         1. / (g.dy[0] * g.dy[0]), 1. / (g.dz[0] * g.dz[0]),
-                                                        ctx->d_partials, ctx->d_partials + nb);
+                                                        ctx->d_partials, ctx->d_partials + nb));
     ARTSS_LAUNCH_CK(ctx);
     int st;
     LoopState a{}, c{};

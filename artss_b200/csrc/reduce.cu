@@ -35,19 +35,19 @@ __global__ void k_init_loop(LoopState *st, double r0, long long it0, int cond0) 
 }
 
 int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it) {
-    k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, tol, max_it, 0);
+    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, tol, max_it, 0));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int finalize_sum(artss_ctx *ctx, int slot, int nblocks) {
-    k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1);
+    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int init_loop(artss_ctx *ctx, int slot, double r0, long long it0, int cond0) {
-    k_init_loop<<<1, 1, 0, ctx->stream>>>(ctx->d_loop + slot, r0, it0, cond0);
+    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_init_loop<<<1, 1, 0, ctx->stream>>>(ctx->d_loop + slot, r0, it0, cond0));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }

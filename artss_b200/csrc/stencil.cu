@@ -345,8 +345,8 @@ int artss_advect_sl(artss_ctx *ctx, double *out, const double *in, const double 
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
-    k_advect<1><<<g, box_block(), 0, ctx->stream>>>(out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
-                                                    ctx->d_flags[0], L, box, c);
+    ARTSS_LAUNCH(ctx, FAM_ADVECT, k_advect<1><<<g, box_block(), 0, ctx->stream>>>(out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
+                                                    ctx->d_flags[0], L, box, c));
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, out, 0, out_field_type);
 }
@@ -360,8 +360,8 @@ int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *ou
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
-    k_advect<3><<<g, box_block(), 0, ctx->stream>>>(out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
-                                                    ctx->d_flags[0], L, box, c);
+    ARTSS_LAUNCH(ctx, FAM_ADVECT, k_advect<3><<<g, box_block(), 0, ctx->stream>>>(out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
+                                                    ctx->d_flags[0], L, box, c));
     ARTSS_LAUNCH_CK(ctx);
     if ((st = apply_bc(ctx, out_u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, out_v, 0, ARTSS_FIELD_V))) return st;
@@ -377,8 +377,8 @@ int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t, const double *u, 
     const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
     const double delta_s = cbrt(dx * dy * dz);
     const double cs2d2 = cs * cs * delta_s * delta_s;
-    k_smagorinsky<<<zgrid(box), box_block(), 0, ctx->stream>>>(nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
-                                                               1. / dy, 1. / dz, cs2d2);
+    ARTSS_LAUNCH(ctx, FAM_SMAGORINSKY, k_smagorinsky<<<zgrid(box), box_block(), 0, ctx->stream>>>(nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
+                                                               1. / dy, 1. / dz, cs2d2));
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, nu_t, 0, ARTSS_FIELD_NU);
 }
@@ -391,10 +391,10 @@ int artss_divergence(artss_ctx *ctx, double *rhs, const double *u, const double 
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    k_divergence<<<zgrid(box), box_block(), 0, ctx->stream>>>(rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz);
+    ARTSS_LAUNCH(ctx, FAM_DIVERGENCE, k_divergence<<<zgrid(box), box_block(), 0, ctx->stream>>>(rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz));
     ARTSS_LAUNCH_CK(ctx);
     const Box3 ring = domain_box(L);
-    k_ghost_ring_zero<<<zgrid(ring), box_block(), 0, ctx->stream>>>(rhs, L, ring);
+    ARTSS_LAUNCH(ctx, FAM_DIVERGENCE, k_ghost_ring_zero<<<zgrid(ring), box_block(), 0, ctx->stream>>>(rhs, L, ring));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -408,8 +408,8 @@ int artss_projection(artss_ctx *ctx, double *u, double *v, double *w, const doub
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    k_projection<<<zgrid(box), box_block(), 0, ctx->stream>>>(u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
-                                                              hy, hz);
+    ARTSS_LAUNCH(ctx, FAM_PROJECTION, k_projection<<<zgrid(box), box_block(), 0, ctx->stream>>>(u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
+                                                              hy, hz));
     ARTSS_LAUNCH_CK(ctx);
     if ((st = apply_bc(ctx, u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, v, 0, ARTSS_FIELD_V))) return st;
@@ -421,7 +421,7 @@ int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const d
     if (st) return st;
     const Level &L = ctx->lvl[0];
     const Box3 box = domain_box(L);
-    k_buoyancy<<<zgrid(box), box_block(), 0, ctx->stream>>>(force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
+    ARTSS_LAUNCH(ctx, FAM_BUOYANCY, k_buoyancy<<<zgrid(box), box_block(), 0, ctx->stream>>>(force, T, Ta, ctx->d_flags[0], L, box, -beta, g));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -431,7 +431,7 @@ int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, in
     if (st || (st = check_field_type(field_type))) return st;
     const Level &L = ctx->lvl[0];
     const Box3 box = inner_box(L);
-    k_add_source<<<zgrid(box), box_block(), 0, ctx->stream>>>(out, S, ctx->d_flags[0], L, box, dt);
+    ARTSS_LAUNCH(ctx, FAM_ADD_SOURCE, k_add_source<<<zgrid(box), box_block(), 0, ctx->stream>>>(out, S, ctx->d_flags[0], L, box, dt));
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, out, 0, field_type);
 }
@@ -460,17 +460,17 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     while (cond) {
         if (!in_is_scratch && (st = artss_copy(ctx, in, out, 0))) return st;
         if (ev) {
-            k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 0, c,
-                                                                  ctx->d_partials);
+            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 0, c,
+                                                                  ctx->d_partials));
             ARTSS_LAUNCH_CK(ctx);
-            k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 1, c,
-                                                                  ctx->d_partials + nb);
+            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 1, c,
+                                                                  ctx->d_partials + nb));
         } else {
-            k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 0, c,
-                                                                   ctx->d_partials);
+            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 0, c,
+                                                                   ctx->d_partials));
             ARTSS_LAUNCH_CK(ctx);
-            k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 1, c,
-                                                                   ctx->d_partials + nb);
+            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 1, c,
+                                                                   ctx->d_partials + nb));
         }
         ARTSS_LAUNCH_CK(ctx);
         if ((st = apply_bc(ctx, out, 0, field_type))) return st;
@@ -504,16 +504,16 @@ int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *
     LoopState ls{};
     while (cond) {
         if (ev) {
-            k_jacobi_diffuse<true><<<g, box_block(), 0, ctx->stream>>>(out, in, b, ev, ctx->d_flags[0], L, box, c,
-                                                                       ctx->d_partials);
+            ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<true><<<g, box_block(), 0, ctx->stream>>>(out, in, b, ev, ctx->d_flags[0], L, box, c,
+                                                                       ctx->d_partials));
         } else {
-            k_jacobi_diffuse<false><<<g, box_block(), 0, ctx->stream>>>(out, in, b, nullptr, ctx->d_flags[0], L, box,
-                                                                        c, ctx->d_partials);
+            ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<false><<<g, box_block(), 0, ctx->stream>>>(out, in, b, nullptr, ctx->d_flags[0], L, box,
+                                                                        c, ctx->d_partials));
         }
         ARTSS_LAUNCH_CK(ctx);
         if ((st = apply_bc(ctx, out, 0, field_type))) return st;
         if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
-        k_copy_domain<<<zgrid(dbox), box_block(), 0, ctx->stream>>>(in, out, ctx->d_flags[0], L, dbox);
+        ARTSS_LAUNCH(ctx, FAM_COPY_DOMAIN, k_copy_domain<<<zgrid(dbox), box_block(), 0, ctx->stream>>>(in, out, ctx->d_flags[0], L, dbox));
         ARTSS_LAUNCH_CK(ctx);
         if ((st = read_loop(ctx, slot, &ls))) return st;
         it = ls.it;

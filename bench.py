@@ -1,0 +1,374 @@
+"""Benchmark of the ARTSS fractional-step timestep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload channel|box]
+
+A step is one NSTempTurbSolver timestep (SolverController::solver_do_step +
+update_sources + update_data, ARTSS src/TimeIntegration.cpp:86-145) of the
+workload scene.  Default workload: the plain-FP64 channel, 256x128x128 cells,
+one 0.4 m cube, Dirichlet inflow, 100 kW Gaussian source, dt = 0.002 s
+(artss_b200.scenes.channel_with_cube); the metric is cell-updates/s =
+inner cells x steps / time.  Warm-up steps include step 1, whose pressure
+solve iterates to tolerance.
+
+N > 1 (torchrun): the single scene does not shard, every rank runs its own
+replica on its own GPU and `value` is the sum over ranks (weak scaling).
+`--impl reference` times the reference serial build (oracle/_ref) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+STATE_FIELDS = ["u", "v", "w", "p", "T"]
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["channel", "box"], default="channel")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name: str, steps: int):
+    from artss_b200 import scenes
+    if name == "channel":
+        return "channel_256x128x128_cube_fp64", scenes.channel_with_cube(steps=steps)
+    return "box_64cubed_plume_fp64", scenes.plume_box(n=64, steps=steps, n_level=4)
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                cols = [c.strip() for c in line.split(",")]
+                if len(cols) < 9:
+                    continue
+                try:
+                    sm.append(float(cols[1]))
+                    mx = float(cols[2])
+                except ValueError:
+                    continue
+                for n, c in zip(names, cols[5:9]):
+                    if c.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class Dist:
+    """torch.distributed plumbing for N > 1 (one rank per GPU)."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            self.pg.barrier(device_ids=[self.local])
+            torch.cuda.synchronize()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# Algorithmic bytes of one launch, per inner cell of level 0 (n) or per array
+# cell (N) -- FP64, each array element read or written once; neighbour
+# re-reads are not counted.
+def launch_bytes(family: str, n: int, N: int, launches: int) -> float:
+    if family == "advect":       # per step: fused u,v,w (read u0,v0,w0; write u,v,w: 48 B) + T (read u,v,w,T0; write T: 40 B)
+        return launches / 2 * (48 + 40) * n
+    if family == "cgs_color":    # one colour: read x (all), b, EV and write x of half the cells: 8 + 0.5*24 B
+        return launches * 20.0 * n
+    if family == "smagorinsky":  # read u, v, w; write nu_t
+        return launches * 32.0 * n
+    if family == "couple":       # per step 4 vector couples (read 3, write 6 arrays) + 4 scalar (read 1, write 2)
+        return launches / 2 * (72 + 24) * N
+    if family == "projection":   # read u*, v*, w*, p; write u, v, w
+        return launches * 56.0 * n
+    return 0.0
+
+
+MODELED = ("advect", "cgs_color", "smagorinsky", "couple", "projection")
+
+
+def run_b200(args, dist):
+    import numpy as np
+    import torch
+
+    import artss_b200 as A
+    from artss_b200 import scenes
+
+    torch.cuda.set_device(dist.local)
+    total_steps = args.warmup + 2 + args.steps + args.e2e_steps + 2
+    name, sc = workload(args.workload, total_steps)
+    tmp = tempfile.mkdtemp(prefix="artss_bench_")
+    xml = scenes.write(sc, os.path.join(tmp, f"{name}_r{dist.rank}.xml"))
+    sim = A.Simulation(xml, device=dist.local)
+    cuda = A.load_cuda()
+    ctx = sim.context
+    inner = sim.inner_cells
+    size = sim.size
+    stream = torch.cuda.ExternalStream(cuda.artss_ctx_stream(ctx), device=torch.device("cuda", dist.local))
+
+    sim.run(args.warmup)
+
+    # family shares over two untimed steps, then events on the dominant modeled family only
+    nf = 20
+    cuda.artss_ctx_profile(ctx, (1 << nf) - 1)
+    cuda.artss_ctx_profile_reset(ctx)
+    sim.run(2)
+    L = (C.c_int64 * nf)()
+    M = (C.c_double * nf)()
+    A.cuda_check(cuda.artss_ctx_profile_read(ctx, L, M, nf), "profile")
+    fam_names = [cuda.artss_kernel_family_name(f).decode() for f in range(nf)]
+    share_ms = {fam_names[f]: M[f] for f in range(nf) if L[f]}
+    total_kernel_ms = sum(share_ms.values())
+    dom = max((f for f in range(nf) if fam_names[f] in MODELED and L[f]), key=lambda f: M[f])
+    cuda.artss_ctx_profile(ctx, 1 << dom)
+    cuda.artss_ctx_profile_reset(ctx)
+
+    sampler = ClockSampler(dist.local)
+    sampler.start()
+    launches0 = sim.kernel_launches()
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    done = sim.run(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    assert done == args.steps, "scene ended early"
+    ms = e0.elapsed_time(e1)
+    gpu_launches = sim.kernel_launches() - launches0
+    A.cuda_check(cuda.artss_ctx_profile_read(ctx, L, M, nf), "profile")
+    dom_launches, dom_ms = int(L[dom]), float(M[dom])
+    cuda.artss_ctx_profile(ctx, 0)
+
+    # end to end: state from pinned host memory in, state back out, every step
+    pinned_in = {f: torch.from_numpy(sim.field(f)).pin_memory() for f in STATE_FIELDS}
+    pinned_out = {f: torch.empty(size, dtype=torch.float64).pin_memory() for f in STATE_FIELDS}
+    dev = {f: C.cast(C.c_void_p(sim.device_pointer(f)), C.POINTER(C.c_double)) for f in STATE_FIELDS}
+    hp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        for f in STATE_FIELDS:
+            A.cuda_check(cuda.artss_upload(ctx, dev[f], hp(pinned_in[f]), size), "upload")
+        sim.run(1)
+        for f in STATE_FIELDS:
+            A.cuda_check(cuda.artss_download(ctx, hp(pinned_out[f]), dev[f], size), "download")
+        for f in STATE_FIELDS:
+            pinned_in[f].copy_(pinned_out[f])
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if not np.isfinite(pinned_out["T"].numpy()).all():
+        raise RuntimeError("non-finite temperature after the end-to-end steps")
+
+    ms_max = dist.max(ms)
+    e2e_ms_max = dist.max(e2e_ms)
+    cells_all = dist.sum(float(inner) * args.steps)
+    e2e_cells_all = dist.sum(float(inner) * args.e2e_steps)
+    hbm, peak_kind = peaks()
+    fam = fam_names[dom]
+    achieved = launch_bytes(fam, inner, size, dom_launches) / (dom_ms * 1e-3) / 1e9 if dom_ms > 0 else 0.0
+    out = {
+        "metric": "cell-updates/s per timestep",
+        "value": cells_all / (ms_max * 1e-3),
+        "unit": "cell-updates/s",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": name, "cells": f"{sc.nx}x{sc.ny}x{sc.nz}", "inner_cells": inner,
+                   "obstacles": len(sc.obstacles), "dt": sc.dt, "mg_levels": sc.n_level,
+                   "diffusion": sc.diffusion, "parallelism": "replicas" if dist.world > 1 else "single",
+                   "l2": "no flush: the ~25 resident FP64 arrays (~870 MB) exceed the 126 MB L2"},
+        "clocks": clocks,
+        "e2e": {"value": e2e_cells_all / (e2e_ms_max * 1e-3), "unit": "cell-updates/s",
+                "h2d_bytes_per_step": len(STATE_FIELDS) * size * 8,
+                "d2h_bytes_per_step": len(STATE_FIELDS) * size * 8,
+                "what": "per step: u,v,w,p,T uploaded from pinned host memory, one timestep, u,v,w,p,T read back"},
+        "gpu_launches": int(gpu_launches),
+        "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "launches": dom_launches, "avg_launch_us": 1e3 * dom_ms / max(dom_launches, 1)},
+        "kernel_share_ms": {k: round(v, 4) for k, v in sorted(share_ms.items(), key=lambda kv: -kv[1])},
+        "kernel_ms_of_two_steps": round(total_kernel_ms, 4),
+    }
+    sim.close()
+    return out, xml, inner
+
+
+def cpu_baseline(args, inner):
+    """The reference serial build (oracle/_ref) on a bounded sample of the same
+    workload: the first steps of the same scene, steady-state steps timed."""
+    from tests import refdriver
+    if not refdriver.available():
+        return None
+    name, sc = workload(args.workload, args.cpu_steps)
+    tmp = tempfile.mkdtemp(prefix="artss_cpu_")
+    from artss_b200 import scenes
+    xml = scenes.write(sc, os.path.join(tmp, f"{name}_cpu.xml"))
+    t = refdriver.timing(xml, args.cpu_steps)
+    steady = t["step_ms"][1:] or t["step_ms"]
+    value = t["inner_cells"] * len(steady) / (sum(steady) * 1e-3)
+    return {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "sample": f"{args.cpu_steps} steps of the same scene with the unmodified ARTSS serial build "
+                      f"(g++ -O3, one core); steps 2..{args.cpu_steps} timed, step 1 (first-step pressure solve "
+                      f"to tolerance) {t['step_ms'][0]:.0f} ms excluded like the GPU warm-up"}
+
+
+def run_reference(args, dist):
+    """--impl reference: the reference serial build, rank 0 only."""
+    from tests import refdriver
+    name, sc = workload(args.workload, args.warmup + args.steps)
+    if not refdriver.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/artss_ref_driver is not built (make -C oracle ref)"}
+    from artss_b200 import scenes
+    tmp = tempfile.mkdtemp(prefix="artss_ref_")
+    xml = scenes.write(sc, os.path.join(tmp, f"{name}_ref.xml"))
+    t = refdriver.timing(xml, args.warmup + args.steps, timeout=7200)
+    timed = t["step_ms"][args.warmup:args.warmup + args.steps]
+    ms = sum(timed)
+    value = t["inner_cells"] * len(timed) / (ms * 1e-3)
+    return {
+        "impl": "reference",
+        "metric": "cell-updates/s per timestep",
+        "value": value,
+        "unit": "cell-updates/s",
+        "n_gpus": dist.world,
+        "steps": len(timed),
+        "warmup": args.warmup,
+        "ms_per_step": ms / max(len(timed), 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": name, "cells": f"{sc.nx}x{sc.ny}x{sc.nz}", "inner_cells": t["inner_cells"]},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"{args.warmup} warm-up + {len(timed)} timed steps of the unmodified ARTSS "
+                                   "serial build (it has no multi-threaded CPU path; its OpenACC multicore build "
+                                   "needs NVHPC, absent here)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            if dist.rank == 0:
+                print(json.dumps(run_reference(args, dist)), flush=True)
+            return
+        out, xml, inner = run_b200(args, dist)
+        if dist.rank == 0:
+            if dist.world == 1 and not args.no_cpu_baseline:
+                out["cpu_baseline"] = cpu_baseline(args, inner)
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

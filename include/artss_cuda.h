@@ -128,6 +128,18 @@ const char *artss_last_error(void);
 /* Number of kernels this context has launched so far. */
 int64_t artss_ctx_kernel_launches(artss_ctx *ctx);
 
+/* Per-kernel-family timing.  Families whose bit is set in `mask` (bit k =
+ * family k, see artss_kernel_family_name) get a CUDA event pair recorded
+ * around every launch on the context's stream; artss_ctx_profile_read
+ * synchronises the stream and returns, per family, the launches counted since
+ * the last reset (all families, profiled or not) and the summed device time
+ * of the profiled ones. */
+#define ARTSS_KERNEL_FAMILIES 20
+int artss_ctx_profile(artss_ctx *ctx, uint64_t mask);
+int artss_ctx_profile_read(artss_ctx *ctx, int64_t *launches, double *ms, int n_families);
+int artss_ctx_profile_reset(artss_ctx *ctx);
+const char *artss_kernel_family_name(int family);
+
 /* Replaces Field's `new real[]` + `acc enter data` (src/field/Field.cpp:12-53):
  * a zero-filled device array of Nx*Ny*Nz doubles of `level`. */
 int artss_field_alloc(artss_ctx *ctx, int level, double **out);

@@ -60,6 +60,8 @@
 #include "src/field/FieldController.h"
 #include "src/pressure/VCycleMG.h"
 #include "src/solver/SolverSelection.h"
+#include "src/solver/NSTempTurbSolver.h"
+#include "src/source/GaussFunction.h"
 #undef private
 #undef protected
 
@@ -278,7 +280,14 @@ int main(int argc, char **argv) {
         auto dd = DomainData::getInstance();
         const double dt = dd->get_physical_parameters().dt;
         const double t_end = dd->get_physical_parameters().t_end;
-        if (!dump_dir.empty()) dump_fields(dump_dir, 0, fc);
+        if (!dump_dir.empty()) {
+            dump_fields(dump_dir, 0, fc);
+            // spatial part of the Gaussian heat source (GaussFunction.cpp:53-107)
+            if (auto *ns = dynamic_cast<NSTempTurbSolver *>(sc->m_solver))
+                if (auto *gf = dynamic_cast<GaussFunction *>(ns->m_source_function_temperature))
+                    write_raw(dump_dir + "/gauss_spatial.f64", gf->m_field_spatial_values.data,
+                              gf->m_field_spatial_values.get_size() * sizeof(double));
+        }
 
         double t_cur = dt;
         long step = 1;
@@ -303,7 +312,10 @@ int main(int argc, char **argv) {
             double loop_ms = std::chrono::duration<double, std::milli>(loop1 - loop0).count();
             double steady = 0.;
             for (size_t s = 1; s < step_ms.size(); s++) steady += step_ms[s];
-            std::printf("{\"steps\": %ld, \"loop_ms\": %.3f, \"first_step_ms\": %.3f, \"steady_ms_per_step\": %.3f,"
+            std::printf("{\"step_ms\": [");
+            for (size_t s = 0; s < step_ms.size(); s++) std::printf("%s%.3f", s ? ", " : "", step_ms[s]);
+            std::printf("], ");
+            std::printf("\"steps\": %ld, \"loop_ms\": %.3f, \"first_step_ms\": %.3f, \"steady_ms_per_step\": %.3f,"
                         " \"setup_ms\": %.3f, \"inner_cells\": %zu, \"cell_updates_per_s\": %.6e}\n",
                         steps_run, loop_ms, step_ms.empty() ? 0. : step_ms[0],
                         step_ms.size() > 1 ? steady / (double) (step_ms.size() - 1) : 0.,
