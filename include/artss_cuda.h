@@ -251,6 +251,23 @@ int artss_mg_vcycle(artss_mg *mg, double *p);
 /* ||b - A p||_2 over level-0 inner cells (VCycleMG.cpp:186-194) and ||b||_2. */
 int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out);
 
+/* The same two norms for callers that cannot allocate device memory (a host
+ * code whose allocator owns the device, a memory pool that must not grow):
+ * no context, no allocation.  No counterpart in the reference.
+ *  - grid: level 0 of the geometry; flags: device array of the level-0 cell
+ *    flags (bit 0 = inner cell), or NULL when every computational-domain cell
+ *    is inner; p, b: device arrays; stream: cudaStream_t or NULL.
+ *  - The per-block partial sums live in one fixed 128 KiB device array of
+ *    this library, kept on every GPU that loads it until the process exits;
+ *    grids with more than 8192 tiles of 64x4 cells in an x-y plane are
+ *    rejected with ARTSS_ERR_LIMIT.
+ *  - The first call on a device looks the array's address up (with that
+ *    device current); make it before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU race.
+ *  - Blocks until the results are on the host. */
+int artss_residual_norm_static(const artss_grid_desc *grid, const uint8_t *flags, const double *p, const double *b,
+                               void *stream, double *res_out, double *b_norm_out);
+
 #ifdef __cplusplus
 }
 #endif
