@@ -62,7 +62,7 @@ class IterStats(C.Structure):
 
 class MgCfg(C.Structure):
     _fields_ = [("n_level", C.c_int32), ("n_cycle", C.c_int32), ("max_cycle", C.c_int32), ("n_relax", C.c_int32),
-                ("tol_res", C.c_double), ("smoother", C.c_int32), ("reserved", C.c_int32),
+                ("tol_res", C.c_double), ("smoother", C.c_int32), ("flags", C.c_int32),
                 ("smoother_max_iter", C.c_int64), ("smoother_tol_res", C.c_double), ("smoother_w", C.c_double)]
 
 

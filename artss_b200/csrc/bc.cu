@@ -27,7 +27,8 @@ namespace artss {
 __global__ void k_bc_wave(double *__restrict__ f, const int64_t *__restrict__ target,
                           const int64_t *__restrict__ root, const uint8_t *__restrict__ depth,
                           const uint8_t *__restrict__ neg, const double *__restrict__ value,
-                          int64_t begin, int64_t end, int64_t n_total) {
+                          int64_t begin, int64_t end, int64_t n_total, const LoopState *__restrict__ pred) {
+    if (pred && !pred->cond) return;
     for (int64_t q = begin + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < end;
          q += (int64_t) gridDim.x * blockDim.x) {
         double x = f[root[q]];
@@ -41,14 +42,14 @@ __global__ void k_bc_wave(double *__restrict__ f, const int64_t *__restrict__ ta
     }
 }
 
-int apply_bc(artss_ctx *ctx, double *f, int level, int field_type) {
+int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopState *pred) {
     const BcProgram &p = ctx->bc[level][field_type];
     if (!p.present || p.n == 0) return ARTSS_OK;
     for (int w = 0; w < p.waves; w++) {
         const int64_t b = p.wave_begin[w], e = p.wave_begin[w + 1];
         if (e <= b) continue;
         ARTSS_LAUNCH(ctx, FAM_BC, k_bc_wave<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(f, p.d_target, p.d_root, p.d_depth, p.d_neg,
-                                                               p.d_value, b, e, p.n));
+                                                               p.d_value, b, e, p.n, pred));
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;

@@ -86,6 +86,8 @@ struct artss_ctx {
     int64_t launches = 0;
     std::set<double *> fields;
     artss::Profile prof;
+    int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},
+                               {1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1}};
 };
 
 namespace artss {
@@ -171,7 +173,8 @@ inline int check_reduce_blocks(const dim3 &g) {
 }
 
 // Boundary program execution (bc.cu).
-int apply_bc(artss_ctx *ctx, double *f, int level, int field_type);
+// pred != NULL: every launch returns at once when pred->cond == 0 (predicated loop body)
+int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopState *pred = nullptr);
 
 // Reductions (reduce.cu): sum of per-block partials -> loop state `slot`.
 //   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it
@@ -180,6 +183,8 @@ int init_loop(artss_ctx *ctx, int slot, double residual0, long long it0, int con
 int read_loop(artss_ctx *ctx, int slot, LoopState *out);
 // Plain sum of partials into loop slot (no iteration bookkeeping).
 int finalize_sum(artss_ctx *ctx, int slot, int nblocks);
+// sum of partials -> residual = sqrt(sum), no loop bookkeeping
+int finalize_residual(artss_ctx *ctx, int slot, int nblocks);
 
 }  // namespace artss
 

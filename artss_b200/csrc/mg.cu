@@ -10,11 +10,14 @@
 #include "internal.cuh"
 
 #include <algorithm>
+#include <cooperative_groups.h>
 
 struct artss_mg {
     artss_ctx *ctx = nullptr;
     artss_mg_cfg cfg{};
     int L = 0;
+    bool fused_coarse = true;
+    bool cluster_coarse = true;
     double *r0[artss::kMaxLevel + 1]{};   // residuum0[level]   (levels 0..L-1)
     double *r1[artss::kMaxLevel + 1]{};   // residuum1[level]   (levels 0..L)
     double *e0[artss::kMaxLevel + 1]{};   // error0[level]      (levels 0..L-1)
@@ -220,7 +223,7 @@ int mg_resnorm(artss_mg *mg, const double *x, const double *b, int level, int sl
     ARTSS_LAUNCH_CK(ctx);
     const int nb = (int) (grid.x * grid.y * grid.z);
     if (iterate) return finalize_loop(ctx, slot, nb, tol, max_it);
-    return finalize_loop(ctx, slot, nb, -1.0, 1);  // residual only
+    return finalize_residual(ctx, slot, nb);
 }
 
 // VCycleMG::Smooth + call_smooth_{jacobi,colored_gauss_seidel} (VCycleMG.cpp:299-305, :583-723)
@@ -246,12 +249,437 @@ int mg_smooth(artss_mg *mg, double *out, double *tmp, const double *b, int level
 }
 
 // VCycleMG::Solve + call_solve_{jacobi,colored_gauss_seidel} (VCycleMG.cpp:562-581, :620-798)
+// ---------------------------------------------------------------- single-block coarse solve
+//
+// VCycleMG::Solve on a small level runs up to smoother_max_iter sweeps, each
+// followed by the boundary program and a residual norm that decides whether
+// to continue (VCycleMG.cpp:725-798).  On a level of a few thousand cells
+// every one of these passes is launch- and latency-bound, so one 1024-thread
+// block runs the whole loop: sweep, __syncthreads, boundary waves, residual
+// reduced inside the block, decision, next sweep.  The arithmetic per cell is
+// the multigrid Jacobi / colored Gauss-Seidel stencil of the multi-block path.
+
+constexpr int kCoarseThreads = 1024;
+constexpr int64_t kCoarseMaxCells = 1 << 17;  // level array size handled by one block
+constexpr int kCoarseMaxWaves = 8;
+
+struct BcView {
+    const int64_t *target, *root;
+    const uint8_t *depth, *neg;
+    const double *value;
+    int64_t n;
+    int waves;
+    int64_t begin[kCoarseMaxWaves + 1];
+};
+
+// The level's boundary program executed by one block, wave after wave.
+__device__ __forceinline__ void coarse_bc(double *__restrict__ f, const BcView &bc, int tid, int nthr) {
+    for (int w = 0; w < bc.waves; w++) {
+        for (int64_t q = bc.begin[w] + tid; q < bc.begin[w + 1]; q += nthr) {
+            double x = f[bc.root[q]];
+            const int d = bc.depth[q];
+            const uint8_t m = bc.neg[q];
+#pragma unroll
+            for (int s = 0; s < kBcMaxDepth; s++)
+                if (s < d) x = ((m >> s) & 1 ? -x : x) + bc.value[s * bc.n + q];
+            f[bc.target[q]] = x;
+        }
+        __syncthreads();
+    }
+}
+
+// VCycleMG::Solve loop of one level inside one block.  SMEM: the level's
+// arrays (out, and tmp for Jacobi) are copied into shared memory, iterated
+// there, and written back; otherwise they are iterated in global memory.
+template <bool CGS, bool SMEM>
+__global__ void __launch_bounds__(kCoarseThreads)
+k_mg_coarse_solve(double *__restrict__ out, double *__restrict__ tmp, const double *__restrict__ b,
+                  const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
+                  BcView bc, double tol, long long max_it, LoopState *__restrict__ st) {
+    extern __shared__ double sm[];
+    __shared__ double red[32];
+    __shared__ double s_res;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int nj = (int) L.Nx, nk = (int) (L.Nx * L.Ny), ntot = (int) (L.Nx * L.Ny * L.Nz);
+    const int nx = (int) box.nx(), nxy = (int) (box.nx() * box.ny()), ncell = (int) (nxy * box.nz());
+    const int x0 = (int) box.x0, y0 = (int) box.y0, z0 = (int) box.z0;
+    double *A = out, *B = tmp;
+    if (SMEM) {
+        A = sm;
+        B = sm + ntot;
+        for (int q = tid; q < ntot; q += nthr) A[q] = out[q];
+        __syncthreads();
+    }
+    coarse_bc(A, bc, tid, nthr);
+    if (!CGS) {
+        for (int q = tid; q < ntot; q += nthr) B[q] = A[q];
+        __syncthreads();
+    }
+    double res = 10000.;
+    long long it = 0;
+    while (res > tol && it < max_it) {
+        if (CGS) {
+            for (int color = 0; color < 2; color++) {
+                for (int lin = tid; lin < ncell; lin += nthr) {
+                    const int k = z0 + lin / nxy, r = lin % nxy, j = y0 + r / nx, i = x0 + r % nx;
+                    if (((i + j + k) & 1) != color) continue;
+                    const int q = i + nj * j + nk * k;
+                    if (!(__ldg(flags + q) & kInner)) continue;
+                    const double out_h = c.beta * (c.dsign * __ldg(b + q) + c.ax * (A[q + 1] + A[q - 1]) +
+                                                   c.ay * (A[q + nj] + A[q - nj]) + c.az * (A[q + nk] + A[q - nk]));
+                    A[q] = c.omw * A[q] + c.w * out_h;
+                }
+                __syncthreads();
+            }
+        } else {
+            for (int lin = tid; lin < ncell; lin += nthr) {
+                const int k = z0 + lin / nxy, r = lin % nxy, j = y0 + r / nx, i = x0 + r % nx;
+                const int q = i + nj * j + nk * k;
+                if (!(__ldg(flags + q) & kInner)) continue;
+                const double out_h = c.beta * (c.dsign * __ldg(b + q) + c.ax * (B[q + 1] + B[q - 1]) +
+                                               c.ay * (B[q + nj] + B[q - nj]) + c.az * (B[q + nk] + B[q - nk]));
+                A[q] = c.omw * B[q] + c.w * out_h;
+            }
+            __syncthreads();
+        }
+        coarse_bc(A, bc, tid, nthr);
+        double acc = 0.0;
+        for (int lin = tid; lin < ncell; lin += nthr) {
+            const int k = z0 + lin / nxy, r = lin % nxy, j = y0 + r / nx, i = x0 + r % nx;
+            const int q = i + nj * j + nk * k;
+            if (!(__ldg(flags + q) & kInner)) continue;
+            const double rr = __ldg(b + q) - (rx * (A[q - 1] - 2 * A[q] + A[q + 1]) +
+                                             ry * (A[q - nj] - 2 * A[q] + A[q + nj]) +
+                                             rz * (A[q - nk] - 2 * A[q] + A[q + nk]));
+            acc += rr * rr;
+        }
+        acc = artss_block_sum(acc, red);
+        if (tid == 0) s_res = sqrt(acc);
+        __syncthreads();
+        res = s_res;
+        __syncthreads();
+        if (!CGS) {
+            double *t = A;
+            A = B;
+            B = t;
+        }
+        it++;
+    }
+    if (SMEM) {
+        // sm[0..ntot) is out's storage and sm[ntot..) tmp's, whatever the swaps did
+        for (int q = tid; q < ntot; q += nthr) out[q] = sm[q];
+        if (!CGS)
+            for (int q = tid; q < ntot; q += nthr) tmp[q] = sm[ntot + q];
+    }
+    if (tid == 0 && st) {
+        st->it = it;
+        st->residual = res;
+        st->cond = 0;
+    }
+}
+
+constexpr int64_t kCoarseSmemBytes = 200 * 1024;
+
+// ---------------------------------------------------------------- cluster coarse solve
+//
+// The same VCycleMG::Solve loop spread over a thread-block cluster: rank r
+// keeps the z-planes [kb[r], kb[r+1]) of the level's arrays in its shared
+// memory and reaches the other ranks' planes through distributed shared
+// memory (a per-plane pointer table).  Each rank sweeps its own inner cells,
+// whose indices and right-hand side stay in registers for the whole loop; the
+// boundary assignments are dealt out over all ranks; the residual is reduced
+// per block, every rank receives all partial sums and adds them in rank
+// order, so all ranks take the same loop decision.  Cluster barriers separate
+// sweep, boundary waves and reduction.  Per cell the arithmetic is that of
+// k_mg_coarse_solve.
+
+constexpr int kClusterSize = 8;
+constexpr int kClusterThreads = 512;
+constexpr int kClusterCells = 8;        // inner cells per thread
+constexpr int kClusterMaxPlanes = 256;  // z-planes of the level
+
+// Boundary waves over the whole cluster; T maps a z-plane to its storage.
+__device__ __forceinline__ void cluster_bc(double *const *T, const int64_t *begin, int waves, const int64_t *root,
+                                           const int64_t *target, const uint8_t *depth, const uint8_t *neg,
+                                           const double *value, int64_t n, int gtid, int nthr, int nk,
+                                           cooperative_groups::cluster_group &cl) {
+    for (int w = 0; w < waves; w++) {
+        for (int64_t q = begin[w] + gtid; q < begin[w + 1]; q += nthr) {
+            const int r = (int) __ldg(root + q), t = (int) __ldg(target + q);
+            const int kr = r / nk, kt = t / nk;
+            double x = T[kr][r - kr * nk];
+            const int d = __ldg(depth + q);
+            const uint8_t m = __ldg(neg + q);
+#pragma unroll
+            for (int s = 0; s < kBcMaxDepth; s++)
+                if (s < d) x = ((m >> s) & 1 ? -x : x) + __ldg(value + s * n + q);
+            T[kt][t - kt * nk] = x;
+        }
+        cl.sync();
+    }
+}
+
+template <bool CGS>
+__global__ void __launch_bounds__(kClusterThreads, 1)
+k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const double *__restrict__ b,
+                    const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
+                    BcView bc, double tol, long long max_it, int plane_cap, LoopState *__restrict__ st) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ double sm[];
+    __shared__ double *tab0[kClusterMaxPlanes];
+    __shared__ double *tab1[kClusterMaxPlanes];
+    __shared__ double red[32];
+    __shared__ double parts[kClusterSize];
+    __shared__ double s_acc;
+    __shared__ int64_t s_begin[kCoarseMaxWaves + 1];
+    const int tid = threadIdx.x;
+    const int rank = (int) cl.block_rank();
+    const int cs = (int) cl.num_blocks();
+    const int nj = (int) L.Nx, nk = (int) (L.Nx * L.Ny), nz = (int) L.Nz;
+    const int kb0 = (int) ((int64_t) rank * nz / cs), kb1 = (int) ((int64_t) (rank + 1) * nz / cs);
+    double *X0 = sm, *X1 = sm + (int64_t) plane_cap * nk;
+#pragma unroll
+    for (int w = 0; w <= kCoarseMaxWaves; w++)
+        if (tid == w) s_begin[w] = bc.begin[w];
+
+    // own planes of out (and, for Jacobi, nothing yet of tmp)
+    for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) X0[q] = out[(int64_t) kb0 * nk + q];
+    // plane k lives on rank r with kb(r) <= k < kb(r+1)
+    for (int k = tid; k < nz; k += kClusterThreads) {
+        for (int r = 0; r < cs; r++) {
+            const int a = (int) ((int64_t) r * nz / cs), e = (int) ((int64_t) (r + 1) * nz / cs);
+            if (k >= a && k < e) {
+                tab0[k] = cl.map_shared_rank(X0, r) + (int64_t) (k - a) * nk;
+                tab1[k] = cl.map_shared_rank(X1, r) + (int64_t) (k - a) * nk;
+            }
+        }
+    }
+    // this thread's inner cells: plane, in-plane offset and b, in registers
+    int ck[kClusterCells], co[kClusterCells];
+    double cb[kClusterCells];
+    unsigned m0 = 0, m1 = 0;  // cells of colour 0 / 1 (Jacobi: all in m0)
+    {
+        const int z0 = max((int) box.z0, kb0), z1 = min((int) box.z1, kb1 - 1);
+        const int nx = (int) box.nx(), nxy = (int) (box.nx() * box.ny());
+        const int ncell = z1 >= z0 ? (z1 - z0 + 1) * nxy : 0;
+#pragma unroll
+        for (int m = 0; m < kClusterCells; m++) {
+            const int lin = tid + m * kClusterThreads;
+            ck[m] = 0;
+            co[m] = 0;
+            cb[m] = 0.0;
+            if (lin < ncell) {
+                const int k = z0 + lin / nxy, r = lin % nxy, j = (int) box.y0 + r / nx, i = (int) box.x0 + r % nx;
+                const int o = i + nj * j;
+                const int64_t q = (int64_t) k * nk + o;
+                if (__ldg(flags + q) & kInner) {
+                    ck[m] = k;
+                    co[m] = o;
+                    cb[m] = __ldg(b + q);
+                    if (!CGS || ((i + j + k) & 1) == 0) m0 |= 1u << m;
+                    else m1 |= 1u << m;
+                }
+            }
+        }
+    }
+    cl.sync();
+
+    double **TA = tab0, **TB = tab1;
+    const int nthr = cs * kClusterThreads, gtid = rank * kClusterThreads + tid;
+    cluster_bc(TA, s_begin, bc.waves, bc.root, bc.target, bc.depth, bc.neg, bc.value, bc.n, gtid, nthr, nk, cl);
+    if (!CGS) {
+        for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) X1[q] = X0[q];
+        cl.sync();
+    }
+    double res = 10000.;
+    long long it = 0;
+    while (res > tol && it < max_it) {
+        if (CGS) {
+#pragma unroll
+            for (int color = 0; color < 2; color++) {
+                const unsigned mask = color ? m1 : m0;
+#pragma unroll
+                for (int m = 0; m < kClusterCells; m++) {
+                    if (!(mask >> m & 1)) continue;
+                    double *A = TA[ck[m]];
+                    const double *Am = TA[ck[m] - 1], *Ap = TA[ck[m] + 1];
+                    const int o = co[m];
+                    const double out_h = c.beta * (c.dsign * cb[m] + c.ax * (A[o + 1] + A[o - 1]) +
+                                                   c.ay * (A[o + nj] + A[o - nj]) + c.az * (Ap[o] + Am[o]));
+                    A[o] = c.omw * A[o] + c.w * out_h;
+                }
+                cl.sync();
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < kClusterCells; m++) {
+                if (!(m0 >> m & 1)) continue;
+                const double *B = TB[ck[m]], *Bm = TB[ck[m] - 1], *Bp = TB[ck[m] + 1];
+                const int o = co[m];
+                const double out_h = c.beta * (c.dsign * cb[m] + c.ax * (B[o + 1] + B[o - 1]) +
+                                               c.ay * (B[o + nj] + B[o - nj]) + c.az * (Bp[o] + Bm[o]));
+                TA[ck[m]][o] = c.omw * B[o] + c.w * out_h;
+            }
+            cl.sync();
+        }
+        cluster_bc(TA, s_begin, bc.waves, bc.root, bc.target, bc.depth, bc.neg, bc.value, bc.n, gtid, nthr, nk, cl);
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < kClusterCells; m++) {
+            if (!((m0 | m1) >> m & 1)) continue;
+            const double *A = TA[ck[m]], *Am = TA[ck[m] - 1], *Ap = TA[ck[m] + 1];
+            const int o = co[m];
+            const double rr = cb[m] - (rx * (A[o - 1] - 2 * A[o] + A[o + 1]) + ry * (A[o - nj] - 2 * A[o] + A[o + nj]) +
+                                       rz * (Am[o] - 2 * A[o] + Ap[o]));
+            acc += rr * rr;
+        }
+        acc = artss_block_sum(acc, red);
+        if (tid == 0) s_acc = acc;
+        __syncthreads();
+        // thread r sends this rank's sum to rank r
+        if (tid < cs) cl.map_shared_rank(parts, tid)[rank] = s_acc;
+        cl.sync();
+        double s = 0.0;
+        for (int r = 0; r < cs; r++) s += parts[r];
+        res = sqrt(s);
+        if (!CGS) {
+            double **t = TA;
+            TA = TB;
+            TB = t;
+        }
+        it++;
+    }
+    // X0 is out's storage and X1 tmp's, whatever the swaps did
+    for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) {
+        out[(int64_t) kb0 * nk + q] = X0[q];
+        if (!CGS) tmp[(int64_t) kb0 * nk + q] = X1[q];
+    }
+    if (rank == 0 && tid == 0 && st) {
+        st->it = it;
+        st->residual = res;
+        st->cond = 0;
+    }
+    cl.sync();
+}
+
+// Launch shape of the cluster coarse solve, or false when the level does not fit it.
+bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int64_t *smem) {
+    const Level &L = ctx->lvl[level];
+    const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    if (p.present && p.waves > kCoarseMaxWaves) return false;
+    if (L.Nz < kClusterSize || L.Nz > kClusterMaxPlanes || L.size() > (int64_t) 1 << 24) return false;
+    int cap = 0;
+    for (int r = 0; r < kClusterSize; r++) {
+        const int64_t a = (int64_t) r * L.Nz / kClusterSize, e = (int64_t) (r + 1) * L.Nz / kClusterSize;
+        cap = std::max<int>(cap, (int) (e - a));
+        // inner cells of the rank's planes, one thread each per register slot
+        const int64_t z0 = std::max<int64_t>(a, L.k1), z1 = std::min<int64_t>(e - 1, L.k2);
+        const int64_t cells = z1 >= z0 ? (z1 - z0 + 1) * (L.i2 - L.i1 + 1) * (L.j2 - L.j1 + 1) : 0;
+        if (cells > (int64_t) kClusterThreads * kClusterCells) return false;
+    }
+    const int64_t bytes = (cgs ? 1 : 2) * (int64_t) cap * L.nxy() * (int64_t) sizeof(double);
+    if (bytes > kCoarseSmemBytes) return false;
+    *plane_cap = cap;
+    *smem = bytes;
+    return true;
+}
+
+template <bool CGS>
+int launch_coarse_cluster(artss_ctx *ctx, double *out, double *tmp, const double *b, int level, const MgCoef &c,
+                          double rx, double ry, double rz, const BcView &v, double tol, long long mi, int cap,
+                          int64_t smem) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_cluster<CGS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) kCoarseSmemBytes));
+        attr_set = true;
+    }
+    const Level &L = ctx->lvl[level];
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(kClusterSize, 1, 1);
+    lc.blockDim = dim3(kClusterThreads, 1, 1);
+    lc.dynamicSmemBytes = (size_t) smem;
+    lc.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kClusterSize;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_cluster<CGS>, out, tmp, b,
+                                                                  (const uint8_t *) ctx->d_flags[level], L,
+                                                                  inner_box(L), c, rx, ry, rz, v, tol, mi, cap,
+                                                                  ctx->d_loop + 1)));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+// true when the level is handled by k_mg_coarse_solve
+bool coarse_fits(const artss_ctx *ctx, int level) {
+    const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    return ctx->lvl[level].size() <= kCoarseMaxCells && (!p.present || p.waves <= kCoarseMaxWaves);
+}
+
+int mg_coarse_solve(artss_mg *mg, double *out, double *tmp, const double *b, int level) {
+    artss_ctx *ctx = mg->ctx;
+    const Level &L = ctx->lvl[level];
+    const Box3 box = inner_box(L);
+    const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    BcView v{};
+    if (p.present && p.n > 0) {
+        v = BcView{p.d_target, p.d_root, p.d_depth, p.d_neg, p.d_value, p.n, p.waves, {}};
+        for (int w = 0; w <= p.waves; w++) v.begin[w] = p.wave_begin[w];
+    }
+    const artss_grid_desc &g = ctx->grid;
+    const double rx = 1. / (g.dx[level] * g.dx[level]), ry = 1. / (g.dy[level] * g.dy[level]),
+                 rz = 1. / (g.dz[level] * g.dz[level]);
+    const MgCoef c = mg_coef(mg, level);
+    const bool cgs = mg->cfg.smoother == ARTSS_SMOOTHER_CGS;
+    const int64_t smem = (cgs ? 1 : 2) * L.size() * (int64_t) sizeof(double);
+    const double tol = mg->cfg.smoother_tol_res;
+    const long long mi = mg->cfg.smoother_max_iter;
+    int cap = 0;
+    int64_t csmem = 0;
+    if (mg->cluster_coarse && cluster_fits(ctx, level, cgs, &cap, &csmem)) {
+        if (cgs) return launch_coarse_cluster<true>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, mi, cap, csmem);
+        return launch_coarse_cluster<false>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, mi, cap, csmem);
+    }
+    if (smem <= kCoarseSmemBytes) {
+        static bool attr_set[2] = {false, false};
+        if (!attr_set[cgs]) {
+            if (cgs) ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_solve<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kCoarseSmemBytes));
+            else ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_solve<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kCoarseSmemBytes));
+            attr_set[cgs] = true;
+        }
+        if (cgs)
+            ARTSS_LAUNCH(ctx, FAM_MG_COARSE, k_mg_coarse_solve<true, true><<<1, kCoarseThreads, smem, ctx->stream>>>(
+                out, tmp, b, ctx->d_flags[level], L, box, c, rx, ry, rz, v, tol, mi, ctx->d_loop + 1));
+        else
+            ARTSS_LAUNCH(ctx, FAM_MG_COARSE, k_mg_coarse_solve<false, true><<<1, kCoarseThreads, smem, ctx->stream>>>(
+                out, tmp, b, ctx->d_flags[level], L, box, c, rx, ry, rz, v, tol, mi, ctx->d_loop + 1));
+    } else if (cgs) {
+        ARTSS_LAUNCH(ctx, FAM_MG_COARSE, k_mg_coarse_solve<true, false><<<1, kCoarseThreads, 0, ctx->stream>>>(
+            out, tmp, b, ctx->d_flags[level], L, box, c, rx, ry, rz, v, tol, mi, ctx->d_loop + 1));
+    } else {
+        ARTSS_LAUNCH(ctx, FAM_MG_COARSE, k_mg_coarse_solve<false, false><<<1, kCoarseThreads, 0, ctx->stream>>>(
+            out, tmp, b, ctx->d_flags[level], L, box, c, rx, ry, rz, v, tol, mi, ctx->d_loop + 1));
+    }
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
 int mg_solve(artss_mg *mg, double *out, double *tmp, const double *b, int level, int64_t *iterations) {
     artss_ctx *ctx = mg->ctx;
     const Level &L = ctx->lvl[level];
     if (L.Nx <= 4 && L.Ny <= 4) {
         if (iterations) *iterations = 0;
         return mg_smooth(mg, out, tmp, b, level);
+    }
+    if (mg->fused_coarse && coarse_fits(ctx, level)) {
+        if (iterations) *iterations = -1;  // kept on the device (loop slot 1), read on demand
+        return mg_coarse_solve(mg, out, tmp, b, level);
     }
     int st;
     const int slot = 1;
@@ -373,6 +801,8 @@ int artss_mg_create(artss_ctx *ctx, const artss_mg_cfg *cfg, artss_mg **out) {
     mg->ctx = ctx;
     mg->cfg = *cfg;
     mg->L = cfg->n_level;
+    mg->fused_coarse = !(cfg->flags & ARTSS_MG_NO_FUSED_COARSE);
+    mg->cluster_coarse = !(cfg->flags & ARTSS_MG_NO_CLUSTER_COARSE);
     int st = ARTSS_OK;
     // VCycleMG.cpp:51-99: level-0 r1/e1/tmp, levels 0..L-1 r0/e0, 1..L r1/e1/tmp
     st = st ? st : artss_field_alloc(ctx, 0, &mg->r1[0]);

@@ -13,6 +13,8 @@ namespace artss {
 __global__ void k_finalize_loop(const double *__restrict__ partials, int nblocks, LoopState *__restrict__ st,
                                 double tol, long long max_it, int mode) {
     __shared__ double smem[32];
+    // a predicated iteration enqueued after the loop ended changes nothing
+    if (mode == 0 && !st->cond) return;
     double v = 0.0;
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[b];
     v = artss_block_sum(v, smem);
@@ -23,6 +25,8 @@ __global__ void k_finalize_loop(const double *__restrict__ partials, int nblocks
             st->residual = r;
             st->it += 1;
             st->cond = (r > tol && st->it < max_it) ? 1 : 0;
+        } else if (mode == 2) {
+            st->residual = sqrt(v);
         }
     }
 }
@@ -42,6 +46,12 @@ int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long m
 
 int finalize_sum(artss_ctx *ctx, int slot, int nblocks) {
     ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int finalize_residual(artss_ctx *ctx, int slot, int nblocks) {
+    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 2));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }

@@ -221,33 +221,71 @@ __device__ __forceinline__ void turb_alpha(const DiffCoef &c, double ev, double 
 // ColoredGaussSeidelDiffuse.cpp:316-341), in place on `out`; also writes the
 // block partial of sum (rbeta * (new - old))^2, the convergence measure of
 // ColoredGaussSeidelDiffuse.cpp:77-85.
+//
+// Layout: a thread owns a pair of x-neighbours and updates the one of the
+// requested colour, so no lane idles on the other colour; it walks kCgsZ
+// planes two at a time and issues all loads of both cells before either
+// store (cells of one colour never read each other), which keeps enough
+// loads in flight to cover DRAM latency.
+constexpr int kCgsBx = 32, kCgsBy = 8, kCgsZ = 4;
+
+inline dim3 cgs_grid(const Box3 &b) {
+    const int64_t pairs = (b.nx() + 1) / 2;
+    return dim3((unsigned) ((pairs + kCgsBx - 1) / kCgsBx), (unsigned) ((b.ny() + kCgsBy - 1) / kCgsBy),
+                (unsigned) ((b.nz() + kCgsZ - 1) / kCgsZ));
+}
+
 template <bool TURB>
-__global__ void k_cgs_color(double *__restrict__ out, const double *__restrict__ b, const double *__restrict__ ev,
-                            const uint8_t *__restrict__ flags, Level L, Box3 box, int color, DiffCoef c,
-                            double *__restrict__ partials) {
+__global__ void __launch_bounds__(kCgsBx * kCgsBy)
+k_cgs_color(double *__restrict__ out, const double *__restrict__ b, const double *__restrict__ ev,
+            const uint8_t *__restrict__ flags, Level L, Box3 box, int color, DiffCoef c,
+            double *__restrict__ partials, const LoopState *__restrict__ pred) {
     __shared__ double smem[32];
-    ARTSS_COLUMN(box);
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    const int64_t bx = box.x0 + 2 * ((int64_t) blockIdx.x * kCgsBx + threadIdx.x);
+    const int64_t j = box.y0 + (int64_t) blockIdx.y * kCgsBy + threadIdx.y;
+    const int64_t kb = box.z0 + (int64_t) blockIdx.z * kCgsZ;
     const int64_t nj = L.Nx, nk = L.nxy();
     double acc = 0.0;
-    if (col) {
-        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-            if (((i + j + k) & 1) != color) continue;
-            const int64_t q = i + L.Nx * j + nk * k;
-            if (!(flags[q] & kInner)) continue;
-            double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
-            if (TURB) {
-                turb_alpha(c, ev[q], ax, ay, az, rb);
-                beta = 1. / rb;
+    if (bx <= box.x1 && j <= box.y1) {
+#pragma unroll
+        for (int dk = 0; dk < kCgsZ; dk += 2) {
+            bool act[2];
+            int64_t q[2];
+            double xp[2], xm[2], yp[2], ym[2], zp[2], zm[2], old[2], bq[2], eq[2];
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int64_t k = kb + dk + s;
+                const int64_t i = bx + ((bx + j + k + color) & 1);  // (i + j + k) % 2 == color
+                q[s] = i + nj * j + nk * k;
+                act[s] = k <= box.z1 && i <= box.x1 && (flags[q[s]] & kInner);
+                if (act[s]) {
+                    xp[s] = out[q[s] + 1];
+                    xm[s] = out[q[s] - 1];
+                    yp[s] = out[q[s] + nj];
+                    ym[s] = out[q[s] - nj];
+                    zp[s] = out[q[s] + nk];
+                    zm[s] = out[q[s] - nk];
+                    old[s] = out[q[s]];
+                    bq[s] = b[q[s]];
+                    eq[s] = TURB ? ev[q[s]] : 0.0;
+                }
             }
-            const double xp = out[q + 1], xm = out[q - 1];
-            const double yp = out[q + nj], ym = out[q - nj];
-            const double zp = out[q + nk], zm = out[q - nk];
-            const double old = out[q];
-            const double out_h = beta * (c.dsign * b[q] + ax * (xp + xm) + ay * (yp + ym) + az * (zp + zm));
-            const double nw = c.omw * old + c.w * out_h;
-            out[q] = nw;
-            const double res = rb * (nw - old);
-            acc += res * res;
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                if (!act[s]) continue;
+                double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+                if (TURB) {
+                    turb_alpha(c, eq[s], ax, ay, az, rb);
+                    beta = 1. / rb;
+                }
+                const double out_h = beta * (c.dsign * bq[s] + ax * (xp[s] + xm[s]) + ay * (yp[s] + ym[s]) +
+                                             az * (zp[s] + zm[s]));
+                const double nw = c.omw * old[s] + c.w * out_h;
+                out[q[s]] = nw;
+                const double res = rb * (nw - old[s]);
+                acc += res * res;
+            }
         }
     }
     acc = artss_block_sum(acc, smem);
@@ -260,8 +298,9 @@ __global__ void k_cgs_color(double *__restrict__ out, const double *__restrict__
 template <bool TURB>
 __global__ void k_jacobi_diffuse(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
                                  const double *__restrict__ ev, const uint8_t *__restrict__ flags, Level L, Box3 box,
-                                 DiffCoef c, double *__restrict__ partials) {
+                                 DiffCoef c, double *__restrict__ partials, const LoopState *__restrict__ pred) {
     __shared__ double smem[32];
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
     ARTSS_COLUMN(box);
     const int64_t nj = L.Nx, nk = L.nxy();
     double acc = 0.0;
@@ -295,13 +334,30 @@ __global__ void k_jacobi_diffuse(double *__restrict__ out, const double *__restr
 
 // in = out over the domain list (JacobiDiffuse.cpp:85-89)
 __global__ void k_copy_domain(double *__restrict__ dst, const double *__restrict__ src,
-                              const uint8_t *__restrict__ flags, Level L, Box3 box) {
+                              const uint8_t *__restrict__ flags, Level L, Box3 box, const LoopState *__restrict__ pred) {
+    if (pred && !pred->cond) return;
     ARTSS_COLUMN(box);
     if (!col) return;
     for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
         const int64_t q = i + L.Nx * j + L.nxy() * k;
         if (flags[q] & kDomain) dst[q] = src[q];
     }
+}
+
+// whole-array copy that skips itself past convergence (in.copy_data(out) of
+// ColoredGaussSeidelDiffuse.cpp:71 inside a predicated loop)
+__global__ void k_copy_pred(double *__restrict__ dst, const double *__restrict__ src, int64_t n,
+                            const LoopState *__restrict__ pred) {
+    if (!pred->cond) return;
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+// Iterations enqueued per host round trip of a predicated loop: the count the
+// same call site needed last time (usually exact, one round trip), doubled
+// when a batch ends without convergence.
+inline int64_t& loop_hint(artss_ctx *ctx, int site, int field_type) {
+    return ctx->loop_hint[site][field_type & 7];
 }
 
 int check_field_args(artss_ctx *ctx, std::initializer_list<const void *> ptrs) {
@@ -444,9 +500,10 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
     const Level &L = ctx->lvl[0];
     const Box3 box = inner_box(L);
-    const dim3 g = zgrid(box);
+    const dim3 g = cgs_grid(box);
     if ((st = check_reduce_blocks(g))) return st;
     const int nb = nblocks(g);
+    const dim3 blk(kCgsBx, kCgsBy, 1);
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
     if ((st = artss_copy(ctx, out, in, 0))) return st;
@@ -457,29 +514,35 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     bool cond = res > cfg->tol_res && it < cfg->max_iter;
     if ((st = init_loop(ctx, slot, res, 0, cond ? 1 : 0))) return st;
     LoopState ls{};
+    const LoopState *pred = ctx->d_loop + slot;
+    int64_t batch = std::max<int64_t>(1, std::min<int64_t>(loop_hint(ctx, 0, field_type), cfg->max_iter));
+    const int64_t n = L.size();
     while (cond) {
-        if (!in_is_scratch && (st = artss_copy(ctx, in, out, 0))) return st;
-        if (ev) {
-            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 0, c,
-                                                                  ctx->d_partials));
-            ARTSS_LAUNCH_CK(ctx);
-            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, box_block(), 0, ctx->stream>>>(out, b, ev, ctx->d_flags[0], L, box, 1, c,
-                                                                  ctx->d_partials + nb));
-        } else {
-            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 0, c,
-                                                                   ctx->d_partials));
-            ARTSS_LAUNCH_CK(ctx);
-            ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, box_block(), 0, ctx->stream>>>(out, b, nullptr, ctx->d_flags[0], L, box, 1, c,
-                                                                   ctx->d_partials + nb));
+        // `batch` iterations per host round trip; iterations past convergence skip themselves
+        for (int64_t r = 0; r < batch; r++) {
+            if (!in_is_scratch) {
+                ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_copy_pred<<<flat_blocks(n), 256, 0, ctx->stream>>>(in, out, n, pred));
+                ARTSS_LAUNCH_CK(ctx);
+            }
+            for (int color = 0; color < 2; color++) {
+                if (ev)
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, blk, 0, ctx->stream>>>(
+                        out, b, ev, ctx->d_flags[0], L, box, color, c, ctx->d_partials + color * nb, pred));
+                else
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, blk, 0, ctx->stream>>>(
+                        out, b, nullptr, ctx->d_flags[0], L, box, color, c, ctx->d_partials + color * nb, pred));
+                ARTSS_LAUNCH_CK(ctx);
+            }
+            if ((st = apply_bc(ctx, out, 0, field_type, pred))) return st;
+            if ((st = finalize_loop(ctx, slot, 2 * nb, cfg->tol_res, cfg->max_iter))) return st;
         }
-        ARTSS_LAUNCH_CK(ctx);
-        if ((st = apply_bc(ctx, out, 0, field_type))) return st;
-        if ((st = finalize_loop(ctx, slot, 2 * nb, cfg->tol_res, cfg->max_iter))) return st;
         if ((st = read_loop(ctx, slot, &ls))) return st;
         it = ls.it;
         res = ls.residual;
         cond = ls.cond != 0;
+        batch = std::min<int64_t>(2 * batch, std::max<int64_t>(1, cfg->max_iter - it));
     }
+    loop_hint(ctx, 0, field_type) = std::max<int64_t>(1, it);
     if (stats) { stats->iterations = it; stats->residual = res; }
     return ARTSS_OK;
 }
@@ -502,24 +565,31 @@ int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *
     bool cond = res > cfg->tol_res && it < cfg->max_iter;
     if ((st = init_loop(ctx, slot, res, 0, cond ? 1 : 0))) return st;
     LoopState ls{};
+    const LoopState *pred = ctx->d_loop + slot;
+    int64_t batch = std::max<int64_t>(1, std::min<int64_t>(loop_hint(ctx, 1, field_type), cfg->max_iter));
     while (cond) {
-        if (ev) {
-            ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<true><<<g, box_block(), 0, ctx->stream>>>(out, in, b, ev, ctx->d_flags[0], L, box, c,
-                                                                       ctx->d_partials));
-        } else {
-            ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<false><<<g, box_block(), 0, ctx->stream>>>(out, in, b, nullptr, ctx->d_flags[0], L, box,
-                                                                        c, ctx->d_partials));
+        for (int64_t r = 0; r < batch; r++) {
+            if (ev)
+                ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<true><<<g, box_block(), 0, ctx->stream>>>(
+                    out, in, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+            else
+                ARTSS_LAUNCH(ctx, FAM_JACOBI, k_jacobi_diffuse<false><<<g, box_block(), 0, ctx->stream>>>(
+                    out, in, b, nullptr, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+            ARTSS_LAUNCH_CK(ctx);
+            if ((st = apply_bc(ctx, out, 0, field_type, pred))) return st;
+            // in = out before the loop decision: the residual partials are already taken
+            ARTSS_LAUNCH(ctx, FAM_COPY_DOMAIN, k_copy_domain<<<zgrid(dbox), box_block(), 0, ctx->stream>>>(
+                in, out, ctx->d_flags[0], L, dbox, pred));
+            ARTSS_LAUNCH_CK(ctx);
+            if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
         }
-        ARTSS_LAUNCH_CK(ctx);
-        if ((st = apply_bc(ctx, out, 0, field_type))) return st;
-        if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
-        ARTSS_LAUNCH(ctx, FAM_COPY_DOMAIN, k_copy_domain<<<zgrid(dbox), box_block(), 0, ctx->stream>>>(in, out, ctx->d_flags[0], L, dbox));
-        ARTSS_LAUNCH_CK(ctx);
         if ((st = read_loop(ctx, slot, &ls))) return st;
         it = ls.it;
         res = ls.residual;
         cond = ls.cond != 0;
+        batch = std::min<int64_t>(2 * batch, std::max<int64_t>(1, cfg->max_iter - it));
     }
+    loop_hint(ctx, 1, field_type) = std::max<int64_t>(1, it);
     // the final odd-count copy of JacobiDiffuse.cpp:92-99 repeats the last
     // in = out over the domain list and changes nothing
     if (stats) { stats->iterations = it; stats->residual = res; }

@@ -222,7 +222,10 @@ def run_b200(args, dist):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    # NVTX range: a profiler can restrict itself to the timed steps (ncu --nvtx-include "timed_steps/")
+    torch.cuda.nvtx.range_push("timed_steps")
     done = sim.run(args.steps)
+    torch.cuda.nvtx.range_pop()
     e1.record(stream)
     e1.synchronize()
     torch.cuda.synchronize()

@@ -93,6 +93,13 @@ typedef struct {
 
 /* VCycleMG settings (Settings::solver::pressure_solvers::vcycle_mg). */
 enum artss_smoother { ARTSS_SMOOTHER_JACOBI = 0, ARTSS_SMOOTHER_CGS = 1 };
+/* run the coarse solve as separate kernels per sweep (multi-block), not as
+ * one single-block kernel; same results, for levels too large for one block
+ * the multi-block form is used anyway */
+#define ARTSS_MG_NO_FUSED_COARSE 1
+/* keep the fused coarse solve in one thread block instead of spreading it
+ * over a thread-block cluster (distributed shared memory); same results */
+#define ARTSS_MG_NO_CLUSTER_COARSE 2
 typedef struct {
     int32_t n_level;
     int32_t n_cycle;
@@ -100,7 +107,7 @@ typedef struct {
     int32_t n_relax;
     double tol_res;           /* first-step absolute residual tolerance */
     int32_t smoother;         /* enum artss_smoother */
-    int32_t reserved;
+    int32_t flags;            /* ARTSS_MG_* bits */
     int64_t smoother_max_iter;
     double smoother_tol_res;
     double smoother_w;

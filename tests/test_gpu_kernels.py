@@ -1,0 +1,182 @@
+"""Kernel-level parity through the C ABI: every entry point of
+include/artss_cuda.h against the C oracle (oracle/artss_oracle.c, pinned to
+the reference build by test_oracle.py) on seeded random inputs, on a scene
+with an obstacle and three multigrid levels.  Integer/index work and every
+field value must match exactly; only loop-termination residuals are reduced
+in a different order."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import artss_b200 as A
+from artss_b200 import scenes
+from tests import cabi, oracle
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.available(), reason="oracle not built")]
+
+_D = C.POINTER(C.c_double)
+FT = {"u": 1, "v": 2, "w": 3, "p": 4, "T": 5, "nu": 6}
+
+
+@pytest.fixture(scope="module")
+def env(tmp_path_factory):
+    sc = scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=1, n_level=3)
+    xml = scenes.write(sc, str(tmp_path_factory.mktemp("k") / "ch.xml"))
+    geom = A.Geometry(xml)
+    ctx = cabi.Context(geom)
+    osc = oracle.OracleScene(geom)
+    yield sc, geom, ctx, osc
+    ctx.close()
+
+
+def rnd(seed, n, lo=-1.0, hi=1.0):
+    return np.random.default_rng(seed).uniform(lo, hi, n)
+
+
+def P(a):
+    return oracle.p(a)
+
+
+def test_boundary_programs(env):
+    sc, geom, ctx, osc = env
+    L = oracle.lib()
+    for level in range(geom.levels + 1):
+        n = ctx.size(level)
+        for name, ft in FT.items():
+            if geom.boundary_program(level, ft).size == 0:
+                continue
+            x = rnd(level * 10 + ft, n)
+            d = ctx.field(x, level)
+            A.cuda_check(ctx.lib.artss_apply_boundary(ctx.h, d, level, ft), "bc")
+            ref = x.copy()
+            L.oracle_apply_bc(osc.ptr, P(ref), level, ft)
+            assert np.array_equal(ctx.download(d, level), ref), f"level {level} field {name}"
+            assert ctx.lib.artss_boundary_program_waves(ctx.h, level, ft) == 1
+
+
+def test_advect(env):
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    u, v, w = rnd(1, n, -150, 150), rnd(2, n, -150, 150), rnd(3, n, -150, 150)
+    src, out0 = rnd(4, n), rnd(5, n)
+    du, dv, dw, ds, do = (ctx.field(a) for a in (u, v, w, src, out0))
+    A.cuda_check(ctx.lib.artss_advect_sl(ctx.h, do, ds, du, dv, dw, sc.dt, FT["T"]), "advect")
+    ref = out0.copy()
+    oracle.lib().oracle_advect(osc.ptr, P(ref), P(src), P(u), P(v), P(w), sc.dt, FT["T"])
+    assert np.array_equal(ctx.download(do), ref)
+    # fused u,v,w: each output advected by (u,v,w), the inputs being the velocities
+    o1, o2, o3 = ctx.field(out0), ctx.field(out0), ctx.field(out0)
+    A.cuda_check(ctx.lib.artss_advect_sl_uvw(ctx.h, o1, o2, o3, du, dv, dw, du, dv, dw, sc.dt), "uvw")
+    for o, a, ft in ((o1, u, 1), (o2, v, 2), (o3, w, 3)):
+        ref = out0.copy()
+        oracle.lib().oracle_advect(osc.ptr, P(ref), P(a), P(u), P(v), P(w), sc.dt, ft)
+        assert np.array_equal(ctx.download(o), ref)
+
+
+def test_smagorinsky_divergence_projection_sources(env):
+    sc, geom, ctx, osc = env
+    L = oracle.lib()
+    n = ctx.size()
+    u, v, w, p = rnd(11, n), rnd(12, n), rnd(13, n), rnd(14, n)
+    du, dv, dw, dp = (ctx.field(a) for a in (u, v, w, p))
+    ev0 = rnd(15, n)
+    dev = ctx.field(ev0)
+    A.cuda_check(ctx.lib.artss_turb_const_smagorinsky(ctx.h, dev, du, dv, dw, 0.2), "smag")
+    ref = ev0.copy()
+    L.oracle_smagorinsky(osc.ptr, P(ref), P(u), P(v), P(w), 0.2)
+    assert np.array_equal(ctx.download(dev), ref)
+
+    rhs0 = rnd(16, n)
+    drhs = ctx.field(rhs0)
+    A.cuda_check(ctx.lib.artss_divergence(ctx.h, drhs, du, dv, dw), "div")
+    ref = rhs0.copy()
+    L.oracle_divergence(osc.ptr, P(ref), P(u), P(v), P(w))
+    assert np.array_equal(ctx.download(drhs), ref)
+
+    o = [rnd(17 + k, n) for k in range(3)]
+    do = [ctx.field(a) for a in o]
+    A.cuda_check(ctx.lib.artss_projection(ctx.h, do[0], do[1], do[2], du, dv, dw, dp), "proj")
+    ref = [a.copy() for a in o]
+    L.oracle_projection(osc.ptr, P(ref[0]), P(ref[1]), P(ref[2]), P(u), P(v), P(w), P(p))
+    for k in range(3):
+        assert np.array_equal(ctx.download(do[k]), ref[k])
+
+    T, Ta, f0 = rnd(21, n, 290, 310), rnd(22, n, 290, 300), rnd(23, n)
+    dT, dTa, df = ctx.field(T), ctx.field(Ta), ctx.field(f0)
+    A.cuda_check(ctx.lib.artss_buoyancy_force(ctx.h, df, dT, dTa, sc.beta, sc.g), "buoy")
+    ref = f0.copy()
+    L.oracle_buoyancy(osc.ptr, P(ref), P(T), P(Ta), sc.beta, sc.g)
+    assert np.array_equal(ctx.download(df), ref)
+
+    S = rnd(24, n, 0, 50)
+    dS = ctx.field(S)
+    A.cuda_check(ctx.lib.artss_add_source(ctx.h, dT, dS, sc.dt, FT["T"]), "source")
+    ref = T.copy()
+    L.oracle_add_source(osc.ptr, P(ref), P(S), sc.dt, FT["T"])
+    assert np.array_equal(ctx.download(dT), ref)
+
+
+@pytest.mark.parametrize("method", ["cgs", "jacobi"])
+@pytest.mark.parametrize("turbulent", [False, True])
+@pytest.mark.parametrize("scratch", [0, 1])
+def test_diffusion(env, method, turbulent, scratch):
+    if method == "jacobi" and scratch:
+        pytest.skip("the Jacobi solver always keeps its input")
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    out0, in0, b = rnd(31, n, 290, 300), rnd(32, n, 290, 300), rnd(33, n, 290, 300)
+    ev = rnd(34, n, 0, 1e-3)
+    dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
+    cfg = A.IterCfg(9, 1e-12, 1.0)
+    stats = A.IterStats()
+    D = 4.2e-5
+    evp = dev if turbulent else None
+    if method == "cgs":
+        A.cuda_check(ctx.lib.artss_diffuse_cgs(ctx.h, dout, din, db, D, evp, sc.dt, FT["T"], C.byref(cfg), scratch,
+                                               C.byref(stats)), "cgs")
+        fn = oracle.lib().oracle_diffuse_cgs
+    else:
+        A.cuda_check(ctx.lib.artss_diffuse_jacobi(ctx.h, dout, din, db, D, evp, sc.dt, FT["T"], C.byref(cfg),
+                                                  C.byref(stats)), "jacobi")
+        fn = oracle.lib().oracle_diffuse_jacobi
+    ro, ri = out0.copy(), in0.copy()
+    res = C.c_double()
+    its = fn(osc.ptr, P(ro), P(ri), P(b), D, P(ev) if turbulent else None, sc.dt, FT["T"], 9, 1e-12, 1.0,
+             C.byref(res))
+    assert stats.iterations == its and its >= 3
+    assert np.array_equal(ctx.download(dout), ro)
+    if not scratch:
+        assert np.array_equal(ctx.download(din), ri)
+    assert abs(stats.residual - res.value) <= 1e-12 * res.value
+
+
+# coarse solve: "cluster" = one thread-block cluster, "block" = one block,
+# "multi" = separate multi-block launches per sweep
+COARSE_FLAGS = {"cluster": 0, "block": 2, "multi": 1}
+
+
+@pytest.mark.parametrize("smoother", [0, 1])
+@pytest.mark.parametrize("coarse", list(COARSE_FLAGS))
+@pytest.mark.parametrize("first_step", [1, 0])
+def test_vcycle_mg(env, smoother, coarse, first_step):
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    p0, rhs = rnd(41, n), rnd(42, n)
+    cfg = A.MgCfg(3, 2, 3, 2, 1e-30, smoother, COARSE_FLAGS[coarse], 40, 1e-9, 0.6666666667)
+    mg = C.c_void_p()
+    A.cuda_check(ctx.lib.artss_mg_create(ctx.h, C.byref(cfg), C.byref(mg)), "mg")
+    try:
+        dp, drhs = ctx.field(p0), ctx.field(rhs)
+        st = A.MgStats()
+        A.cuda_check(ctx.lib.artss_mg_pressure(mg, dp, drhs, first_step, C.byref(st)), "pressure")
+        ocfg = oracle.MgCfg(3, 2, 3, 2, 1e-30, smoother, 0, 40, 1e-9, 0.6666666667)
+        om = oracle.lib().oracle_mg_create(osc.ptr, C.byref(ocfg))
+        ref = p0.copy()
+        res = C.c_double()
+        cyc = oracle.lib().oracle_mg_pressure(om, P(ref), P(rhs), first_step, C.byref(res))
+        oracle.lib().oracle_mg_destroy(om)
+        assert st.cycles == cyc
+        assert np.array_equal(ctx.download(dp), ref)
+    finally:
+        ctx.lib.artss_mg_destroy(mg)
