@@ -217,79 +217,166 @@ __device__ __forceinline__ void turb_alpha(const DiffCoef &c, double ev, double 
     rb = (1. + 2. * (ax + ay + az));
 }
 
-// One colour of a colored Gauss-Seidel sweep (stencil at
-// ColoredGaussSeidelDiffuse.cpp:316-341), in place on `out`; also writes the
-// block partial of sum (rbeta * (new - old))^2, the convergence measure of
-// ColoredGaussSeidelDiffuse.cpp:77-85.
+// One colored Gauss-Seidel iteration, red then black (stencil at
+// ColoredGaussSeidelDiffuse.cpp:316-341, sweep order :190-295), in ONE pass
+// over the arrays, out of place: `in` holds iterate n (never written), `out`
+// receives iterate n+1 on the inner box; also writes the block partial of
+// sum (rbeta * (new - old))^2 over both colours, the convergence measure of
+// ColoredGaussSeidelDiffuse.cpp:77-85.  The values equal the in-place
+// two-colour sweep: red cells read only black neighbours (old), black cells
+// read only red neighbours (new).
 //
-// Layout: a thread owns a pair of x-neighbours and updates the one of the
-// requested colour, so no lane idles on the other colour; it walks kCgsZ
-// planes two at a time and issues all loads of both cells before either
-// store (cells of one colour never read each other), which keeps enough
-// loads in flight to cover DRAM latency.
-constexpr int kCgsBx = 32, kCgsBy = 8, kCgsZ = 4;
+// A block owns a tile of kSwTx x kSwTy columns over kSwZ planes and marches
+// up in z.  At plane step k it computes red on plane k for the tile plus a
+// one-cell ring (the ring's red values feed the tile's black cells; they are
+// recomputed, never written), then black on plane k-1 for the tile, and
+// writes plane k-1 of the tile to `out`.  Planes of `in`, `b` and `EV` (tile
+// plus a two-cell ring) stream through shared-memory ring buffers by
+// cp.async, kSwD planes ahead of use; a tile's red values replace the old
+// ones in the `in` plane buffer, since only black cells read them afterwards.
+// Non-inner cells of the tile are copied from `in`; the boundary program
+// rewrites the ones anything reads.
+constexpr int kSwTx = 64, kSwTy = 8, kSwZ = 16, kSwD = 2;
+constexpr int kSwThreads = (kSwTx / 2) * kSwTy;            // one thread per x-pair of the tile
+constexpr int kSwWx = kSwTx + 4, kSwWy = kSwTy + 4;         // staged window: tile + 2-cell ring
+constexpr int kSwPlane = kSwWx * kSwWy;
+constexpr int kSwSlotsX = kSwD + 4;                         // x planes k-2 .. k+1+D
+constexpr int kSwSlotsB = kSwD + 3;                         // b / EV planes k-1 .. k+1+D
+constexpr int kSwRedPairs = ((kSwTx + 2) / 2) * (kSwTy + 2);  // x-pairs of the tile + 1-cell ring
 
-inline dim3 cgs_grid(const Box3 &b) {
-    const int64_t pairs = (b.nx() + 1) / 2;
-    return dim3((unsigned) ((pairs + kCgsBx - 1) / kCgsBx), (unsigned) ((b.ny() + kCgsBy - 1) / kCgsBy),
-                (unsigned) ((b.nz() + kCgsZ - 1) / kCgsZ));
+inline dim3 sweep_grid(const Box3 &b) {
+    return dim3((unsigned) ((b.nx() + kSwTx - 1) / kSwTx), (unsigned) ((b.ny() + kSwTy - 1) / kSwTy),
+                (unsigned) ((b.nz() + kSwZ - 1) / kSwZ));
+}
+inline size_t sweep_smem(bool turb) {
+    return sizeof(double) * (size_t) kSwPlane * (kSwSlotsX + (turb ? 2 : 1) * kSwSlotsB);
 }
 
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned) __cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 template <bool TURB>
-__global__ void __launch_bounds__(kCgsBx * kCgsBy)
-k_cgs_color(double *__restrict__ out, const double *__restrict__ b, const double *__restrict__ ev,
-            const uint8_t *__restrict__ flags, Level L, Box3 box, int color, DiffCoef c,
+__global__ void __launch_bounds__(kSwThreads, 2)
+k_cgs_sweep(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
+            const double *__restrict__ ev, const uint8_t *__restrict__ flags, Level L, Box3 box, DiffCoef c,
             double *__restrict__ partials, const LoopState *__restrict__ pred) {
+    extern __shared__ double sw[];
     __shared__ double smem[32];
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
-    const int64_t bx = box.x0 + 2 * ((int64_t) blockIdx.x * kCgsBx + threadIdx.x);
-    const int64_t j = box.y0 + (int64_t) blockIdx.y * kCgsBy + threadIdx.y;
-    const int64_t kb = box.z0 + (int64_t) blockIdx.z * kCgsZ;
+    double *X = sw;                                  // [kSwSlotsX][kSwPlane]
+    double *B = sw + kSwSlotsX * kSwPlane;           // [kSwSlotsB][kSwPlane]
+    double *E = B + kSwSlotsB * kSwPlane;            // [kSwSlotsB][kSwPlane] (TURB)
+    const int tid = threadIdx.x + (kSwTx / 2) * threadIdx.y;
     const int64_t nj = L.Nx, nk = L.nxy();
-    double acc = 0.0;
-    if (bx <= box.x1 && j <= box.y1) {
-#pragma unroll
-        for (int dk = 0; dk < kCgsZ; dk += 2) {
-            bool act[2];
-            int64_t q[2];
-            double xp[2], xm[2], yp[2], ym[2], zp[2], zm[2], old[2], bq[2], eq[2];
-#pragma unroll
-            for (int s = 0; s < 2; s++) {
-                const int64_t k = kb + dk + s;
-                const int64_t i = bx + ((bx + j + k + color) & 1);  // (i + j + k) % 2 == color
-                q[s] = i + nj * j + nk * k;
-                act[s] = k <= box.z1 && i <= box.x1 && (flags[q[s]] & kInner);
-                if (act[s]) {
-                    xp[s] = out[q[s] + 1];
-                    xm[s] = out[q[s] - 1];
-                    yp[s] = out[q[s] + nj];
-                    ym[s] = out[q[s] - nj];
-                    zp[s] = out[q[s] + nk];
-                    zm[s] = out[q[s] - nk];
-                    old[s] = out[q[s]];
-                    bq[s] = b[q[s]];
-                    eq[s] = TURB ? ev[q[s]] : 0.0;
+    const int64_t wx0 = box.x0 + (int64_t) blockIdx.x * kSwTx - 2;  // global i of window column 0
+    const int64_t wy0 = box.y0 + (int64_t) blockIdx.y * kSwTy - 2;
+    const int64_t kc0 = box.z0 + (int64_t) blockIdx.z * kSwZ;
+    const int64_t kc1 = min(kc0 + kSwZ - 1, box.z1);
+
+    // stage plane p of x, b (and EV) into their ring slots; one commit group per plane
+    auto stage = [&](int64_t p) {
+        // planes kc0-2 .. kc1+2 are read; the ring is kept in step past them
+        if (p >= 0 && p < L.Nz && p <= kc1 + 2) {
+            double *xs = X + (int) ((p - kc0 + 2 + 2 * kSwSlotsX) % kSwSlotsX) * kSwPlane;
+            double *bs = B + (int) ((p - kc0 + 2 + 2 * kSwSlotsB) % kSwSlotsB) * kSwPlane;
+            double *es = E + (int) ((p - kc0 + 2 + 2 * kSwSlotsB) % kSwSlotsB) * kSwPlane;
+            for (int e = tid; e < kSwPlane; e += kSwThreads) {
+                const int ly = e / kSwWx, lx = e - ly * kSwWx;
+                const int64_t gi = wx0 + lx, gj = wy0 + ly;
+                if (gi < 0 || gi >= L.Nx || gj < 0 || gj >= L.Ny) continue;
+                const int64_t q = gi + nj * gj + nk * p;
+                cp_async8(xs + e, in + q);
+                // b and EV are read on the tile and its 1-cell ring only
+                if (lx >= 1 && lx <= kSwTx + 2 && ly >= 1 && ly <= kSwTy + 2) {
+                    cp_async8(bs + e, b + q);
+                    if (TURB) cp_async8(es + e, ev + q);
                 }
             }
+        }
+        cp_async_commit();
+    };
+    auto xslot = [&](int64_t p) { return X + (int) ((p - kc0 + 2 + 2 * kSwSlotsX) % kSwSlotsX) * kSwPlane; };
+    auto bslot = [&](int64_t p) { return (int) ((p - kc0 + 2 + 2 * kSwSlotsB) % kSwSlotsB) * kSwPlane; };
+
+    // one stencil update; returns the new value and the residual term
+    auto update = [&](const double *xm, const double *x0, const double *xp, int e, int bo, double &res2) {
+        double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+        if (TURB) {
+            turb_alpha(c, E[bo + e], ax, ay, az, rb);
+            beta = 1. / rb;
+        }
+        const double old = x0[e];
+        const double out_h = beta * (c.dsign * B[bo + e] + ax * (x0[e + 1] + x0[e - 1]) +
+                                     ay * (x0[e + kSwWx] + x0[e - kSwWx]) + az * (xp[e] + xm[e]));
+        const double nw = c.omw * old + c.w * out_h;
+        const double r = rb * (nw - old);
+        res2 = r * r;
+        return nw;
+    };
+
+    for (int64_t p = kc0 - 2; p <= kc0 - 1 + kSwD; p++) stage(p);
+    double acc = 0.0;
+    for (int64_t k = kc0 - 1; k <= kc1 + 1; k++) {
+        cp_async_wait<kSwD - 1>();  // planes up to k+1 have landed
+        __syncthreads();            // ... and step k-1 is done with the slots refilled next
+        stage(k + 1 + kSwD);
+        // red on plane k, tile + 1-cell ring
+        if (k >= box.z0 && k <= box.z1) {
+            const double *xm = xslot(k - 1), *xp = xslot(k + 1);
+            double *x0 = xslot(k);
+            const int bo = bslot(k);
+            for (int pr = tid; pr < kSwRedPairs; pr += kSwThreads) {
+                const int ry = 1 + pr / ((kSwTx + 2) / 2);
+                const int px = pr - (ry - 1) * ((kSwTx + 2) / 2);
+                const int64_t gj = wy0 + ry;
+                const int rx = 1 + 2 * px + (int) ((wx0 + 1 + gj + k) & 1);  // (i + j + k) even
+                const int64_t gi = wx0 + rx;
+                if (gi < box.x0 || gi > box.x1 || gj < box.y0 || gj > box.y1) continue;
+                if (!(__ldg(flags + gi + nj * gj + nk * k) & kInner)) continue;
+                const int e = rx + kSwWx * ry;
+                double r2;
+                const double nw = update(xm, x0, xp, e, bo, r2);
+                x0[e] = nw;
+                if (rx >= 2 && rx < kSwTx + 2 && ry >= 2 && ry < kSwTy + 2 && k >= kc0 && k <= kc1) acc += r2;
+            }
+        }
+        __syncthreads();
+        // black on plane k-1, tile only, and the tile's plane k-1 out
+        const int64_t kb = k - 1;
+        if (kb >= kc0 && kb <= kc1) {
+            const double *xm = xslot(kb - 1), *xp = xslot(kb + 1);
+            const double *x0 = xslot(kb);
+            const int bo = bslot(kb);
+            const int ty = threadIdx.y, tx = threadIdx.x;
+            const int64_t gj = wy0 + 2 + ty;
+            const int lx0 = 2 + 2 * tx;
+            const int par = (int) ((wx0 + lx0 + gj + kb + 1) & 1);  // (i + j + k) odd
+            const int e0 = lx0 + kSwWx * (2 + ty);
+            if (gj <= box.y1) {
 #pragma unroll
-            for (int s = 0; s < 2; s++) {
-                if (!act[s]) continue;
-                double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
-                if (TURB) {
-                    turb_alpha(c, eq[s], ax, ay, az, rb);
-                    beta = 1. / rb;
+                for (int s = 0; s < 2; s++) {
+                    const int64_t gi = wx0 + lx0 + s;
+                    if (gi > box.x1) continue;
+                    const int64_t q = gi + nj * gj + nk * kb;
+                    double v = x0[e0 + s];
+                    if (s == par && (__ldg(flags + q) & kInner)) {
+                        double r2;
+                        v = update(xm, x0, xp, e0 + s, bo, r2);
+                        acc += r2;
+                    }
+                    out[q] = v;
                 }
-                const double out_h = beta * (c.dsign * bq[s] + ax * (xp[s] + xm[s]) + ay * (yp[s] + ym[s]) +
-                                             az * (zp[s] + zm[s]));
-                const double nw = c.omw * old[s] + c.w * out_h;
-                out[q[s]] = nw;
-                const double res = rb * (nw - old[s]);
-                acc += res * res;
             }
         }
     }
+    cp_async_wait<0>();
     acc = artss_block_sum(acc, smem);
-    if (partials && threadIdx.x == 0 && threadIdx.y == 0) partials[block_linear()] = acc;
+    if (partials && tid == 0) partials[block_linear()] = acc;
 }
 
 // One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
@@ -344,13 +431,13 @@ __global__ void k_copy_domain(double *__restrict__ dst, const double *__restrict
     }
 }
 
-// whole-array copy that skips itself past convergence (in.copy_data(out) of
-// ColoredGaussSeidelDiffuse.cpp:71 inside a predicated loop)
-__global__ void k_copy_pred(double *__restrict__ dst, const double *__restrict__ src, int64_t n,
-                            const LoopState *__restrict__ pred) {
-    if (!pred->cond) return;
-    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
-        dst[i] = src[i];
+// exchanges two arrays element by element
+__global__ void k_swap(double *__restrict__ x, double *__restrict__ y, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        const double t = x[i];
+        x[i] = y[i];
+        y[i] = t;
+    }
 }
 
 // Iterations enqueued per host round trip of a predicated loop: the count the
@@ -498,12 +585,15 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     int st = check_field_args(ctx, {out, in, b, cfg});
     if (st || (st = check_field_type(field_type))) return st;
     if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
+    if (out == in || b == out || b == in) { set_error("out, in and b must be distinct arrays"); return ARTSS_ERR_ARG; }
     const Level &L = ctx->lvl[0];
     const Box3 box = inner_box(L);
-    const dim3 g = cgs_grid(box);
+    const dim3 g = sweep_grid(box);
     if ((st = check_reduce_blocks(g))) return st;
     const int nb = nblocks(g);
-    const dim3 blk(kCgsBx, kCgsBy, 1);
+    const size_t smem = sweep_smem(ev != nullptr);
+    if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
     if ((st = artss_copy(ctx, out, in, 0))) return st;
@@ -516,31 +606,44 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     LoopState ls{};
     const LoopState *pred = ctx->d_loop + slot;
     int64_t batch = std::max<int64_t>(1, std::min<int64_t>(loop_hint(ctx, 0, field_type), cfg->max_iter));
-    const int64_t n = L.size();
+    // The reference sweeps `out` in place after in.copy_data(out) (:69-76); here
+    // iteration n reads iterate n-1 from one of {out, in} and writes iterate n
+    // into the other, so after n iterations the two arrays hold exactly what the
+    // reference's out and in hold, possibly exchanged.  The first direction is
+    // chosen so that a solve of the predicted length ends in out.
+    double *buf[2] = {out, in};
+    const int s0 = (int) (batch & 1);  // iteration n writes buf[(s0 + n) & 1]
     while (cond) {
         // `batch` iterations per host round trip; iterations past convergence skip themselves
         for (int64_t r = 0; r < batch; r++) {
-            if (!in_is_scratch) {
-                ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_copy_pred<<<flat_blocks(n), 256, 0, ctx->stream>>>(in, out, n, pred));
-                ARTSS_LAUNCH_CK(ctx);
-            }
-            for (int color = 0; color < 2; color++) {
-                if (ev)
-                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<true><<<g, blk, 0, ctx->stream>>>(
-                        out, b, ev, ctx->d_flags[0], L, box, color, c, ctx->d_partials + color * nb, pred));
-                else
-                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_color<false><<<g, blk, 0, ctx->stream>>>(
-                        out, b, nullptr, ctx->d_flags[0], L, box, color, c, ctx->d_partials + color * nb, pred));
-                ARTSS_LAUNCH_CK(ctx);
-            }
-            if ((st = apply_bc(ctx, out, 0, field_type, pred))) return st;
-            if ((st = finalize_loop(ctx, slot, 2 * nb, cfg->tol_res, cfg->max_iter))) return st;
+            const long long n = it + 1 + r;
+            double *w = buf[(s0 + n) & 1];
+            const double *rd = buf[(s0 + n + 1) & 1];
+            if (ev)
+                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, kSwThreads, smem, ctx->stream>>>(
+                    w, rd, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+            else
+                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<false><<<g, kSwThreads, smem, ctx->stream>>>(
+                    w, rd, b, nullptr, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+            ARTSS_LAUNCH_CK(ctx);
+            if ((st = apply_bc(ctx, w, 0, field_type, pred))) return st;
+            if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
         }
         if ((st = read_loop(ctx, slot, &ls))) return st;
         it = ls.it;
         res = ls.residual;
         cond = ls.cond != 0;
         batch = std::min<int64_t>(2 * batch, std::max<int64_t>(1, cfg->max_iter - it));
+    }
+    if (it > 0 && ((s0 + it) & 1)) {
+        // the last iterate sits in `in`: exchange (the caller keeps in) or copy back
+        const int64_t n = L.size();
+        if (in_is_scratch) {
+            if ((st = artss_copy(ctx, out, in, 0))) return st;
+        } else {
+            ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_swap<<<flat_blocks(n), 256, 0, ctx->stream>>>(out, in, n));
+            ARTSS_LAUNCH_CK(ctx);
+        }
     }
     loop_hint(ctx, 0, field_type) = std::max<int64_t>(1, it);
     if (stats) { stats->iterations = it; stats->residual = res; }

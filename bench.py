@@ -164,8 +164,8 @@ class Dist:
 def launch_bytes(family: str, n: int, N: int, launches: int) -> float:
     if family == "advect":       # per step: fused u,v,w (read u0,v0,w0; write u,v,w: 48 B) + T (read u,v,w,T0; write T: 40 B)
         return launches / 2 * (48 + 40) * n
-    if family == "cgs_color":    # one colour: read x (all), b, EV and write x of half the cells: 8 + 0.5*24 B
-        return launches * 20.0 * n
+    if family == "cgs_sweep":    # one red+black iteration: read x, b, EV (turbulent), write x: 32 B
+        return launches * 32.0 * n
     if family == "smagorinsky":  # read u, v, w; write nu_t
         return launches * 32.0 * n
     if family == "couple":       # per step 4 vector couples (read 3, write 6 arrays) + 4 scalar (read 1, write 2)
@@ -175,7 +175,7 @@ def launch_bytes(family: str, n: int, N: int, launches: int) -> float:
     return 0.0
 
 
-MODELED = ("advect", "cgs_color", "smagorinsky", "couple", "projection")
+MODELED = ("advect", "cgs_sweep", "smagorinsky", "couple", "projection")
 
 
 def run_b200(args, dist):

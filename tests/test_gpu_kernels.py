@@ -180,3 +180,28 @@ def test_vcycle_mg(env, smoother, coarse, first_step):
         assert np.array_equal(ctx.download(dp), ref)
     finally:
         ctx.lib.artss_mg_destroy(mg)
+
+
+@pytest.mark.parametrize("scratch", [0, 1])
+def test_cgs_iteration_parity(env, scratch):
+    """Solves of 3..6 iterations in a row: the sweep alternates between out and
+    in, so each length ends in either array depending on the previous length;
+    out (and in, when kept) must always match the in-place reference."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    for its_req in (3, 4, 4, 5, 6, 3):
+        out0, in0, b = rnd(51, n, 290, 300), rnd(52 + its_req, n, 290, 300), rnd(53, n, 290, 300)
+        ev = rnd(54, n, 0, 1e-3)
+        dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
+        cfg = A.IterCfg(its_req, 1e-300, 1.0)
+        stats = A.IterStats()
+        A.cuda_check(ctx.lib.artss_diffuse_cgs(ctx.h, dout, din, db, 4.2e-5, dev, sc.dt, FT["u"], C.byref(cfg),
+                                               scratch, C.byref(stats)), "cgs")
+        ro, ri = out0.copy(), in0.copy()
+        res = C.c_double()
+        its = oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev), sc.dt, FT["u"], its_req,
+                                              1e-300, 1.0, C.byref(res))
+        assert stats.iterations == its == its_req
+        assert np.array_equal(ctx.download(dout), ro)
+        if not scratch:
+            assert np.array_equal(ctx.download(din), ri)
