@@ -55,6 +55,36 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopSta
     return ARTSS_OK;
 }
 
+// The boundary program with every value taken as zero, on FP32 storage: the
+// homogeneous conditions of a correction equation (mixed-precision pressure
+// solve); only the sign chain of each folded assignment remains.
+__global__ void k_bc_wave_f32(float *__restrict__ f, const int64_t *__restrict__ target,
+                              const int64_t *__restrict__ root, const uint8_t *__restrict__ depth,
+                              const uint8_t *__restrict__ neg, int64_t begin, int64_t end,
+                              const LoopState *__restrict__ pred) {
+    if (pred && !pred->cond) return;
+    for (int64_t q = begin + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < end;
+         q += (int64_t) gridDim.x * blockDim.x) {
+        const int d = depth[q];
+        const unsigned flips = __popc((unsigned) neg[q] & ((1u << d) - 1u));
+        const float x = f[root[q]];
+        f[target[q]] = (flips & 1u) ? -x : x;
+    }
+}
+
+int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const LoopState *pred) {
+    const BcProgram &p = ctx->bc[level][field_type];
+    if (!p.present || p.n == 0) return ARTSS_OK;
+    for (int w = 0; w < p.waves; w++) {
+        const int64_t b = p.wave_begin[w], e = p.wave_begin[w + 1];
+        if (e <= b) continue;
+        ARTSS_LAUNCH(ctx, FAM_BC, k_bc_wave_f32<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(
+                                      f, p.d_target, p.d_root, p.d_depth, p.d_neg, b, e, pred));
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    return ARTSS_OK;
+}
+
 namespace {
 
 struct Folded {

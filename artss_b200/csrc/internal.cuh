@@ -176,6 +176,13 @@ inline int check_reduce_blocks(const dim3 &g) {
 // pred != NULL: every launch returns at once when pred->cond == 0 (predicated loop body)
 int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopState *pred = nullptr);
 
+// Homogeneous boundary program (values zero) on FP32 storage (bc.cu).
+int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const LoopState *pred = nullptr);
+// FP64 cluster solve of a level's pressure equation on FP32 storage, zero
+// boundary values, tolerance relative to the initial residual (mg.cu).
+int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
+                       long long max_it, const LoopState *pred);
+
 // Reductions (reduce.cu): sum of per-block partials -> loop state `slot`.
 //   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it
 int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it);

@@ -412,19 +412,51 @@ __device__ __forceinline__ void cluster_bc(double *const *T, const int64_t *begi
             const uint8_t m = __ldg(neg + q);
 #pragma unroll
             for (int s = 0; s < kBcMaxDepth; s++)
-                if (s < d) x = ((m >> s) & 1 ? -x : x) + __ldg(value + s * n + q);
+                if (s < d) x = ((m >> s) & 1 ? -x : x) + (value ? __ldg(value + s * n + q) : 0.0);
             T[kt][t - kt * nk] = x;
         }
         cl.sync();
     }
 }
 
-template <bool CGS>
+// ||b - A x||_2 over the cluster's inner cells, identical in every rank
+template <int NC>
+__device__ __forceinline__ double cluster_resnorm(double *const *T, const int (&ck)[NC], const int (&co)[NC],
+                                                  const double (&cb)[NC], unsigned mask, int nj, double rx, double ry,
+                                                  double rz, double *red, double *s_acc, double *parts, int rank,
+                                                  int cs, cooperative_groups::cluster_group &cl) {
+    double acc = 0.0;
+#pragma unroll
+    for (int m = 0; m < NC; m++) {
+        if (!(mask >> m & 1)) continue;
+        const double *A = T[ck[m]], *Am = T[ck[m] - 1], *Ap = T[ck[m] + 1];
+        const int o = co[m];
+        const double rr = cb[m] - (rx * (A[o - 1] - 2 * A[o] + A[o + 1]) + ry * (A[o - nj] - 2 * A[o] + A[o + nj]) +
+                                   rz * (Am[o] - 2 * A[o] + Ap[o]));
+        acc += rr * rr;
+    }
+    acc = artss_block_sum(acc, red);
+    if (threadIdx.x == 0) *s_acc = acc;
+    __syncthreads();
+    // thread r sends this rank's sum to rank r
+    if ((int) threadIdx.x < cs) cl.map_shared_rank(parts, (int) threadIdx.x)[rank] = *s_acc;
+    cl.sync();
+    double s = 0.0;
+    for (int r = 0; r < cs; r++) s += parts[r];
+    return sqrt(s);
+}
+
+// TS: storage type of out / tmp / b (the arithmetic is FP64 either way).
+// rel: tol is relative to the residual of the initial iterate.
+// pred: the launch does nothing when pred->cond == 0 (predicated loops).
+template <bool CGS, typename TS>
 __global__ void __launch_bounds__(kClusterThreads, 1)
-k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const double *__restrict__ b,
+k_mg_coarse_cluster(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restrict__ b,
                     const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
-                    BcView bc, double tol, long long max_it, int plane_cap, LoopState *__restrict__ st) {
+                    BcView bc, double tol, int rel, long long max_it, int plane_cap, LoopState *__restrict__ st,
+                    const LoopState *__restrict__ pred) {
     namespace cg = cooperative_groups;
+    if (pred && !pred->cond) return;  // every rank reads the same flag
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double sm[];
     __shared__ double *tab0[kClusterMaxPlanes];
@@ -444,7 +476,7 @@ k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const do
         if (tid == w) s_begin[w] = bc.begin[w];
 
     // own planes of out (and, for Jacobi, nothing yet of tmp)
-    for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) X0[q] = out[(int64_t) kb0 * nk + q];
+    for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) X0[q] = (double) out[(int64_t) kb0 * nk + q];
     // plane k lives on rank r with kb(r) <= k < kb(r+1)
     for (int k = tid; k < nz; k += kClusterThreads) {
         for (int r = 0; r < cs; r++) {
@@ -476,7 +508,7 @@ k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const do
                 if (__ldg(flags + q) & kInner) {
                     ck[m] = k;
                     co[m] = o;
-                    cb[m] = __ldg(b + q);
+                    cb[m] = (double) b[q];
                     if (!CGS || ((i + j + k) & 1) == 0) m0 |= 1u << m;
                     else m1 |= 1u << m;
                 }
@@ -494,6 +526,7 @@ k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const do
     }
     double res = 10000.;
     long long it = 0;
+    if (rel) tol *= cluster_resnorm(TA, ck, co, cb, m0 | m1, nj, rx, ry, rz, red, &s_acc, parts, rank, cs, cl);
     while (res > tol && it < max_it) {
         if (CGS) {
 #pragma unroll
@@ -524,25 +557,7 @@ k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const do
             cl.sync();
         }
         cluster_bc(TA, s_begin, bc.waves, bc.root, bc.target, bc.depth, bc.neg, bc.value, bc.n, gtid, nthr, nk, cl);
-        double acc = 0.0;
-#pragma unroll
-        for (int m = 0; m < kClusterCells; m++) {
-            if (!((m0 | m1) >> m & 1)) continue;
-            const double *A = TA[ck[m]], *Am = TA[ck[m] - 1], *Ap = TA[ck[m] + 1];
-            const int o = co[m];
-            const double rr = cb[m] - (rx * (A[o - 1] - 2 * A[o] + A[o + 1]) + ry * (A[o - nj] - 2 * A[o] + A[o + nj]) +
-                                       rz * (Am[o] - 2 * A[o] + Ap[o]));
-            acc += rr * rr;
-        }
-        acc = artss_block_sum(acc, red);
-        if (tid == 0) s_acc = acc;
-        __syncthreads();
-        // thread r sends this rank's sum to rank r
-        if (tid < cs) cl.map_shared_rank(parts, tid)[rank] = s_acc;
-        cl.sync();
-        double s = 0.0;
-        for (int r = 0; r < cs; r++) s += parts[r];
-        res = sqrt(s);
+        res = cluster_resnorm(TA, ck, co, cb, m0 | m1, nj, rx, ry, rz, red, &s_acc, parts, rank, cs, cl);
         if (!CGS) {
             double **t = TA;
             TA = TB;
@@ -552,8 +567,8 @@ k_mg_coarse_cluster(double *__restrict__ out, double *__restrict__ tmp, const do
     }
     // X0 is out's storage and X1 tmp's, whatever the swaps did
     for (int q = tid; q < (kb1 - kb0) * nk; q += kClusterThreads) {
-        out[(int64_t) kb0 * nk + q] = X0[q];
-        if (!CGS) tmp[(int64_t) kb0 * nk + q] = X1[q];
+        out[(int64_t) kb0 * nk + q] = (TS) X0[q];
+        if (!CGS && tmp) tmp[(int64_t) kb0 * nk + q] = (TS) X1[q];
     }
     if (rank == 0 && tid == 0 && st) {
         st->it = it;
@@ -585,13 +600,13 @@ bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int
     return true;
 }
 
-template <bool CGS>
-int launch_coarse_cluster(artss_ctx *ctx, double *out, double *tmp, const double *b, int level, const MgCoef &c,
-                          double rx, double ry, double rz, const BcView &v, double tol, long long mi, int cap,
-                          int64_t smem) {
+template <bool CGS, typename TS>
+int launch_coarse_cluster(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level, const MgCoef &c, double rx,
+                          double ry, double rz, const BcView &v, double tol, int rel, long long mi, int cap,
+                          int64_t smem, LoopState *st, const LoopState *pred) {
     static bool attr_set = false;
     if (!attr_set) {
-        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_cluster<CGS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_cluster<CGS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int) kCoarseSmemBytes));
         attr_set = true;
     }
@@ -608,12 +623,53 @@ int launch_coarse_cluster(artss_ctx *ctx, double *out, double *tmp, const double
     at[0].val.clusterDim.z = 1;
     lc.attrs = at;
     lc.numAttrs = 1;
-    ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_cluster<CGS>, out, tmp, b,
+    ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_cluster<CGS, TS>, out, tmp, b,
                                                                   (const uint8_t *) ctx->d_flags[level], L,
-                                                                  inner_box(L), c, rx, ry, rz, v, tol, mi, cap,
-                                                                  ctx->d_loop + 1)));
+                                                                  inner_box(L), c, rx, ry, rz, v, tol, rel, mi, cap,
+                                                                  st, pred)));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
+}
+
+BcView bc_view(const artss_ctx *ctx, int level) {
+    const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    BcView v{};
+    if (p.present && p.n > 0) {
+        v = BcView{p.d_target, p.d_root, p.d_depth, p.d_neg, p.d_value, p.n, p.waves, {}};
+        for (int w = 0; w <= p.waves; w++) v.begin[w] = p.wave_begin[w];
+    }
+    return v;
+}
+
+// FP64 solve of one level's pressure system by the cluster kernel on FP32
+// storage (the coarsest-grid solve of the mixed-precision V-cycle); the
+// level's boundary values are taken as zero, tol is relative to the initial
+// residual.
+int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
+                       long long max_it, const LoopState *pred) {
+    const bool cgs = smoother == ARTSS_SMOOTHER_CGS;
+    int cap = 0;
+    int64_t smem = 0;
+    if (!cluster_fits(ctx, level, cgs, &cap, &smem)) {
+        set_error("the coarsest level does not fit the cluster coarse solve");
+        return ARTSS_ERR_LIMIT;
+    }
+    const artss_grid_desc &g = ctx->grid;
+    MgCoef c{};
+    c.ax = 1. / (g.dx[level] * g.dx[level]);
+    c.ay = 1. / (g.dy[level] * g.dy[level]);
+    c.az = 1. / (g.dz[level] * g.dz[level]);
+    c.beta = 1. / (2. * (c.ax + c.ay + c.az));
+    c.dsign = -1;
+    c.w = w;
+    c.omw = 1 - w;
+    BcView v = bc_view(ctx, level);
+    v.value = nullptr;  // homogeneous: the correction equation has zero boundary values
+    if (cgs)
+        return launch_coarse_cluster<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
+                                                  cap, smem, nullptr, pred);
+    return launch_coarse_cluster<false, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it, cap,
+                                               smem, nullptr, pred);
 }
 
 // true when the level is handled by k_mg_coarse_solve
@@ -643,8 +699,11 @@ int mg_coarse_solve(artss_mg *mg, double *out, double *tmp, const double *b, int
     int cap = 0;
     int64_t csmem = 0;
     if (mg->cluster_coarse && cluster_fits(ctx, level, cgs, &cap, &csmem)) {
-        if (cgs) return launch_coarse_cluster<true>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, mi, cap, csmem);
-        return launch_coarse_cluster<false>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, mi, cap, csmem);
+        if (cgs)
+            return launch_coarse_cluster<true, double>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, 0, mi, cap, csmem,
+                                                       ctx->d_loop + 1, nullptr);
+        return launch_coarse_cluster<false, double>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, 0, mi, cap, csmem,
+                                                    ctx->d_loop + 1, nullptr);
     }
     if (smem <= kCoarseSmemBytes) {
         static bool attr_set[2] = {false, false};

@@ -268,6 +268,7 @@ k_cgs_sweep(double *__restrict__ out, const double *__restrict__ in, const doubl
     extern __shared__ double sw[];
     __shared__ double smem[32];
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    if (blockDim.x != kSwTx / 2 || blockDim.y != kSwTy || blockDim.z != 1) return;  // launch shape is fixed
     double *X = sw;                                  // [kSwSlotsX][kSwPlane]
     double *B = sw + kSwSlotsX * kSwPlane;           // [kSwSlotsB][kSwPlane]
     double *E = B + kSwSlotsB * kSwPlane;            // [kSwSlotsB][kSwPlane] (TURB)
@@ -620,10 +621,10 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
             double *w = buf[(s0 + n) & 1];
             const double *rd = buf[(s0 + n + 1) & 1];
             if (ev)
-                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, kSwThreads, smem, ctx->stream>>>(
+                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
                     w, rd, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
             else
-                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<false><<<g, kSwThreads, smem, ctx->stream>>>(
+                ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<false><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
                     w, rd, b, nullptr, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
             ARTSS_LAUNCH_CK(ctx);
             if ((st = apply_bc(ctx, w, 0, field_type, pred))) return st;
