@@ -70,6 +70,18 @@ class MgStats(C.Structure):
     _fields_ = [("cycles", C.c_int64), ("coarse_iterations", C.c_int64), ("residual", C.c_double)]
 
 
+class MixedCfg(C.Structure):
+    _fields_ = [("n_level", C.c_int32), ("n_relax", C.c_int32), ("coarse_smoother", C.c_int32), ("flags", C.c_int32),
+                ("w", C.c_double), ("coarse_w", C.c_double), ("coarse_rel_tol", C.c_double),
+                ("coarse_max_iter", C.c_int64), ("rel_tol", C.c_double), ("max_cycles", C.c_int64)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("cycles", C.c_int64), ("residual", C.c_double), ("rel_residual", C.c_double), ("b_norm", C.c_double)]
+
+
+MIXED_REMOVE_MEAN = 1
+
 BC_DTYPE = np.dtype([("target", "<i8"), ("source", "<i8"), ("value", "<f8"), ("sign", "<i4"), ("reserved", "<i4")])
 
 _cuda: Optional[C.CDLL] = None
@@ -133,6 +145,10 @@ def load_cuda() -> C.CDLL:
             "artss_mg_set_rhs": ([_P, _D, _D], C.c_int),
             "artss_mg_vcycle": ([_P, _D], C.c_int),
             "artss_residual_norm": ([_P, _D, _D, _D, _D], C.c_int),
+            "artss_mg_solve_rel": ([_P, _D, _D, C.c_double, C.c_int64, C.POINTER(SolveStats)], C.c_int),
+            "artss_mixed_create": ([_P, C.POINTER(MixedCfg), C.POINTER(_P)], C.c_int),
+            "artss_mixed_destroy": ([_P], C.c_int),
+            "artss_mixed_solve": ([_P, _D, _D, C.POINTER(SolveStats)], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
             "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),
             "artss_ctx_profile_reset": ([_P], C.c_int),
@@ -330,3 +346,55 @@ class Simulation:
 
     def kernel_launches(self) -> int:
         return int(load_cuda().artss_ctx_kernel_launches(self.context))
+
+
+class Context:
+    """A device context built directly through the C ABI (include/artss_cuda.h),
+    the way a reference-side integration would: grid descriptor, the level
+    lists and the ordered boundary assignments of a Geometry, and device
+    arrays allocated by the library."""
+
+    def __init__(self, geom: "Geometry", device: int = 0):
+        self.lib = load_cuda()
+        self.geom = geom
+        self.grid = geom.grid_desc()
+        self.h = C.c_void_p()
+        cuda_check(self.lib.artss_ctx_create(C.byref(self.grid), device, C.byref(self.h)), "ctx")
+        self.fields = []
+        for l in range(self.grid.n_levels + 1):
+            inner = np.ascontiguousarray(geom.list("inner", l))
+            dom = np.ascontiguousarray(geom.list("domain", l))
+            cuda_check(self.lib.artss_set_cell_lists(self.h, l, inner.ctypes.data_as(_I64P), inner.size,
+                                                       dom.ctypes.data_as(_I64P), dom.size), "lists")
+            for ft in range(7):
+                prog = geom.boundary_program(l, ft)
+                if prog.size:
+                    arr = (BcAssign * prog.size)()
+                    C.memmove(arr, prog.ctypes.data, prog.nbytes)
+                    cuda_check(self.lib.artss_set_boundary_program(self.h, l, ft, arr, prog.size), "bc")
+
+    def size(self, level: int = 0) -> int:
+        g = self.grid
+        return g.Nx[level] * g.Ny[level] * g.Nz[level]
+
+    def field(self, values=None, level: int = 0):
+        p = _D()
+        cuda_check(self.lib.artss_field_alloc(self.h, level, C.byref(p)), "alloc")
+        self.fields.append(p)
+        if values is not None:
+            self.upload(p, values)
+        return p
+
+    def upload(self, p, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        cuda_check(self.lib.artss_upload(self.h, p, v.ctypes.data_as(_D), v.size), "upload")
+
+    def download(self, p, level: int = 0) -> np.ndarray:
+        out = np.empty(self.size(level))
+        cuda_check(self.lib.artss_download(self.h, out.ctypes.data_as(_D), p, out.size), "download")
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.artss_ctx_destroy(self.h)
+            self.h = C.c_void_p()

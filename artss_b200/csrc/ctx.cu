@@ -286,6 +286,7 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
         set_error("bad list arguments"); return ARTSS_ERR_ARG;
     }
     const Level &L = ctx->lvl[level];
+    ctx->n_inner[level] = n_inner;
     // every inner cell must lie in the computational domain, every domain-list
     // cell in the box one layer larger; lists are strictly ascending
     auto check = [&](const int64_t *list, int64_t n, int64_t grow, const char *name) -> bool {

@@ -4,8 +4,10 @@
 // a*b+c rounds twice, as the reference serial build does.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <map>
 #include <string>
 #include <vector>
 #include <set>
@@ -19,6 +21,7 @@ constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
 constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
 constexpr int kReduceThreads = 256;
 constexpr int kMaxPartials = 1 << 16;   // per-block partial sums of up to two reduction passes
+constexpr int kTmaBoxX = 72, kTmaBoxY = 12;  // TMA plane window (cells): a 64 x 8 tile, a 2-cell ring, x aligned to 2
 
 enum CellFlag : uint8_t { kInner = 1, kDomain = 2 };
 
@@ -50,7 +53,7 @@ struct LoopState {
     double residual;   // sqrt(sum) (or caller-defined)
     long long it;      // iterations done
     int cond;          // loop continues
-    int pad;
+    int pad;           // error flag: a bounded wait in a kernel of the loop gave up
 };
 
 // Kernel families for launch counting and event timing (artss_ctx_profile).
@@ -79,6 +82,7 @@ struct artss_ctx {
     artss_grid_desc grid{};
     artss::Level lvl[artss::kMaxLevel + 1]{};
     uint8_t *d_flags[artss::kMaxLevel + 1]{};
+    int64_t n_inner[artss::kMaxLevel + 1]{};  // inner cells per level (artss_set_cell_lists)
     artss::BcProgram bc[artss::kMaxLevel + 1][artss::kFieldTypes];
     double *d_partials = nullptr;       // kMaxPartials doubles
     artss::LoopState *d_loop = nullptr; // device loop blocks (16)
@@ -86,6 +90,7 @@ struct artss_ctx {
     int64_t launches = 0;
     std::set<double *> fields;
     artss::Profile prof;
+    std::map<std::pair<const void *, int>, CUtensorMap> tmaps;  // TMA descriptors per (array, level)
     int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},
                                {1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1}};
 };
@@ -180,8 +185,14 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopSta
 int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const LoopState *pred = nullptr);
 // FP64 cluster solve of a level's pressure equation on FP32 storage, zero
 // boundary values, tolerance relative to the initial residual (mg.cu).
+bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int64_t *smem);
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
                        long long max_it, const LoopState *pred);
+
+// TMA descriptor of a level array for kTmaBoxX x kTmaBoxY plane windows (tma.cu);
+// tma_level_ok: the level's row pitch allows TMA (Nx even).
+bool tma_level_ok(const artss_ctx *ctx, int level);
+int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorMap **out);
 
 // Reductions (reduce.cu): sum of per-block partials -> loop state `slot`.
 //   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it

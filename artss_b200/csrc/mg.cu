@@ -943,6 +943,34 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
     return ARTSS_OK;
 }
 
+int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_tol, int64_t max_cycles,
+                       artss_solve_stats *stats) {
+    if (!mg || !p || !rhs) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (max_cycles < 0 || !(rel_tol >= 0)) { set_error("invalid tolerance or cycle limit"); return ARTSS_ERR_ARG; }
+    int st;
+    if ((st = artss_mg_set_rhs(mg, p, rhs))) return st;
+    double res = 0, b_norm = 0;
+    if ((st = artss_residual_norm(mg->ctx, p, rhs, &res, &b_norm))) return st;
+    const double tol = rel_tol * b_norm;
+    int64_t cycles = 0, coarse = 0;
+    const int slot = 2;
+    while (res > tol && cycles < max_cycles) {
+        if ((st = mg_vcycle(mg, p, &coarse))) return st;
+        cycles++;
+        if ((st = mg_resnorm(mg, p, rhs, 0, slot, -1.0, 1, false))) return st;
+        LoopState ls{};
+        if ((st = read_loop(mg->ctx, slot, &ls))) return st;
+        res = ls.residual;
+    }
+    if (stats) {
+        stats->cycles = cycles;
+        stats->residual = res;
+        stats->rel_residual = b_norm > 0 ? res / b_norm : res;
+        stats->b_norm = b_norm;
+    }
+    return ARTSS_OK;
+}
+
 int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out) {
     if (!ctx || !p || !b) { set_error("null argument"); return ARTSS_ERR_ARG; }
     const Level &L = ctx->lvl[0];

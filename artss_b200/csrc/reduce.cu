@@ -36,6 +36,7 @@ __global__ void k_init_loop(LoopState *st, double r0, long long it0, int cond0) 
     st->residual = r0;
     st->it = it0;
     st->cond = cond0;
+    st->pad = 0;  // error flag of kernels with bounded waits
 }
 
 int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it) {

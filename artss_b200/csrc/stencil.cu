@@ -380,6 +380,213 @@ k_cgs_sweep(double *__restrict__ out, const double *__restrict__ in, const doubl
     if (partials && tid == 0) partials[block_linear()] = acc;
 }
 
+// ---- the same sweep with TMA plane staging -------------------------------
+//
+// One thread issues, per z-plane, one cp.async.bulk.tensor load of the
+// kTmaBoxX x kTmaBoxY window of x, b (and EV) into the plane's ring slot;
+// the loads complete on the slot's mbarrier.  The window starts at an even x
+// (a TMA box must start on a 16-byte boundary), so the tile sits ox = 0 or 1
+// cells further right in it than in the cp.async variant.  Red work is one
+// x-pair per thread (33 x 10 pairs: tile plus ring), black one x-pair per
+// thread of the first 256.  Waits on an mbarrier give up after a bounded
+// number of polls and raise the loop state's error flag instead of hanging.
+constexpr int kStThreads = ((kSwTx + 2) / 2) * (kSwTy + 2);  // 330 red pairs
+constexpr int kStPlane = kTmaBoxX * kTmaBoxY;                 // doubles per slot
+constexpr int kStSlotsX = kSwD + 4, kStSlotsB = kSwD + 3;
+constexpr unsigned kStPlaneBytes = kStPlane * sizeof(double);
+static_assert(kTmaBoxX >= kSwTx + 5 && kTmaBoxY == kSwTy + 4, "TMA window covers tile + ring + alignment");
+static_assert(kStPlaneBytes % 128 == 0, "slots stay 128-byte aligned");
+
+inline size_t sweep_tma_smem(bool turb) {
+    return (size_t) kStPlaneBytes * (kStSlotsX + (turb ? 2 : 1) * kStSlotsB);
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// true once the phase with the given parity has completed; gives up after `polls` tries
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int polls) {
+    for (int n = 0; n < polls; n++) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_plane(double *dst, const CUtensorMap *map, int x, int y, int z,
+                                               uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(smem_u32(dst)),
+        "l"((uint64_t) map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+constexpr int kStPolls = 1 << 22;  // mbarrier polls before a wait gives up
+
+template <bool TURB>
+__global__ void __launch_bounds__(kStThreads, 2)
+k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
+                const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out,
+                const uint8_t *__restrict__ flags, Level L, Box3 box, DiffCoef c, double *__restrict__ partials,
+                LoopState *__restrict__ pred) {
+    extern __shared__ __align__(1024) double st_sm[];
+    __shared__ double smem[32];
+    __shared__ __align__(8) uint64_t bars[kStSlotsX];
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
+    double *X = st_sm;                          // [kStSlotsX][kStPlane]
+    double *B = st_sm + kStSlotsX * kStPlane;   // [kStSlotsB][kStPlane]
+    double *E = B + kStSlotsB * kStPlane;       // [kStSlotsB][kStPlane] (TURB)
+    const int tid = threadIdx.x;
+    const int64_t nj = L.Nx, nk = L.nxy();
+    const int64_t wx0 = box.x0 + (int64_t) blockIdx.x * kSwTx - 2;  // global i of ring column 0
+    const int64_t wxa = wx0 - (wx0 & 1);                             // TMA window start, even
+    const int ox = (int) (wx0 - wxa);
+    const int64_t wy0 = box.y0 + (int64_t) blockIdx.y * kSwTy - 2;
+    const int64_t kc0 = box.z0 + (int64_t) blockIdx.z * kSwZ;
+    const int64_t kc1 = min(kc0 + kSwZ - 1, box.z1);
+    const int64_t pbase = kc0 - 2, plast = kc1 + 2;  // staged planes
+
+    if (tid == 0) {
+        for (int s = 0; s < kStSlotsX; s++) mbar_init(&bars[s], 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    // thread 0: load plane p into its slots
+    auto issue = [&](int64_t p) {
+        if (p > plast) return;
+        const int u = (int) (p - pbase);
+        uint64_t *bar = &bars[u % kStSlotsX];
+        mbar_expect_tx(bar, kStPlaneBytes * (TURB ? 3u : 2u));
+        tma_load_plane(X + (u % kStSlotsX) * kStPlane, &tm_x, (int) wxa, (int) wy0, (int) p, bar);
+        tma_load_plane(B + (u % kStSlotsB) * kStPlane, &tm_b, (int) wxa, (int) wy0, (int) p, bar);
+        if (TURB) tma_load_plane(E + (u % kStSlotsB) * kStPlane, &tm_e, (int) wxa, (int) wy0, (int) p, bar);
+    };
+    auto ready = [&](int64_t p) -> bool {
+        const int u = (int) (p - pbase);
+        return mbar_wait(&bars[u % kStSlotsX], (unsigned) ((u / kStSlotsX) & 1), kStPolls);
+    };
+    auto xslot = [&](int64_t p) { return X + (int) ((p - pbase) % kStSlotsX) * kStPlane; };
+    auto bslot = [&](int64_t p) { return (int) ((p - pbase) % kStSlotsB) * kStPlane; };
+    auto update = [&](const double *xm, const double *x0, const double *xp, int e, int bo, double &res2) {
+        double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+        if (TURB) {
+            turb_alpha(c, E[bo + e], ax, ay, az, rb);
+            beta = 1. / rb;
+        }
+        const double old = x0[e];
+        const double out_h = beta * (c.dsign * B[bo + e] + ax * (x0[e + 1] + x0[e - 1]) +
+                                     ay * (x0[e + kTmaBoxX] + x0[e - kTmaBoxX]) + az * (xp[e] + xm[e]));
+        const double nw = c.omw * old + c.w * out_h;
+        const double r = rb * (nw - old);
+        res2 = r * r;
+        return nw;
+    };
+
+    // this thread's red x-pair (tile + ring) and black x-pair (tile)
+    const int ry = 1 + tid / ((kSwTx + 2) / 2), px = tid % ((kSwTx + 2) / 2);
+    const int64_t gjr = wy0 + ry;
+    const bool red_row = gjr >= box.y0 && gjr <= box.y1;
+    const bool red_tile = ry >= 2 && ry < kSwTy + 2;
+    const bool has_black = tid < (kSwTx / 2) * kSwTy;
+    const int tx = tid % (kSwTx / 2), ty = tid / (kSwTx / 2);
+    const int64_t gjb = wy0 + 2 + ty;
+    const int lx0 = 2 + 2 * tx;
+    auto red_x = [&](int64_t k) { return 1 + 2 * px + (int) ((wx0 + 1 + gjr + k) & 1); };  // (i + j + k) even
+    auto red_flag = [&](int64_t k) -> uint8_t {
+        if (!red_row || k < box.z0 || k > box.z1) return 0;
+        const int64_t gi = wx0 + red_x(k);
+        if (gi < box.x0 || gi > box.x1) return 0;
+        return __ldg(flags + gi + nj * gjr + nk * k);
+    };
+    auto black_par = [&](int64_t kb) { return (int) ((wx0 + lx0 + gjb + kb + 1) & 1); };  // (i + j + k) odd
+    auto black_flag = [&](int64_t kb) -> uint8_t {
+        if (!has_black || gjb > box.y1 || kb < kc0 || kb > kc1) return 0;
+        const int64_t gi = wx0 + lx0 + black_par(kb);
+        if (gi > box.x1) return 0;
+        return __ldg(flags + gi + nj * gjb + nk * kb);
+    };
+
+    double acc = 0.0;
+    int64_t issued = kc0 - 1 + kSwD;  // thread 0's last issued plane
+    if (tid == 0)
+        for (int64_t p = pbase; p <= issued; p++) issue(p);
+    bool ok = ready(pbase) && ready(pbase + 1);
+    uint8_t fr = red_flag(kc0 - 1), fb = black_flag(kc0 - 2);
+    bool failed = false;
+    int64_t waited = pbase + 1;  // planes up to here have landed
+    for (int64_t k = kc0 - 1; k <= kc1 + 1; k++) {
+        // the next step's flags, loaded early
+        const uint8_t fr_next = red_flag(k + 1), fb_next = black_flag(k);
+        ok = ok && ready(k + 1);
+        fence_proxy_async();  // this thread's shared-memory writes before the slot refill below
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        waited = k + 1;
+        if (tid == 0 && k + 1 + kSwD <= plast) {
+            issue(k + 1 + kSwD);
+            issued = k + 1 + kSwD;
+        }
+        // red on plane k, tile + 1-cell ring
+        if (fr & kInner) {
+            const int rx = red_x(k);
+            const int e = rx + ox + kTmaBoxX * ry;
+            double *x0 = xslot(k);
+            double r2;
+            const double nw = update(xslot(k - 1), x0, xslot(k + 1), e, bslot(k), r2);
+            x0[e] = nw;
+            if (red_tile && rx >= 2 && rx < kSwTx + 2 && k >= kc0 && k <= kc1) acc += r2;
+        }
+        __syncthreads();
+        // black on plane k-1, tile only, and the tile's plane k-1 out
+        const int64_t kb = k - 1;
+        if (has_black && kb >= kc0 && kb <= kc1 && gjb <= box.y1) {
+            const double *x0 = xslot(kb);
+            const int par = black_par(kb);
+            const int e0 = lx0 + ox + kTmaBoxX * (2 + ty);
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int64_t gi = wx0 + lx0 + s;
+                if (gi > box.x1) continue;
+                double v = x0[e0 + s];
+                if (s == par && (fb & kInner)) {
+                    double r2;
+                    v = update(xslot(kb - 1), x0, xslot(kb + 1), e0 + s, bslot(kb), r2);
+                    acc += r2;
+                }
+                out[gi + nj * gjb + nk * kb] = v;
+            }
+        }
+        fr = fr_next;
+        fb = fb_next;
+    }
+    if (failed) {
+        // a plane never arrived: flag it, let the loads in flight land, leave
+        if (tid == 0) {
+            if (pred) *(volatile int *) &pred->pad = 1;
+            for (int64_t p = waited + 1; p <= issued; p++) (void) ready(p);
+        }
+        __syncthreads();
+        return;
+    }
+    acc = artss_block_sum(acc, smem);
+    if (partials && tid == 0) partials[block_linear()] = acc;
+}
+
 // One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
 // the division by reciprocal_beta; turbulent: :345-362) + residual partials
 // of sum (rbeta * (out - in))^2 (:72-79).
@@ -592,9 +799,17 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     const dim3 g = sweep_grid(box);
     if ((st = check_reduce_blocks(g))) return st;
     const int nb = nblocks(g);
-    const size_t smem = sweep_smem(ev != nullptr);
-    if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    // TMA plane staging where the row pitch allows it, cp.async otherwise
+    const bool tma = tma_level_ok(ctx, 0);
+    const size_t smem = tma ? sweep_tma_smem(ev != nullptr) : sweep_smem(ev != nullptr);
+    if (tma) {
+        if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    } else {
+        if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    }
+    const CUtensorMap *tm_b = nullptr, *tm_e = nullptr, *tm_x[2] = {nullptr, nullptr};
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
     if ((st = artss_copy(ctx, out, in, 0))) return st;
@@ -614,13 +829,29 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     // chosen so that a solve of the predicted length ends in out.
     double *buf[2] = {out, in};
     const int s0 = (int) (batch & 1);  // iteration n writes buf[(s0 + n) & 1]
+    if (tma) {
+        if ((st = tensor_map_3d(ctx, out, 0, &tm_x[0]))) return st;
+        if ((st = tensor_map_3d(ctx, in, 0, &tm_x[1]))) return st;
+        if ((st = tensor_map_3d(ctx, b, 0, &tm_b))) return st;
+        tm_e = tm_b;
+        if (ev && (st = tensor_map_3d(ctx, ev, 0, &tm_e))) return st;
+    }
+    LoopState *pred_rw = ctx->d_loop + slot;
     while (cond) {
         // `batch` iterations per host round trip; iterations past convergence skip themselves
         for (int64_t r = 0; r < batch; r++) {
             const long long n = it + 1 + r;
             double *w = buf[(s0 + n) & 1];
             const double *rd = buf[(s0 + n + 1) & 1];
-            if (ev)
+            if (tma) {
+                const CUtensorMap &mx = *tm_x[(s0 + n + 1) & 1];
+                if (ev)
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<true><<<g, kStThreads, smem, ctx->stream>>>(
+                        mx, *tm_b, *tm_e, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred_rw));
+                else
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<false><<<g, kStThreads, smem, ctx->stream>>>(
+                        mx, *tm_b, *tm_e, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred_rw));
+            } else if (ev)
                 ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
                     w, rd, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
             else
@@ -631,6 +862,7 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
             if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
         }
         if ((st = read_loop(ctx, slot, &ls))) return st;
+        if (ls.pad) { set_error("colored Gauss-Seidel sweep: a TMA plane load did not arrive"); return ARTSS_ERR_CUDA; }
         it = ls.it;
         res = ls.residual;
         cond = ls.cond != 0;

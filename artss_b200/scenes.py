@@ -207,6 +207,36 @@ def random_boxes(n_cells: Tuple[int, int, int], lo: int, hi: int, count: int, se
     return out
 
 
+def poisson_boxes(n: int = 256, seed: int = 0, n_level: int = 5, **kw) -> Scene:
+    """Pure-Neumann pressure problem on a unit-spacing n^3 grid with 1-6
+    axis-aligned box obstacles whose edges are uniform in [8, 48] cells at
+    uniform positions (count, sizes and positions from `seed`): the
+    mixed-precision pressure workload at n = 256.  The right-hand side is not
+    part of the scene; poisson_rhs() draws it."""
+    rng = random.Random(10007 * seed + 17)
+    count = rng.randint(1, 6)
+    lo, hi = max(2, 8 * n // 256), max(3, 48 * n // 256)
+    boxes = random_boxes((n, n, n), lo, hi, count, seed, (1.0, 1.0, 1.0), levels=n_level - 1)
+    bcs = [("p", "front,back,bottom,top,left,right", "neumann", 0.0)]
+    obcs = [("p", "front,back,left,right,top,bottom", "neumann", 0.0)]
+    base = dict(solver="PressureSolver", nx=n, ny=n, nz=n, X=(0.0, float(n)), Y=(0.0, float(n)), Z=(0.0, float(n)),
+                dt=1.0, steps=1, n_level=n_level, boundaries=bcs, obstacles=boxes, obstacle_bcs=obcs, noise=False,
+                ic="Zero")
+    base.update(kw)
+    return Scene(**base)
+
+
+def poisson_rhs(inner, size: int, seed: int):
+    """Seeded N(0, 1) right-hand side on the inner cells, projected to zero
+    mean over them (every other cell 0)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    b = np.zeros(size)
+    v = rng.standard_normal(len(inner))
+    b[inner] = v - v.mean()
+    return b
+
+
 def to_xml(s: Scene) -> str:
     L = []
     a = L.append

@@ -40,7 +40,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["channel", "box"], default="channel")
+    ap.add_argument("--workload", choices=["channel", "box", "poisson"], default="channel",
+                    help="poisson: ms per pressure solve to a 1e-8 relative residual, plain FP64 VCycleMG "
+                         "against the mixed-precision solve, on the 256^3 Neumann problem with box obstacles")
+    ap.add_argument("--poisson-n", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -301,6 +305,88 @@ def run_b200(args, dist):
     return out, xml, inner
 
 
+def run_poisson(args, dist):
+    """ms per pressure solve to ||b - A p|| <= 1e-8 ||b|| from p = 0: the plain
+    FP64 VCycleMG (reference V-cycle structure: 5 levels, V(2,2) Jacobi
+    w = 2/3, 100-sweep Jacobi coarse solve) against the mixed-precision solve
+    (FP32 V-cycles of the same shape, FP64 defect correction, FP64 red-black
+    coarse solve).  `steps` solves of each are timed with CUDA events on the
+    context stream, after `warmup` untimed ones."""
+    import numpy as np
+    import torch
+
+    import artss_b200 as A
+    from artss_b200 import scenes
+
+    torch.cuda.set_device(dist.local)
+    n = args.poisson_n
+    sc = scenes.poisson_boxes(n=n, seed=args.seed, n_level=5)
+    xml = scenes.write(sc, os.path.join(tempfile.mkdtemp(prefix="artss_poisson_"), "poisson.xml"))
+    geom = A.Geometry(xml)
+    ctx = A.Context(geom, device=dist.local)
+    cuda = ctx.lib
+    stream = torch.cuda.ExternalStream(cuda.artss_ctx_stream(ctx.h), device=torch.device("cuda", dist.local))
+    inner = geom.list("inner", 0)
+    b = scenes.poisson_rhs(inner, ctx.size(), 1000 + args.seed)
+    db = ctx.field(b)
+    dp = ctx.field()
+    mg = C.c_void_p()
+    mcfg = A.MgCfg(5, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
+    A.cuda_check(cuda.artss_mg_create(ctx.h, C.byref(mcfg), C.byref(mg)), "mg")
+    mx = C.c_void_p()
+    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 0.6666666667, 1.0, 1e-3, 400, 1e-8, 200)
+    A.cuda_check(cuda.artss_mixed_create(ctx.h, C.byref(xcfg), C.byref(mx)), "mixed")
+
+    def plain(st):
+        return cuda.artss_mg_solve_rel(mg, dp, db, 1e-8, 2000, C.byref(st))
+
+    def mixed(st):
+        return cuda.artss_mixed_solve(mx, dp, db, C.byref(st))
+
+    res = {}
+    for name, fn in (("plain_fp64", plain), ("mixed", mixed)):
+        st = A.SolveStats()
+        for _ in range(args.warmup):
+            A.cuda_check(cuda.artss_fill(ctx.h, dp, 0, 0.0), "fill")
+            A.cuda_check(fn(st), name)
+        times = []
+        for _ in range(args.steps):
+            A.cuda_check(cuda.artss_fill(ctx.h, dp, 0, 0.0), "fill")
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            A.cuda_check(fn(st), name)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        res[name] = {"ms_per_solve": float(np.median(times)), "ms_all": [round(t, 3) for t in times],
+                     "cycles": int(st.cycles), "rel_residual": float(st.rel_residual)}
+    cuda.artss_mixed_destroy(mx)
+    cuda.artss_mg_destroy(mg)
+    ctx.close()
+    ms = dist.max(res["mixed"]["ms_per_solve"])
+    return {
+        "metric": "ms per pressure solve to 1e-8 relative residual",
+        "value": ms,
+        "unit": "ms",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 V-cycles in f64 defect correction",
+        "data": "synthetic",
+        "config": {"workload": f"poisson_{n}cubed_neumann_boxes", "cells": f"{n}x{n}x{n}",
+                   "inner_cells": int(len(inner)), "boxes": len(sc.obstacles), "seed": args.seed,
+                   "levels": 5, "rhs": "N(0,1), projected to zero mean over fluid cells", "start": "p = 0"},
+        "plain_fp64": res["plain_fp64"],
+        "mixed": res["mixed"],
+        "speedup_vs_plain_fp64": res["plain_fp64"]["ms_per_solve"] / res["mixed"]["ms_per_solve"],
+    }
+
+
 def cpu_baseline(args, inner):
     """The reference serial build (oracle/_ref) on a bounded sample of the same
     workload: the first steps of the same scene, steady-state steps timed."""
@@ -363,6 +449,11 @@ def main():
         if args.impl == "reference":
             if dist.rank == 0:
                 print(json.dumps(run_reference(args, dist)), flush=True)
+            return
+        if args.workload == "poisson":
+            out = run_poisson(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
             return
         out, xml, inner = run_b200(args, dist)
         if dist.rank == 0:

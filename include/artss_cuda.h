@@ -255,6 +255,46 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
  * artss_mg_pressure / artss_mg_set_rhs. */
 int artss_mg_set_rhs(artss_mg *mg, const double *p, const double *rhs);
 int artss_mg_vcycle(artss_mg *mg, double *p);
+/* VCycleMG iterated to a relative tolerance: V-cycles (VCycleMG.cpp:215-288)
+ * on p until ||b - A p||_2 <= rel_tol * ||b||_2 over the level-0 inner cells
+ * or max_cycles; the plain FP64 solve the mixed-precision one is measured
+ * against.  stats may be NULL. */
+typedef struct {
+    int64_t cycles;        /* V-cycles done */
+    double residual;       /* ||b - A p||_2 at the end */
+    double rel_residual;   /* residual / b_norm */
+    double b_norm;         /* ||b - mean||_2 (mean 0 unless removed) */
+} artss_solve_stats;
+int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_tol, int64_t max_cycles,
+                       artss_solve_stats *stats);
+
+/* Mixed-precision pressure solve; no counterpart in the reference (it plugs
+ * in where IPressure::pressure, src/interfaces/IPressure.h:17, is called).
+ * FP64 defect correction on level 0 around FP32 V-cycles:
+ *     r = (b - mean_b) - A p  (FP64);  stop when ||r|| <= rel_tol ||b - mean_b||;
+ *     e = V-cycle(r) in FP32 with zero boundary values, coarsest level solved
+ *     in FP64;  p += e  (FP64)
+ * mean_b and the final mean of p are removed over the inner cells when
+ * flags has ARTSS_MIXED_REMOVE_MEAN (pure-Neumann pressure problems, whose
+ * solution is defined up to a constant). */
+#define ARTSS_MIXED_REMOVE_MEAN 1
+typedef struct {
+    int32_t n_level;          /* V-cycle levels 0 .. n_level-1; the coarse solve is on n_level-1 */
+    int32_t n_relax;          /* weighted-Jacobi sweeps before and after each coarse correction */
+    int32_t coarse_smoother;  /* ARTSS_SMOOTHER_JACOBI or ARTSS_SMOOTHER_CGS (FP64, one cluster kernel) */
+    int32_t flags;            /* ARTSS_MIXED_REMOVE_MEAN */
+    double w;                 /* Jacobi weight of the FP32 sweeps */
+    double coarse_w;          /* relaxation weight of the coarse solve */
+    double coarse_rel_tol;    /* coarse solve stops at this fraction of its initial residual ... */
+    int64_t coarse_max_iter;  /* ... or after this many sweeps */
+    double rel_tol;           /* outer stopping rule */
+    int64_t max_cycles;       /* outer V-cycle limit */
+} artss_mixed_cfg;
+typedef struct artss_mixed artss_mixed;
+int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed **out);
+int artss_mixed_destroy(artss_mixed *m);
+int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_stats *stats);
+
 /* ||b - A p||_2 over level-0 inner cells (VCycleMG.cpp:186-194) and ||b||_2. */
 int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out);
 

@@ -205,3 +205,31 @@ def test_cgs_iteration_parity(env, scratch):
         assert np.array_equal(ctx.download(dout), ro)
         if not scratch:
             assert np.array_equal(ctx.download(din), ri)
+
+
+@pytest.mark.parametrize("turbulent", [False, True])
+def test_cgs_odd_pitch(tmp_path, turbulent):
+    """An odd row pitch (nx + 2 odd) rules out TMA plane loads; the cp.async
+    variant of the sweep must give the same values."""
+    sc = scenes.channel_with_cube(nx=63, ny=20, nz=19, steps=1, n_level=1)
+    geom = A.Geometry(scenes.write(sc, str(tmp_path / "odd.xml")))
+    ctx = cabi.Context(geom)
+    try:
+        osc = oracle.OracleScene(geom)
+        n = ctx.size()
+        assert (geom.grid_desc().Nx[0] % 2) == 1
+        out0, in0, b, ev = rnd(61, n, 290, 300), rnd(62, n, 290, 300), rnd(63, n, 290, 300), rnd(64, n, 0, 1e-3)
+        dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
+        cfg = A.IterCfg(5, 1e-300, 1.0)
+        stats = A.IterStats()
+        A.cuda_check(ctx.lib.artss_diffuse_cgs(ctx.h, dout, din, db, 4.2e-5, dev if turbulent else None, sc.dt,
+                                               FT["v"], C.byref(cfg), 0, C.byref(stats)), "cgs")
+        ro, ri = out0.copy(), in0.copy()
+        res = C.c_double()
+        its = oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev) if turbulent else None,
+                                              sc.dt, FT["v"], 5, 1e-300, 1.0, C.byref(res))
+        assert stats.iterations == its == 5
+        assert np.array_equal(ctx.download(dout), ro)
+        assert np.array_equal(ctx.download(din), ri)
+    finally:
+        ctx.close()

@@ -1,0 +1,98 @@
+"""Mixed-precision pressure solve (FP32 V-cycles inside FP64 defect
+correction) against the plain FP64 VCycleMG iterated to a relative tolerance.
+
+The mixed solver's claim, ||b - A p|| <= 1e-8 ||b||, is checked on the CPU
+with the oracle's boundary program and a numpy Laplacian, and its solution is
+compared with a plain FP64 solve taken to 1e-11."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import artss_b200 as A
+from artss_b200 import scenes
+from tests import cabi, oracle
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not oracle.available(), reason="oracle not built")]
+
+FT_P = 4
+
+
+def residual_cpu(osc, geom, p, b):
+    """b - A p on the level-0 inner cells, FP64, after the oracle's pressure
+    boundary program (VCycleMG.cpp:186-194 arithmetic)."""
+    d = geom.grid_desc()
+    q = p.copy()
+    oracle.lib().oracle_apply_bc(osc.ptr, oracle.p(q), 0, FT_P)
+    inner = geom.list("inner", 0)
+    nj, nk = d.Nx[0], d.Nx[0] * d.Ny[0]
+    rx, ry, rz = 1 / d.dx[0] ** 2, 1 / d.dy[0] ** 2, 1 / d.dz[0] ** 2
+    c = 2 * q[inner]
+    lap = (rx * (q[inner - 1] - c + q[inner + 1]) + ry * (q[inner - nj] - c + q[inner + nj]) +
+           rz * (q[inner - nk] - c + q[inner + nk]))
+    return b[inner] - lap
+
+
+def solve_pair(sc, seed, mixed_flags, rel_tol=1e-8):
+    import tempfile, os
+    xml = scenes.write(sc, os.path.join(tempfile.mkdtemp(), "poisson.xml"))
+    geom = A.Geometry(xml)
+    ctx = cabi.Context(geom)
+    osc = oracle.OracleScene(geom)
+    try:
+        n = ctx.size()
+        inner = geom.list("inner", 0)
+        b = scenes.poisson_rhs(inner, n, seed)
+        db = ctx.field(b)
+        # plain FP64 reference V-cycle, taken far below the target tolerance
+        cfg = A.MgCfg(sc.n_level, 2, 100, 2, 1e-30, 0, 0, 100, 1e-10, 0.6666666667)
+        mg = C.c_void_p()
+        A.cuda_check(ctx.lib.artss_mg_create(ctx.h, C.byref(cfg), C.byref(mg)), "mg")
+        dp_ref = ctx.field(np.zeros(n))
+        ref_stats = A.SolveStats()
+        A.cuda_check(ctx.lib.artss_mg_solve_rel(mg, dp_ref, db, 1e-11, 2000, C.byref(ref_stats)), "plain")
+        ctx.lib.artss_mg_destroy(mg)
+        p_ref = ctx.download(dp_ref)
+        # mixed precision to the target tolerance
+        mcfg = A.MixedCfg(sc.n_level, 2, 1, mixed_flags, 0.6666666667, 1.0, 1e-3, 400, rel_tol, 200)
+        mx = C.c_void_p()
+        A.cuda_check(ctx.lib.artss_mixed_create(ctx.h, C.byref(mcfg), C.byref(mx)), "mixed")
+        dp = ctx.field(np.zeros(n))
+        st = A.SolveStats()
+        A.cuda_check(ctx.lib.artss_mixed_solve(mx, dp, db, C.byref(st)), "mixed solve")
+        # a second solve from the same start reuses the batch hint
+        dp2 = ctx.field(np.zeros(n))
+        st2 = A.SolveStats()
+        A.cuda_check(ctx.lib.artss_mixed_solve(mx, dp2, db, C.byref(st2)), "mixed solve 2")
+        ctx.lib.artss_mixed_destroy(mx)
+        p = ctx.download(dp)
+        p2 = ctx.download(dp2)
+        return geom, osc, b, inner, p, p2, p_ref, st, st2, ref_stats
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_mixed_neumann_boxes(seed):
+    sc = scenes.poisson_boxes(n=32, seed=seed, n_level=3)
+    geom, osc, b, inner, p, p2, p_ref, st, st2, ref = solve_pair(sc, seed, A.MIXED_REMOVE_MEAN)
+    assert 0 < st.cycles < 200 and st.rel_residual <= 1e-8
+    assert st2.cycles == st.cycles and np.array_equal(p, p2)
+    r = residual_cpu(osc, geom, p, b)
+    assert np.linalg.norm(r) <= 1.0000001e-8 * np.linalg.norm(b[inner])
+    assert abs(p[inner].mean()) <= 1e-12 * np.abs(p[inner]).max()
+    # both solve the same singular system: compare up to the constant
+    d = (p[inner] - p[inner].mean()) - (p_ref[inner] - p_ref[inner].mean())
+    assert np.abs(d).max() <= 1e-5 * np.abs(p_ref[inner]).max()
+    assert ref.rel_residual <= 1e-11
+
+
+def test_mixed_dirichlet_channel():
+    """Outflow with Dirichlet p = 0 (no mean removal) and an obstacle."""
+    sc = scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=1, n_level=3)
+    geom, osc, b, inner, p, p2, p_ref, st, st2, ref = solve_pair(sc, 7, 0)
+    assert 0 < st.cycles < 200 and st.rel_residual <= 1e-8
+    r = residual_cpu(osc, geom, p, b)
+    assert np.linalg.norm(r) <= 1.0000001e-8 * np.linalg.norm(b[inner])
+    d = p[inner] - p_ref[inner]
+    assert np.abs(d).max() <= 1e-5 * np.abs(p_ref[inner]).max()
