@@ -149,6 +149,7 @@ def load_cuda() -> C.CDLL:
             "artss_mixed_create": ([_P, C.POINTER(MixedCfg), C.POINTER(_P)], C.c_int),
             "artss_mixed_destroy": ([_P], C.c_int),
             "artss_mixed_solve": ([_P, _D, _D, C.POINTER(SolveStats)], C.c_int),
+            "artss_laplacian": ([_P, _D, _D, C.c_int], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
             "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),
             "artss_ctx_profile_reset": ([_P], C.c_int),
@@ -398,3 +399,26 @@ class Context:
         if self.h:
             self.lib.artss_ctx_destroy(self.h)
             self.h = C.c_void_p()
+
+
+def consistent_rhs(ctx: Context, b: np.ndarray, n_level: int, cycles: int = 40):
+    """A right-hand side in the range of the level-0 pressure operator A close
+    to `b`: b' = A p_inf, where p_inf is what `cycles` mixed-precision V-cycles
+    reach from p = 0 (their residual stalls at the part of b outside the range
+    of A).  Pure-Neumann scenes with obstacles need this, since the reference's
+    obstacle boundary programs make A non-symmetric and a mean-free b is not
+    solvable to a small residual.  Returns (device array, host copy)."""
+    lib = ctx.lib
+    db = ctx.field(b)
+    dp = ctx.field(np.zeros(ctx.size()))
+    cfg = MixedCfg(n_level, 2, 1, MIXED_REMOVE_MEAN, 0.6666666667, 1.0, 1e-3, 400, 0.0, cycles)
+    mx = C.c_void_p()
+    cuda_check(lib.artss_mixed_create(ctx.h, C.byref(cfg), C.byref(mx)), "mixed")
+    try:
+        st = SolveStats()
+        cuda_check(lib.artss_mixed_solve(mx, dp, db, C.byref(st)), "mixed solve")
+    finally:
+        lib.artss_mixed_destroy(mx)
+    out = ctx.field(np.zeros(ctx.size()))
+    cuda_check(lib.artss_laplacian(ctx.h, out, dp, 0), "laplacian")
+    return out, ctx.download(out)

@@ -5,12 +5,15 @@
 // (src/pressure/VCycleMG.cpp) iterated to the same relative residual.
 //
 // Outer loop, FP64 on level 0:
-//     r = (b - mean_b) - A p          (mean_b = 0 unless the mean is removed)
-//     stop when ||r||_2 <= rel_tol * ||b - mean_b||_2
+//     r = b - A p                      stop when ||r||_2 <= rel_tol * ||b||_2
 //     e = V(r)                         FP32 V-cycle on A e = r, e = 0 at start
 //     p += e                           FP64
-// and, for pure-Neumann problems, the mean of p over the inner cells is removed
-// at the end.  The V-cycle has the structure of VCycleMG::VCycleMultigrid
+// and, for pure-Neumann problems (A 1 = 0), the mean of p over the inner
+// cells is removed at the end.  b must lie in the range of A: with the
+// reference's obstacle boundary programs (edge and corner cells copy one of
+// their fluid neighbours) A is not symmetric, so a mean-free b is not enough
+// for a pure-Neumann problem; artss_laplacian builds consistent right-hand
+// sides.  The V-cycle has the structure of VCycleMG::VCycleMultigrid
 // (n_relax weighted-Jacobi sweeps, each followed by the level's boundary
 // program, residual, restriction, prolongation with the trilinear weights of
 // VCycleMG::Prolongate), all in FP32 with the boundary values set to zero
@@ -155,9 +158,9 @@ __global__ void k_mx_prolong_add(float *__restrict__ fine, const float *__restri
     }
 }
 
-// FP64 outer residual r = (b - mean_b) - A p on level 0, stored as the FP32
-// right-hand side of the correction equation; block partials of ||r||^2
-__global__ void k_mx_outer_residual(const double *__restrict__ p, const double *__restrict__ b, double mean_b,
+// FP64 outer residual r = b - A p on level 0, stored as the FP32 right-hand
+// side of the correction equation; block partials of ||r||^2
+__global__ void k_mx_outer_residual(const double *__restrict__ p, const double *__restrict__ b,
                                     float *__restrict__ r, const uint8_t *__restrict__ flags, Level L, Box3 box,
                                     double rx, double ry, double rz, double *__restrict__ partials,
                                     const LoopState *__restrict__ pred) {
@@ -171,8 +174,8 @@ __global__ void k_mx_outer_residual(const double *__restrict__ p, const double *
             const int64_t x = i + nj * j + nk * k;
             if (!(flags[x] & kInner)) continue;
             const double c2 = 2 * p[x];
-            const double v = (b[x] - mean_b) - (rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) +
-                                                rz * (p[x - nk] - c2 + p[x + nk]));
+            const double v = b[x] - (rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) +
+                                     rz * (p[x - nk] - c2 + p[x + nk]));
             r[x] = (float) v;
             acc += v * v;
         }
@@ -218,6 +221,20 @@ __global__ void k_mx_moments(const double *__restrict__ x, double shift, const u
     __syncthreads();
     s2 = artss_block_sum(s2, smem);
     if (threadIdx.x == 0 && threadIdx.y == 0) p2[bl] = s2;
+}
+
+// out = A p on the inner cells (FP64)
+__global__ void k_mx_laplacian(double *__restrict__ out, const double *__restrict__ p,
+                               const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz) {
+    MX_COLUMN(box);
+    if (!col) return;
+    const int64_t nj = L.Nx, nk = L.nxy();
+    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+        const int64_t x = i + nj * j + nk * k;
+        if (!(flags[x] & kInner)) continue;
+        const double c2 = 2 * p[x];
+        out[x] = rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) + rz * (p[x - nk] - c2 + p[x + nk]);
+    }
 }
 
 __global__ void k_mx_fill(float *__restrict__ f, int64_t n, const LoopState *__restrict__ pred) {
@@ -405,6 +422,21 @@ int artss_mixed_destroy(artss_mixed *m) {
     return ARTSS_OK;
 }
 
+int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level) {
+    if (!ctx || !out || !p || out == p) { set_error("null or aliased argument"); return ARTSS_ERR_ARG; }
+    int st = check_level(ctx, level);
+    if (st) return st;
+    if ((st = apply_bc(ctx, p, level, ARTSS_FIELD_P))) return st;
+    const Level &L = ctx->lvl[level];
+    const Box3 box = inner_box(L);
+    const artss_grid_desc &g = ctx->grid;
+    ARTSS_LAUNCH(ctx, FAM_MG_RESIDUUM, k_mx_laplacian<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
+                                           out, p, ctx->d_flags[level], L, box, 1. / (g.dx[level] * g.dx[level]),
+                                           1. / (g.dy[level] * g.dy[level]), 1. / (g.dz[level] * g.dz[level])));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
 int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_stats *stats) {
     if (!m || !p || !b) { set_error("null argument"); return ARTSS_ERR_ARG; }
     artss_ctx *ctx = m->ctx;
@@ -414,13 +446,9 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     const bool remove_mean = (m->cfg.flags & ARTSS_MIXED_REMOVE_MEAN) != 0;
     const int64_t n_inner = ctx->n_inner[0];
     int st;
-    // right-hand side: mean (pure-Neumann problems) and norm
-    double s1 = 0, s2 = 0, mean_b = 0;
+    // ||b|| for the relative stopping rule
+    double s1 = 0, s2 = 0;
     if ((st = mx_moments(m, b, 0.0, &s1, &s2))) return st;
-    if (remove_mean && n_inner > 0) {
-        mean_b = s1 / (double) n_inner;
-        if ((st = mx_moments(m, b, mean_b, &s1, &s2))) return st;
-    }
     const double b_norm = sqrt(s2);
     const double tol = m->cfg.rel_tol * b_norm;
     if ((st = apply_bc(ctx, p, 0, ARTSS_FIELD_P))) return st;
@@ -439,7 +467,7 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     while (cond) {
         for (int64_t r = 0; r < batch; r++) {
             ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_outer_residual<<<grid, box_block(), 0, ctx->stream>>>(
-                                                  p, b, mean_b, m->r[0], ctx->d_flags[0], L, box, rx, ry, rz,
+                                                  p, b, m->r[0], ctx->d_flags[0], L, box, rx, ry, rz,
                                                   ctx->d_partials, pred));
             ARTSS_LAUNCH_CK(ctx);
             if ((st = finalize_loop(ctx, kSlotOuter, nb, tol, max_eval))) return st;

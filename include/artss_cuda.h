@@ -263,7 +263,7 @@ typedef struct {
     int64_t cycles;        /* V-cycles done */
     double residual;       /* ||b - A p||_2 at the end */
     double rel_residual;   /* residual / b_norm */
-    double b_norm;         /* ||b - mean||_2 (mean 0 unless removed) */
+    double b_norm;         /* ||b||_2 over the inner cells */
 } artss_solve_stats;
 int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_tol, int64_t max_cycles,
                        artss_solve_stats *stats);
@@ -271,12 +271,14 @@ int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_to
 /* Mixed-precision pressure solve; no counterpart in the reference (it plugs
  * in where IPressure::pressure, src/interfaces/IPressure.h:17, is called).
  * FP64 defect correction on level 0 around FP32 V-cycles:
- *     r = (b - mean_b) - A p  (FP64);  stop when ||r|| <= rel_tol ||b - mean_b||;
+ *     r = b - A p  (FP64);  stop when ||r|| <= rel_tol ||b||;
  *     e = V-cycle(r) in FP32 with zero boundary values, coarsest level solved
  *     in FP64;  p += e  (FP64)
- * mean_b and the final mean of p are removed over the inner cells when
- * flags has ARTSS_MIXED_REMOVE_MEAN (pure-Neumann pressure problems, whose
- * solution is defined up to a constant). */
+ * With ARTSS_MIXED_REMOVE_MEAN the mean of p over the inner cells is removed
+ * at the end (pure-Neumann pressure problems: p is defined up to a constant).
+ * b must lie in the range of A; for pure-Neumann scenes with obstacles a
+ * mean-free b is not enough (the obstacle edge and corner cells make A
+ * non-symmetric) -- artss_laplacian gives consistent right-hand sides. */
 #define ARTSS_MIXED_REMOVE_MEAN 1
 typedef struct {
     int32_t n_level;          /* V-cycle levels 0 .. n_level-1; the coarse solve is on n_level-1 */
@@ -294,6 +296,10 @@ typedef struct artss_mixed artss_mixed;
 int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed **out);
 int artss_mixed_destroy(artss_mixed *m);
 int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_stats *stats);
+/* out = A p on the inner cells of `level` (the VCycleMG operator, after the
+ * level's pressure boundary program is applied to p); other cells of out are
+ * left as they are. */
+int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level);
 
 /* ||b - A p||_2 over level-0 inner cells (VCycleMG.cpp:186-194) and ||b||_2. */
 int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out);
