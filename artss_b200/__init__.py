@@ -411,7 +411,8 @@ def consistent_rhs(ctx: Context, b: np.ndarray, n_level: int, cycles: int = 40):
     lib = ctx.lib
     db = ctx.field(b)
     dp = ctx.field(np.zeros(ctx.size()))
-    cfg = MixedCfg(n_level, 2, 1, MIXED_REMOVE_MEAN, 0.6666666667, 1.0, 1e-3, 400, 0.0, cycles)
+    # no mean removal: A p_inf must not change where A 1 != 0 (Dirichlet boundaries)
+    cfg = MixedCfg(n_level, 2, 1, 0, 0.6666666667, 1.0, 1e-3, 400, 0.0, cycles)
     mx = C.c_void_p()
     cuda_check(lib.artss_mixed_create(ctx.h, C.byref(cfg), C.byref(mx)), "mixed")
     try:
