@@ -65,6 +65,20 @@ enum Family : int {
 };
 static_assert(FAM_COUNT == ARTSS_KERNEL_FAMILIES, "family table");
 
+// Autotuner key: kernel id, level shape, kernel flavour.
+struct TuneKey {
+    int kernel;
+    int64_t nx, ny, nz;
+    int flavour;
+    bool operator<(const TuneKey &o) const {
+        if (kernel != o.kernel) return kernel < o.kernel;
+        if (nx != o.nx) return nx < o.nx;
+        if (ny != o.ny) return ny < o.ny;
+        if (nz != o.nz) return nz < o.nz;
+        return flavour < o.flavour;
+    }
+};
+
 struct Profile {
     uint64_t mask = 0;
     int64_t launches[FAM_COUNT] = {};
@@ -91,6 +105,8 @@ struct artss_ctx {
     std::set<double *> fields;
     artss::Profile prof;
     std::map<std::pair<const void *, int>, CUtensorMap> tmaps;  // TMA descriptors per (array, level)
+    bool autotune = true;                                        // time kernel variants on first use
+    std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
     int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},
                                {1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1}};
 };

@@ -327,8 +327,15 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
         const int64_t n = ctx->lvl[Lc].size();
         ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mx_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(m->e[Lc], n, pred));
         ARTSS_LAUNCH_CK(ctx);
-        if ((st = coarse_cluster_f32(ctx, m->e[Lc], m->r[Lc], Lc, m->cfg.coarse_smoother, m->cfg.coarse_w,
-                                     m->cfg.coarse_rel_tol, m->cfg.coarse_max_iter, pred)))
+        double w = m->cfg.coarse_w;
+        if (w <= 0) {
+            // red-black SOR with the optimal weight of the model problem on this grid
+            const Level &C = ctx->lvl[Lc];
+            const double n = (double) std::max({C.i2 - C.i1 + 1, C.j2 - C.j1 + 1, C.k2 - C.k1 + 1});
+            w = m->cfg.coarse_smoother == ARTSS_SMOOTHER_CGS ? 2. / (1. + sin(M_PI / (n + 1.))) : 0.6666666667;
+        }
+        if ((st = coarse_cluster_f32(ctx, m->e[Lc], m->r[Lc], Lc, m->cfg.coarse_smoother, w, m->cfg.coarse_rel_tol,
+                                     m->cfg.coarse_max_iter, pred)))
             return st;
     }
     for (int l = Lc - 1; l >= 0; l--) {

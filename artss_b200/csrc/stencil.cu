@@ -397,6 +397,13 @@ constexpr unsigned kStPlaneBytes = kStPlane * sizeof(double);
 static_assert(kTmaBoxX >= kSwTx + 5 && kTmaBoxY == kSwTy + 4, "TMA window covers tile + ring + alignment");
 static_assert(kStPlaneBytes % 128 == 0, "slots stay 128-byte aligned");
 
+// z-planes per block of the TMA sweep: the autotuned choice among these
+constexpr int kStDepths[3] = {8, 16, 32};
+inline dim3 sweep_tma_grid(const Box3 &b, int zb) {
+    return dim3((unsigned) ((b.nx() + kSwTx - 1) / kSwTx), (unsigned) ((b.ny() + kSwTy - 1) / kSwTy),
+                (unsigned) ((b.nz() + zb - 1) / zb));
+}
+
 inline size_t sweep_tma_smem(bool turb) {
     return (size_t) kStPlaneBytes * (kStSlotsX + (turb ? 2 : 1) * kStSlotsB);
 }
@@ -435,7 +442,7 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 
 constexpr int kStPolls = 1 << 22;  // mbarrier polls before a wait gives up
 
-template <bool TURB>
+template <bool TURB, int ZB>
 __global__ void __launch_bounds__(kStThreads, 2)
 k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
                 const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out,
@@ -455,8 +462,8 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     const int64_t wxa = wx0 - (wx0 & 1);                             // TMA window start, even
     const int ox = (int) (wx0 - wxa);
     const int64_t wy0 = box.y0 + (int64_t) blockIdx.y * kSwTy - 2;
-    const int64_t kc0 = box.z0 + (int64_t) blockIdx.z * kSwZ;
-    const int64_t kc1 = min(kc0 + kSwZ - 1, box.z1);
+    const int64_t kc0 = box.z0 + (int64_t) blockIdx.z * ZB;
+    const int64_t kc1 = min(kc0 + ZB - 1, box.z1);
     const int64_t pbase = kc0 - 2, plast = kc1 + 2;  // staged planes
 
     if (tid == 0) {
@@ -498,25 +505,27 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     // this thread's red x-pair (tile + ring) and black x-pair (tile)
     const int ry = 1 + tid / ((kSwTx + 2) / 2), px = tid % ((kSwTx + 2) / 2);
     const int64_t gjr = wy0 + ry;
-    const bool red_row = gjr >= box.y0 && gjr <= box.y1;
+    const bool red_row_ok = gjr >= box.y0 && gjr <= box.y1;
+    const int64_t red_row = nj * gjr;
     const bool red_tile = ry >= 2 && ry < kSwTy + 2;
     const bool has_black = tid < (kSwTx / 2) * kSwTy;
     const int tx = tid % (kSwTx / 2), ty = tid / (kSwTx / 2);
     const int64_t gjb = wy0 + 2 + ty;
+    const int64_t black_row = nj * gjb;
     const int lx0 = 2 + 2 * tx;
     auto red_x = [&](int64_t k) { return 1 + 2 * px + (int) ((wx0 + 1 + gjr + k) & 1); };  // (i + j + k) even
     auto red_flag = [&](int64_t k) -> uint8_t {
-        if (!red_row || k < box.z0 || k > box.z1) return 0;
+        if (!red_row_ok || k < box.z0 || k > box.z1) return 0;
         const int64_t gi = wx0 + red_x(k);
         if (gi < box.x0 || gi > box.x1) return 0;
-        return __ldg(flags + gi + nj * gjr + nk * k);
+        return __ldg(flags + gi + red_row + nk * k);
     };
     auto black_par = [&](int64_t kb) { return (int) ((wx0 + lx0 + gjb + kb + 1) & 1); };  // (i + j + k) odd
     auto black_flag = [&](int64_t kb) -> uint8_t {
         if (!has_black || gjb > box.y1 || kb < kc0 || kb > kc1) return 0;
         const int64_t gi = wx0 + lx0 + black_par(kb);
         if (gi > box.x1) return 0;
-        return __ldg(flags + gi + nj * gjb + nk * kb);
+        return __ldg(flags + gi + black_row + nk * kb);
     };
 
     double acc = 0.0;
@@ -568,7 +577,7 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
                     v = update(xslot(kb - 1), x0, xslot(kb + 1), e0 + s, bslot(kb), r2);
                     acc += r2;
                 }
-                out[gi + nj * gjb + nk * kb] = v;
+                out[gi + black_row + nk * kb] = v;
             }
         }
         fr = fr_next;
@@ -787,6 +796,93 @@ int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, in
     return apply_bc(ctx, out, 0, field_type);
 }
 
+namespace {
+
+// The TMA sweep with z-depth kStDepths[v]; returns the number of blocks (partials).
+int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, size_t smem, const CUtensorMap &mx,
+                     const CUtensorMap &mb, const CUtensorMap &me, double *w, const Level &L, const DiffCoef &c,
+                     LoopState *pred, int *nb) {
+    const dim3 g = sweep_tma_grid(box, kStDepths[v]);
+    *nb = nblocks(g);
+#define ARTSS_SWEEP_TMA(T, Z)                                                                               \
+    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<T, Z><<<g, kStThreads, smem, ctx->stream>>>(                 \
+                                   mx, mb, me, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred))
+    switch (v * 2 + (turb ? 1 : 0)) {
+        case 0: ARTSS_SWEEP_TMA(false, 8); break;
+        case 1: ARTSS_SWEEP_TMA(true, 8); break;
+        case 2: ARTSS_SWEEP_TMA(false, 16); break;
+        case 3: ARTSS_SWEEP_TMA(true, 16); break;
+        case 4: ARTSS_SWEEP_TMA(false, 32); break;
+        default: ARTSS_SWEEP_TMA(true, 32); break;
+    }
+#undef ARTSS_SWEEP_TMA
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int set_sweep_smem(bool turb, size_t smem) {
+    const int b = (int) smem;
+    if (turb) {
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    } else {
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+    }
+    return ARTSS_OK;
+}
+
+// Autotuner of the sweep's z-depth: the first solve on a level shape times
+// every depth on that solve's first iteration (the sweep reads `rd`, b, EV and
+// writes only `w` and the partials, so repeating it changes nothing) and keeps
+// the fastest for the context.
+int tune_sweep(artss_ctx *ctx, bool turb, const Box3 &box, size_t smem, const CUtensorMap &mx, const CUtensorMap &mb,
+               const CUtensorMap &me, double *w, const Level &L, const DiffCoef &c, LoopState *pred, int *choice) {
+    const TuneKey key{0, L.Nx, L.Ny, L.Nz, turb ? 1 : 0};
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end()) { *choice = it->second; return ARTSS_OK; }
+    if (!ctx->autotune) { *choice = 1; return ARTSS_OK; }
+    cudaEvent_t e0, e1;
+    ARTSS_CK(cudaEventCreate(&e0));
+    ARTSS_CK(cudaEventCreate(&e1));
+    int best = 1, st = ARTSS_OK, nb = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < 3 && !st; v++) {
+        if ((st = launch_sweep_tma(ctx, turb, v, box, smem, mx, mb, me, w, L, c, pred, &nb))) break;  // warm
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < 3 && !st; r++) st = launch_sweep_tma(ctx, turb, v, box, smem, mx, mb, me, w, L, c, pred, &nb);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { st = cuda_fail(cudaGetLastError(), "autotune"); break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    ctx->tuned[key] = best;
+    *choice = best;
+    return ARTSS_OK;
+}
+
+}  // namespace
+
+int artss_ctx_autotune(artss_ctx *ctx, int enable) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    ctx->autotune = enable != 0;
+    if (!enable) ctx->tuned.clear();
+    return ARTSS_OK;
+}
+
+int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
+    if (!ctx) return 0;
+    const Level &L = ctx->lvl[0];
+    auto it = ctx->tuned.find(TuneKey{0, L.Nx, L.Ny, L.Nz, turbulent ? 1 : 0});
+    return it == ctx->tuned.end() ? 0 : kStDepths[it->second];
+}
+
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
                       double dt, int field_type, const artss_iter_cfg *cfg, int in_is_scratch,
                       artss_iter_stats *stats) {
@@ -798,13 +894,13 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     const Box3 box = inner_box(L);
     const dim3 g = sweep_grid(box);
     if ((st = check_reduce_blocks(g))) return st;
-    const int nb = nblocks(g);
+    if ((st = check_reduce_blocks(sweep_tma_grid(box, kStDepths[0])))) return st;
+    int nb = nblocks(g);
     // TMA plane staging where the row pitch allows it, cp.async otherwise
     const bool tma = tma_level_ok(ctx, 0);
     const size_t smem = tma ? sweep_tma_smem(ev != nullptr) : sweep_smem(ev != nullptr);
     if (tma) {
-        if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        if ((st = set_sweep_smem(ev != nullptr, smem))) return st;
     } else {
         if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
@@ -837,6 +933,12 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
         if (ev && (st = tensor_map_3d(ctx, ev, 0, &tm_e))) return st;
     }
     LoopState *pred_rw = ctx->d_loop + slot;
+    int depth = 1;
+    if (tma && cond) {
+        const int n1 = (s0 + 1) & 1;
+        if ((st = tune_sweep(ctx, ev != nullptr, box, smem, *tm_x[1 - n1], *tm_b, *tm_e, buf[n1], L, c, pred_rw, &depth)))
+            return st;
+    }
     while (cond) {
         // `batch` iterations per host round trip; iterations past convergence skip themselves
         for (int64_t r = 0; r < batch; r++) {
@@ -844,20 +946,16 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
             double *w = buf[(s0 + n) & 1];
             const double *rd = buf[(s0 + n + 1) & 1];
             if (tma) {
-                const CUtensorMap &mx = *tm_x[(s0 + n + 1) & 1];
-                if (ev)
-                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<true><<<g, kStThreads, smem, ctx->stream>>>(
-                        mx, *tm_b, *tm_e, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred_rw));
-                else
-                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<false><<<g, kStThreads, smem, ctx->stream>>>(
-                        mx, *tm_b, *tm_e, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred_rw));
+                if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, smem, *tm_x[(s0 + n + 1) & 1], *tm_b,
+                                           *tm_e, w, L, c, pred_rw, &nb)))
+                    return st;
             } else if (ev)
                 ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
                     w, rd, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
             else
                 ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<false><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
                     w, rd, b, nullptr, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
-            ARTSS_LAUNCH_CK(ctx);
+            if (!tma) ARTSS_LAUNCH_CK(ctx);
             if ((st = apply_bc(ctx, w, 0, field_type, pred))) return st;
             if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
         }

@@ -334,7 +334,7 @@ def run_poisson(args, dist):
     mcfg = A.MgCfg(5, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
     A.cuda_check(cuda.artss_mg_create(ctx.h, C.byref(mcfg), C.byref(mg)), "mg")
     mx = C.c_void_p()
-    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 0.6666666667, 1.0, 1e-3, 400, 1e-8, 200)
+    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 0.6666666667, 0.0, 1e-3, 200, 1e-8, 200)
     A.cuda_check(cuda.artss_mixed_create(ctx.h, C.byref(xcfg), C.byref(mx)), "mixed")
 
     def plain(st):
@@ -359,8 +359,20 @@ def run_poisson(args, dist):
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
+        # one more solve with per-family event timing (not part of the timed numbers)
+        nf = 20
+        cuda.artss_ctx_profile(ctx.h, (1 << nf) - 1)
+        cuda.artss_ctx_profile_reset(ctx.h)
+        A.cuda_check(cuda.artss_fill(ctx.h, dp, 0, 0.0), "fill")
+        A.cuda_check(fn(st), name)
+        Lc = (C.c_int64 * nf)()
+        Mc = (C.c_double * nf)()
+        A.cuda_check(cuda.artss_ctx_profile_read(ctx.h, Lc, Mc, nf), "profile")
+        cuda.artss_ctx_profile(ctx.h, 0)
+        fam = {cuda.artss_kernel_family_name(f).decode(): (int(Lc[f]), round(Mc[f], 3)) for f in range(nf) if Lc[f]}
         res[name] = {"ms_per_solve": float(np.median(times)), "ms_all": [round(t, 3) for t in times],
-                     "cycles": int(st.cycles), "rel_residual": float(st.rel_residual)}
+                     "cycles": int(st.cycles), "rel_residual": float(st.rel_residual),
+                     "kernel_launches_ms": dict(sorted(fam.items(), key=lambda kv: -kv[1][1]))}
     cuda.artss_mixed_destroy(mx)
     cuda.artss_mg_destroy(mg)
     ctx.close()

@@ -223,6 +223,13 @@ int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t,
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
                       double D, const double *ev, double dt, int field_type,
                       const artss_iter_cfg *cfg, int in_is_scratch, artss_iter_stats *stats);
+/* Autotuner (no counterpart in the reference): the first colored Gauss-Seidel
+ * solve on a level shape times the sweep's z-depths (8, 16, 32 planes per
+ * block) on its first iteration and keeps the fastest for the context.
+ * enable = 0 switches tuning off (16 planes) and forgets earlier choices;
+ * artss_cgs_sweep_depth returns the chosen depth, 0 before the first solve. */
+int artss_ctx_autotune(artss_ctx *ctx, int enable);
+int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent);
 /* IDiffusion::diffuse, JacobiDiffuse (src/diffusion/JacobiDiffuse.cpp:31-203). */
 int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b,
                          double D, const double *ev, double dt, int field_type,
@@ -286,7 +293,9 @@ typedef struct {
     int32_t coarse_smoother;  /* ARTSS_SMOOTHER_JACOBI or ARTSS_SMOOTHER_CGS (FP64, one cluster kernel) */
     int32_t flags;            /* ARTSS_MIXED_REMOVE_MEAN */
     double w;                 /* Jacobi weight of the FP32 sweeps */
-    double coarse_w;          /* relaxation weight of the coarse solve */
+    double coarse_w;          /* relaxation weight of the coarse solve; <= 0: red-black SOR with the
+                               * model problem's optimal weight 2 / (1 + sin(pi / (n + 1))) for CGS,
+                               * 2/3 for Jacobi */
     double coarse_rel_tol;    /* coarse solve stops at this fraction of its initial residual ... */
     int64_t coarse_max_iter;  /* ... or after this many sweeps */
     double rel_tol;           /* outer stopping rule */

@@ -233,3 +233,26 @@ def test_cgs_odd_pitch(tmp_path, turbulent):
         assert np.array_equal(ctx.download(din), ri)
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("autotune", [0, 1])
+def test_cgs_autotune(env, autotune):
+    """Every z-depth of the sweep gives the same result; the tuner records one."""
+    sc, geom, ctx, osc = env
+    A.cuda_check(ctx.lib.artss_ctx_autotune(ctx.h, autotune), "autotune")
+    n = ctx.size()
+    out0, in0, b, ev = rnd(71, n, 290, 300), rnd(72, n, 290, 300), rnd(73, n, 290, 300), rnd(74, n, 0, 1e-3)
+    dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
+    cfg = A.IterCfg(4, 1e-300, 1.0)
+    stats = A.IterStats()
+    A.cuda_check(ctx.lib.artss_diffuse_cgs(ctx.h, dout, din, db, 4.2e-5, dev, sc.dt, FT["w"], C.byref(cfg), 0,
+                                           C.byref(stats)), "cgs")
+    ro, ri = out0.copy(), in0.copy()
+    res = C.c_double()
+    oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev), sc.dt, FT["w"], 4, 1e-300, 1.0,
+                                    C.byref(res))
+    assert np.array_equal(ctx.download(dout), ro)
+    assert np.array_equal(ctx.download(din), ri)
+    depth = ctx.lib.artss_cgs_sweep_depth(ctx.h, 1)
+    assert depth in ((8, 16, 32) if autotune else (0,))
+    A.cuda_check(ctx.lib.artss_ctx_autotune(ctx.h, 1), "autotune")
