@@ -82,6 +82,11 @@ class SolveStats(C.Structure):
 
 MIXED_REMOVE_MEAN = 1
 
+
+class ConvDesc(C.Structure):
+    _fields_ = [("D", C.c_int32), ("H", C.c_int32), ("W", C.c_int32), ("cin", C.c_int32), ("cout", C.c_int32),
+                ("relu", C.c_int32)]
+
 BC_DTYPE = np.dtype([("target", "<i8"), ("source", "<i8"), ("value", "<f8"), ("sign", "<i4"), ("reserved", "<i4")])
 
 _cuda: Optional[C.CDLL] = None
@@ -151,6 +156,8 @@ def load_cuda() -> C.CDLL:
             "artss_mixed_solve": ([_P, _D, _D, C.POINTER(SolveStats)], C.c_int),
             "artss_laplacian": ([_P, _D, _D, C.c_int], C.c_int),
             "artss_ctx_autotune": ([_P, C.c_int], C.c_int),
+            "artss_conv3d_fwd": ([_P, C.POINTER(ConvDesc), _P, _P, _P, _P], C.c_int),
+            "artss_nn_check": ([_P], C.c_int),
             "artss_cgs_sweep_depth": ([_P, C.c_int], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
             "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),
@@ -414,7 +421,7 @@ def consistent_rhs(ctx: Context, b: np.ndarray, n_level: int, cycles: int = 40):
     db = ctx.field(b)
     dp = ctx.field(np.zeros(ctx.size()))
     # no mean removal: A p_inf must not change where A 1 != 0 (Dirichlet boundaries)
-    cfg = MixedCfg(n_level, 2, 1, 0, 0.6666666667, 0.0, 1e-3, 200, 0.0, cycles)
+    cfg = MixedCfg(n_level, 2, 1, 0, 0.6666666667, 0.0, 1e-3, 40, 0.0, cycles)
     mx = C.c_void_p()
     cuda_check(lib.artss_mixed_create(ctx.h, C.byref(cfg), C.byref(mx)), "mixed")
     try:

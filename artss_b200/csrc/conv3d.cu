@@ -1,0 +1,241 @@
+// BF16 implicit-GEMM 3-D convolution on the 5th-generation tensor cores
+// (tcgen05.mma, FP32 accumulation in tensor memory) for the learned
+// initial guess of the pressure solve.  No counterpart in the reference.
+//
+// Activations are channels-last, [D][H][W][C] bf16, C a multiple of 16.
+// Kernel 3x3x3, stride 1, zero padding 1 (cross-correlation):
+//     y[z,y,x,co] = bias[co] + sum_{t, ci} w[t][co][ci] * x[z+dz, y+dy, x+dx, ci]
+// with tap t = 9 (dz+1) + 3 (dy+1) + (dx+1).
+//
+// GEMM view: M = 128 output voxels (a run of x, several y rows when W < 128),
+// N = C_out, K = 27 taps x C_in.  Per tap one TMA load brings the 128 shifted
+// input rows (out-of-range voxels arrive as zeros, which is the padding) in
+// the K-major core-matrix layout [C_in/8][128][8], and one bulk copy brings
+// the tap's weights, pre-packed as [C_in/8][C_out][8]; one thread issues the
+// C_in/16 MMAs of the tap and commits them to the stage's "empty" barrier.
+// After the 27th tap the accumulator (128 lanes x C_out FP32 columns) is read
+// by all 128 threads with tcgen05.ld: bias, optional ReLU, BF16, store.
+// Blocks are persistent over output tiles; loads run kConvStages taps ahead,
+// across tile boundaries.  Every wait is bounded and raises an error flag.
+#include "internal.cuh"
+#include "tc.cuh"
+
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+#include <mutex>
+#include <tuple>
+
+namespace artss {
+
+namespace {
+
+constexpr int kConvThreads = 128;
+constexpr int kConvStages = 4;
+constexpr int kConvPolls = 1 << 20;
+constexpr size_t kConvGuard = 64 * 1024;  // shared memory past the last stage, never addressed by a correct descriptor
+
+struct ConvShape {
+    int D, H, W, cin, cout;
+    int tw, th;               // tile: tw x th voxels of one z-plane, tw * th = 128
+    int tiles_x, tiles_y, tiles;
+    unsigned a_bytes, b_bytes, stage_bytes;
+};
+
+__global__ void __launch_bounds__(kConvThreads, 1)
+k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__restrict__ wp,
+             const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y, ConvShape s, int relu,
+             int *__restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t cv_sm[];
+    __shared__ __align__(8) uint64_t full[kConvStages], empty[kConvStages], accb;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const unsigned tcols = s.cout <= 32 ? 32u : (s.cout <= 64 ? 64u : 128u);
+    if (tid == 0) {
+        for (int i = 0; i < kConvStages; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        tc::mbar_init(&accb, 1);
+        tc::fence_barrier_init();
+        s_fail = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, tcols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const int my_tiles = (s.tiles - (int) blockIdx.x + (int) gridDim.x - 1) / (int) gridDim.x;
+    const int nsteps = my_tiles * 27;
+    const int kk_n = s.cin / 16;
+    const uint32_t idesc = tc::idesc_bf16(128, s.cout, 0, 0);
+    const unsigned lbo_a = 128 * 16, lbo_b = (unsigned) s.cout * 16;
+
+    // thread 0: issue the loads of step p
+    auto produce = [&](int p) {
+        const int st = p % kConvStages;
+        if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
+            return false;
+        const int tile = (int) blockIdx.x + (p / 27) * (int) gridDim.x, tap = p % 27;
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+        tc::mbar_expect_tx(&full[st], s.a_bytes + s.b_bytes);
+        tc::tma_load_5d(a, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, 0, z + dz, &full[st]);
+        tc::bulk_load(a + s.a_bytes, wp + (size_t) tap * s.cout * s.cin, s.b_bytes, &full[st]);
+        return true;
+    };
+
+    int step = 0;
+    bool ok = true;
+    if (tid == 0)
+        for (int p = 0; p < kConvStages - 1 && p < nsteps && ok; p++) ok = produce(p);
+    for (int it = 0; it < my_tiles; it++) {
+        const int tile = (int) blockIdx.x + it * (int) gridDim.x;
+        if (tid == 0 && ok) {
+            for (int tap = 0; tap < 27 && ok; tap++, step++) {
+                if (step + kConvStages - 1 < nsteps) ok = produce(step + kConvStages - 1);
+                const int st = step % kConvStages;
+                if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / kConvStages) & 1), kConvPolls);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+                const uint8_t *b = a + s.a_bytes;
+                for (int kk = 0; kk < kk_n; kk++) {
+                    const uint64_t da = tc::smem_desc(a + 2 * kk * lbo_a, lbo_a, 128);
+                    const uint64_t db = tc::smem_desc(b + 2 * kk * lbo_b, lbo_b, 128);
+                    tc::mma_bf16(tmem, da, db, idesc, (tap | kk) != 0);
+                }
+                tc::mma_commit(&empty[st]);
+                if (tap == 26) tc::mma_commit(&accb);
+            }
+            if (!ok) s_fail = 1;
+        }
+        // epilogue: lane = voxel of the tile, columns = output channels
+        bool acc_ok = tc::mbar_wait(&accb, (unsigned) (it & 1), kConvPolls);
+        if (__syncthreads_or(!acc_ok || s_fail)) {
+            if (tid == 0 && err) atomicExch(err, 1);
+            break;
+        }
+        tc::tc_fence_after();
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
+        const int vx = tx * s.tw + tid % s.tw, vy = ty * s.th + tid / s.tw;
+        __nv_bfloat16 *yo = y + (((size_t) z * s.H + vy) * s.W + vx) * s.cout;
+        for (int c0 = 0; c0 < s.cout; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) c0, v);
+            __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                float r = v[i] + (bias ? bias[c0 + i] : 0.f);
+                if (relu) r = fmaxf(r, 0.f);
+                o[i] = __float2bfloat16_rn(r);
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(yo + c0);
+            dst[0] = reinterpret_cast<const uint4 *>(o)[0];
+            dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+        }
+        tc::tc_fence_before();
+        __syncthreads();
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_enc = nullptr;
+std::once_flag g_enc_once;
+
+int encode_x_map(const __nv_bfloat16 *x, const ConvShape &s, CUtensorMap *m) {
+    std::call_once(g_enc_once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_enc = (PFN_cuTensorMapEncodeTiled_v12000) fn;
+    });
+    if (!g_enc) { set_error("cuTensorMapEncodeTiled is not available"); return ARTSS_ERR_CUDA; }
+    // dims: channel-in-chunk (8), x, y, chunk, z -> box lands as [chunk][y][x][8]
+    const cuuint64_t dim[5] = {8, (cuuint64_t) s.W, (cuuint64_t) s.H, (cuuint64_t) (s.cin / 8), (cuuint64_t) s.D};
+    const cuuint64_t es = 2;
+    const cuuint64_t stride[4] = {(cuuint64_t) s.cin * es, (cuuint64_t) s.W * s.cin * es, 16,
+                                  (cuuint64_t) s.H * s.W * s.cin * es};
+    const cuuint32_t box[5] = {8, (cuuint32_t) s.tw, (cuuint32_t) s.th, (cuuint32_t) (s.cin / 8), 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult r = g_enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *) x, dim, stride, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { set_error("conv3d: input tensor map rejected"); return ARTSS_ERR_ARG; }
+    return ARTSS_OK;
+}
+
+int conv_shape(const artss_conv_desc *d, ConvShape *s) {
+    if (d->D < 1 || d->H < 1 || d->W < 1 || d->cin < 16 || d->cin % 16 || d->cin > 256 ||
+        (d->cout != 16 && d->cout != 32 && d->cout != 64 && d->cout != 128)) {
+        set_error("conv3d: channels must be multiples of 16 (C_in <= 256, C_out in 16/32/64/128)");
+        return ARTSS_ERR_ARG;
+    }
+    s->D = d->D; s->H = d->H; s->W = d->W; s->cin = d->cin; s->cout = d->cout;
+    if (d->W % 128 == 0) { s->tw = 128; s->th = 1; }
+    else if (128 % d->W == 0 && d->H % (128 / d->W) == 0 && d->W >= 8) { s->tw = d->W; s->th = 128 / d->W; }
+    else { set_error("conv3d: W must be a multiple of 128 or divide 128 (>= 8) with H a multiple of 128/W"); return ARTSS_ERR_ARG; }
+    s->tiles_x = d->W / s->tw;
+    s->tiles_y = d->H / s->th;
+    s->tiles = s->tiles_x * s->tiles_y * d->D;
+    s->a_bytes = 128u * (unsigned) d->cin * 2u;
+    s->b_bytes = (unsigned) d->cout * (unsigned) d->cin * 2u;
+    s->stage_bytes = (s->a_bytes + s->b_bytes + 1023u) & ~1023u;
+    if ((size_t) s->stage_bytes * kConvStages + kConvGuard > 220 * 1024) {
+        set_error("conv3d: stages too large"); return ARTSS_ERR_LIMIT;
+    }
+    return ARTSS_OK;
+}
+
+}  // namespace
+
+int conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *wp, const float *bias, void *y) {
+    ConvShape s;
+    int st = conv_shape(d, &s);
+    if (st) return st;
+    if (((uintptr_t) x & 15) || ((uintptr_t) wp & 15) || ((uintptr_t) y & 15)) {
+        set_error("conv3d: arrays must be 16-byte aligned"); return ARTSS_ERR_ARG;
+    }
+    CUtensorMap m;
+    if ((st = encode_x_map((const __nv_bfloat16 *) x, s, &m))) return st;
+    const size_t smem = (size_t) s.stage_bytes * kConvStages + kConvGuard;
+    ARTSS_CK(cudaFuncSetAttribute(k_conv3d_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const int grid = std::min(s.tiles, sms);
+    ARTSS_LAUNCH(ctx, FAM_CONV, k_conv3d_fwd<<<grid, kConvThreads, smem, ctx->stream>>>(
+                                    m, (const __nv_bfloat16 *) wp, bias, (__nv_bfloat16 *) y, s, d->relu,
+                                    &ctx->d_loop[kNnErrSlot].pad));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+}  // namespace artss
+
+using namespace artss;
+
+extern "C" int artss_conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *w_packed,
+                                const float *bias, void *y) {
+    if (!ctx || !d || !x || !w_packed || !y) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    return conv3d_fwd(ctx, d, x, w_packed, bias, y);
+}
+
+extern "C" int artss_nn_check(artss_ctx *ctx) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    LoopState ls{};
+    int st = read_loop(ctx, kNnErrSlot, &ls);
+    if (st) return st;
+    if (ls.pad) {
+        ARTSS_CK(cudaMemsetAsync(&ctx->d_loop[kNnErrSlot].pad, 0, sizeof(int), ctx->stream));
+        ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+        set_error("a network kernel gave up waiting for its operands");
+        return ARTSS_ERR_CUDA;
+    }
+    return ARTSS_OK;
+}

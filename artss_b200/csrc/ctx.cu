@@ -97,7 +97,7 @@ cudaEvent_t prof_event(artss_ctx *ctx) {
 static const char *const kFamilyNames[FAM_COUNT] = {
     "advect", "smagorinsky", "divergence", "projection", "buoyancy", "add_source", "cgs_sweep",
     "jacobi_diffuse", "copy_domain", "bc_wave", "field_op", "couple", "mg_jacobi", "mg_cgs", "mg_residuum",
-    "mg_restrict", "mg_prolongate", "mg_resnorm", "reduce", "mg_coarse"};
+    "mg_restrict", "mg_prolongate", "mg_resnorm", "reduce", "mg_coarse", "conv3d", "nn_elementwise"};
 
 }  // namespace artss
 

@@ -21,6 +21,7 @@ constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
 constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
 constexpr int kReduceThreads = 256;
 constexpr int kMaxPartials = 1 << 16;   // per-block partial sums of up to two reduction passes
+constexpr int kNnErrSlot = 15;          // loop slot whose error flag the network kernels raise
 constexpr int kTmaBoxX = 72, kTmaBoxY = 12;  // TMA plane window (cells): a 64 x 8 tile, a 2-cell ring, x aligned to 2
 
 enum CellFlag : uint8_t { kInner = 1, kDomain = 2 };
@@ -61,6 +62,7 @@ enum Family : int {
     FAM_ADVECT = 0, FAM_SMAGORINSKY, FAM_DIVERGENCE, FAM_PROJECTION, FAM_BUOYANCY, FAM_ADD_SOURCE,
     FAM_CGS, FAM_JACOBI, FAM_COPY_DOMAIN, FAM_BC, FAM_FIELD_OP, FAM_COUPLE, FAM_MG_JACOBI, FAM_MG_CGS,
     FAM_MG_RESIDUUM, FAM_MG_RESTRICT, FAM_MG_PROLONGATE, FAM_MG_RESNORM, FAM_REDUCE, FAM_MG_COARSE,
+    FAM_CONV, FAM_NN,
     FAM_COUNT
 };
 static_assert(FAM_COUNT == ARTSS_KERNEL_FAMILIES, "family table");

@@ -334,7 +334,7 @@ def run_poisson(args, dist):
     mcfg = A.MgCfg(5, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
     A.cuda_check(cuda.artss_mg_create(ctx.h, C.byref(mcfg), C.byref(mg)), "mg")
     mx = C.c_void_p()
-    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 0.6666666667, 0.0, 1e-3, 200, 1e-8, 200)
+    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 0.6666666667, 0.0, 1e-3, 40, 1e-8, 200)
     A.cuda_check(cuda.artss_mixed_create(ctx.h, C.byref(xcfg), C.byref(mx)), "mixed")
 
     def plain(st):

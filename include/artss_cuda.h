@@ -141,7 +141,7 @@ int64_t artss_ctx_kernel_launches(artss_ctx *ctx);
  * synchronises the stream and returns, per family, the launches counted since
  * the last reset (all families, profiled or not) and the summed device time
  * of the profiled ones. */
-#define ARTSS_KERNEL_FAMILIES 20
+#define ARTSS_KERNEL_FAMILIES 22
 int artss_ctx_profile(artss_ctx *ctx, uint64_t mask);
 int artss_ctx_profile_read(artss_ctx *ctx, int64_t *launches, double *ms, int n_families);
 int artss_ctx_profile_reset(artss_ctx *ctx);
@@ -309,6 +309,26 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
  * level's pressure boundary program is applied to p); other cells of out are
  * left as they are. */
 int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level);
+
+/* ---- learned initial guess: BF16 3-D convolution on the tensor cores ----
+ * No counterpart in the reference.  Activations are channels-last [D][H][W][C]
+ * bf16 with C a multiple of 16; 3x3x3 kernel, stride 1, zero padding 1:
+ *   y[z,y,x,co] = bias[co] + sum_{t,ci} w[t][co][ci] x[z+dz, y+dy, x+dx, ci],
+ *   t = 9(dz+1) + 3(dy+1) + (dx+1).
+ * w_packed holds w as [27][C_in/8][C_out][8] bf16 (per tap the shared-memory
+ * layout of the MMA's B operand); bias (FP32, C_out) may be NULL; relu != 0
+ * clamps the output at 0.  W must be a multiple of 128, or divide 128 (>= 8)
+ * with H a multiple of 128/W; C_out in {16, 32, 64, 128}; C_in <= 256. */
+typedef struct {
+    int32_t D, H, W;
+    int32_t cin, cout;
+    int32_t relu;
+} artss_conv_desc;
+int artss_conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *w_packed,
+                     const float *bias, void *y);
+/* Reads and clears the error flag the network kernels raise when a bounded
+ * wait gives up (returns ARTSS_ERR_CUDA then); synchronizes the stream. */
+int artss_nn_check(artss_ctx *ctx);
 
 /* ||b - A p||_2 over level-0 inner cells (VCycleMG.cpp:186-194) and ||b||_2. */
 int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double *res_out, double *b_norm_out);

@@ -58,7 +58,7 @@ def solve_pair(sc, seed, mixed_flags, rel_tol=1e-8):
         ctx.lib.artss_mg_destroy(mg)
         p_ref = ctx.download(dp_ref)
         # mixed precision to the target tolerance
-        mcfg = A.MixedCfg(sc.n_level, 2, 1, mixed_flags, 0.6666666667, 0.0, 1e-3, 200, rel_tol, 200)
+        mcfg = A.MixedCfg(sc.n_level, 2, 1, mixed_flags, 0.6666666667, 0.0, 1e-3, 40, rel_tol, 200)
         mx = C.c_void_p()
         A.cuda_check(ctx.lib.artss_mixed_create(ctx.h, C.byref(mcfg), C.byref(mx)), "mixed")
         dp = ctx.field(np.zeros(n))
