@@ -301,8 +301,8 @@ k_cgs_sweep(double *__restrict__ out, const double *__restrict__ in, const doubl
         }
         cp_async_commit();
     };
-    auto xslot = [&](int64_t p) { return X + (int) ((p - kc0 + 2 + 2 * kSwSlotsX) % kSwSlotsX) * kSwPlane; };
-    auto bslot = [&](int64_t p) { return (int) ((p - kc0 + 2 + 2 * kSwSlotsB) % kSwSlotsB) * kSwPlane; };
+    auto xslot = [&](int64_t p) { return X + ((unsigned) (p - kc0 + 2) % (unsigned) kSwSlotsX) * kSwPlane; };
+    auto bslot = [&](int64_t p) { return (int) (((unsigned) (p - kc0 + 2) % (unsigned) kSwSlotsB) * kSwPlane); };
 
     // one stencil update; returns the new value and the residual term
     auto update = [&](const double *xm, const double *x0, const double *xp, int e, int bo, double &res2) {
@@ -474,7 +474,7 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     // thread 0: load plane p into its slots
     auto issue = [&](int64_t p) {
         if (p > plast) return;
-        const int u = (int) (p - pbase);
+        const unsigned u = (unsigned) (p - pbase);
         uint64_t *bar = &bars[u % kStSlotsX];
         mbar_expect_tx(bar, kStPlaneBytes * (TURB ? 3u : 2u));
         tma_load_plane(X + (u % kStSlotsX) * kStPlane, &tm_x, (int) wxa, (int) wy0, (int) p, bar);
@@ -482,11 +482,12 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
         if (TURB) tma_load_plane(E + (u % kStSlotsB) * kStPlane, &tm_e, (int) wxa, (int) wy0, (int) p, bar);
     };
     auto ready = [&](int64_t p) -> bool {
-        const int u = (int) (p - pbase);
-        return mbar_wait(&bars[u % kStSlotsX], (unsigned) ((u / kStSlotsX) & 1), kStPolls);
+        const unsigned u = (unsigned) (p - pbase);
+        return mbar_wait(&bars[u % kStSlotsX], (u / kStSlotsX) & 1u, kStPolls);
     };
-    auto xslot = [&](int64_t p) { return X + (int) ((p - pbase) % kStSlotsX) * kStPlane; };
-    auto bslot = [&](int64_t p) { return (int) ((p - pbase) % kStSlotsB) * kStPlane; };
+    // ring slots by local plane number (32-bit, constant divisors)
+    auto xslot = [&](int64_t p) { return X + ((unsigned) (p - pbase) % (unsigned) kStSlotsX) * kStPlane; };
+    auto bslot = [&](int64_t p) { return (int) (((unsigned) (p - pbase) % (unsigned) kStSlotsB) * kStPlane); };
     auto update = [&](const double *xm, const double *x0, const double *xp, int e, int bo, double &res2) {
         double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
         if (TURB) {
