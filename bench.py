@@ -179,6 +179,10 @@ def launch_bytes(family: str, n: int, N: int, launches: int) -> float:
     return 0.0
 
 
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel on
+# the 256x128x128 channel, per inner cell: profiles/k_cgs_sweep_tma_channel256x128x128.md
+NCU_TRAFFIC_PER_CELL = {"cgs_sweep": (118.077440e6 + 13.617152e6) / 4190208}
+
 MODELED = ("advect", "cgs_sweep", "smagorinsky", "couple", "projection")
 
 
@@ -296,7 +300,10 @@ def run_b200(args, dist):
         "gpu_launches": int(gpu_launches),
         "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": (NCU_TRAFFIC_PER_CELL[fam] * inner if fam in NCU_TRAFFIC_PER_CELL else None),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, per inner "
+                                       "cell, scaled to this workload's cells",
                      "launches": dom_launches, "avg_launch_us": 1e3 * dom_ms / max(dom_launches, 1)},
         "kernel_share_ms": {k: round(v, 4) for k, v in sorted(share_ms.items(), key=lambda kv: -kv[1])},
         "kernel_ms_of_two_steps": round(total_kernel_ms, 4),
