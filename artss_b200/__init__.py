@@ -158,6 +158,7 @@ def load_cuda() -> C.CDLL:
             "artss_ctx_autotune": ([_P, C.c_int], C.c_int),
             "artss_conv3d_fwd": ([_P, C.POINTER(ConvDesc), _P, _P, _P, _P], C.c_int),
             "artss_nn_check": ([_P], C.c_int),
+            "artss_conv3d_wgrad": ([_P, C.POINTER(ConvDesc), _P, _P, _P], C.c_int),
             "artss_cgs_sweep_depth": ([_P, C.c_int], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
             "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),

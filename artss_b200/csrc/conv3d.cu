@@ -50,7 +50,7 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
     __shared__ uint32_t tmem_base;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
-    const unsigned tcols = s.cout <= 32 ? 32u : (s.cout <= 64 ? 64u : 128u);
+    const unsigned tcols = s.cout <= 32 ? 32u : (s.cout <= 64 ? 64u : (s.cout <= 128 ? 128u : 256u));
     if (tid == 0) {
         for (int i = 0; i < kConvStages; i++) {
             tc::mbar_init(&full[i], 1);
@@ -145,10 +145,125 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
     if (warp == 0) tc::tmem_dealloc(tmem, tcols);
 }
 
+// Weight gradient dW[t][co][ci] += sum_v dY[v][co] x[v + off_t][ci] as a GEMM
+// with M = C_out (padded to 128 by TMA's zero fill), N = C_in, K = voxels.
+// The activation tiles keep the forward's shared-memory layout
+// [channel/8][128 voxels][8], which read as MN-major operands is exactly the
+// canonical layout: 8 voxels (K) x 8 channels (M or N) per core matrix, the
+// core matrices of one channel group 128 bytes apart (LBO), channel groups
+// 2048 bytes apart (SBO).  A block accumulates one tap over its range of
+// voxel tiles in tensor memory, then adds the C_out x C_in block to dW with
+// FP32 atomics (dW must be zeroed by the caller), and moves to the next tap.
+constexpr int kWgradMRows = 128;
+
+__global__ void __launch_bounds__(kConvThreads, 1)
+k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_dy,
+               float *__restrict__ dw, ConvShape s, int tiles_per_block, int *__restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t cv_sm[];
+    __shared__ __align__(8) uint64_t full[kConvStages], empty[kConvStages], accb;
+    __shared__ uint32_t tmem_base;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const unsigned tcols = s.cin <= 32 ? 32u : (s.cin <= 64 ? 64u : (s.cin <= 128 ? 128u : 256u));
+    const int t_begin = (int) blockIdx.x * tiles_per_block;
+    const int t_end = min(s.tiles, t_begin + tiles_per_block);
+    const int ntile = t_end - t_begin;
+    if (ntile <= 0) return;
+    if (tid == 0) {
+        for (int i = 0; i < kConvStages; i++) {
+            tc::mbar_init(&full[i], 1);
+            tc::mbar_init(&empty[i], 1);
+        }
+        tc::mbar_init(&accb, 1);
+        tc::fence_barrier_init();
+        s_fail = 0;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(&tmem_base, tcols);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_base;
+    const int nsteps = 27 * ntile;
+    const uint32_t idesc = tc::idesc_bf16(kWgradMRows, s.cin, 1, 1);
+    const unsigned a_bytes = (unsigned) kWgradMRows * 128u * 2u;  // dY tile, 16 channel groups
+    const unsigned b_bytes = s.a_bytes;                            // x tile, C_in/8 channel groups
+
+    auto produce = [&](int p) {
+        const int st = p % kConvStages;
+        if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
+            return false;
+        const int tap = p / ntile, tile = t_begin + p % ntile;
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+        tc::mbar_expect_tx(&full[st], a_bytes + b_bytes);
+        tc::tma_load_5d(a, &tm_dy, 0, tx * s.tw, ty * s.th, 0, z, &full[st]);
+        tc::tma_load_5d(a + a_bytes, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, 0, z + dz, &full[st]);
+        return true;
+    };
+
+    bool ok = true;
+    int step = 0;
+    if (tid == 0)
+        for (int p = 0; p < kConvStages - 1 && p < nsteps && ok; p++) ok = produce(p);
+    for (int tap = 0; tap < 27; tap++) {
+        if (tid == 0 && ok) {
+            for (int i = 0; i < ntile && ok; i++, step++) {
+                if (step + kConvStages - 1 < nsteps) ok = produce(step + kConvStages - 1);
+                const int st = step % kConvStages;
+                if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / kConvStages) & 1), kConvPolls);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+                const uint8_t *b = a + a_bytes;
+#pragma unroll
+                for (int kk = 0; kk < 8; kk++) {  // 16 voxels per MMA
+                    const uint64_t da = tc::smem_desc(a + kk * 256, 128, 2048);
+                    const uint64_t db = tc::smem_desc(b + kk * 256, 128, 2048);
+                    tc::mma_bf16(tmem, da, db, idesc, (i | kk) != 0);
+                }
+                tc::mma_commit(&empty[st]);
+                if (i == ntile - 1) tc::mma_commit(&accb);
+            }
+            if (!ok) s_fail = 1;
+        }
+        bool acc_ok = tc::mbar_wait(&accb, (unsigned) (tap & 1), kConvPolls);
+        if (__syncthreads_or(!acc_ok || s_fail)) {
+            if (tid == 0 && err) atomicExch(err, 1);
+            break;
+        }
+        tc::tc_fence_after();
+        // lane = output channel co, columns = input channels
+        for (int c0 = 0; c0 < s.cin; c0 += 16) {
+            float v[16];
+            tc::tmem_ld16(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) c0, v);
+            if (tid < s.cout) {
+                float *d = dw + ((size_t) tap * s.cout + tid) * s.cin + c0;
+#pragma unroll
+                for (int i = 0; i < 16; i++) atomicAdd(d + i, v[i]);
+            }
+        }
+        tc::tc_fence_before();
+        __syncthreads();
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 g_enc = nullptr;
 std::once_flag g_enc_once;
 
+// map of a [D][H][W][c] activation whose box lands as [box_chunks][th][tw][8]
+int encode_act_map(const __nv_bfloat16 *x, const ConvShape &s, int c, int box_chunks, CUtensorMap *m);
+
 int encode_x_map(const __nv_bfloat16 *x, const ConvShape &s, CUtensorMap *m) {
+    return encode_act_map(x, s, s.cin, s.cin / 8, m);
+}
+
+int encode_act_map(const __nv_bfloat16 *x, const ConvShape &s, int c, int box_chunks, CUtensorMap *m) {
     std::call_once(g_enc_once, [] {
         cudaDriverEntryPointQueryResult q;
         void *fn = nullptr;
@@ -158,11 +273,10 @@ int encode_x_map(const __nv_bfloat16 *x, const ConvShape &s, CUtensorMap *m) {
     });
     if (!g_enc) { set_error("cuTensorMapEncodeTiled is not available"); return ARTSS_ERR_CUDA; }
     // dims: channel-in-chunk (8), x, y, chunk, z -> box lands as [chunk][y][x][8]
-    const cuuint64_t dim[5] = {8, (cuuint64_t) s.W, (cuuint64_t) s.H, (cuuint64_t) (s.cin / 8), (cuuint64_t) s.D};
+    const cuuint64_t dim[5] = {8, (cuuint64_t) s.W, (cuuint64_t) s.H, (cuuint64_t) (c / 8), (cuuint64_t) s.D};
     const cuuint64_t es = 2;
-    const cuuint64_t stride[4] = {(cuuint64_t) s.cin * es, (cuuint64_t) s.W * s.cin * es, 16,
-                                  (cuuint64_t) s.H * s.W * s.cin * es};
-    const cuuint32_t box[5] = {8, (cuuint32_t) s.tw, (cuuint32_t) s.th, (cuuint32_t) (s.cin / 8), 1};
+    const cuuint64_t stride[4] = {(cuuint64_t) c * es, (cuuint64_t) s.W * c * es, 16, (cuuint64_t) s.H * s.W * c * es};
+    const cuuint32_t box[5] = {8, (cuuint32_t) s.tw, (cuuint32_t) s.th, (cuuint32_t) box_chunks, 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     const CUresult r = g_enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *) x, dim, stride, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -173,8 +287,8 @@ int encode_x_map(const __nv_bfloat16 *x, const ConvShape &s, CUtensorMap *m) {
 
 int conv_shape(const artss_conv_desc *d, ConvShape *s) {
     if (d->D < 1 || d->H < 1 || d->W < 1 || d->cin < 16 || d->cin % 16 || d->cin > 256 ||
-        (d->cout != 16 && d->cout != 32 && d->cout != 64 && d->cout != 128)) {
-        set_error("conv3d: channels must be multiples of 16 (C_in <= 256, C_out in 16/32/64/128)");
+        d->cout < 16 || d->cout % 16 || d->cout > 256) {
+        set_error("conv3d: channels must be multiples of 16, at most 256");
         return ARTSS_ERR_ARG;
     }
     s->D = d->D; s->H = d->H; s->W = d->W; s->cin = d->cin; s->cout = d->cout;
@@ -194,6 +308,32 @@ int conv_shape(const artss_conv_desc *d, ConvShape *s) {
 }
 
 }  // namespace
+
+int conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *dy, float *dw) {
+    ConvShape s;
+    int st = conv_shape(d, &s);
+    if (st) return st;
+    if (d->cout > kWgradMRows || d->cin > 128) { set_error("conv3d wgrad: C_out and C_in at most 128"); return ARTSS_ERR_ARG; }
+    if (((uintptr_t) x & 15) || ((uintptr_t) dy & 15)) { set_error("conv3d: arrays must be 16-byte aligned"); return ARTSS_ERR_ARG; }
+    CUtensorMap mx, mdy;
+    if ((st = encode_act_map((const __nv_bfloat16 *) x, s, s.cin, s.cin / 8, &mx))) return st;
+    if ((st = encode_act_map((const __nv_bfloat16 *) dy, s, s.cout, kWgradMRows / 8, &mdy))) return st;
+    // stage: dY tile (128 voxels x 128 padded channels) + x tile
+    const unsigned stage = ((unsigned) kWgradMRows * 128u * 2u + s.a_bytes + 1023u) & ~1023u;
+    s.stage_bytes = stage;
+    const size_t smem = (size_t) stage * kConvStages + kConvGuard;
+    if (smem > 227 * 1024) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    ARTSS_CK(cudaFuncSetAttribute(k_conv3d_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const int grid = std::min(s.tiles, sms);
+    const int per = (s.tiles + grid - 1) / grid;
+    const int blocks = (s.tiles + per - 1) / per;
+    ARTSS_LAUNCH(ctx, FAM_CONV, k_conv3d_wgrad<<<blocks, kConvThreads, smem, ctx->stream>>>(
+                                    mx, mdy, dw, s, per, &ctx->d_loop[kNnErrSlot].pad));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
 
 int conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *wp, const float *bias, void *y) {
     ConvShape s;
@@ -238,4 +378,9 @@ extern "C" int artss_nn_check(artss_ctx *ctx) {
         return ARTSS_ERR_CUDA;
     }
     return ARTSS_OK;
+}
+
+extern "C" int artss_conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *dy, float *dw) {
+    if (!ctx || !d || !x || !dy || !dw) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    return conv3d_wgrad(ctx, d, x, dy, dw);
 }

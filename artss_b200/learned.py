@@ -51,3 +51,23 @@ def conv3d_ref(x: np.ndarray, w: np.ndarray, bias=None, relu=False) -> np.ndarra
     if relu:
         y = np.maximum(y, 0)
     return y
+
+
+def flip_weights(w: np.ndarray) -> np.ndarray:
+    """Weights of the input-gradient convolution: w'[ci][co][t] = w[co][ci][26 - t]."""
+    return np.ascontiguousarray(w.transpose(1, 0, 2, 3, 4)[:, :, ::-1, ::-1, ::-1])
+
+
+def conv3d_wgrad_ref(x: np.ndarray, dy: np.ndarray) -> np.ndarray:
+    """FP32 reference: dw[t][co][ci] = sum_v dy[v][co] x[v + off_t][ci]."""
+    D, H, W, ci = x.shape
+    co = dy.shape[3]
+    xp = np.zeros((D + 2, H + 2, W + 2, ci), np.float32)
+    xp[1:-1, 1:-1, 1:-1] = x
+    dw = np.zeros((27, co, ci), np.float32)
+    for kz in range(3):
+        for ky in range(3):
+            for kx in range(3):
+                dw[9 * kz + 3 * ky + kx] = np.einsum("zyxo,zyxc->oc", dy, xp[kz:kz + D, ky:ky + H, kx:kx + W],
+                                                     optimize=True)
+    return dw

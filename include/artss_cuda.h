@@ -318,7 +318,9 @@ int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level);
  * w_packed holds w as [27][C_in/8][C_out][8] bf16 (per tap the shared-memory
  * layout of the MMA's B operand); bias (FP32, C_out) may be NULL; relu != 0
  * clamps the output at 0.  W must be a multiple of 128, or divide 128 (>= 8)
- * with H a multiple of 128/W; C_out in {16, 32, 64, 128}; C_in <= 256. */
+ * with H a multiple of 128/W; C_in and C_out multiples of 16, at most 256.
+ * The backward pass w.r.t. the input is this same convolution with the
+ * weights flipped in space and C_in, C_out exchanged. */
 typedef struct {
     int32_t D, H, W;
     int32_t cin, cout;
@@ -326,6 +328,11 @@ typedef struct {
 } artss_conv_desc;
 int artss_conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *w_packed,
                      const float *bias, void *y);
+/* Weight gradient of artss_conv3d_fwd: dw[t][co][ci] += sum over voxels of
+ * dy[v][co] * x[v + offset(t)][ci] (FP32, dw zeroed by the caller); x is the
+ * forward input, dy the gradient of the forward output (same D, H, W).
+ * C_in, C_out multiples of 16, at most 128. */
+int artss_conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *dy, float *dw);
 /* Reads and clears the error flag the network kernels raise when a bounded
  * wait gives up (returns ARTSS_ERR_CUDA then); synchronizes the stream. */
 int artss_nn_check(artss_ctx *ctx);

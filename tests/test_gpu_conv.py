@@ -52,3 +52,47 @@ def test_conv3d_fwd(ctx, shape, cin, cout, relu):
     got = dy.float().cpu().numpy()
     err = np.abs(got - ref).max()
     assert err <= 1e-2 * np.abs(ref).max() + 1e-6, err
+
+
+@pytest.mark.parametrize("shape,cin,cout", [((4, 8, 32), 16, 32), ((2, 2, 128), 32, 16)])
+def test_conv3d_input_grad(ctx, shape, cin, cout):
+    """dX = the forward convolution of dY with flipped, transposed weights."""
+    import torch
+    D, H, W = shape
+    rng = np.random.default_rng(3 * cin + cout)
+    w = LN.round_bf16((rng.standard_normal((cout, cin, 3, 3, 3)) / np.sqrt(27 * cout)).astype(np.float32))
+    dy = LN.round_bf16(rng.standard_normal((D, H, W, cout)).astype(np.float32))
+    wf = LN.flip_weights(w)
+    ref = LN.conv3d_ref(dy, wf)
+    # the same as the adjoint of the forward map: <conv(x), dy> = <x, dx>
+    x = rng.standard_normal((D, H, W, cin)).astype(np.float32)
+    assert abs(np.vdot(LN.conv3d_ref(x, w), dy) - np.vdot(x, ref)) <= 1e-3 * abs(np.vdot(x, ref)) + 1e-3
+    ddy, dwf = dev_bf16(dy), dev_bf16(LN.pack_conv_weights(wf))
+    dx = torch.zeros((D, H, W, cin), dtype=torch.bfloat16, device="cuda")
+    torch.cuda.synchronize()
+    d = A.ConvDesc(D, H, W, cout, cin, 0)
+    A.cuda_check(ctx.lib.artss_conv3d_fwd(ctx.h, C.byref(d), ddy.data_ptr(), dwf.data_ptr(), None, dx.data_ptr()),
+                 "conv dgrad")
+    A.cuda_check(ctx.lib.artss_nn_check(ctx.h), "wait")
+    got = dx.float().cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-2 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("shape,cin,cout", [((4, 8, 32), 16, 32), ((2, 4, 64), 32, 16), ((2, 2, 128), 16, 64)])
+def test_conv3d_weight_grad(ctx, shape, cin, cout):
+    import torch
+    D, H, W = shape
+    rng = np.random.default_rng(5 * cin + cout)
+    x = LN.round_bf16(rng.standard_normal((D, H, W, cin)).astype(np.float32))
+    dy = LN.round_bf16(rng.standard_normal((D, H, W, cout)).astype(np.float32))
+    ref = LN.conv3d_wgrad_ref(x, dy)
+    dx_, ddy = dev_bf16(x), dev_bf16(dy)
+    dw = torch.zeros((27, cout, cin), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    d = A.ConvDesc(D, H, W, cin, cout, 0)
+    for _ in range(2):  # accumulates
+        A.cuda_check(ctx.lib.artss_conv3d_wgrad(ctx.h, C.byref(d), dx_.data_ptr(), ddy.data_ptr(), dw.data_ptr()),
+                     "wgrad")
+    A.cuda_check(ctx.lib.artss_nn_check(ctx.h), "wait")
+    got = dw.cpu().numpy()
+    assert np.abs(got - 2 * ref).max() <= 1e-4 * np.abs(ref).max() + 1e-4
