@@ -159,6 +159,19 @@ def load_cuda() -> C.CDLL:
             "artss_conv3d_fwd": ([_P, C.POINTER(ConvDesc), _P, _P, _P, _P], C.c_int),
             "artss_nn_check": ([_P], C.c_int),
             "artss_conv3d_wgrad": ([_P, C.POINTER(ConvDesc), _P, _P, _P], C.c_int),
+            "artss_nn_zero": ([_P, _P, C.c_int64], C.c_int),
+            "artss_nn_relu_bwd": ([_P, _P, _P, C.c_int64], C.c_int),
+            "artss_nn_pool2": ([_P, _P, _P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+            "artss_nn_up2": ([_P, _P, _P] + [C.c_int] * 7, C.c_int),
+            "artss_nn_copy_channels": ([_P, _P, C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int],
+                                       C.c_int),
+            "artss_nn_bias_grad": ([_P, _P, _P, C.c_int64, C.c_int], C.c_int),
+            "artss_nn_pack_weights": ([_P, _P, _P, C.c_int, C.c_int, C.c_int], C.c_int),
+            "artss_nn_adam": ([_P, _P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int],
+                              C.c_int),
+            "artss_nn_inputs": ([_P, C.c_int, _P, _P, C.c_double, C.c_double, _P, C.c_int], C.c_int),
+            "artss_nn_apply": ([_P, C.c_int, _P, C.c_int, _P, C.c_double, _P], C.c_int),
+            "artss_nn_mse": ([_P, _P, C.c_int, _P, _P, _P, C.c_int64, C.c_float, _P, C.c_int], C.c_int),
             "artss_cgs_sweep_depth": ([_P, C.c_int], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),
             "artss_ctx_profile_read": ([_P, _I64P, _D, C.c_int], C.c_int),

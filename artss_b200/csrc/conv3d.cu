@@ -7,10 +7,12 @@
 //     y[z,y,x,co] = bias[co] + sum_{t, ci} w[t][co][ci] * x[z+dz, y+dy, x+dx, ci]
 // with tap t = 9 (dz+1) + 3 (dy+1) + (dx+1).
 //
-// GEMM view: M = 128 output voxels (a run of x, several y rows when W < 128),
+// GEMM view: M = 128 output voxels (a run of x, several y rows and z planes
+// when W or W*H is below 128),
 // N = C_out, K = 27 taps x C_in.  Per tap one TMA load brings the 128 shifted
 // input rows (out-of-range voxels arrive as zeros, which is the padding) in
-// the K-major core-matrix layout [C_in/8][128][8], and one bulk copy brings
+// the K-major core-matrix layout [C_in/8][128][8] (the tensor map orders the
+// dimensions channel-in-group, x, y, z, channel group), and one bulk copy brings
 // the tap's weights, pre-packed as [C_in/8][C_out][8]; one thread issues the
 // C_in/16 MMAs of the tap and commits them to the stage's "empty" barrier.
 // After the 27th tap the accumulator (128 lanes x C_out FP32 columns) is read
@@ -36,8 +38,8 @@ constexpr size_t kConvGuard = 64 * 1024;  // shared memory past the last stage, 
 
 struct ConvShape {
     int D, H, W, cin, cout;
-    int tw, th;               // tile: tw x th voxels of one z-plane, tw * th = 128
-    int tiles_x, tiles_y, tiles;
+    int tw, th, tz;           // tile: tw x th x tz voxels, tw * th * tz = 128 (x fastest)
+    int tiles_x, tiles_y, tiles_z, tiles;
     unsigned a_bytes, b_bytes, stage_bytes;
 };
 
@@ -80,11 +82,11 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
         if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
             return false;
         const int tile = (int) blockIdx.x + (p / 27) * (int) gridDim.x, tap = p % 27;
-        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
         const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
         uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
         tc::mbar_expect_tx(&full[st], s.a_bytes + s.b_bytes);
-        tc::tma_load_5d(a, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, 0, z + dz, &full[st]);
+        tc::tma_load_5d(a, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, tzi * s.tz + dz, 0, &full[st]);
         tc::bulk_load(a + s.a_bytes, wp + (size_t) tap * s.cout * s.cin, s.b_bytes, &full[st]);
         return true;
     };
@@ -121,9 +123,9 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
             break;
         }
         tc::tc_fence_after();
-        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
-        const int vx = tx * s.tw + tid % s.tw, vy = ty * s.th + tid / s.tw;
-        __nv_bfloat16 *yo = y + (((size_t) z * s.H + vy) * s.W + vx) * s.cout;
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
+        const int vx = tx * s.tw + tid % s.tw, vy = ty * s.th + (tid / s.tw) % s.th, vz = tzi * s.tz + tid / (s.tw * s.th);
+        __nv_bfloat16 *yo = y + (((size_t) vz * s.H + vy) * s.W + vx) * s.cout;
         for (int c0 = 0; c0 < s.cout; c0 += 16) {
             float v[16];
             tc::tmem_ld16(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) c0, v);
@@ -196,12 +198,12 @@ k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__
         if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
             return false;
         const int tap = p / ntile, tile = t_begin + p % ntile;
-        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, z = tile / (s.tiles_x * s.tiles_y);
+        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
         const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
         uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
         tc::mbar_expect_tx(&full[st], a_bytes + b_bytes);
-        tc::tma_load_5d(a, &tm_dy, 0, tx * s.tw, ty * s.th, 0, z, &full[st]);
-        tc::tma_load_5d(a + a_bytes, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, 0, z + dz, &full[st]);
+        tc::tma_load_5d(a, &tm_dy, 0, tx * s.tw, ty * s.th, tzi * s.tz, 0, &full[st]);
+        tc::tma_load_5d(a + a_bytes, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, tzi * s.tz + dz, 0, &full[st]);
         return true;
     };
 
@@ -272,11 +274,11 @@ int encode_act_map(const __nv_bfloat16 *x, const ConvShape &s, int c, int box_ch
             g_enc = (PFN_cuTensorMapEncodeTiled_v12000) fn;
     });
     if (!g_enc) { set_error("cuTensorMapEncodeTiled is not available"); return ARTSS_ERR_CUDA; }
-    // dims: channel-in-chunk (8), x, y, chunk, z -> box lands as [chunk][y][x][8]
-    const cuuint64_t dim[5] = {8, (cuuint64_t) s.W, (cuuint64_t) s.H, (cuuint64_t) (c / 8), (cuuint64_t) s.D};
+    // dims: channel-in-chunk (8), x, y, z, chunk -> a box lands as [chunk][z][y][x][8]
+    const cuuint64_t dim[5] = {8, (cuuint64_t) s.W, (cuuint64_t) s.H, (cuuint64_t) s.D, (cuuint64_t) (c / 8)};
     const cuuint64_t es = 2;
-    const cuuint64_t stride[4] = {(cuuint64_t) c * es, (cuuint64_t) s.W * c * es, 16, (cuuint64_t) s.H * s.W * c * es};
-    const cuuint32_t box[5] = {8, (cuuint32_t) s.tw, (cuuint32_t) s.th, (cuuint32_t) box_chunks, 1};
+    const cuuint64_t stride[4] = {(cuuint64_t) c * es, (cuuint64_t) s.W * c * es, (cuuint64_t) s.H * s.W * c * es, 16};
+    const cuuint32_t box[5] = {8, (cuuint32_t) s.tw, (cuuint32_t) s.th, (cuuint32_t) s.tz, (cuuint32_t) box_chunks};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     const CUresult r = g_enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void *) x, dim, stride, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -292,16 +294,24 @@ int conv_shape(const artss_conv_desc *d, ConvShape *s) {
         return ARTSS_ERR_ARG;
     }
     s->D = d->D; s->H = d->H; s->W = d->W; s->cin = d->cin; s->cout = d->cout;
+    s->tz = 1;
     if (d->W % 128 == 0) { s->tw = 128; s->th = 1; }
-    else if (128 % d->W == 0 && d->H % (128 / d->W) == 0 && d->W >= 8) { s->tw = d->W; s->th = 128 / d->W; }
-    else { set_error("conv3d: W must be a multiple of 128 or divide 128 (>= 8) with H a multiple of 128/W"); return ARTSS_ERR_ARG; }
+    else if (128 % d->W == 0 && d->W * d->H >= 128 && d->H % (128 / d->W) == 0) { s->tw = d->W; s->th = 128 / d->W; }
+    else if (128 % (d->W * d->H) == 0 && d->D % (128 / (d->W * d->H)) == 0) {
+        s->tw = d->W; s->th = d->H; s->tz = 128 / (d->W * d->H);
+    } else {
+        set_error("conv3d: 128-voxel tiles must fit: W a multiple of 128, or W dividing 128 with H a multiple of "
+                  "128/W, or W*H dividing 128 with D a multiple of 128/(W*H)");
+        return ARTSS_ERR_ARG;
+    }
     s->tiles_x = d->W / s->tw;
     s->tiles_y = d->H / s->th;
-    s->tiles = s->tiles_x * s->tiles_y * d->D;
+    s->tiles_z = d->D / s->tz;
+    s->tiles = s->tiles_x * s->tiles_y * s->tiles_z;
     s->a_bytes = 128u * (unsigned) d->cin * 2u;
     s->b_bytes = (unsigned) d->cout * (unsigned) d->cin * 2u;
     s->stage_bytes = (s->a_bytes + s->b_bytes + 1023u) & ~1023u;
-    if ((size_t) s->stage_bytes * kConvStages + kConvGuard > 220 * 1024) {
+    if ((size_t) s->stage_bytes * kConvStages > 227 * 1024) {
         set_error("conv3d: stages too large"); return ARTSS_ERR_LIMIT;
     }
     return ARTSS_OK;
@@ -321,8 +331,9 @@ int conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const 
     // stage: dY tile (128 voxels x 128 padded channels) + x tile
     const unsigned stage = ((unsigned) kWgradMRows * 128u * 2u + s.a_bytes + 1023u) & ~1023u;
     s.stage_bytes = stage;
-    const size_t smem = (size_t) stage * kConvStages + kConvGuard;
-    if (smem > 227 * 1024) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    const size_t stages = (size_t) stage * kConvStages;
+    if (stages > 227 * 1024) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    const size_t smem = stages + std::min<size_t>(kConvGuard, 227 * 1024 - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -344,7 +355,8 @@ int conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const vo
     }
     CUtensorMap m;
     if ((st = encode_x_map((const __nv_bfloat16 *) x, s, &m))) return st;
-    const size_t smem = (size_t) s.stage_bytes * kConvStages + kConvGuard;
+    const size_t stages = (size_t) s.stage_bytes * kConvStages;
+    const size_t smem = stages + std::min<size_t>(kConvGuard, 227 * 1024 - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

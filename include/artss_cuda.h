@@ -317,8 +317,9 @@ int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level);
  *   t = 9(dz+1) + 3(dy+1) + (dx+1).
  * w_packed holds w as [27][C_in/8][C_out][8] bf16 (per tap the shared-memory
  * layout of the MMA's B operand); bias (FP32, C_out) may be NULL; relu != 0
- * clamps the output at 0.  W must be a multiple of 128, or divide 128 (>= 8)
- * with H a multiple of 128/W; C_in and C_out multiples of 16, at most 256.
+ * clamps the output at 0.  Tiles of 128 voxels must fit: W a multiple of
+ * 128, or W dividing 128 with H a multiple of 128/W, or W*H dividing 128 with
+ * D a multiple of 128/(W*H); C_in and C_out multiples of 16, at most 256.
  * The backward pass w.r.t. the input is this same convolution with the
  * weights flipped in space and C_in, C_out exchanged. */
 typedef struct {
@@ -333,6 +334,35 @@ int artss_conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, co
  * forward input, dy the gradient of the forward output (same D, H, W).
  * C_in, C_out multiples of 16, at most 128. */
 int artss_conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const void *dy, float *dw);
+/* Element-wise and data-movement kernels of the network (bf16 activations
+ * [D][H][W][C], FP32 parameters).  relu_bwd: dy *= (y > 0).  pool2: 2x2x2
+ * average (backward != 0: x is the coarse gradient, y the fine one, /8).
+ * up2: nearest 2x upsampling of x [D][H][W][C] into channels
+ * [c_off, c_off + C) of y [2D][2H][2W][c_total] (backward: sum of the 8
+ * children).  copy_channels: channel slice copy or add (concatenation).
+ * bias_grad: db[c] += sum_v dy[v][c].  pack_weights: FP32 w[27][co][ci] to the
+ * convolution's packed BF16 operand (flip != 0: input-gradient weights).
+ * adam: Adam with bias correction (step >= 1).  inputs: network input from
+ * level arrays (ch0 = s_rhs rhs, ch1 = inner-cell mask, ch2 = s_p p_prev, the
+ * rest 0) over the level's inner box.  apply: p = p_prev + scale * y[.][0] on
+ * inner cells.  mse: 0.5 sum over masked voxels (y[.][0] - target)^2 as block
+ * partials and its gradient (times inv_n) in channel 0 of dy. */
+int artss_nn_zero(artss_ctx *ctx, void *p, int64_t bytes);
+int artss_nn_relu_bwd(artss_ctx *ctx, void *dy, const void *y, int64_t n);
+int artss_nn_pool2(artss_ctx *ctx, const void *x, void *y, int D, int H, int W, int C, int backward);
+int artss_nn_up2(artss_ctx *ctx, const void *x, void *y, int D, int H, int W, int C, int c_total, int c_off,
+                 int backward);
+int artss_nn_copy_channels(artss_ctx *ctx, const void *src, int s_total, int s_off, void *dst, int d_total, int d_off,
+                           int C, int64_t voxels, int accumulate);
+int artss_nn_bias_grad(artss_ctx *ctx, const void *dy, float *db, int64_t voxels, int C);
+int artss_nn_pack_weights(artss_ctx *ctx, const float *w, void *packed, int cout, int cin, int flip);
+int artss_nn_adam(artss_ctx *ctx, float *w, const float *g, float *m, float *v, int64_t n, float lr, float b1,
+                  float b2, float eps, int step);
+int artss_nn_inputs(artss_ctx *ctx, int level, const double *rhs, const double *p_prev, double s_rhs, double s_p,
+                    void *out, int C);
+int artss_nn_apply(artss_ctx *ctx, int level, const void *y, int C, const double *p_prev, double scale, double *p);
+int artss_nn_mse(artss_ctx *ctx, const void *y, int C, const float *target, const void *inputs, void *dy,
+                 int64_t voxels, float inv_n, float *partials, int n_partials);
 /* Reads and clears the error flag the network kernels raise when a bounded
  * wait gives up (returns ARTSS_ERR_CUDA then); synchronizes the stream. */
 int artss_nn_check(artss_ctx *ctx);

@@ -31,6 +31,7 @@ def dev_bf16(a):
     ((4, 8, 32), 32, 64, 1),
     ((3, 4, 64), 48, 32, 1),
     ((2, 2, 128), 16, 16, 0),
+    ((8, 4, 16), 32, 16, 1),
 ])
 def test_conv3d_fwd(ctx, shape, cin, cout, relu):
     import torch
@@ -78,7 +79,8 @@ def test_conv3d_input_grad(ctx, shape, cin, cout):
     assert np.abs(got - ref).max() <= 1e-2 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("shape,cin,cout", [((4, 8, 32), 16, 32), ((2, 4, 64), 32, 16), ((2, 2, 128), 16, 64)])
+@pytest.mark.parametrize("shape,cin,cout", [((4, 8, 32), 16, 32), ((2, 4, 64), 32, 16), ((2, 2, 128), 16, 64),
+                                            ((4, 4, 16), 96, 32)])
 def test_conv3d_weight_grad(ctx, shape, cin, cout):
     import torch
     D, H, W = shape
