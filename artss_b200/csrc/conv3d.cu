@@ -34,7 +34,8 @@ namespace {
 constexpr int kConvThreads = 128;
 constexpr int kConvStages = 4;
 constexpr int kConvPolls = 1 << 20;
-constexpr size_t kConvGuard = 64 * 1024;  // shared memory past the last stage, never addressed by a correct descriptor
+constexpr size_t kConvGuard = 64 * 1024;           // shared memory past the last stage, never addressed by a correct descriptor
+constexpr size_t kConvSmemMax = 227 * 1024 - 2048;  // dynamic limit minus the kernels' static shared memory
 
 struct ConvShape {
     int D, H, W, cin, cout;
@@ -311,7 +312,7 @@ int conv_shape(const artss_conv_desc *d, ConvShape *s) {
     s->a_bytes = 128u * (unsigned) d->cin * 2u;
     s->b_bytes = (unsigned) d->cout * (unsigned) d->cin * 2u;
     s->stage_bytes = (s->a_bytes + s->b_bytes + 1023u) & ~1023u;
-    if ((size_t) s->stage_bytes * kConvStages > 227 * 1024) {
+    if ((size_t) s->stage_bytes * kConvStages > kConvSmemMax) {
         set_error("conv3d: stages too large"); return ARTSS_ERR_LIMIT;
     }
     return ARTSS_OK;
@@ -332,8 +333,8 @@ int conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const 
     const unsigned stage = ((unsigned) kWgradMRows * 128u * 2u + s.a_bytes + 1023u) & ~1023u;
     s.stage_bytes = stage;
     const size_t stages = (size_t) stage * kConvStages;
-    if (stages > 227 * 1024) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
-    const size_t smem = stages + std::min<size_t>(kConvGuard, 227 * 1024 - stages);
+    if (stages > kConvSmemMax) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    const size_t smem = stages + std::min<size_t>(kConvGuard, kConvSmemMax - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -356,7 +357,7 @@ int conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const vo
     CUtensorMap m;
     if ((st = encode_x_map((const __nv_bfloat16 *) x, s, &m))) return st;
     const size_t stages = (size_t) s.stage_bytes * kConvStages;
-    const size_t smem = stages + std::min<size_t>(kConvGuard, 227 * 1024 - stages);
+    const size_t smem = stages + std::min<size_t>(kConvGuard, kConvSmemMax - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

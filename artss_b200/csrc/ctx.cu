@@ -13,6 +13,9 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 
 int cuda_fail(cudaError_t e, const char *what) {
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    // a failed runtime call also sets the thread's last error; clear it so the
+    // next launch check does not report it again (sticky errors stay)
+    (void) cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? ARTSS_ERR_NOMEM
          : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? ARTSS_ERR_NO_DEVICE
          : ARTSS_ERR_CUDA;

@@ -183,6 +183,21 @@ __global__ void k_nn_apply(const __nv_bfloat16 *__restrict__ y, int C, const dou
     }
 }
 
+// training target: t[v] = scale * (p_star[a] - p_prev[a]) over the inner box
+// (0 outside the inner list), voxel order x fastest
+__global__ void k_nn_target(const double *__restrict__ p_star, const double *__restrict__ p_prev,
+                            const uint8_t *__restrict__ flags, Level L, int D, int H, int W, double scale,
+                            float *__restrict__ t) {
+    const int64_t n = (int64_t) D * H * W;
+    NN_LOOP(n) {
+        const int x = (int) (q % W);
+        const int y = (int) ((q / W) % H);
+        const int z = (int) (q / ((int64_t) W * H));
+        const int64_t a = (L.i1 + x) + L.Nx * (L.j1 + y) + L.nxy() * (L.k1 + z);
+        t[q] = (flags[a] & kInner) ? (float) (scale * (p_star[a] - p_prev[a])) : 0.f;
+    }
+}
+
 // loss 0.5 * sum over inner cells (y[v][0] - t[v])^2 and its gradient into
 // channel 0 of dy (other channels zero); block partials of the loss
 __global__ void k_mse(const __nv_bfloat16 *__restrict__ y, int C, const float *__restrict__ t,
@@ -311,6 +326,18 @@ int artss_nn_apply(artss_ctx *ctx, int level, const void *y, int C, const double
     const int W = (int) (L.i2 - L.i1 + 1), H = (int) (L.j2 - L.j1 + 1), D = (int) (L.k2 - L.k1 + 1);
     ARTSS_LAUNCH(ctx, FAM_NN, k_nn_apply<<<nblk((int64_t) D * H * W), 256, 0, ctx->stream>>>(
                                  (const __nv_bfloat16 *) y, C, p_prev, ctx->d_flags[level], L, D, H, W, scale, p));
+    NN_CK(ctx);
+    return ARTSS_OK;
+}
+
+int artss_nn_target(artss_ctx *ctx, int level, const double *p_star, const double *p_prev, double scale, float *t) {
+    NN_ARGS_OK(ctx && p_star && p_prev && t);
+    int st = check_level(ctx, level);
+    if (st) return st;
+    const Level &L = ctx->lvl[level];
+    const int W = (int) (L.i2 - L.i1 + 1), H = (int) (L.j2 - L.j1 + 1), D = (int) (L.k2 - L.k1 + 1);
+    ARTSS_LAUNCH(ctx, FAM_NN, k_nn_target<<<nblk((int64_t) D * H * W), 256, 0, ctx->stream>>>(
+                                 p_star, p_prev, ctx->d_flags[level], L, D, H, W, scale, t));
     NN_CK(ctx);
     return ARTSS_OK;
 }

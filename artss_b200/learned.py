@@ -149,9 +149,12 @@ class UNet:
     C_IN = 16
 
     def __init__(self, ctx, dims, seed: int = 0):
+        """ctx: an artss_b200.Context or a raw artss_ctx handle (the network's
+        kernels run on that context's stream)."""
         import torch
         from artss_b200 import load_cuda
-        self.ctx, self.h, self.lib = ctx, ctx.h, load_cuda()
+        self.ctx, self.lib = ctx, load_cuda()
+        self.h = ctx.h if hasattr(ctx, "h") else ctx
         self.device = torch.device("cuda", torch.cuda.current_device())
         D, H, W = dims
         assert D % 4 == 0 and H % 4 == 0 and W % 4 == 0
@@ -193,10 +196,12 @@ class UNet:
         for l in self.layers:
             l.pack()
 
-    def forward(self):
-        """Runs the network on buf['x'] ([D][H][W][16] bf16); returns buf['out']."""
+    def forward(self, x=None):
+        """Runs the network on x ([D][H][W][16] bf16; default buf['x']);
+        returns buf['out'].  backward() and loss_grad() use the same x."""
         B, L, h, d = self.buf, self.lib, self.h, self.dims
-        self.e0a.fwd(B["x"], B["a0"], d[0])
+        self.x = B["x"] if x is None else x
+        self.e0a.fwd(self.x, B["a0"], d[0])
         self.e0b.fwd(B["a0"], B["s0"], d[0])
         _ck(L.artss_nn_pool2(h, _p(B["s0"]), _p(B["p0"]), *d[0], 16, 0), "pool")
         self.e1a.fwd(B["p0"], B["a1"], d[1])
@@ -237,7 +242,7 @@ class UNet:
         _ck(L.artss_nn_pool2(h, _p(G["p0"]), _p(G["t0"]), *d[0], 16, 1), "pool bwd")
         _ck(L.artss_nn_copy_channels(h, _p(G["t0"]), 16, 0, _p(G["s0"]), 16, 0, 16, self.vox(0), 1), "add")
         self.e0b.bwd(B["a0"], B["s0"], G["s0"], G["a0"], d[0])
-        self.e0a.bwd(B["x"], B["a0"], G["a0"], None, d[0])
+        self.e0a.bwd(self.x, B["a0"], G["a0"], None, d[0])
 
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
         self.step_no += 1
@@ -252,7 +257,206 @@ class UNet:
         import torch
         nb = 296
         part = torch.empty(nb, dtype=torch.float32, device=self.device)
-        _ck(self.lib.artss_nn_mse(self.h, _p(self.buf["out"]), 16, _p(target), _p(self.buf["x"]),
+        _ck(self.lib.artss_nn_mse(self.h, _p(self.buf["out"]), 16, _p(target), _p(self.x),
                                   _p(self.grad["out"]), self.vox(0), 1.0 / max(n_fluid, 1), _p(part), nb), "mse")
         _ck(self.lib.artss_nn_check(self.h), "network")
         return float(part.cpu().numpy().astype(np.float64).sum()) / max(n_fluid, 1)
+
+
+# ------------------------------------------------------- data, training, use
+def plume_channel(seed: int, nx: int = 128, ny: int = 64, nz: int = 64, steps: int = 10 ** 6):
+    """A seeded scene of the ensemble family: the 6.4 x 3.2 x 3.2 m channel with
+    an open (Dirichlet p) outflow, inflow U[0.2, 1.0] m/s, a Gaussian source of
+    U[10, 150] kW centred at U[0.2, 0.8] of the extent, 0-3 box obstacles with
+    edges of 2-8 coarse cells.  The open outflow keeps the pressure problem
+    non-singular, so every right-hand side is solvable to any tolerance."""
+    import random
+    from artss_b200 import scenes
+    rng = random.Random(7919 * seed + 1)
+    sc = scenes.channel_with_cube(nx=nx, ny=ny, nz=nz, steps=steps, n_level=4)
+    u_in = rng.uniform(0.2, 1.0)
+    sc.boundaries = [b if not (b[0] == "u" and b[1] == "left") else ("u", "left", "dirichlet", u_in)
+                     for b in sc.boundaries]
+    sc.hrr = rng.uniform(10.0, 150.0)
+    ext = (sc.X[1] - sc.X[0], sc.Y[1] - sc.Y[0], sc.Z[1] - sc.Z[0])
+    sc.source_pos = tuple(lo + rng.uniform(0.2, 0.8) * e for lo, e in zip((sc.X[0], sc.Y[0], sc.Z[0]), ext))
+    h = (ext[0] / nx, ext[1] / ny, ext[2] / nz)
+    sc.obstacles = scenes.random_boxes((nx, ny, nz), 2 * 8, 8 * 8, rng.randint(0, 3), seed, h,
+                                       origin=(sc.X[0], sc.Y[0], sc.Z[0]), levels=3)
+    sc.seed = seed
+    return sc
+
+
+class Sampler:
+    """Pressure problems of a running simulation: each sample() advances the
+    scene by one timestep and records (rhs, mask, p_prev) -> p_star, where
+    p_prev is the pressure before the step and p_star the step's pressure
+    equation solved to `rel_tol` from p_prev by the mixed-precision solver.
+    Inputs and targets are stored on the device in the network's layout."""
+
+    def __init__(self, sim, dims, rel_tol: float = 1e-8, n_level: int = 4):
+        import torch
+        from artss_b200 import MixedCfg, load_cuda
+        self.sim, self.ctx, self.lib = sim, sim.context, load_cuda()
+        self.dims = dims
+        self.vox = dims[0] * dims[1] * dims[2]
+        self.size = sim.size
+        self.p_prev = self._field()
+        self.p_star = self._field()
+        self.zero = self._field()
+        _ck(self.lib.artss_fill(self.ctx, self.zero, 0, 0.0), "fill")
+        cfg = MixedCfg(n_level, 2, 1, 0, 0.6666666667, 0.0, 1e-3, 40, rel_tol, 200)
+        self.mx = _C.c_void_p()
+        _ck(self.lib.artss_mixed_create(self.ctx, _C.byref(cfg), _C.byref(self.mx)), "mixed")
+        self.device = torch.device("cuda", torch.cuda.current_device())
+
+    def _field(self):
+        from artss_b200 import _D
+        p = _D()
+        _ck(self.lib.artss_field_alloc(self.ctx, 0, _C.byref(p)), "alloc")
+        return p
+
+    def norm(self, f) -> float:
+        r, bn = _C.c_double(), _C.c_double()
+        _ck(self.lib.artss_residual_norm(self.ctx, self.zero, f, _C.byref(r), _C.byref(bn)), "norm")
+        return bn.value
+
+    def scales(self, rhs, p_prev):
+        n = float(self.vox)
+        nr, npv = self.norm(rhs), self.norm(p_prev)
+        s_rhs = np.sqrt(n) / nr if nr > 0 else 1.0
+        s_p = np.sqrt(n) / npv if npv > 0 else s_rhs
+        return s_rhs, s_p
+
+    def inputs(self, rhs, p_prev, s_rhs, s_p, out):
+        _ck(self.lib.artss_nn_inputs(self.ctx, 0, rhs, p_prev, s_rhs, s_p, _p(out), 16), "inputs")
+
+    def solve(self, p, rhs):
+        from artss_b200 import SolveStats
+        st = SolveStats()
+        _ck(self.lib.artss_mixed_solve(self.mx, p, rhs, _C.byref(st)), "solve")
+        return st
+
+    def sample(self):
+        import torch
+        from artss_b200 import _D
+        p = _C.cast(_C.c_void_p(self.sim.device_pointer("p")), _D)
+        rhs = _C.cast(_C.c_void_p(self.sim.device_pointer("rhs")), _D)
+        _ck(self.lib.artss_copy(self.ctx, self.p_prev, p, 0), "copy")
+        self.sim.run(1)
+        _ck(self.lib.artss_copy(self.ctx, self.p_star, self.p_prev, 0), "copy")
+        st = self.solve(self.p_star, rhs)
+        s_rhs, s_p = self.scales(rhs, self.p_prev)
+        x = torch.empty(self.vox * 16, dtype=torch.bfloat16, device=self.device)
+        t = torch.empty(self.vox, dtype=torch.float32, device=self.device)
+        self.inputs(rhs, self.p_prev, s_rhs, s_p, x)
+        _ck(self.lib.artss_nn_target(self.ctx, 0, self.p_star, self.p_prev, s_p, _p(t)), "target")
+        _ck(self.lib.artss_nn_check(self.ctx), "sample")
+        return {"x": x, "t": t, "cycles": int(st.cycles), "n_fluid": int(self.sim.inner_cells)}
+
+    def close(self):
+        if self.mx:
+            self.lib.artss_mixed_destroy(self.mx)
+            self.mx = _C.c_void_p()
+        for f in (self.p_prev, self.p_star, self.zero):
+            self.lib.artss_field_free(self.ctx, f)
+
+
+def collect(seeds, per_scene: int, warmup: int, dims, tmpdir: str, device: int = 0):
+    """Training samples from the plain solver: per seeded scene, `warmup`
+    timesteps, then `per_scene` sampled timesteps (see Sampler)."""
+    import os
+    from artss_b200 import Simulation, scenes
+    out = []
+    for seed in seeds:
+        sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
+        sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"train_{seed}.xml")), device=device)
+        sim.run(warmup)
+        smp = Sampler(sim, dims)
+        for _ in range(per_scene):
+            out.append(smp.sample())
+        smp.close()
+        sim.close()
+    return out
+
+
+def train(net: UNet, samples, epochs: int, lr: float = 1e-3, seed: int = 0):
+    """Adam on 0.5 mean (prediction - target)^2 over fluid cells, one sample
+    per step; returns the mean loss of every epoch."""
+    rng = np.random.default_rng(seed)
+    history = []
+    for _ in range(epochs):
+        tot = 0.0
+        for i in rng.permutation(len(samples)):
+            s = samples[i]
+            net.forward(s["x"])
+            tot += net.loss_grad(s["t"], s["n_fluid"])
+            net.backward()
+            net.adam(lr=lr)
+        history.append(tot / max(len(samples), 1))
+    return history
+
+
+def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0):
+    """Per timestep of unseen scenes: the pressure equation solved to 1e-8 by
+    the mixed-precision solver from (a) the previous pressure and (b) the
+    network's guess p_prev + correction, falling back to (a) when the guess's
+    initial residual is larger.  Returns cycles and ms (CUDA events on the
+    context stream; (b) includes the network's inference)."""
+    import os
+    import torch
+    from artss_b200 import Simulation, SolveStats, _D, scenes
+    res = {"baseline_cycles": [], "baseline_ms": [], "learned_cycles": [], "learned_ms": [], "fallbacks": 0,
+           "infer_ms": []}
+    for seed in seeds:
+        sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
+        sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"eval_{seed}.xml")), device=device)
+        sim.run(warmup)
+        smp = Sampler(sim, dims)
+        lib, ctx = smp.lib, smp.ctx
+        stream = torch.cuda.ExternalStream(lib.artss_ctx_stream(ctx))
+        guess = smp._field()
+        x = torch.empty(smp.vox * 16, dtype=torch.bfloat16, device=smp.device)
+        for _ in range(steps):
+            p = _C.cast(_C.c_void_p(sim.device_pointer("p")), _D)
+            rhs = _C.cast(_C.c_void_p(sim.device_pointer("rhs")), _D)
+            _ck(lib.artss_copy(ctx, smp.p_prev, p, 0), "copy")
+            sim.run(1)
+            # (a) from the previous pressure
+            _ck(lib.artss_copy(ctx, smp.p_star, smp.p_prev, 0), "copy")
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = smp.solve(smp.p_star, rhs)
+            e1.record(stream)
+            e1.synchronize()
+            res["baseline_cycles"].append(int(st.cycles))
+            res["baseline_ms"].append(e0.elapsed_time(e1))
+            # (b) from the network's guess
+            s_rhs, s_p = smp.scales(rhs, smp.p_prev)
+            e0.record(stream)
+            smp.inputs(rhs, smp.p_prev, s_rhs, s_p, x)
+            out = net.forward(x)
+            _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.p_prev, 1.0 / s_p, guess), "apply")
+            e2 = torch.cuda.Event(enable_timing=True)
+            e2.record(stream)
+            r_g, _ = _resnorm(lib, ctx, guess, rhs)
+            r_p, _ = _resnorm(lib, ctx, smp.p_prev, rhs)
+            if r_g > r_p:
+                res["fallbacks"] += 1
+                _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
+            st = smp.solve(guess, rhs)
+            e1.record(stream)
+            e1.synchronize()
+            res["learned_cycles"].append(int(st.cycles))
+            res["learned_ms"].append(e0.elapsed_time(e1))
+            res["infer_ms"].append(e0.elapsed_time(e2))
+        lib.artss_field_free(ctx, guess)
+        smp.close()
+        sim.close()
+    return res
+
+
+def _resnorm(lib, ctx, p, b):
+    r, bn = _C.c_double(), _C.c_double()
+    _ck(lib.artss_residual_norm(ctx, p, b, _C.byref(r), _C.byref(bn)), "residual")
+    return r.value, bn.value
