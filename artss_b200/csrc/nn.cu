@@ -147,24 +147,34 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ g, float
     }
 }
 
-// Network input from level-0 arrays of the pressure problem: for inner cell
-// (i, j, k) of the box [x0..x0+W) x [y0..y0+H) x [z0..z0+D):
-//   ch0 = s_rhs * rhs, ch1 = inner flag, ch2 = s_p * p_prev, ch3.. = 0.
-// Cells outside the inner list get zeros in every channel.
-__global__ void k_nn_inputs(const double *__restrict__ rhs, const double *__restrict__ p_prev,
-                            const uint8_t *__restrict__ flags, Level L, int D, int H, int W, double s_rhs, double s_p,
-                            __nv_bfloat16 *__restrict__ out, int C) {
+// Network input from level arrays of the pressure problem A p = rhs, for the
+// inner box [i1..i2] x [j1..j2] x [k1..k2] (x fastest):
+//   ch0 = s_r (rhs - A p_prev)   (the residual of the previous pressure; p_prev
+//                                 must carry its boundary values)
+//   ch1 = inner-cell mask,  ch2 = s_b rhs,  ch3.. = 0;  zeros off the inner list.
+__global__ void k_nn_inputs(const double *__restrict__ rhs, const double *__restrict__ p,
+                            const uint8_t *__restrict__ flags, Level L, int D, int H, int W, double s_r, double s_b,
+                            double rx, double ry, double rz, __nv_bfloat16 *__restrict__ out, int C) {
     const int64_t n = (int64_t) D * H * W;
+    const int64_t nj = L.Nx, nk = L.nxy();
     NN_LOOP(n) {
         const int x = (int) (q % W);
         const int y = (int) ((q / W) % H);
         const int z = (int) (q / ((int64_t) W * H));
-        const int64_t a = (L.i1 + x) + L.Nx * (L.j1 + y) + L.nxy() * (L.k1 + z);
+        const int64_t a = (L.i1 + x) + nj * (L.j1 + y) + nk * (L.k1 + z);
         const bool in = (flags[a] & kInner) != 0;
+        float r = 0.f, bb = 0.f;
+        if (in) {
+            const double c2 = 2 * p[a];
+            const double lap = rx * (p[a - 1] - c2 + p[a + 1]) + ry * (p[a - nj] - c2 + p[a + nj]) +
+                               rz * (p[a - nk] - c2 + p[a + nk]);
+            r = (float) (s_r * (rhs[a] - lap));
+            bb = (float) (s_b * rhs[a]);
+        }
         __nv_bfloat16 *o = out + q * C;
-        o[0] = __float2bfloat16_rn(in ? (float) (s_rhs * rhs[a]) : 0.f);
+        o[0] = __float2bfloat16_rn(r);
         o[1] = __float2bfloat16_rn(in ? 1.f : 0.f);
-        o[2] = __float2bfloat16_rn(in ? (float) (s_p * p_prev[a]) : 0.f);
+        o[2] = __float2bfloat16_rn(bb);
         for (int c = 3; c < C; c++) o[c] = __float2bfloat16_rn(0.f);
     }
 }
@@ -305,15 +315,18 @@ int artss_nn_adam(artss_ctx *ctx, float *w, const float *g, float *m, float *v, 
     return ARTSS_OK;
 }
 
-int artss_nn_inputs(artss_ctx *ctx, int level, const double *rhs, const double *p_prev, double s_rhs, double s_p,
+int artss_nn_inputs(artss_ctx *ctx, int level, const double *rhs, const double *p_prev, double s_r, double s_b,
                     void *out, int C) {
     NN_ARGS_OK(ctx && rhs && p_prev && out && C >= 3);
     int st = check_level(ctx, level);
     if (st) return st;
     const Level &L = ctx->lvl[level];
+    const artss_grid_desc &g = ctx->grid;
     const int W = (int) (L.i2 - L.i1 + 1), H = (int) (L.j2 - L.j1 + 1), D = (int) (L.k2 - L.k1 + 1);
     ARTSS_LAUNCH(ctx, FAM_NN, k_nn_inputs<<<nblk((int64_t) D * H * W), 256, 0, ctx->stream>>>(
-                                 rhs, p_prev, ctx->d_flags[level], L, D, H, W, s_rhs, s_p, (__nv_bfloat16 *) out, C));
+                                 rhs, p_prev, ctx->d_flags[level], L, D, H, W, s_r, s_b,
+                                 1. / (g.dx[level] * g.dx[level]), 1. / (g.dy[level] * g.dy[level]),
+                                 1. / (g.dz[level] * g.dz[level]), (__nv_bfloat16 *) out, C));
     NN_CK(ctx);
     return ARTSS_OK;
 }

@@ -294,7 +294,7 @@ class Sampler:
     equation solved to `rel_tol` from p_prev by the mixed-precision solver.
     Inputs and targets are stored on the device in the network's layout."""
 
-    def __init__(self, sim, dims, rel_tol: float = 1e-8, n_level: int = 4):
+    def __init__(self, sim, dims, h: float, rel_tol: float = 1e-8, n_level: int = 4):
         import torch
         from artss_b200 import MixedCfg, load_cuda
         self.sim, self.ctx, self.lib = sim, sim.context, load_cuda()
@@ -309,6 +309,8 @@ class Sampler:
         self.mx = _C.c_void_p()
         _ck(self.lib.artss_mixed_create(self.ctx, _C.byref(cfg), _C.byref(self.mx)), "mixed")
         self.device = torch.device("cuda", torch.cuda.current_device())
+        ext = min(dims) * h  # shortest domain extent (cell size h, isotropic grid)
+        self.c = ext * ext / (np.pi * np.pi)
 
     def _field(self):
         from artss_b200 import _D
@@ -322,14 +324,20 @@ class Sampler:
         return bn.value
 
     def scales(self, rhs, p_prev):
+        """(s_r, s_b, s_t): inputs scaled to unit RMS (the residual of p_prev and
+        rhs) and the target's scale s_t = s_r / c, where c = L^2 / pi^2 for the
+        shortest domain extent L converts a residual into a correction of the
+        smoothest mode, A^-1 r ~ c r."""
         n = float(self.vox)
-        nr, npv = self.norm(rhs), self.norm(p_prev)
-        s_rhs = np.sqrt(n) / nr if nr > 0 else 1.0
-        s_p = np.sqrt(n) / npv if npv > 0 else s_rhs
-        return s_rhs, s_p
+        r, bn = _C.c_double(), _C.c_double()
+        _ck(self.lib.artss_apply_boundary(self.ctx, p_prev, 0, 4), "bc")
+        _ck(self.lib.artss_residual_norm(self.ctx, p_prev, rhs, _C.byref(r), _C.byref(bn)), "norm")
+        s_r = np.sqrt(n) / r.value if r.value > 0 else 1.0
+        s_b = np.sqrt(n) / bn.value if bn.value > 0 else 1.0
+        return s_r, s_b, s_r / self.c
 
-    def inputs(self, rhs, p_prev, s_rhs, s_p, out):
-        _ck(self.lib.artss_nn_inputs(self.ctx, 0, rhs, p_prev, s_rhs, s_p, _p(out), 16), "inputs")
+    def inputs(self, rhs, p_prev, s_r, s_b, out):
+        _ck(self.lib.artss_nn_inputs(self.ctx, 0, rhs, p_prev, s_r, s_b, _p(out), 16), "inputs")
 
     def solve(self, p, rhs):
         from artss_b200 import SolveStats
@@ -346,11 +354,11 @@ class Sampler:
         self.sim.run(1)
         _ck(self.lib.artss_copy(self.ctx, self.p_star, self.p_prev, 0), "copy")
         st = self.solve(self.p_star, rhs)
-        s_rhs, s_p = self.scales(rhs, self.p_prev)
+        s_r, s_b, s_t = self.scales(rhs, self.p_prev)
         x = torch.empty(self.vox * 16, dtype=torch.bfloat16, device=self.device)
         t = torch.empty(self.vox, dtype=torch.float32, device=self.device)
-        self.inputs(rhs, self.p_prev, s_rhs, s_p, x)
-        _ck(self.lib.artss_nn_target(self.ctx, 0, self.p_star, self.p_prev, s_p, _p(t)), "target")
+        self.inputs(rhs, self.p_prev, s_r, s_b, x)
+        _ck(self.lib.artss_nn_target(self.ctx, 0, self.p_star, self.p_prev, s_t, _p(t)), "target")
         _ck(self.lib.artss_nn_check(self.ctx), "sample")
         return {"x": x, "t": t, "cycles": int(st.cycles), "n_fluid": int(self.sim.inner_cells)}
 
@@ -372,7 +380,7 @@ def collect(seeds, per_scene: int, warmup: int, dims, tmpdir: str, device: int =
         sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
         sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"train_{seed}.xml")), device=device)
         sim.run(warmup)
-        smp = Sampler(sim, dims)
+        smp = Sampler(sim, dims, (sc.X[1] - sc.X[0]) / sc.nx)
         for _ in range(per_scene):
             out.append(smp.sample())
         smp.close()
@@ -407,12 +415,12 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
     import torch
     from artss_b200 import Simulation, SolveStats, _D, scenes
     res = {"baseline_cycles": [], "baseline_ms": [], "learned_cycles": [], "learned_ms": [], "fallbacks": 0,
-           "infer_ms": []}
+           "infer_ms": [], "residual_ratio": []}
     for seed in seeds:
         sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
         sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"eval_{seed}.xml")), device=device)
         sim.run(warmup)
-        smp = Sampler(sim, dims)
+        smp = Sampler(sim, dims, (sc.X[1] - sc.X[0]) / sc.nx)
         lib, ctx = smp.lib, smp.ctx
         stream = torch.cuda.ExternalStream(lib.artss_ctx_stream(ctx))
         guess = smp._field()
@@ -432,15 +440,17 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             res["baseline_cycles"].append(int(st.cycles))
             res["baseline_ms"].append(e0.elapsed_time(e1))
             # (b) from the network's guess
-            s_rhs, s_p = smp.scales(rhs, smp.p_prev)
             e0.record(stream)
-            smp.inputs(rhs, smp.p_prev, s_rhs, s_p, x)
+            s_r, s_b, s_t = smp.scales(rhs, smp.p_prev)
+            smp.inputs(rhs, smp.p_prev, s_r, s_b, x)
             out = net.forward(x)
-            _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.p_prev, 1.0 / s_p, guess), "apply")
+            _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
+            _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.p_prev, 1.0 / s_t, guess), "apply")
             e2 = torch.cuda.Event(enable_timing=True)
             e2.record(stream)
             r_g, _ = _resnorm(lib, ctx, guess, rhs)
             r_p, _ = _resnorm(lib, ctx, smp.p_prev, rhs)
+            res["residual_ratio"].append(r_g / r_p if r_p > 0 else 1.0)
             if r_g > r_p:
                 res["fallbacks"] += 1
                 _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")

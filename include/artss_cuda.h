@@ -343,9 +343,9 @@ int artss_conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, 
  * bias_grad: db[c] += sum_v dy[v][c].  pack_weights: FP32 w[27][co][ci] to the
  * convolution's packed BF16 operand (flip != 0: input-gradient weights).
  * adam: Adam with bias correction (step >= 1).  inputs: network input from
- * level arrays (ch0 = s_rhs rhs, ch1 = inner-cell mask, ch2 = s_p p_prev, the
- * rest 0) over the level's inner box.  apply: p = p_prev + scale * y[.][0] on
- * inner cells.  mse: 0.5 sum over masked voxels (y[.][0] - target)^2 as block
+ * level arrays over the level's inner box: ch0 = s_r (rhs - A p_prev) (p_prev
+ * with its boundary values applied), ch1 = inner-cell mask, ch2 = s_b rhs, the
+ * rest 0.  apply: p = p_prev + scale * y[.][0] on inner cells.  mse: 0.5 sum over masked voxels (y[.][0] - target)^2 as block
  * partials and its gradient (times inv_n) in channel 0 of dy. */
 int artss_nn_zero(artss_ctx *ctx, void *p, int64_t bytes);
 int artss_nn_relu_bwd(artss_ctx *ctx, void *dy, const void *y, int64_t n);
@@ -358,9 +358,11 @@ int artss_nn_bias_grad(artss_ctx *ctx, const void *dy, float *db, int64_t voxels
 int artss_nn_pack_weights(artss_ctx *ctx, const float *w, void *packed, int cout, int cin, int flip);
 int artss_nn_adam(artss_ctx *ctx, float *w, const float *g, float *m, float *v, int64_t n, float lr, float b1,
                   float b2, float eps, int step);
-int artss_nn_inputs(artss_ctx *ctx, int level, const double *rhs, const double *p_prev, double s_rhs, double s_p,
+int artss_nn_inputs(artss_ctx *ctx, int level, const double *rhs, const double *p_prev, double s_r, double s_b,
                     void *out, int C);
 int artss_nn_apply(artss_ctx *ctx, int level, const void *y, int C, const double *p_prev, double scale, double *p);
+/* training target t = scale (p_star - p_prev) over the inner box (FP32, 0 off the inner list) */
+int artss_nn_target(artss_ctx *ctx, int level, const double *p_star, const double *p_prev, double scale, float *t);
 int artss_nn_mse(artss_ctx *ctx, const void *y, int C, const float *target, const void *inputs, void *dy,
                  int64_t voxels, float inv_n, float *partials, int n_partials);
 /* Reads and clears the error flag the network kernels raise when a bounded
