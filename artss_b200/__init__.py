@@ -172,6 +172,7 @@ def load_cuda() -> C.CDLL:
             "artss_nn_inputs": ([_P, C.c_int, _P, _P, C.c_double, C.c_double, _P, C.c_int], C.c_int),
             "artss_nn_apply": ([_P, C.c_int, _P, C.c_int, _P, C.c_double, _P], C.c_int),
             "artss_nn_target": ([_P, C.c_int, _P, _P, C.c_double, _P], C.c_int),
+            "artss_coarse_project": ([_P, _D, C.c_int], C.c_int),
             "artss_nn_mse": ([_P, _P, C.c_int, _P, _P, _P, C.c_int64, C.c_float, _P, C.c_int], C.c_int),
             "artss_cgs_sweep_depth": ([_P, C.c_int], C.c_int),
             "artss_ctx_profile": ([_P, C.c_uint64], C.c_int),

@@ -99,6 +99,7 @@ struct artss_ctx {
     artss::Level lvl[artss::kMaxLevel + 1]{};
     uint8_t *d_flags[artss::kMaxLevel + 1]{};
     int64_t n_inner[artss::kMaxLevel + 1]{};  // inner cells per level (artss_set_cell_lists)
+    double *proj[artss::kMaxLevel + 1]{};     // scratch of artss_coarse_project (lazily, freed with fields)
     artss::BcProgram bc[artss::kMaxLevel + 1][artss::kFieldTypes];
     double *d_partials = nullptr;       // kMaxPartials doubles
     artss::LoopState *d_loop = nullptr; // device loop blocks (16)

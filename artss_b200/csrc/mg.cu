@@ -943,6 +943,37 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
     return ARTSS_OK;
 }
 
+int artss_coarse_project(artss_ctx *ctx, double *d, int levels) {
+    if (!ctx || !d) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (levels < 1 || levels > ctx->grid.n_levels) { set_error("levels out of range"); return ARTSS_ERR_ARG; }
+    int st;
+    double *arr[kMaxLevel + 1] = {d};
+    for (int l = 1; l <= levels; l++) {
+        if (!ctx->proj[l] && (st = artss_field_alloc(ctx, l, &ctx->proj[l]))) return st;
+        arr[l] = ctx->proj[l];
+    }
+    // restrict: coarse inner cell = mean of its 8 children (VCycleMG::Restrict)
+    for (int l = 1; l <= levels; l++) {
+        const Level &C = ctx->lvl[l];
+        const Box3 box = inner_box(C);
+        if ((st = artss_fill(ctx, arr[l], l, 0.0))) return st;
+        ARTSS_LAUNCH(ctx, FAM_MG_RESTRICT, k_mg_restrict<<<mg_grid(box), box_block(), 0, ctx->stream>>>(
+                                               arr[l], arr[l - 1], ctx->d_flags[l], C, ctx->lvl[l - 1], box));
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    // prolongate back (VCycleMG::Prolongate), the coarse level's boundary values first
+    for (int l = levels; l >= 1; l--) {
+        if ((st = apply_bc(ctx, arr[l], l, ARTSS_FIELD_P))) return st;
+        if ((st = artss_fill(ctx, arr[l - 1], l - 1, 0.0))) return st;
+        const Level &C = ctx->lvl[l];
+        const Box3 box = inner_box(C);
+        ARTSS_LAUNCH(ctx, FAM_MG_PROLONGATE, k_mg_prolongate<<<mg_grid(box), box_block(), 0, ctx->stream>>>(
+                                                 arr[l - 1], arr[l], ctx->d_flags[l], C, ctx->lvl[l - 1], box));
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    return ARTSS_OK;
+}
+
 int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_tol, int64_t max_cycles,
                        artss_solve_stats *stats) {
     if (!mg || !p || !rhs) { set_error("null argument"); return ARTSS_ERR_ARG; }

@@ -106,6 +106,32 @@ void VCycleMG::pressure(Field &out, const Field &b, real t, bool) {
     last_residual = st.residual;
 }
 
+// ---------------------------------------------------------------- VCycleMGMixed
+
+MixedVCycle::MixedVCycle(Runtime &rt, const settings::Pressure &s) : m_rt(rt) {
+    artss_mixed_cfg c{};
+    c.n_level = (int32_t) s.n_level;
+    c.n_relax = (int32_t) s.n_relax;
+    c.coarse_smoother = ARTSS_SMOOTHER_CGS;
+    c.flags = 0;
+    c.w = s.smoother.w;
+    c.coarse_w = 0.0;  // red-black SOR, optimal weight of the model problem
+    c.coarse_rel_tol = 1e-3;
+    c.coarse_max_iter = 40;
+    c.rel_tol = s.tol_res;
+    c.max_cycles = (int64_t) s.max_cycle;
+    check(artss_mixed_create(rt.ctx(), &c, &m_mx), "VCycleMGMixed");
+}
+
+MixedVCycle::~MixedVCycle() { artss_mixed_destroy(m_mx); }
+
+void MixedVCycle::pressure(Field &out, const Field &b, real, bool) {
+    artss_solve_stats st{};
+    check(artss_mixed_solve(m_mx, out.data, b.data, &st), "VCycleMGMixed::pressure");
+    last_cycles = st.cycles;
+    last_residual = st.residual;
+}
+
 // ---------------------------------------------------------------- turbulence / sources
 
 void ConstSmagorinsky::calc_turbulent_viscosity(Field &ev, const Field &in_u, const Field &in_v, const Field &in_w,

@@ -125,6 +125,20 @@ class VCycleMG : public IPressure {
     artss_mg *m_mg = nullptr;
 };
 
+// Mixed-precision pressure solve (no reference counterpart; artss_mixed_*):
+// every call iterates FP32 V-cycles inside FP64 defect correction from the
+// current pressure until ||b - A p|| <= tol_res ||b|| or max_cycle cycles.
+class MixedVCycle : public IPressure {
+ public:
+    MixedVCycle(Runtime &rt, const settings::Pressure &s);
+    ~MixedVCycle() override;
+    void pressure(Field &out, const Field &b, real t, bool sync) override;
+
+ private:
+    Runtime &m_rt;
+    artss_mixed *m_mx = nullptr;
+};
+
 class ConstSmagorinsky : public ITurbulence {
  public:
     ConstSmagorinsky(Runtime &rt, real cs) : m_rt(rt), m_cs(cs) {}

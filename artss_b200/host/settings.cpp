@@ -243,7 +243,10 @@ Pressure parse_pressure(const XmlElement *head, const std::string &parent) {
     Pressure p;
     p.type = req_str(s.values, "type", context);
     p.field = match_field(req_str(s.values, "field", context));
-    if (p.type != "VCycleMG") throw config_error("pressure solver '" + p.type + "' has no parsing implementation.");
+    // VCycleMGMixed (no reference counterpart) reads the same keys; tol_res is
+    // its relative tolerance and max_cycle its cycle limit per solve
+    if (p.type != "VCycleMG" && p.type != "VCycleMGMixed")
+        throw config_error("pressure solver '" + p.type + "' has no parsing implementation.");
     const std::string c2 = ctx_join(context, "vcycle");
     p.n_level = req_size(s.values, "n_level", c2);
     p.n_cycle = req_size(s.values, "n_cycle", c2);

@@ -25,6 +25,7 @@ std::unique_ptr<ITurbulence> make_turbulence(Runtime &rt, const settings::Turbul
 
 std::unique_ptr<IPressure> make_pressure(Runtime &rt, const settings::Pressure &s) {
     if (s.type == "VCycleMG") return std::make_unique<VCycleMG>(rt, s);
+    if (s.type == "VCycleMGMixed") return std::make_unique<MixedVCycle>(rt, s);
     throw config_error("pressure method '" + s.type + "' is not implemented");
 }
 

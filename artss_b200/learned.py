@@ -405,11 +405,12 @@ def train(net: UNet, samples, epochs: int, lr: float = 1e-3, seed: int = 0):
     return history
 
 
-def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0):
+def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0, project: int = 2):
     """Per timestep of unseen scenes: the pressure equation solved to 1e-8 by
     the mixed-precision solver from (a) the previous pressure and (b) the
-    network's guess p_prev + correction, falling back to (a) when the guess's
-    initial residual is larger.  Returns cycles and ms (CUDA events on the
+    network's guess p_prev + correction, the correction restricted `project`
+    times and prolongated back (its smooth part; artss_coarse_project),
+    falling back to (a) when the guess's initial residual is larger.  Returns cycles and ms (CUDA events on the
     context stream; (b) includes the network's inference)."""
     import os
     import torch
@@ -423,7 +424,7 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
         smp = Sampler(sim, dims, (sc.X[1] - sc.X[0]) / sc.nx)
         lib, ctx = smp.lib, smp.ctx
         stream = torch.cuda.ExternalStream(lib.artss_ctx_stream(ctx))
-        guess = smp._field()
+        guess, corr = smp._field(), smp._field()
         x = torch.empty(smp.vox * 16, dtype=torch.bfloat16, device=smp.device)
         for _ in range(steps):
             p = _C.cast(_C.c_void_p(sim.device_pointer("p")), _D)
@@ -444,8 +445,15 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             s_r, s_b, s_t = smp.scales(rhs, smp.p_prev)
             smp.inputs(rhs, smp.p_prev, s_r, s_b, x)
             out = net.forward(x)
+            # correction = the network's output, kept to the coarse space of
+            # `project` levels (its smooth part), added to p_prev
+            _ck(lib.artss_fill(ctx, corr, 0, 0.0), "fill")
+            _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.zero, 1.0 / s_t, corr), "apply")
+            if project:
+                _ck(lib.artss_coarse_project(ctx, corr, project), "project")
             _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
-            _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.p_prev, 1.0 / s_t, guess), "apply")
+            _ck(lib.artss_add_field(ctx, guess, corr, 0), "add")
+            _ck(lib.artss_apply_boundary(ctx, guess, 0, 4), "bc")
             e2 = torch.cuda.Event(enable_timing=True)
             e2.record(stream)
             r_g, _ = _resnorm(lib, ctx, guess, rhs)
@@ -461,6 +469,7 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             res["learned_ms"].append(e0.elapsed_time(e1))
             res["infer_ms"].append(e0.elapsed_time(e2))
         lib.artss_field_free(ctx, guess)
+        lib.artss_field_free(ctx, corr)
         smp.close()
         sim.close()
     return res

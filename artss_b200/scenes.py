@@ -76,6 +76,7 @@ class Scene:
     obstacles: List[Box] = field(default_factory=list)
     obstacle_bcs: List[Tuple[str, str, str, float]] = field(default_factory=list)
     ic: str = "Uniform"
+    pressure: str = "VCycleMG"  # or "VCycleMGMixed" (mixed-precision solve to mg_tol, relative)
 
     @property
     def t_end(self) -> float:
@@ -237,6 +238,29 @@ def poisson_rhs(inner, size: int, seed: int):
     return b
 
 
+def plume_ensemble(count: int = 64, seed: int = 0, steps: int = 100, sizes=(32, 48, 64, 96, 128)) -> List[Scene]:
+    """The ensemble workload: `count` closed plume boxes whose cell counts per
+    axis are drawn from `sizes`, 0.0375 m cells, heat release U[10, 150] kW
+    centred at U[0.2, 0.8] of the extent (0.3 of the height), 0-3 box
+    obstacles, dt 0.005 s, the mixed-precision pressure solve to 1e-8
+    relative or 20 cycles per step."""
+    rng = random.Random(seed)
+    out = []
+    h = 0.0375
+    for n in range(count):
+        nx, ny, nz = (rng.choice(sizes) for _ in range(3))
+        ext = (nx * h, ny * h, nz * h)
+        sc = Scene(nx=nx, ny=ny, nz=nz, X=(0.0, ext[0]), Y=(0.0, ext[1]), Z=(0.0, ext[2]), dt=0.005, steps=steps,
+                   n_level=3, boundaries=closed_box_bcs(), hrr=rng.uniform(10.0, 150.0),
+                   source_pos=(rng.uniform(0.2, 0.8) * ext[0], rng.uniform(0.2, 0.8) * ext[1], 0.3 * ext[2]),
+                   seed=rng.randint(0, 10 ** 6), pressure="VCycleMGMixed", max_cycle=20)
+        sc.obstacles = random_boxes((nx, ny, nz), 4, 12, rng.randint(0, 3), rng.randint(0, 10 ** 6), (h, h, h),
+                                    levels=2)
+        sc.obstacle_bcs = solid_obstacle_bcs()
+        out.append(sc)
+    return out
+
+
 def to_xml(s: Scene) -> str:
     L = []
     a = L.append
@@ -271,7 +295,7 @@ def to_xml(s: Scene) -> str:
         a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
         a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
         a("    </source>")
-    a('    <pressure type="VCycleMG" field="p">')
+    a(f'    <pressure type="{s.pressure}" field="p">')
     a(f"      <n_level> {s.n_level} </n_level>")
     a(f"      <n_cycle> {s.n_cycle} </n_cycle>")
     a(f"      <max_cycle> {s.max_cycle} </max_cycle>")

@@ -365,6 +365,12 @@ int artss_nn_apply(artss_ctx *ctx, int level, const void *y, int C, const double
 int artss_nn_target(artss_ctx *ctx, int level, const double *p_star, const double *p_prev, double scale, float *t);
 int artss_nn_mse(artss_ctx *ctx, const void *y, int C, const float *target, const void *inputs, void *dy,
                  int64_t voxels, float inv_n, float *partials, int n_partials);
+/* d <- P^k R^k d for a level-0 correction d: restricted `levels` times with
+ * the multigrid restriction and prolongated back with its trilinear
+ * prolongation, which keeps only what the coarse level represents (the
+ * smooth part); cells outside the prolongation's reach become 0.  Uses
+ * context-owned scratch arrays, allocated on first use. */
+int artss_coarse_project(artss_ctx *ctx, double *d, int levels);
 /* Reads and clears the error flag the network kernels raise when a bounded
  * wait gives up (returns ARTSS_ERR_CUDA then); synchronizes the stream. */
 int artss_nn_check(artss_ctx *ctx);
