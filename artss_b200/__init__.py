@@ -306,9 +306,13 @@ class Simulation:
         self.size = int(self._lib.artss_sim_field_size(self._h))
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
-            self._lib.artss_sim_destroy(self._h)
-            self._h = _P()
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h:
+            try:
+                self._lib.artss_sim_destroy(h)
+            except TypeError:  # interpreter shutdown: ctypes objects already torn down
+                pass
 
     __del__ = close
 

@@ -229,8 +229,10 @@ int mg_resnorm(artss_mg *mg, const double *x, const double *b, int level, int sl
 // VCycleMG::Smooth + call_smooth_{jacobi,colored_gauss_seidel} (VCycleMG.cpp:299-305, :583-723)
 int mg_smooth(artss_mg *mg, double *out, double *tmp, const double *b, int level) {
     int st;
-    if ((st = mg_bc(mg, out, level))) return st;   // Smooth
-    if ((st = mg_bc(mg, out, level))) return st;   // call_smooth_*
+    // VCycleMG::Smooth and call_smooth_* each apply the boundary program first;
+    // the program is idempotent (ghost values are functions of inner values it
+    // does not write), so one application gives the same array
+    if ((st = mg_bc(mg, out, level))) return st;
     if (mg->cfg.smoother == ARTSS_SMOOTHER_CGS) {
         for (int r = 0; r < mg->cfg.n_relax; r++) {
             if ((st = mg_cgs_step(mg, out, b, level))) return st;
@@ -579,14 +581,18 @@ k_mg_coarse_cluster(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__rest
 }
 
 // Launch shape of the cluster coarse solve, or false when the level does not fit it.
+// ranks of the cluster for a level: one per z-plane up to kClusterSize
+inline int cluster_ranks(const Level &L) { return (int) std::min<int64_t>(kClusterSize, L.Nz); }
+
 bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int64_t *smem) {
     const Level &L = ctx->lvl[level];
     const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
     if (p.present && p.waves > kCoarseMaxWaves) return false;
-    if (L.Nz < kClusterSize || L.Nz > kClusterMaxPlanes || L.size() > (int64_t) 1 << 24) return false;
+    const int cs = cluster_ranks(L);
+    if (cs < 2 || L.Nz > kClusterMaxPlanes || L.size() > (int64_t) 1 << 24) return false;
     int cap = 0;
-    for (int r = 0; r < kClusterSize; r++) {
-        const int64_t a = (int64_t) r * L.Nz / kClusterSize, e = (int64_t) (r + 1) * L.Nz / kClusterSize;
+    for (int r = 0; r < cs; r++) {
+        const int64_t a = (int64_t) r * L.Nz / cs, e = (int64_t) (r + 1) * L.Nz / cs;
         cap = std::max<int>(cap, (int) (e - a));
         // inner cells of the rank's planes, one thread each per register slot
         const int64_t z0 = std::max<int64_t>(a, L.k1), z1 = std::min<int64_t>(e - 1, L.k2);
@@ -611,14 +617,15 @@ int launch_coarse_cluster(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int lev
         attr_set = true;
     }
     const Level &L = ctx->lvl[level];
+    const int cs = cluster_ranks(L);
     cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(kClusterSize, 1, 1);
+    lc.gridDim = dim3(cs, 1, 1);
     lc.blockDim = dim3(kClusterThreads, 1, 1);
     lc.dynamicSmemBytes = (size_t) smem;
     lc.stream = ctx->stream;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kClusterSize;
+    at[0].val.clusterDim.x = cs;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     lc.attrs = at;
@@ -821,7 +828,9 @@ int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its) {
         if ((st = mg_residuum(mg, mg->r0[l], mg->e1[l], mg->r1[l], l))) return st;
         if ((st = mg_bc(mg, mg->r0[l], l))) return st;
         if ((st = mg_restrict(mg, mg->r1[l + 1], mg->r0[l], l + 1))) return st;
-        if ((st = mg_bc(mg, mg->r1[l + 1], l + 1))) return st;
+        // the reference also applies the boundary program to the restricted
+        // residual; nothing reads r1's boundary cells (it is only a right-hand
+        // side, read on inner cells), so that launch is left out
         if ((st = artss_fill(ctx, mg->e1[l + 1], l + 1, 0.0))) return st;
     }
     // out.copy_data(*m_error0[0]) at VCycleMG.cpp:254 is overwritten below

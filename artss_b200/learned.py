@@ -294,7 +294,7 @@ class Sampler:
     equation solved to `rel_tol` from p_prev by the mixed-precision solver.
     Inputs and targets are stored on the device in the network's layout."""
 
-    def __init__(self, sim, dims, h: float, rel_tol: float = 1e-8, n_level: int = 4):
+    def __init__(self, sim, dims, h: float, rel_tol: float = 1e-8, n_level: int = 4, project: int = 0):
         import torch
         from artss_b200 import MixedCfg, load_cuda
         self.sim, self.ctx, self.lib = sim, sim.context, load_cuda()
@@ -304,6 +304,8 @@ class Sampler:
         self.p_prev = self._field()
         self.p_star = self._field()
         self.zero = self._field()
+        self.diff = self._field()
+        self.project = project
         _ck(self.lib.artss_fill(self.ctx, self.zero, 0, 0.0), "fill")
         cfg = MixedCfg(n_level, 2, 1, 0, 0.6666666667, 0.0, 1e-3, 40, rel_tol, 200)
         self.mx = _C.c_void_p()
@@ -358,7 +360,14 @@ class Sampler:
         x = torch.empty(self.vox * 16, dtype=torch.bfloat16, device=self.device)
         t = torch.empty(self.vox, dtype=torch.float32, device=self.device)
         self.inputs(rhs, self.p_prev, s_r, s_b, x)
-        _ck(self.lib.artss_nn_target(self.ctx, 0, self.p_star, self.p_prev, s_t, _p(t)), "target")
+        if self.project:
+            # target = the smooth part of p_star - p_prev (artss_coarse_project)
+            _ck(self.lib.artss_scale_copy(self.ctx, self.diff, self.p_prev, -1.0, 0), "neg")
+            _ck(self.lib.artss_add_field(self.ctx, self.diff, self.p_star, 0), "diff")
+            _ck(self.lib.artss_coarse_project(self.ctx, self.diff, self.project), "project")
+            _ck(self.lib.artss_nn_target(self.ctx, 0, self.diff, self.zero, s_t, _p(t)), "target")
+        else:
+            _ck(self.lib.artss_nn_target(self.ctx, 0, self.p_star, self.p_prev, s_t, _p(t)), "target")
         _ck(self.lib.artss_nn_check(self.ctx), "sample")
         return {"x": x, "t": t, "cycles": int(st.cycles), "n_fluid": int(self.sim.inner_cells)}
 
@@ -366,11 +375,11 @@ class Sampler:
         if self.mx:
             self.lib.artss_mixed_destroy(self.mx)
             self.mx = _C.c_void_p()
-        for f in (self.p_prev, self.p_star, self.zero):
+        for f in (self.p_prev, self.p_star, self.zero, self.diff):
             self.lib.artss_field_free(self.ctx, f)
 
 
-def collect(seeds, per_scene: int, warmup: int, dims, tmpdir: str, device: int = 0):
+def collect(seeds, per_scene: int, warmup: int, dims, tmpdir: str, device: int = 0, project: int = 0):
     """Training samples from the plain solver: per seeded scene, `warmup`
     timesteps, then `per_scene` sampled timesteps (see Sampler)."""
     import os
@@ -380,7 +389,7 @@ def collect(seeds, per_scene: int, warmup: int, dims, tmpdir: str, device: int =
         sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
         sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"train_{seed}.xml")), device=device)
         sim.run(warmup)
-        smp = Sampler(sim, dims, (sc.X[1] - sc.X[0]) / sc.nx)
+        smp = Sampler(sim, dims, (sc.X[1] - sc.X[0]) / sc.nx, project=project)
         for _ in range(per_scene):
             out.append(smp.sample())
         smp.close()

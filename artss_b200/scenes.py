@@ -251,11 +251,11 @@ def plume_ensemble(count: int = 64, seed: int = 0, steps: int = 100, sizes=(32, 
         nx, ny, nz = (rng.choice(sizes) for _ in range(3))
         ext = (nx * h, ny * h, nz * h)
         sc = Scene(nx=nx, ny=ny, nz=nz, X=(0.0, ext[0]), Y=(0.0, ext[1]), Z=(0.0, ext[2]), dt=0.005, steps=steps,
-                   n_level=3, boundaries=closed_box_bcs(), hrr=rng.uniform(10.0, 150.0),
+                   n_level=4, boundaries=closed_box_bcs(), hrr=rng.uniform(10.0, 150.0),
                    source_pos=(rng.uniform(0.2, 0.8) * ext[0], rng.uniform(0.2, 0.8) * ext[1], 0.3 * ext[2]),
                    seed=rng.randint(0, 10 ** 6), pressure="VCycleMGMixed", max_cycle=20)
-        sc.obstacles = random_boxes((nx, ny, nz), 4, 12, rng.randint(0, 3), rng.randint(0, 10 ** 6), (h, h, h),
-                                    levels=2)
+        sc.obstacles = random_boxes((nx, ny, nz), 8, 16, rng.randint(0, 3), rng.randint(0, 10 ** 6), (h, h, h),
+                                    levels=3)
         sc.obstacle_bcs = solid_obstacle_bcs()
         out.append(sc)
     return out

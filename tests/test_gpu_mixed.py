@@ -76,9 +76,10 @@ def solve_pair(sc, seed, mixed_flags, rel_tol=1e-8):
         ctx.close()
 
 
-@pytest.mark.parametrize("seed", [0, 1, 2])
-def test_mixed_neumann_boxes(seed):
-    sc = scenes.poisson_boxes(n=32, seed=seed, n_level=3)
+@pytest.mark.parametrize("seed,n_level", [(0, 3), (1, 3), (2, 3), (3, 4)])
+def test_mixed_neumann_boxes(seed, n_level):
+    """n_level 4 puts the coarse solve on a 4^3 level: a cluster of 6 blocks."""
+    sc = scenes.poisson_boxes(n=32, seed=seed, n_level=n_level)
     geom, osc, b, inner, p, p2, p_ref, st, st2, ref = solve_pair(sc, seed, A.MIXED_REMOVE_MEAN)
     assert 0 < st.cycles < 200 and st.rel_residual <= 1e-8
     assert st2.cycles == st.cycles and np.array_equal(p, p2)
