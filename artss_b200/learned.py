@@ -311,6 +311,7 @@ class Sampler:
         self.mx = _C.c_void_p()
         _ck(self.lib.artss_mixed_create(self.ctx, _C.byref(cfg), _C.byref(self.mx)), "mixed")
         self.device = torch.device("cuda", torch.cuda.current_device())
+        self.rel_tol = rel_tol
         ext = min(dims) * h  # shortest domain extent (cell size h, isotropic grid)
         self.c = ext * ext / (np.pi * np.pi)
 
@@ -414,18 +415,21 @@ def train(net: UNet, samples, epochs: int, lr: float = 1e-3, seed: int = 0):
     return history
 
 
-def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0, project: int = 2):
+def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0, project: int = 2,
+             with_plain: bool = False):
     """Per timestep of unseen scenes: the pressure equation solved to 1e-8 by
     the mixed-precision solver from (a) the previous pressure and (b) the
     network's guess p_prev + correction, the correction restricted `project`
     times and prolongated back (its smooth part; artss_coarse_project),
-    falling back to (a) when the guess's initial residual is larger.  Returns cycles and ms (CUDA events on the
-    context stream; (b) includes the network's inference)."""
+    falling back to (a) when the guess's initial residual is larger, and, with
+    `with_plain`, (c) the plain FP64 VCycleMG from the previous pressure.
+    Returns cycles and ms (CUDA events on the context stream; (b) includes the
+    network's inference)."""
     import os
     import torch
     from artss_b200 import Simulation, SolveStats, _D, scenes
     res = {"baseline_cycles": [], "baseline_ms": [], "learned_cycles": [], "learned_ms": [], "fallbacks": 0,
-           "infer_ms": [], "residual_ratio": []}
+           "infer_ms": [], "residual_ratio": [], "plain_cycles": [], "plain_ms": []}
     for seed in seeds:
         sc = plume_channel(seed, nx=dims[2], ny=dims[1], nz=dims[0])
         sim = Simulation(scenes.write(sc, os.path.join(tmpdir, f"eval_{seed}.xml")), device=device)
@@ -434,6 +438,12 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
         lib, ctx = smp.lib, smp.ctx
         stream = torch.cuda.ExternalStream(lib.artss_ctx_stream(ctx))
         guess, corr = smp._field(), smp._field()
+        plain = None
+        if with_plain:
+            from artss_b200 import MgCfg
+            mc = MgCfg(sc.n_level, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
+            plain = _C.c_void_p()
+            _ck(lib.artss_mg_create(ctx, _C.byref(mc), _C.byref(plain)), "plain")
         x = torch.empty(smp.vox * 16, dtype=torch.bfloat16, device=smp.device)
         for _ in range(steps):
             p = _C.cast(_C.c_void_p(sim.device_pointer("p")), _D)
@@ -449,6 +459,16 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             e1.synchronize()
             res["baseline_cycles"].append(int(st.cycles))
             res["baseline_ms"].append(e0.elapsed_time(e1))
+            # (c) the plain FP64 VCycleMG from the previous pressure
+            if plain is not None:
+                _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
+                pst = SolveStats()
+                e0.record(stream)
+                _ck(lib.artss_mg_solve_rel(plain, guess, rhs, smp.rel_tol, 1000, _C.byref(pst)), "plain")
+                e1.record(stream)
+                e1.synchronize()
+                res["plain_cycles"].append(int(pst.cycles))
+                res["plain_ms"].append(e0.elapsed_time(e1))
             # (b) from the network's guess
             e0.record(stream)
             s_r, s_b, s_t = smp.scales(rhs, smp.p_prev)
@@ -477,6 +497,8 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             res["learned_cycles"].append(int(st.cycles))
             res["learned_ms"].append(e0.elapsed_time(e1))
             res["infer_ms"].append(e0.elapsed_time(e2))
+        if plain is not None:
+            lib.artss_mg_destroy(plain)
         lib.artss_field_free(ctx, guess)
         lib.artss_field_free(ctx, corr)
         smp.close()

@@ -40,7 +40,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["channel", "box", "poisson", "ensemble"], default="channel",
+    ap.add_argument("--workload", choices=["channel", "box", "poisson", "ensemble", "learned"], default="channel",
                     help="poisson: ms per pressure solve to a 1e-8 relative residual, plain FP64 VCycleMG "
                          "against the mixed-precision solve, on the 256^3 Neumann problem with box obstacles")
     ap.add_argument("--poisson-n", type=int, default=256)
@@ -469,6 +469,63 @@ def run_ensemble(args, dist):
     }
 
 
+def run_learned(args, dist):
+    """ms per pressure solve to a 1e-8 relative residual inside time stepping
+    (128x64x64 channel scenes of the ensemble family with 0-3 boxes): plain
+    FP64 VCycleMG vs mixed precision vs learned guess + mixed precision, all
+    from the previous step's pressure.  The network is trained first on
+    samples the solver generates from other seeds (bounded budget, untimed)."""
+    import numpy as np
+    import torch
+
+    from artss_b200 import learned as LN
+    from artss_b200 import scenes
+
+    torch.cuda.set_device(dist.local)
+    dims = (64, 64, 128)
+    tmp = tempfile.mkdtemp(prefix="artss_learned_")
+    t0 = time.time()
+    samples = LN.collect(range(100, 116), 16, 20, dims, tmp, device=dist.local, project=2)
+    t1 = time.time()
+    sc = LN.plume_channel(0, nx=dims[2], ny=dims[1], nz=dims[0])
+    import artss_b200 as A
+    sim = A.Simulation(scenes.write(sc, os.path.join(tmp, "net.xml")), device=dist.local)
+    net = LN.UNet(sim.context, dims, seed=0)
+    hist = LN.train(net, samples, epochs=4, lr=1e-3)
+    t2 = time.time()
+    res = LN.evaluate(net, [900 + 10 * dist.rank + k for k in range(2)], max(args.steps, 1), 20, dims, tmp,
+                      device=dist.local, project=2, with_plain=True)
+    sim.close()
+    m = lambda k: float(np.mean(res[k]))  # noqa: E731
+    learned_ms = dist.max(m("learned_ms"))
+    return {
+        "metric": "ms per pressure solve to 1e-8: learned vs plain MG",
+        "value": learned_ms,
+        "unit": "ms",
+        "n_gpus": dist.world,
+        "steps": len(res["learned_ms"]),
+        "warmup": 20,
+        "ms_per_step": learned_ms,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16 network (fp32 accumulation); f32 V-cycles in f64 defect correction",
+        "data": "synthetic",
+        "config": {"workload": "learned_guess_channel_128x64x64", "train_samples": len(samples), "epochs": 4,
+                   "network": "3-level U-Net 16-32-64, 3x3x3 tcgen05 convolutions",
+                   "guess": "p_prev + coarse-projected (2 levels) network correction, fallback to p_prev "
+                            "when its initial residual is larger"},
+        "plain_fp64": {"ms_per_solve": m("plain_ms"), "cycles": m("plain_cycles")},
+        "mixed_from_p_prev": {"ms_per_solve": m("baseline_ms"), "cycles": m("baseline_cycles")},
+        "learned_plus_mixed": {"ms_per_solve": m("learned_ms"), "cycles": m("learned_cycles"),
+                               "inference_ms": m("infer_ms"), "fallbacks": res["fallbacks"],
+                               "guess_residual_over_p_prev_residual": m("residual_ratio")},
+        "speedup_vs_plain_fp64": m("plain_ms") / m("learned_ms"),
+        "training": {"collect_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1),
+                     "loss_per_epoch": [round(h, 4) for h in hist]},
+    }
+
+
 def cpu_baseline(args, inner):
     """The reference serial build (oracle/_ref) on a bounded sample of the same
     workload: the first steps of the same scene, steady-state steps timed."""
@@ -532,8 +589,8 @@ def main():
             if dist.rank == 0:
                 print(json.dumps(run_reference(args, dist)), flush=True)
             return
-        if args.workload in ("poisson", "ensemble"):
-            out = run_poisson(args, dist) if args.workload == "poisson" else run_ensemble(args, dist)
+        if args.workload in ("poisson", "ensemble", "learned"):
+            out = {"poisson": run_poisson, "ensemble": run_ensemble, "learned": run_learned}[args.workload](args, dist)
             if dist.rank == 0:
                 print(json.dumps(out), flush=True)
             return
