@@ -438,6 +438,11 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
         lib, ctx = smp.lib, smp.ctx
         stream = torch.cuda.ExternalStream(lib.artss_ctx_stream(ctx))
         guess, corr = smp._field(), smp._field()
+        # L2 flush between timed solves: a buffer twice the 126 MB L2, zeroed on the stream
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=smp.device)
+
+        def flush_l2():
+            _ck(lib.artss_nn_zero(ctx, _p(flush), flush.numel()), "flush")
         plain = None
         if with_plain:
             from artss_b200 import MgCfg
@@ -453,6 +458,7 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             # (a) from the previous pressure
             _ck(lib.artss_copy(ctx, smp.p_star, smp.p_prev, 0), "copy")
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush_l2()
             e0.record(stream)
             st = smp.solve(smp.p_star, rhs)
             e1.record(stream)
@@ -463,6 +469,7 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             if plain is not None:
                 _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
                 pst = SolveStats()
+                flush_l2()
                 e0.record(stream)
                 _ck(lib.artss_mg_solve_rel(plain, guess, rhs, smp.rel_tol, 1000, _C.byref(pst)), "plain")
                 e1.record(stream)
@@ -470,6 +477,7 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
                 res["plain_cycles"].append(int(pst.cycles))
                 res["plain_ms"].append(e0.elapsed_time(e1))
             # (b) from the network's guess
+            flush_l2()
             e0.record(stream)
             s_r, s_b, s_t = smp.scales(rhs, smp.p_prev)
             smp.inputs(rhs, smp.p_prev, s_r, s_b, x)
