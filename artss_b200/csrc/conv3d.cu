@@ -117,8 +117,12 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
             }
             if (!ok) s_fail = 1;
         }
-        // epilogue: lane = voxel of the tile, columns = output channels
-        bool acc_ok = tc::mbar_wait(&accb, (unsigned) (it & 1), kConvPolls);
+        // epilogue: lane = voxel of the tile, columns = output channels.  Only
+        // the issuing thread polls the accumulator barrier; the others wait at
+        // the block barrier (polling threads of its own warp would compete with
+        // it for the warp's issue slots)
+        bool acc_ok = true;
+        if (tid == 0) acc_ok = ok && tc::mbar_wait(&accb, (unsigned) (it & 1), kConvPolls);
         if (__syncthreads_or(!acc_ok || s_fail)) {
             if (tid == 0 && err) atomicExch(err, 1);
             break;
@@ -233,7 +237,8 @@ k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__
             }
             if (!ok) s_fail = 1;
         }
-        bool acc_ok = tc::mbar_wait(&accb, (unsigned) (tap & 1), kConvPolls);
+        bool acc_ok = true;
+        if (tid == 0) acc_ok = ok && tc::mbar_wait(&accb, (unsigned) (tap & 1), kConvPolls);
         if (__syncthreads_or(!acc_ok || s_fail)) {
             if (tid == 0 && err) atomicExch(err, 1);
             break;

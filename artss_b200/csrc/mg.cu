@@ -23,6 +23,15 @@ struct artss_mg {
     double *e0[artss::kMaxLevel + 1]{};   // error0[level]      (levels 0..L-1)
     double *e1[artss::kMaxLevel + 1]{};   // error1[level]      (levels 0..L)
     double *tmp[artss::kMaxLevel + 1]{};  // temporal solution  (levels 0..L)
+    // CUDA graphs of the fixed launch sequence of a later-step pressure call
+    // (set_rhs + n_cycle V-cycles), one per (p, rhs) pair
+    struct Graph {
+        const double *p, *rhs;
+        cudaGraphExec_t exec;
+        int64_t launches, fam[artss::FAM_COUNT];
+    };
+    std::vector<Graph> graphs;
+    bool use_graphs = true;
 };
 
 namespace artss {
@@ -890,6 +899,7 @@ int artss_mg_create(artss_ctx *ctx, const artss_mg_cfg *cfg, artss_mg **out) {
 
 int artss_mg_destroy(artss_mg *mg) {
     if (!mg) return ARTSS_OK;
+    for (auto &g : mg->graphs) cudaGraphExecDestroy(g.exec);
     for (int l = 0; l <= kMaxLevel; l++) {
         for (double *p : {mg->r0[l], mg->r1[l], mg->e0[l], mg->e1[l], mg->tmp[l]})
             if (p) artss_field_free(mg->ctx, p);
@@ -912,13 +922,54 @@ int artss_mg_vcycle(artss_mg *mg, double *p) {
     return mg_vcycle(mg, p, nullptr);
 }
 
+// kernel families a V-cycle launches: event profiling of any of them needs eager launches
+constexpr uint64_t kMgFamilies = (1ull << FAM_FIELD_OP) | (1ull << FAM_BC) | (1ull << FAM_MG_JACOBI) |
+                                 (1ull << FAM_MG_CGS) | (1ull << FAM_MG_RESIDUUM) | (1ull << FAM_MG_RESTRICT) |
+                                 (1ull << FAM_MG_PROLONGATE) | (1ull << FAM_MG_COARSE) | (1ull << FAM_REDUCE);
+
+// Captures set_rhs + n_cycle V-cycles for (p, rhs) into a graph of mg->graphs
+// (at most 8 are kept; the oldest is dropped).
+static int mg_capture(artss_mg *mg, double *p, const double *rhs) {
+    artss_ctx *ctx = mg->ctx;
+    const int64_t l0 = ctx->launches;
+    int64_t f0[FAM_COUNT];
+    for (int f = 0; f < FAM_COUNT; f++) f0[f] = ctx->prof.launches[f];
+    ARTSS_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int st = artss_mg_set_rhs(mg, p, rhs);
+    int64_t coarse = 0;
+    for (int c = 0; c < mg->cfg.n_cycle && !st; c++) st = mg_vcycle(mg, p, &coarse);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+    if (st) { if (graph) cudaGraphDestroy(graph); return st; }
+    if (ec != cudaSuccess) return cuda_fail(ec, "V-cycle capture");
+    artss_mg::Graph g{};
+    g.p = p;
+    g.rhs = rhs;
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return cuda_fail(ei, "V-cycle graph");
+    // the capture only recorded the launches: count them per replay instead
+    g.launches = ctx->launches - l0;
+    ctx->launches = l0;
+    for (int f = 0; f < FAM_COUNT; f++) {
+        g.fam[f] = ctx->prof.launches[f] - f0[f];
+        ctx->prof.launches[f] = f0[f];
+    }
+    if (mg->graphs.size() >= 8) {
+        cudaGraphExecDestroy(mg->graphs.front().exec);
+        mg->graphs.erase(mg->graphs.begin());
+    }
+    mg->graphs.push_back(g);
+    return ARTSS_OK;
+}
+
 int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step, artss_mg_stats *stats) {
     if (!mg || !p || !rhs) { set_error("null argument"); return ARTSS_ERR_ARG; }
     int st;
-    if ((st = artss_mg_set_rhs(mg, p, rhs))) return st;
     int64_t cycles = 0, coarse = 0;
     double residual = -1.0;
     if (first_step) {
+        if ((st = artss_mg_set_rhs(mg, p, rhs))) return st;
         // VCycleMG.cpp:150-197
         const long long max_cycles = mg->cfg.max_cycle;
         const long long max_relaxs = mg->cfg.smoother_max_iter;
@@ -938,7 +989,23 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
             set_relax += mg->cfg.n_relax;
         }
         residual = r;
+    } else if (mg->use_graphs && !(mg->ctx->prof.mask & kMgFamilies) && mg->fused_coarse) {
+        // the later-step call is a fixed launch sequence: replay it as one graph
+        artss_ctx *ctx = mg->ctx;
+        artss_mg::Graph *g = nullptr;
+        for (auto &e : mg->graphs)
+            if (e.p == p && e.rhs == rhs) g = &e;
+        if (!g) {
+            if ((st = mg_capture(mg, p, rhs))) return st;
+            g = &mg->graphs.back();
+        }
+        ARTSS_CK(cudaGraphLaunch(g->exec, ctx->stream));
+        ctx->launches += g->launches;
+        for (int f = 0; f < FAM_COUNT; f++) ctx->prof.launches[f] += g->fam[f];
+        cycles = mg->cfg.n_cycle;
+        coarse = -1;
     } else {
+        if ((st = artss_mg_set_rhs(mg, p, rhs))) return st;
         for (int c = 0; c < mg->cfg.n_cycle; c++) {
             if ((st = mg_vcycle(mg, p, &coarse))) return st;
             cycles++;

@@ -256,3 +256,34 @@ def test_cgs_autotune(env, autotune):
     depth = ctx.lib.artss_cgs_sweep_depth(ctx.h, 1)
     assert depth in ((8, 16, 32) if autotune else (0,))
     A.cuda_check(ctx.lib.artss_ctx_autotune(ctx.h, 1), "autotune")
+
+
+def test_vcycle_graph_replay(env):
+    """Later-step pressure calls run as a captured graph; replaying it on the
+    same arrays gives the eager result again, and launches are still counted."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    p0, rhs = rnd(81, n), rnd(82, n)
+    cfg = A.MgCfg(3, 2, 3, 2, 1e-30, 0, 0, 40, 1e-9, 0.6666666667)
+    mg = C.c_void_p()
+    A.cuda_check(ctx.lib.artss_mg_create(ctx.h, C.byref(cfg), C.byref(mg)), "mg")
+    try:
+        dp, drhs = ctx.field(p0), ctx.field(rhs)
+        st = A.MgStats()
+        outs = []
+        for _ in range(3):
+            ctx.upload(dp, p0)
+            l0 = ctx.lib.artss_ctx_kernel_launches(ctx.h)
+            A.cuda_check(ctx.lib.artss_mg_pressure(mg, dp, drhs, 0, C.byref(st)), "pressure")
+            assert ctx.lib.artss_ctx_kernel_launches(ctx.h) - l0 > 20
+            outs.append(ctx.download(dp))
+        ocfg = oracle.MgCfg(3, 2, 3, 2, 1e-30, 0, 0, 40, 1e-9, 0.6666666667)
+        om = oracle.lib().oracle_mg_create(osc.ptr, C.byref(ocfg))
+        ref = p0.copy()
+        res = C.c_double()
+        oracle.lib().oracle_mg_pressure(om, P(ref), P(rhs), 0, C.byref(res))
+        oracle.lib().oracle_mg_destroy(om)
+        for o in outs:
+            assert np.array_equal(o, ref)
+    finally:
+        ctx.lib.artss_mg_destroy(mg)
