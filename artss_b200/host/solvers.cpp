@@ -255,6 +255,56 @@ void NSSolver::do_step(real t, bool sync) {
     pres->projection(f.u, f.v, f.w, f.u_tmp, f.v_tmp, f.w_tmp, f.p, sync);
 }
 
+// ---------------------------------------------------------------- velocity-only solvers
+
+VelocitySolver::VelocitySolver(Runtime &rt, FieldController &fc, Kind kind, std::array<real, 3> velocity_lin)
+    : m_rt(rt), m_fc(fc), m_kind(kind) {
+    const settings::Solver &s = rt.settings().solver;
+    if (kind == ADVECTION || kind == ADVECTION_DIFFUSION) adv = make_advection(rt, s.advection);
+    if (kind != ADVECTION) dif = make_diffusion(rt, s.diffusion);
+    if (kind == DIFFUSION_TURB) mu_tub = make_turbulence(rt, s.turbulence);
+    if (kind == ADVECTION) {
+        // AdvectionSolver.cpp:17-27: constant fields of the GaussBubble velocity
+        m_u_lin = std::make_unique<Field>(rt, F_U, velocity_lin[0]);
+        m_v_lin = std::make_unique<Field>(rt, F_V, velocity_lin[1]);
+        m_w_lin = std::make_unique<Field>(rt, F_W, velocity_lin[2]);
+    }
+}
+
+void VelocitySolver::do_step(real, bool sync) {
+    FieldController &f = m_fc;
+    const real nu = m_rt.settings().physical.nu.value_or(0.0);
+    switch (m_kind) {
+        case ADVECTION:  // AdvectionSolver.cpp:47-66
+            adv->advect(f.u, f.u0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
+            adv->advect(f.v, f.v0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
+            adv->advect(f.w, f.w0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
+            break;
+        case ADVECTION_DIFFUSION:  // AdvectionDiffusionSolver.cpp:45-95
+            adv->advect(f.u, f.u0, f.u0, f.v0, f.w0, sync);
+            adv->advect(f.v, f.v0, f.u0, f.v0, f.w0, sync);
+            adv->advect(f.w, f.w0, f.u0, f.v0, f.w0, sync);
+            FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+            if (nu != 0.) {
+                dif->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
+                dif->diffuse(f.v, f.v0, f.v_tmp, nu, sync);
+                dif->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
+            }
+            break;
+        case DIFFUSION:  // DiffusionSolver.cpp:40-62
+            dif->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
+            dif->diffuse(f.v, f.v0, f.v_tmp, nu, sync);
+            dif->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
+            break;
+        case DIFFUSION_TURB:  // DiffusionTurbSolver.cpp:44-77
+            mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
+            dif->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
+            dif->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
+            dif->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
+            break;
+    }
+}
+
 // ---------------------------------------------------------------- PressureSolver
 
 PressureSolver::PressureSolver(Runtime &rt, FieldController &fc) : m_fc(fc) {
@@ -277,6 +327,20 @@ SolverController::SolverController(Runtime &rt) : m_rt(rt) {
         m_has_momentum_source = true;
     } else if (d == "PressureSolver") {
         m_solver = std::make_unique<PressureSolver>(rt, *m_fc);
+    } else if (d == "AdvectionSolver") {
+        // SolverController.cpp:54-56: the transport velocity is the GaussBubble's
+        const auto &v = rt.settings().ic.values;
+        if (rt.settings().ic.usr_fct != "GaussBubble")
+            throw config_error("AdvectionSolver takes its velocity from the GaussBubble initial condition");
+        m_solver = std::make_unique<VelocitySolver>(
+            rt, *m_fc, VelocitySolver::ADVECTION,
+            std::array<real, 3>{std::stod(v.at("u_lin")), std::stod(v.at("v_lin")), std::stod(v.at("w_lin"))});
+    } else if (d == "AdvectionDiffusionSolver") {
+        m_solver = std::make_unique<VelocitySolver>(rt, *m_fc, VelocitySolver::ADVECTION_DIFFUSION);
+    } else if (d == "DiffusionSolver") {
+        m_solver = std::make_unique<VelocitySolver>(rt, *m_fc, VelocitySolver::DIFFUSION);
+    } else if (d == "DiffusionTurbSolver") {
+        m_solver = std::make_unique<VelocitySolver>(rt, *m_fc, VelocitySolver::DIFFUSION_TURB);
     } else {
         throw config_error("Solver " + d + " not yet implemented on this path");
     }
@@ -326,10 +390,54 @@ void SolverController::set_up_fields() {
             rhs[(size_t) idx] = std::sin(l * M_PI * xi) * std::sin(l * M_PI * yj) * std::sin(l * M_PI * zk);
         }
         m_fc->rhs.from_host(rhs);
+    } else if (ic.usr_fct == "ExpSinusProd" || ic.usr_fct == "GaussBubble" || ic.usr_fct == "Hat") {
+        // Functions::exp_sinus_prod / gauss_bubble / hat (src/Functions.cpp:324-353,
+        // 471-511, hat) at t = 0 on the inner cells of u, v and w
+        const GridLevel &g = geo.grid().level(0);
+        const auto &X1 = geo.grid().start_pd;
+        const size_t Nx = g.N[0], Nxy = g.N[0] * g.N[1];
+        auto num = [&](const char *k) { return std::stod(ic.values.at(k)); };
+        const real t = 0.;
+        std::vector<real> out(m_fc->u.get_size());
+        for (Idx idx : inner) {
+            const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx, i = (size_t) idx - k * Nxy - j * Nx;
+            const real xi = X1[0] + ((real) i - 0.5) * g.spacing[0];
+            const real yj = X1[1] + ((real) j - 0.5) * g.spacing[1];
+            const real zk = X1[2] + ((real) k - 0.5) * g.spacing[2];
+            real v;
+            if (ic.usr_fct == "ExpSinusProd") {
+                const real A = 1.0, l = num("l");
+                const real kpinu = 3 * l * l * M_PI * M_PI * m_rt.settings().physical.nu.value_or(0.0);
+                v = A * std::exp(-kpinu * t) * std::sin(l * M_PI * xi) * std::sin(l * M_PI * yj) *
+                    std::sin(l * M_PI * zk);
+            } else if (ic.usr_fct == "GaussBubble") {
+                const real u_lin = num("u_lin"), v_lin = num("v_lin"), w_lin = num("w_lin");
+                const real l = num("l");
+                const real xs = (xi - num("x_shift")) / u_lin - t, ys = (yj - num("y_shift")) / v_lin - t;
+                const real x2 = xs * xs, y2 = ys * ys;
+                real z2 = 0;
+                if (w_lin != 0) {
+                    const real zs = (zk - num("z_shift")) / w_lin - t;
+                    z2 = zs * zs;
+                }
+                const real quot = 1. / (2. * l * l);
+                v = std::exp(-(x2 + y2 + z2) * quot);
+            } else {
+                const bool in = (num("x1") <= xi && xi <= num("x2")) && (num("y1") <= yj && yj <= num("y2")) &&
+                                (num("z1") <= zk && zk <= num("z2"));
+                v = in ? num("val_in") : num("val_out");
+            }
+            out[(size_t) idx] = v;
+        }
+        for (Field *f : {&m_fc->u, &m_fc->v, &m_fc->w}) {
+            std::vector<real> h = f->to_host();
+            for (Idx idx : inner) h[(size_t) idx] = out[(size_t) idx];
+            f->from_host(h);
+        }
     } else if (ic.usr_fct != "Zero") {
         throw config_error("initial condition '" + ic.usr_fct +
-                           "' is not one of Uniform, SinSinSin, Zero (the initial conditions of the "
-                           "fractional-step path this library runs)");
+                           "' is not one of Uniform, SinSinSin, ExpSinusProd, GaussBubble, Hat, Zero (the "
+                           "initial conditions of the solvers this library runs)");
     }
     const std::string &d = m_rt.settings().solver.description;
     if (d == "NSTempTurbSolver") force_source();

@@ -2,6 +2,8 @@
 // loop of ARTSS (src/field/FieldController.*, src/solver/*, src/TimeIntegration.*).
 #pragma once
 
+#include <array>
+
 #include <chrono>
 #include <memory>
 #include <string>
@@ -88,6 +90,27 @@ class NSSolver : public ISolver {
     std::unique_ptr<IPressure> pres;
     std::unique_ptr<ISource> sou_vel;
     bool m_add_source = false;
+};
+
+// AdvectionSolver, AdvectionDiffusionSolver, DiffusionSolver, DiffusionTurbSolver
+// (src/solver/AdvectionSolver.cpp, AdvectionDiffusionSolver.cpp, DiffusionSolver.cpp,
+// DiffusionTurbSolver.cpp): the velocity-only compositions of the same plugins.
+class VelocitySolver : public ISolver {
+ public:
+    enum Kind { ADVECTION, ADVECTION_DIFFUSION, DIFFUSION, DIFFUSION_TURB };
+    VelocitySolver(Runtime &rt, FieldController &fc, Kind kind, std::array<real, 3> velocity_lin = {0, 0, 0});
+    void do_step(real t, bool sync) override;
+    void update_source(real) override {}
+    void update_obstacle_change() override {}
+
+ private:
+    Runtime &m_rt;
+    FieldController &m_fc;
+    Kind m_kind;
+    std::unique_ptr<IAdvection> adv;
+    std::unique_ptr<IDiffusion> dif;
+    std::unique_ptr<ITurbulence> mu_tub;
+    std::unique_ptr<Field> m_u_lin, m_v_lin, m_w_lin;  // AdvectionSolver's constant transport velocity
 };
 
 // PressureSolver (src/solver/PressureSolver.cpp:30-43)

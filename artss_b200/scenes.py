@@ -77,6 +77,7 @@ class Scene:
     obstacle_bcs: List[Tuple[str, str, str, float]] = field(default_factory=list)
     ic: str = "Uniform"
     pressure: str = "VCycleMG"  # or "VCycleMGMixed" (mixed-precision solve to mg_tol, relative)
+    ic_params: dict = field(default_factory=dict)  # parameters of ExpSinusProd / GaussBubble / Hat
 
     @property
     def t_end(self) -> float:
@@ -238,6 +239,29 @@ def poisson_rhs(inner, size: int, seed: int):
     return b
 
 
+VELOCITY_SOLVERS = ("AdvectionSolver", "AdvectionDiffusionSolver", "DiffusionSolver", "DiffusionTurbSolver")
+
+
+def velocity_scene(solver: str, n: int = 32, steps: int = 5, diffusion: str = "Jacobi", **kw) -> Scene:
+    """A velocity-only scene of the reference's test family (tests/diffusion,
+    tests/advection, tests/diffusionTurb): a 2 x 2 x 1 m box with Dirichlet
+    u = v = w = 0 walls, n x n x n/2 cells, initial u, v, w from ExpSinusProd
+    (diffusion solvers) or GaussBubble (advection solvers)."""
+    if solver not in VELOCITY_SOLVERS:
+        raise ValueError(solver)
+    if solver in ("AdvectionSolver", "AdvectionDiffusionSolver"):
+        ic, params = "GaussBubble", {"u_lin": 0.5, "v_lin": 0.5, "w_lin": 0.25, "x_shift": 0.6, "y_shift": 0.7,
+                                     "z_shift": 0.5, "l": 0.25}
+    else:
+        ic, params = "ExpSinusProd", {"l": 2.5}
+    base = dict(solver=solver, nx=n, ny=n, nz=max(n // 2, 2), X=(0.0, 2.0), Y=(0.0, 2.0), Z=(0.0, 1.0), dt=0.0125,
+                steps=steps, nu=0.001, diffusion=diffusion, diff_tol=1e-7, diff_max_iter=100,
+                boundaries=[("u,v,w", "front,back,left,right,bottom,top", "dirichlet", 0.0)], noise=False, ic=ic,
+                ic_params=params)
+    base.update(kw)
+    return Scene(**base)
+
+
 def plume_ensemble(count: int = 64, seed: int = 0, steps: int = 100, sizes=(32, 48, 64, 96, 128)) -> List[Scene]:
     """The ensemble workload: `count` closed plume boxes whose cell counts per
     axis are drawn from `sizes`, 0.0375 m cells, heat release U[10, 150] kW
@@ -269,7 +293,11 @@ def to_xml(s: Scene) -> str:
     a("  <physical_parameters>")
     a(f"    <t_end> {_f(s.t_end)} </t_end>")
     a(f"    <dt> {_f(s.dt)} </dt>")
-    if s.solver != "PressureSolver":
+    velocity_only = s.solver in VELOCITY_SOLVERS
+    if velocity_only:
+        if s.solver != "AdvectionSolver":
+            a(f"    <nu> {_f(s.nu)} </nu>")
+    elif s.solver != "PressureSolver":
         a(f"    <nu> {_f(s.nu)} </nu>")
         a(f"    <beta> {_f(s.beta)} </beta>")
         a(f"    <g> {_f(s.g)} </g>")
@@ -285,7 +313,17 @@ def to_xml(s: Scene) -> str:
         a(f"{indent}  <w> {_f(w)} </w>")
         a(f"{indent}</diffusion>")
 
-    if s.solver != "PressureSolver":
+    if velocity_only:
+        if s.solver in ("AdvectionSolver", "AdvectionDiffusionSolver"):
+            a('    <advection type="SemiLagrangian" field="u,v,w">')
+            a("    </advection>")
+        if s.solver != "AdvectionSolver":
+            diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
+        if s.solver == "DiffusionTurbSolver":
+            a('    <turbulence type="ConstSmagorinsky">')
+            a(f"      <Cs> {_f(s.cs)} </Cs>")
+            a("    </turbulence>")
+    elif s.solver != "PressureSolver":
         a('    <advection type="SemiLagrangian" field="u,v,w">')
         a("    </advection>")
         diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
@@ -295,15 +333,16 @@ def to_xml(s: Scene) -> str:
         a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
         a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
         a("    </source>")
-    a(f'    <pressure type="{s.pressure}" field="p">')
-    a(f"      <n_level> {s.n_level} </n_level>")
-    a(f"      <n_cycle> {s.n_cycle} </n_cycle>")
-    a(f"      <max_cycle> {s.max_cycle} </max_cycle>")
-    a(f"      <tol_res> {_f(s.mg_tol)} </tol_res>")
-    a(f"      <n_relax> {s.n_relax} </n_relax>")
-    diffusion_block("p", "      ", s.smoother, s.smoother_max_iter, s.smoother_tol, s.smoother_w)
-    a("    </pressure>")
-    if s.solver != "PressureSolver":
+    if not velocity_only:
+        a(f'    <pressure type="{s.pressure}" field="p">')
+        a(f"      <n_level> {s.n_level} </n_level>")
+        a(f"      <n_cycle> {s.n_cycle} </n_cycle>")
+        a(f"      <max_cycle> {s.max_cycle} </max_cycle>")
+        a(f"      <tol_res> {_f(s.mg_tol)} </tol_res>")
+        a(f"      <n_relax> {s.n_relax} </n_relax>")
+        diffusion_block("p", "      ", s.smoother, s.smoother_max_iter, s.smoother_tol, s.smoother_w)
+        a("    </pressure>")
+    if not velocity_only and s.solver != "PressureSolver":
         a("    <temperature>")
         a('      <advection type="SemiLagrangian" field="T">')
         a("      </advection>")
@@ -365,6 +404,8 @@ def to_xml(s: Scene) -> str:
         a("  </initial_conditions>")
     else:
         a(f'  <initial_conditions usr_fct="{s.ic}" random="No">')
+        for k, v in s.ic_params.items():
+            a(f"    <{k}> {_f(v)} </{k}>")
         a("  </initial_conditions>")
     a('  <visualisation save_vtk="No" save_csv="No">')
     a("  </visualisation>")

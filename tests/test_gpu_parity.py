@@ -31,6 +31,12 @@ def _scenes():
         "channel_cube": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=4, n_level=3),
         "room_jacobi": scenes.room_with_door(n=32, steps=4, n_level=2),
         "room_cgs": scenes.room_with_door(n=32, steps=3, n_level=2, diffusion="ColoredGaussSeidel"),
+        # the velocity-only solver compositions (src/solver/AdvectionSolver.cpp, ...)
+        "advection": scenes.velocity_scene("AdvectionSolver", n=32, steps=4),
+        "advection_diffusion": scenes.velocity_scene("AdvectionDiffusionSolver", n=32, steps=4),
+        "diffusion_jacobi": scenes.velocity_scene("DiffusionSolver", n=32, steps=4),
+        "diffusion_cgs": scenes.velocity_scene("DiffusionSolver", n=32, steps=4, diffusion="ColoredGaussSeidel"),
+        "diffusion_turb": scenes.velocity_scene("DiffusionTurbSolver", n=32, steps=4),
     }
 
 
