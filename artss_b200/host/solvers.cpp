@@ -118,12 +118,15 @@ Field *FieldController::by_name(const std::string &n) {
 
 // ---------------------------------------------------------------- NSTempTurbSolver
 
-NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc) : m_rt(rt), m_fc(fc) {
+NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent)
+    : m_rt(rt), m_fc(fc), m_turb(turbulent) {
+    // NSTempSolver (src/solver/NSTempSolver.cpp:19-48) is the same composition
+    // without the turbulence model
     const settings::Solver &s = rt.settings().solver;
     adv_vel = make_advection(rt, s.advection);
     adv_temp = make_advection(rt, s.temperature.advection);
     dif_vel = make_diffusion(rt, s.diffusion);
-    mu_tub = make_turbulence(rt, s.turbulence);
+    if (turbulent) mu_tub = make_turbulence(rt, s.turbulence);
     dif_temp = make_diffusion(rt, s.diffusion);  // NSTempTurbSolver.cpp:45: the velocity settings
     pres = make_pressure(rt, s.pressure);
     sou_vel = make_source(rt, s.source.type, s.source.dir);
@@ -161,15 +164,26 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     }
     FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
 
-    // 2. turbulent viscosity and diffusion (:140-152)
-    mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
-    dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
-    stats.diffusion_iterations[0] = dif_vel->last_iterations;
-    dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
-    stats.diffusion_iterations[1] = dif_vel->last_iterations;
-    dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
-    stats.diffusion_iterations[2] = dif_vel->last_iterations;
-    FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    // 2. turbulent viscosity and diffusion (:140-152); NSTempSolver: laminar
+    //    diffusion when nu != 0 (NSTempSolver.cpp:99-108)
+    if (m_turb) {
+        mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
+        dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
+        stats.diffusion_iterations[0] = dif_vel->last_iterations;
+        dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
+        stats.diffusion_iterations[1] = dif_vel->last_iterations;
+        dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
+        stats.diffusion_iterations[2] = dif_vel->last_iterations;
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    } else if (nu != 0.) {
+        dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
+        stats.diffusion_iterations[0] = dif_vel->last_iterations;
+        dif_vel->diffuse(f.v, f.v0, f.v_tmp, nu, sync);
+        stats.diffusion_iterations[1] = dif_vel->last_iterations;
+        dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
+        stats.diffusion_iterations[2] = dif_vel->last_iterations;
+        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+    }
 
     // 3. momentum source (:155-163)
     if (m_add_source) {
@@ -188,7 +202,7 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     adv_temp->advect(f.T, f.T0, f.u, f.v, f.w, sync);
     FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
     const auto &ts = m_rt.settings().solver.temperature;
-    if (ts.has_turbulence) {
+    if (m_turb && ts.has_turbulence) {
         const real rPr_T = 1. / ts.prandtl_number.value();
         check(artss_scale_copy(m_rt.ctx(), f.kappa_t.data, f.nu_t.data, rPr_T, 0), "kappa_t");
         dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, f.kappa_t, sync);
@@ -319,8 +333,8 @@ void PressureSolver::do_step(real t, bool sync) { pres->pressure(m_fc.p, m_fc.rh
 SolverController::SolverController(Runtime &rt) : m_rt(rt) {
     m_fc = std::make_unique<FieldController>(rt);
     const std::string &d = rt.settings().solver.description;
-    if (d == "NSTempTurbSolver") {
-        m_solver = std::make_unique<NSTempTurbSolver>(rt, *m_fc);
+    if (d == "NSTempTurbSolver" || d == "NSTempSolver") {
+        m_solver = std::make_unique<NSTempTurbSolver>(rt, *m_fc, d == "NSTempTurbSolver");
         m_has_momentum_source = true;
     } else if (d == "NSSolver" || d == "NSTurbSolver") {
         m_solver = std::make_unique<NSSolver>(rt, *m_fc, d == "NSTurbSolver");
@@ -434,13 +448,66 @@ void SolverController::set_up_fields() {
             for (Idx idx : inner) h[(size_t) idx] = out[(size_t) idx];
             f->from_host(h);
         }
+    } else if (ic.usr_fct == "Drift" || ic.usr_fct == "McDermott" || ic.usr_fct == "Vortex") {
+        // the Navier-Stokes test states on the inner cells of u, v, w and p:
+        // Functions::drift (src/Functions.cpp:297-317), Functions::mcdermott
+        // (:696-729, at t = 0) and Functions::vortex (:842-886); McDermott and
+        // Vortex are followed by p = 0 everywhere (SolverController.cpp:130-148)
+        const GridLevel &g = geo.grid().level(0);
+        const auto &X1 = geo.grid().start_pd;
+        const size_t Nx = g.N[0], Nxy = g.N[0] * g.N[1];
+        auto num = [&](const char *k) { return std::stod(ic.values.at(k)); };
+        std::vector<real> u = m_fc->u.to_host(), v = m_fc->v.to_host(), w = m_fc->w.to_host(), p = m_fc->p.to_host();
+        auto xi = [&](size_t i) { return X1[0] + ((real) i - 0.5) * g.spacing[0]; };
+        auto yj = [&](size_t j) { return X1[1] + ((real) j - 0.5) * g.spacing[1]; };
+        if (ic.usr_fct == "Drift") {
+            const real u_lin = num("u_lin"), v_lin = num("v_lin"), w_lin = num("w_lin"), pa = num("pa");
+            for (Idx idx : inner) {
+                u[(size_t) idx] = u_lin;
+                v[(size_t) idx] = v_lin;
+                w[(size_t) idx] = w_lin;
+                p[(size_t) idx] = pa;
+            }
+        } else if (ic.usr_fct == "McDermott") {
+            const real A = num("A"), nu = m_rt.settings().physical.nu.value(), t = 0.;
+            for (Idx idx : inner) {
+                const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx, i = (size_t) idx - k * Nxy - j * Nx;
+                u[(size_t) idx] = 1. - A * std::cos(xi(i) - t) * std::sin(yj(j) - t) * std::exp(-2 * nu * t);
+                v[(size_t) idx] = 1. + A * std::sin(xi(i) - t) * std::cos(yj(j) - t) * std::exp(-2 * nu * t);
+                w[(size_t) idx] = 0.;
+                p[(size_t) idx] = -0.25 * A * A * (std::cos(2 * (xi(i) - t)) + std::cos(2 * (yj(j) - t))) *
+                                  std::exp(-4 * nu * t);
+            }
+        } else {
+            // the reference reads the vortex's v from w_lin and its w from v_lin
+            const real u_lin = num("u_lin"), v_lin = num("w_lin"), rhoa = num("rhoa"), pa = num("pa");
+            const real L = geo.grid().length_cd(0);
+            const real R_c = L / 20.;
+            const real G = 0.04 * u_lin * R_c * std::sqrt(std::exp(1));
+            const real GrR_c = G / (R_c * R_c);
+            const real rR_c = 1. / (2. * R_c * R_c);
+            const real rhoGrR_c = rhoa * G * G * rR_c;
+            for (Idx idx : inner) {
+                const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx, i = (size_t) idx - k * Nxy - j * Nx;
+                const real x = xi(i), y = yj(j);
+                u[(size_t) idx] = u_lin - GrR_c * y * std::exp(-rR_c * (x * x + y * y));
+                v[(size_t) idx] = v_lin + GrR_c * x * std::exp(-rR_c * (x * x + y * y));
+                w[(size_t) idx] = 0.;
+                p[(size_t) idx] = pa - rhoGrR_c * std::exp(-rR_c * (x * x + y * y));
+            }
+        }
+        m_fc->u.from_host(u);
+        m_fc->v.from_host(v);
+        m_fc->w.from_host(w);
+        m_fc->p.from_host(p);
+        if (ic.usr_fct != "Drift") m_fc->p.set_value(0.);
     } else if (ic.usr_fct != "Zero") {
         throw config_error("initial condition '" + ic.usr_fct +
-                           "' is not one of Uniform, SinSinSin, ExpSinusProd, GaussBubble, Hat, Zero (the "
-                           "initial conditions of the solvers this library runs)");
+                           "' is not one of Uniform, SinSinSin, ExpSinusProd, GaussBubble, Hat, Drift, McDermott, "
+                           "Vortex, Zero (the initial conditions of the solvers this library runs)");
     }
     const std::string &d = m_rt.settings().solver.description;
-    if (d == "NSTempTurbSolver") force_source();
+    if (d == "NSTempTurbSolver" || d == "NSTempSolver") force_source();
 }
 
 void SolverController::force_source() {
@@ -449,7 +516,15 @@ void SolverController::force_source() {
     if (src.force_fct == "Buoyancy") {
         if (!src.use_init_values) m_fc->T_ambient.set_value(src.ambient_temperature.value());
     } else if (src.force_fct == "Uniform") {
-        throw config_error("a uniform momentum force is not part of the fractional-step path implemented here");
+        // Functions::uniform on the force components named by dir, inner cells only
+        const IdxList &inner = m_rt.geometry().inner(0);
+        Field *force[3] = {&m_fc->f_x, &m_fc->f_y, &m_fc->f_z};
+        for (int a = 0; a < 3; a++) {
+            if (std::find(src.dir.begin(), src.dir.end(), a) == src.dir.end()) continue;
+            std::vector<real> h = force[a]->to_host();
+            for (Idx idx : inner) h[(size_t) idx] = src.uniform_value[a];
+            force[a]->from_host(h);
+        }
     }
 }
 

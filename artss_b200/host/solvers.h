@@ -54,7 +54,7 @@ struct StepStats {
 // NSTempTurbSolver (src/solver/NSTempTurbSolver.cpp:94-248)
 class NSTempTurbSolver : public ISolver {
  public:
-    NSTempTurbSolver(Runtime &rt, FieldController &fc);
+    NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent = true);
     void do_step(real t, bool sync) override;
     void update_source(real t_cur) override;
     void update_obstacle_change() override;
@@ -63,6 +63,7 @@ class NSTempTurbSolver : public ISolver {
  private:
     Runtime &m_rt;
     FieldController &m_fc;
+    bool m_turb = true;
     std::unique_ptr<IAdvection> adv_vel, adv_temp;
     std::unique_ptr<IDiffusion> dif_vel, dif_temp;
     std::unique_ptr<ITurbulence> mu_tub;

@@ -8,6 +8,7 @@ XML (tests/navierStokesTempTurb/steckler/Test_NavierStokesTempTurb_Steckler.xml)
 """
 from __future__ import annotations
 
+import math
 import os
 import random
 from dataclasses import dataclass, field
@@ -77,7 +78,9 @@ class Scene:
     obstacle_bcs: List[Tuple[str, str, str, float]] = field(default_factory=list)
     ic: str = "Uniform"
     pressure: str = "VCycleMG"  # or "VCycleMGMixed" (mixed-precision solve to mg_tol, relative)
-    ic_params: dict = field(default_factory=dict)  # parameters of ExpSinusProd / GaussBubble / Hat
+    ic_params: dict = field(default_factory=dict)  # parameters of ExpSinusProd / GaussBubble / Hat / ...
+    force: str = "Buoyancy"  # momentum source force_fct: Buoyancy, Uniform or Zero
+    force_value: Tuple[float, float, float] = (0.0, 0.0, 0.0)  # Uniform: val_x, val_y, val_z
 
     @property
     def t_end(self) -> float:
@@ -262,6 +265,51 @@ def velocity_scene(solver: str, n: int = 32, steps: int = 5, diffusion: str = "J
     return Scene(**base)
 
 
+NS_SOLVERS = ("NSSolver", "NSTurbSolver")
+
+
+def ns_scene(kind: str, solver: str = "NSSolver", n: int = 32, steps: int = 4, **kw) -> Scene:
+    """Isothermal Navier-Stokes scenes of the reference's test family
+    (tests/navierStokes, tests/navierStokesTurb), in 3-D:
+      cavity   lid-driven unit cube, u = 1 on the top wall, n x n x n/2 cells;
+      mcdermott  periodic 2 pi box with the McDermott vortex array (A = 2);
+      vortex   periodic box centred on the origin with one travelling vortex;
+      channel  Drift start u = 0.5 between no-slip walls, periodic in x,
+               with a uniform x force (which NSSolver never sets, as in the
+               reference, whose force_source runs only for the temperature solvers)."""
+    if solver not in NS_SOLVERS:
+        raise ValueError(solver)
+    nz = max(n // 2, 2)
+    periodic = [("u,v,w", "front,back,left,right,bottom,top", "periodic", 0.0),
+                ("p", "front,back,left,right,bottom,top", "periodic", 0.0)]
+    base = dict(solver=solver, nx=n, ny=n, nz=nz, steps=steps, noise=False, diffusion="Jacobi", diff_tol=1e-7,
+                force="Zero", buoyancy_dir="x,y,z", n_level=3, smoother_tol=1e-7)
+    if kind == "cavity":
+        base.update(X=(0.0, 1.0), Y=(0.0, 1.0), Z=(0.0, 0.5), dt=0.005, nu=0.01, ic="Zero",
+                    boundaries=[("u", "top", "dirichlet", 1.0), ("u", "front,back,left,right,bottom", "dirichlet", 0.0),
+                                ("v,w", "front,back,left,right,bottom,top", "dirichlet", 0.0),
+                                ("p", "top", "dirichlet", 0.0), ("p", "front,back,left,right,bottom", "neumann", 0.0)])
+    elif kind == "mcdermott":
+        L = 2.0 * math.pi
+        base.update(X=(0.0, L), Y=(0.0, L), Z=(0.0, L / 2), dt=0.01, nu=0.1, ic="McDermott", ic_params={"A": 2.0},
+                    boundaries=periodic)
+    elif kind == "vortex":
+        base.update(X=(-0.16, 0.16), Y=(-0.16, 0.16), Z=(-0.08, 0.08), dt=0.002, nu=1e-4, ic="Vortex",
+                    ic_params={"u_lin": 0.5, "v_lin": 0.0, "w_lin": 0.1, "pa": 0.0, "rhoa": 1.0},
+                    boundaries=periodic)
+    elif kind == "channel":
+        base.update(X=(0.0, 2.0), Y=(0.0, 1.0), Z=(0.0, 1.0), dt=0.01, nu=0.01, ic="Drift",
+                    ic_params={"u_lin": 0.5, "v_lin": 0.0, "w_lin": 0.0, "pa": 0.0}, force="Uniform",
+                    buoyancy_dir="x", force_value=(0.2, 0.0, 0.0),
+                    boundaries=[("u,v,w", "left,right", "periodic", 0.0),
+                                ("u,v,w", "front,back,bottom,top", "dirichlet", 0.0),
+                                ("p", "left,right", "periodic", 0.0), ("p", "front,back,bottom,top", "neumann", 0.0)])
+    else:
+        raise ValueError(kind)
+    base.update(kw)
+    return Scene(**base)
+
+
 def plume_ensemble(count: int = 64, seed: int = 0, steps: int = 100, sizes=(32, 48, 64, 96, 128)) -> List[Scene]:
     """The ensemble workload: `count` closed plume boxes whose cell counts per
     axis are drawn from `sizes`, 0.0375 m cells, heat release U[10, 150] kW
@@ -294,6 +342,10 @@ def to_xml(s: Scene) -> str:
     a(f"    <t_end> {_f(s.t_end)} </t_end>")
     a(f"    <dt> {_f(s.dt)} </dt>")
     velocity_only = s.solver in VELOCITY_SOLVERS
+    # NSTempSolver and NSSolver (src/solver/NSTempSolver.cpp, NSSolver.cpp) read
+    # no turbulence blocks; NSSolver and NSTurbSolver carry no temperature
+    turbulent = s.solver not in ("NSTempSolver", "NSSolver")
+    temperature = s.solver not in NS_SOLVERS + ("PressureSolver",)
     if velocity_only:
         if s.solver != "AdvectionSolver":
             a(f"    <nu> {_f(s.nu)} </nu>")
@@ -302,7 +354,8 @@ def to_xml(s: Scene) -> str:
         a(f"    <beta> {_f(s.beta)} </beta>")
         a(f"    <g> {_f(s.g)} </g>")
         a("    <rhoa> 1 </rhoa>")
-        a(f"    <kappa> {_f(s.kappa)} </kappa>")
+        if temperature:
+            a(f"    <kappa> {_f(s.kappa)} </kappa>")
     a("  </physical_parameters>")
     a(f'  <solver description="{s.solver}" >')
 
@@ -327,11 +380,19 @@ def to_xml(s: Scene) -> str:
         a('    <advection type="SemiLagrangian" field="u,v,w">')
         a("    </advection>")
         diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
-        a('    <turbulence type="ConstSmagorinsky">')
-        a(f"      <Cs> {_f(s.cs)} </Cs>")
-        a("    </turbulence>")
-        a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
-        a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
+        if turbulent:
+            a('    <turbulence type="ConstSmagorinsky">')
+            a(f"      <Cs> {_f(s.cs)} </Cs>")
+            a("    </turbulence>")
+        if s.force == "Buoyancy":
+            a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
+            a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
+        elif s.force == "Uniform":
+            a(f'    <source type="ExplicitEuler" force_fct="Uniform" dir="{s.buoyancy_dir}">')
+            for ax, val in zip("xyz", s.force_value):
+                a(f"      <val_{ax}> {_f(val)} </val_{ax}>")
+        else:
+            a(f'    <source type="ExplicitEuler" force_fct="{s.force}" dir="{s.buoyancy_dir}">')
         a("    </source>")
     if not velocity_only:
         a(f'    <pressure type="{s.pressure}" field="p">')
@@ -342,14 +403,15 @@ def to_xml(s: Scene) -> str:
         a(f"      <n_relax> {s.n_relax} </n_relax>")
         diffusion_block("p", "      ", s.smoother, s.smoother_max_iter, s.smoother_tol, s.smoother_w)
         a("    </pressure>")
-    if not velocity_only and s.solver != "PressureSolver":
+    if temperature and not velocity_only:
         a("    <temperature>")
         a('      <advection type="SemiLagrangian" field="T">')
         a("      </advection>")
         diffusion_block("T", "      ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
-        a('      <turbulence include="Yes">')
-        a(f"        <Pr_T> {_f(s.pr_t)} </Pr_T>")
-        a("      </turbulence>")
+        if turbulent:
+            a('      <turbulence include="Yes">')
+            a(f"        <Pr_T> {_f(s.pr_t)} </Pr_T>")
+            a("      </turbulence>")
         a(f'      <source type="ExplicitEuler" dir="{s.buoyancy_dir}" temp_fct="Gauss" dissipation="No" random="No">')
         a(f"        <HRR> {_f(s.hrr)} </HRR>")
         a(f"        <cp> {_f(s.cp)} </cp>")

@@ -37,6 +37,19 @@ def _scenes():
         "diffusion_jacobi": scenes.velocity_scene("DiffusionSolver", n=32, steps=4),
         "diffusion_cgs": scenes.velocity_scene("DiffusionSolver", n=32, steps=4, diffusion="ColoredGaussSeidel"),
         "diffusion_turb": scenes.velocity_scene("DiffusionTurbSolver", n=32, steps=4),
+        # NSTempTurbSolver without the turbulence model (src/solver/NSTempSolver.cpp)
+        "nstemp_box": scenes.plume_box(n=32, steps=4, n_level=3, solver="NSTempSolver"),
+        "nstemp_channel": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=3, n_level=3,
+                                                   solver="NSTempSolver"),
+        "nstemp_uniform_force": scenes.plume_box(n=32, steps=3, n_level=3, solver="NSTempSolver", force="Uniform",
+                                                 buoyancy_dir="x,z", force_value=(0.1, 0.0, 0.3)),
+        # the isothermal compositions (src/solver/NSSolver.cpp, NSTurbSolver.cpp) with
+        # periodic boundaries and the Drift / McDermott / Vortex initial states
+        "ns_cavity": scenes.ns_scene("cavity", n=32, steps=4),
+        "ns_mcdermott": scenes.ns_scene("mcdermott", n=32, steps=4),
+        "ns_channel": scenes.ns_scene("channel", n=32, steps=4),
+        "nsturb_vortex": scenes.ns_scene("vortex", "NSTurbSolver", n=32, steps=4),
+        "nsturb_cavity_cgs": scenes.ns_scene("cavity", "NSTurbSolver", n=32, steps=3, diffusion="ColoredGaussSeidel"),
     }
 
 
