@@ -214,6 +214,8 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
     p.waves = waves;
     p.wave_begin = begin;
     p.n = n;
+    p.h_target = tgt;
+    p.h_root = root;
     if (n == 0) return ARTSS_OK;
     ARTSS_CK(cudaMalloc(&p.d_target, n * sizeof(int64_t)));
     ARTSS_CK(cudaMalloc(&p.d_root, n * sizeof(int64_t)));

@@ -307,6 +307,9 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
         return true;
     };
     if (!check(inner, n_inner, 0, "inner") || !check(domain, n_domain, 1, "domain")) return ARTSS_ERR_ARG;
+    ctx->h_inner[level].assign((size_t) L.size(), false);
+    for (int64_t q = 0; q < n_inner; q++) ctx->h_inner[level][(size_t) inner[q]] = true;
+    for (auto &prog : ctx->bc[level]) prog.pipe_state = -2;
     int64_t *d_list = nullptr;
     const int64_t nmax = std::max<int64_t>(std::max(n_inner, n_domain), 1);
     ARTSS_CK(cudaMalloc(&d_list, nmax * sizeof(int64_t)));

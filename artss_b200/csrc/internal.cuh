@@ -46,6 +46,13 @@ struct BcProgram {
     uint8_t *d_depth = nullptr;
     uint8_t *d_neg = nullptr;          // bit d: step d negates
     double *d_value = nullptr;         // [kBcMaxDepth][n]
+    std::vector<int64_t> h_target;     // targets, host copy
+    std::vector<int64_t> h_root;       // roots, host copy
+    // plan of the pipelined coarse solve: state -2 unknown, -1 not eligible, 1 planned
+    int pipe_state = -2;
+    std::vector<int> pipe_kb;          // plane split, ranks + 1 entries
+    int pipe_ranks = 0, pipe_cap = 0, pipe_tcap = 0;
+    int64_t pipe_smem = 0;
 };
 
 // Device-resident control block of one bounded iteration loop.
@@ -98,6 +105,7 @@ struct artss_ctx {
     artss_grid_desc grid{};
     artss::Level lvl[artss::kMaxLevel + 1]{};
     uint8_t *d_flags[artss::kMaxLevel + 1]{};
+    std::vector<bool> h_inner[artss::kMaxLevel + 1];  // inner-cell bitmap per level, host copy
     int64_t n_inner[artss::kMaxLevel + 1]{};  // inner cells per level (artss_set_cell_lists)
     double *proj[artss::kMaxLevel + 1]{};     // scratch of artss_coarse_project (lazily, freed with fields)
     artss::BcProgram bc[artss::kMaxLevel + 1][artss::kFieldTypes];
@@ -204,7 +212,7 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopSta
 int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const LoopState *pred = nullptr);
 // FP64 cluster solve of a level's pressure equation on FP32 storage, zero
 // boundary values, tolerance relative to the initial residual (mg.cu).
-bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int64_t *smem);
+bool cluster_fits(const artss_ctx *ctx, int level, int buffers, int *plane_cap, int64_t *smem);
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
                        long long max_it, const LoopState *pred);
 

@@ -8,6 +8,7 @@
 // hands back the second-to-last iterate (:699-722, pointer swaps); every
 // smoothing sweep and transfer is followed by the level's boundary program.
 #include "internal.cuh"
+#include "tc.cuh"
 
 #include <algorithm>
 #include <cooperative_groups.h>
@@ -18,6 +19,7 @@ struct artss_mg {
     int L = 0;
     bool fused_coarse = true;
     bool cluster_coarse = true;
+    bool pipelined_coarse = true;
     double *r0[artss::kMaxLevel + 1]{};   // residuum0[level]   (levels 0..L-1)
     double *r1[artss::kMaxLevel + 1]{};   // residuum1[level]   (levels 0..L)
     double *e0[artss::kMaxLevel + 1]{};   // error0[level]      (levels 0..L-1)
@@ -589,11 +591,342 @@ k_mg_coarse_cluster(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__rest
     cl.sync();
 }
 
+// ---------------------------------------------------------------- pipelined Jacobi coarse solve
+//
+// VCycleMG::call_solve_jacobi (src/pressure/VCycleMG.cpp:727-800) on the
+// cluster with every access to the rank's own shared memory and one cluster
+// barrier per sweep, for boundary programs of a single wave (every
+// configuration of the reference's tests):
+//  * rank r owns the z-planes [kb[r], kb[r+1]) of a split chosen on the host
+//    so that no boundary assignment with an inner root crosses a rank; it
+//    keeps them plus one halo plane on each side, in three buffers of the
+//    same layout in every rank;
+//  * after a sweep each rank sends its two edge planes to the neighbours'
+//    halos as two bulk shared-memory copies that complete on the receiver's
+//    mbarrier (point to point, no multicast); the receiver waits on it
+//    before the next sweep reads the halo;
+//  * the boundary program runs inside the sweep: in a single-wave program no
+//    root is ever a target, so a root is either an inner cell, and the thread
+//    that computes the root's new value also evaluates the target's chain
+//    from it (a per-thread target list built at launch), or a cell that
+//    nothing writes, whose targets are set once before the loop;
+//  * the residual of iterate k-1 is summed in the pass that computes iterate
+//    k (both read only iterate k-1), so the loop decision for k arrives one
+//    sweep late.  Three buffers keep iterates k-2, k-1 and k apart and the
+//    reference's result is still there when the loop stops: after `it`
+//    sweeps and swaps, out holds iterate it when it is odd and iterate it-1
+//    when it is even, tmp the other one.
+// Values, iteration count and residual are those of k_mg_coarse_cluster.
+
+// boundary assignment with an inner root in the rank's planes: the target's
+// and the root's local index in a buffer, the chain
+struct HaloTarget {
+    double val[kBcMaxDepth];
+    uint32_t dst, root;
+    uint32_t depth_neg;  // depth | neg << 8
+    uint32_t pad;
+};
+
+// ranks of the pipelined coarse solve: up to 16 CTAs (a non-portable cluster size)
+constexpr int kPipeMaxRanks = 16;
+
+// z-planes of each rank: rank r owns [kb[r], kb[r+1])
+struct PlaneSplit {
+    int kb[kPipeMaxRanks + 1];
+};
+
+// smem -> the same-layout smem of a peer CTA, completing on the peer's
+// mbarrier (a point-to-point bulk copy, no multicast)
+__device__ __forceinline__ void bulk_copy_to_peer(uint32_t dst, uint32_t src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     dst),
+                 "r"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, int rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+
+constexpr int kHaloPolls = 1 << 20;  // mbarrier polls before a halo wait gives up
+constexpr int kPipeCells = 4;        // inner cells per thread of k_mg_coarse_jacobi_pipe
+
+template <typename TS>
+__global__ void __launch_bounds__(kClusterThreads, 1)
+k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restrict__ b,
+                        const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
+                        BcView bc, double tol, int rel, long long max_it, PlaneSplit sp, int plane_cap,
+                        int target_cap, LoopState *__restrict__ st, const LoopState *__restrict__ pred) {
+    namespace cg = cooperative_groups;
+    if (pred && !pred->cond) return;  // every rank reads the same flag
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[32];
+    __shared__ double parts[2][kPipeMaxRanks];
+    __shared__ int s_nt, s_over, s_overs[kPipeMaxRanks], s_fail;
+    __shared__ __align__(8) uint64_t hb[3];  // halo arrivals per buffer
+    const int tid = threadIdx.x;
+    const int rank = (int) cl.block_rank();
+    const int cs = (int) cl.num_blocks();
+    const int nj = (int) L.Nx, nk = (int) (L.Nx * L.Ny);
+    const int kb0 = sp.kb[rank], kb1 = sp.kb[rank + 1], own = kb1 - kb0;
+    const int bstride = (plane_cap + 2) * nk;  // doubles per buffer (nk even: 16-byte planes)
+    double *X = sm;
+    HaloTarget *tg = (HaloTarget *) (sm + 3 * (int64_t) bstride);
+    const uint32_t base = (uint32_t) __cvta_generic_to_shared(sm);
+    if (tid == 0) {
+        s_nt = 0;
+        s_over = 0;
+        s_fail = 0;
+        for (int s = 0; s < 3; s++) tc::mbar_init(&hb[s], 1);
+        tc::fence_barrier_init();
+    }
+    // buffer 0: planes kb0-1 .. kb1 of out (local plane lp = k - kb0 + 1)
+    for (int q = tid; q < (own + 2) * nk; q += kClusterThreads) {
+        const int k = kb0 - 1 + q / nk;
+        X[q] = (k >= 0 && k < (int) L.Nz) ? (double) out[(int64_t) k * nk + q % nk] : 0.0;
+    }
+    // this thread's inner cells: slot m holds box cell lin = tid + m * threads
+    // of the rank's planes; local index and right-hand side
+    const int z0 = max((int) box.z0, kb0), z1 = min((int) box.z1, kb1 - 1);
+    const int nx = (int) box.nx(), nxy = (int) (box.nx() * box.ny());
+    int ca[kPipeCells];
+    double cb[kPipeCells];
+    unsigned m0 = 0;
+    {
+        const int ncell = z1 >= z0 ? (z1 - z0 + 1) * nxy : 0;
+#pragma unroll
+        for (int m = 0; m < kPipeCells; m++) {
+            const int lin = tid + m * kClusterThreads;
+            ca[m] = nk;
+            cb[m] = 0.0;
+            if (lin < ncell) {
+                const int k = z0 + lin / nxy, r = lin % nxy, j = (int) box.y0 + r / nx, i = (int) box.x0 + r % nx;
+                const int o = i + nj * j;
+                const int64_t q = (int64_t) k * nk + o;
+                if (__ldg(flags + q) & kInner) {
+                    ca[m] = (k - kb0 + 1) * nk + o;
+                    cb[m] = (double) b[q];
+                    m0 |= 1u << m;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // the boundary program on iterate 0 for the targets in own planes (roots
+    // lie within one plane, in own or halo planes, and are never targets), and
+    // the table of the targets whose root is an inner cell (the split keeps
+    // such a root in its target's rank); the others stay as set here
+    const int64_t q_begin = bc.waves > 0 ? bc.begin[0] : 0, q_end = bc.waves > 0 ? bc.begin[1] : 0;
+    for (int64_t q0 = q_begin; q0 < q_end; q0 += kClusterThreads) {
+        const int64_t qq = q0 + tid;
+        if (qq >= q_end) continue;
+        const int t = (int) __ldg(bc.target + qq), kt = t / nk;
+        if (kt < kb0 || kt >= kb1) continue;
+        const int r = (int) __ldg(bc.root + qq), kr = r / nk;
+        const int d = __ldg(bc.depth + qq);
+        const uint8_t mneg = __ldg(bc.neg + qq);
+        double x = X[(kr - kb0 + 1) * nk + (r - kr * nk)];
+#pragma unroll
+        for (int s = 0; s < kBcMaxDepth; s++)
+            if (s < d) x = ((mneg >> s) & 1 ? -x : x) + (bc.value ? __ldg(bc.value + s * bc.n + qq) : 0.0);
+        X[(kt - kb0 + 1) * nk + (t - kt * nk)] = x;
+        if (!(__ldg(flags + r) & kInner)) continue;  // constant root: set once above
+        if (kr < kb0 || kr >= kb1) {
+            s_over = 1;  // the split did not keep the root with its target
+            continue;
+        }
+        const int slot = atomicAdd(&s_nt, 1);
+        if (slot >= target_cap) {
+            s_over = 1;
+            continue;
+        }
+        HaloTarget &h = tg[slot];
+#pragma unroll
+        for (int s = 0; s < kBcMaxDepth; s++) h.val[s] = (s < d && bc.value) ? __ldg(bc.value + s * bc.n + qq) : 0.0;
+        h.dst = (uint32_t) ((kt - kb0 + 1) * nk + (t - kt * nk));
+        h.root = (uint32_t) ((kr - kb0 + 1) * nk + (r - kr * nk));
+        h.depth_neg = (uint32_t) d | (uint32_t) mneg << 8;
+        h.pad = 0;
+    }
+    __syncthreads();
+    const int nt = min(s_nt, target_cap);
+    cl.sync();
+    // every rank learns every rank's error flag, so all take the same path
+    if (tid < cs) cl.map_shared_rank(s_overs, tid)[rank] = s_over;
+    // halo planes of iterate 0 from the neighbours' own planes
+    if (rank > 0) {
+        const double *src = cl.map_shared_rank(X, rank - 1) + (int64_t) (kb0 - sp.kb[rank - 1]) * nk;
+        for (int q = tid; q < nk; q += kClusterThreads) X[q] = src[q];
+    }
+    if (rank < cs - 1) {
+        const double *src = cl.map_shared_rank(X, rank + 1) + nk;
+        for (int q = tid; q < nk; q += kClusterThreads) X[(own + 1) * nk + q] = src[q];
+    }
+    __syncthreads();
+    for (int q = tid; q < (own + 2) * nk; q += kClusterThreads) X[2 * bstride + q] = X[bstride + q] = X[q];
+    cl.sync();
+    int over = 0;
+    for (int r = 0; r < cs; r++) over |= s_overs[r];
+
+    // edge planes sent per sweep: own plane 1 to rank-1's upper halo (its local
+    // plane own(rank-1) + 1), own plane `own` to rank+1's lower halo (plane 0)
+    const uint32_t plane_bytes = (uint32_t) nk * 8u;
+    const uint32_t halo_bytes = plane_bytes * (uint32_t) ((rank > 0) + (rank < cs - 1));
+    uint32_t dst_lo = 0, dst_hi = 0, bar_lo = 0, bar_hi = 0;
+    if (tid == 0) {
+        if (rank > 0) {
+            const int own_lo = kb0 - sp.kb[rank - 1];
+            dst_lo = mapa_u32(base + (uint32_t) ((own_lo + 1) * nk) * 8u, rank - 1);
+            bar_lo = mapa_u32((uint32_t) __cvta_generic_to_shared(hb), rank - 1);
+        }
+        if (rank < cs - 1) {
+            dst_hi = mapa_u32(base, rank + 1);
+            bar_hi = mapa_u32((uint32_t) __cvta_generic_to_shared(hb), rank + 1);
+        }
+    }
+    unsigned par = 0;       // bit s: parity of the pending phase of hb[s]
+    long long unwaited = 0; // a phase whose halos were sent and not yet waited for (0: none)
+
+    double res = 10000.;
+    long long it = 0;
+    if (over) {
+        it = -1;  // target table too small or split violated: nothing computed, reported as an error
+    } else if (rel || (res > tol && it < max_it)) {
+        // phase k: iterate k from iterate k-1 (unless k-1 == max_it) and the
+        // residual of iterate k-1 (k >= 2, or k = 1 for the relative
+        // tolerance); iterate k-1 is accepted on entry
+        for (long long k = 1;; k++) {
+            const int sp_ = (int) ((k - 1) % 3), sn = (int) (k % 3);
+            const double *P = X + sp_ * bstride;
+            double *N = X + sn * bstride;
+            const bool sweep = k - 1 < max_it, resid = k >= 2 || rel;
+            if (unwaited) {
+                // halos of iterate k-1 (sent in phase k-1) must have landed
+                if (tid == 0) {
+                    if (!tc::mbar_wait(&hb[sp_], (par >> sp_) & 1u, kHaloPolls)) s_fail = 1;
+                    par ^= 1u << sp_;
+                }
+                unwaited = 0;
+                __syncthreads();
+            }
+            double acc = 0.0, v[kPipeCells];
+#pragma unroll
+            for (int m = 0; m < kPipeCells; m++) {
+                v[m] = 0.0;
+                if (!(m0 >> m & 1)) continue;
+                const int a = ca[m];
+                const double c0 = P[a], xm = P[a - 1], xp = P[a + 1], ym = P[a - nj], yp = P[a + nj],
+                             zm = P[a - nk], zp = P[a + nk];
+                if (resid) {
+                    const double rr = cb[m] - (rx * (xm - 2 * c0 + xp) + ry * (ym - 2 * c0 + yp) +
+                                               rz * (zm - 2 * c0 + zp));
+                    acc += rr * rr;
+                }
+                const double out_h = c.beta * (c.dsign * cb[m] + c.ax * (xp + xm) + c.ay * (yp + ym) + c.az * (zp + zm));
+                v[m] = c.omw * c0 + c.w * out_h;
+            }
+            bool reduced = false;
+            if (sweep) {
+#pragma unroll
+                for (int m = 0; m < kPipeCells; m++)
+                    if (m0 >> m & 1) N[ca[m]] = v[m];
+                if (resid) {
+                    // first stage of artss_block_sum, second stage below by warp 0
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                    if ((tid & 31) == 0) red[tid >> 5] = acc;
+                }
+                __syncthreads();  // the roots' new values are in N, the warp sums in red
+                if (resid && tid < 32) {
+                    acc = tid < kClusterThreads / 32 ? red[tid] : 0.0;
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+                    acc = __shfl_sync(0xffffffffu, acc, 0);
+                    if (tid < cs) cl.map_shared_rank(parts[k & 1], tid)[rank] = acc;
+                }
+                reduced = resid;
+                for (int t = tid; t < nt; t += kClusterThreads) {
+                    const HaloTarget &h = tg[t];
+                    double x = N[h.root];
+                    const int d = (int) (h.depth_neg & 0xffu);
+                    const uint32_t mneg = h.depth_neg >> 8;
+#pragma unroll
+                    for (int s = 0; s < kBcMaxDepth; s++)
+                        if (s < d) x = ((mneg >> s) & 1 ? -x : x) + h.val[s];
+                    N[h.dst] = x;
+                }
+                if (tid == 0) tc::mbar_expect_tx(&hb[sn], halo_bytes);  // this rank's incoming halos
+                __syncthreads();  // the edge planes are complete
+                if (tid == 0) {
+                    tc::fence_proxy_async();
+                    const uint32_t nb = base + (uint32_t) (sn * bstride) * 8u;
+                    if (rank > 0)
+                        bulk_copy_to_peer(dst_lo + (uint32_t) (sn * bstride) * 8u, nb + plane_bytes, plane_bytes,
+                                          bar_lo + (uint32_t) sn * 8u);
+                    if (rank < cs - 1)
+                        bulk_copy_to_peer(dst_hi + (uint32_t) (sn * bstride) * 8u, nb + (uint32_t) own * plane_bytes,
+                                          plane_bytes, bar_hi + (uint32_t) sn * 8u);
+                }
+                unwaited = k;
+            }
+            if (resid && !reduced) {
+                acc = artss_block_sum(acc, red);  // complete in thread 0
+                acc = __shfl_sync(0xffffffffu, acc, 0);
+                if (tid < cs) cl.map_shared_rank(parts[k & 1], tid)[rank] = acc;
+            }
+            cl.sync();
+            if (!resid) {
+                it = k;  // cond(0): res = 10000 > tol and 0 < max_it
+                continue;
+            }
+            double s = 0.0;
+            for (int r = 0; r < cs; r++) s += parts[k & 1][r];
+            if (k == 1) {
+                // relative tolerance: scaled by the residual of iterate 0
+                tol *= sqrt(s);
+                if (!(res > tol && 0 < max_it)) break;
+                it = 1;
+                continue;
+            }
+            res = sqrt(s);  // residual of iterate k-1
+            if (!(res > tol && k - 1 < max_it)) break;  // it = k-1 stands
+            it = k;
+        }
+    }
+    // the last halos sent must land before any rank leaves (their source and
+    // destination are shared memory)
+    if (unwaited && tid == 0) {
+        const int s = (int) (unwaited % 3);
+        if (!tc::mbar_wait(&hb[s], (par >> s) & 1u, kHaloPolls)) s_fail = 1;
+    }
+    // iterate `it` lives in buffer it%3, iterate it-1 in (it-1)%3 (it >= 1)
+    if (it >= 0) {
+        const double *Xo = X + (it % 3) * bstride, *Xt = Xo;
+        if (it >= 1) {
+            const double *Xprev = X + ((it - 1) % 3) * bstride;
+            if (it % 2 == 0) Xo = Xprev;
+            else Xt = Xprev;
+        }
+        for (int q = tid; q < own * nk; q += kClusterThreads) {
+            out[(int64_t) kb0 * nk + q] = (TS) Xo[nk + q];
+            if (tmp) tmp[(int64_t) kb0 * nk + q] = (TS) Xt[nk + q];
+        }
+    }
+    __syncthreads();
+    if (st && tid == 0 && (s_fail || it < 0)) st->pad = 1;
+    if (rank == 0 && tid == 0 && st) {
+        st->it = it < 0 ? 0 : it;
+        st->residual = res;
+        st->cond = 0;
+    }
+    cl.sync();
+}
+
 // Launch shape of the cluster coarse solve, or false when the level does not fit it.
 // ranks of the cluster for a level: one per z-plane up to kClusterSize
 inline int cluster_ranks(const Level &L) { return (int) std::min<int64_t>(kClusterSize, L.Nz); }
 
-bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int64_t *smem) {
+bool cluster_fits(const artss_ctx *ctx, int level, int buffers, int *plane_cap, int64_t *smem) {
     const Level &L = ctx->lvl[level];
     const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
     if (p.present && p.waves > kCoarseMaxWaves) return false;
@@ -608,11 +941,120 @@ bool cluster_fits(const artss_ctx *ctx, int level, bool cgs, int *plane_cap, int
         const int64_t cells = z1 >= z0 ? (z1 - z0 + 1) * (L.i2 - L.i1 + 1) * (L.j2 - L.j1 + 1) : 0;
         if (cells > (int64_t) kClusterThreads * kClusterCells) return false;
     }
-    const int64_t bytes = (cgs ? 1 : 2) * (int64_t) cap * L.nxy() * (int64_t) sizeof(double);
+    const int64_t bytes = buffers * (int64_t) cap * L.nxy() * (int64_t) sizeof(double);
     if (bytes > kCoarseSmemBytes) return false;
     *plane_cap = cap;
     *smem = bytes;
     return true;
+}
+
+// Launch data of k_mg_coarse_jacobi_pipe for the level, or false when its
+// pressure boundary program does not qualify (more than one wave, an inner
+// target, a chain leaving its target's neighbouring planes, no plane split
+// that keeps every inner root with its target) or the level does not fit.
+// The split cuts the planes as evenly as the forbidden cuts allow.
+struct PipeLaunch {
+    PlaneSplit split;
+    int ranks, plane_cap, target_cap;
+    int64_t smem;
+};
+
+bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl);
+
+bool coarse_pipe_plan(artss_ctx *ctx, int level, PipeLaunch *pl) {
+    BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    if (p.pipe_state == -2) {
+        PipeLaunch fresh{};
+        const bool ok = coarse_pipe_plan_new(ctx, level, &fresh);
+        p.pipe_state = ok ? 1 : -1;
+        if (ok) {
+            p.pipe_kb.assign(fresh.split.kb, fresh.split.kb + kPipeMaxRanks + 1);
+            p.pipe_ranks = fresh.ranks;
+            p.pipe_cap = fresh.plane_cap;
+            p.pipe_tcap = fresh.target_cap;
+            p.pipe_smem = fresh.smem;
+        }
+    }
+    if (p.pipe_state != 1) return false;
+    for (int r = 0; r <= kPipeMaxRanks; r++) pl->split.kb[r] = p.pipe_kb[r];
+    pl->ranks = p.pipe_ranks;
+    pl->plane_cap = p.pipe_cap;
+    pl->target_cap = p.pipe_tcap;
+    pl->smem = p.pipe_smem;
+    return true;
+}
+
+bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
+    BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    const Level &L = ctx->lvl[level];
+    const std::vector<bool> &in = ctx->h_inner[level];
+    const int nz = (int) L.Nz;
+    if (cluster_ranks(L) < 2 || L.nxy() % 2 || in.empty() || (int64_t) in.size() != L.size()) return false;
+    if (p.present && p.waves > 1) return false;
+    std::vector<char> forbidden(nz + 1, 0);  // forbidden[c]: no rank boundary between planes c-1 and c
+    const int64_t n = p.present ? p.n : 0;
+    for (int64_t q = 0; q < n; q++) {
+        const int64_t t = p.h_target[q], r = p.h_root[q];
+        const int kt = (int) (t / L.nxy()), kr = (int) (r / L.nxy());
+        if (in[(size_t) t] || kr < kt - 1 || kr > kt + 1) return false;
+        if (in[(size_t) r] && kr != kt) forbidden[std::max(kr, kt)] = 1;
+    }
+    // the most ranks (up to one per plane, at most kPipeMaxRanks) that admit a split
+    PlaneSplit sp{};
+    int cs = (int) std::min<int64_t>(kPipeMaxRanks, L.Nz);
+    for (; cs >= 2; cs--) {
+        bool ok = true;
+        sp = PlaneSplit{};
+        for (int r = 1; r < cs && ok; r++) {
+            const int ideal = (int) ((int64_t) r * nz / cs);
+            const int lo = sp.kb[r - 1] + 1, hi = nz - (cs - r);  // every rank keeps at least one plane
+            int best = -1;
+            for (int cut = lo; cut <= hi; cut++)
+                if (!forbidden[cut] && (best < 0 || std::abs(cut - ideal) < std::abs(best - ideal))) best = cut;
+            if (best < 0) ok = false;
+            else sp.kb[r] = best;
+        }
+        if (ok) break;
+    }
+    if (cs < 2) return false;
+    sp.kb[cs] = nz;
+    int cap = 0, tcap = 0;
+    const int64_t nxy_in = (L.i2 - L.i1 + 1) * (L.j2 - L.j1 + 1);
+    for (int r = 0; r < cs; r++) {
+        cap = std::max(cap, sp.kb[r + 1] - sp.kb[r]);
+        const int64_t z0 = std::max<int64_t>(sp.kb[r], L.k1), z1 = std::min<int64_t>(sp.kb[r + 1] - 1, L.k2);
+        if (z1 >= z0 && (z1 - z0 + 1) * nxy_in > (int64_t) kClusterThreads * kPipeCells) return false;
+        int nt = 0;
+        for (int64_t q = 0; q < n; q++) {
+            const int kt = (int) (p.h_target[q] / L.nxy());
+            if (kt >= sp.kb[r] && kt < sp.kb[r + 1] && in[(size_t) p.h_root[q]]) nt++;
+        }
+        tcap = std::max(tcap, nt);
+    }
+    const int64_t smem = 3 * (int64_t) (cap + 2) * L.nxy() * (int64_t) sizeof(double) +
+                         (int64_t) tcap * (int64_t) sizeof(HaloTarget);
+    if (smem > kCoarseSmemBytes) return false;
+    pl->split = sp;
+    pl->ranks = cs;
+    pl->plane_cap = cap;
+    pl->target_cap = tcap;
+    pl->smem = smem;
+    return true;
+}
+
+inline cudaLaunchConfig_t cluster_config(artss_ctx *ctx, int cs, int64_t smem, cudaLaunchAttribute *at) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(cs, 1, 1);
+    lc.blockDim = dim3(kClusterThreads, 1, 1);
+    lc.dynamicSmemBytes = (size_t) smem;
+    lc.stream = ctx->stream;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    return lc;
 }
 
 template <bool CGS, typename TS>
@@ -626,23 +1068,34 @@ int launch_coarse_cluster(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int lev
         attr_set = true;
     }
     const Level &L = ctx->lvl[level];
-    const int cs = cluster_ranks(L);
-    cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(cs, 1, 1);
-    lc.blockDim = dim3(kClusterThreads, 1, 1);
-    lc.dynamicSmemBytes = (size_t) smem;
-    lc.stream = ctx->stream;
     cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = cs;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    lc.attrs = at;
-    lc.numAttrs = 1;
+    cudaLaunchConfig_t lc = cluster_config(ctx, cluster_ranks(L), smem, at);
     ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_cluster<CGS, TS>, out, tmp, b,
                                                                   (const uint8_t *) ctx->d_flags[level], L,
                                                                   inner_box(L), c, rx, ry, rz, v, tol, rel, mi, cap,
                                                                   st, pred)));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+template <typename TS>
+int launch_coarse_pipe(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level, const MgCoef &c, double rx,
+                       double ry, double rz, const BcView &v, double tol, int rel, long long mi, const PipeLaunch &pl,
+                       LoopState *st, const LoopState *pred) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_jacobi_pipe<TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) kCoarseSmemBytes));
+        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_jacobi_pipe<TS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        attr_set = true;
+    }
+    const Level &L = ctx->lvl[level];
+    cudaLaunchAttribute at[1];
+    cudaLaunchConfig_t lc = cluster_config(ctx, pl.ranks, pl.smem, at);
+    ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_jacobi_pipe<TS>, out, tmp, b,
+                                                                  (const uint8_t *) ctx->d_flags[level], L,
+                                                                  inner_box(L), c, rx, ry, rz, v, tol, rel, mi,
+                                                                  pl.split, pl.plane_cap, pl.target_cap, st, pred)));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -666,7 +1119,9 @@ int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, in
     const bool cgs = smoother == ARTSS_SMOOTHER_CGS;
     int cap = 0;
     int64_t smem = 0;
-    if (!cluster_fits(ctx, level, cgs, &cap, &smem)) {
+    PipeLaunch pl{};
+    const bool pipe = !cgs && coarse_pipe_plan(ctx, level, &pl);
+    if (!pipe && !cluster_fits(ctx, level, cgs ? 1 : 2, &cap, &smem)) {
         set_error("the coarsest level does not fit the cluster coarse solve");
         return ARTSS_ERR_LIMIT;
     }
@@ -684,6 +1139,9 @@ int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, in
     if (cgs)
         return launch_coarse_cluster<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
                                                   cap, smem, nullptr, pred);
+    if (pipe)
+        return launch_coarse_pipe<float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it, pl, nullptr,
+                                         pred);
     return launch_coarse_cluster<false, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it, cap,
                                                smem, nullptr, pred);
 }
@@ -714,7 +1172,11 @@ int mg_coarse_solve(artss_mg *mg, double *out, double *tmp, const double *b, int
     const long long mi = mg->cfg.smoother_max_iter;
     int cap = 0;
     int64_t csmem = 0;
-    if (mg->cluster_coarse && cluster_fits(ctx, level, cgs, &cap, &csmem)) {
+    PipeLaunch pl{};
+    if (mg->cluster_coarse && !cgs && mg->pipelined_coarse && coarse_pipe_plan(ctx, level, &pl))
+        return launch_coarse_pipe<double>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, 0, mi, pl, ctx->d_loop + 1,
+                                          nullptr);
+    if (mg->cluster_coarse && cluster_fits(ctx, level, cgs ? 1 : 2, &cap, &csmem)) {
         if (cgs)
             return launch_coarse_cluster<true, double>(ctx, out, tmp, b, level, c, rx, ry, rz, v, tol, 0, mi, cap, csmem,
                                                        ctx->d_loop + 1, nullptr);
@@ -880,6 +1342,7 @@ int artss_mg_create(artss_ctx *ctx, const artss_mg_cfg *cfg, artss_mg **out) {
     mg->L = cfg->n_level;
     mg->fused_coarse = !(cfg->flags & ARTSS_MG_NO_FUSED_COARSE);
     mg->cluster_coarse = !(cfg->flags & ARTSS_MG_NO_CLUSTER_COARSE);
+    mg->pipelined_coarse = !(cfg->flags & ARTSS_MG_NO_PIPELINED_COARSE);
     int st = ARTSS_OK;
     // VCycleMG.cpp:51-99: level-0 r1/e1/tmp, levels 0..L-1 r0/e0, 1..L r1/e1/tmp
     st = st ? st : artss_field_alloc(ctx, 0, &mg->r1[0]);

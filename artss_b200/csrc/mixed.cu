@@ -408,7 +408,7 @@ int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed *
     if (!st) {
         int cap = 0;
         int64_t smem = 0;
-        if (!cluster_fits(ctx, m->L - 1, cfg->coarse_smoother == ARTSS_SMOOTHER_CGS, &cap, &smem)) {
+        if (!cluster_fits(ctx, m->L - 1, cfg->coarse_smoother == ARTSS_SMOOTHER_CGS ? 1 : 2, &cap, &smem)) {
             set_error("the coarsest level is too large for the cluster coarse solve; use more levels");
             st = ARTSS_ERR_LIMIT;
         }

@@ -100,6 +100,10 @@ enum artss_smoother { ARTSS_SMOOTHER_JACOBI = 0, ARTSS_SMOOTHER_CGS = 1 };
 /* keep the fused coarse solve in one thread block instead of spreading it
  * over a thread-block cluster (distributed shared memory); same results */
 #define ARTSS_MG_NO_CLUSTER_COARSE 2
+/* run the Jacobi coarse solve on the cluster with three cluster barriers per
+ * sweep (sweep, boundary program, residual) instead of the pipelined form
+ * with one; same results */
+#define ARTSS_MG_NO_PIPELINED_COARSE 4
 typedef struct {
     int32_t n_level;
     int32_t n_cycle;

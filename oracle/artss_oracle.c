@@ -294,6 +294,7 @@ struct oracle_mg {
     oracle_mg_cfg cfg;
     double *r0[ORACLE_MAX_LEVEL + 1], *r1[ORACLE_MAX_LEVEL + 1], *e0[ORACLE_MAX_LEVEL + 1];
     double *e1[ORACLE_MAX_LEVEL + 1], *tmp[ORACLE_MAX_LEVEL + 1];
+    int64_t last_coarse_it;  /* sweeps of the last coarse solve */
 };
 
 static double *zeros(const oracle_scene *s, int l) { return (double *) calloc((size_t) oracle_size(s, l), sizeof(double)); }
@@ -406,6 +407,7 @@ static void mg_solve(oracle_mg *mg, double *out, double *tmp, const double *b, i
             res = mg_resnorm(s, l, out, b);
             it++;
         }
+        mg->last_coarse_it = it;
         return;
     }
     memcpy(tmp, out, (size_t) oracle_size(s, l) * sizeof(double));
@@ -419,6 +421,7 @@ static void mg_solve(oracle_mg *mg, double *out, double *tmp, const double *b, i
         B = t;
         it++;
     }
+    mg->last_coarse_it = it;
 }
 
 /* VCycleMG::VCycleMultigrid (VCycleMG.cpp:215-288) with Residuum :319-360,
@@ -528,3 +531,5 @@ int64_t oracle_mg_pressure(oracle_mg *mg, double *p, const double *rhs, int firs
     if (residual) *residual = r;
     return cycles;
 }
+
+int64_t oracle_mg_last_coarse_iterations(const oracle_mg *mg) { return mg->last_coarse_it; }

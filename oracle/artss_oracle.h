@@ -83,6 +83,8 @@ typedef struct oracle_mg oracle_mg;
 oracle_mg *oracle_mg_create(const oracle_scene *s, const oracle_mg_cfg *cfg);
 void oracle_mg_destroy(oracle_mg *mg);
 int64_t oracle_mg_pressure(oracle_mg *mg, double *p, const double *rhs, int first_step, double *residual);
+/* sweeps of the last coarse-level solve (VCycleMG::Solve) */
+int64_t oracle_mg_last_coarse_iterations(const oracle_mg *mg);
 
 #ifdef __cplusplus
 }

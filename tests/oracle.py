@@ -72,6 +72,8 @@ def lib():
         L.oracle_mg_destroy.argtypes = [C.c_void_p]
         L.oracle_mg_pressure.argtypes = [C.c_void_p, _D, _D, C.c_int, _D]
         L.oracle_mg_pressure.restype = C.c_int64
+        L.oracle_mg_last_coarse_iterations.argtypes = [C.c_void_p]
+        L.oracle_mg_last_coarse_iterations.restype = C.c_int64
         _lib = L
     return _lib
 

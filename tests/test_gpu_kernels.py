@@ -151,9 +151,10 @@ def test_diffusion(env, method, turbulent, scratch):
     assert abs(stats.residual - res.value) <= 1e-12 * res.value
 
 
-# coarse solve: "cluster" = one thread-block cluster, "block" = one block,
-# "multi" = separate multi-block launches per sweep
-COARSE_FLAGS = {"cluster": 0, "block": 2, "multi": 1}
+# coarse solve: "cluster" = one thread-block cluster (Jacobi: pipelined, one
+# cluster barrier per sweep), "cluster3" = the cluster with three barriers per
+# sweep, "block" = one block, "multi" = separate multi-block launches per sweep
+COARSE_FLAGS = {"cluster": 0, "cluster3": 4, "block": 2, "multi": 1}
 
 
 @pytest.mark.parametrize("smoother", [0, 1])
@@ -180,6 +181,39 @@ def test_vcycle_mg(env, smoother, coarse, first_step):
         assert np.array_equal(ctx.download(dp), ref)
     finally:
         ctx.lib.artss_mg_destroy(mg)
+
+
+@pytest.mark.parametrize("coarse", ["cluster", "cluster3"])
+def test_coarse_solve_stops_early(env, coarse):
+    """Coarse solves that stop on the tolerance after odd and even sweep
+    counts: the reference leaves iterate it (odd) or it-1 (even) in out, and
+    the pipelined kernel decides one sweep late, so both parities must still
+    give the reference's pressure."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    p0, rhs = rnd(45, n), rnd(46, n)
+    seen = set()
+    # 1, 2, 3, 6, 13 and 23 sweeps on this scene, then the 200-sweep cap
+    for tol in (100.0, 30.0, 20.0, 10.0, 5.0, 3.0, 1e-30):
+        cfg = A.MgCfg(3, 1, 1, 2, 1e-30, 0, COARSE_FLAGS[coarse], 200, tol, 0.6666666667)
+        mg = C.c_void_p()
+        A.cuda_check(ctx.lib.artss_mg_create(ctx.h, C.byref(cfg), C.byref(mg)), "mg")
+        try:
+            dp, drhs = ctx.field(p0), ctx.field(rhs)
+            st = A.MgStats()
+            A.cuda_check(ctx.lib.artss_mg_pressure(mg, dp, drhs, 0, C.byref(st)), "pressure")
+            ocfg = oracle.MgCfg(3, 1, 1, 2, 1e-30, 0, 0, 200, tol, 0.6666666667)
+            om = oracle.lib().oracle_mg_create(osc.ptr, C.byref(ocfg))
+            ref = p0.copy()
+            res = C.c_double()
+            oracle.lib().oracle_mg_pressure(om, P(ref), P(rhs), 0, C.byref(res))
+            sweeps = oracle.lib().oracle_mg_last_coarse_iterations(om)
+            oracle.lib().oracle_mg_destroy(om)
+            seen.add(sweeps % 2)
+            assert np.array_equal(ctx.download(dp), ref), (tol, sweeps)
+        finally:
+            ctx.lib.artss_mg_destroy(mg)
+    assert seen == {0, 1}
 
 
 @pytest.mark.parametrize("scratch", [0, 1])
