@@ -457,14 +457,17 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     double *B = st_sm + kStSlotsX * kStPlane;   // [kStSlotsB][kStPlane]
     double *E = B + kStSlotsB * kStPlane;       // [kStSlotsB][kStPlane] (TURB)
     const int tid = threadIdx.x;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    const int64_t wx0 = box.x0 + (int64_t) blockIdx.x * kSwTx - 2;  // global i of ring column 0
-    const int64_t wxa = wx0 - (wx0 & 1);                             // TMA window start, even
-    const int ox = (int) (wx0 - wxa);
-    const int64_t wy0 = box.y0 + (int64_t) blockIdx.y * kSwTy - 2;
-    const int64_t kc0 = box.z0 + (int64_t) blockIdx.z * ZB;
-    const int64_t kc1 = min(kc0 + ZB - 1, box.z1);
-    const int64_t pbase = kc0 - 2, plast = kc1 + 2;  // staged planes
+    // 32-bit indices: the host takes this kernel only for levels of fewer than 2^31 cells
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    const int bx0 = (int) box.x0, bx1 = (int) box.x1, by0 = (int) box.y0, by1 = (int) box.y1;
+    const int bz0 = (int) box.z0, bz1 = (int) box.z1;
+    const int wx0 = bx0 + (int) blockIdx.x * kSwTx - 2;  // global i of ring column 0
+    const int wxa = wx0 - (wx0 & 1);                      // TMA window start, even
+    const int ox = wx0 - wxa;
+    const int wy0 = by0 + (int) blockIdx.y * kSwTy - 2;
+    const int kc0 = bz0 + (int) blockIdx.z * ZB;
+    const int kc1 = min(kc0 + ZB - 1, bz1);
+    const int pbase = kc0 - 2, plast = kc1 + 2;  // staged planes
 
     if (tid == 0) {
         for (int s = 0; s < kStSlotsX; s++) mbar_init(&bars[s], 1);
@@ -472,22 +475,22 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     }
     __syncthreads();
     // thread 0: load plane p into its slots
-    auto issue = [&](int64_t p) {
+    auto issue = [&](int p) {
         if (p > plast) return;
         const unsigned u = (unsigned) (p - pbase);
         uint64_t *bar = &bars[u % kStSlotsX];
         mbar_expect_tx(bar, kStPlaneBytes * (TURB ? 3u : 2u));
-        tma_load_plane(X + (u % kStSlotsX) * kStPlane, &tm_x, (int) wxa, (int) wy0, (int) p, bar);
-        tma_load_plane(B + (u % kStSlotsB) * kStPlane, &tm_b, (int) wxa, (int) wy0, (int) p, bar);
-        if (TURB) tma_load_plane(E + (u % kStSlotsB) * kStPlane, &tm_e, (int) wxa, (int) wy0, (int) p, bar);
+        tma_load_plane(X + (u % kStSlotsX) * kStPlane, &tm_x, wxa, wy0, p, bar);
+        tma_load_plane(B + (u % kStSlotsB) * kStPlane, &tm_b, wxa, wy0, p, bar);
+        if (TURB) tma_load_plane(E + (u % kStSlotsB) * kStPlane, &tm_e, wxa, wy0, p, bar);
     };
-    auto ready = [&](int64_t p) -> bool {
+    auto ready = [&](int p) -> bool {
         const unsigned u = (unsigned) (p - pbase);
         return mbar_wait(&bars[u % kStSlotsX], (u / kStSlotsX) & 1u, kStPolls);
     };
     // ring slots by local plane number (32-bit, constant divisors)
-    auto xslot = [&](int64_t p) { return X + ((unsigned) (p - pbase) % (unsigned) kStSlotsX) * kStPlane; };
-    auto bslot = [&](int64_t p) { return (int) (((unsigned) (p - pbase) % (unsigned) kStSlotsB) * kStPlane); };
+    auto xslot = [&](int p) { return X + ((unsigned) (p - pbase) % (unsigned) kStSlotsX) * kStPlane; };
+    auto bslot = [&](int p) { return (int) (((unsigned) (p - pbase) % (unsigned) kStSlotsB) * kStPlane); };
     auto update = [&](const double *xm, const double *x0, const double *xp, int e, int bo, double &res2) {
         double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
         if (TURB) {
@@ -505,42 +508,43 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
 
     // this thread's red x-pair (tile + ring) and black x-pair (tile)
     const int ry = 1 + tid / ((kSwTx + 2) / 2), px = tid % ((kSwTx + 2) / 2);
-    const int64_t gjr = wy0 + ry;
-    const bool red_row_ok = gjr >= box.y0 && gjr <= box.y1;
-    const int64_t red_row = nj * gjr;
+    const int gjr = wy0 + ry;
+    const bool red_row_ok = gjr >= by0 && gjr <= by1;
+    const int red_row = nj * gjr;
     const bool red_tile = ry >= 2 && ry < kSwTy + 2;
     const bool has_black = tid < (kSwTx / 2) * kSwTy;
     const int tx = tid % (kSwTx / 2), ty = tid / (kSwTx / 2);
-    const int64_t gjb = wy0 + 2 + ty;
-    const int64_t black_row = nj * gjb;
+    const int gjb = wy0 + 2 + ty;
+    const int black_row = nj * gjb;
     const int lx0 = 2 + 2 * tx;
-    auto red_x = [&](int64_t k) { return 1 + 2 * px + (int) ((wx0 + 1 + gjr + k) & 1); };  // (i + j + k) even
-    auto red_flag = [&](int64_t k) -> uint8_t {
-        if (!red_row_ok || k < box.z0 || k > box.z1) return 0;
-        const int64_t gi = wx0 + red_x(k);
-        if (gi < box.x0 || gi > box.x1) return 0;
+    auto red_x = [&](int k) { return 1 + 2 * px + ((wx0 + 1 + gjr + k) & 1); };  // (i + j + k) even
+    auto red_flag = [&](int k) -> uint8_t {
+        if (!red_row_ok || k < bz0 || k > bz1) return 0;
+        const int gi = wx0 + red_x(k);
+        if (gi < bx0 || gi > bx1) return 0;
         return __ldg(flags + gi + red_row + nk * k);
     };
-    auto black_par = [&](int64_t kb) { return (int) ((wx0 + lx0 + gjb + kb + 1) & 1); };  // (i + j + k) odd
-    auto black_flag = [&](int64_t kb) -> uint8_t {
-        if (!has_black || gjb > box.y1 || kb < kc0 || kb > kc1) return 0;
-        const int64_t gi = wx0 + lx0 + black_par(kb);
-        if (gi > box.x1) return 0;
+    auto black_par = [&](int kb) { return (wx0 + lx0 + gjb + kb + 1) & 1; };  // (i + j + k) odd
+    auto black_flag = [&](int kb) -> uint8_t {
+        if (!has_black || gjb > by1 || kb < kc0 || kb > kc1) return 0;
+        const int gi = wx0 + lx0 + black_par(kb);
+        if (gi > bx1) return 0;
         return __ldg(flags + gi + black_row + nk * kb);
     };
 
     double acc = 0.0;
-    int64_t issued = kc0 - 1 + kSwD;  // thread 0's last issued plane
+    int issued = kc0 - 1 + kSwD;  // thread 0's last issued plane
     if (tid == 0)
-        for (int64_t p = pbase; p <= issued; p++) issue(p);
-    bool ok = ready(pbase) && ready(pbase + 1);
+        for (int p = pbase; p <= issued; p++) issue(p);
+    bool ok = tid != 0 || (ready(pbase) && ready(pbase + 1));
     uint8_t fr = red_flag(kc0 - 1), fb = black_flag(kc0 - 2);
     bool failed = false;
-    int64_t waited = pbase + 1;  // planes up to here have landed
-    for (int64_t k = kc0 - 1; k <= kc1 + 1; k++) {
+    int waited = pbase + 1;  // planes up to here have landed
+    for (int k = kc0 - 1; k <= kc1 + 1; k++) {
         // the next step's flags, loaded early
         const uint8_t fr_next = red_flag(k + 1), fb_next = black_flag(k);
-        ok = ok && ready(k + 1);
+        // thread 0 waits for plane k+1; the barrier below publishes it to the block
+        if (tid == 0) ok = ok && ready(k + 1);
         fence_proxy_async();  // this thread's shared-memory writes before the slot refill below
         if (__syncthreads_or(!ok)) {
             failed = true;
@@ -563,15 +567,15 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
         }
         __syncthreads();
         // black on plane k-1, tile only, and the tile's plane k-1 out
-        const int64_t kb = k - 1;
-        if (has_black && kb >= kc0 && kb <= kc1 && gjb <= box.y1) {
+        const int kb = k - 1;
+        if (has_black && kb >= kc0 && kb <= kc1 && gjb <= by1) {
             const double *x0 = xslot(kb);
             const int par = black_par(kb);
             const int e0 = lx0 + ox + kTmaBoxX * (2 + ty);
 #pragma unroll
             for (int s = 0; s < 2; s++) {
-                const int64_t gi = wx0 + lx0 + s;
-                if (gi > box.x1) continue;
+                const int gi = wx0 + lx0 + s;
+                if (gi > bx1) continue;
                 double v = x0[e0 + s];
                 if (s == par && (fb & kInner)) {
                     double r2;
@@ -588,7 +592,7 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
         // a plane never arrived: flag it, let the loads in flight land, leave
         if (tid == 0) {
             if (pred) *(volatile int *) &pred->pad = 1;
-            for (int64_t p = waited + 1; p <= issued; p++) (void) ready(p);
+            for (int p = waited + 1; p <= issued; p++) (void) ready(p);
         }
         __syncthreads();
         return;
@@ -898,7 +902,7 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     if ((st = check_reduce_blocks(sweep_tma_grid(box, kStDepths[0])))) return st;
     int nb = nblocks(g);
     // TMA plane staging where the row pitch allows it, cp.async otherwise
-    const bool tma = tma_level_ok(ctx, 0);
+    const bool tma = tma_level_ok(ctx, 0) && L.size() < ((int64_t) 1 << 31);
     const size_t smem = tma ? sweep_tma_smem(ev != nullptr) : sweep_smem(ev != nullptr);
     if (tma) {
         if ((st = set_sweep_smem(ev != nullptr, smem))) return st;
