@@ -121,6 +121,8 @@ def load_cuda() -> C.CDLL:
             "artss_field_size": ([_P, C.c_int], C.c_int64),
             "artss_upload": ([_P, _D, _D, C.c_int64], C.c_int),
             "artss_download": ([_P, _D, _D, C.c_int64], C.c_int),
+            "artss_upload_async": ([_P, _D, _D, C.c_int64], C.c_int),
+            "artss_download_async": ([_P, _D, _D, C.c_int64], C.c_int),
             "artss_set_cell_lists": ([_P, C.c_int, _I64P, C.c_int64, _I64P, C.c_int64], C.c_int),
             "artss_get_cell_flags": ([_P, C.c_int, C.POINTER(C.c_uint8), C.c_int64], C.c_int),
             "artss_set_boundary_program": ([_P, C.c_int, C.c_int, C.POINTER(BcAssign), C.c_int64], C.c_int),

@@ -281,6 +281,18 @@ int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n) {
     return ARTSS_OK;
 }
 
+int artss_upload_async(artss_ctx *ctx, double *dst, const double *host, int64_t n) {
+    if (!ctx || !dst || !host || n < 0) { set_error("bad upload arguments"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    return ARTSS_OK;
+}
+
+int artss_download_async(artss_ctx *ctx, double *host, const double *src, int64_t n) {
+    if (!ctx || !src || !host || n < 0) { set_error("bad download arguments"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return ARTSS_OK;
+}
+
 int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_t n_inner,
                          const int64_t *domain, int64_t n_domain) {
     int st = check_level(ctx, level);

@@ -246,26 +246,27 @@ def run_b200(args, dist):
     dom_launches, dom_ms = int(L[dom]), float(M[dom])
     cuda.artss_ctx_profile(ctx, 0)
 
-    # end to end: state from pinned host memory in, state back out, every step
-    pinned_in = {f: torch.from_numpy(sim.field(f)).pin_memory() for f in STATE_FIELDS}
-    pinned_out = {f: torch.empty(size, dtype=torch.float64).pin_memory() for f in STATE_FIELDS}
+    # end to end: every step uploads the state from page-locked host memory,
+    # runs one timestep and reads the state back into the other host buffer,
+    # which feeds the next step; copies are ordered on the simulation's stream
+    pinned = [{f: torch.from_numpy(sim.field(f)).pin_memory() for f in STATE_FIELDS},
+              {f: torch.empty(size, dtype=torch.float64).pin_memory() for f in STATE_FIELDS}]
     dev = {f: C.cast(C.c_void_p(sim.device_pointer(f)), C.POINTER(C.c_double)) for f in STATE_FIELDS}
     hp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
     dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.e2e_steps):
+    for s_ in range(args.e2e_steps):
+        src, dst = pinned[s_ & 1], pinned[(s_ + 1) & 1]
         for f in STATE_FIELDS:
-            A.cuda_check(cuda.artss_upload(ctx, dev[f], hp(pinned_in[f]), size), "upload")
+            A.cuda_check(cuda.artss_upload_async(ctx, dev[f], hp(src[f]), size), "upload")
         sim.run(1)
         for f in STATE_FIELDS:
-            A.cuda_check(cuda.artss_download(ctx, hp(pinned_out[f]), dev[f], size), "download")
-        for f in STATE_FIELDS:
-            pinned_in[f].copy_(pinned_out[f])
+            A.cuda_check(cuda.artss_download_async(ctx, hp(dst[f]), dev[f], size), "download")
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if not np.isfinite(pinned_out["T"].numpy()).all():
+    if not np.isfinite(pinned[args.e2e_steps & 1]["T"].numpy()).all():
         raise RuntimeError("non-finite temperature after the end-to-end steps")
 
     ms_max = dist.max(ms)

@@ -159,6 +159,12 @@ int64_t artss_field_size(artss_ctx *ctx, int level);
 /* Field::update_dev / update_host (src/field/Field.h:41-49). */
 int artss_upload(artss_ctx *ctx, double *dst, const double *host, int64_t n);
 int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
+/* The same copies ordered on the context's stream without waiting for them:
+ * the copy runs after the work already enqueued and before any later work of
+ * the context; `host` must stay valid (and, for overlap, be page-locked) until
+ * then.  Field::update_dev / update_host with async = true. */
+int artss_upload_async(artss_ctx *ctx, double *dst, const double *host, int64_t n);
+int artss_download_async(artss_ctx *ctx, double *host, const double *src, int64_t n);
 
 /* ------------------------------------------------------------------ */
 /* geometry: GPU lists -> device cell flags and boundary programs     */
