@@ -209,6 +209,8 @@ def load_host() -> C.CDLL:
             "artss_sim_create": ([C.c_char_p, C.c_int, C.POINTER(_P)], C.c_int),
             "artss_sim_destroy": ([_P], None),
             "artss_sim_run": ([_P, C.c_int64, _I64P], C.c_int),
+            "artss_sim_step_io": ([_P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_D), C.c_int,
+                                   C.POINTER(C.c_char_p), C.POINTER(_D)], C.c_int),
             "artss_sim_finished": ([_P], C.c_int),
             "artss_sim_time": ([_P], C.c_double),
             "artss_sim_step_index": ([_P], C.c_int64),
@@ -328,6 +330,20 @@ class Simulation:
         done = C.c_int64()
         _host_check(self._lib.artss_sim_run(self._h, steps, C.byref(done)), "run")
         return done.value
+
+    def step_io(self, inputs: Dict[str, int], outputs: Dict[str, int]) -> None:
+        """One timestep with host transfers overlapped with it: `inputs` and
+        `outputs` map field names to host addresses of Nx*Ny*Nz doubles
+        (page-locked for overlap); inputs are set before they are read,
+        outputs read back after their last write of the step."""
+        names_in = [k.encode() for k in inputs]
+        names_out = [k.encode() for k in outputs]
+        a_in = (C.c_char_p * len(names_in))(*names_in)
+        a_out = (C.c_char_p * len(names_out))(*names_out)
+        p_in = (_D * len(inputs))(*[C.cast(C.c_void_p(v), _D) for v in inputs.values()])
+        p_out = (_D * len(outputs))(*[C.cast(C.c_void_p(v), _D) for v in outputs.values()])
+        _host_check(self._lib.artss_sim_step_io(self._h, len(names_in), a_in, p_in, len(names_out), a_out, p_out),
+                    "step_io")
 
     @property
     def finished(self) -> bool:

@@ -220,6 +220,13 @@ int artss_ctx_destroy(artss_ctx *ctx) {
     for (auto &pe : ctx->prof.pending) cudaEventDestroy(pe.first);
     for (auto e : ctx->prof.events) cudaEventDestroy(e);
     for (auto e : ctx->prof.pool) cudaEventDestroy(e);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        for (auto e : ctx->copy_ev) cudaEventDestroy(e);
+        cudaEventDestroy(ctx->copy_mark);
+        cudaEventDestroy(ctx->copy_tail);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_loop);
     if (ctx->h_loop) cudaFreeHost(ctx->h_loop);
@@ -290,6 +297,63 @@ int artss_upload_async(artss_ctx *ctx, double *dst, const double *host, int64_t 
 int artss_download_async(artss_ctx *ctx, double *host, const double *src, int64_t n) {
     if (!ctx || !src || !host || n < 0) { set_error("bad download arguments"); return ARTSS_ERR_ARG; }
     ARTSS_CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    return ARTSS_OK;
+}
+
+namespace {
+// the copy stream and its events, created on first use
+int copy_stream_ready(artss_ctx *ctx) {
+    if (ctx->copy_stream) return ARTSS_OK;
+    ARTSS_CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    for (auto &e : ctx->copy_ev) ARTSS_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ARTSS_CK(cudaEventCreateWithFlags(&ctx->copy_mark, cudaEventDisableTiming));
+    ARTSS_CK(cudaEventCreateWithFlags(&ctx->copy_tail, cudaEventDisableTiming));
+    return ARTSS_OK;
+}
+// the copy stream continues after the main stream's work enqueued so far
+int copy_after_main(artss_ctx *ctx) {
+    int st = copy_stream_ready(ctx);
+    if (st) return st;
+    ARTSS_CK(cudaEventRecord(ctx->copy_mark, ctx->stream));
+    ARTSS_CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_mark, 0));
+    return ARTSS_OK;
+}
+}  // namespace
+
+int artss_copy_upload(artss_ctx *ctx, int slot, double *dst, const double *host, int64_t n) {
+    if (!ctx || !dst || !host || n < 0 || slot < 0 || slot >= kCopySlots) {
+        set_error("bad copy upload arguments");
+        return ARTSS_ERR_ARG;
+    }
+    int st = copy_after_main(ctx);
+    if (st) return st;
+    ARTSS_CK(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->copy_stream));
+    ARTSS_CK(cudaEventRecord(ctx->copy_ev[slot], ctx->copy_stream));
+    return ARTSS_OK;
+}
+
+int artss_copy_wait(artss_ctx *ctx, int slot) {
+    if (!ctx || slot < 0 || slot >= kCopySlots || !ctx->copy_stream) {
+        set_error("bad copy wait arguments");
+        return ARTSS_ERR_ARG;
+    }
+    ARTSS_CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_ev[slot], 0));
+    return ARTSS_OK;
+}
+
+int artss_copy_download(artss_ctx *ctx, double *host, const double *src, int64_t n) {
+    if (!ctx || !src || !host || n < 0) { set_error("bad copy download arguments"); return ARTSS_ERR_ARG; }
+    int st = copy_after_main(ctx);
+    if (st) return st;
+    ARTSS_CK(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->copy_stream));
+    return ARTSS_OK;
+}
+
+int artss_copy_join(artss_ctx *ctx) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (!ctx->copy_stream) return ARTSS_OK;
+    ARTSS_CK(cudaEventRecord(ctx->copy_tail, ctx->copy_stream));
+    ARTSS_CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_tail, 0));
     return ARTSS_OK;
 }
 

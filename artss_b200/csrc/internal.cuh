@@ -18,6 +18,7 @@ namespace artss {
 
 constexpr int kMaxLevel = ARTSS_MAX_LEVEL;
 constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
+constexpr int kCopySlots = 8;           // uploads on the copy stream waited for by slot
 constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
 constexpr int kReduceThreads = 256;
 constexpr int kMaxPartials = 1 << 16;   // per-block partial sums of up to two reduction passes
@@ -118,6 +119,11 @@ struct artss_ctx {
     std::map<std::pair<const void *, int>, CUtensorMap> tmaps;  // TMA descriptors per (array, level)
     bool autotune = true;                                        // time kernel variants on first use
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
+    // host transfers overlapped with the step: a second stream, completion
+    // events of its uploads by slot, a mark of the main stream, its tail
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev[artss::kCopySlots]{};
+    cudaEvent_t copy_mark = nullptr, copy_tail = nullptr;
     int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},
                                {1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1}};
 };

@@ -109,3 +109,41 @@ void Field::from_host(const std::vector<real> &v) {
 }
 
 }  // namespace artss
+
+namespace artss {
+
+void StepIO::upload_late(Field &f, const real *host) {
+    const int slot = (int) m_in.size();
+    if (slot >= 8) throw std::invalid_argument("at most 8 inputs are uploaded during a step");
+    check(artss_copy_upload(m_ctx, slot, f.data, host, (int64_t) f.get_size()), "upload");
+    m_in.push_back({&f, host, slot, false});
+}
+
+bool StepIO::need(Field &f) {
+    bool found = false;
+    for (In &i : m_in)
+        if (i.f == &f && !i.waited) {
+            check(artss_copy_wait(m_ctx, i.slot), "upload wait");
+            i.waited = true;
+            found = true;
+        }
+    return found;
+}
+
+void StepIO::done(Field &f) {
+    for (Out &o : m_out)
+        if (o.f == &f && !o.sent) {
+            check(artss_copy_download(m_ctx, o.host, f.data, (int64_t) f.get_size()), "download");
+            o.sent = true;
+        }
+}
+
+void StepIO::finish() {
+    for (In &i : m_in)
+        if (!i.waited) need(*i.f);
+    for (Out &o : m_out)
+        if (!o.sent) done(*o.f);
+    check(artss_copy_join(m_ctx), "transfers");
+}
+
+}  // namespace artss

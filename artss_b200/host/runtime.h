@@ -61,6 +61,38 @@ class Field {
     real *m_owned = nullptr;
 };
 
+// Host transfers of one timestep overlapped with its computation (the
+// context's second stream): inputs a solver reads late are uploaded there
+// while the step runs and waited for at their first use (need); outputs are
+// read back as soon as the solver has written them for the last time (done).
+// Solvers without these calls get every input before and every output after
+// the step.
+class StepIO {
+ public:
+    struct In {
+        Field *f;
+        const real *host;
+        int slot;
+        bool waited;
+    };
+    struct Out {
+        Field *f;
+        real *host;
+        bool sent;
+    };
+    explicit StepIO(artss_ctx *ctx) : m_ctx(ctx) {}
+    void upload_late(Field &f, const real *host);  // on the second stream, after the uploads before it
+    bool need(Field &f);                           // the step's later work waits for f's upload (true: f was uploaded)
+    void add_output(Field &f, real *host) { m_out.push_back({&f, host, false}); }
+    void done(Field &f);                           // f's value is final: read it back beside later work
+    void finish();                                 // the rest, then the context waits for the transfers
+
+ private:
+    artss_ctx *m_ctx;
+    std::vector<In> m_in;
+    std::vector<Out> m_out;
+};
+
 class Runtime {
  public:
     Runtime(const settings::Settings &s, int device);
@@ -76,6 +108,9 @@ class Runtime {
 
     // DomainController::apply_boundary
     void apply_boundary(Field &f) const;
+
+    // transfers of the running step, when it runs through TimeIntegration::step_io
+    StepIO *io = nullptr;
 
  private:
     settings::Settings m_settings;

@@ -193,10 +193,17 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
 
     // 4. pressure and projection (:167-176)
     pres->divergence(f.rhs, f.u_tmp, f.v_tmp, f.w_tmp, sync);
+    if (m_rt.io) m_rt.io->need(f.p);
     pres->pressure(f.p, f.rhs, t, sync);
     stats.pressure_cycles = pres->last_cycles;
     stats.pressure_residual = pres->last_residual;
     pres->projection(f.u, f.v, f.w, f.u_tmp, f.v_tmp, f.w_tmp, f.p, sync);
+    if (m_rt.io) {
+        // u, v, w and p are final for this step; an uploaded T is the state
+        // the temperature step advances (its copies follow, as after a step)
+        for (Field *x : {&f.u, &f.v, &f.w, &f.p}) m_rt.io->done(*x);
+        if (m_rt.io->need(f.T)) FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
+    }
 
     // 5. temperature (:184-240)
     adv_temp->advect(f.T, f.T0, f.u, f.v, f.w, sync);
@@ -548,6 +555,39 @@ TimeIntegration::TimeIntegration(Runtime &rt, SolverController &sc)
     : m_rt(rt), m_sc(sc), m_dt(rt.settings().physical.dt), m_t_end(rt.settings().physical.t_end), m_t_cur(m_dt) {}
 
 bool TimeIntegration::finished() const { return !(m_t_cur < m_t_end + m_dt / 2); }
+
+void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>> &in,
+                              const std::vector<std::pair<Field *, real *>> &out) {
+    if (finished()) throw std::invalid_argument("the simulation has reached t_end");
+    StepIO io(m_rt.ctx());
+    // NSTempTurbSolver / NSTempSolver read p and T late: those arrive on the
+    // second stream during the step; the rest before it
+    const bool late_ok = dynamic_cast<NSTempTurbSolver *>(&m_sc.solver()) != nullptr;
+    FieldController &fc = m_sc.fields();
+    bool vel = false, temp_now = false;
+    for (const auto &i : in) {
+        if (late_ok && (i.first == &fc.p || i.first == &fc.T)) continue;
+        check(artss_upload_async(m_rt.ctx(), i.first->data, i.second, (int64_t) i.first->get_size()), "upload");
+        vel = vel || i.first == &fc.u || i.first == &fc.v || i.first == &fc.w;
+        temp_now = temp_now || i.first == &fc.T;
+    }
+    // uploaded u, v, w (T) are the state the step advances: their copies
+    // follow, as FieldController::update_data sets them after a step
+    if (vel) FieldController::couple_vector(fc.u, fc.u0, fc.u_tmp, fc.v, fc.v0, fc.v_tmp, fc.w, fc.w0, fc.w_tmp);
+    if (temp_now) FieldController::couple_scalar(fc.T, fc.T0, fc.T_tmp);
+    for (const auto &i : in)
+        if (late_ok && (i.first == &fc.p || i.first == &fc.T)) io.upload_late(*i.first, i.second);
+    for (const auto &o : out) io.add_output(*o.first, o.second);
+    m_rt.io = &io;
+    try {
+        run(1);
+    } catch (...) {
+        m_rt.io = nullptr;
+        throw;
+    }
+    m_rt.io = nullptr;
+    io.finish();
+}
 
 int64_t TimeIntegration::run(int64_t steps) {
     int64_t done = 0;

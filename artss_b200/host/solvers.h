@@ -153,6 +153,12 @@ class TimeIntegration {
     TimeIntegration(Runtime &rt, SolverController &sc);
     // runs until t_end (steps < 0) or for `steps` steps; returns steps run
     int64_t run(int64_t steps = -1);
+    // one step with its host transfers: the inputs are uploaded into their
+    // fields, the outputs read back, overlapped with the step where the
+    // solver marks first uses and final writes (StepIO); the transfers are
+    // complete when the context's stream reaches them
+    void step_io(const std::vector<std::pair<Field *, const real *>> &in,
+                 const std::vector<std::pair<Field *, real *>> &out);
     real time() const { return m_t_cur; }
     int64_t step_index() const { return m_step; }
     bool finished() const;

@@ -251,18 +251,14 @@ def run_b200(args, dist):
     # which feeds the next step; copies are ordered on the simulation's stream
     pinned = [{f: torch.from_numpy(sim.field(f)).pin_memory() for f in STATE_FIELDS},
               {f: torch.empty(size, dtype=torch.float64).pin_memory() for f in STATE_FIELDS}]
-    dev = {f: C.cast(C.c_void_p(sim.device_pointer(f)), C.POINTER(C.c_double)) for f in STATE_FIELDS}
-    hp = lambda t: C.cast(C.c_void_p(t.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
     dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
     for s_ in range(args.e2e_steps):
         src, dst = pinned[s_ & 1], pinned[(s_ + 1) & 1]
-        for f in STATE_FIELDS:
-            A.cuda_check(cuda.artss_upload_async(ctx, dev[f], hp(src[f]), size), "upload")
-        sim.run(1)
-        for f in STATE_FIELDS:
-            A.cuda_check(cuda.artss_download_async(ctx, hp(dst[f]), dev[f], size), "download")
+        # the public step-with-transfers call: p and T arrive while the
+        # velocity is computed, u, v, w, p leave while T is
+        sim.step_io({f: src[f].data_ptr() for f in STATE_FIELDS}, {f: dst[f].data_ptr() for f in STATE_FIELDS})
     e1.record(stream)
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
@@ -297,7 +293,9 @@ def run_b200(args, dist):
         "e2e": {"value": e2e_cells_all / (e2e_ms_max * 1e-3), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": len(STATE_FIELDS) * size * 8,
                 "d2h_bytes_per_step": len(STATE_FIELDS) * size * 8,
-                "what": "per step: u,v,w,p,T uploaded from pinned host memory, one timestep, u,v,w,p,T read back"},
+                "what": "per step through Simulation.step_io (artss_sim_step_io): u,v,w,p,T uploaded from page-locked host "
+                        "memory as the state the step advances (p and T while the velocity is computed), one "
+                        "timestep, u,v,w,p,T read back (u,v,w,p while the temperature is computed)"},
         "gpu_launches": int(gpu_launches),
         "roofline": {"bound": "hbm", "kernel": fam, "achieved": achieved, "peak": hbm,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,

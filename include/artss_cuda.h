@@ -165,6 +165,16 @@ int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
  * then.  Field::update_dev / update_host with async = true. */
 int artss_upload_async(artss_ctx *ctx, double *dst, const double *host, int64_t n);
 int artss_download_async(artss_ctx *ctx, double *host, const double *src, int64_t n);
+/* Host transfers overlapped with computation, on a second stream of the
+ * context.  artss_copy_upload starts after the work enqueued on the context
+ * so far and marks its completion in `slot` (0..7); artss_copy_wait makes the
+ * context's later work wait for that slot.  artss_copy_download starts after
+ * the work enqueued so far and runs beside later work; artss_copy_join makes
+ * the context's later work wait for every transfer of the second stream. */
+int artss_copy_upload(artss_ctx *ctx, int slot, double *dst, const double *host, int64_t n);
+int artss_copy_wait(artss_ctx *ctx, int slot);
+int artss_copy_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
+int artss_copy_join(artss_ctx *ctx);
 
 /* ------------------------------------------------------------------ */
 /* geometry: GPU lists -> device cell flags and boundary programs     */

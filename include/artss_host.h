@@ -47,6 +47,17 @@ int artss_sim_create(const char *xml_path, int device, artss_sim **out);
 void artss_sim_destroy(artss_sim *s);
 /* runs up to `steps` timesteps (all remaining when steps < 0); *done = steps run */
 int artss_sim_run(artss_sim *s, int64_t steps, int64_t *done);
+/* One timestep with its host transfers: the n_in named fields are set from
+ * in_host[k] before they are read, the n_out named fields are read into
+ * out_host[k] after their last write; transfers run beside the step where
+ * the solver allows (NSTempTurbSolver / NSTempSolver: p and T arrive while
+ * the velocity is computed, u, v, w, p leave while T is).  Inputs u, v, w
+ * and T are the state the step advances: their copies (u0, u_tmp, ..., T0,
+ * T_tmp) are set from them, as FieldController::update_data sets them after
+ * a step.  Buffers should be page-locked; they are complete when the call
+ * returns. */
+int artss_sim_step_io(artss_sim *s, int n_in, const char *const *in_names, const double *const *in_host, int n_out,
+                      const char *const *out_names, double *const *out_host);
 int artss_sim_finished(artss_sim *s);
 double artss_sim_time(artss_sim *s);
 int64_t artss_sim_step_index(artss_sim *s);
