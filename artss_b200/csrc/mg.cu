@@ -999,12 +999,23 @@ bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
         if (in[(size_t) t] || kr < kt - 1 || kr > kt + 1) return false;
         if (in[(size_t) r] && kr != kt) forbidden[std::max(kr, kt)] = 1;
     }
-    // the most ranks (up to one per plane, at most kPipeMaxRanks) that admit a split
-    PlaneSplit sp{};
-    int cs = (int) std::min<int64_t>(kPipeMaxRanks, L.Nz);
-    for (; cs >= 2; cs--) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(k_mg_coarse_jacobi_pipe<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) kCoarseSmemBytes) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mg_coarse_jacobi_pipe<double>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        attr_set = true;
+    }
+    // the most ranks (up to one per plane, at most kPipeMaxRanks) that admit a
+    // split, fit the rank's cell slots and shared memory and can be placed
+    const int64_t nxy_in = (L.i2 - L.i1 + 1) * (L.j2 - L.j1 + 1);
+    for (int cs = (int) std::min<int64_t>(kPipeMaxRanks, L.Nz); cs >= 2; cs--) {
+        PlaneSplit sp{};
         bool ok = true;
-        sp = PlaneSplit{};
         for (int r = 1; r < cs && ok; r++) {
             const int ideal = (int) ((int64_t) r * nz / cs);
             const int lo = sp.kb[r - 1] + 1, hi = nz - (cs - r);  // every rank keeps at least one plane
@@ -1014,32 +1025,49 @@ bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
             if (best < 0) ok = false;
             else sp.kb[r] = best;
         }
-        if (ok) break;
-    }
-    if (cs < 2) return false;
-    sp.kb[cs] = nz;
-    int cap = 0, tcap = 0;
-    const int64_t nxy_in = (L.i2 - L.i1 + 1) * (L.j2 - L.j1 + 1);
-    for (int r = 0; r < cs; r++) {
-        cap = std::max(cap, sp.kb[r + 1] - sp.kb[r]);
-        const int64_t z0 = std::max<int64_t>(sp.kb[r], L.k1), z1 = std::min<int64_t>(sp.kb[r + 1] - 1, L.k2);
-        if (z1 >= z0 && (z1 - z0 + 1) * nxy_in > (int64_t) kClusterThreads * kPipeCells) return false;
-        int nt = 0;
-        for (int64_t q = 0; q < n; q++) {
-            const int kt = (int) (p.h_target[q] / L.nxy());
-            if (kt >= sp.kb[r] && kt < sp.kb[r + 1] && in[(size_t) p.h_root[q]]) nt++;
+        if (!ok) continue;
+        sp.kb[cs] = nz;
+        int cap = 0, tcap = 0;
+        for (int r = 0; r < cs && ok; r++) {
+            cap = std::max(cap, sp.kb[r + 1] - sp.kb[r]);
+            const int64_t z0 = std::max<int64_t>(sp.kb[r], L.k1), z1 = std::min<int64_t>(sp.kb[r + 1] - 1, L.k2);
+            if (z1 >= z0 && (z1 - z0 + 1) * nxy_in > (int64_t) kClusterThreads * kPipeCells) ok = false;
+            int nt = 0;
+            for (int64_t q = 0; q < n; q++) {
+                const int kt = (int) (p.h_target[q] / L.nxy());
+                if (kt >= sp.kb[r] && kt < sp.kb[r + 1] && in[(size_t) p.h_root[q]]) nt++;
+            }
+            tcap = std::max(tcap, nt);
         }
-        tcap = std::max(tcap, nt);
+        const int64_t smem = 3 * (int64_t) (cap + 2) * L.nxy() * (int64_t) sizeof(double) +
+                             (int64_t) tcap * (int64_t) sizeof(HaloTarget);
+        if (!ok || smem > kCoarseSmemBytes) continue;
+        // the device must be able to place a cluster of this size (more than 8 is non-portable)
+        cudaLaunchConfig_t lc = {};
+        cudaLaunchAttribute at[1];
+        lc.gridDim = dim3(cs, 1, 1);
+        lc.blockDim = dim3(kClusterThreads, 1, 1);
+        lc.dynamicSmemBytes = (size_t) smem;
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_mg_coarse_jacobi_pipe<double>, &lc) != cudaSuccess ||
+            clusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        pl->split = sp;
+        pl->ranks = cs;
+        pl->plane_cap = cap;
+        pl->target_cap = tcap;
+        pl->smem = smem;
+        return true;
     }
-    const int64_t smem = 3 * (int64_t) (cap + 2) * L.nxy() * (int64_t) sizeof(double) +
-                         (int64_t) tcap * (int64_t) sizeof(HaloTarget);
-    if (smem > kCoarseSmemBytes) return false;
-    pl->split = sp;
-    pl->ranks = cs;
-    pl->plane_cap = cap;
-    pl->target_cap = tcap;
-    pl->smem = smem;
-    return true;
+    return false;
 }
 
 inline cudaLaunchConfig_t cluster_config(artss_ctx *ctx, int cs, int64_t smem, cudaLaunchAttribute *at) {
