@@ -209,6 +209,8 @@ def load_host() -> C.CDLL:
             "artss_sim_create": ([C.c_char_p, C.c_int, C.POINTER(_P)], C.c_int),
             "artss_sim_destroy": ([_P], None),
             "artss_sim_run": ([_P, C.c_int64, _I64P], C.c_int),
+            "artss_sim_set_graphs": ([_P, C.c_int], C.c_int),
+            "artss_sim_graph_steps": ([_P], C.c_int64),
             "artss_sim_step_io": ([_P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_D), C.c_int,
                                    C.POINTER(C.c_char_p), C.POINTER(_D)], C.c_int),
             "artss_sim_finished": ([_P], C.c_int),
@@ -330,6 +332,16 @@ class Simulation:
         done = C.c_int64()
         _host_check(self._lib.artss_sim_run(self._h, steps, C.byref(done)), "run")
         return done.value
+
+    def set_graphs(self, enable: bool = True) -> None:
+        """Whole-step CUDA graphs: from the third step on each step is one
+        graph launch (solver loops as device-decided conditional nodes)."""
+        _host_check(self._lib.artss_sim_set_graphs(self._h, 1 if enable else 0), "graphs")
+
+    @property
+    def graph_steps(self) -> int:
+        """Steps run as one graph launch so far."""
+        return int(self._lib.artss_sim_graph_steps(self._h))
 
     def step_io(self, inputs: Dict[str, int], outputs: Dict[str, int]) -> None:
         """One timestep with host transfers overlapped with it: `inputs` and

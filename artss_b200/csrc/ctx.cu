@@ -191,6 +191,10 @@ int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
     if ((e = cudaMalloc(&ctx->d_partials, kMaxPartials * sizeof(double))) != cudaSuccess) return fail(e, "partials");
     if ((e = cudaMalloc(&ctx->d_loop, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "loop state");
+    if ((e = cudaMalloc(&ctx->d_param, kParams * sizeof(double))) != cudaSuccess) return fail(e, "parameters");
+    if ((e = cudaMemset(ctx->d_param, 0, kParams * sizeof(double))) != cudaSuccess) return fail(e, "parameters");
+    if ((e = cudaStreamCreateWithFlags(&ctx->body_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(e, "capture stream");
     if ((e = cudaMemset(ctx->d_loop, 0, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "loop state");
     if ((e = cudaMallocHost(&ctx->h_loop, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "pinned loop state");
     for (int l = 0; l <= grid->n_levels; l++) {
@@ -229,6 +233,8 @@ int artss_ctx_destroy(artss_ctx *ctx) {
     }
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_loop);
+    cudaFree(ctx->d_param);
+    if (ctx->body_stream) cudaStreamDestroy(ctx->body_stream);
     if (ctx->h_loop) cudaFreeHost(ctx->h_loop);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -319,6 +325,113 @@ int copy_after_main(artss_ctx *ctx) {
     return ARTSS_OK;
 }
 }  // namespace
+
+// ---------------------------------------------------------------- whole-step graphs
+
+struct artss_graph {
+    artss_ctx *ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;
+    int64_t fam[artss::FAM_COUNT]{};
+};
+
+namespace {
+int64_t g_capture_launches0 = 0;
+int64_t g_capture_fam0[artss::FAM_COUNT]{};
+__global__ void k_set_param(double *slot, double v) { *slot = v; }
+__global__ void k_scale_copy_param(double *__restrict__ dst, const double *__restrict__ src,
+                                   const double *__restrict__ x, int64_t n) {
+    const double f = *x;
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
+        dst[i] = src[i] * f;
+}
+}  // namespace
+
+int artss_graph_begin(artss_ctx *ctx) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("a capture is already running"); return ARTSS_ERR_ARG; }
+    if (ctx->prof.mask) { set_error("kernel-family timing cannot run inside a captured graph"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    ctx->capturing = true;
+    g_capture_launches0 = ctx->launches;
+    for (int f = 0; f < FAM_COUNT; f++) g_capture_fam0[f] = ctx->prof.launches[f];
+    return ARTSS_OK;
+}
+
+int artss_graph_end(artss_ctx *ctx, int discard, artss_graph **out) {
+    if (!ctx || (!discard && !out)) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (!ctx->capturing) { set_error("no capture is running"); return ARTSS_ERR_ARG; }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->capturing = false;
+    // the captured work did not run: its launches are counted when the graph is
+    const int64_t launches = ctx->launches - g_capture_launches0;
+    int64_t fam[FAM_COUNT];
+    for (int f = 0; f < FAM_COUNT; f++) {
+        fam[f] = ctx->prof.launches[f] - g_capture_fam0[f];
+        ctx->prof.launches[f] = g_capture_fam0[f];
+    }
+    ctx->launches = g_capture_launches0;
+    if (e != cudaSuccess || discard) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (discard) return ARTSS_OK;
+        return cuda_fail(e, "capture");
+    }
+    auto *gr = new artss_graph();
+    gr->ctx = ctx;
+    gr->graph = g;
+    gr->launches = launches;
+    for (int f = 0; f < FAM_COUNT; f++) gr->fam[f] = fam[f];
+    const cudaError_t ei = cudaGraphInstantiate(&gr->exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        delete gr;
+        return cuda_fail(ei, "graph instantiate");
+    }
+    *out = gr;
+    return ARTSS_OK;
+}
+
+int artss_graph_launch(artss_graph *g) {
+    if (!g) { set_error("null graph"); return ARTSS_ERR_ARG; }
+    artss_ctx *ctx = g->ctx;
+    ARTSS_CK(cudaGraphLaunch(g->exec, ctx->stream));
+    ctx->launches += g->launches;
+    for (int f = 0; f < FAM_COUNT; f++) ctx->prof.launches[f] += g->fam[f];
+    return ARTSS_OK;
+}
+
+int artss_graph_destroy(artss_graph *g) {
+    if (!g) return ARTSS_OK;
+    if (g->ctx && g->ctx->stream) cudaStreamSynchronize(g->ctx->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return ARTSS_OK;
+}
+
+int artss_graph_capturing(artss_ctx *ctx) { return ctx && ctx->capturing ? 1 : 0; }
+
+int artss_param_set(artss_ctx *ctx, int slot, double value) {
+    if (!ctx || slot < 0 || slot >= kParams) { set_error("bad parameter slot"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("parameters are set outside a capture"); return ARTSS_ERR_ARG; }
+    ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_set_param<<<1, 1, 0, ctx->stream>>>(ctx->d_param + slot, value));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
+int artss_scale_copy_param(artss_ctx *ctx, double *dst, const double *src, int slot, int level) {
+    if (!ctx || !dst || !src || slot < 0 || slot >= kParams) { set_error("bad arguments"); return ARTSS_ERR_ARG; }
+    int st = check_level(ctx, level);
+    if (st) return st;
+    const int64_t n = ctx->lvl[level].size();
+    ARTSS_LAUNCH(ctx, FAM_FIELD_OP,
+                 k_scale_copy_param<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, ctx->d_param + slot, n));
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
 
 int artss_copy_upload(artss_ctx *ctx, int slot, double *dst, const double *host, int64_t n) {
     if (!ctx || !dst || !host || n < 0 || slot < 0 || slot >= kCopySlots) {

@@ -19,6 +19,7 @@ namespace artss {
 constexpr int kMaxLevel = ARTSS_MAX_LEVEL;
 constexpr int kFieldTypes = ARTSS_NUM_FIELD_TYPES;
 constexpr int kCopySlots = 8;           // uploads on the copy stream waited for by slot
+constexpr int kParams = 16;             // parameter slots of captured steps
 constexpr int kBcMaxDepth = 4;          // boundary assignments folded per thread
 constexpr int kReduceThreads = 256;
 constexpr int kMaxPartials = 1 << 16;   // per-block partial sums of up to two reduction passes
@@ -62,7 +63,9 @@ struct LoopState {
     double residual;   // sqrt(sum) (or caller-defined)
     long long it;      // iterations done
     int cond;          // loop continues
-    int pad;           // error flag: a bounded wait in a kernel of the loop gave up
+    int pad;           // error flag: a bounded wait in a kernel of the loop gave up (2: a graph loop hit its cap)
+    int guard;         // bodies run by a graph loop (conditional node) since the loop's init
+    int unused;
 };
 
 // Kernel families for launch counting and event timing (artss_ctx_profile).
@@ -121,6 +124,11 @@ struct artss_ctx {
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
     // host transfers overlapped with the step: a second stream, completion
     // events of its uploads by slot, a mark of the main stream, its tail
+    // whole-step capture (artss_graph_begin .. artss_graph_end): loops become
+    // conditional WHILE nodes whose bodies are captured on body_stream
+    bool capturing = false;
+    cudaStream_t body_stream = nullptr;
+    double *d_param = nullptr;  // per-launch parameters of captured work (artss_param_set), kParams doubles
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev[artss::kCopySlots]{};
     cudaEvent_t copy_mark = nullptr, copy_tail = nullptr;
@@ -231,7 +239,23 @@ int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorM
 //   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it
 int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it);
 int init_loop(artss_ctx *ctx, int slot, double residual0, long long it0, int cond0);
+// loop step whose tolerance is rel_tol * sqrt(sum of loop slot ref_slot), on the device
+int finalize_loop_rel(artss_ctx *ctx, int slot, int nblocks, double rel_tol, int ref_slot, long long max_it);
 int read_loop(artss_ctx *ctx, int slot, LoopState *out);
+
+// A loop inside a whole-step capture: a WHILE conditional node whose body is
+// everything enqueued on the context between begin and end (the context's
+// stream is the body's capture stream meanwhile).  end() appends the kernel
+// that sets the node's condition from loop slot `slot`'s cond, or stops the
+// loop (error flag 2) after `cap` bodies.
+struct GraphLoop {
+    artss_ctx *ctx = nullptr;
+    cudaStream_t outer = nullptr;
+    cudaGraphNode_t node = nullptr;
+    cudaGraphConditionalHandle handle = 0;
+    int begin(artss_ctx *c, int cond0);
+    int end(int slot, long long cap);
+};
 // Plain sum of partials into loop slot (no iteration bookkeeping).
 int finalize_sum(artss_ctx *ctx, int slot, int nblocks);
 // sum of partials -> residual = sqrt(sum), no loop bookkeeping

@@ -1455,6 +1455,10 @@ static int mg_capture(artss_mg *mg, double *p, const double *rhs) {
 }
 
 int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step, artss_mg_stats *stats) {
+    if (mg && mg->ctx && mg->ctx->capturing && first_step) {
+        set_error("the first-step pressure solve reads its residual on the host and cannot be captured");
+        return ARTSS_ERR_ARG;
+    }
     if (!mg || !p || !rhs) { set_error("null argument"); return ARTSS_ERR_ARG; }
     int st;
     int64_t cycles = 0, coarse = 0;
@@ -1480,7 +1484,7 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
             set_relax += mg->cfg.n_relax;
         }
         residual = r;
-    } else if (mg->use_graphs && !(mg->ctx->prof.mask & kMgFamilies) && mg->fused_coarse) {
+    } else if (mg->use_graphs && !(mg->ctx->prof.mask & kMgFamilies) && mg->fused_coarse && !mg->ctx->capturing) {
         // the later-step call is a fixed launch sequence: replay it as one graph
         artss_ctx *ctx = mg->ctx;
         artss_mg::Graph *g = nullptr;

@@ -453,16 +453,27 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     const bool remove_mean = (m->cfg.flags & ARTSS_MIXED_REMOVE_MEAN) != 0;
     const int64_t n_inner = ctx->n_inner[0];
     int st;
-    // ||b|| for the relative stopping rule
+    const dim3 grid = mx_grid(box);
+    if ((st = check_reduce_blocks(grid))) return st;
+    const int nb = (int) (grid.x * grid.y * grid.z);
+    // ||b|| for the relative stopping rule: on the host, or (inside a capture)
+    // kept in loop slot kSlotSum and applied by the loop step on the device
     double s1 = 0, s2 = 0;
-    if ((st = mx_moments(m, b, 0.0, &s1, &s2))) return st;
+    if (ctx->capturing) {
+        if (remove_mean) { set_error("the mean removal reads sums on the host and cannot be captured"); return ARTSS_ERR_ARG; }
+        ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_moments<<<grid, box_block(), 0, ctx->stream>>>(
+                                              b, 0.0, ctx->d_flags[0], L, box, ctx->d_partials, ctx->d_partials + nb));
+        ARTSS_LAUNCH_CK(ctx);
+        ARTSS_CK(cudaMemcpyAsync(ctx->d_partials, ctx->d_partials + nb, nb * sizeof(double), cudaMemcpyDeviceToDevice,
+                                 ctx->stream));
+        if ((st = finalize_sum(ctx, kSlotSum, nb))) return st;
+    } else if ((st = mx_moments(m, b, 0.0, &s1, &s2))) {
+        return st;
+    }
     const double b_norm = sqrt(s2);
     const double tol = m->cfg.rel_tol * b_norm;
     if ((st = apply_bc(ctx, p, 0, ARTSS_FIELD_P))) return st;
 
-    const dim3 grid = mx_grid(box);
-    if ((st = check_reduce_blocks(grid))) return st;
-    const int nb = (int) (grid.x * grid.y * grid.z);
     const double rx = 1. / (g.dx[0] * g.dx[0]), ry = 1. / (g.dy[0] * g.dy[0]), rz = 1. / (g.dz[0] * g.dz[0]);
     const long long max_eval = m->cfg.max_cycles + 1;
     if ((st = init_loop(ctx, kSlotOuter, 1e300, 0, 1))) return st;
@@ -471,18 +482,31 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     long long it = 0;
     bool cond = true;
     int64_t batch = std::max<int64_t>(1, std::min<int64_t>(m->hint, max_eval));
+    GraphLoop gl;
+    if (ctx->capturing) {
+        // one outer iteration per body of a WHILE node decided on the device
+        if ((st = gl.begin(ctx, 1))) return st;
+        batch = 1;
+    }
     while (cond) {
         for (int64_t r = 0; r < batch; r++) {
             ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_outer_residual<<<grid, box_block(), 0, ctx->stream>>>(
                                                   p, b, m->r[0], ctx->d_flags[0], L, box, rx, ry, rz,
                                                   ctx->d_partials, pred));
             ARTSS_LAUNCH_CK(ctx);
-            if ((st = finalize_loop(ctx, kSlotOuter, nb, tol, max_eval))) return st;
+            if (ctx->capturing) st = finalize_loop_rel(ctx, kSlotOuter, nb, m->cfg.rel_tol, kSlotSum, max_eval);
+            else st = finalize_loop(ctx, kSlotOuter, nb, tol, max_eval);
+            if (st) return st;
             if ((st = mx_vcycle(m, pred))) return st;
             ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mx_correct<<<grid, box_block(), 0, ctx->stream>>>(
                                                 p, m->e[0], ctx->d_flags[0], L, box, pred));
             ARTSS_LAUNCH_CK(ctx);
             if ((st = apply_bc(ctx, p, 0, ARTSS_FIELD_P, pred))) return st;
+        }
+        if (ctx->capturing) {
+            if ((st = gl.end(kSlotOuter, max_eval + 2))) return st;
+            if (stats) *stats = artss_solve_stats{-1, -1.0, -1.0, -1.0};
+            return ARTSS_OK;
         }
         if ((st = read_loop(ctx, kSlotOuter, &ls))) return st;
         it = ls.it;

@@ -654,6 +654,20 @@ __global__ void k_copy_domain(double *__restrict__ dst, const double *__restrict
 }
 
 // exchanges two arrays element by element
+// After a captured colored Gauss-Seidel loop: the last iterate sits in `in`
+// when (s0 + it) is odd; exchange the arrays (the caller keeps in) or copy it
+// back, as the host does after an uncaptured loop.
+__global__ void k_cgs_fixup(double *__restrict__ out, double *__restrict__ in, const LoopState *__restrict__ st,
+                            int s0, int in_is_scratch, int64_t n) {
+    const long long it = st->it;
+    if (it <= 0 || !((s0 + it) & 1)) return;
+    for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        const double v = in[i];
+        if (!in_is_scratch) in[i] = out[i];
+        out[i] = v;
+    }
+}
+
 __global__ void k_swap(double *__restrict__ x, double *__restrict__ y, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
         const double t = x[i];
@@ -848,7 +862,7 @@ int tune_sweep(artss_ctx *ctx, bool turb, const Box3 &box, size_t smem, const CU
     const TuneKey key{0, L.Nx, L.Ny, L.Nz, turb ? 1 : 0};
     auto it = ctx->tuned.find(key);
     if (it != ctx->tuned.end()) { *choice = it->second; return ARTSS_OK; }
-    if (!ctx->autotune) { *choice = 1; return ARTSS_OK; }
+    if (!ctx->autotune || ctx->capturing) { *choice = 1; return ARTSS_OK; }
     cudaEvent_t e0, e1;
     ARTSS_CK(cudaEventCreate(&e0));
     ARTSS_CK(cudaEventCreate(&e1));
@@ -944,6 +958,38 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
         if ((st = tune_sweep(ctx, ev != nullptr, box, smem, *tm_x[1 - n1], *tm_b, *tm_e, buf[n1], L, c, pred_rw, &depth)))
             return st;
     }
+    if (ctx->capturing) {
+        // a WHILE node whose body is two iterations (the second writes back into
+        // the first's source); the loop state decides on the device
+        if (cond) {
+            GraphLoop gl;
+            if ((st = gl.begin(ctx, 1))) return st;
+            for (int n = 1; n <= 2; n++) {
+                double *w = buf[(s0 + n) & 1];
+                const double *rd = buf[(s0 + n + 1) & 1];
+                if (tma) {
+                    if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, smem, *tm_x[(s0 + n + 1) & 1], *tm_b,
+                                               *tm_e, w, L, c, pred_rw, &nb)))
+                        return st;
+                } else if (ev)
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
+                        w, rd, b, ev, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+                else
+                    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<false><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
+                        w, rd, b, nullptr, ctx->d_flags[0], L, box, c, ctx->d_partials, pred));
+                if (!tma) ARTSS_LAUNCH_CK(ctx);
+                if ((st = apply_bc(ctx, w, 0, field_type, pred))) return st;
+                if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
+            }
+            if ((st = gl.end(slot, cfg->max_iter / 2 + 2))) return st;
+            const int64_t n = L.size();
+            ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_cgs_fixup<<<flat_blocks(n), 256, 0, ctx->stream>>>(
+                                                out, in, ctx->d_loop + slot, s0, in_is_scratch, n));
+            ARTSS_LAUNCH_CK(ctx);
+        }
+        if (stats) { stats->iterations = -1; stats->residual = -1.0; }
+        return ARTSS_OK;
+    }
     while (cond) {
         // `batch` iterations per host round trip; iterations past convergence skip themselves
         for (int64_t r = 0; r < batch; r++) {
@@ -1006,6 +1052,16 @@ int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *
     LoopState ls{};
     const LoopState *pred = ctx->d_loop + slot;
     int64_t batch = std::max<int64_t>(1, std::min<int64_t>(loop_hint(ctx, 1, field_type), cfg->max_iter));
+    GraphLoop gl;
+    if (ctx->capturing) {
+        // one iteration per body of a WHILE node decided on the device
+        if (!cond) {
+            if (stats) { stats->iterations = 0; stats->residual = res; }
+            return ARTSS_OK;
+        }
+        if ((st = gl.begin(ctx, 1))) return st;
+        batch = 1;
+    }
     while (cond) {
         for (int64_t r = 0; r < batch; r++) {
             if (ev)
@@ -1021,6 +1077,11 @@ int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *
                 in, out, ctx->d_flags[0], L, dbox, pred));
             ARTSS_LAUNCH_CK(ctx);
             if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
+        }
+        if (ctx->capturing) {
+            if ((st = gl.end(slot, cfg->max_iter + 2))) return st;
+            if (stats) { stats->iterations = -1; stats->residual = -1.0; }
+            return ARTSS_OK;
         }
         if ((st = read_loop(ctx, slot, &ls))) return st;
         it = ls.it;

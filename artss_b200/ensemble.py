@@ -31,11 +31,18 @@ def partition(costs: Sequence[float], parts: int) -> List[List[int]]:
 
 
 class Ensemble:
-    """Independent scenes on one GPU, stepped concurrently."""
+    """Independent scenes on one GPU, stepped concurrently.  With graphs=True
+    every scene's step is one CUDA graph launch from the third step on.  The
+    scenes' streams overlap best with CUDA_DEVICE_MAX_CONNECTIONS=32 in the
+    environment before the process creates its CUDA context."""
 
-    def __init__(self, xml_paths: Sequence[str], device: int = 0):
+    def __init__(self, xml_paths: Sequence[str], device: int = 0, graphs: bool = False):
         from artss_b200 import Simulation
         self.sims = [Simulation(x, device=device) for x in xml_paths]
+        if graphs:
+            # from the third step on, every scene's step is one graph launch
+            for s in self.sims:
+                s.set_graphs(True)
 
     @property
     def inner_cells(self) -> int:

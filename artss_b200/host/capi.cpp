@@ -182,6 +182,14 @@ int artss_sim_step_io(artss_sim *s, int n_in, const char *const *in_names, const
     });
 }
 
+int artss_sim_set_graphs(artss_sim *s, int enable) {
+    if (!s) return ARTSS_ERR_ARG;
+    s->rt->graphs = enable != 0;
+    return ARTSS_OK;
+}
+
+int64_t artss_sim_graph_steps(artss_sim *s) { return s ? s->ti->graph_steps : -1; }
+
 int artss_sim_finished(artss_sim *s) { return s ? (s->ti->finished() ? 1 : 0) : -1; }
 double artss_sim_time(artss_sim *s) { return s ? s->ti->time() : -1.0; }
 int64_t artss_sim_step_index(artss_sim *s) { return s ? s->ti->step_index() : -1; }

@@ -216,6 +216,20 @@ void GaussFunction::create_spatial_values() {
 
 void GaussFunction::update_source(Field &out, real t_cur) {
     // GaussFunction::update_source (src/source/GaussFunction.cpp:27-40)
+    if (m_rt.capturing()) {
+        // a captured step: the factor comes from a parameter slot set before each replay
+        if (m_noise) throw std::runtime_error("a source with noise cannot be captured");
+        if (m_param < 0) {
+            m_param = m_rt.next_param_slot++;
+            const real tau = m_settings.tau;
+            artss_ctx *ctx = m_rt.ctx();
+            const int slot = m_param;
+            m_rt.step_params.push_back(
+                [ctx, slot, tau](real t) { check(artss_param_set(ctx, slot, std::tanh(t / tau)), "source factor"); });
+        }
+        check(artss_scale_copy_param(m_rt.ctx(), out.data, m_spatial.data, m_param, 0), "source");
+        return;
+    }
     const real time_val = std::tanh(t_cur / m_settings.tau);
     out.copy_data(m_spatial);
     out *= time_val;

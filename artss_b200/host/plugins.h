@@ -201,6 +201,7 @@ class GaussFunction : public ISourceFunction {
     Field m_spatial;
     std::unique_ptr<UniformRandom> m_noise;
     bool m_absolute = false;
+    int m_param = -1;  // parameter slot of tanh(t / tau) in captured steps
 };
 
 class ZeroSource : public ISourceFunction {

@@ -6,6 +6,7 @@
 // every operation is a C-ABI call from include/artss_cuda.h.
 #pragma once
 
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -111,6 +112,14 @@ class Runtime {
 
     // transfers of the running step, when it runs through TimeIntegration::step_io
     StepIO *io = nullptr;
+
+    // whole-step graphs (TimeIntegration): a captured step is replayed from
+    // the third step on; values that change per step are set before each
+    // replay by the providers plugins register here, into parameter slots
+    bool graphs = false;
+    std::vector<std::function<void(real)>> step_params;
+    int next_param_slot = 0;
+    bool capturing() const { return artss_graph_capturing(m_ctx) != 0; }
 
  private:
     settings::Settings m_settings;

@@ -589,9 +589,44 @@ void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>
     io.finish();
 }
 
+TimeIntegration::~TimeIntegration() { artss_graph_destroy(m_graph); }
+
+void TimeIntegration::capture_step() {
+    artss_ctx *ctx = m_rt.ctx();
+    if (artss_graph_begin(ctx) != ARTSS_OK) {
+        m_graph_failed = true;
+        return;
+    }
+    bool ok = true;
+    try {
+        m_sc.solver_do_step(m_t_cur, false);
+        m_sc.update_sources(m_t_cur, false);
+        m_sc.fields().update_data();
+    } catch (const std::exception &) {
+        ok = false;
+    }
+    if (!ok || artss_graph_end(ctx, 0, &m_graph) != ARTSS_OK) {
+        if (!ok) artss_graph_end(ctx, 1, nullptr);
+        m_graph = nullptr;
+        m_graph_failed = true;
+    }
+}
+
 int64_t TimeIntegration::run(int64_t steps) {
     int64_t done = 0;
     while (!finished() && (steps < 0 || done < steps)) {
+        if (m_rt.graphs && m_step >= kGraphStep && !m_graph_failed && !m_rt.io) {
+            if (!m_graph) capture_step();
+            if (m_graph) {
+                for (auto &p : m_rt.step_params) p(m_t_cur);
+                check(artss_graph_launch(m_graph), "step graph");
+                graph_steps++;
+                m_step++;
+                m_t_cur = (real) m_step * m_dt;
+                done++;
+                continue;
+            }
+        }
         m_sc.solver_do_step(m_t_cur, false);
         m_sc.update_sources(m_t_cur, false);
         m_sc.fields().update_data();

@@ -151,6 +151,9 @@ class SolverController {
 class TimeIntegration {
  public:
     TimeIntegration(Runtime &rt, SolverController &sc);
+    ~TimeIntegration();
+    TimeIntegration(const TimeIntegration &) = delete;
+    TimeIntegration &operator=(const TimeIntegration &) = delete;
     // runs until t_end (steps < 0) or for `steps` steps; returns steps run
     int64_t run(int64_t steps = -1);
     // one step with its host transfers: the inputs are uploaded into their
@@ -164,6 +167,18 @@ class TimeIntegration {
     bool finished() const;
 
  private:
+    // the step as one graph (Runtime::graphs): captured at step kGraphStep,
+    // replayed after; a step that cannot be captured keeps the eager path
+    void capture_step();
+    static constexpr int64_t kGraphStep = 3;
+    artss_graph *m_graph = nullptr;
+    bool m_graph_failed = false;
+
+ public:
+    int64_t graph_steps = 0;  // steps run as a graph launch
+
+ private:
+
     Runtime &m_rt;
     SolverController &m_sc;
     real m_dt, m_t_end, m_t_cur;

@@ -176,6 +176,24 @@ int artss_copy_wait(artss_ctx *ctx, int slot);
 int artss_copy_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
 int artss_copy_join(artss_ctx *ctx);
 
+/* Whole-step graphs.  Between artss_graph_begin and artss_graph_end every
+ * call on the context is captured instead of run: its bounded solver loops
+ * (diffusion, mixed-precision pressure) become conditional WHILE nodes that
+ * test the device loop state, so the captured work needs no host decision;
+ * calls that must read results on the host fail inside a capture.
+ * artss_graph_launch runs the captured work once more on the context's
+ * stream.  Values that change from launch to launch live in parameter slots
+ * (artss_param_set, set before the launch) read by kernels such as
+ * artss_scale_copy_param (dst = src * param[slot]). */
+typedef struct artss_graph artss_graph;
+int artss_graph_begin(artss_ctx *ctx);
+int artss_graph_end(artss_ctx *ctx, int discard, artss_graph **out);
+int artss_graph_launch(artss_graph *g);
+int artss_graph_destroy(artss_graph *g);
+int artss_graph_capturing(artss_ctx *ctx);
+int artss_param_set(artss_ctx *ctx, int slot, double value);
+int artss_scale_copy_param(artss_ctx *ctx, double *dst, const double *src, int slot, int level);
+
 /* ------------------------------------------------------------------ */
 /* geometry: GPU lists -> device cell flags and boundary programs     */
 /* ------------------------------------------------------------------ */

@@ -58,6 +58,14 @@ int artss_sim_run(artss_sim *s, int64_t steps, int64_t *done);
  * returns. */
 int artss_sim_step_io(artss_sim *s, int n_in, const char *const *in_names, const double *const *in_host, int n_out,
                       const char *const *out_names, double *const *out_host);
+/* Whole-step graphs on or off (off by default): from the third step on, a
+ * step is captured once (its solver loops as conditional WHILE nodes on the
+ * device loop state) and replayed per step; a scene whose step cannot be
+ * captured (a noisy source, the mixed solver's mean removal) keeps running
+ * step by step.  Per-step statistics are not updated while replaying. */
+int artss_sim_set_graphs(artss_sim *s, int enable);
+/* steps run as one graph launch so far */
+int64_t artss_sim_graph_steps(artss_sim *s);
 int artss_sim_finished(artss_sim *s);
 double artss_sim_time(artss_sim *s);
 int64_t artss_sim_step_index(artss_sim *s);
