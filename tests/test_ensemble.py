@@ -70,20 +70,26 @@ def test_partition_two_gloo_ranks():
 
 
 @pytest.mark.gpu
-def test_ensemble_concurrent_matches_alone(tmp_path):
+@pytest.mark.parametrize("graphs", [False, True])
+def test_ensemble_concurrent_matches_alone(tmp_path, graphs):
+    """Scenes stepped concurrently (optionally as whole-step graphs from the
+    third step on) give exactly the fields of each scene run alone, step by step."""
     import artss_b200 as A
     from artss_b200 import scenes
     from artss_b200.ensemble import Ensemble
-    scs = scenes.plume_ensemble(3, seed=5, steps=3, sizes=(32, 48))
+    steps = 6 if graphs else 3
+    scs = scenes.plume_ensemble(3, seed=5, steps=steps, sizes=(32, 48))
     xmls = [scenes.write(sc, str(tmp_path / f"e{i}.xml")) for i, sc in enumerate(scs)]
-    ens = Ensemble(xmls)
+    ens = Ensemble(xmls, graphs=graphs)
     try:
-        assert ens.run(3) == [3, 3, 3]
+        assert ens.run(steps) == [steps] * 3
+        if graphs:
+            assert all(s.graph_steps == steps - 2 for s in ens.sims)
         together = [{f: s.field(f) for f in ("u", "p", "T")} for s in ens.sims]
     finally:
         ens.close()
     for x, ref in zip(xmls, together):
         with A.Simulation(x) as sim:
-            sim.run(3)
+            sim.run(steps)
             for f in ("u", "p", "T"):
                 assert np.array_equal(sim.field(f), ref[f]), f
