@@ -40,27 +40,30 @@ struct AdvCoef {
 };
 
 // Backtrace of SLAdvect.cpp:79-126 for one axis.
-__device__ __forceinline__ void sl_axis(double C, int64_t c, int64_t cs, int64_t ce,
-                                        int64_t &c0, int64_t &c1, double &r) {
+// fmod(x, 1.0) for x >= 0: x - trunc(x), the exact remainder fmod returns,
+// without the general fmod
+__device__ __forceinline__ double frac1(double x) { return x < 1.0 ? x : x - trunc(x); }
+
+// 32-bit indices: the host runs the advection only on levels below 2^31 cells
+__device__ __forceinline__ void sl_axis(double C, int c, int cs, int ce, int &c0, int &c1, double &r) {
     const double eps = 1e-6;
     c0 = c; c1 = c; r = 1.0;
     if (C > eps) {
-        const int64_t t = c - (int64_t) C;
+        const int t = c - (int) C;
         c0 = t > cs ? t : cs;
         c1 = c0 - 1;
-        r = fmod(C, 1.0);
+        r = frac1(C);
     } else if (C < -eps) {
-        const int64_t t = c - (int64_t) C;
+        const int t = c - (int) C;
         c0 = t < ce ? t : ce;
         c1 = c0 + 1;
-        r = fmod(-C, 1.0);
+        r = frac1(-C);
     }
 }
 
 // Trilinear blend of SLAdvect.cpp:131-162, same operation order.
-__device__ __forceinline__ double sl_interp(const double *__restrict__ in, int64_t Nx, int64_t nxy,
-                                            int64_t i0, int64_t i1, int64_t j0, int64_t j1, int64_t k0, int64_t k1,
-                                            double r, double s, double t) {
+__device__ __forceinline__ double sl_interp(const double *__restrict__ in, int Nx, int nxy, int i0, int i1, int j0,
+                                            int j1, int k0, int k1, double r, double s, double t) {
     const double d000 = in[i0 + Nx * j0 + nxy * k0];
     const double d100 = in[i1 + Nx * j0 + nxy * k0];
     const double d010 = in[i0 + Nx * j1 + nxy * k0];
@@ -85,19 +88,20 @@ __global__ void k_advect(double *__restrict__ o0, double *__restrict__ o1, doubl
                          const uint8_t *__restrict__ flags, Level L, Box3 box, AdvCoef c) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    const int64_t nxy = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t idx = i + L.Nx * j + nxy * k;
+    const int Nx = (int) L.Nx, nxy = (int) L.nxy();
+    const int is = (int) c.is, ie = (int) c.ie, js = (int) c.js, je = (int) c.je, ks = (int) c.ks, ke = (int) c.ke;
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int idx = (int) i + Nx * (int) j + nxy * k;
         if (!(flags[idx] & kInner)) continue;
-        int64_t i0, i1, j0, j1, k0, k1;
+        int i0, i1, j0, j1, k0, k1;
         double r, s, t;
-        sl_axis(c.dtx * u[idx], i, c.is, c.ie, i0, i1, r);
-        sl_axis(c.dty * v[idx], j, c.js, c.je, j0, j1, s);
-        sl_axis(c.dtz * w[idx], k, c.ks, c.ke, k0, k1, t);
-        o0[idx] = sl_interp(n0, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+        sl_axis(c.dtx * u[idx], (int) i, is, ie, i0, i1, r);
+        sl_axis(c.dty * v[idx], (int) j, js, je, j0, j1, s);
+        sl_axis(c.dtz * w[idx], k, ks, ke, k0, k1, t);
+        o0[idx] = sl_interp(n0, Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
         if (NF == 3) {
-            o1[idx] = sl_interp(n1, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
-            o2[idx] = sl_interp(n2, L.Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+            o1[idx] = sl_interp(n1, Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
+            o2[idx] = sl_interp(n2, Nx, nxy, i0, i1, j0, j1, k0, k1, r, s, t);
         }
     }
 }
@@ -721,6 +725,7 @@ int artss_advect_sl(artss_ctx *ctx, double *out, const double *in, const double 
     int st = check_field_args(ctx, {out, in, u, v, w});
     if (st || (st = check_field_type(out_field_type))) return st;
     const Level &L = ctx->lvl[0];
+    if (L.size() >= ((int64_t) 1 << 31)) { set_error("advection: level of 2^31 cells or more"); return ARTSS_ERR_LIMIT; }
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
@@ -736,6 +741,7 @@ int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *ou
     int st = check_field_args(ctx, {out_u, out_v, out_w, in_u, in_v, in_w, u, v, w});
     if (st) return st;
     const Level &L = ctx->lvl[0];
+    if (L.size() >= ((int64_t) 1 << 31)) { set_error("advection: level of 2^31 cells or more"); return ARTSS_ERR_LIMIT; }
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
