@@ -167,6 +167,11 @@ int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
             set_error("inconsistent grid description at level " + std::to_string(l));
             return ARTSS_ERR_ARG;
         }
+        // kernels index cells with 32-bit integers
+        if ((int64_t) grid->Nx[l] * grid->Ny[l] * grid->Nz[l] >= ((int64_t) 1 << 31)) {
+            set_error("level " + std::to_string(l) + " has 2^31 cells or more");
+            return ARTSS_ERR_LIMIT;
+        }
     }
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);

@@ -48,10 +48,11 @@ inline dim3 mg_grid(const Box3 &b) {
     return g;
 }
 
-#define MG_COLUMN(box)                                                     \
-    const int64_t i = (box).x0 + (int64_t) blockIdx.x * blockDim.x + threadIdx.x; \
-    const int64_t j = (box).y0 + (int64_t) blockIdx.y * blockDim.y + threadIdx.y; \
-    const bool col = (i <= (box).x1) && (j <= (box).y1)
+// 32-bit cell indices: artss_ctx_create rejects levels of 2^31 cells or more
+#define MG_COLUMN(box)                                                                    \
+    const int i = (int) (box).x0 + (int) (blockIdx.x * blockDim.x + threadIdx.x);        \
+    const int j = (int) (box).y0 + (int) (blockIdx.y * blockDim.y + threadIdx.y);        \
+    const bool col = (i <= (int) (box).x1) && (j <= (int) (box).y1)
 
 struct MgCoef {
     double ax, ay, az;   // 1/(dx*dx) ... of the level (VCycleMG.cpp:595-601)
@@ -64,9 +65,9 @@ __global__ void k_mg_jacobi(double *__restrict__ out, const double *__restrict__
                             const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c) {
     MG_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + nk * k;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         const double out_h = c.beta * (c.dsign * b[q] + c.ax * (in[q + 1] + in[q - 1]) +
                                        c.ay * (in[q + nj] + in[q - nj]) + c.az * (in[q + nk] + in[q - nk]));
@@ -80,10 +81,10 @@ __global__ void k_mg_cgs_color(double *__restrict__ out, const double *__restric
                                const uint8_t *__restrict__ flags, Level L, Box3 box, int color, MgCoef c) {
     MG_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
         if (((i + j + k) & 1) != color) continue;
-        const int64_t q = i + L.Nx * j + nk * k;
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         const double out_h = c.beta * (c.dsign * b[q] + c.ax * (out[q + 1] + out[q - 1]) +
                                        c.ay * (out[q + nj] + out[q - nj]) + c.az * (out[q + nk] + out[q - nk]));
@@ -96,9 +97,9 @@ __global__ void k_mg_residuum(double *__restrict__ out, const double *__restrict
                               const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz) {
     MG_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + nk * k;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         const double weighted = (rx * (in[q - 1] - 2 * in[q] + in[q + 1]) + ry * (in[q - nj] - 2 * in[q] + in[q + nj]) +
                                  rz * (in[q - nk] - 2 * in[q] + in[q + nk]));
@@ -113,11 +114,11 @@ __global__ void k_mg_resnorm(const double *__restrict__ x, const double *__restr
                              double *__restrict__ partials, double *__restrict__ partials_b) {
     __shared__ double smem[32];
     MG_COLUMN(box);
-    const int64_t nj = L.Nx, nk = L.nxy();
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
     double acc = 0.0, accb = 0.0;
     if (col) {
-        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-            const int64_t q = i + L.Nx * j + nk * k;
+        for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+            const int q = i + (int) L.Nx * j + nk * k;
             if (!(flags[q] & kInner)) continue;
             const double r = b[q] - (rx * (x[q - 1] - 2 * x[q] + x[q + 1]) + ry * (x[q - nj] - 2 * x[q] + x[q + nj]) +
                                      rz * (x[q - nk] - 2 * x[q] + x[q + nk]));
@@ -140,11 +141,11 @@ __global__ void k_mg_restrict(double *__restrict__ out, const double *__restrict
                               const uint8_t *__restrict__ flags, Level C, Level F, Box3 box) {
     MG_COLUMN(box);
     if (!col) return;
-    const int64_t fx = F.Nx, fxy = F.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + C.Nx * j + C.nxy() * k;
+    const int fx = (int) F.Nx, fxy = (int) F.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) C.Nx * j + (int) C.nxy() * k;
         if (!(flags[q] & kInner)) continue;
-        const int64_t a = 2 * i - 1, bx = 2 * i, c = 2 * j - 1, d = 2 * j, e = 2 * k - 1, f = 2 * k;
+        const int a = 2 * i - 1, bx = 2 * i, c = 2 * j - 1, d = 2 * j, e = 2 * k - 1, f = 2 * k;
         out[q] = 0.125 * (in[a + fx * c + fxy * e] + in[bx + fx * c + fxy * e] + in[a + fx * d + fxy * e] +
                           in[bx + fx * d + fxy * e] + in[a + fx * c + fxy * f] + in[bx + fx * c + fxy * f] +
                           in[a + fx * d + fxy * f] + in[bx + fx * d + fxy * f]);
@@ -156,10 +157,10 @@ __global__ void k_mg_prolongate(double *__restrict__ out, const double *__restri
                                 const uint8_t *__restrict__ flags, Level C, Level F, Box3 box) {
     MG_COLUMN(box);
     if (!col) return;
-    const int64_t ni = 1, nj = C.Nx, nk = C.nxy();
-    const int64_t fx = F.Nx, fxy = F.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + C.Nx * j + C.nxy() * k;
+    const int ni = 1, nj = (int) C.Nx, nk = (int) C.nxy();
+    const int fx = (int) F.Nx, fxy = (int) F.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) C.Nx * j + (int) C.nxy() * k;
         if (!(flags[q] & kInner)) continue;
         // sx, sy, sz in {+1, -1}: fine cell 2i (+) or 2i-1 (-) per axis
 #define ARTSS_PROLONG(SX, SY, SZ, FI, FJ, FK)                                                         \

@@ -25,10 +25,11 @@ inline dim3 zgrid(const Box3 &b) {
 }
 inline int nblocks(const dim3 &g) { return (int) (g.x * g.y * g.z); }
 
-#define ARTSS_COLUMN(box)                                                  \
-    const int64_t i = (box).x0 + (int64_t) blockIdx.x * blockDim.x + threadIdx.x; \
-    const int64_t j = (box).y0 + (int64_t) blockIdx.y * blockDim.y + threadIdx.y; \
-    const bool col = (i <= (box).x1) && (j <= (box).y1)
+// 32-bit cell indices: artss_ctx_create rejects levels of 2^31 cells or more
+#define ARTSS_COLUMN(box)                                                                 \
+    const int i = (int) (box).x0 + (int) (blockIdx.x * blockDim.x + threadIdx.x);        \
+    const int j = (int) (box).y0 + (int) (blockIdx.y * blockDim.y + threadIdx.y);        \
+    const bool col = (i <= (int) (box).x1) && (j <= (int) (box).y1)
 
 __device__ __forceinline__ int block_linear() { return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); }
 
@@ -114,9 +115,9 @@ __global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict_
                               double rdx, double rdy, double rdz, double cs2d2) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    const int64_t ni = 1, nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + nk * k;
+    const int ni = 1, nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         const double S11 = (u[q + ni] - u[q - ni]) * 0.5 * rdx;
         const double S22 = (v[q + nj] - v[q - nj]) * 0.5 * rdy;
@@ -138,9 +139,9 @@ __global__ void k_divergence(double *__restrict__ out, const double *__restrict_
                              double hx, double hy, double hz) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + nk * k;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         const double a = hx * (u[q + 1] - u[q - 1]);
         const double b = hy * (v[q + nj] - v[q - nj]);
@@ -153,9 +154,9 @@ __global__ void k_divergence(double *__restrict__ out, const double *__restrict_
 __global__ void k_ghost_ring_zero(double *__restrict__ out, Level L, Box3 ring) {
     ARTSS_COLUMN(ring);
     if (!col) return;
-    for (int64_t k = ring.z0 + blockIdx.z; k <= ring.z1; k += gridDim.z) {
+    for (int k = (int) ring.z0 + (int) blockIdx.z; k <= (int) ring.z1; k += (int) gridDim.z) {
         if (i == ring.x0 || i == ring.x1 || j == ring.y0 || j == ring.y1 || k == ring.z0 || k == ring.z1)
-            out[i + L.Nx * j + L.nxy() * k] = 0.0;
+            out[i + (int) L.Nx * j + (int) L.nxy() * k] = 0.0;
     }
 }
 
@@ -166,9 +167,9 @@ __global__ void k_projection(double *__restrict__ ou, double *__restrict__ ov, d
                              const uint8_t *__restrict__ flags, Level L, Box3 box, double hx, double hy, double hz) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + nk * k;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + nk * k;
         if (!(flags[q] & kInner)) continue;
         ou[q] = us[q] - hx * (p[q + 1] - p[q - 1]);
         ov[q] = vs[q] - hy * (p[q + nj] - p[q - nj]);
@@ -183,8 +184,8 @@ __global__ void k_buoyancy(double *__restrict__ f, const double *__restrict__ T,
                            const uint8_t *__restrict__ flags, Level L, Box3 box, double nbeta, double g) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + L.nxy() * k;
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + (int) L.nxy() * k;
         if (!(flags[q] & kDomain)) continue;
         f[q] = nbeta * (T[q] - Ta[q]) * g;
     }
@@ -195,8 +196,8 @@ __global__ void k_add_source(double *__restrict__ out, const double *__restrict_
                              const uint8_t *__restrict__ flags, Level L, Box3 box, double dt) {
     ARTSS_COLUMN(box);
     if (!col) return;
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + L.nxy() * k;
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + (int) L.nxy() * k;
         if (!(flags[q] & kInner)) continue;
         out[q] += dt * S[q];
     }
@@ -615,11 +616,11 @@ __global__ void k_jacobi_diffuse(double *__restrict__ out, const double *__restr
     __shared__ double smem[32];
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
     ARTSS_COLUMN(box);
-    const int64_t nj = L.Nx, nk = L.nxy();
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
     double acc = 0.0;
     if (col) {
-        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-            const int64_t q = i + L.Nx * j + nk * k;
+        for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+            const int q = i + (int) L.Nx * j + nk * k;
             if (!(flags[q] & kInner)) continue;
             double out_h, rb;
             if (TURB) {
@@ -651,8 +652,8 @@ __global__ void k_copy_domain(double *__restrict__ dst, const double *__restrict
     if (pred && !pred->cond) return;
     ARTSS_COLUMN(box);
     if (!col) return;
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t q = i + L.Nx * j + L.nxy() * k;
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + (int) L.Nx * j + (int) L.nxy() * k;
         if (flags[q] & kDomain) dst[q] = src[q];
     }
 }
