@@ -1316,16 +1316,21 @@ int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, in
     return ARTSS_OK;
 }
 
-// VCycleMG::VCycleMultigrid (VCycleMG.cpp:215-288)
-int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its) {
+// VCycleMG::VCycleMultigrid (VCycleMG.cpp:215-288).  The reference copies out
+// into error1[0], works on error1[0] and copies it back; nothing reads out in
+// between, so level 0's error1 is out itself here.  b0: the level-0 right-hand
+// side (residuum1[0] when null).
+int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its, const double *b0 = nullptr) {
     artss_ctx *ctx = mg->ctx;
     const int L = mg->L;
     int st;
-    if (L == 0) return mg_solve(mg, out, mg->tmp[0], mg->r1[0], 0, coarse_its);
-    if ((st = artss_copy(ctx, mg->e1[0], out, 0))) return st;
+    const double *R0 = b0 ? b0 : mg->r1[0];
+    if (L == 0) return mg_solve(mg, out, mg->tmp[0], R0, 0, coarse_its);
+    auto e1 = [&](int l) { return l == 0 ? out : mg->e1[l]; };
+    auto r1 = [&](int l) { return l == 0 ? R0 : (const double *) mg->r1[l]; };
     for (int l = 0; l < L; l++) {
-        if ((st = mg_smooth(mg, mg->e1[l], mg->tmp[l], mg->r1[l], l))) return st;
-        if ((st = mg_residuum(mg, mg->r0[l], mg->e1[l], mg->r1[l], l))) return st;
+        if ((st = mg_smooth(mg, e1(l), mg->tmp[l], r1(l), l))) return st;
+        if ((st = mg_residuum(mg, mg->r0[l], e1(l), r1(l), l))) return st;
         if ((st = mg_bc(mg, mg->r0[l], l))) return st;
         if ((st = mg_restrict(mg, mg->r1[l + 1], mg->r0[l], l + 1))) return st;
         // the reference also applies the boundary program to the restricted
@@ -1336,16 +1341,15 @@ int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its) {
     // out.copy_data(*m_error0[0]) at VCycleMG.cpp:254 is overwritten below
     // before anything reads it
     for (int l = L; l > 0; l--) {
-        if ((st = mg_prolongate(mg, mg->e0[l - 1], mg->e1[l], l))) return st;
+        if ((st = mg_prolongate(mg, mg->e0[l - 1], e1(l), l))) return st;
         if ((st = mg_bc(mg, mg->e0[l - 1], l - 1))) return st;
-        if ((st = artss_add_field(ctx, mg->e1[l - 1], mg->e0[l - 1], l - 1))) return st;
+        if ((st = artss_add_field(ctx, e1(l - 1), mg->e0[l - 1], l - 1))) return st;
         if (l == L) {
-            if ((st = mg_solve(mg, mg->e1[l - 1], mg->tmp[l - 1], mg->r1[l - 1], l - 1, coarse_its))) return st;
+            if ((st = mg_solve(mg, e1(l - 1), mg->tmp[l - 1], r1(l - 1), l - 1, coarse_its))) return st;
         } else {
-            if ((st = mg_smooth(mg, mg->e1[l - 1], mg->tmp[l - 1], mg->r1[l - 1], l - 1))) return st;
+            if ((st = mg_smooth(mg, e1(l - 1), mg->tmp[l - 1], r1(l - 1), l - 1))) return st;
         }
     }
-    if ((st = artss_copy(ctx, out, mg->e1[0], 0))) return st;
     return mg_bc(mg, out, 0);
 }
 
@@ -1427,9 +1431,11 @@ static int mg_capture(artss_mg *mg, double *p, const double *rhs) {
     int64_t f0[FAM_COUNT];
     for (int f = 0; f < FAM_COUNT; f++) f0[f] = ctx->prof.launches[f];
     ARTSS_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    int st = artss_mg_set_rhs(mg, p, rhs);
+    // VCycleMG::UpdateInput's copies are not needed: level 0 works on p and
+    // reads rhs directly, and the smoother sets its scratch itself
+    int st = ARTSS_OK;
     int64_t coarse = 0;
-    for (int c = 0; c < mg->cfg.n_cycle && !st; c++) st = mg_vcycle(mg, p, &coarse);
+    for (int c = 0; c < mg->cfg.n_cycle && !st; c++) st = mg_vcycle(mg, p, &coarse, rhs);
     cudaGraph_t graph = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
     if (st) { if (graph) cudaGraphDestroy(graph); return st; }
@@ -1501,9 +1507,8 @@ int artss_mg_pressure(artss_mg *mg, double *p, const double *rhs, int first_step
         cycles = mg->cfg.n_cycle;
         coarse = -1;
     } else {
-        if ((st = artss_mg_set_rhs(mg, p, rhs))) return st;
         for (int c = 0; c < mg->cfg.n_cycle; c++) {
-            if ((st = mg_vcycle(mg, p, &coarse))) return st;
+            if ((st = mg_vcycle(mg, p, &coarse, rhs))) return st;
             cycles++;
         }
     }

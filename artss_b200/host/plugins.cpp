@@ -231,8 +231,8 @@ void GaussFunction::update_source(Field &out, real t_cur) {
         return;
     }
     const real time_val = std::tanh(t_cur / m_settings.tau);
-    out.copy_data(m_spatial);
-    out *= time_val;
+    // out.copy_data(spatial); out *= time_val; as one pass (the same product)
+    check(artss_scale_copy(m_rt.ctx(), out.data, m_spatial.data, time_val, (int) out.get_level()), "source");
     if (m_noise) {
         std::vector<real> noise = m_noise->random_field(out.get_size());
         if (m_absolute) {
