@@ -233,7 +233,8 @@ int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, in
 // TMA descriptor of a level array for kTmaBoxX x kTmaBoxY plane windows (tma.cu);
 // tma_level_ok: the level's row pitch allows TMA (Nx even).
 bool tma_level_ok(const artss_ctx *ctx, int level);
-int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorMap **out);
+int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorMap **out, int box_x = kTmaBoxX,
+                  int box_y = kTmaBoxY);
 
 // Reductions (reduce.cu): sum of per-block partials -> loop state `slot`.
 //   mode 0: residual = sqrt(sum); it += 1; cond = residual > tol && it < max_it

@@ -606,6 +606,197 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     if (partials && tid == 0) partials[block_linear()] = acc;
 }
 
+// ---- the sweep with red and black in one phase ------------------------------
+//
+// The same iteration with black two planes behind red: at plane step k a
+// block updates red on plane k (tile + 1-cell ring) and black on plane k-2
+// (tile).  Black on k-2 reads only red values that are final (planes k-3..k-1,
+// red on k-1 done in the previous step) and none that this step's red update
+// writes; red on k reads planes k-1..k+1, whose black cells are still the old
+// ones.  One block barrier per step therefore separates the steps, and every
+// thread has two independent updates in the phase between them.  x arrives in
+// a 70 x 12 window (tile + 2-cell ring from the even x at or below the ring),
+// b and EV in 66 x 10 windows (tile + 1-cell ring, which starts at an even x
+// when the inner box starts at an odd one), seven and six planes deep, two
+// planes ahead; all three loads of a plane complete on its mbarrier, whose
+// waits are bounded.
+constexpr int kSt2BoxX = 70, kSt2BoxBX = kSwTx + 2, kSt2BoxBY = kSwTy + 2;
+constexpr int kSt2SlotsX = 7, kSt2SlotsB = 6;
+constexpr int kSt2PlaneX = 848;  // doubles per x slot: 70 x 12 = 840, padded to a 128-byte multiple
+constexpr int kSt2PlaneB = 672;  // doubles per b / EV slot: 66 x 10 = 660, padded
+constexpr unsigned kSt2BytesX = kSt2BoxX * kTmaBoxY * sizeof(double);
+constexpr unsigned kSt2BytesB = kSt2BoxBX * kSt2BoxBY * sizeof(double);
+static_assert(kSt2BoxX >= kSwTx + 5 && (kSt2PlaneX * 8) % 128 == 0 && (kSt2PlaneB * 8) % 128 == 0, "slots");
+static_assert(kSt2BoxX * kTmaBoxY <= kSt2PlaneX && kSt2BoxBX * kSt2BoxBY <= kSt2PlaneB, "windows fit their slots");
+
+inline size_t sweep_tma2_smem(bool turb) {
+    return (size_t) kSt2PlaneX * kSt2SlotsX * sizeof(double) +
+           (size_t) kSt2PlaneB * kSt2SlotsB * (turb ? 2 : 1) * sizeof(double);
+}
+
+template <bool TURB, int ZB>
+__global__ void __launch_bounds__(kStThreads, 2)
+k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
+                 const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out,
+                 const uint8_t *__restrict__ flags, Level L, Box3 box, DiffCoef c, double *__restrict__ partials,
+                 LoopState *__restrict__ pred) {
+    extern __shared__ __align__(1024) double st_sm[];
+    __shared__ double smem[32];
+    __shared__ __align__(8) uint64_t bars[kSt2SlotsX];
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
+    double *X = st_sm;                                // [kSt2SlotsX][kSt2PlaneX]
+    double *B = st_sm + kSt2SlotsX * kSt2PlaneX;      // [kSt2SlotsB][kSt2PlaneB]
+    double *E = B + kSt2SlotsB * kSt2PlaneB;          // [kSt2SlotsB][kSt2PlaneB] (TURB)
+    const int tid = threadIdx.x;
+    // 32-bit indices: the host takes this kernel only for levels of fewer than 2^31 cells
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    const int bx0 = (int) box.x0, bx1 = (int) box.x1, by0 = (int) box.y0, by1 = (int) box.y1;
+    const int bz0 = (int) box.z0, bz1 = (int) box.z1;
+    const int wx0 = bx0 + (int) blockIdx.x * kSwTx - 2;  // global i of ring column 0
+    const int wxa = wx0 - (wx0 & 1);                      // x window start, even
+    const int ox = wx0 - wxa;
+    const int wb = wx0 + 1;                               // b / EV window start (even: box.x0 odd)
+    const int wy0 = by0 + (int) blockIdx.y * kSwTy - 2;
+    const int kc0 = bz0 + (int) blockIdx.z * ZB;
+    const int kc1 = min(kc0 + ZB - 1, bz1);
+    const int pbase = kc0 - 2, plast = kc1 + 2;  // staged planes
+
+    if (tid == 0) {
+        for (int s = 0; s < kSt2SlotsX; s++) mbar_init(&bars[s], 1);
+        fence_proxy_async();
+    }
+    __syncthreads();
+    // thread 0: load plane p into its slots
+    auto issue = [&](int p) {
+        if (p > plast) return;
+        const unsigned u = (unsigned) (p - pbase);
+        uint64_t *bar = &bars[u % kSt2SlotsX];
+        mbar_expect_tx(bar, kSt2BytesX + kSt2BytesB * (TURB ? 2u : 1u));
+        tma_load_plane(X + (u % kSt2SlotsX) * kSt2PlaneX, &tm_x, wxa, wy0, p, bar);
+        tma_load_plane(B + (u % kSt2SlotsB) * kSt2PlaneB, &tm_b, wb, wy0 + 1, p, bar);
+        if (TURB) tma_load_plane(E + (u % kSt2SlotsB) * kSt2PlaneB, &tm_e, wb, wy0 + 1, p, bar);
+    };
+    auto ready = [&](int p) -> bool {
+        const unsigned u = (unsigned) (p - pbase);
+        return mbar_wait(&bars[u % kSt2SlotsX], (u / kSt2SlotsX) & 1u, kStPolls);
+    };
+    // ring slots by local plane number (32-bit, constant divisors)
+    auto xslot = [&](int p) { return X + ((unsigned) (p - pbase) % (unsigned) kSt2SlotsX) * kSt2PlaneX; };
+    auto bslot = [&](int p) { return (int) (((unsigned) (p - pbase) % (unsigned) kSt2SlotsB) * kSt2PlaneB); };
+    // e: the cell in the x window, eb: in the b / EV window
+    auto update = [&](const double *xm, const double *x0, const double *xp, int e, int eb, double &res2) {
+        double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+        if (TURB) {
+            turb_alpha(c, E[eb], ax, ay, az, rb);
+            beta = 1. / rb;
+        }
+        const double old = x0[e];
+        const double out_h = beta * (c.dsign * B[eb] + ax * (x0[e + 1] + x0[e - 1]) +
+                                     ay * (x0[e + kSt2BoxX] + x0[e - kSt2BoxX]) + az * (xp[e] + xm[e]));
+        const double nw = c.omw * old + c.w * out_h;
+        const double r = rb * (nw - old);
+        res2 = r * r;
+        return nw;
+    };
+
+    // this thread's red x-pair (tile + ring) and black x-pair (tile)
+    const int ry = 1 + tid / ((kSwTx + 2) / 2), px = tid % ((kSwTx + 2) / 2);
+    const int gjr = wy0 + ry;
+    const bool red_row_ok = gjr >= by0 && gjr <= by1;
+    const int red_row = nj * gjr;
+    const bool red_tile = ry >= 2 && ry < kSwTy + 2;
+    const bool has_black = tid < (kSwTx / 2) * kSwTy;
+    const int tx = tid % (kSwTx / 2), ty = tid / (kSwTx / 2);
+    const int gjb = wy0 + 2 + ty;
+    const int black_row = nj * gjb;
+    const int lx0 = 2 + 2 * tx;
+    auto red_x = [&](int k) { return 1 + 2 * px + ((wx0 + 1 + gjr + k) & 1); };  // (i + j + k) even
+    auto red_flag = [&](int k) -> uint8_t {
+        if (!red_row_ok || k < bz0 || k > bz1) return 0;
+        const int gi = wx0 + red_x(k);
+        if (gi < bx0 || gi > bx1) return 0;
+        return __ldg(flags + gi + red_row + nk * k);
+    };
+    auto black_par = [&](int kb) { return (wx0 + lx0 + gjb + kb + 1) & 1; };  // (i + j + k) odd
+    auto black_flag = [&](int kb) -> uint8_t {
+        if (!has_black || gjb > by1 || kb < kc0 || kb > kc1) return 0;
+        const int gi = wx0 + lx0 + black_par(kb);
+        if (gi > bx1) return 0;
+        return __ldg(flags + gi + black_row + nk * kb);
+    };
+
+    double acc = 0.0;
+    int issued = kc0 - 1 + kSwD;  // thread 0's last issued plane
+    if (tid == 0)
+        for (int p = pbase; p <= issued; p++) issue(p);
+    bool ok = tid != 0 || (ready(pbase) && ready(pbase + 1));
+    uint8_t fr = red_flag(kc0 - 1), fb = black_flag(kc0 - 3);
+    bool failed = false;
+    int waited = pbase + 1;  // planes up to here have landed
+    for (int k = kc0 - 1; k <= kc1 + 2; k++) {
+        // the next step's flags, loaded early
+        const uint8_t fr_next = red_flag(k + 1), fb_next = black_flag(k - 1);
+        // thread 0 waits for plane k+1; the barrier below publishes it (and the
+        // previous step's red writes) to the block
+        if (tid == 0 && k + 1 <= plast) ok = ok && ready(k + 1);
+        fence_proxy_async();  // this thread's shared-memory writes before the slot refill below
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        if (k + 1 <= plast) waited = k + 1;
+        if (tid == 0 && k + 1 + kSwD <= plast) {
+            issue(k + 1 + kSwD);
+            issued = k + 1 + kSwD;
+        }
+        // red on plane k, tile + 1-cell ring (planes up to kc1 + 1 are staged around it)
+        if ((fr & kInner) && k <= kc1 + 1) {
+            const int rx = red_x(k);
+            const int e = rx + ox + kSt2BoxX * ry;
+            const int eb = bslot(k) + (rx - 1) + kSt2BoxBX * (ry - 1);
+            double *x0 = xslot(k);
+            double r2;
+            const double nw = update(xslot(k - 1), x0, xslot(k + 1), e, eb, r2);
+            x0[e] = nw;
+            if (red_tile && rx >= 2 && rx < kSwTx + 2 && k >= kc0 && k <= kc1) acc += r2;
+        }
+        // black on plane k-2, tile only, and the tile's plane k-2 out
+        const int kb = k - 2;
+        if (has_black && kb >= kc0 && kb <= kc1 && gjb <= by1) {
+            const double *x0 = xslot(kb);
+            const int par = black_par(kb);
+            const int e0 = lx0 + ox + kSt2BoxX * (2 + ty);
+            const int eb0 = bslot(kb) + (lx0 - 1) + kSt2BoxBX * (1 + ty);
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int gi = wx0 + lx0 + s;
+                if (gi > bx1) continue;
+                double v = x0[e0 + s];
+                if (s == par && (fb & kInner)) {
+                    double r2;
+                    v = update(xslot(kb - 1), x0, xslot(kb + 1), e0 + s, eb0 + s, r2);
+                    acc += r2;
+                }
+                out[gi + black_row + nk * kb] = v;
+            }
+        }
+        fr = fr_next;
+        fb = fb_next;
+    }
+    if (failed) {
+        // a plane never arrived: flag it, let the loads in flight land, leave
+        if (tid == 0) {
+            if (pred) *(volatile int *) &pred->pad = 1;
+            for (int p = waited + 1; p <= issued; p++) (void) ready(p);
+        }
+        __syncthreads();
+        return;
+    }
+    acc = artss_block_sum(acc, smem);
+    if (partials && tid == 0) partials[block_linear()] = acc;
+}
+
 // One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
 // the division by reciprocal_beta; turbulent: :345-362) + residual partials
 // of sum (rbeta * (out - in))^2 (:72-79).
@@ -824,61 +1015,89 @@ int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, in
 
 namespace {
 
-// The TMA sweep with z-depth kStDepths[v]; returns the number of blocks (partials).
-int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, size_t smem, const CUtensorMap &mx,
-                     const CUtensorMap &mb, const CUtensorMap &me, double *w, const Level &L, const DiffCoef &c,
-                     LoopState *pred, int *nb) {
-    const dim3 g = sweep_tma_grid(box, kStDepths[v]);
+// TMA descriptors of one sweep: x (the array read), b, EV, for the kernel with
+// 72 x 12 windows and for the one-phase kernel (70 x 12 and 66 x 10)
+struct SweepMaps {
+    const CUtensorMap *x = nullptr, *b = nullptr, *e = nullptr;
+    const CUtensorMap *x2 = nullptr, *b2 = nullptr, *e2 = nullptr;
+};
+
+// Variants of the TMA sweep: v < 3 the kernel with two barriers per plane step
+// and z-depth kStDepths[v]; v >= 3 the one-phase kernel with kStDepths[v - 3]
+// (only where its b / EV window starts at an even x).  Returns the number of
+// blocks (partials) in *nb.
+int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, const SweepMaps &m, double *w,
+                     const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
+    const int zb = kStDepths[v % 3];
+    const dim3 g = sweep_tma_grid(box, zb);
     *nb = nblocks(g);
-#define ARTSS_SWEEP_TMA(T, Z)                                                                               \
-    ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep_tma<T, Z><<<g, kStThreads, smem, ctx->stream>>>(                 \
-                                   mx, mb, me, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred))
+    const size_t smem1 = sweep_tma_smem(turb), smem2 = sweep_tma2_smem(turb);
+#define ARTSS_SWEEP_TMA(K, T, Z, SM, MX, MB, ME)                                                           \
+    ARTSS_LAUNCH(ctx, FAM_CGS, K<T, Z><<<g, kStThreads, SM, ctx->stream>>>(                                \
+                                   *MX, *MB, *ME, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred))
     switch (v * 2 + (turb ? 1 : 0)) {
-        case 0: ARTSS_SWEEP_TMA(false, 8); break;
-        case 1: ARTSS_SWEEP_TMA(true, 8); break;
-        case 2: ARTSS_SWEEP_TMA(false, 16); break;
-        case 3: ARTSS_SWEEP_TMA(true, 16); break;
-        case 4: ARTSS_SWEEP_TMA(false, 32); break;
-        default: ARTSS_SWEEP_TMA(true, 32); break;
+        case 0: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, false, 8, smem1, m.x, m.b, m.e); break;
+        case 1: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, true, 8, smem1, m.x, m.b, m.e); break;
+        case 2: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, false, 16, smem1, m.x, m.b, m.e); break;
+        case 3: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, true, 16, smem1, m.x, m.b, m.e); break;
+        case 4: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, false, 32, smem1, m.x, m.b, m.e); break;
+        case 5: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, true, 32, smem1, m.x, m.b, m.e); break;
+        case 6: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, false, 8, smem2, m.x2, m.b2, m.e2); break;
+        case 7: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, true, 8, smem2, m.x2, m.b2, m.e2); break;
+        case 8: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, false, 16, smem2, m.x2, m.b2, m.e2); break;
+        case 9: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, true, 16, smem2, m.x2, m.b2, m.e2); break;
+        case 10: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, false, 32, smem2, m.x2, m.b2, m.e2); break;
+        default: ARTSS_SWEEP_TMA(k_cgs_sweep_tma2, true, 32, smem2, m.x2, m.b2, m.e2); break;
     }
 #undef ARTSS_SWEEP_TMA
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
-int set_sweep_smem(bool turb, size_t smem) {
-    const int b = (int) smem;
+int set_sweep_smem(bool turb) {
+    static bool done[2] = {false, false};
+    if (done[turb]) return ARTSS_OK;
+    const int b1 = (int) sweep_tma_smem(turb), b2 = (int) sweep_tma2_smem(turb);
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (turb) {
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 8>, attr, b2));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 16>, attr, b2));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 32>, attr, b2));
     } else {
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, attr, b1));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<false, 8>, attr, b2));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<false, 16>, attr, b2));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<false, 32>, attr, b2));
     }
+    done[turb] = true;
     return ARTSS_OK;
 }
 
-// Autotuner of the sweep's z-depth: the first solve on a level shape times
-// every depth on that solve's first iteration (the sweep reads `rd`, b, EV and
-// writes only `w` and the partials, so repeating it changes nothing) and keeps
-// the fastest for the context.
-int tune_sweep(artss_ctx *ctx, bool turb, const Box3 &box, size_t smem, const CUtensorMap &mx, const CUtensorMap &mb,
-               const CUtensorMap &me, double *w, const Level &L, const DiffCoef &c, LoopState *pred, int *choice) {
+// Autotuner of the sweep: the first solve on a level shape times every
+// variant (kernel and z-depth) on that solve's first iteration (the sweep
+// reads `rd`, b, EV and writes only `w` and the partials, so repeating it
+// changes nothing) and keeps the fastest for the context.
+int tune_sweep(artss_ctx *ctx, bool turb, bool one_phase, const Box3 &box, const SweepMaps &m, double *w,
+               const Level &L, const DiffCoef &c, LoopState *pred, int *choice) {
     const TuneKey key{0, L.Nx, L.Ny, L.Nz, turb ? 1 : 0};
     auto it = ctx->tuned.find(key);
-    if (it != ctx->tuned.end()) { *choice = it->second; return ARTSS_OK; }
-    if (!ctx->autotune || ctx->capturing) { *choice = 1; return ARTSS_OK; }
+    if (it != ctx->tuned.end() && (one_phase || it->second < 3)) { *choice = it->second; return ARTSS_OK; }
+    const int fallback = one_phase ? 4 : 1;
+    if (!ctx->autotune || ctx->capturing) { *choice = fallback; return ARTSS_OK; }
     cudaEvent_t e0, e1;
     ARTSS_CK(cudaEventCreate(&e0));
     ARTSS_CK(cudaEventCreate(&e1));
-    int best = 1, st = ARTSS_OK, nb = 0;
+    int best = fallback, st = ARTSS_OK, nb = 0;
     float best_ms = 1e30f;
-    for (int v = 0; v < 3 && !st; v++) {
-        if ((st = launch_sweep_tma(ctx, turb, v, box, smem, mx, mb, me, w, L, c, pred, &nb))) break;  // warm
+    for (int v = 0; v < (one_phase ? 6 : 3) && !st; v++) {
+        if ((st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb))) break;  // warm
         cudaEventRecord(e0, ctx->stream);
-        for (int r = 0; r < 3 && !st; r++) st = launch_sweep_tma(ctx, turb, v, box, smem, mx, mb, me, w, L, c, pred, &nb);
+        for (int r = 0; r < 3 && !st; r++) st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb);
         cudaEventRecord(e1, ctx->stream);
         if (cudaEventSynchronize(e1) != cudaSuccess) { st = cuda_fail(cudaGetLastError(), "autotune"); break; }
         float ms = 0;
@@ -906,7 +1125,7 @@ int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
     if (!ctx) return 0;
     const Level &L = ctx->lvl[0];
     auto it = ctx->tuned.find(TuneKey{0, L.Nx, L.Ny, L.Nz, turbulent ? 1 : 0});
-    return it == ctx->tuned.end() ? 0 : kStDepths[it->second];
+    return it == ctx->tuned.end() ? 0 : kStDepths[it->second % 3];
 }
 
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
@@ -926,12 +1145,14 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     const bool tma = tma_level_ok(ctx, 0) && L.size() < ((int64_t) 1 << 31);
     const size_t smem = tma ? sweep_tma_smem(ev != nullptr) : sweep_smem(ev != nullptr);
     if (tma) {
-        if ((st = set_sweep_smem(ev != nullptr, smem))) return st;
+        if ((st = set_sweep_smem(ev != nullptr))) return st;
     } else {
         if (ev) ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         else ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     }
-    const CUtensorMap *tm_b = nullptr, *tm_e = nullptr, *tm_x[2] = {nullptr, nullptr};
+    // one-phase kernel: its b / EV window starts at an even x when the inner box starts at an odd one
+    const bool one_phase = tma && (box.x0 & 1) == 1;
+    SweepMaps maps[2];  // by the array read: buf[0] = out, buf[1] = in
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
     // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
     if ((st = artss_copy(ctx, out, in, 0))) return st;
@@ -952,17 +1173,25 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     double *buf[2] = {out, in};
     const int s0 = (int) (batch & 1);  // iteration n writes buf[(s0 + n) & 1]
     if (tma) {
-        if ((st = tensor_map_3d(ctx, out, 0, &tm_x[0]))) return st;
-        if ((st = tensor_map_3d(ctx, in, 0, &tm_x[1]))) return st;
-        if ((st = tensor_map_3d(ctx, b, 0, &tm_b))) return st;
-        tm_e = tm_b;
-        if (ev && (st = tensor_map_3d(ctx, ev, 0, &tm_e))) return st;
+        for (int r = 0; r < 2; r++) {
+            SweepMaps &m = maps[r];
+            if ((st = tensor_map_3d(ctx, buf[r], 0, &m.x))) return st;
+            if ((st = tensor_map_3d(ctx, b, 0, &m.b))) return st;
+            m.e = m.b;
+            if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e))) return st;
+            if (one_phase) {
+                if ((st = tensor_map_3d(ctx, buf[r], 0, &m.x2, kSt2BoxX, kTmaBoxY))) return st;
+                if ((st = tensor_map_3d(ctx, b, 0, &m.b2, kSt2BoxBX, kSt2BoxBY))) return st;
+                m.e2 = m.b2;
+                if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e2, kSt2BoxBX, kSt2BoxBY))) return st;
+            }
+        }
     }
     LoopState *pred_rw = ctx->d_loop + slot;
-    int depth = 1;
+    int depth = 1;  // the sweep variant (launch_sweep_tma)
     if (tma && cond) {
         const int n1 = (s0 + 1) & 1;
-        if ((st = tune_sweep(ctx, ev != nullptr, box, smem, *tm_x[1 - n1], *tm_b, *tm_e, buf[n1], L, c, pred_rw, &depth)))
+        if ((st = tune_sweep(ctx, ev != nullptr, one_phase, box, maps[1 - n1], buf[n1], L, c, pred_rw, &depth)))
             return st;
     }
     if (ctx->capturing) {
@@ -975,8 +1204,8 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
                 double *w = buf[(s0 + n) & 1];
                 const double *rd = buf[(s0 + n + 1) & 1];
                 if (tma) {
-                    if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, smem, *tm_x[(s0 + n + 1) & 1], *tm_b,
-                                               *tm_e, w, L, c, pred_rw, &nb)))
+                    if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, maps[(s0 + n + 1) & 1], w, L, c,
+                                               pred_rw, &nb)))
                         return st;
                 } else if (ev)
                     ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(
@@ -1004,8 +1233,8 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
             double *w = buf[(s0 + n) & 1];
             const double *rd = buf[(s0 + n + 1) & 1];
             if (tma) {
-                if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, smem, *tm_x[(s0 + n + 1) & 1], *tm_b,
-                                           *tm_e, w, L, c, pred_rw, &nb)))
+                if ((st = launch_sweep_tma(ctx, ev != nullptr, depth, box, maps[(s0 + n + 1) & 1], w, L, c, pred_rw,
+                                           &nb)))
                     return st;
             } else if (ev)
                 ARTSS_LAUNCH(ctx, FAM_CGS, k_cgs_sweep<true><<<g, dim3(kSwTx / 2, kSwTy), smem, ctx->stream>>>(

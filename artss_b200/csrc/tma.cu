@@ -23,8 +23,9 @@ bool tma_level_ok(const artss_ctx *ctx, int level) {
     return (ctx->lvl[level].Nx % 2) == 0;
 }
 
-int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorMap **out) {
-    const auto key = std::make_pair((const void *) base, level);
+int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorMap **out, int box_x, int box_y) {
+    // cached per (array, level, box)
+    const auto key = std::make_pair((const void *) base, level | (box_x << 8) | (box_y << 20));
     auto it = ctx->tmaps.find(key);
     if (it != ctx->tmaps.end()) {
         *out = &it->second;
@@ -45,7 +46,10 @@ int tensor_map_3d(artss_ctx *ctx, const double *base, int level, const CUtensorM
     CUtensorMap m;
     const cuuint64_t dim[3] = {(cuuint64_t) L.Nx, (cuuint64_t) L.Ny, (cuuint64_t) L.Nz};
     const cuuint64_t stride[2] = {(cuuint64_t) L.Nx * sizeof(double), (cuuint64_t) L.Nx * L.Ny * sizeof(double)};
-    const cuuint32_t box[3] = {kTmaBoxX, kTmaBoxY, 1};
+    if ((box_x * (int) sizeof(double)) % 16 != 0 || box_x > 256 || box_y > 256) {
+        set_error("TMA box not a multiple of 16 bytes"); return ARTSS_ERR_ARG;
+    }
+    const cuuint32_t box[3] = {(cuuint32_t) box_x, (cuuint32_t) box_y, 1};
     const cuuint32_t estride[3] = {1, 1, 1};
     const CUresult r = g_encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *) base, dim, stride, box, estride,
                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
