@@ -1121,6 +1121,13 @@ int artss_ctx_autotune(artss_ctx *ctx, int enable) {
     return ARTSS_OK;
 }
 
+int artss_cgs_sweep_variant(artss_ctx *ctx, int turbulent) {
+    if (!ctx) return -1;
+    const Level &L = ctx->lvl[0];
+    auto it = ctx->tuned.find(TuneKey{0, L.Nx, L.Ny, L.Nz, turbulent ? 1 : 0});
+    return it == ctx->tuned.end() ? -1 : it->second;
+}
+
 int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
     if (!ctx) return 0;
     const Level &L = ctx->lvl[0];

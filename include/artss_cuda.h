@@ -268,6 +268,9 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
  * artss_cgs_sweep_depth returns the chosen depth, 0 before the first solve. */
 int artss_ctx_autotune(artss_ctx *ctx, int enable);
 int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent);
+/* the tuned sweep variant of level 0 (0-2: two-phase kernel of z-depth 8,
+ * 16, 32; 3-5: one-phase kernel), -1 before the first solve */
+int artss_cgs_sweep_variant(artss_ctx *ctx, int turbulent);
 /* IDiffusion::diffuse, JacobiDiffuse (src/diffusion/JacobiDiffuse.cpp:31-203). */
 int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b,
                          double D, const double *ev, double dt, int field_type,
