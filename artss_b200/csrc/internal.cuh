@@ -53,7 +53,7 @@ struct BcProgram {
     // plan of the pipelined coarse solve: state -2 unknown, -1 not eligible, 1 planned
     int pipe_state = -2;
     std::vector<int> pipe_kb;          // plane split, ranks + 1 entries
-    int pipe_ranks = 0, pipe_cap = 0, pipe_tcap = 0;
+    int pipe_ranks = 0, pipe_cap = 0, pipe_tcap = 0, pipe_fcap = 0;
     int64_t pipe_smem = 0;
 };
 

@@ -658,14 +658,14 @@ __global__ void __launch_bounds__(kClusterThreads, 1)
 k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restrict__ b,
                         const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
                         BcView bc, double tol, int rel, long long max_it, PlaneSplit sp, int plane_cap,
-                        int target_cap, LoopState *__restrict__ st, const LoopState *__restrict__ pred) {
+                        int target_cap, int fix_cap, LoopState *__restrict__ st, const LoopState *__restrict__ pred) {
     namespace cg = cooperative_groups;
     if (pred && !pred->cond) return;  // every rank reads the same flag
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) double sm[];
     __shared__ double red[32];
     __shared__ double parts[2][kPipeMaxRanks];
-    __shared__ int s_nt, s_over, s_overs[kPipeMaxRanks], s_fail;
+    __shared__ int s_nt, s_nf, s_over, s_overs[kPipeMaxRanks], s_fail;
     __shared__ __align__(8) uint64_t hb[3];  // halo arrivals per buffer
     const int tid = threadIdx.x;
     const int rank = (int) cl.block_rank();
@@ -674,10 +674,12 @@ k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__
     const int kb0 = sp.kb[rank], kb1 = sp.kb[rank + 1], own = kb1 - kb0;
     const int bstride = (plane_cap + 2) * nk;  // doubles per buffer (nk even: 16-byte planes)
     double *X = sm;
-    HaloTarget *tg = (HaloTarget *) (sm + 3 * (int64_t) bstride);
+    HaloTarget *tg = (HaloTarget *) (sm + 3 * (int64_t) bstride);  // targets and roots in own planes
+    HaloTarget *fx = tg + target_cap;                                  // the chain crosses to a neighbour
     const uint32_t base = (uint32_t) __cvta_generic_to_shared(sm);
     if (tid == 0) {
         s_nt = 0;
+        s_nf = 0;
         s_over = 0;
         s_fail = 0;
         for (int s = 0; s < 3; s++) tc::mbar_init(&hb[s], 1);
@@ -715,44 +717,53 @@ k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__
         }
     }
     __syncthreads();
-    // the boundary program on iterate 0 for the targets in own planes (roots
+    // The boundary program on iterate 0 for the targets in own planes (roots
     // lie within one plane, in own or halo planes, and are never targets), and
-    // the table of the targets whose root is an inner cell (the split keeps
-    // such a root in its target's rank); the others stay as set here
+    // two tables of the targets whose root is an inner cell: target and root in
+    // own planes (re-evaluated in the sweep from the root's new value), and a
+    // chain that crosses to a neighbouring rank, target or root in a halo plane
+    // (re-evaluated at the start of the next sweep, once the halo has arrived,
+    // by both ranks); targets of constant roots stay as set here.
     const int64_t q_begin = bc.waves > 0 ? bc.begin[0] : 0, q_end = bc.waves > 0 ? bc.begin[1] : 0;
     for (int64_t q0 = q_begin; q0 < q_end; q0 += kClusterThreads) {
         const int64_t qq = q0 + tid;
         if (qq >= q_end) continue;
         const int t = (int) __ldg(bc.target + qq), kt = t / nk;
-        if (kt < kb0 || kt >= kb1) continue;
         const int r = (int) __ldg(bc.root + qq), kr = r / nk;
+        const bool own_t = kt >= kb0 && kt < kb1, own_r = kr >= kb0 && kr < kb1;
+        const bool halo_t = kt == kb0 - 1 || kt == kb1, halo_r = kr == kb0 - 1 || kr == kb1;
+        if (!own_t && !own_r) continue;
         const int d = __ldg(bc.depth + qq);
         const uint8_t mneg = __ldg(bc.neg + qq);
-        double x = X[(kr - kb0 + 1) * nk + (r - kr * nk)];
+        if (own_t) {
+            double x = X[(kr - kb0 + 1) * nk + (r - kr * nk)];
 #pragma unroll
-        for (int s = 0; s < kBcMaxDepth; s++)
-            if (s < d) x = ((mneg >> s) & 1 ? -x : x) + (bc.value ? __ldg(bc.value + s * bc.n + qq) : 0.0);
-        X[(kt - kb0 + 1) * nk + (t - kt * nk)] = x;
+            for (int s = 0; s < kBcMaxDepth; s++)
+                if (s < d) x = ((mneg >> s) & 1 ? -x : x) + (bc.value ? __ldg(bc.value + s * bc.n + qq) : 0.0);
+            X[(kt - kb0 + 1) * nk + (t - kt * nk)] = x;
+        }
         if (!(__ldg(flags + r) & kInner)) continue;  // constant root: set once above
-        if (kr < kb0 || kr >= kb1) {
-            s_over = 1;  // the split did not keep the root with its target
+        HaloTarget *h = nullptr;
+        if (own_t && own_r) {
+            const int slot = atomicAdd(&s_nt, 1);
+            if (slot < target_cap) h = &tg[slot];
+        } else if ((own_t && halo_r) || (own_r && halo_t)) {
+            const int slot = atomicAdd(&s_nf, 1);
+            if (slot < fix_cap) h = &fx[slot];
+        }
+        if (!h) {
+            s_over = 1;  // a table overflowed, or a chain spans more than one plane
             continue;
         }
-        const int slot = atomicAdd(&s_nt, 1);
-        if (slot >= target_cap) {
-            s_over = 1;
-            continue;
-        }
-        HaloTarget &h = tg[slot];
 #pragma unroll
-        for (int s = 0; s < kBcMaxDepth; s++) h.val[s] = (s < d && bc.value) ? __ldg(bc.value + s * bc.n + qq) : 0.0;
-        h.dst = (uint32_t) ((kt - kb0 + 1) * nk + (t - kt * nk));
-        h.root = (uint32_t) ((kr - kb0 + 1) * nk + (r - kr * nk));
-        h.depth_neg = (uint32_t) d | (uint32_t) mneg << 8;
-        h.pad = 0;
+        for (int s = 0; s < kBcMaxDepth; s++) h->val[s] = (s < d && bc.value) ? __ldg(bc.value + s * bc.n + qq) : 0.0;
+        h->dst = (uint32_t) ((kt - kb0 + 1) * nk + (t - kt * nk));
+        h->root = (uint32_t) ((kr - kb0 + 1) * nk + (r - kr * nk));
+        h->depth_neg = (uint32_t) d | (uint32_t) mneg << 8;
+        h->pad = 0;
     }
     __syncthreads();
-    const int nt = min(s_nt, target_cap);
+    const int nt = min(s_nt, target_cap), nf = min(s_nf, fix_cap);
     cl.sync();
     // every rank learns every rank's error flag, so all take the same path
     if (tid < cs) cl.map_shared_rank(s_overs, tid)[rank] = s_over;
@@ -811,6 +822,21 @@ k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__
                 }
                 unwaited = 0;
                 __syncthreads();
+                if (nf > 0) {
+                    // chains across ranks: iterate k-1's targets from its roots, now all present
+                    double *Pw = X + sp_ * bstride;
+                    for (int t = tid; t < nf; t += kClusterThreads) {
+                        const HaloTarget &h = fx[t];
+                        double x = Pw[h.root];
+                        const int d = (int) (h.depth_neg & 0xffu);
+                        const uint32_t mneg = h.depth_neg >> 8;
+#pragma unroll
+                        for (int s = 0; s < kBcMaxDepth; s++)
+                            if (s < d) x = ((mneg >> s) & 1 ? -x : x) + h.val[s];
+                        Pw[h.dst] = x;
+                    }
+                    __syncthreads();
+                }
             }
             double acc = 0.0, v[kPipeCells];
 #pragma unroll
@@ -956,7 +982,7 @@ bool cluster_fits(const artss_ctx *ctx, int level, int buffers, int *plane_cap, 
 // The split cuts the planes as evenly as the forbidden cuts allow.
 struct PipeLaunch {
     PlaneSplit split;
-    int ranks, plane_cap, target_cap;
+    int ranks, plane_cap, target_cap, fix_cap;
     int64_t smem;
 };
 
@@ -973,6 +999,7 @@ bool coarse_pipe_plan(artss_ctx *ctx, int level, PipeLaunch *pl) {
             p.pipe_ranks = fresh.ranks;
             p.pipe_cap = fresh.plane_cap;
             p.pipe_tcap = fresh.target_cap;
+            p.pipe_fcap = fresh.fix_cap;
             p.pipe_smem = fresh.smem;
         }
     }
@@ -981,6 +1008,7 @@ bool coarse_pipe_plan(artss_ctx *ctx, int level, PipeLaunch *pl) {
     pl->ranks = p.pipe_ranks;
     pl->plane_cap = p.pipe_cap;
     pl->target_cap = p.pipe_tcap;
+    pl->fix_cap = p.pipe_fcap;
     pl->smem = p.pipe_smem;
     return true;
 }
@@ -992,13 +1020,15 @@ bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
     const int nz = (int) L.Nz;
     if (cluster_ranks(L) < 2 || L.nxy() % 2 || in.empty() || (int64_t) in.size() != L.size()) return false;
     if (p.present && p.waves > 1) return false;
-    std::vector<char> forbidden(nz + 1, 0);  // forbidden[c]: no rank boundary between planes c-1 and c
+    // forbidden[c]: no rank boundary between planes c-1 and c; the ghost planes
+    // stay with their neighbour (a rank of a ghost plane alone has no cells)
+    std::vector<char> forbidden(nz + 1, 0);
+    forbidden[1] = forbidden[nz - 1] = 1;
     const int64_t n = p.present ? p.n : 0;
     for (int64_t q = 0; q < n; q++) {
         const int64_t t = p.h_target[q], r = p.h_root[q];
         const int kt = (int) (t / L.nxy()), kr = (int) (r / L.nxy());
         if (in[(size_t) t] || kr < kt - 1 || kr > kt + 1) return false;
-        if (in[(size_t) r] && kr != kt) forbidden[std::max(kr, kt)] = 1;
     }
     static bool attr_set = false;
     if (!attr_set) {
@@ -1028,20 +1058,28 @@ bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
         }
         if (!ok) continue;
         sp.kb[cs] = nz;
-        int cap = 0, tcap = 0;
+        int cap = 0, tcap = 0, fcap = 0;
         for (int r = 0; r < cs && ok; r++) {
-            cap = std::max(cap, sp.kb[r + 1] - sp.kb[r]);
-            const int64_t z0 = std::max<int64_t>(sp.kb[r], L.k1), z1 = std::min<int64_t>(sp.kb[r + 1] - 1, L.k2);
+            const int a = sp.kb[r], e = sp.kb[r + 1];
+            cap = std::max(cap, e - a);
+            const int64_t z0 = std::max<int64_t>(a, L.k1), z1 = std::min<int64_t>(e - 1, L.k2);
             if (z1 >= z0 && (z1 - z0 + 1) * nxy_in > (int64_t) kClusterThreads * kPipeCells) ok = false;
-            int nt = 0;
+            int nt = 0, nf = 0;
             for (int64_t q = 0; q < n; q++) {
-                const int kt = (int) (p.h_target[q] / L.nxy());
-                if (kt >= sp.kb[r] && kt < sp.kb[r + 1] && in[(size_t) p.h_root[q]]) nt++;
+                if (!in[(size_t) p.h_root[q]]) continue;
+                const int kt = (int) (p.h_target[q] / L.nxy()), kr = (int) (p.h_root[q] / L.nxy());
+                const bool own_t = kt >= a && kt < e, own_r = kr >= a && kr < e;
+                if (own_t && own_r) nt++;
+                else if ((own_t && (kr == a - 1 || kr == e)) || (own_r && (kt == a - 1 || kt == e))) nf++;
+                // a rank of one plane sends its plane both ways before such a
+                // target is set, and the far neighbour cannot set it itself
+                if (own_t && !own_r && e - a == 1) ok = false;
             }
             tcap = std::max(tcap, nt);
+            fcap = std::max(fcap, nf);
         }
         const int64_t smem = 3 * (int64_t) (cap + 2) * L.nxy() * (int64_t) sizeof(double) +
-                             (int64_t) tcap * (int64_t) sizeof(HaloTarget);
+                             (int64_t) (tcap + fcap) * (int64_t) sizeof(HaloTarget);
         if (!ok || smem > kCoarseSmemBytes) continue;
         // the device must be able to place a cluster of this size (more than 8 is non-portable)
         cudaLaunchConfig_t lc = {};
@@ -1065,6 +1103,7 @@ bool coarse_pipe_plan_new(artss_ctx *ctx, int level, PipeLaunch *pl) {
         pl->ranks = cs;
         pl->plane_cap = cap;
         pl->target_cap = tcap;
+        pl->fix_cap = fcap;
         pl->smem = smem;
         return true;
     }
@@ -1124,7 +1163,8 @@ int launch_coarse_pipe(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level,
     ARTSS_LAUNCH(ctx, FAM_MG_COARSE, ARTSS_CK(cudaLaunchKernelEx(&lc, k_mg_coarse_jacobi_pipe<TS>, out, tmp, b,
                                                                   (const uint8_t *) ctx->d_flags[level], L,
                                                                   inner_box(L), c, rx, ry, rz, v, tol, rel, mi,
-                                                                  pl.split, pl.plane_cap, pl.target_cap, st, pred)));
+                                                                  pl.split, pl.plane_cap, pl.target_cap, pl.fix_cap,
+                                                                  st, pred)));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
