@@ -159,6 +159,7 @@ def load_cuda() -> C.CDLL:
             "artss_laplacian": ([_P, _D, _D, C.c_int], C.c_int),
             "artss_cgs_sweep_variant": ([_P, C.c_int], C.c_int),
             "artss_ctx_autotune": ([_P, C.c_int], C.c_int),
+            "artss_ctx_pdl": ([_P, C.c_int], C.c_int),
             "artss_conv3d_fwd": ([_P, C.POINTER(ConvDesc), _P, _P, _P, _P], C.c_int),
             "artss_nn_check": ([_P], C.c_int),
             "artss_conv3d_wgrad": ([_P, C.POINTER(ConvDesc), _P, _P, _P], C.c_int),

@@ -28,17 +28,40 @@ __global__ void k_bc_wave(double *__restrict__ f, const int64_t *__restrict__ ta
                           const int64_t *__restrict__ root, const uint8_t *__restrict__ depth,
                           const uint8_t *__restrict__ neg, const double *__restrict__ value,
                           int64_t begin, int64_t end, int64_t n_total, const LoopState *__restrict__ pred) {
+    // the program's tables are constant: the first assignment's entries are
+    // read before waiting for the kernel that wrote f
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    int64_t q = begin + blockIdx.x * (int64_t) blockDim.x + threadIdx.x;
+    int64_t t = 0, r = 0;
+    int d = 0;
+    uint8_t m = 0;
+    double val[kBcMaxDepth];
+    if (q < end) {
+        t = target[q];
+        r = root[q];
+        d = depth[q];
+        m = neg[q];
+    }
+#pragma unroll
+    for (int s = 0; s < kBcMaxDepth; s++) val[s] = (q < end && s < d) ? value[s * n_total + q] : 0.0;
+    pdl_wait();
+    pdl_trigger();
     if (pred && !pred->cond) return;
-    for (int64_t q = begin + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < end;
-         q += (int64_t) gridDim.x * blockDim.x) {
-        double x = f[root[q]];
-        const int d = depth[q];
-        const uint8_t m = neg[q];
+    while (q < end) {
+        double x = f[r];
 #pragma unroll
         for (int s = 0; s < kBcMaxDepth; s++) {
-            if (s < d) x = ((m >> s) & 1 ? -x : x) + value[s * n_total + q];
+            if (s < d) x = ((m >> s) & 1 ? -x : x) + val[s];
         }
-        f[target[q]] = x;
+        f[t] = x;
+        q += stride;
+        if (q >= end) break;
+        t = target[q];
+        r = root[q];
+        d = depth[q];
+        m = neg[q];
+#pragma unroll
+        for (int s = 0; s < kBcMaxDepth; s++) val[s] = s < d ? value[s * n_total + q] : 0.0;
     }
 }
 
@@ -48,8 +71,13 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopSta
     for (int w = 0; w < p.waves; w++) {
         const int64_t b = p.wave_begin[w], e = p.wave_begin[w + 1];
         if (e <= b) continue;
-        ARTSS_LAUNCH(ctx, FAM_BC, k_bc_wave<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(f, p.d_target, p.d_root, p.d_depth, p.d_neg,
-                                                               p.d_value, b, e, p.n, pred));
+        cudaError_t err;
+        ARTSS_LAUNCH(ctx, FAM_BC,
+                     err = launch_pdl(ctx, k_bc_wave, dim3((unsigned) flat_blocks(e - b)), dim3(256), 0, f,
+                                      (const int64_t *) p.d_target, (const int64_t *) p.d_root,
+                                      (const uint8_t *) p.d_depth, (const uint8_t *) p.d_neg,
+                                      (const double *) p.d_value, b, e, p.n, pred));
+        if (err != cudaSuccess) return cuda_fail(err, "kernel launch");
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;

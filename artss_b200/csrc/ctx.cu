@@ -38,16 +38,22 @@ int check_field_type(int ft) {
 // ---------------------------------------------------------------- kernels
 
 __global__ void k_fill(double *__restrict__ f, int64_t n, double v) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
         f[i] = v;
 }
 
 __global__ void k_copy(double *__restrict__ d, const double *__restrict__ s, int64_t n) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
         d[i] = s[i];
 }
 
 __global__ void k_add_field(double *__restrict__ d, const double *__restrict__ s, int64_t n) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
         d[i] += s[i];
 }
@@ -58,11 +64,15 @@ __global__ void k_add_scalar(double *__restrict__ d, double x, int64_t n) {
 }
 
 __global__ void k_scale(double *__restrict__ d, double x, int64_t n) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
         d[i] *= x;
 }
 
 __global__ void k_scale_copy(double *__restrict__ d, const double *__restrict__ s, double x, int64_t n) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x)
         d[i] = s[i] * x;
 }
@@ -72,6 +82,8 @@ __global__ void k_couple3(const double *__restrict__ a, double *__restrict__ a0,
                           const double *__restrict__ b, double *__restrict__ b0, double *__restrict__ bt,
                           const double *__restrict__ c, double *__restrict__ c0, double *__restrict__ ct,
                           int64_t n) {
+    artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
         if (a) { const double x = a[i]; a0[i] = x; at[i] = x; }
         if (b) { const double x = b[i]; b0[i] = x; bt[i] = x; }
@@ -546,18 +558,18 @@ int artss_get_cell_flags(artss_ctx *ctx, int level, uint8_t *host_out, int64_t n
 
 int artss_fill(artss_ctx *ctx, double *f, int level, double value) {
     if (!f) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(f, n, value)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_fill, flat_blocks(n), 256, 0, f, n, value))
 }
 
 int artss_copy(artss_ctx *ctx, double *dst, const double *src, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
     if (dst == src) return check_level(ctx, level);
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_copy, flat_blocks(n), 256, 0, dst, src, n))
 }
 
 int artss_add_field(artss_ctx *ctx, double *dst, const double *src, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_add_field<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_add_field, flat_blocks(n), 256, 0, dst, src, n))
 }
 
 int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level) {
@@ -567,12 +579,12 @@ int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level) {
 
 int artss_scale(artss_ctx *ctx, double *dst, double x, int level) {
     if (!dst) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_scale<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, x, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_scale, flat_blocks(n), 256, 0, dst, x, n))
 }
 
 int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, int level) {
     if (!dst || !src) { set_error("null field"); return ARTSS_ERR_ARG; }
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_scale_copy<<<flat_blocks(n), 256, 0, ctx->stream>>>(dst, src, x, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_scale_copy, flat_blocks(n), 256, 0, dst, src, x, n))
 }
 
 int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
@@ -582,7 +594,7 @@ int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
         set_error("couple: incomplete triple"); return ARTSS_ERR_ARG;
     }
     const int level = 0;
-    ARTSS_FIELD_OP(ARTSS_LAUNCH(ctx, FAM_COUPLE, k_couple3<<<flat_blocks(n), 256, 0, ctx->stream>>>(a, a0, a_tmp, b, b0, b_tmp, c, c0, c_tmp, n)))
+    ARTSS_FIELD_OP(ARTSS_LAUNCH_PDL(ctx, FAM_COUPLE, k_couple3, flat_blocks(n), 256, 0, a, a0, a_tmp, b, b0, b_tmp, c, c0, c_tmp, n))
 }
 
 }  // extern "C"

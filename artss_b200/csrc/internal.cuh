@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <map>
+#include <utility>
 #include <string>
 #include <vector>
 #include <set>
@@ -127,6 +128,7 @@ struct artss_ctx {
     // whole-step capture (artss_graph_begin .. artss_graph_end): loops become
     // conditional WHILE nodes whose bodies are captured on body_stream
     bool capturing = false;
+    bool pdl = true;  // launch_pdl may overlap a launch with its predecessor's tail (eager runs)
     cudaStream_t body_stream = nullptr;
     double *d_param = nullptr;  // per-launch parameters of captured work (artss_param_set), kParams doubles
     cudaStream_t copy_stream = nullptr;
@@ -138,6 +140,30 @@ struct artss_ctx {
 
 namespace artss {
 cudaEvent_t prof_event(artss_ctx *ctx);
+
+// Programmatic dependent launch.  A kernel started by launch_pdl may begin while
+// its predecessor on the stream is still running: before pdl_wait() returns (the
+// predecessor complete, its writes visible) it reads only data that no kernel of
+// the step writes.  pdl_trigger() in a predecessor lets its dependent launch
+// once every block of the predecessor has passed it.  Both are no-ops for
+// ordinary launches; while a graph is captured launch_pdl launches ordinarily.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... K, typename... A>
+cudaError_t launch_pdl(artss_ctx *ctx, void (*kern)(K...), dim3 grid, dim3 block, size_t smem, A &&...args) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = block;
+    lc.dynamicSmemBytes = smem;
+    lc.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = (ctx->pdl && !ctx->capturing) ? 1 : 0;
+    return cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
+}
 // Brackets one kernel launch: counts it under its family and, when the
 // family is profiled, records an event pair around it on the context stream.
 struct ProfScope {
@@ -286,4 +312,15 @@ __device__ __forceinline__ double artss_block_sum(double v, double *smem) {
     do {                                            \
         artss::ProfScope ps_((ctx), (fam));         \
         __VA_ARGS__;                                \
+    } while (0)
+
+// ARTSS_LAUNCH of a kernel that begins with pdl_wait() (artss::launch_pdl)
+#define ARTSS_LAUNCH_PDL(ctx, fam, kern, grid, block, smem, ...)                                       \
+    do {                                                                                             \
+        cudaError_t e_pdl_;                                                                          \
+        {                                                                                            \
+            artss::ProfScope ps_((ctx), (fam));                                                      \
+            e_pdl_ = artss::launch_pdl((ctx), kern, dim3(grid), dim3(block), (size_t) (smem), __VA_ARGS__); \
+        }                                                                                            \
+        if (e_pdl_ != cudaSuccess) return artss::cuda_fail(e_pdl_, "kernel launch");                \
     } while (0)

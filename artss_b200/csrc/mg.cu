@@ -63,6 +63,8 @@ struct MgCoef {
 // JacobiDiffuse::JacobiStep, multigrid variant (JacobiDiffuse.cpp:274-305)
 __global__ void k_mg_jacobi(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
                             const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
@@ -95,6 +97,8 @@ __global__ void k_mg_cgs_color(double *__restrict__ out, const double *__restric
 // VCycleMG::Residuum (VCycleMG.cpp:346-354)
 __global__ void k_mg_residuum(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
                               const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
@@ -139,6 +143,8 @@ __global__ void k_mg_resnorm(const double *__restrict__ x, const double *__restr
 // VCycleMG::Restrict (VCycleMG.cpp:402-421), over coarse inner cells
 __global__ void k_mg_restrict(double *__restrict__ out, const double *__restrict__ in,
                               const uint8_t *__restrict__ flags, Level C, Level F, Box3 box) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int fx = (int) F.Nx, fxy = (int) F.nxy();
@@ -155,6 +161,8 @@ __global__ void k_mg_restrict(double *__restrict__ out, const double *__restrict
 // VCycleMG::Prolongate (VCycleMG.cpp:464-546): 8 fine cells per coarse inner cell
 __global__ void k_mg_prolongate(double *__restrict__ out, const double *__restrict__ in,
                                 const uint8_t *__restrict__ flags, Level C, Level F, Box3 box) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int ni = 1, nj = (int) C.Nx, nk = (int) C.nxy();
@@ -200,8 +208,8 @@ int mg_jacobi_step(artss_mg *mg, double *out, const double *in, const double *b,
     artss_ctx *ctx = mg->ctx;
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
-    ARTSS_LAUNCH(ctx, FAM_MG_JACOBI, k_mg_jacobi<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
-                                                               mg_coef(mg, level)));
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mg_jacobi, mg_grid(box), box_block(), 0, out, in, b, ctx->d_flags[level], L, box,
+                                                               mg_coef(mg, level));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1327,8 +1335,8 @@ int mg_restrict(artss_mg *mg, double *coarse, const double *fine, int coarse_lev
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    ARTSS_LAUNCH(ctx, FAM_MG_RESTRICT, k_mg_restrict<<<mg_grid(box), box_block(), 0, ctx->stream>>>(coarse, fine, ctx->d_flags[coarse_level], C,
-                                                                 ctx->lvl[coarse_level - 1], box));
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mg_restrict, mg_grid(box), box_block(), 0, coarse, fine, ctx->d_flags[coarse_level], C,
+                                                                 ctx->lvl[coarse_level - 1], box);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1337,8 +1345,8 @@ int mg_prolongate(artss_mg *mg, double *fine, const double *coarse, int coarse_l
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    ARTSS_LAUNCH(ctx, FAM_MG_PROLONGATE, k_mg_prolongate<<<mg_grid(box), box_block(), 0, ctx->stream>>>(fine, coarse, ctx->d_flags[coarse_level], C,
-                                                                   ctx->lvl[coarse_level - 1], box));
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mg_prolongate, mg_grid(box), box_block(), 0, fine, coarse, ctx->d_flags[coarse_level], C,
+                                                                   ctx->lvl[coarse_level - 1], box);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1348,10 +1356,10 @@ int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, in
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
-    ARTSS_LAUNCH(ctx, FAM_MG_RESIDUUM, k_mg_residuum<<<mg_grid(box), box_block(), 0, ctx->stream>>>(out, in, b, ctx->d_flags[level], L, box,
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mg_residuum, mg_grid(box), box_block(), 0, out, in, b, ctx->d_flags[level], L, box,
                                                                  1. / (g.dx[level] * g.dx[level]),
                                                                  1. / (g.dy[level] * g.dy[level]),
-                                                                 1. / (g.dz[level] * g.dz[level])));
+                                                                 1. / (g.dz[level] * g.dz[level]));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1574,8 +1582,8 @@ int artss_coarse_project(artss_ctx *ctx, double *d, int levels) {
         const Level &C = ctx->lvl[l];
         const Box3 box = inner_box(C);
         if ((st = artss_fill(ctx, arr[l], l, 0.0))) return st;
-        ARTSS_LAUNCH(ctx, FAM_MG_RESTRICT, k_mg_restrict<<<mg_grid(box), box_block(), 0, ctx->stream>>>(
-                                               arr[l], arr[l - 1], ctx->d_flags[l], C, ctx->lvl[l - 1], box));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mg_restrict, mg_grid(box), box_block(), 0, 
+                                               arr[l], arr[l - 1], ctx->d_flags[l], C, ctx->lvl[l - 1], box);
         ARTSS_LAUNCH_CK(ctx);
     }
     // prolongate back (VCycleMG::Prolongate), the coarse level's boundary values first
@@ -1584,8 +1592,8 @@ int artss_coarse_project(artss_ctx *ctx, double *d, int levels) {
         if ((st = artss_fill(ctx, arr[l - 1], l - 1, 0.0))) return st;
         const Level &C = ctx->lvl[l];
         const Box3 box = inner_box(C);
-        ARTSS_LAUNCH(ctx, FAM_MG_PROLONGATE, k_mg_prolongate<<<mg_grid(box), box_block(), 0, ctx->stream>>>(
-                                                 arr[l - 1], arr[l], ctx->d_flags[l], C, ctx->lvl[l - 1], box));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mg_prolongate, mg_grid(box), box_block(), 0, 
+                                                 arr[l - 1], arr[l], ctx->d_flags[l], C, ctx->lvl[l - 1], box);
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;

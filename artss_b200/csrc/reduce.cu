@@ -14,6 +14,8 @@ namespace artss {
 // 1: plain sum; 2: sum and its square root
 __global__ void k_finalize_loop(const double *__restrict__ partials, int nblocks, LoopState *__restrict__ st,
                                 double tol, long long max_it, int mode, const LoopState *__restrict__ ref) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     __shared__ double smem[32];
     if (mode == 3) {
         tol = tol * sqrt(ref->sum);
@@ -38,6 +40,8 @@ __global__ void k_finalize_loop(const double *__restrict__ partials, int nblocks
 }
 
 __global__ void k_init_loop(LoopState *st, double r0, long long it0, int cond0) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     st->sum = 0.0;
     st->residual = r0;
     st->it = it0;
@@ -59,33 +63,33 @@ __global__ void k_loop_continue(LoopState *st, cudaGraphConditionalHandle h, lon
 }
 
 int finalize_loop(artss_ctx *ctx, int slot, int nblocks, double tol, long long max_it) {
-    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, tol, max_it, 0, nullptr));
+    ARTSS_LAUNCH_PDL(ctx, FAM_REDUCE, k_finalize_loop, 1, kReduceThreads, 0, ctx->d_partials, nblocks, ctx->d_loop + slot, tol, max_it, 0, nullptr);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int finalize_loop_rel(artss_ctx *ctx, int slot, int nblocks, double rel_tol, int ref_slot, long long max_it) {
-    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(
+    ARTSS_LAUNCH_PDL(ctx, FAM_REDUCE, k_finalize_loop, 1, kReduceThreads, 0, 
                                       ctx->d_partials, nblocks, ctx->d_loop + slot, rel_tol, max_it, 3,
-                                      ctx->d_loop + ref_slot));
+                                      ctx->d_loop + ref_slot);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int finalize_sum(artss_ctx *ctx, int slot, int nblocks) {
-    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1, nullptr));
+    ARTSS_LAUNCH_PDL(ctx, FAM_REDUCE, k_finalize_loop, 1, kReduceThreads, 0, ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 1, nullptr);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int finalize_residual(artss_ctx *ctx, int slot, int nblocks) {
-    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_finalize_loop<<<1, kReduceThreads, 0, ctx->stream>>>(ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 2, nullptr));
+    ARTSS_LAUNCH_PDL(ctx, FAM_REDUCE, k_finalize_loop, 1, kReduceThreads, 0, ctx->d_partials, nblocks, ctx->d_loop + slot, 0.0, 0, 2, nullptr);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
 
 int init_loop(artss_ctx *ctx, int slot, double r0, long long it0, int cond0) {
-    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_init_loop<<<1, 1, 0, ctx->stream>>>(ctx->d_loop + slot, r0, it0, cond0));
+    ARTSS_LAUNCH_PDL(ctx, FAM_REDUCE, k_init_loop, 1, 1, 0, ctx->d_loop + slot, r0, it0, cond0);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }

@@ -456,6 +456,7 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     extern __shared__ __align__(1024) double st_sm[];
     __shared__ double smem[32];
     __shared__ __align__(8) uint64_t bars[kStSlotsX];
+    pdl_trigger();  // the boundary kernel after the sweep may launch (it waits for the sweep)
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
     if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
     double *X = st_sm;                          // [kStSlotsX][kStPlane]
@@ -643,6 +644,7 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
     extern __shared__ __align__(1024) double st_sm[];
     __shared__ double smem[32];
     __shared__ __align__(8) uint64_t bars[kSt2SlotsX];
+    pdl_trigger();  // the boundary kernel after the sweep may launch (it waits for the sweep)
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
     if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
     double *X = st_sm;                                // [kSt2SlotsX][kSt2PlaneX]
@@ -1118,6 +1120,12 @@ int artss_ctx_autotune(artss_ctx *ctx, int enable) {
     if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
     ctx->autotune = enable != 0;
     if (!enable) ctx->tuned.clear();
+    return ARTSS_OK;
+}
+
+int artss_ctx_pdl(artss_ctx *ctx, int enable) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    ctx->pdl = enable != 0;
     return ARTSS_OK;
 }
 

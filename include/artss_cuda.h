@@ -267,6 +267,11 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
  * enable = 0 switches tuning off (16 planes) and forgets earlier choices;
  * artss_cgs_sweep_depth returns the chosen depth, 0 before the first solve. */
 int artss_ctx_autotune(artss_ctx *ctx, int enable);
+/* Programmatic dependent launch (on by default): kernels whose start does not
+ * depend on their predecessor's results (the boundary programs) are launched
+ * so that they begin while the predecessor finishes.  enable = 0 launches
+ * every kernel after its predecessor has completed. */
+int artss_ctx_pdl(artss_ctx *ctx, int enable);
 int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent);
 /* the tuned sweep variant of level 0 (0-2: two-phase kernel of z-depth 8,
  * 16, 32; 3-5: one-phase kernel), -1 before the first solve */
