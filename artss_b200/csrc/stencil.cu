@@ -87,6 +87,8 @@ __global__ void k_advect(double *__restrict__ o0, double *__restrict__ o1, doubl
                          const double *__restrict__ n0, const double *__restrict__ n1, const double *__restrict__ n2,
                          const double *__restrict__ u, const double *__restrict__ v, const double *__restrict__ w,
                          const uint8_t *__restrict__ flags, Level L, Box3 box, AdvCoef c) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     const int Nx = (int) L.Nx, nxy = (int) L.nxy();
@@ -113,6 +115,8 @@ __global__ void k_advect(double *__restrict__ o0, double *__restrict__ o1, doubl
 __global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict__ u, const double *__restrict__ v,
                               const double *__restrict__ w, const uint8_t *__restrict__ flags, Level L, Box3 box,
                               double rdx, double rdy, double rdz, double cs2d2) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     const int ni = 1, nj = (int) L.Nx, nk = (int) L.nxy();
@@ -137,6 +141,8 @@ __global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict_
 __global__ void k_divergence(double *__restrict__ out, const double *__restrict__ u, const double *__restrict__ v,
                              const double *__restrict__ w, const uint8_t *__restrict__ flags, Level L, Box3 box,
                              double hx, double hy, double hz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
@@ -152,6 +158,8 @@ __global__ void k_divergence(double *__restrict__ out, const double *__restrict_
 
 // zero the ghost ring of the computational domain (IPressure.cpp:69-104)
 __global__ void k_ghost_ring_zero(double *__restrict__ out, Level L, Box3 ring) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(ring);
     if (!col) return;
     for (int k = (int) ring.z0 + (int) blockIdx.z; k <= (int) ring.z1; k += (int) gridDim.z) {
@@ -165,6 +173,8 @@ __global__ void k_projection(double *__restrict__ ou, double *__restrict__ ov, d
                              const double *__restrict__ us, const double *__restrict__ vs,
                              const double *__restrict__ ws, const double *__restrict__ p,
                              const uint8_t *__restrict__ flags, Level L, Box3 box, double hx, double hy, double hz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
@@ -182,6 +192,8 @@ __global__ void k_projection(double *__restrict__ ou, double *__restrict__ ov, d
 // ISource.cpp:41-46 on the domain list; nbeta = -beta (host)
 __global__ void k_buoyancy(double *__restrict__ f, const double *__restrict__ T, const double *__restrict__ Ta,
                            const uint8_t *__restrict__ flags, Level L, Box3 box, double nbeta, double g) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
@@ -194,6 +206,8 @@ __global__ void k_buoyancy(double *__restrict__ f, const double *__restrict__ T,
 // ExplicitEulerSource.cpp:92-96
 __global__ void k_add_source(double *__restrict__ out, const double *__restrict__ S,
                              const uint8_t *__restrict__ flags, Level L, Box3 box, double dt) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
     for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
@@ -456,7 +470,8 @@ k_cgs_sweep_tma(const __grid_constant__ CUtensorMap tm_x, const __grid_constant_
     extern __shared__ __align__(1024) double st_sm[];
     __shared__ double smem[32];
     __shared__ __align__(8) uint64_t bars[kStSlotsX];
-    pdl_trigger();  // the boundary kernel after the sweep may launch (it waits for the sweep)
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
     if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
     double *X = st_sm;                          // [kStSlotsX][kStPlane]
@@ -644,7 +659,8 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
     extern __shared__ __align__(1024) double st_sm[];
     __shared__ double smem[32];
     __shared__ __align__(8) uint64_t bars[kSt2SlotsX];
-    pdl_trigger();  // the boundary kernel after the sweep may launch (it waits for the sweep)
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
     if (blockDim.x != kStThreads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
     double *X = st_sm;                                // [kSt2SlotsX][kSt2PlaneX]
@@ -923,8 +939,8 @@ int artss_advect_sl(artss_ctx *ctx, double *out, const double *in, const double 
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
-    ARTSS_LAUNCH(ctx, FAM_ADVECT, k_advect<1><<<g, box_block(), 0, ctx->stream>>>(out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
-                                                    ctx->d_flags[0], L, box, c));
+    ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<1>), g, box_block(), 0, out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
+                                                    ctx->d_flags[0], L, box, c);
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, out, 0, out_field_type);
 }
@@ -939,8 +955,8 @@ int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *ou
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     const dim3 g = zgrid(box);
-    ARTSS_LAUNCH(ctx, FAM_ADVECT, k_advect<3><<<g, box_block(), 0, ctx->stream>>>(out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
-                                                    ctx->d_flags[0], L, box, c));
+    ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<3>), g, box_block(), 0, out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
+                                                    ctx->d_flags[0], L, box, c);
     ARTSS_LAUNCH_CK(ctx);
     if ((st = apply_bc(ctx, out_u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, out_v, 0, ARTSS_FIELD_V))) return st;
@@ -956,8 +972,8 @@ int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t, const double *u, 
     const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
     const double delta_s = cbrt(dx * dy * dz);
     const double cs2d2 = cs * cs * delta_s * delta_s;
-    ARTSS_LAUNCH(ctx, FAM_SMAGORINSKY, k_smagorinsky<<<zgrid(box), box_block(), 0, ctx->stream>>>(nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
-                                                               1. / dy, 1. / dz, cs2d2));
+    ARTSS_LAUNCH_PDL(ctx, FAM_SMAGORINSKY, k_smagorinsky, zgrid(box), box_block(), 0, nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
+                                                               1. / dy, 1. / dz, cs2d2);
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, nu_t, 0, ARTSS_FIELD_NU);
 }
@@ -970,10 +986,10 @@ int artss_divergence(artss_ctx *ctx, double *rhs, const double *u, const double 
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    ARTSS_LAUNCH(ctx, FAM_DIVERGENCE, k_divergence<<<zgrid(box), box_block(), 0, ctx->stream>>>(rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz));
+    ARTSS_LAUNCH_PDL(ctx, FAM_DIVERGENCE, k_divergence, zgrid(box), box_block(), 0, rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz);
     ARTSS_LAUNCH_CK(ctx);
     const Box3 ring = domain_box(L);
-    ARTSS_LAUNCH(ctx, FAM_DIVERGENCE, k_ghost_ring_zero<<<zgrid(ring), box_block(), 0, ctx->stream>>>(rhs, L, ring));
+    ARTSS_LAUNCH_PDL(ctx, FAM_DIVERGENCE, k_ghost_ring_zero, zgrid(ring), box_block(), 0, rhs, L, ring);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -987,8 +1003,8 @@ int artss_projection(artss_ctx *ctx, double *u, double *v, double *w, const doub
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    ARTSS_LAUNCH(ctx, FAM_PROJECTION, k_projection<<<zgrid(box), box_block(), 0, ctx->stream>>>(u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
-                                                              hy, hz));
+    ARTSS_LAUNCH_PDL(ctx, FAM_PROJECTION, k_projection, zgrid(box), box_block(), 0, u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
+                                                              hy, hz);
     ARTSS_LAUNCH_CK(ctx);
     if ((st = apply_bc(ctx, u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, v, 0, ARTSS_FIELD_V))) return st;
@@ -1000,7 +1016,7 @@ int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const d
     if (st) return st;
     const Level &L = ctx->lvl[0];
     const Box3 box = domain_box(L);
-    ARTSS_LAUNCH(ctx, FAM_BUOYANCY, k_buoyancy<<<zgrid(box), box_block(), 0, ctx->stream>>>(force, T, Ta, ctx->d_flags[0], L, box, -beta, g));
+    ARTSS_LAUNCH_PDL(ctx, FAM_BUOYANCY, k_buoyancy, zgrid(box), box_block(), 0, force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1010,7 +1026,7 @@ int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, in
     if (st || (st = check_field_type(field_type))) return st;
     const Level &L = ctx->lvl[0];
     const Box3 box = inner_box(L);
-    ARTSS_LAUNCH(ctx, FAM_ADD_SOURCE, k_add_source<<<zgrid(box), box_block(), 0, ctx->stream>>>(out, S, ctx->d_flags[0], L, box, dt));
+    ARTSS_LAUNCH_PDL(ctx, FAM_ADD_SOURCE, k_add_source, zgrid(box), box_block(), 0, out, S, ctx->d_flags[0], L, box, dt);
     ARTSS_LAUNCH_CK(ctx);
     return apply_bc(ctx, out, 0, field_type);
 }
@@ -1034,9 +1050,9 @@ int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, const Sw
     const dim3 g = sweep_tma_grid(box, zb);
     *nb = nblocks(g);
     const size_t smem1 = sweep_tma_smem(turb), smem2 = sweep_tma2_smem(turb);
-#define ARTSS_SWEEP_TMA(K, T, Z, SM, MX, MB, ME)                                                           \
-    ARTSS_LAUNCH(ctx, FAM_CGS, K<T, Z><<<g, kStThreads, SM, ctx->stream>>>(                                \
-                                   *MX, *MB, *ME, w, ctx->d_flags[0], L, box, c, ctx->d_partials, pred))
+#define ARTSS_SWEEP_TMA(K, T, Z, SM, MX, MB, ME)                                                      \
+    ARTSS_LAUNCH_PDL(ctx, FAM_CGS, (K<T, Z>), g, kStThreads, SM, *MX, *MB, *ME, w,                     \
+                     (const uint8_t *) ctx->d_flags[0], L, box, c, ctx->d_partials, pred)
     switch (v * 2 + (turb ? 1 : 0)) {
         case 0: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, false, 8, smem1, m.x, m.b, m.e); break;
         case 1: ARTSS_SWEEP_TMA(k_cgs_sweep_tma, true, 8, smem1, m.x, m.b, m.e); break;
