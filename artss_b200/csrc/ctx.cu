@@ -77,7 +77,8 @@ __global__ void k_scale_copy(double *__restrict__ d, const double *__restrict__ 
         d[i] = s[i] * x;
 }
 
-// a0 = a, a_tmp = a for up to three vectors in one pass (couple_vector).
+// a0 = a (unless a0 is null), a_tmp = a for up to three vectors in one pass
+// (couple_vector).
 __global__ void k_couple3(const double *__restrict__ a, double *__restrict__ a0, double *__restrict__ at,
                           const double *__restrict__ b, double *__restrict__ b0, double *__restrict__ bt,
                           const double *__restrict__ c, double *__restrict__ c0, double *__restrict__ ct,
@@ -85,9 +86,9 @@ __global__ void k_couple3(const double *__restrict__ a, double *__restrict__ a0,
     artss::pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     artss::pdl_trigger();
     for (int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
-        if (a) { const double x = a[i]; a0[i] = x; at[i] = x; }
-        if (b) { const double x = b[i]; b0[i] = x; bt[i] = x; }
-        if (c) { const double x = c[i]; c0[i] = x; ct[i] = x; }
+        if (a) { const double x = a[i]; if (a0) a0[i] = x; at[i] = x; }
+        if (b) { const double x = b[i]; if (b0) b0[i] = x; bt[i] = x; }
+        if (c) { const double x = c[i]; if (c0) c0[i] = x; ct[i] = x; }
     }
 }
 
@@ -590,7 +591,7 @@ int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, i
 int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
                  const double *b, double *b0, double *b_tmp,
                  const double *c, double *c0, double *c_tmp) {
-    if ((a && (!a0 || !a_tmp)) || (b && (!b0 || !b_tmp)) || (c && (!c0 || !c_tmp))) {
+    if ((a && !a_tmp) || (b && !b_tmp) || (c && !c_tmp)) {
         set_error("couple: incomplete triple"); return ARTSS_ERR_ARG;
     }
     const int level = 0;

@@ -1160,8 +1160,9 @@ int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
 }
 
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
-                      double dt, int field_type, const artss_iter_cfg *cfg, int in_is_scratch,
+                      double dt, int field_type, const artss_iter_cfg *cfg, int flags,
                       artss_iter_stats *stats) {
+    const int in_is_scratch = flags & ARTSS_DIFFUSE_IN_SCRATCH;
     int st = check_field_args(ctx, {out, in, b, cfg});
     if (st || (st = check_field_type(field_type))) return st;
     if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
@@ -1185,8 +1186,8 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
     const bool one_phase = tma && (box.x0 & 1) == 1;
     SweepMaps maps[2];  // by the array read: buf[0] = out, buf[1] = in
     const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
-    // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
-    if ((st = artss_copy(ctx, out, in, 0))) return st;
+    // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114), unless out holds in already
+    if (!(flags & ARTSS_DIFFUSE_OUT_HOLDS_IN) && (st = artss_copy(ctx, out, in, 0))) return st;
     const int slot = 0;
     // while (res > tol_res && it < max_iter), res starts at 1
     long long it = 0;

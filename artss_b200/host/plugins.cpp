@@ -47,7 +47,9 @@ void ColoredGaussSeidelDiffuse::run(Field &out, const Field &in, const Field &b,
     artss_iter_stats st{};
     // the reference overwrites its const `in` argument (ColoredGaussSeidelDiffuse.cpp:71)
     check(artss_diffuse_cgs(m_rt.ctx(), out.data, in.data, b.data, D, ev ? ev->data : nullptr, m_rt.dt(),
-                            out.get_type(), &cfg, in_is_scratch ? 1 : 0, &st),
+                            out.get_type(), &cfg,
+                            (in_is_scratch ? ARTSS_DIFFUSE_IN_SCRATCH : 0) | (out_holds_in ? ARTSS_DIFFUSE_OUT_HOLDS_IN : 0),
+                            &st),
           "ColoredGaussSeidelDiffuse::diffuse");
     last_iterations = st.iterations;
     last_residual = st.residual;

@@ -32,6 +32,7 @@ class IDiffusion {
     // Declares that `in` is dead after diffuse() (the caller overwrites it
     // before reading), letting the solver skip the per-sweep snapshot copy.
     bool in_is_scratch = false;
+    bool out_holds_in = false;  // the caller coupled out and in from one field before diffuse()
 };
 
 // IPressure (src/interfaces/IPressure.h:13-25)

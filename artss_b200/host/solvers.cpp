@@ -84,6 +84,13 @@ void FieldController::couple_vector(const Field &a, Field &a0, Field &a_tmp, con
           "couple_vector");
 }
 
+void FieldController::couple_tmp(const Field &a, Field &a_tmp, const Field &b, Field &b_tmp, const Field &c,
+                                 Field &c_tmp) {
+    check(artss_couple(a.runtime().ctx(), a.data, nullptr, a_tmp.data, b.data, nullptr, b_tmp.data, c.data, nullptr,
+                       c_tmp.data),
+          "couple_tmp");
+}
+
 void FieldController::couple_scalar(const Field &a, Field &a0, Field &a_tmp) {
     check(artss_couple(a.runtime().ctx(), a.data, a0.data, a_tmp.data, nullptr, nullptr, nullptr, nullptr, nullptr,
                        nullptr),
@@ -143,9 +150,12 @@ NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbul
         throw config_error("Fields not specified correctly!");
     if (s.temperature.source.dissipation)
         throw config_error("temperature dissipation is not part of the fractional-step path implemented here");
-    // `in` of every diffuse() call below is re-coupled before it is read again
+    // `in` of every diffuse() call below is re-coupled before it is read again,
+    // and out and in are coupled from one field just before each call
     dif_vel->in_is_scratch = true;
     dif_temp->in_is_scratch = true;
+    dif_vel->out_holds_in = true;
+    dif_temp->out_holds_in = true;
 }
 
 void NSTempTurbSolver::do_step(real t, bool sync) {
@@ -174,7 +184,7 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
         stats.diffusion_iterations[1] = dif_vel->last_iterations;
         dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, f.nu_t, sync);
         stats.diffusion_iterations[2] = dif_vel->last_iterations;
-        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+        couple_after_diffusion();
     } else if (nu != 0.) {
         dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
         stats.diffusion_iterations[0] = dif_vel->last_iterations;
@@ -182,13 +192,14 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
         stats.diffusion_iterations[1] = dif_vel->last_iterations;
         dif_vel->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
         stats.diffusion_iterations[2] = dif_vel->last_iterations;
-        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+        couple_after_diffusion();
     }
 
-    // 3. momentum source (:155-163)
+    // 3. momentum source (:155-163); its couple_vector (:162) writes u0, v0, w0 that
+    //    update_data rewrites before they are read: the u_tmp half only
     if (m_add_source) {
         sou_vel->add_source(f.u, f.v, f.w, f.f_x, f.f_y, f.f_z, sync);
-        FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
+        FieldController::couple_tmp(f.u, f.u_tmp, f.v, f.v_tmp, f.w, f.w_tmp);
     }
 
     // 4. pressure and projection (:167-176)
@@ -209,21 +220,29 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     adv_temp->advect(f.T, f.T0, f.u, f.v, f.w, sync);
     FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
     const auto &ts = m_rt.settings().solver.temperature;
+    // The couple_scalar calls that follow the temperature's diffusion and source
+    // (:206, :216, :239) are left out: the source reads T and S_T only, and
+    // nothing reads T0 or T_tmp before update_data couples T again at the end
+    // of the step (TimeIntegration::run), so the fields after the step are the same.
     if (m_turb && ts.has_turbulence) {
         const real rPr_T = 1. / ts.prandtl_number.value();
         check(artss_scale_copy(m_rt.ctx(), f.kappa_t.data, f.nu_t.data, rPr_T, 0), "kappa_t");
         dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, f.kappa_t, sync);
         stats.diffusion_iterations[3] = dif_temp->last_iterations;
-        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
     } else if (kappa != 0.) {
         dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, sync);
         stats.diffusion_iterations[3] = dif_temp->last_iterations;
-        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
     }
-    if (m_add_temp_source) {
-        sou_temp->add_source(f.T, f.S_T, sync);
-        FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
-    }
+    if (m_add_temp_source) sou_temp->add_source(f.T, f.S_T, sync);
+}
+
+// couple_vector after the velocity diffusion (:152): with a momentum source
+// next, which reads u, v, w and the forces only and is followed by its own
+// couple, it is left out; otherwise the divergence reads u_tmp, v_tmp, w_tmp
+// and u0, v0, w0 are rewritten by update_data before they are read.
+void NSTempTurbSolver::couple_after_diffusion() {
+    FieldController &f = m_fc;
+    if (!m_add_source) FieldController::couple_tmp(f.u, f.u_tmp, f.v, f.v_tmp, f.w, f.w_tmp);
 }
 
 void NSTempTurbSolver::update_source(real t_cur) { m_source_function_temperature->update_source(m_fc.S_T, t_cur); }

@@ -30,6 +30,9 @@ class FieldController {
     static void couple_vector(const Field &a, Field &a0, Field &a_tmp, const Field &b, Field &b0, Field &b_tmp,
                               const Field &c, Field &c0, Field &c_tmp);
     static void couple_scalar(const Field &a, Field &a0, Field &a_tmp);
+    // a_tmp = a, b_tmp = b, c_tmp = c: the half of couple_vector that is read
+    // when a0, b0, c0 are rewritten (update_data) before anything reads them
+    static void couple_tmp(const Field &a, Field &a_tmp, const Field &b, Field &b_tmp, const Field &c, Field &c_tmp);
     Field *by_name(const std::string &name);
 
  private:
@@ -61,6 +64,7 @@ class NSTempTurbSolver : public ISolver {
     StepStats stats;
 
  private:
+    void couple_after_diffusion();
     Runtime &m_rt;
     FieldController &m_fc;
     bool m_turb = true;

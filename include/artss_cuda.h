@@ -229,7 +229,9 @@ int artss_add_scalar(artss_ctx *ctx, double *dst, double x, int level);         
 int artss_scale(artss_ctx *ctx, double *dst, double x, int level);              /* dst *= x */
 int artss_scale_copy(artss_ctx *ctx, double *dst, const double *src, double x, int level); /* dst = src * x */
 /* FieldController::couple_vector / couple_scalar (src/field/FieldController.cpp:151-186):
- * a0 = a and a_tmp = a for each non-null triple, one pass over memory. */
+ * a0 = a and a_tmp = a for each non-null triple, one pass over memory.  a0 may
+ * be NULL (a_tmp = a only), for a caller that knows a0 is rewritten before it
+ * is read. */
 int artss_couple(artss_ctx *ctx, const double *a, double *a0, double *a_tmp,
                  const double *b, double *b0, double *b_tmp,
                  const double *c, double *c0, double *c_tmp);
@@ -256,11 +258,16 @@ int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t,
 
 /* IDiffusion::diffuse, ColoredGaussSeidelDiffuse (src/diffusion/ColoredGaussSeidelDiffuse.cpp:38-173).
  * ev == NULL selects the laminar variant.  `in` is overwritten as in the
- * reference (it holds the state before the last sweep) unless
- * in_is_scratch != 0, in which case its final contents are unspecified. */
+ * reference (it holds the state before the last sweep) unless flags has
+ * ARTSS_DIFFUSE_IN_SCRATCH, in which case its final contents are unspecified.
+ * ARTSS_DIFFUSE_OUT_HOLDS_IN: the caller guarantees out already equals in
+ * (both coupled from one field), and the reference's out.copy_data(in) is
+ * skipped. */
+#define ARTSS_DIFFUSE_IN_SCRATCH 1
+#define ARTSS_DIFFUSE_OUT_HOLDS_IN 2
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
                       double D, const double *ev, double dt, int field_type,
-                      const artss_iter_cfg *cfg, int in_is_scratch, artss_iter_stats *stats);
+                      const artss_iter_cfg *cfg, int flags, artss_iter_stats *stats);
 /* Autotuner (no counterpart in the reference): the first colored Gauss-Seidel
  * solve on a level shape times the sweep's z-depths (8, 16, 32 planes per
  * block) on its first iteration and keeps the fastest for the context.
