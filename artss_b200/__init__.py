@@ -123,6 +123,9 @@ def load_cuda() -> C.CDLL:
             "artss_download": ([_P, _D, _D, C.c_int64], C.c_int),
             "artss_upload_async": ([_P, _D, _D, C.c_int64], C.c_int),
             "artss_download_async": ([_P, _D, _D, C.c_int64], C.c_int),
+            "artss_io_in": ([_P, C.c_int, C.POINTER(_D), C.POINTER(_D), C.c_int64], C.c_int),
+            "artss_io_out": ([_P, C.c_int, C.POINTER(_D), C.POINTER(_D), C.c_int64], C.c_int),
+            "artss_io_sync": ([_P], C.c_int),
             "artss_set_cell_lists": ([_P, C.c_int, _I64P, C.c_int64, _I64P, C.c_int64], C.c_int),
             "artss_get_cell_flags": ([_P, C.c_int, C.POINTER(C.c_uint8), C.c_int64], C.c_int),
             "artss_set_boundary_program": ([_P, C.c_int, C.c_int, C.POINTER(BcAssign), C.c_int64], C.c_int),
@@ -215,6 +218,9 @@ def load_host() -> C.CDLL:
             "artss_sim_graph_steps": ([_P], C.c_int64),
             "artss_sim_step_io": ([_P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_D), C.c_int,
                                    C.POINTER(C.c_char_p), C.POINTER(_D)], C.c_int),
+            "artss_sim_step_io_async": ([_P, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_D), C.c_int,
+                                         C.POINTER(C.c_char_p), C.POINTER(_D)], C.c_int),
+            "artss_sim_io_sync": ([_P], C.c_int),
             "artss_sim_finished": ([_P], C.c_int),
             "artss_sim_time": ([_P], C.c_double),
             "artss_sim_step_index": ([_P], C.c_int64),
@@ -358,6 +364,24 @@ class Simulation:
         p_out = (_D * len(outputs))(*[C.cast(C.c_void_p(v), _D) for v in outputs.values()])
         _host_check(self._lib.artss_sim_step_io(self._h, len(names_in), a_in, p_in, len(names_out), a_out, p_out),
                     "step_io")
+
+    def step_io_async(self, inputs: Dict[str, int], outputs: Dict[str, int]) -> None:
+        """step_io pipelined: returns once the uploads, the step and the
+        read-back are enqueued; inputs go up while the previous call's outputs
+        come down.  The host arrays of a call may be reused once the call two
+        after it has returned, or after io_sync()."""
+        names_in = [k.encode() for k in inputs]
+        names_out = [k.encode() for k in outputs]
+        a_in = (C.c_char_p * len(names_in))(*names_in)
+        a_out = (C.c_char_p * len(names_out))(*names_out)
+        p_in = (_D * len(inputs))(*[C.cast(C.c_void_p(v), _D) for v in inputs.values()])
+        p_out = (_D * len(outputs))(*[C.cast(C.c_void_p(v), _D) for v in outputs.values()])
+        _host_check(self._lib.artss_sim_step_io_async(self._h, len(names_in), a_in, p_in, len(names_out), a_out,
+                                                      p_out), "step_io_async")
+
+    def io_sync(self) -> None:
+        """Waits for every transfer and step enqueued by step_io_async."""
+        _host_check(self._lib.artss_sim_io_sync(self._h), "io_sync")
 
     @property
     def finished(self) -> bool:

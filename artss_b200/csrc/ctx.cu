@@ -249,6 +249,21 @@ int artss_ctx_destroy(artss_ctx *ctx) {
         cudaEventDestroy(ctx->copy_tail);
         cudaStreamDestroy(ctx->copy_stream);
     }
+    if (ctx->io_up) {
+        cudaStreamSynchronize(ctx->io_up);
+        cudaStreamSynchronize(ctx->io_down);
+        for (double *a : ctx->io_stage_in) cudaFree(a);
+        for (auto &v : ctx->io_stage_out)
+            for (double *a : v) cudaFree(a);
+        cudaEventDestroy(ctx->io_in_ready);
+        cudaEventDestroy(ctx->io_in_free);
+        for (int b = 0; b < 2; b++) {
+            cudaEventDestroy(ctx->io_out_ready[b]);
+            cudaEventDestroy(ctx->io_out_free[b]);
+        }
+        cudaStreamDestroy(ctx->io_up);
+        cudaStreamDestroy(ctx->io_down);
+    }
     cudaFree(ctx->d_partials);
     cudaFree(ctx->d_loop);
     cudaFree(ctx->d_param);
@@ -485,6 +500,117 @@ int artss_copy_join(artss_ctx *ctx) {
     if (!ctx->copy_stream) return ARTSS_OK;
     ARTSS_CK(cudaEventRecord(ctx->copy_tail, ctx->copy_stream));
     ARTSS_CK(cudaStreamWaitEvent(ctx->stream, ctx->copy_tail, 0));
+    return ARTSS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// the pipeline's streams and events on first use; staging arrays of n doubles
+int io_ready(artss_ctx *ctx, int64_t n, int n_in, int n_out) {
+    if (!ctx->io_up) {
+        ARTSS_CK(cudaStreamCreateWithFlags(&ctx->io_up, cudaStreamNonBlocking));
+        ARTSS_CK(cudaStreamCreateWithFlags(&ctx->io_down, cudaStreamNonBlocking));
+        ARTSS_CK(cudaEventCreateWithFlags(&ctx->io_in_ready, cudaEventDisableTiming));
+        ARTSS_CK(cudaEventCreateWithFlags(&ctx->io_in_free, cudaEventDisableTiming));
+        for (int b = 0; b < 2; b++) {
+            ARTSS_CK(cudaEventCreateWithFlags(&ctx->io_out_ready[b], cudaEventDisableTiming));
+            ARTSS_CK(cudaEventCreateWithFlags(&ctx->io_out_free[b], cudaEventDisableTiming));
+        }
+    }
+    if (n != ctx->io_n) {
+        // a new field size: every transfer in flight ends before the staging changes
+        ARTSS_CK(cudaStreamSynchronize(ctx->io_up));
+        ARTSS_CK(cudaStreamSynchronize(ctx->io_down));
+        ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+        for (double *a : ctx->io_stage_in) cudaFree(a);
+        ctx->io_stage_in.clear();
+        for (auto &v : ctx->io_stage_out) {
+            for (double *a : v) cudaFree(a);
+            v.clear();
+        }
+        ctx->io_n = n;
+    }
+    while ((int) ctx->io_stage_in.size() < n_in) {
+        double *a = nullptr;
+        ARTSS_CK(cudaMalloc(&a, (size_t) n * sizeof(double)));
+        ctx->io_stage_in.push_back(a);
+    }
+    for (auto &v : ctx->io_stage_out)
+        while ((int) v.size() < n_out) {
+            double *a = nullptr;
+            ARTSS_CK(cudaMalloc(&a, (size_t) n * sizeof(double)));
+            v.push_back(a);
+        }
+    return ARTSS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int artss_io_in(artss_ctx *ctx, int n_in, double *const *fields, const double *const *host, int64_t n) {
+    if (!ctx || n_in < 0 || n < 0 || (n_in && (!fields || !host))) {
+        set_error("bad io_in arguments");
+        return ARTSS_ERR_ARG;
+    }
+    for (int k = 0; k < n_in; k++)
+        if (!fields[k] || !host[k]) { set_error("null io_in array"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("io_in while a graph is captured"); return ARTSS_ERR_ARG; }
+    if (n_in == 0) return ARTSS_OK;
+    int st = io_ready(ctx, n, n_in, 0);
+    if (st) return st;
+    // the staging is overwritten once the previous call's inputs have left it
+    ARTSS_CK(cudaStreamWaitEvent(ctx->io_up, ctx->io_in_free, 0));
+    for (int k = 0; k < n_in; k++)
+        ARTSS_CK(cudaMemcpyAsync(ctx->io_stage_in[k], host[k], (size_t) n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->io_up));
+    ARTSS_CK(cudaEventRecord(ctx->io_in_ready, ctx->io_up));
+    ARTSS_CK(cudaStreamWaitEvent(ctx->stream, ctx->io_in_ready, 0));
+    for (int k = 0; k < n_in; k++) {
+        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_copy, flat_blocks(n), 256, 0, fields[k],
+                         (const double *) ctx->io_stage_in[k], n);
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    ARTSS_CK(cudaEventRecord(ctx->io_in_free, ctx->stream));
+    return ARTSS_OK;
+}
+
+int artss_io_out(artss_ctx *ctx, int n_out, const double *const *fields, double *const *host, int64_t n) {
+    if (!ctx || n_out < 0 || n < 0 || (n_out && (!fields || !host))) {
+        set_error("bad io_out arguments");
+        return ARTSS_ERR_ARG;
+    }
+    for (int k = 0; k < n_out; k++)
+        if (!fields[k] || !host[k]) { set_error("null io_out array"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("io_out while a graph is captured"); return ARTSS_ERR_ARG; }
+    int st = io_ready(ctx, n, 0, n_out);
+    if (st) return st;
+    const int b = (int) (ctx->io_calls & 1);
+    ctx->io_calls++;
+    // call k returns once call k-2 (the last user of this parity's staging) is
+    // complete: its host arrays are then free
+    ARTSS_CK(cudaEventSynchronize(ctx->io_out_free[b]));
+    if (n_out == 0) return ARTSS_OK;
+    for (int k = 0; k < n_out; k++) {
+        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_copy, flat_blocks(n), 256, 0, ctx->io_stage_out[b][k], fields[k], n);
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    ARTSS_CK(cudaEventRecord(ctx->io_out_ready[b], ctx->stream));
+    ARTSS_CK(cudaStreamWaitEvent(ctx->io_down, ctx->io_out_ready[b], 0));
+    for (int k = 0; k < n_out; k++)
+        ARTSS_CK(cudaMemcpyAsync(host[k], ctx->io_stage_out[b][k], (size_t) n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->io_down));
+    ARTSS_CK(cudaEventRecord(ctx->io_out_free[b], ctx->io_down));
+    return ARTSS_OK;
+}
+
+int artss_io_sync(artss_ctx *ctx) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (ctx->io_up) {
+        ARTSS_CK(cudaStreamSynchronize(ctx->io_up));
+        ARTSS_CK(cudaStreamSynchronize(ctx->io_down));
+    }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
     return ARTSS_OK;
 }
 

@@ -128,12 +128,18 @@ struct artss_ctx {
     // whole-step capture (artss_graph_begin .. artss_graph_end): loops become
     // conditional WHILE nodes whose bodies are captured on body_stream
     bool capturing = false;
-    bool pdl = true;  // launch_pdl may overlap a launch with its predecessor's tail (eager runs)
+    int pdl = 2;  // launch_pdl overlaps a launch with its predecessor's tail: 1 eager runs, 2 also captured graphs
     cudaStream_t body_stream = nullptr;
     double *d_param = nullptr;  // per-launch parameters of captured work (artss_param_set), kParams doubles
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev[artss::kCopySlots]{};
     cudaEvent_t copy_mark = nullptr, copy_tail = nullptr;
+    // pipelined whole-field transfers (artss_io_in / artss_io_out): uploads on
+    // io_up, read-backs on io_down (one copy engine each), device staging
+    cudaStream_t io_up = nullptr, io_down = nullptr;
+    std::vector<double *> io_stage_in, io_stage_out[2];
+    int64_t io_n = 0, io_calls = 0;
+    cudaEvent_t io_in_ready = nullptr, io_in_free = nullptr, io_out_ready[2]{}, io_out_free[2]{};
     int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},
                                {1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1}};
 };
@@ -146,7 +152,8 @@ cudaEvent_t prof_event(artss_ctx *ctx);
 // predecessor complete, its writes visible) it reads only data that no kernel of
 // the step writes.  pdl_trigger() in a predecessor lets its dependent launch
 // once every block of the predecessor has passed it.  Both are no-ops for
-// ordinary launches; while a graph is captured launch_pdl launches ordinarily.
+// ordinary launches.  Whether launch_pdl also sets the attribute while a graph
+// is captured (a programmatic edge in the graph) is the context's pdl mode.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
@@ -161,7 +168,7 @@ cudaError_t launch_pdl(artss_ctx *ctx, void (*kern)(K...), dim3 grid, dim3 block
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     at[0].val.programmaticStreamSerializationAllowed = 1;
     lc.attrs = at;
-    lc.numAttrs = (ctx->pdl && !ctx->capturing) ? 1 : 0;
+    lc.numAttrs = (ctx->pdl == 2 || (ctx->pdl == 1 && !ctx->capturing)) ? 1 : 0;
     return cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
 }
 // Brackets one kernel launch: counts it under its family and, when the

@@ -1141,7 +1141,8 @@ int artss_ctx_autotune(artss_ctx *ctx, int enable) {
 
 int artss_ctx_pdl(artss_ctx *ctx, int enable) {
     if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
-    ctx->pdl = enable != 0;
+    if (enable < 0 || enable > 2) { set_error("pdl mode is 0, 1 or 2"); return ARTSS_ERR_ARG; }
+    ctx->pdl = enable;
     return ARTSS_OK;
 }
 

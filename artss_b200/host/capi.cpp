@@ -182,6 +182,39 @@ int artss_sim_step_io(artss_sim *s, int n_in, const char *const *in_names, const
     });
 }
 
+int artss_sim_step_io_async(artss_sim *s, int n_in, const char *const *in_names, const double *const *in_host,
+                            int n_out, const char *const *out_names, double *const *out_host) {
+    return guarded([&] {
+        if (!s || n_in < 0 || n_out < 0 || (n_in && (!in_names || !in_host)) || (n_out && (!out_names || !out_host)))
+            throw std::invalid_argument("bad step arguments");
+        auto field = [&](const char *name) {
+            Field *f = name ? s->sc->fields().by_name(name) : nullptr;
+            if (!f) throw std::invalid_argument(std::string("unknown field ") + (name ? name : "(null)"));
+            return f;
+        };
+        std::vector<std::pair<Field *, const real *>> in;
+        std::vector<std::pair<Field *, real *>> out;
+        for (int k = 0; k < n_in; k++) {
+            if (!in_host[k]) throw std::invalid_argument("null input buffer");
+            in.emplace_back(field(in_names[k]), in_host[k]);
+        }
+        for (int k = 0; k < n_out; k++) {
+            if (!out_host[k]) throw std::invalid_argument("null output buffer");
+            out.emplace_back(field(out_names[k]), out_host[k]);
+        }
+        s->ti->step_io_async(in, out);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_io_sync(artss_sim *s) {
+    return guarded([&] {
+        if (!s) throw std::invalid_argument("null argument");
+        check(artss_io_sync(s->rt->ctx()), "io_sync");
+        return ARTSS_OK;
+    });
+}
+
 int artss_sim_set_graphs(artss_sim *s, int enable) {
     if (!s) return ARTSS_ERR_ARG;
     s->rt->graphs = enable != 0;

@@ -608,6 +608,39 @@ void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>
     io.finish();
 }
 
+void TimeIntegration::step_io_async(const std::vector<std::pair<Field *, const real *>> &in,
+                                    const std::vector<std::pair<Field *, real *>> &out) {
+    if (finished()) throw std::invalid_argument("the simulation has reached t_end");
+    artss_ctx *ctx = m_rt.ctx();
+    FieldController &fc = m_sc.fields();
+    const int64_t n = (int64_t) fc.u.get_size();
+    std::vector<double *> in_dev;
+    std::vector<const double *> in_host;
+    bool vel = false, temp = false;
+    for (const auto &i : in) {
+        if ((int64_t) i.first->get_size() != n) throw std::invalid_argument("step_io_async: level-0 fields only");
+        in_dev.push_back(i.first->data);
+        in_host.push_back(i.second);
+        vel = vel || i.first == &fc.u || i.first == &fc.v || i.first == &fc.w;
+        temp = temp || i.first == &fc.T;
+    }
+    check(artss_io_in(ctx, (int) in.size(), in_dev.data(), in_host.data(), n), "io_in");
+    // uploaded u, v, w, T are the state the step advances (as in step_io); p
+    // and T set at the start instead of during the velocity: nothing of the
+    // step reads them before (the buoyancy force was formed from the previous T)
+    if (vel) FieldController::couple_vector(fc.u, fc.u0, fc.u_tmp, fc.v, fc.v0, fc.v_tmp, fc.w, fc.w0, fc.w_tmp);
+    if (temp) FieldController::couple_scalar(fc.T, fc.T0, fc.T_tmp);
+    run(1);
+    std::vector<const double *> out_dev;
+    std::vector<double *> out_host;
+    for (const auto &o : out) {
+        if ((int64_t) o.first->get_size() != n) throw std::invalid_argument("step_io_async: level-0 fields only");
+        out_dev.push_back(o.first->data);
+        out_host.push_back(o.second);
+    }
+    check(artss_io_out(ctx, (int) out.size(), out_dev.data(), out_host.data(), n), "io_out");
+}
+
 TimeIntegration::~TimeIntegration() { artss_graph_destroy(m_graph); }
 
 void TimeIntegration::capture_step() {

@@ -166,6 +166,10 @@ class TimeIntegration {
     // complete when the context's stream reaches them
     void step_io(const std::vector<std::pair<Field *, const real *>> &in,
                  const std::vector<std::pair<Field *, real *>> &out);
+    // the step with pipelined transfers (artss_io_in / artss_io_out): returns
+    // once they and the step are enqueued
+    void step_io_async(const std::vector<std::pair<Field *, const real *>> &in,
+                       const std::vector<std::pair<Field *, real *>> &out);
     real time() const { return m_t_cur; }
     int64_t step_index() const { return m_step; }
     bool finished() const;

@@ -176,6 +176,22 @@ int artss_copy_wait(artss_ctx *ctx, int slot);
 int artss_copy_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
 int artss_copy_join(artss_ctx *ctx);
 
+/* Pipelined whole-field transfers (no reference counterpart).  Uploads run on
+ * one copy engine and read-backs on the other, so that the inputs of one call
+ * go up while the outputs of the previous one come down, both beside the
+ * context's work.
+ * artss_io_in: the n_in host arrays (n doubles each, page-locked for overlap)
+ * are copied into device staging once the previous call's inputs have left
+ * it, and from there into `fields`, ordered before the context's later work.
+ * artss_io_out: the values of `fields` as of the work enqueued so far are
+ * copied into staging (two sets, used alternately) and from there to the
+ * host beside later work.  The k-th artss_io_out returns once the (k-2)-th
+ * has completed: host arrays given to call pair k-2 may then be reused.
+ * artss_io_sync waits for every transfer and for the context's work. */
+int artss_io_in(artss_ctx *ctx, int n_in, double *const *fields, const double *const *host, int64_t n);
+int artss_io_out(artss_ctx *ctx, int n_out, const double *const *fields, double *const *host, int64_t n);
+int artss_io_sync(artss_ctx *ctx);
+
 /* Whole-step graphs.  Between artss_graph_begin and artss_graph_end every
  * call on the context is captured instead of run: its bounded solver loops
  * (diffusion, mixed-precision pressure) become conditional WHILE nodes that
@@ -274,10 +290,11 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b,
  * enable = 0 switches tuning off (16 planes) and forgets earlier choices;
  * artss_cgs_sweep_depth returns the chosen depth, 0 before the first solve. */
 int artss_ctx_autotune(artss_ctx *ctx, int enable);
-/* Programmatic dependent launch (on by default): kernels whose start does not
- * depend on their predecessor's results (the boundary programs) are launched
- * so that they begin while the predecessor finishes.  enable = 0 launches
- * every kernel after its predecessor has completed. */
+/* Programmatic dependent launch: kernels launched so that they begin while
+ * their predecessor finishes (each waits on the device for the predecessor's
+ * results before it reads them).  enable = 2 (default): eager launches and
+ * the launches captured into whole-step graphs; 1: eager launches only; 0:
+ * every kernel starts after its predecessor has completed. */
 int artss_ctx_pdl(artss_ctx *ctx, int enable);
 int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent);
 /* the tuned sweep variant of level 0 (0-2: two-phase kernel of z-depth 8,

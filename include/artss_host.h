@@ -58,6 +58,15 @@ int artss_sim_run(artss_sim *s, int64_t steps, int64_t *done);
  * returns. */
 int artss_sim_step_io(artss_sim *s, int n_in, const char *const *in_names, const double *const *in_host, int n_out,
                       const char *const *out_names, double *const *out_host);
+/* The same step, pipelined: the call returns once the inputs, the step and
+ * the read-back are enqueued.  Inputs go up on one copy engine while the
+ * previous call's outputs come down on the other, beside the steps.  The
+ * host arrays of a call may be reused once the call two after it has
+ * returned, or after artss_sim_io_sync, which waits for everything.  The
+ * fields read back are the step's final values, as from artss_sim_step_io. */
+int artss_sim_step_io_async(artss_sim *s, int n_in, const char *const *in_names, const double *const *in_host,
+                            int n_out, const char *const *out_names, double *const *out_host);
+int artss_sim_io_sync(artss_sim *s);
 /* Whole-step graphs on or off (off by default): from the third step on, a
  * step is captured once (its solver loops as conditional WHILE nodes on the
  * device loop state) and replayed per step; a scene whose step cannot be
