@@ -262,7 +262,12 @@ int mg_smooth(artss_mg *mg, double *out, double *tmp, const double *b, int level
     }
     if ((st = artss_copy(mg->ctx, tmp, out, level))) return st;
     double *A = out, *B = tmp;   // Field data pointers as swapped by Field::swap
-    for (int r = 0; r < mg->cfg.n_relax; r++) {
+    // VCycleMG::call_smooth_jacobi (VCycleMG.cpp:710-721) leaves `out` with
+    // iterate n_relax - 1 when n_relax is even: the last relaxation writes only
+    // tmp, which the next smoothing or coarse solve overwrites before reading
+    // it.  That relaxation and its boundary program are left out.
+    const int n_relax = mg->cfg.n_relax - (mg->cfg.n_relax > 0 && mg->cfg.n_relax % 2 == 0 ? 1 : 0);
+    for (int r = 0; r < n_relax; r++) {
         if ((st = mg_jacobi_step(mg, A, B, b, level))) return st;
         if ((st = mg_bc(mg, A, level))) return st;
         std::swap(A, B);
