@@ -20,6 +20,7 @@
 #include "internal.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <unordered_map>
 
 namespace artss {
@@ -244,6 +245,12 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
     p.n = n;
     p.h_target = tgt;
     p.h_root = root;
+    p.zero_values = true;
+    for (double v : val) {
+        uint64_t bits;
+        std::memcpy(&bits, &v, sizeof bits);
+        if (bits != 0) p.zero_values = false;
+    }
     if (n == 0) return ARTSS_OK;
     ARTSS_CK(cudaMalloc(&p.d_target, n * sizeof(int64_t)));
     ARTSS_CK(cudaMalloc(&p.d_root, n * sizeof(int64_t)));

@@ -51,6 +51,7 @@ struct BcProgram {
     double *d_value = nullptr;         // [kBcMaxDepth][n]
     std::vector<int64_t> h_target;     // targets, host copy
     std::vector<int64_t> h_root;       // roots, host copy
+    bool zero_values = false;          // every value of the program is +0.0: x_t = +-x_r + 0
     // plan of the pipelined coarse solve: state -2 unknown, -1 not eligible, 1 planned
     int pipe_state = -2;
     std::vector<int> pipe_kb;          // plane split, ranks + 1 entries

@@ -34,6 +34,9 @@ struct artss_mg {
     };
     std::vector<Graph> graphs;
     bool use_graphs = true;
+    // the restriction of level l+1's inner cells reads no target of level l's
+    // boundary program: the program on residuum0[l] has no reader
+    bool r0_bc_dead[artss::kMaxLevel + 1]{};
 };
 
 namespace artss {
@@ -247,12 +250,17 @@ int mg_resnorm(artss_mg *mg, const double *x, const double *b, int level, int sl
 }
 
 // VCycleMG::Smooth + call_smooth_{jacobi,colored_gauss_seidel} (VCycleMG.cpp:299-305, :583-723)
-int mg_smooth(artss_mg *mg, double *out, double *tmp, const double *b, int level) {
+int mg_smooth(artss_mg *mg, double *out, double *tmp, const double *b, int level, bool out_satisfies_bc = false) {
     int st;
     // VCycleMG::Smooth and call_smooth_* each apply the boundary program first;
     // the program is idempotent (ghost values are functions of inner values it
-    // does not write), so one application gives the same array
-    if ((st = mg_bc(mg, out, level))) return st;
+    // does not write), so one application gives the same array.  With every
+    // value +0.0 (x_t = +-x_r + 0) an array of zeros, and the sum of two arrays
+    // that satisfy the program, satisfy it bit for bit (sign flips commute with
+    // round-to-nearest addition; the + 0 turns -0 into +0 on both sides): the
+    // caller says so and the application is left out.
+    if (!(out_satisfies_bc && mg->ctx->bc[level][ARTSS_FIELD_P].zero_values) && (st = mg_bc(mg, out, level)))
+        return st;
     if (mg->cfg.smoother == ARTSS_SMOOTHER_CGS) {
         for (int r = 0; r < mg->cfg.n_relax; r++) {
             if ((st = mg_cgs_step(mg, out, b, level))) return st;
@@ -1382,9 +1390,10 @@ int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its, const double *b0 =
     auto e1 = [&](int l) { return l == 0 ? out : mg->e1[l]; };
     auto r1 = [&](int l) { return l == 0 ? R0 : (const double *) mg->r1[l]; };
     for (int l = 0; l < L; l++) {
-        if ((st = mg_smooth(mg, e1(l), mg->tmp[l], r1(l), l))) return st;
+        // levels >= 1 start from the zeros set below
+        if ((st = mg_smooth(mg, e1(l), mg->tmp[l], r1(l), l, l > 0))) return st;
         if ((st = mg_residuum(mg, mg->r0[l], e1(l), r1(l), l))) return st;
-        if ((st = mg_bc(mg, mg->r0[l], l))) return st;
+        if (!mg->r0_bc_dead[l] && (st = mg_bc(mg, mg->r0[l], l))) return st;
         if ((st = mg_restrict(mg, mg->r1[l + 1], mg->r0[l], l + 1))) return st;
         // the reference also applies the boundary program to the restricted
         // residual; nothing reads r1's boundary cells (it is only a right-hand
@@ -1400,7 +1409,8 @@ int mg_vcycle(artss_mg *mg, double *out, int64_t *coarse_its, const double *b0 =
         if (l == L) {
             if ((st = mg_solve(mg, e1(l - 1), mg->tmp[l - 1], r1(l - 1), l - 1, coarse_its))) return st;
         } else {
-            if ((st = mg_smooth(mg, e1(l - 1), mg->tmp[l - 1], r1(l - 1), l - 1))) return st;
+            // e1 (smoothed, the program applied last) plus e0 (the program applied last)
+            if ((st = mg_smooth(mg, e1(l - 1), mg->tmp[l - 1], r1(l - 1), l - 1, true))) return st;
         }
     }
     return mg_bc(mg, out, 0);
@@ -1442,6 +1452,28 @@ int artss_mg_create(artss_ctx *ctx, const artss_mg_cfg *cfg, artss_mg **out) {
         st = st ? st : artss_field_alloc(ctx, l + 1, &mg->tmp[l + 1]);
     }
     if (st) { artss_mg_destroy(mg); return st; }
+    // residuum0[l] is read only by the restriction to level l+1, at the 8 fine
+    // cells of each coarse inner cell
+    for (int l = 0; l < mg->L; l++) {
+        const BcProgram &p = ctx->bc[l][ARTSS_FIELD_P];
+        const Level &F = ctx->lvl[l], &Cl = ctx->lvl[l + 1];
+        const std::vector<bool> &cin = ctx->h_inner[l + 1];
+        if (!p.present || (int64_t) cin.size() != Cl.size()) continue;
+        std::vector<bool> is_target((size_t) F.size(), false);
+        for (int64_t t : p.h_target) is_target[(size_t) t] = true;
+        bool read = false;
+        for (int64_t k = 0; k < Cl.Nz && !read; k++)
+            for (int64_t j = 0; j < Cl.Ny && !read; j++)
+                for (int64_t i = 0; i < Cl.Nx && !read; i++) {
+                    if (!cin[(size_t) (i + Cl.Nx * j + Cl.nxy() * k)]) continue;
+                    for (int c = 0; c < 8 && !read; c++) {
+                        const int64_t fi = 2 * i - 1 + (c & 1), fj = 2 * j - 1 + (c >> 1 & 1), fk = 2 * k - 1 + (c >> 2);
+                        if (fi < 0 || fj < 0 || fk < 0 || fi >= F.Nx || fj >= F.Ny || fk >= F.Nz) read = true;
+                        else read = is_target[(size_t) (fi + F.Nx * fj + F.nxy() * fk)];
+                    }
+                }
+        mg->r0_bc_dead[l] = !read;
+    }
     *out = mg;
     return ARTSS_OK;
 }
