@@ -37,3 +37,23 @@ def test_graph_steps_equal_eager_steps(tmp_path, name):
                 assert np.array_equal(a, b), (name, f, eager.step_index)
         # steps 3.. ran as graph launches
         assert graph.graph_steps == sc.steps - 2
+
+
+@pytest.mark.parametrize("name", ["box_cgs", "channel_cube"])
+def test_programmatic_launch_changes_nothing(tmp_path, name):
+    """Kernels launched to overlap their predecessor's tail (artss_ctx_pdl 2,
+    the default, eager and inside graphs) give the fields that plain launches
+    (mode 0) give."""
+    sc = _scenes()[name]
+    xml = scenes.write(sc, str(tmp_path / f"{name}.xml"))
+    with A.Simulation(xml) as plain, A.Simulation(xml) as pdl, A.Simulation(xml) as pdl_graph:
+        lib = plain._lib
+        assert lib.artss_ctx_pdl(plain.context, 0) == 0
+        pdl_graph.set_graphs(True)
+        for s in (plain, pdl, pdl_graph):
+            assert s.run(sc.steps - 1) == sc.steps - 1
+        for f in FIELDS:
+            ref = plain.field(f)
+            assert np.array_equal(pdl.field(f), ref), (name, f)
+            assert np.array_equal(pdl_graph.field(f), ref), (name, f)
+        assert pdl_graph.graph_steps == sc.steps - 3
