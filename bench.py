@@ -45,7 +45,7 @@ def parse_args():
                          "against the mixed-precision solve, on the 256^3 Neumann problem with box obstacles")
     ap.add_argument("--poisson-n", type=int, default=256)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
