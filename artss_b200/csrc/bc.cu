@@ -91,6 +91,8 @@ __global__ void k_bc_wave_f32(float *__restrict__ f, const int64_t *__restrict__
                               const int64_t *__restrict__ root, const uint8_t *__restrict__ depth,
                               const uint8_t *__restrict__ neg, int64_t begin, int64_t end,
                               const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     for (int64_t q = begin + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < end;
          q += (int64_t) gridDim.x * blockDim.x) {
@@ -107,8 +109,8 @@ int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const Loop
     for (int w = 0; w < p.waves; w++) {
         const int64_t b = p.wave_begin[w], e = p.wave_begin[w + 1];
         if (e <= b) continue;
-        ARTSS_LAUNCH(ctx, FAM_BC, k_bc_wave_f32<<<flat_blocks(e - b), 256, 0, ctx->stream>>>(
-                                      f, p.d_target, p.d_root, p.d_depth, p.d_neg, b, e, pred));
+        ARTSS_LAUNCH_PDL(ctx, FAM_BC, k_bc_wave_f32, flat_blocks(e - b), 256, 0, 
+                                      f, p.d_target, p.d_root, p.d_depth, p.d_neg, b, e, pred);
         ARTSS_LAUNCH_CK(ctx);
     }
     return ARTSS_OK;

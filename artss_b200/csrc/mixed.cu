@@ -69,6 +69,8 @@ struct CoefF {
 __global__ void k_mx_jacobi(float *__restrict__ out, const float *__restrict__ in, const float *__restrict__ b,
                             const uint8_t *__restrict__ flags, Level L, Box3 box, CoefF c,
                             const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -86,6 +88,8 @@ __global__ void k_mx_jacobi(float *__restrict__ out, const float *__restrict__ i
 __global__ void k_mx_residuum(float *__restrict__ out, const float *__restrict__ e, const float *__restrict__ b,
                               const uint8_t *__restrict__ flags, Level L, Box3 box, float rx, float ry, float rz,
                               const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -103,6 +107,8 @@ __global__ void k_mx_residuum(float *__restrict__ out, const float *__restrict__
 __global__ void k_mx_restrict(float *__restrict__ out, const float *__restrict__ in,
                               const uint8_t *__restrict__ flags, Level C, Level F, Box3 box,
                               const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -120,6 +126,8 @@ __global__ void k_mx_restrict(float *__restrict__ out, const float *__restrict__
 // e = w * beta * (-b) on the inner cells
 __global__ void k_mx_jacobi0(float *__restrict__ out, const float *__restrict__ b, const uint8_t *__restrict__ flags,
                              Level L, Box3 box, CoefF c, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -137,6 +145,8 @@ __global__ void k_mx_jacobi0(float *__restrict__ out, const float *__restrict__ 
 __global__ void k_mx_prolong_add(float *__restrict__ fine, const float *__restrict__ in,
                                  const uint8_t *__restrict__ cflags, const uint8_t *__restrict__ fflags, Level C,
                                  Level F, Box3 box, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -164,6 +174,8 @@ __global__ void k_mx_outer_residual(const double *__restrict__ p, const double *
                                     float *__restrict__ r, const uint8_t *__restrict__ flags, Level L, Box3 box,
                                     double rx, double ry, double rz, double *__restrict__ partials,
                                     const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     __shared__ double smem[32];
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
@@ -188,6 +200,8 @@ __global__ void k_mx_outer_residual(const double *__restrict__ p, const double *
 // p += e on the inner cells (FP64 += FP32)
 __global__ void k_mx_correct(double *__restrict__ p, const float *__restrict__ e, const uint8_t *__restrict__ flags,
                              Level L, Box3 box, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
@@ -202,6 +216,8 @@ __global__ void k_mx_correct(double *__restrict__ p, const float *__restrict__ e
 // block partials of sum(x - shift) and sum((x - shift)^2) over the inner cells
 __global__ void k_mx_moments(const double *__restrict__ x, double shift, const uint8_t *__restrict__ flags, Level L,
                              Box3 box, double *__restrict__ p1, double *__restrict__ p2) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     __shared__ double smem[32];
     MX_COLUMN(box);
     const int64_t nj = L.Nx, nk = L.nxy();
@@ -226,6 +242,8 @@ __global__ void k_mx_moments(const double *__restrict__ x, double shift, const u
 // out = A p on the inner cells (FP64)
 __global__ void k_mx_laplacian(double *__restrict__ out, const double *__restrict__ p,
                                const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     MX_COLUMN(box);
     if (!col) return;
     const int64_t nj = L.Nx, nk = L.nxy();
@@ -238,6 +256,8 @@ __global__ void k_mx_laplacian(double *__restrict__ out, const double *__restric
 }
 
 __global__ void k_mx_fill(float *__restrict__ f, int64_t n, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
     if (pred && !pred->cond) return;
     for (int64_t q = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < n; q += (int64_t) gridDim.x * blockDim.x)
         f[q] = 0.f;
@@ -269,13 +289,13 @@ int mx_smooth_from_zero(artss_mixed *m, int l, const LoopState *pred) {
     const Box3 box = inner_box(L);
     const CoefF c = coef_f(ctx, l, m->cfg.w);
     int st;
-    ARTSS_LAUNCH(ctx, FAM_MG_JACOBI, k_mx_jacobi0<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
-                                         m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred));
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi0, mx_grid(box), box_block(), 0, 
+                                         m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
     ARTSS_LAUNCH_CK(ctx);
     if ((st = mx_bc(m, m->e[l], l, pred))) return st;
     for (int s = 1; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH(ctx, FAM_MG_JACOBI, k_mx_jacobi<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
-                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, 
+                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
         ARTSS_LAUNCH_CK(ctx);
         std::swap(m->e[l], m->t[l]);
         if ((st = mx_bc(m, m->e[l], l, pred))) return st;
@@ -291,8 +311,8 @@ int mx_smooth(artss_mixed *m, int l, const LoopState *pred) {
     const CoefF c = coef_f(ctx, l, m->cfg.w);
     int st;
     for (int s = 0; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH(ctx, FAM_MG_JACOBI, k_mx_jacobi<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
-                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, 
+                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
         ARTSS_LAUNCH_CK(ctx);
         std::swap(m->e[l], m->t[l]);
         if ((st = mx_bc(m, m->e[l], l, pred))) return st;
@@ -310,22 +330,22 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
         if ((st = mx_smooth_from_zero(m, l, pred))) return st;
         const Level &L = ctx->lvl[l];
         const Box3 box = inner_box(L);
-        ARTSS_LAUNCH(ctx, FAM_MG_RESIDUUM, k_mx_residuum<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_residuum, mx_grid(box), box_block(), 0, 
                                                m->q[l], m->e[l], m->r[l], ctx->d_flags[l], L, box,
                                                (float) (1. / (g.dx[l] * g.dx[l])), (float) (1. / (g.dy[l] * g.dy[l])),
-                                               (float) (1. / (g.dz[l] * g.dz[l])), pred));
+                                               (float) (1. / (g.dz[l] * g.dz[l])), pred);
         ARTSS_LAUNCH_CK(ctx);
         if ((st = mx_bc(m, m->q[l], l, pred))) return st;
         const Level &C = ctx->lvl[l + 1];
         const Box3 cbox = inner_box(C);
-        ARTSS_LAUNCH(ctx, FAM_MG_RESTRICT, k_mx_restrict<<<mx_grid(cbox), box_block(), 0, ctx->stream>>>(
-                                               m->r[l + 1], m->q[l], ctx->d_flags[l + 1], C, L, cbox, pred));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mx_restrict, mx_grid(cbox), box_block(), 0, 
+                                               m->r[l + 1], m->q[l], ctx->d_flags[l + 1], C, L, cbox, pred);
         ARTSS_LAUNCH_CK(ctx);
     }
     // coarsest level: FP64 solve from zero
     {
         const int64_t n = ctx->lvl[Lc].size();
-        ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mx_fill<<<flat_blocks(n), 256, 0, ctx->stream>>>(m->e[Lc], n, pred));
+        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_mx_fill, flat_blocks(n), 256, 0, m->e[Lc], n, pred);
         ARTSS_LAUNCH_CK(ctx);
         double w = m->cfg.coarse_w;
         if (w <= 0) {
@@ -341,9 +361,9 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
     for (int l = Lc - 1; l >= 0; l--) {
         const Level &C = ctx->lvl[l + 1], &F = ctx->lvl[l];
         const Box3 cbox = inner_box(C);
-        ARTSS_LAUNCH(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add<<<mx_grid(cbox), box_block(), 0, ctx->stream>>>(
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add, mx_grid(cbox), box_block(), 0, 
                                                  m->e[l], m->e[l + 1], ctx->d_flags[l + 1], ctx->d_flags[l], C, F,
-                                                 cbox, pred));
+                                                 cbox, pred);
         ARTSS_LAUNCH_CK(ctx);
         if ((st = mx_bc(m, m->e[l], l, pred))) return st;
         if ((st = mx_smooth(m, l, pred))) return st;
@@ -360,8 +380,8 @@ int mx_moments(artss_mixed *m, const double *x, double shift, double *s1, double
     int st;
     if ((st = check_reduce_blocks(grid))) return st;
     const int nb = (int) (grid.x * grid.y * grid.z);
-    ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_moments<<<grid, box_block(), 0, ctx->stream>>>(
-                                          x, shift, ctx->d_flags[0], L, box, ctx->d_partials, ctx->d_partials + nb));
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESNORM, k_mx_moments, grid, box_block(), 0, 
+                                          x, shift, ctx->d_flags[0], L, box, ctx->d_partials, ctx->d_partials + nb);
     ARTSS_LAUNCH_CK(ctx);
     LoopState a{}, b{};
     if ((st = finalize_sum(ctx, kSlotSum, nb))) return st;
@@ -437,9 +457,9 @@ int artss_laplacian(artss_ctx *ctx, double *out, double *p, int level) {
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
-    ARTSS_LAUNCH(ctx, FAM_MG_RESIDUUM, k_mx_laplacian<<<mx_grid(box), box_block(), 0, ctx->stream>>>(
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_laplacian, mx_grid(box), box_block(), 0, 
                                            out, p, ctx->d_flags[level], L, box, 1. / (g.dx[level] * g.dx[level]),
-                                           1. / (g.dy[level] * g.dy[level]), 1. / (g.dz[level] * g.dz[level])));
+                                           1. / (g.dy[level] * g.dy[level]), 1. / (g.dz[level] * g.dz[level]));
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -461,8 +481,8 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     double s1 = 0, s2 = 0;
     if (ctx->capturing) {
         if (remove_mean) { set_error("the mean removal reads sums on the host and cannot be captured"); return ARTSS_ERR_ARG; }
-        ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_moments<<<grid, box_block(), 0, ctx->stream>>>(
-                                              b, 0.0, ctx->d_flags[0], L, box, ctx->d_partials, ctx->d_partials + nb));
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESNORM, k_mx_moments, grid, box_block(), 0, 
+                                              b, 0.0, ctx->d_flags[0], L, box, ctx->d_partials, ctx->d_partials + nb);
         ARTSS_LAUNCH_CK(ctx);
         ARTSS_CK(cudaMemcpyAsync(ctx->d_partials, ctx->d_partials + nb, nb * sizeof(double), cudaMemcpyDeviceToDevice,
                                  ctx->stream));
@@ -490,16 +510,16 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     }
     while (cond) {
         for (int64_t r = 0; r < batch; r++) {
-            ARTSS_LAUNCH(ctx, FAM_MG_RESNORM, k_mx_outer_residual<<<grid, box_block(), 0, ctx->stream>>>(
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESNORM, k_mx_outer_residual, grid, box_block(), 0, 
                                                   p, b, m->r[0], ctx->d_flags[0], L, box, rx, ry, rz,
-                                                  ctx->d_partials, pred));
+                                                  ctx->d_partials, pred);
             ARTSS_LAUNCH_CK(ctx);
             if (ctx->capturing) st = finalize_loop_rel(ctx, kSlotOuter, nb, m->cfg.rel_tol, kSlotSum, max_eval);
             else st = finalize_loop(ctx, kSlotOuter, nb, tol, max_eval);
             if (st) return st;
             if ((st = mx_vcycle(m, pred))) return st;
-            ARTSS_LAUNCH(ctx, FAM_FIELD_OP, k_mx_correct<<<grid, box_block(), 0, ctx->stream>>>(
-                                                p, m->e[0], ctx->d_flags[0], L, box, pred));
+            ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_mx_correct, grid, box_block(), 0, 
+                                                p, m->e[0], ctx->d_flags[0], L, box, pred);
             ARTSS_LAUNCH_CK(ctx);
             if ((st = apply_bc(ctx, p, 0, ARTSS_FIELD_P, pred))) return st;
         }
