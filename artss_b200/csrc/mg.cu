@@ -830,8 +830,16 @@ k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__
         // phase k: iterate k from iterate k-1 (unless k-1 == max_it) and the
         // residual of iterate k-1 (k >= 2, or k = 1 for the relative
         // tolerance); iterate k-1 is accepted on entry
-        for (long long k = 1;; k++) {
-            const int sp_ = (int) ((k - 1) % 3), sn = (int) (k % 3);
+        // res > tol is decided on the squared sum where that is exact: outside
+        // +-16 units of roundoff around tol^2 the rounded square root lies on
+        // the same side of tol; inside that band, or for tol^2 outside the
+        // normal range, the square root is taken.  Buffers rotate without a
+        // 64-bit modulo.
+        double tol2 = tol * tol;
+        bool have_s = false;
+        double s_last = 0.0;
+        int sp_ = 0, sn = 1;
+        for (long long k = 1;; k++, sp_ = sn, sn = sn == 2 ? 0 : sn + 1) {
             const double *P = X + sp_ * bstride;
             double *N = X + sn * bstride;
             const bool sweep = k - 1 < max_it, resid = k >= 2 || rel;
@@ -932,14 +940,23 @@ k_mg_coarse_jacobi_pipe(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__
             if (k == 1) {
                 // relative tolerance: scaled by the residual of iterate 0
                 tol *= sqrt(s);
+                tol2 = tol * tol;
                 if (!(res > tol && 0 < max_it)) break;
                 it = 1;
                 continue;
             }
-            res = sqrt(s);  // residual of iterate k-1
-            if (!(res > tol && k - 1 < max_it)) break;  // it = k-1 stands
+            // residual of iterate k-1: sqrt(s)
+            const bool fast = tol2 > 1e-280 && tol2 < 1e280;
+            bool above;
+            if (fast && s > tol2 * (1.0 + 0x1p-49)) above = true;
+            else if (fast && s < tol2 * (1.0 - 0x1p-49)) above = false;
+            else above = sqrt(s) > tol;
+            have_s = true;
+            s_last = s;
+            if (!(above && k - 1 < max_it)) break;  // it = k-1 stands
             it = k;
         }
+        if (have_s) res = sqrt(s_last);
     }
     // the last halos sent must land before any rank leaves (their source and
     // destination are shared memory)
