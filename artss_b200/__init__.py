@@ -163,6 +163,9 @@ def load_cuda() -> C.CDLL:
             "artss_cgs_sweep_variant": ([_P, C.c_int], C.c_int),
             "artss_ctx_autotune": ([_P, C.c_int], C.c_int),
             "artss_ctx_pdl": ([_P, C.c_int], C.c_int),
+            "artss_ctx_stage_timing": ([_P, C.c_int], C.c_int),
+            "artss_ctx_stage_mark": ([_P, C.c_int], C.c_int),
+            "artss_ctx_stage_read": ([_P, C.POINTER(C.c_double), C.c_int], C.c_int),
             "artss_conv3d_fwd": ([_P, C.POINTER(ConvDesc), _P, _P, _P, _P], C.c_int),
             "artss_nn_check": ([_P], C.c_int),
             "artss_conv3d_wgrad": ([_P, C.POINTER(ConvDesc), _P, _P, _P], C.c_int),

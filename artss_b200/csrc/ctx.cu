@@ -165,6 +165,47 @@ int artss_ctx_profile_read(artss_ctx *ctx, int64_t *launches, double *ms, int n_
     return ARTSS_OK;
 }
 
+int artss_ctx_stage_timing(artss_ctx *ctx, int enable) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    Profile &p = ctx->prof;
+    for (auto &m : p.marks) p.pool.push_back(m.first);
+    p.marks.clear();
+    for (int s = 0; s < ARTSS_STAGES; s++) p.stage_ms[s] = 0.0;
+    p.stages = enable != 0;
+    return ARTSS_OK;
+}
+
+int artss_ctx_stage_mark(artss_ctx *ctx, int stage) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    if (stage < ARTSS_STAGE_END || stage >= ARTSS_STAGES) { set_error("stage out of range"); return ARTSS_ERR_ARG; }
+    Profile &p = ctx->prof;
+    if (!p.stages || ctx->capturing) return ARTSS_OK;
+    cudaEvent_t e = prof_event(ctx);
+    if (!e) { set_error("cudaEventCreate failed"); return ARTSS_ERR_CUDA; }
+    ARTSS_CK(cudaEventRecord(e, ctx->stream));
+    p.marks.push_back({e, stage});
+    return ARTSS_OK;
+}
+
+int artss_ctx_stage_read(artss_ctx *ctx, double *ms, int n_stages) {
+    if (!ctx) { set_error("null context"); return ARTSS_ERR_ARG; }
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    Profile &p = ctx->prof;
+    // the interval from one mark to the next belongs to the stage the first opens
+    for (size_t q = 0; q + 1 < p.marks.size(); q++) {
+        if (p.marks[q].second >= 0) {
+            float t = 0.f;
+            ARTSS_CK(cudaEventElapsedTime(&t, p.marks[q].first, p.marks[q + 1].first));
+            p.stage_ms[p.marks[q].second] += t;
+        }
+        p.pool.push_back(p.marks[q].first);
+    }
+    if (!p.marks.empty()) p.marks.erase(p.marks.begin(), p.marks.end() - 1);  // the last mark opens the next interval
+    for (int s = 0; s < n_stages && s < ARTSS_STAGES; s++) ms[s] = p.stage_ms[s];
+    return ARTSS_OK;
+}
+
 int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
     if (!grid || !out) { set_error("null argument"); return ARTSS_ERR_ARG; }
     *out = nullptr;

@@ -101,6 +101,9 @@ struct Profile {
     std::vector<std::pair<cudaEvent_t, int>> pending;  // start event (end = next) + family
     std::vector<cudaEvent_t> events;                    // recorded, in order
     std::vector<cudaEvent_t> pool;                      // free events
+    bool stages = false;                                // stage marks recorded (artss_ctx_stage_timing)
+    std::vector<std::pair<cudaEvent_t, int>> marks;     // stage boundary events, in order, with the stage they open
+    double stage_ms[ARTSS_STAGES] = {};
 };
 
 }  // namespace artss

@@ -1,19 +1,22 @@
 // Residual norm that allocates nothing.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// residual: code running inside a memory pool that must not grow, a host
+// residual: code running inside a memory pool that must not grow, or a host
 // application whose allocator owns the device (a coupled solver that hands us
-// only its arrays), or a step captured for replay where new allocations are
-// not allowed.  For them artss_residual_norm_static computes the same
+// only its arrays).  For them artss_residual_norm_static computes the same
 // ||b - A p||_2 and ||b||_2 as artss_residual_norm without a context: the
 // per-block partial sums go to the fixed array below, which every GPU that
-// loads this library keeps until the process exits.
+// loads this library keeps until the process exits.  The call waits for its
+// result, so it refuses a stream that is being captured into a graph.
 //
 // Host code cannot use `g_static_partials` as a device address (it names a
 // host-side shadow); the device address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current.
+// cudaGetSymbolAddress on the first call made with that device current, and
+// kept for the life of the process: after a cudaDeviceReset of that device
+// the kept address is stale, so the entry point must not be used across one.
 #include "internal.cuh"
 
+#include <cmath>
 #include <mutex>
 
 namespace artss {
@@ -100,6 +103,19 @@ extern "C" int artss_residual_norm_static(const artss_grid_desc *grid, const uin
         set_error("inconsistent grid description");
         return ARTSS_ERR_ARG;
     }
+    const double dx = grid->dx[0], dy = grid->dy[0], dz = grid->dz[0];
+    if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0) || !std::isfinite(dx) || !std::isfinite(dy) ||
+        !std::isfinite(dz)) {
+        set_error("cell spacing must be positive and finite");
+        return ARTSS_ERR_ARG;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ARTSS_CK(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error("artss_residual_norm_static waits for its result and cannot run on a capturing stream");
+        return ARTSS_ERR_ARG;
+    }
     const Box3 box{L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
     dim3 g = box_grid(box);
     const int64_t xy = (int64_t) g.x * g.y;
@@ -113,9 +129,7 @@ extern "C" int artss_residual_norm_static(const artss_grid_desc *grid, const uin
     double *scratch = nullptr;
     int st = static_scratch(&scratch);
     if (st) return st;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_static_resnorm<<<g, box_block(), 0, s>>>(p, b, flags, L, box, 1. / (grid->dx[0] * grid->dx[0]),
-                                               1. / (grid->dy[0] * grid->dy[0]), 1. / (grid->dz[0] * grid->dz[0]),
+    k_static_resnorm<<<g, box_block(), 0, s>>>(p, b, flags, L, box, 1. / (dx * dx), 1. / (dy * dy), 1. / (dz * dz),
                                                scratch);
     ARTSS_CK(cudaGetLastError());
     k_static_finalize<<<1, kReduceThreads, 0, s>>>(scratch, nb);

@@ -163,8 +163,10 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     const auto &phys = m_rt.settings().physical;
     const real nu = phys.nu.value();
     const real kappa = phys.kappa.value();
+    artss_ctx *ctx = m_rt.ctx();
 
     // 1. advection of velocity with the old velocity (:129-131)
+    artss_ctx_stage_mark(ctx, ARTSS_STAGE_ADVECTION);
     if (auto *sl = dynamic_cast<SLAdvect *>(adv_vel.get())) {
         sl->advect_vector(f.u, f.v, f.w, f.u0, f.v0, f.w0, f.u0, f.v0, f.w0);
     } else {
@@ -176,6 +178,7 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
 
     // 2. turbulent viscosity and diffusion (:140-152); NSTempSolver: laminar
     //    diffusion when nu != 0 (NSTempSolver.cpp:99-108)
+    artss_ctx_stage_mark(ctx, ARTSS_STAGE_DIFFUSION);
     if (m_turb) {
         mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
         dif_vel->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
@@ -197,12 +200,14 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
 
     // 3. momentum source (:155-163); its couple_vector (:162) writes u0, v0, w0 that
     //    update_data rewrites before they are read: the u_tmp half only
+    artss_ctx_stage_mark(ctx, ARTSS_STAGE_SOURCE);
     if (m_add_source) {
         sou_vel->add_source(f.u, f.v, f.w, f.f_x, f.f_y, f.f_z, sync);
         FieldController::couple_tmp(f.u, f.u_tmp, f.v, f.v_tmp, f.w, f.w_tmp);
     }
 
     // 4. pressure and projection (:167-176)
+    artss_ctx_stage_mark(ctx, ARTSS_STAGE_PRESSURE);
     pres->divergence(f.rhs, f.u_tmp, f.v_tmp, f.w_tmp, sync);
     if (m_rt.io) m_rt.io->need(f.p);
     pres->pressure(f.p, f.rhs, t, sync);
@@ -217,6 +222,7 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     }
 
     // 5. temperature (:184-240)
+    artss_ctx_stage_mark(ctx, ARTSS_STAGE_TEMPERATURE);
     adv_temp->advect(f.T, f.T0, f.u, f.v, f.w, sync);
     FieldController::couple_scalar(f.T, f.T0, f.T_tmp);
     const auto &ts = m_rt.settings().solver.temperature;
@@ -680,8 +686,10 @@ int64_t TimeIntegration::run(int64_t steps) {
             }
         }
         m_sc.solver_do_step(m_t_cur, false);
+        artss_ctx_stage_mark(m_rt.ctx(), ARTSS_STAGE_UPDATE);
         m_sc.update_sources(m_t_cur, false);
         m_sc.fields().update_data();
+        artss_ctx_stage_mark(m_rt.ctx(), ARTSS_STAGE_END);
         m_step++;
         m_t_cur = (real) m_step * m_dt;
         done++;

@@ -32,6 +32,8 @@ sys.path.insert(0, ROOT)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 STATE_FIELDS = ["u", "v", "w", "p", "T"]
+# stages of NSTempTurbSolver::do_step + the time loop's update (ARTSS_STAGE_* of artss_cuda.h)
+STAGES = ["advection", "diffusion", "momentum_source", "pressure", "temperature", "update"]
 
 
 def parse_args():
@@ -56,6 +58,14 @@ def workload(name: str, steps: int):
     if name == "channel":
         return "channel_256x128x128_cube_fp64", scenes.channel_with_cube(steps=steps)
     return "box_64cubed_plume_fp64", scenes.plume_box(n=64, steps=steps, n_level=4)
+
+
+def step_config(name: str, sc, inner: int, world: int) -> dict:
+    """The `config` object of a timestep line; both arms print the same one."""
+    return {"workload": name, "cells": f"{sc.nx}x{sc.ny}x{sc.nz}", "inner_cells": inner,
+            "obstacles": len(sc.obstacles), "dt": sc.dt, "mg_levels": sc.n_level,
+            "diffusion": sc.diffusion, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "no flush: the ~25 resident FP64 arrays (~870 MB) exceed the 126 MB L2"}
 
 
 def peaks():
@@ -194,7 +204,7 @@ def run_b200(args, dist):
     from artss_b200 import scenes
 
     torch.cuda.set_device(dist.local)
-    total_steps = args.warmup + 2 + 2 * args.steps + 2 * args.e2e_steps + 3 + 2
+    total_steps = args.warmup + 2 + 3 * args.steps + 2 * args.e2e_steps + 3 + 2
     name, sc = workload(args.workload, total_steps)
     tmp = tempfile.mkdtemp(prefix="artss_bench_")
     xml = scenes.write(sc, os.path.join(tmp, f"{name}_r{dist.rank}.xml"))
@@ -217,7 +227,6 @@ def run_b200(args, dist):
     A.cuda_check(cuda.artss_ctx_profile_read(ctx, L, M, nf), "profile")
     fam_names = [cuda.artss_kernel_family_name(f).decode() for f in range(nf)]
     share_ms = {fam_names[f]: M[f] for f in range(nf) if L[f]}
-    total_kernel_ms = sum(share_ms.values())
     dom = max((f for f in range(nf) if fam_names[f] in MODELED and L[f]), key=lambda f: M[f])
     # the timed steps run without per-launch events (they would split the
     # programmatic launch overlap); the dominant kernel is timed after them
@@ -252,6 +261,14 @@ def run_b200(args, dist):
     A.cuda_check(cuda.artss_ctx_profile_read(ctx, L, M, nf), "profile")
     dom_launches, dom_ms = int(L[dom]), float(M[dom])
     cuda.artss_ctx_profile(ctx, 0)
+    # the same number of steps once more with one event per stage boundary
+    # (artss_ctx_stage_mark, six per step): device ms per stage
+    A.cuda_check(cuda.artss_ctx_stage_timing(ctx, 1), "stage timing")
+    assert sim.run(args.steps) == args.steps, "scene ended early"
+    S = (C.c_double * 6)()
+    A.cuda_check(cuda.artss_ctx_stage_read(ctx, S, 6), "stage read")
+    A.cuda_check(cuda.artss_ctx_stage_timing(ctx, 0), "stage timing")
+    stage_ms = {n: round(S[i] / args.steps, 4) for i, n in enumerate(STAGES)}
 
     # end to end, pipelined (the headline): every step uploads its state from
     # page-locked host memory, runs one timestep and reads the state back
@@ -322,10 +339,7 @@ def run_b200(args, dist):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": name, "cells": f"{sc.nx}x{sc.ny}x{sc.nz}", "inner_cells": inner,
-                   "obstacles": len(sc.obstacles), "dt": sc.dt, "mg_levels": sc.n_level,
-                   "diffusion": sc.diffusion, "parallelism": "replicas" if dist.world > 1 else "single",
-                   "l2": "no flush: the ~25 resident FP64 arrays (~870 MB) exceed the 126 MB L2"},
+        "config": step_config(name, sc, inner, dist.world),
         "clocks": clocks,
         "e2e": {"value": e2e_cells_all / (e2e_ms_max * 1e-3), "unit": "cell-updates/s",
                 "h2d_bytes_per_step": len(STATE_FIELDS) * size * 8,
@@ -350,8 +364,12 @@ def run_b200(args, dist):
                      "launches": dom_launches, "avg_launch_us": 1e3 * dom_ms / max(dom_launches, 1),
                      "timing": "CUDA events around each launch on the simulation's stream, over a second run of "
                                "the timed steps (the first runs without them)"},
-        "kernel_share_ms": {k: round(v, 4) for k, v in sorted(share_ms.items(), key=lambda kv: -kv[1])},
-        "kernel_ms_of_two_steps": round(total_kernel_ms, 4),
+        "stage_ms_per_step": stage_ms,
+        "stage_timing": "device ms per stage and step: one CUDA event per stage boundary on the simulation's stream "
+                        "over a third run of the timed steps",
+        "kernel_family_ms_two_steps": {k: round(v, 4) for k, v in sorted(share_ms.items(), key=lambda kv: -kv[1])},
+        "kernel_family_note": "CUDA events around every launch over two untimed steps; the events serialise the "
+                              "programmatic launch overlap, so these sums exceed the step time (shares only)",
     }
     sim.close()
     return out, xml, inner
@@ -628,7 +646,7 @@ def run_reference(args, dist):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": name, "cells": f"{sc.nx}x{sc.ny}x{sc.nz}", "inner_cells": t["inner_cells"]},
+        "config": step_config(name, sc, t["inner_cells"], dist.world),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                          "sample": f"{args.warmup} warm-up + {len(timed)} timed steps of the unmodified ARTSS "
                                    "serial build (it has no multi-threaded CPU path; its OpenACC multicore build "

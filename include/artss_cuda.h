@@ -146,6 +146,29 @@ int64_t artss_ctx_kernel_launches(artss_ctx *ctx);
  * the last reset (all families, profiled or not) and the summed device time
  * of the profiled ones. */
 #define ARTSS_KERNEL_FAMILIES 22
+/* Stage timing (no counterpart in the reference, whose benchmark build only
+ * prints a wall clock per step, src/TimeIntegration.cpp:59,183).  With
+ * enable != 0 the host solvers record one CUDA event on the context stream
+ * at each stage boundary of a timestep (not inside graph capture);
+ * artss_ctx_stage_read synchronizes the stream and returns the device time
+ * summed per stage since the last enable.  Stages of NSTempTurbSolver::do_step
+ * (src/solver/NSTempTurbSolver.cpp:94-248): velocity advection, turbulence
+ * + velocity diffusion, momentum source, pressure (divergence, solve,
+ * projection), temperature (advection, diffusion, source); then the source
+ * update and FieldController::update_data of the time loop. */
+enum {
+    ARTSS_STAGE_ADVECTION = 0,
+    ARTSS_STAGE_DIFFUSION = 1,
+    ARTSS_STAGE_SOURCE = 2,
+    ARTSS_STAGE_PRESSURE = 3,
+    ARTSS_STAGE_TEMPERATURE = 4,
+    ARTSS_STAGE_UPDATE = 5,
+    ARTSS_STAGES = 6
+};
+#define ARTSS_STAGE_END (-1) /* closes the last stage of a step */
+int artss_ctx_stage_timing(artss_ctx *ctx, int enable);
+int artss_ctx_stage_mark(artss_ctx *ctx, int stage);
+int artss_ctx_stage_read(artss_ctx *ctx, double *ms, int n_stages);
 int artss_ctx_profile(artss_ctx *ctx, uint64_t mask);
 int artss_ctx_profile_read(artss_ctx *ctx, int64_t *launches, double *ms, int n_families);
 int artss_ctx_profile_reset(artss_ctx *ctx);
@@ -451,17 +474,21 @@ int artss_residual_norm(artss_ctx *ctx, const double *p, const double *b, double
 /* The same two norms for callers that cannot allocate device memory (a host
  * code whose allocator owns the device, a memory pool that must not grow):
  * no context, no allocation.  No counterpart in the reference.
- *  - grid: level 0 of the geometry; flags: device array of the level-0 cell
- *    flags (bit 0 = inner cell), or NULL when every computational-domain cell
- *    is inner; p, b: device arrays; stream: cudaStream_t or NULL.
+ *  - grid: level 0 of the geometry (positive, finite dx, dy, dz);
+ *    flags: device array of the level-0 cell flags (bit 0 = inner cell)
+ *    holding Nx*Ny*Nz bytes of level 0, or NULL when every
+ *    computational-domain cell is inner; p, b: device arrays of Nx*Ny*Nz
+ *    doubles; stream: cudaStream_t or NULL.
  *  - The per-block partial sums live in one fixed 128 KiB device array of
  *    this library, kept on every GPU that loads it until the process exits;
  *    grids with more than 8192 tiles of 64x4 cells in an x-y plane are
  *    rejected with ARTSS_ERR_LIMIT.
  *  - The first call on a device looks the array's address up (with that
- *    device current); make it before any stream capture.
+ *    device current) and keeps it; do not use this function across a
+ *    cudaDeviceReset of that device.
  *  - All calls share the array: calls that overlap on the GPU race.
- *  - Blocks until the results are on the host. */
+ *  - Blocks until the results are on the host, so it must not be called on
+ *    a stream that is being captured (returns ARTSS_ERR_ARG). */
 int artss_residual_norm_static(const artss_grid_desc *grid, const uint8_t *flags, const double *p, const double *b,
                                void *stream, double *res_out, double *b_norm_out);
 

@@ -11,6 +11,7 @@
 // Usage:
 //   artss_ref_driver <file.xml> [--steps N] [--dump DIR] [--every K]
 //                    [--lists] [--time] [--mg-rhs rhs.f64 --mg-rel-tol TOL]
+//                    [--fields u,v,w,...]   (dump only these fields)
 //
 // Dump layout (all little-endian, raw):
 //   DIR/meta.txt                       grid sizes per level, dt, steps
@@ -135,10 +136,20 @@ std::vector<NamedField> all_fields(FieldController *fc) {
     };
 }
 
+// comma-separated field names to dump; empty = all
+std::string g_dump_only;
+
+bool wanted(const char *name) {
+    if (g_dump_only.empty()) return true;
+    const std::string key = "," + g_dump_only + ",";
+    return key.find("," + std::string(name) + ",") != std::string::npos;
+}
+
 void dump_fields(const std::string &dir, size_t step, FieldController *fc) {
     char prefix[64];
     std::snprintf(prefix, sizeof(prefix), "/step%05zu_", step);
     for (auto &nf : all_fields(fc)) {
+        if (!wanted(nf.name)) continue;
         write_raw(dir + prefix + nf.name + ".f64", nf.f->data, nf.f->get_size() * sizeof(double));
     }
 }
@@ -199,7 +210,7 @@ double relative_residual(const Field &p, const Field &b) {
 int main(int argc, char **argv) {
     if (argc < 2) {
         std::fprintf(stderr, "usage: %s file.xml [--steps N] [--dump DIR] [--every K] [--lists] [--time]"
-                             " [--mg-rhs rhs.f64 --mg-rel-tol TOL --mg-max-cycles N]\n", argv[0]);
+                             " [--mg-rhs rhs.f64 --mg-rel-tol TOL --mg-max-cycles N] [--fields a,b,...]\n", argv[0]);
         return 1;
     }
     std::string xml = argv[1];
@@ -224,6 +235,7 @@ int main(int argc, char **argv) {
         else if (k == "--mg-rhs") mg_rhs = next();
         else if (k == "--mg-rel-tol") mg_rel_tol = std::stod(next());
         else if (k == "--mg-max-cycles") mg_max_cycles = std::stol(next());
+        else if (k == "--fields") g_dump_only = next();
         else { std::fprintf(stderr, "unknown option %s\n", k.c_str()); return 1; }
     }
     if (!dump_dir.empty()) make_dir(dump_dir);

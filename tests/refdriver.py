@@ -19,11 +19,16 @@ def available() -> bool:
     return os.access(DRIVER, os.X_OK)
 
 
-def run(xml: str, out_dir: str, steps: int, every: int = 1, lists: bool = False, timeout: float = 600) -> str:
+def run(xml: str, out_dir: str, steps: int, every: int = 1, lists: bool = False, timeout: float = 600,
+        fields: Optional[List[str]] = None) -> str:
+    """Runs the reference for `steps` steps and dumps the fields (all, or
+    only `fields`) at step 0 and every `every`-th step."""
     os.makedirs(out_dir, exist_ok=True)
     cmd = [DRIVER, xml, "--steps", str(steps), "--dump", out_dir, "--every", str(every)]
     if lists:
         cmd.append("--lists")
+    if fields:
+        cmd += ["--fields", ",".join(fields)]
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL, timeout=timeout)
     return out_dir
 

@@ -2,7 +2,8 @@
 allocate device memory (a host code whose allocator owns the GPU, a memory
 pool that must not grow).  It keeps its partial sums in a fixed device array
 of the library instead of context memory; its results must equal those of
-artss_residual_norm, which uses context scratch, on two calls in a row.
+artss_residual_norm, which uses context scratch, on two calls in a row, and
+the same norms computed on the CPU from the downloaded arrays.
 
 Collected last on purpose (file name), so that a run stopping at the first
 failure has run every other test first."""
@@ -44,17 +45,32 @@ def _check(ref, got):
         assert abs(x - y) <= TOL * max(abs(x), 1e-300), (ref, got)
 
 
+def _cpu_norms(sim, grid, inner):
+    """||b - A p||_2 over the inner cells and ||b||_2, the 7-point Laplacian
+    of VCycleMG.cpp:186-194 evaluated in numpy on the downloaded arrays"""
+    p, b = sim.field("p"), sim.field("rhs")
+    nj, nk = grid.Nx[0], grid.Nx[0] * grid.Ny[0]
+    rx, ry, rz = (1.0 / (grid.dx[0] * grid.dx[0]), 1.0 / (grid.dy[0] * grid.dy[0]), 1.0 / (grid.dz[0] * grid.dz[0]))
+    q = inner
+    r = b[q] - (rx * (p[q - 1] - 2 * p[q] + p[q + 1]) + ry * (p[q - nj] - 2 * p[q] + p[q + nj]) +
+                rz * (p[q - nk] - 2 * p[q] + p[q + nk]))
+    return float(np.sqrt(np.sum(r * r))), float(np.sqrt(np.sum(b[q] * b[q])))
+
+
 def test_static_residual_norm_box(tmp_path):
     """obstacle-free box: flags = NULL (every computational-domain cell is inner)"""
     lib, f = _static_fn()
     xml = scenes.write(scenes.plume_box(n=32, steps=4, n_level=3), str(tmp_path / "box.xml"))
-    grid = A.Geometry(xml).grid_desc()
+    geom = A.Geometry(xml)
+    grid = geom.grid_desc()
+    inner = geom.list("inner", 0)
     with A.Simulation(xml) as sim:
         for _ in range(2):
             sim.run(1)
             ref, got = _norms(sim, lib, f, grid, None)
             assert ref[1] > 0
             _check(ref, got)
+            _check(_cpu_norms(sim, grid, inner), got)
 
 
 def test_static_residual_norm_with_obstacle(tmp_path):
@@ -74,19 +90,48 @@ def test_static_residual_norm_with_obstacle(tmp_path):
             torch.cuda.synchronize()
             ref, got = _norms(sim, lib, f, grid, C.c_void_p(d_flags.data_ptr()))
             _check(ref, got)
+            _check(_cpu_norms(sim, grid, geom.list("inner", 0)), got)
+
+
+def _grid(nx, ny, nz, d=1.0):
+    grid = A.GridDesc()
+    grid.n_levels = 0
+    grid.Nx[0], grid.Ny[0], grid.Nz[0] = nx + 2, ny + 2, nz + 2
+    grid.i1[0], grid.i2[0] = 1, nx
+    grid.j1[0], grid.j2[0] = 1, ny
+    grid.k1[0], grid.k2[0] = 1, nz
+    grid.dx[0] = grid.dy[0] = grid.dz[0] = d
+    return grid
+
+
+def _device_arrays(grid):
+    """zero device arrays p, b covering the whole described grid, so that no
+    access could leave them even if a size check were missing"""
+    torch = pytest.importorskip("torch")
+    n = grid.Nx[0] * grid.Ny[0] * grid.Nz[0]
+    p = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    b = torch.zeros(n, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    return p, b, C.cast(C.c_void_p(p.data_ptr()), _D), C.cast(C.c_void_p(b.data_ptr()), _D)
 
 
 def test_static_residual_norm_rejects_oversized_grid():
     lib, f = _static_fn()
-    grid = A.GridDesc()
-    grid.n_levels = 0
-    grid.Nx[0], grid.Ny[0], grid.Nz[0] = 64 * 200 + 2, 4 * 50 + 2, 3
-    grid.i1[0], grid.i2[0] = 1, 64 * 200
-    grid.j1[0], grid.j2[0] = 1, 4 * 50
-    grid.k1[0], grid.k2[0] = 1, 1
-    grid.dx[0] = grid.dy[0] = grid.dz[0] = 1.0
+    grid = _grid(64 * 200, 4 * 50, 1)  # 10000 tiles of 64x4 cells per plane: above the 8192 limit
+    keep = _device_arrays(grid)
     r, bn = C.c_double(), C.c_double()
-    dummy = C.cast(C.c_void_p(16), _D)  # never dereferenced: the size check comes first
-    st = f(C.byref(grid), None, dummy, dummy, None, C.byref(r), C.byref(bn))
+    st = f(C.byref(grid), None, keep[2], keep[3], None, C.byref(r), C.byref(bn))
     assert st == -6
     assert b"too large" in lib.artss_last_error()
+
+
+@pytest.mark.parametrize("d", [0.0, -1.0, float("inf"), float("nan")])
+def test_static_residual_norm_rejects_bad_spacing(d):
+    lib, f = _static_fn()
+    grid = _grid(8, 8, 8)
+    grid.dy[0] = d
+    keep = _device_arrays(grid)
+    r, bn = C.c_double(), C.c_double()
+    st = f(C.byref(grid), None, keep[2], keep[3], None, C.byref(r), C.byref(bn))
+    assert st == -1
+    assert b"spacing" in lib.artss_last_error()
