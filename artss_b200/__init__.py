@@ -161,6 +161,7 @@ def load_cuda() -> C.CDLL:
             "artss_mixed_solve": ([_P, _D, _D, C.POINTER(SolveStats)], C.c_int),
             "artss_laplacian": ([_P, _D, _D, C.c_int], C.c_int),
             "artss_cgs_sweep_variant": ([_P, C.c_int], C.c_int),
+            "artss_ctx_sweep_variant": ([_P, C.c_int], C.c_int),
             "artss_ctx_autotune": ([_P, C.c_int], C.c_int),
             "artss_ctx_pdl": ([_P, C.c_int], C.c_int),
             "artss_ctx_stage_timing": ([_P, C.c_int], C.c_int),

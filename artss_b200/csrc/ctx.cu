@@ -248,6 +248,8 @@ int artss_ctx_create(const artss_grid_desc *grid, int device, artss_ctx **out) {
         return st;
     };
     if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return fail(e, "multiprocessor count");
     if ((e = cudaMalloc(&ctx->d_partials, kMaxPartials * sizeof(double))) != cudaSuccess) return fail(e, "partials");
     if ((e = cudaMalloc(&ctx->d_loop, 16 * sizeof(LoopState))) != cudaSuccess) return fail(e, "loop state");
     if ((e = cudaMalloc(&ctx->d_param, kParams * sizeof(double))) != cudaSuccess) return fail(e, "parameters");
@@ -280,6 +282,8 @@ int artss_ctx_destroy(artss_ctx *ctx) {
             cudaFree(p.d_target); cudaFree(p.d_root); cudaFree(p.d_depth); cudaFree(p.d_neg); cudaFree(p.d_value);
         }
     }
+    if (ctx->d_sweep3_obst) cudaFree(ctx->d_sweep3_obst);
+    for (auto &m : ctx->prof.marks) cudaEventDestroy(m.first);
     for (auto &pe : ctx->prof.pending) cudaEventDestroy(pe.first);
     for (auto e : ctx->prof.events) cudaEventDestroy(e);
     for (auto e : ctx->prof.pool) cudaEventDestroy(e);
@@ -664,6 +668,12 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
     }
     const Level &L = ctx->lvl[level];
     ctx->n_inner[level] = n_inner;
+    if (level == 0) {
+        // the sweep's obstacle table describes the old lists
+        if (ctx->d_sweep3_obst) cudaFree(ctx->d_sweep3_obst);
+        ctx->d_sweep3_obst = nullptr;
+        ctx->sweep3_obst_state = 0;
+    }
     // every inner cell must lie in the computational domain, every domain-list
     // cell in the box one layer larger; lists are strictly ascending
     auto check = [&](const int64_t *list, int64_t n, int64_t grow, const char *name) -> bool {

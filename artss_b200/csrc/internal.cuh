@@ -126,6 +126,12 @@ struct artss_ctx {
     artss::Profile prof;
     std::map<std::pair<const void *, int>, CUtensorMap> tmaps;  // TMA descriptors per (array, level)
     bool autotune = true;                                        // time kernel variants on first use
+    int sweep_force = -1;                                        // colored Gauss-Seidel sweep variant pinned (-1: tuned)
+    int sm_count = 0;                                            // multiprocessors of the device
+    // tile columns x planes of level 0 whose row-pair sweep tile (+ ring) holds a
+    // box cell that is not inner (k_cgs_sweep3); built on first use
+    uint8_t *d_sweep3_obst = nullptr;
+    int sweep3_obst_state = 0;                                   // 0 not built, 1 built, 2 every box cell inner
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
     // host transfers overlapped with the step: a second stream, completion
     // events of its uploads by slot, a mark of the main stream, its tail

@@ -815,6 +815,284 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
     if (partials && tid == 0) partials[block_linear()] = acc;
 }
 
+// ---- the sweep on row-pair threads with mbarrier pipelines ------------------
+//
+// The one-phase iteration of k_cgs_sweep_tma2 (red on plane k, black on plane
+// k-2), organised for fewer instructions per cell and no block-wide barrier:
+//  * a thread owns one x of a pair of rows (j, j+1): on every plane one of its
+//    two cells is red and the other black, so each step it makes one red update
+//    (plane k) and one black update (plane k-2).  Lanes are consecutive in x, so
+//    every shared-memory access of a warp is conflict-free.  The warps of a
+//    64 x kS3Ty tile cover rows y0-1 .. y0+kS3Ty (the tile and the red ring
+//    rows); a side warp covers the ring columns x0-1 and x0+64, whose two cells
+//    of a row have opposite colours (one red update per lane and plane);
+//  * x (tile + 2-cell ring, 72 x 12 from the even x at x0-3), b and EV (tile +
+//    1-cell ring, 66 x 10 from x0-1) arrive by TMA in shared-memory rings of 7
+//    and 6 planes, two steps ahead, each plane completing on its full mbarrier;
+//    lane 31 of the side warp issues a plane once every warp has arrived on the
+//    step mbarrier of the step that last read the slots it refills;
+//  * red results overwrite their cells of the x ring in place (red updates read
+//    only black cells of plane k, which stay old); a black update waits on the
+//    red mbarrier of the step that computed its plane's red cells, on which
+//    every warp arrives after its red update;
+//  * blocks are persistent: the (tile column, plane) units of the level are
+//    split evenly over the grid, a block taking consecutive planes of one or
+//    two columns (segments); planes ka-2 .. kb+2 of a segment [ka, kb] are
+//    staged, red runs on ka-1 .. kb+1 and black on ka .. kb.
+// Each iteration's values equal the in-place red-then-black sweep; out receives
+// iterate n+1 on the inner box (old values on cells that are not inner).
+// Every mbarrier wait is bounded: a wait that gives up raises the loop state's
+// error flag and the block leaves after the loads it issued have landed.
+constexpr int kS3Ty = 8;                         // tile rows
+constexpr int kS3Pairs = (kS3Ty + 2) / 2;        // row pairs (tile + ring rows)
+constexpr int kS3Warps = 2 * kS3Pairs + 1;       // row-pair warps (two per pair: x halves) + side warp
+constexpr int kS3Threads = 32 * kS3Warps;        // 352
+constexpr int kS3XW = 72, kS3XH = kS3Ty + 4;     // x window (cells)
+constexpr int kS3BW = 66, kS3BH = kS3Ty + 2;     // b / EV window
+constexpr int kS3SlotsX = 7, kS3SlotsB = 6, kS3Bars = 8, kS3Ahead = 2;
+constexpr int kS3PlaneX = kS3XW * kS3XH;         // 864 doubles (6912 B, a multiple of 128)
+constexpr int kS3PlaneB = 672;                   // 66 x 10 = 660 doubles, padded to a 128-byte multiple
+constexpr unsigned kS3BytesX = kS3XW * kS3XH * sizeof(double);
+constexpr unsigned kS3BytesB = kS3BW * kS3BH * sizeof(double);
+constexpr int kS3MinPlanes = 8;                  // planes per block at least
+static_assert((kS3PlaneX * 8) % 128 == 0 && (kS3PlaneB * 8) % 128 == 0 && kS3BW * kS3BH <= kS3PlaneB, "slots");
+static_assert(kS3XW == kTmaBoxX && kS3XH == kTmaBoxY && kS3BW == kSt2BoxBX && kS3BH == kSt2BoxBY, "maps shared");
+static_assert(kS3SlotsX >= kS3Ahead + 5 && kS3SlotsB >= kS3Ahead + 4 && kS3Bars >= kS3SlotsX, "ring depths");
+
+inline size_t sweep3_smem(bool turb) {
+    return (size_t) kS3PlaneX * kS3SlotsX * sizeof(double) +
+           (size_t) kS3PlaneB * kS3SlotsB * (turb ? 2 : 1) * sizeof(double);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// one stencil update at x-window offset e (row pitch kS3XW)
+template <bool TURB>
+__device__ __forceinline__ double cgs3_update(const DiffCoef &c, const double *__restrict__ xm,
+                                              const double *__restrict__ x0, const double *__restrict__ xp, int e,
+                                              double bv, double ev, double &res2) {
+    double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
+    if (TURB) {
+        turb_alpha(c, ev, ax, ay, az, rb);
+        beta = 1. / rb;
+    }
+    const double old = x0[e];
+    const double out_h = beta * (c.dsign * bv + ax * (x0[e + 1] + x0[e - 1]) + ay * (x0[e + kS3XW] + x0[e - kS3XW]) +
+                                 az * (xp[e] + xm[e]));
+    const double nw = c.omw * old + c.w * out_h;
+    const double r = rb * (nw - old);
+    res2 = r * r;
+    return nw;
+}
+
+// the block's segments: units [u0, u1) of (tile column, plane), column-major
+struct S3Walk {
+    int64_t u, u1;
+    int nz, ncx;
+    __device__ bool next(int &col, int &ka, int &kb, int bz0) {
+        if (u >= u1) return false;
+        col = (int) (u / nz);
+        const int k0 = (int) (u - (int64_t) col * nz);
+        const int64_t left = u1 - u;
+        const int k1 = (int) (left < (int64_t) (nz - k0) ? k0 + left - 1 : nz - 1);
+        ka = bz0 + k0;
+        kb = bz0 + k1;
+        u += k1 - k0 + 1;
+        return true;
+    }
+};
+
+template <bool TURB>
+__global__ void __launch_bounds__(kS3Threads, 2)
+k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
+             const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out, const uint8_t *__restrict__ flags,
+             const uint8_t *__restrict__ obst, Level L, Box3 box, DiffCoef c, int ncx, int ncy,
+             double *__restrict__ partials, LoopState *__restrict__ pred) {
+    extern __shared__ __align__(1024) double s3[];
+    __shared__ double red_sm[32];
+    __shared__ __align__(8) uint64_t full[kS3Bars], stepdone[kS3Bars], reddone[kS3Bars];
+    __shared__ int deathx[kS3Bars], deathb[kS3Bars];  // producer: last step reading each plane's x / b, EV
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    if (blockDim.x != kS3Threads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
+    double *X = s3;                                   // [kS3SlotsX][kS3PlaneX]
+    double *B = s3 + kS3SlotsX * kS3PlaneX;           // [kS3SlotsB][kS3PlaneB]
+    double *E = B + kS3SlotsB * kS3PlaneB;            // [kS3SlotsB][kS3PlaneB] (TURB)
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const bool side = warp == 2 * kS3Pairs;
+    const bool producer = side && lane == 31;
+    // 32-bit indices: the host takes this kernel only for levels of fewer than 2^31 cells
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    const int bx0 = (int) box.x0, bx1 = (int) box.x1, by0 = (int) box.y0, by1 = (int) box.y1;
+    const int bz0 = (int) box.z0, bz1 = (int) box.z1;
+    const int nz = bz1 - bz0 + 1;
+    const int64_t units = (int64_t) ncx * ncy * nz;
+    const int64_t u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
+
+    if (tid == 0) {
+        for (int s = 0; s < kS3Bars; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&stepdone[s], kS3Warps);
+            mbar_init(&reddone[s], kS3Warps);
+        }
+        fence_proxy_async();
+    }
+    __syncthreads();
+
+    // thread geometry inside a tile (x relative to x0, rows relative to y0)
+    const int rp = warp >> 1;                          // row pair: rows 2 rp - 1, 2 rp
+    const int hx = ((warp & 1) << 5) + lane;           // x offset 0..63
+    const int rowA = side ? lane - 1 : 2 * rp - 1;     // side: this lane's row
+    const bool tileA = !side && rowA >= 0, tileB = !side && 2 * rp < kS3Ty;  // rows A, B inside the tile
+    const int xoffA = side ? 2 + kS3XW * (lane + 1) : hx + 3 + kS3XW * (2 * rp + 1);  // x window, cell A / left
+    const int boffA = side ? kS3BW * lane : hx + 1 + kS3BW * 2 * rp;                   // b window
+    const bool side_lane = side && lane <= kS3Ty + 1;
+
+    // producer state: its own walk over the segments, one plane ahead of need
+    S3Walk pw{u0, u1, nz, ncx};
+    int p_col = 0, p_ka = 0, p_kb = -1, p_q = 0, p_S0 = 0;  // segment being issued, next local plane, its first step
+    bool p_more = producer && pw.next(p_col, p_ka, p_kb, bz0);
+    int issued = 0;  // global planes issued
+    bool ok = true;
+    auto issue_upto = [&](int target) {
+        while (p_more && issued <= target && ok) {
+            const int n = p_kb - p_ka + 1;
+            // the slots of plane `issued` held planes issued-7 (x) and issued-6 (b, EV):
+            // wait until every warp has finished the last step that read them
+            int d = -1;
+            if (issued >= kS3SlotsX) d = deathx[(issued - kS3SlotsX) % kS3Bars];
+            if (issued >= kS3SlotsB) d = max(d, deathb[(issued - kS3SlotsB) % kS3Bars]);
+            if (d >= 0) {
+                ok = mbar_wait(&stepdone[d % kS3Bars], (unsigned) (d / kS3Bars) & 1u, kStPolls);
+                if (!ok) break;
+            }
+            const int tx = p_col % ncx, ty = p_col / ncx;
+            const int x0 = bx0 + 64 * tx, y0 = by0 + kS3Ty * ty;
+            const int k = p_ka - 2 + p_q;
+            const int bar = issued % kS3Bars;
+            // x of local plane q is read on steps q-2 .. q+2, b and EV on q-1 and q+1 (within 0 .. n+2)
+            deathx[bar] = p_S0 + min(p_q + 2, n + 2);
+            deathb[bar] = p_S0 + min(p_q + 1, n + 2);
+            mbar_expect_tx(&full[bar], kS3BytesX + kS3BytesB * (TURB ? 2u : 1u));
+            tma_load_plane(X + (issued % kS3SlotsX) * kS3PlaneX, &tm_x, x0 - 3, y0 - 2, k, &full[bar]);
+            tma_load_plane(B + (issued % kS3SlotsB) * kS3PlaneB, &tm_b, x0 - 1, y0 - 1, k, &full[bar]);
+            if (TURB) tma_load_plane(E + (issued % kS3SlotsB) * kS3PlaneB, &tm_e, x0 - 1, y0 - 1, k, &full[bar]);
+            issued++;
+            if (++p_q == n + 4) {  // segment staged: the next one starts n + 3 steps later
+                p_S0 += n + 3;
+                p_q = 0;
+                p_more = pw.next(p_col, p_ka, p_kb, bz0);
+            }
+        }
+    };
+
+    double acc = 0.0;
+    S3Walk cw{u0, u1, nz, ncx};
+    int col, ka, kb;
+    int S = 0, P = 0;  // first step and first plane of the segment
+    while (ok && cw.next(col, ka, kb, bz0)) {
+        const int n = kb - ka + 1;
+        const int tx = col % ncx, ty = col / ncx;
+        const int x0 = bx0 + 64 * tx, y0 = by0 + kS3Ty * ty;
+        const bool dirty_col = obst != nullptr;
+        const uint8_t *ob = obst + (int64_t) col * L.Nz;
+        // this thread's cells: row-pair threads (x, rowA) and (x, rowA + 1); side lanes (x0-1, row) and (x0+64, row)
+        const int gx = side ? x0 - 1 : x0 + hx;
+        const int gy = y0 + rowA;
+        const bool xin = side ? (gx >= bx0) : (gx <= bx1);
+        const bool xin2 = side ? (x0 + 64 <= bx1) : xin;  // cell B (row-pair) / right cell (side)
+        const bool yinA = gy >= by0 && gy <= by1, yinB = side ? yinA : (gy + 1 >= by0 && gy + 1 <= by1);
+        const bool okA = (side ? side_lane : true) && xin && yinA;
+        const bool okB = (side ? side_lane : true) && xin2 && yinB;
+        const int gA = gx + nj * gy;                                  // cell A / left, plane 0
+        const int gB = side ? gA + 65 : gA + nj;                      // cell B / right
+        const int pA = (gx + gy) & 1;                                 // A red on plane k when (pA + k) even
+        const int xoffB = side ? xoffA + 65 : xoffA + kS3XW;
+        const int boffB = side ? boffA + 65 : boffA + kS3BW;
+        for (int s = 0; s <= n + 2 && ok; s++) {
+            const int Sg = S + s;
+            if (side) {
+                if (producer) issue_upto(P + min(s + 2, n + 3) + kS3Ahead);
+                ok = __all_sync(0xffffffffu, ok);  // the side warp leaves together
+                if (!ok) break;
+            }
+            // planes needed from this step on: 0..2 at the start, then s+2
+            for (int q = (s == 0 ? 0 : s + 2); q <= min(s + 2, n + 3) && ok; q++) {
+                const int g = P + q;
+                ok = mbar_wait(&full[g % kS3Bars], (unsigned) (g / kS3Bars) & 1u, kStPolls);
+            }
+            if (!ok) break;
+            // red on plane ka - 1 + s (local plane s + 1)
+            if (s <= n + 1) {
+                const int k = ka - 1 + s;
+                if (k >= bz0 && k <= bz1) {
+                    const bool redA = ((pA + k) & 1) == 0;
+                    bool on = redA ? okA : okB;
+                    const int g = gA + (redA ? 0 : gB - gA) + nk * k;
+                    if (on && dirty_col && ob[k]) on = (__ldg(flags + g) & kInner) != 0;
+                    if (on) {
+                        const int q = P + s + 1;
+                        const int e = redA ? xoffA : xoffB, eb = redA ? boffA : boffB;
+                        double *x0s = X + (q % kS3SlotsX) * kS3PlaneX;
+                        const int bo = (q % kS3SlotsB) * kS3PlaneB;
+                        double r2;
+                        const double nw = cgs3_update<TURB>(c, X + ((q - 1) % kS3SlotsX) * kS3PlaneX, x0s,
+                                                            X + ((q + 1) % kS3SlotsX) * kS3PlaneX, e, B[bo + eb],
+                                                            TURB ? E[bo + eb] : 0.0, r2);
+                        x0s[e] = nw;
+                        if ((redA ? tileA : tileB) && k >= ka && k <= kb) acc += r2;
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&reddone[Sg % kS3Bars]);
+            // black on plane ka - 3 + s (local plane s - 1), and the tile's two cells of that plane out
+            if (s >= 3 && !side) {
+                const int k = ka - 3 + s;
+                ok = mbar_wait(&reddone[(Sg - 2) % kS3Bars], (unsigned) ((Sg - 2) / kS3Bars) & 1u, kStPolls);
+                if (!ok) break;
+                const int q = P + s - 1;
+                const double *x0s = X + (q % kS3SlotsX) * kS3PlaneX;
+                const bool blkA = ((pA + k) & 1) != 0;
+                const int e = blkA ? xoffA : xoffB, eb = blkA ? boffA : boffB;
+                const bool tb = blkA ? tileA : tileB;
+                const int g = (blkA ? gA : gB) + nk * k;
+                double vb = x0s[e];
+                bool on = tb && (blkA ? okA : okB);
+                if (on && dirty_col && ob[k]) on = (__ldg(flags + g) & kInner) != 0;
+                if (on) {
+                    const int bo = (q % kS3SlotsB) * kS3PlaneB;
+                    double r2;
+                    vb = cgs3_update<TURB>(c, X + ((q - 1) % kS3SlotsX) * kS3PlaneX, x0s,
+                                           X + ((q + 1) % kS3SlotsX) * kS3PlaneX, e, B[bo + eb],
+                                           TURB ? E[bo + eb] : 0.0, r2);
+                    acc += r2;
+                }
+                if (tileA && okA) out[gA + nk * k] = blkA ? vb : x0s[xoffA];
+                if (tileB && okB) out[gB + nk * k] = blkA ? x0s[xoffB] : vb;
+            }
+            fence_proxy_async();  // this thread's shared-memory writes before slot refills
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&stepdone[Sg % kS3Bars]);
+        }
+        S += n + 3;
+        P += n + 4;
+    }
+    if (!ok) {
+        // a wait gave up: flag it, let the loads this block issued land, leave
+        if (pred) *(volatile int *) &pred->pad = 1;
+        if (producer)
+            for (int g = max(0, issued - kS3Bars); g < issued; g++)
+                (void) mbar_wait(&full[g % kS3Bars], (unsigned) (g / kS3Bars) & 1u, kStPolls);
+        return;
+    }
+    acc = artss_block_sum(acc, red_sm);
+    if (partials && tid == 0) partials[blockIdx.x] = acc;
+}
+
 // One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
 // the division by reciprocal_beta; turbulent: :345-362) + residual partials
 // of sum (rbeta * (out - in))^2 (:72-79).
@@ -1035,17 +1313,82 @@ namespace {
 
 // TMA descriptors of one sweep: x (the array read), b, EV, for the kernel with
 // 72 x 12 windows and for the one-phase kernel (70 x 12 and 66 x 10)
+constexpr int kSweepRowPair = 6;  // variant number of k_cgs_sweep3
 struct SweepMaps {
     const CUtensorMap *x = nullptr, *b = nullptr, *e = nullptr;
     const CUtensorMap *x2 = nullptr, *b2 = nullptr, *e2 = nullptr;
 };
 
+// Obstacle table of the row-pair sweep (k_cgs_sweep3): per tile column (64 x
+// kS3Ty cells, column-major over the inner box) and plane of level 0, 1 where
+// the tile or its 1-cell ring holds a box cell that is not inner (the kernel
+// reads cell flags there only).  *out = nullptr when every box cell is inner.
+// Built on the host from the inner-cell bitmap on first use.
+int sweep3_obst(artss_ctx *ctx, const Box3 &box, int ncx, int ncy, const uint8_t **out) {
+    if (ctx->sweep3_obst_state == 0) {
+        const Level &L = ctx->lvl[0];
+        const std::vector<bool> &in = ctx->h_inner[0];
+        if (!in.empty() && ctx->n_inner[0] == box.nx() * box.ny() * box.nz()) {
+            ctx->sweep3_obst_state = 2;
+        } else {
+            // no lists uploaded: every cell goes through its flag
+            std::vector<uint8_t> t((size_t) ncx * ncy * L.Nz, in.empty() ? 1 : 0);
+            if (!in.empty()) {
+                for (int64_t k = box.z0; k <= box.z1; k++)
+                    for (int64_t y = box.y0; y <= box.y1; y++)
+                        for (int64_t x = box.x0; x <= box.x1; x++) {
+                            if (in[(size_t) (x + L.Nx * y + L.nxy() * k)]) continue;
+                            const int64_t cx = (x - box.x0) / 64, cy = (y - box.y0) / kS3Ty;
+                            for (int64_t ty = std::max<int64_t>(0, cy - 1); ty <= std::min<int64_t>(ncy - 1, cy + 1); ty++)
+                                for (int64_t tx = std::max<int64_t>(0, cx - 1); tx <= std::min<int64_t>(ncx - 1, cx + 1);
+                                     tx++) {
+                                    const int64_t x0 = box.x0 + 64 * tx, y0 = box.y0 + kS3Ty * ty;
+                                    if (x >= x0 - 1 && x <= x0 + 64 && y >= y0 - 1 && y <= y0 + kS3Ty)
+                                        t[(size_t) ((tx + ncx * ty) * L.Nz + k)] = 1;
+                                }
+                        }
+            }
+            if (ctx->capturing) { set_error("sweep obstacle table built inside a capture"); return ARTSS_ERR_STATE; }
+            ARTSS_CK(cudaMalloc(&ctx->d_sweep3_obst, t.size()));
+            ARTSS_CK(cudaMemcpy(ctx->d_sweep3_obst, t.data(), t.size(), cudaMemcpyHostToDevice));
+            ctx->sweep3_obst_state = 1;
+        }
+    }
+    *out = ctx->sweep3_obst_state == 1 ? ctx->d_sweep3_obst : nullptr;
+    return ARTSS_OK;
+}
+
+// the row-pair sweep: persistent blocks, two per multiprocessor, at least
+// kS3MinPlanes (tile column, plane) units each
+int launch_sweep3(artss_ctx *ctx, bool turb, const Box3 &box, const SweepMaps &m, double *w, const Level &L,
+                  const DiffCoef &c, LoopState *pred, int *nb) {
+    const int ncx = (int) ((box.nx() + 63) / 64), ncy = (int) ((box.ny() + kS3Ty - 1) / kS3Ty);
+    const int64_t units = (int64_t) ncx * ncy * box.nz();
+    const int G = (int) std::min<int64_t>(std::min<int64_t>(2 * std::max(ctx->sm_count, 1), kMaxPartials / 2),
+                                          std::max<int64_t>(1, units / kS3MinPlanes));
+    const uint8_t *obst = nullptr;
+    int st = sweep3_obst(ctx, box, ncx, ncy, &obst);
+    if (st) return st;
+    const size_t smem = sweep3_smem(turb);
+    if (turb)
+        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgs_sweep3<true>, dim3(G), kS3Threads, smem, *m.x, *m.b2, *m.e2, w,
+                         (const uint8_t *) ctx->d_flags[0], obst, L, box, c, ncx, ncy, ctx->d_partials, pred);
+    else
+        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgs_sweep3<false>, dim3(G), kS3Threads, smem, *m.x, *m.b2, *m.b2, w,
+                         (const uint8_t *) ctx->d_flags[0], obst, L, box, c, ncx, ncy, ctx->d_partials, pred);
+    ARTSS_LAUNCH_CK(ctx);
+    *nb = G;
+    return ARTSS_OK;
+}
+
 // Variants of the TMA sweep: v < 3 the kernel with two barriers per plane step
-// and z-depth kStDepths[v]; v >= 3 the one-phase kernel with kStDepths[v - 3]
-// (only where its b / EV window starts at an even x).  Returns the number of
-// blocks (partials) in *nb.
+// and z-depth kStDepths[v]; 3 <= v < 6 the one-phase kernel with
+// kStDepths[v - 3]; v = 6 the row-pair kernel (kSweepRowPair); v >= 3 only
+// where the b / EV window starts at an even x.  Returns the number of blocks
+// (partials) in *nb.
 int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, const SweepMaps &m, double *w,
                      const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
+    if (v == kSweepRowPair) return launch_sweep3(ctx, turb, box, m, w, L, c, pred, nb);
     const int zb = kStDepths[v % 3];
     const dim3 g = sweep_tma_grid(box, zb);
     *nb = nblocks(g);
@@ -1077,7 +1420,9 @@ int set_sweep_smem(bool turb) {
     if (done[turb]) return ARTSS_OK;
     const int b1 = (int) sweep_tma_smem(turb), b2 = (int) sweep_tma2_smem(turb);
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    const int b3 = (int) sweep3_smem(turb);
     if (turb) {
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true>, attr, b3));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, attr, b1));
@@ -1085,6 +1430,7 @@ int set_sweep_smem(bool turb) {
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 16>, attr, b2));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 32>, attr, b2));
     } else {
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false>, attr, b3));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, attr, b1));
@@ -1102,17 +1448,25 @@ int set_sweep_smem(bool turb) {
 // changes nothing) and keeps the fastest for the context.
 int tune_sweep(artss_ctx *ctx, bool turb, bool one_phase, const Box3 &box, const SweepMaps &m, double *w,
                const Level &L, const DiffCoef &c, LoopState *pred, int *choice) {
+    if (ctx->sweep_force >= 0) {
+        if (ctx->sweep_force >= 3 && !one_phase) {
+            set_error("sweep variant needs an inner box starting at an odd x");
+            return ARTSS_ERR_ARG;
+        }
+        *choice = ctx->sweep_force;
+        return ARTSS_OK;
+    }
     const TuneKey key{0, L.Nx, L.Ny, L.Nz, turb ? 1 : 0};
     auto it = ctx->tuned.find(key);
     if (it != ctx->tuned.end() && (one_phase || it->second < 3)) { *choice = it->second; return ARTSS_OK; }
-    const int fallback = one_phase ? 4 : 1;
+    const int fallback = one_phase ? kSweepRowPair : 1;
     if (!ctx->autotune || ctx->capturing) { *choice = fallback; return ARTSS_OK; }
     cudaEvent_t e0, e1;
     ARTSS_CK(cudaEventCreate(&e0));
     ARTSS_CK(cudaEventCreate(&e1));
     int best = fallback, st = ARTSS_OK, nb = 0;
     float best_ms = 1e30f;
-    for (int v = 0; v < (one_phase ? 6 : 3) && !st; v++) {
+    for (int v = 0; v < (one_phase ? kSweepRowPair + 1 : 3) && !st; v++) {
         if ((st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb))) break;  // warm
         cudaEventRecord(e0, ctx->stream);
         for (int r = 0; r < 3 && !st; r++) st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb);
@@ -1146,6 +1500,13 @@ int artss_ctx_pdl(artss_ctx *ctx, int enable) {
     return ARTSS_OK;
 }
 
+int artss_ctx_sweep_variant(artss_ctx *ctx, int variant) {
+    if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
+    if (variant < -1 || variant > kSweepRowPair) { set_error("sweep variant is -1 .. 6"); return ARTSS_ERR_ARG; }
+    ctx->sweep_force = variant;
+    return ARTSS_OK;
+}
+
 int artss_cgs_sweep_variant(artss_ctx *ctx, int turbulent) {
     if (!ctx) return -1;
     const Level &L = ctx->lvl[0];
@@ -1157,7 +1518,7 @@ int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
     if (!ctx) return 0;
     const Level &L = ctx->lvl[0];
     auto it = ctx->tuned.find(TuneKey{0, L.Nx, L.Ny, L.Nz, turbulent ? 1 : 0});
-    return it == ctx->tuned.end() ? 0 : kStDepths[it->second % 3];
+    return it == ctx->tuned.end() ? 0 : it->second == kSweepRowPair ? -1 : kStDepths[it->second % 3];
 }
 
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
