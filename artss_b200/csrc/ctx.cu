@@ -282,7 +282,7 @@ int artss_ctx_destroy(artss_ctx *ctx) {
             cudaFree(p.d_target); cudaFree(p.d_root); cudaFree(p.d_depth); cudaFree(p.d_neg); cudaFree(p.d_value);
         }
     }
-    if (ctx->d_sweep3_obst) cudaFree(ctx->d_sweep3_obst);
+    for (uint8_t *t : ctx->d_sweep3_obst) if (t) cudaFree(t);
     for (auto &m : ctx->prof.marks) cudaEventDestroy(m.first);
     for (auto &pe : ctx->prof.pending) cudaEventDestroy(pe.first);
     for (auto e : ctx->prof.events) cudaEventDestroy(e);
@@ -670,9 +670,11 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
     ctx->n_inner[level] = n_inner;
     if (level == 0) {
         // the sweep's obstacle table describes the old lists
-        if (ctx->d_sweep3_obst) cudaFree(ctx->d_sweep3_obst);
-        ctx->d_sweep3_obst = nullptr;
-        ctx->sweep3_obst_state = 0;
+        for (int t = 0; t < 2; t++) {
+            if (ctx->d_sweep3_obst[t]) cudaFree(ctx->d_sweep3_obst[t]);
+            ctx->d_sweep3_obst[t] = nullptr;
+            ctx->sweep3_obst_state[t] = 0;
+        }
     }
     // every inner cell must lie in the computational domain, every domain-list
     // cell in the box one layer larger; lists are strictly ascending

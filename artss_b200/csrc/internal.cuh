@@ -130,8 +130,8 @@ struct artss_ctx {
     int sm_count = 0;                                            // multiprocessors of the device
     // tile columns x planes of level 0 whose row-pair sweep tile (+ ring) holds a
     // box cell that is not inner (k_cgs_sweep3); built on first use
-    uint8_t *d_sweep3_obst = nullptr;
-    int sweep3_obst_state = 0;                                   // 0 not built, 1 built, 2 every box cell inner
+    uint8_t *d_sweep3_obst[2] = {nullptr, nullptr};              // per tile height (64 x 8, 64 x 6)
+    int sweep3_obst_state[2] = {0, 0};                           // 0 not built, 1 built, 2 every box cell inner
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
     // host transfers overlapped with the step: a second stream, completion
     // events of its uploads by slot, a mark of the main stream, its tail

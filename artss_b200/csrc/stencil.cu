@@ -819,22 +819,24 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
 //
 // The one-phase iteration of k_cgs_sweep_tma2 (red on plane k, black on plane
 // k-2), organised for fewer instructions per cell and no block-wide barrier:
-//  * a thread owns one x of a pair of rows (j, j+1): on every plane one of its
-//    two cells is red and the other black, so each step it makes one red update
-//    (plane k) and one black update (plane k-2).  Lanes are consecutive in x, so
-//    every shared-memory access of a warp is conflict-free.  The warps of a
-//    64 x kS3Ty tile cover rows y0-1 .. y0+kS3Ty (the tile and the red ring
+//  * a lane owns two x columns (x and x + 32) of a pair of rows (j, j+1): on
+//    every plane one of a column's two cells is red and the other black, so each
+//    step it makes two red updates (plane k) and two black updates (plane k-2),
+//    four independent chains computed together.  Lanes are consecutive in x, so
+//    every shared-memory access of a warp is conflict-free.  One warp per row
+//    pair covers rows y0-1 .. y0+TY of a 64 x TY tile (the tile and the red ring
 //    rows); a side warp covers the ring columns x0-1 and x0+64, whose two cells
 //    of a row have opposite colours (one red update per lane and plane);
-//  * x (tile + 2-cell ring, 72 x 12 from the even x at x0-3), b and EV (tile +
-//    1-cell ring, 66 x 10 from x0-1) arrive by TMA in shared-memory rings of 7
-//    and 6 planes, two steps ahead, each plane completing on its full mbarrier;
-//    lane 31 of the side warp issues a plane once every warp has arrived on the
-//    step mbarrier of the step that last read the slots it refills;
+//  * x (tile + 2-cell ring, 72 x (TY+4) from the even x at x0-3), b and EV
+//    (tile + 1-cell ring, 66 x (TY+2) from x0-1) arrive by TMA in shared-memory
+//    rings, AHEAD steps ahead, each plane completing on its full mbarrier; lane
+//    31 of the side warp issues a plane once every warp has arrived on the step
+//    mbarrier of the step that last read the slots it refills;
 //  * red results overwrite their cells of the x ring in place (red updates read
 //    only black cells of plane k, which stay old); a black update waits on the
 //    red mbarrier of the step that computed its plane's red cells, on which
-//    every warp arrives after its red update;
+//    every warp arrives after its red updates; waiting threads sleep in
+//    mbarrier.try_wait instead of spinning;
 //  * blocks are persistent: the (tile column, plane) units of the level are
 //    split evenly over the grid, a block taking consecutive planes of one or
 //    two columns (segments); planes ka-2 .. kb+2 of a segment [ka, kb] are
@@ -843,35 +845,43 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
 // iterate n+1 on the inner box (old values on cells that are not inner).
 // Every mbarrier wait is bounded: a wait that gives up raises the loop state's
 // error flag and the block leaves after the loads it issued have landed.
-constexpr int kS3Ty = 8;                         // tile rows
-constexpr int kS3Pairs = (kS3Ty + 2) / 2;        // row pairs (tile + ring rows)
-constexpr int kS3Warps = 2 * kS3Pairs + 1;       // row-pair warps (two per pair: x halves) + side warp
-constexpr int kS3Threads = 32 * kS3Warps;        // 352
-constexpr int kS3XW = 72, kS3XH = kS3Ty + 4;     // x window (cells)
-constexpr int kS3BW = 66, kS3BH = kS3Ty + 2;     // b / EV window
-constexpr int kS3SlotsX = 7, kS3SlotsB = 6, kS3Bars = 8, kS3Ahead = 2;
-constexpr int kS3PlaneX = kS3XW * kS3XH;         // 864 doubles (6912 B, a multiple of 128)
-constexpr int kS3PlaneB = 672;                   // 66 x 10 = 660 doubles, padded to a 128-byte multiple
-constexpr unsigned kS3BytesX = kS3XW * kS3XH * sizeof(double);
-constexpr unsigned kS3BytesB = kS3BW * kS3BH * sizeof(double);
-constexpr int kS3MinPlanes = 8;                  // planes per block at least
-static_assert((kS3PlaneX * 8) % 128 == 0 && (kS3PlaneB * 8) % 128 == 0 && kS3BW * kS3BH <= kS3PlaneB, "slots");
-static_assert(kS3XW == kTmaBoxX && kS3XH == kTmaBoxY && kS3BW == kSt2BoxBX && kS3BH == kSt2BoxBY, "maps shared");
-static_assert(kS3SlotsX >= kS3Ahead + 5 && kS3SlotsB >= kS3Ahead + 4 && kS3Bars >= kS3SlotsX, "ring depths");
-
-inline size_t sweep3_smem(bool turb) {
-    return (size_t) kS3PlaneX * kS3SlotsX * sizeof(double) +
-           (size_t) kS3PlaneB * kS3SlotsB * (turb ? 2 : 1) * sizeof(double);
-}
+// Tile rows, ring depths (planes) and lookahead (steps) of one instance.  The
+// slot of plane I is refilled once every warp has finished the step that last
+// read its previous plane (I - NSX for x, I - NSB for b and EV); with
+// NSX >= AHEAD + 5 and NSB >= AHEAD + 4 that step lies before the producer's
+// current one, so the producer waits for warps at most one step behind it.
+template <int TY_, int NSX_, int NSB_, int AHEAD_>
+struct S3Cfg {
+    static constexpr int TY = TY_, NSX = NSX_, NSB = NSB_, AHEAD = AHEAD_;
+    static constexpr int Pairs = (TY + 2) / 2;      // row pairs (tile + ring rows)
+    static constexpr int Warps = Pairs + 1;         // row-pair warps (two x columns per lane) + side warp
+    static constexpr int Threads = 32 * Warps;
+    static constexpr int XW = 72, XH = TY + 4;      // x window (cells), from the even x at x0 - 3
+    static constexpr int BW = 66, BH = TY + 2;      // b / EV window, from x0 - 1
+    static constexpr int PlaneX = XW * XH;          // doubles per x slot
+    static constexpr int PlaneB = (BW * BH + 15) / 16 * 16;  // doubles per b / EV slot, 128-byte multiple
+    static constexpr unsigned BytesX = XW * XH * sizeof(double), BytesB = BW * BH * sizeof(double);
+    static_assert(TY % 2 == 0 && TY + 2 <= 31, "row pairs; side lanes and the producer lane fit one warp");
+    static_assert((PlaneX * 8) % 128 == 0 && (PlaneB * 8) % 128 == 0, "slots stay 128-byte aligned");
+    static_assert(NSX >= AHEAD + 5 && NSB >= AHEAD + 4 && NSX <= 8, "ring depths (barrier rings of 8)");
+    static size_t smem(bool turb) {
+        return (size_t) PlaneX * NSX * sizeof(double) + (size_t) PlaneB * NSB * (turb ? 2 : 1) * sizeof(double);
+    }
+};
+using S3Tall = S3Cfg<8, 7, 6, 2>;   // 64 x 8 tiles, 192 threads, 112.9 KB (turbulent)
+using S3Flat = S3Cfg<6, 8, 7, 3>;   // 64 x 6 tiles, 160 threads, 105.2 KB, one step more lookahead
+constexpr int kS3Bars = 8;          // mbarriers per ring (full, step, red)
+constexpr int kS3MinPlanes = 8;     // planes per block at least
+static_assert(S3Tall::XH == kTmaBoxY && S3Tall::BW == kSt2BoxBX && S3Tall::BH == kSt2BoxBY, "maps shared");
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// one stencil update at x-window offset e (row pitch kS3XW)
+// one stencil update at x-window offset e (row pitch 72)
 template <bool TURB>
 __device__ __forceinline__ double cgs3_update(const DiffCoef &c, const double *__restrict__ xm,
-                                              const double *__restrict__ x0, const double *__restrict__ xp, int e,
+                                              const double *__restrict__ x0, const double *__restrict__ xp, const int e,
                                               double bv, double ev, double &res2) {
     double ax = c.ax, ay = c.ay, az = c.az, beta = c.beta, rb = c.rbeta;
     if (TURB) {
@@ -879,7 +889,7 @@ __device__ __forceinline__ double cgs3_update(const DiffCoef &c, const double *_
         beta = 1. / rb;
     }
     const double old = x0[e];
-    const double out_h = beta * (c.dsign * bv + ax * (x0[e + 1] + x0[e - 1]) + ay * (x0[e + kS3XW] + x0[e - kS3XW]) +
+    const double out_h = beta * (c.dsign * bv + ax * (x0[e + 1] + x0[e - 1]) + ay * (x0[e + 72] + x0[e - 72]) +
                                  az * (xp[e] + xm[e]));
     const double nw = c.omw * old + c.w * out_h;
     const double r = rb * (nw - old);
@@ -904,8 +914,39 @@ struct S3Walk {
     }
 };
 
-template <bool TURB>
-__global__ void __launch_bounds__(kS3Threads, 2)
+template <int V>
+struct S3Par {
+    static constexpr int value = V;
+};
+
+// Waits on phase (g >> 3) & 1 of a ring barrier (kS3Bars = 8 per ring): each
+// try_wait may suspend the thread in hardware for up to kS3SuspendNs until the
+// phase completes, so a waiting warp does not spin on the issue slots; bounded
+// by kS3Polls tries.
+constexpr unsigned kS3SuspendNs = 2000;
+constexpr int kS3Polls = 1 << 19;
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t *bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kS3SuspendNs)
+        : "memory");
+    return done != 0;
+}
+__device__ __noinline__ bool mbar_wait_s3_slow(uint64_t *bar, unsigned parity) {
+    for (int n = 0; n < kS3Polls; n++)
+        if (mbar_try_sleep(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ bool mbar_wait_s3(uint64_t *bar, int g) {
+    const unsigned parity = (unsigned) (g >> 3) & 1u;
+    return mbar_try_sleep(bar, parity) || mbar_wait_s3_slow(bar, parity);
+}
+static_assert(kS3Bars == 8, "barrier rings are indexed with & 7 and >> 3");
+
+template <bool TURB, class G3>
+__global__ void __launch_bounds__(G3::Threads, 2)
 k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out, const uint8_t *__restrict__ flags,
              const uint8_t *__restrict__ obst, Level L, Box3 box, DiffCoef c, int ncx, int ncy,
@@ -917,166 +958,212 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;  // iteration enqueued past convergence
-    if (blockDim.x != kS3Threads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
-    double *X = s3;                                   // [kS3SlotsX][kS3PlaneX]
-    double *B = s3 + kS3SlotsX * kS3PlaneX;           // [kS3SlotsB][kS3PlaneB]
-    double *E = B + kS3SlotsB * kS3PlaneB;            // [kS3SlotsB][kS3PlaneB] (TURB)
+    if (blockDim.x != G3::Threads || blockDim.y != 1 || blockDim.z != 1) return;  // launch shape is fixed
+    double *X = s3;                                   // [NSX][PlaneX]
+    const double *B = s3 + G3::NSX * G3::PlaneX;      // [NSB][PlaneB]
+    const double *E = B + G3::NSB * G3::PlaneB;       // [NSB][PlaneB] (TURB)
+    constexpr int XW = G3::XW, BW = G3::BW, TY = G3::TY;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const bool side = warp == 2 * kS3Pairs;
-    const bool producer = side && lane == 31;
+    const bool side = warp == G3::Pairs;
     // 32-bit indices: the host takes this kernel only for levels of fewer than 2^31 cells
-    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    const int nj = (int) L.Nx, nk = (int) L.nxy(), nzl = (int) L.Nz;
     const int bx0 = (int) box.x0, bx1 = (int) box.x1, by0 = (int) box.y0, by1 = (int) box.y1;
     const int bz0 = (int) box.z0, bz1 = (int) box.z1;
     const int nz = bz1 - bz0 + 1;
     const int64_t units = (int64_t) ncx * ncy * nz;
     const int64_t u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
 
+    // producer (lane 31 of the side warp): its own walk over the segments, state
+    // in shared memory so that it holds no registers of the other threads
+    struct Prod {
+        S3Walk w;
+        int col, ka, kb, q, S0, issued, more;
+    };
+    __shared__ Prod pr;
     if (tid == 0) {
         for (int s = 0; s < kS3Bars; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&stepdone[s], kS3Warps);
-            mbar_init(&reddone[s], kS3Warps);
+            mbar_init(&stepdone[s], G3::Warps);
+            mbar_init(&reddone[s], G3::Warps);
         }
         fence_proxy_async();
+        pr.w = S3Walk{u0, u1, nz, ncx};
+        pr.kb = -1;
+        pr.q = pr.S0 = pr.issued = 0;
+        pr.more = pr.w.next(pr.col, pr.ka, pr.kb, bz0);
     }
     __syncthreads();
 
-    // thread geometry inside a tile (x relative to x0, rows relative to y0)
-    const int rp = warp >> 1;                          // row pair: rows 2 rp - 1, 2 rp
-    const int hx = ((warp & 1) << 5) + lane;           // x offset 0..63
-    const int rowA = side ? lane - 1 : 2 * rp - 1;     // side: this lane's row
-    const bool tileA = !side && rowA >= 0, tileB = !side && 2 * rp < kS3Ty;  // rows A, B inside the tile
-    const int xoffA = side ? 2 + kS3XW * (lane + 1) : hx + 3 + kS3XW * (2 * rp + 1);  // x window, cell A / left
-    const int boffA = side ? kS3BW * lane : hx + 1 + kS3BW * 2 * rp;                   // b window
-    const bool side_lane = side && lane <= kS3Ty + 1;
-
-    // producer state: its own walk over the segments, one plane ahead of need
-    S3Walk pw{u0, u1, nz, ncx};
-    int p_col = 0, p_ka = 0, p_kb = -1, p_q = 0, p_S0 = 0;  // segment being issued, next local plane, its first step
-    bool p_more = producer && pw.next(p_col, p_ka, p_kb, bz0);
-    int issued = 0;  // global planes issued
+    double acc = 0.0;
     bool ok = true;
     auto issue_upto = [&](int target) {
-        while (p_more && issued <= target && ok) {
-            const int n = p_kb - p_ka + 1;
-            // the slots of plane `issued` held planes issued-7 (x) and issued-6 (b, EV):
-            // wait until every warp has finished the last step that read them
+        while (pr.more && pr.issued <= target && ok) {
+            const int I = pr.issued, n = pr.kb - pr.ka + 1;
+            // the slots of plane I held planes I-NSX (x) and I-NSB (b, EV): wait
+            // until every warp has finished the last step that read them
             int d = -1;
-            if (issued >= kS3SlotsX) d = deathx[(issued - kS3SlotsX) % kS3Bars];
-            if (issued >= kS3SlotsB) d = max(d, deathb[(issued - kS3SlotsB) % kS3Bars]);
-            if (d >= 0) {
-                ok = mbar_wait(&stepdone[d % kS3Bars], (unsigned) (d / kS3Bars) & 1u, kStPolls);
-                if (!ok) break;
-            }
-            const int tx = p_col % ncx, ty = p_col / ncx;
-            const int x0 = bx0 + 64 * tx, y0 = by0 + kS3Ty * ty;
-            const int k = p_ka - 2 + p_q;
-            const int bar = issued % kS3Bars;
+            if (I >= G3::NSX) d = deathx[(I - G3::NSX) & 7];
+            if (I >= G3::NSB) d = max(d, deathb[(I - G3::NSB) & 7]);
+            if (d >= 0 && !(ok = mbar_wait_s3(&stepdone[d & 7], d))) break;
+            const int x0 = bx0 + 64 * (pr.col % ncx), y0 = by0 + TY * (pr.col / ncx);
+            const int k = pr.ka - 2 + pr.q;
+            const int bar = I & 7;
             // x of local plane q is read on steps q-2 .. q+2, b and EV on q-1 and q+1 (within 0 .. n+2)
-            deathx[bar] = p_S0 + min(p_q + 2, n + 2);
-            deathb[bar] = p_S0 + min(p_q + 1, n + 2);
-            mbar_expect_tx(&full[bar], kS3BytesX + kS3BytesB * (TURB ? 2u : 1u));
-            tma_load_plane(X + (issued % kS3SlotsX) * kS3PlaneX, &tm_x, x0 - 3, y0 - 2, k, &full[bar]);
-            tma_load_plane(B + (issued % kS3SlotsB) * kS3PlaneB, &tm_b, x0 - 1, y0 - 1, k, &full[bar]);
-            if (TURB) tma_load_plane(E + (issued % kS3SlotsB) * kS3PlaneB, &tm_e, x0 - 1, y0 - 1, k, &full[bar]);
-            issued++;
-            if (++p_q == n + 4) {  // segment staged: the next one starts n + 3 steps later
-                p_S0 += n + 3;
-                p_q = 0;
-                p_more = pw.next(p_col, p_ka, p_kb, bz0);
+            deathx[bar] = pr.S0 + min(pr.q + 2, n + 2);
+            deathb[bar] = pr.S0 + min(pr.q + 1, n + 2);
+            mbar_expect_tx(&full[bar], G3::BytesX + G3::BytesB * (TURB ? 2u : 1u));
+            tma_load_plane(X + (I % G3::NSX) * G3::PlaneX, &tm_x, x0 - 3, y0 - 2, k, &full[bar]);
+            tma_load_plane((double *) B + (I % G3::NSB) * G3::PlaneB, &tm_b, x0 - 1, y0 - 1, k, &full[bar]);
+            if (TURB) tma_load_plane((double *) E + (I % G3::NSB) * G3::PlaneB, &tm_e, x0 - 1, y0 - 1, k, &full[bar]);
+            pr.issued = I + 1;
+            if (++pr.q == n + 4) {  // segment staged: the next one starts n + 3 steps later
+                pr.S0 += n + 3;
+                pr.q = 0;
+                pr.more = pr.w.next(pr.col, pr.ka, pr.kb, bz0);
             }
         }
     };
 
-    double acc = 0.0;
+    // Cells of this thread.  Row-pair warp rp: lane l owns x = x0 + l and
+    // x0 + 32 + l (columns 0 and 1) of rows A = y0 + 2 rp - 1 and B = A + 1; the
+    // red cell of a column on even local steps is er[0] (x-window offset of
+    // column 0), on odd steps er[1]; the black cell is the other.  Side lane l
+    // (l <= TY + 1): A = (x0 - 1, y0 - 1 + l), B = (x0 + 64, same row).
+    const int rowA = side ? lane - 1 : 2 * warp - 1;  // relative to y0
+    const int lrow = side ? min(lane, TY + 1) : 0;   // side lanes past the ring keep in-window offsets
+    const int xoA = side ? 2 + XW * (lrow + 1) : lane + 3 + XW * (rowA + 2);
+    const int xoB = side ? xoA + 65 : xoA + XW;
+    const int boA = side ? BW * lrow : lane + 1 + BW * (rowA + 1);
+    const int boB = side ? boA + 65 : boA + BW;
+    const bool tileA = !side && rowA >= 0, tileB = !side && rowA + 1 < TY;
+    const int gdB = side ? 65 : nj;  // global index of B minus A
+
     S3Walk cw{u0, u1, nz, ncx};
-    int col, ka, kb;
-    int S = 0, P = 0;  // first step and first plane of the segment
+    int col, ka, kb, S = 0, P = 0;  // segment; its first step and first plane
     while (ok && cw.next(col, ka, kb, bz0)) {
         const int n = kb - ka + 1;
-        const int tx = col % ncx, ty = col / ncx;
-        const int x0 = bx0 + 64 * tx, y0 = by0 + kS3Ty * ty;
-        const bool dirty_col = obst != nullptr;
-        const uint8_t *ob = obst + (int64_t) col * L.Nz;
-        // this thread's cells: row-pair threads (x, rowA) and (x, rowA + 1); side lanes (x0-1, row) and (x0+64, row)
-        const int gx = side ? x0 - 1 : x0 + hx;
-        const int gy = y0 + rowA;
-        const bool xin = side ? (gx >= bx0) : (gx <= bx1);
-        const bool xin2 = side ? (x0 + 64 <= bx1) : xin;  // cell B (row-pair) / right cell (side)
-        const bool yinA = gy >= by0 && gy <= by1, yinB = side ? yinA : (gy + 1 >= by0 && gy + 1 <= by1);
-        const bool okA = (side ? side_lane : true) && xin && yinA;
-        const bool okB = (side ? side_lane : true) && xin2 && yinB;
-        const int gA = gx + nj * gy;                                  // cell A / left, plane 0
-        const int gB = side ? gA + 65 : gA + nj;                      // cell B / right
-        const int pA = (gx + gy) & 1;                                 // A red on plane k when (pA + k) even
-        const int xoffB = side ? xoffA + 65 : xoffA + kS3XW;
-        const int boffB = side ? boffA + 65 : boffA + kS3BW;
-        for (int s = 0; s <= n + 2 && ok; s++) {
-            const int Sg = S + s;
-            if (side) {
-                if (producer) issue_upto(P + min(s + 2, n + 3) + kS3Ahead);
-                ok = __all_sync(0xffffffffu, ok);  // the side warp leaves together
-                if (!ok) break;
-            }
-            // planes needed from this step on: 0..2 at the start, then s+2
-            for (int q = (s == 0 ? 0 : s + 2); q <= min(s + 2, n + 3) && ok; q++) {
-                const int g = P + q;
-                ok = mbar_wait(&full[g % kS3Bars], (unsigned) (g / kS3Bars) & 1u, kStPolls);
-            }
-            if (!ok) break;
-            // red on plane ka - 1 + s (local plane s + 1)
-            if (s <= n + 1) {
-                const int k = ka - 1 + s;
-                if (k >= bz0 && k <= bz1) {
-                    const bool redA = ((pA + k) & 1) == 0;
-                    bool on = redA ? okA : okB;
-                    const int g = gA + (redA ? 0 : gB - gA) + nk * k;
-                    if (on && dirty_col && ob[k]) on = (__ldg(flags + g) & kInner) != 0;
-                    if (on) {
-                        const int q = P + s + 1;
-                        const int e = redA ? xoffA : xoffB, eb = redA ? boffA : boffB;
-                        double *x0s = X + (q % kS3SlotsX) * kS3PlaneX;
-                        const int bo = (q % kS3SlotsB) * kS3PlaneB;
-                        double r2;
-                        const double nw = cgs3_update<TURB>(c, X + ((q - 1) % kS3SlotsX) * kS3PlaneX, x0s,
-                                                            X + ((q + 1) % kS3SlotsX) * kS3PlaneX, e, B[bo + eb],
-                                                            TURB ? E[bo + eb] : 0.0, r2);
-                        x0s[e] = nw;
-                        if ((redA ? tileA : tileB) && k >= ka && k <= kb) acc += r2;
-                    }
+        const int x0 = bx0 + 64 * (col % ncx), y0 = by0 + TY * (col / ncx);
+        const int gx = side ? x0 - 1 : x0 + lane, gy = y0 + rowA;
+        const bool yA = gy >= by0 && gy <= by1, yB = side ? yA : (gy + 1 >= by0 && gy + 1 <= by1);
+        const bool xin0 = side ? (lane <= TY + 1 && gx >= bx0) : gx <= bx1;
+        const bool xin1 = side ? (lane <= TY + 1 && x0 + 64 <= bx1) : gx + 32 <= bx1;
+        const bool okA0 = xin0 && yA, okB0 = (side ? xin1 : xin0) && yB;  // column 0 (side: left A, right B)
+        const bool okA1 = !side && xin1 && yA, okB1 = !side && xin1 && yB;  // column 1
+        const bool redA0 = ((gx + gy + ka - 1) & 1) == 0;  // A red on even local steps (both columns)
+        const int er[2] = {redA0 ? xoA : xoB, redA0 ? xoB : xoA};
+        const int ebr[2] = {redA0 ? boA : boB, redA0 ? boB : boA};
+        const bool ok0[2] = {redA0 ? okA0 : okB0, redA0 ? okB0 : okA0};
+        const bool ok1[2] = {redA0 ? okA1 : okB1, redA0 ? okB1 : okA1};
+        const bool tr[2] = {redA0 ? tileA : tileB, redA0 ? tileB : tileA};  // the cell lies in a tile row
+        const int gA = gx + nj * gy;
+        const bool wA0 = tileA && okA0, wB0 = tileB && okB0, wA1 = tileA && okA1, wB1 = tileB && okB1;
+        const uint8_t *ob = obst ? obst + (int64_t) col * nzl : nullptr;
+        // slot offsets (doubles) of planes qr+1, qr, qr-1, qr-2, qr-3 with qr = P + s + 1 the red plane
+        int xp1 = ((P + 2) % G3::NSX) * G3::PlaneX, x00 = ((P + 1) % G3::NSX) * G3::PlaneX;
+        int xm1 = (P % G3::NSX) * G3::PlaneX, xm2 = ((P + G3::NSX - 1) % G3::NSX) * G3::PlaneX,
+            xm3 = ((P + G3::NSX - 2) % G3::NSX) * G3::PlaneX;  // before P: unused until they hold this segment's planes
+        int b00 = ((P + 1) % G3::NSB) * G3::PlaneB, bm1 = (P % G3::NSB) * G3::PlaneB,
+            bm2 = ((P + G3::NSB - 1) % G3::NSB) * G3::PlaneB;
+        // obstacle bytes of the red planes of steps s, s-1, s-2 (the last is black's plane)
+        int o0 = (ob && ka - 1 >= 0) ? ob[ka - 1] : 0, o1 = 0, o2 = 0;
+
+        // the red (R) and black (K) updates of one step, computed together (independent
+        // chains: red writes plane qr, black reads planes qr-1 .. qr-3)
+        auto updates = [&](auto par, auto do_r, auto do_k, int kr) {
+            constexpr int Q = decltype(par)::value;
+            constexpr bool R = decltype(do_r)::value, K = decltype(do_k)::value;
+            double nr0 = 0, nr1 = 0, rr0 = 0, rr1 = 0, nb0 = 0, nb1 = 0, rb0 = 0, rb1 = 0, ob0 = 0, ob1 = 0;
+            bool onr0 = false, onr1 = false, onb0 = false, onb1 = false;
+            if (R) {
+                const int e = er[Q], eb = b00 + ebr[Q];
+                onr0 = ok0[Q];
+                onr1 = ok1[Q];
+                if (o0) {
+                    const int g = gA + (e == xoA ? 0 : gdB) + nk * kr;
+                    onr0 = onr0 && (__ldg(flags + g) & kInner);
+                    if (!side) onr1 = onr1 && (__ldg(flags + g + 32) & kInner);
                 }
+                double *pc = X + x00 + e;
+                nr0 = cgs3_update<TURB>(c, X + xm1 + e, pc, X + xp1 + e, 0, B[eb], TURB ? E[eb] : 0.0, rr0);
+                if (!side) nr1 = cgs3_update<TURB>(c, X + xm1 + e, pc, X + xp1 + e, 32, B[eb + 32],
+                                                   TURB ? E[eb + 32] : 0.0, rr1);
+            }
+            if (K) {
+                const int e = er[Q ^ 1], eb = bm2 + ebr[Q ^ 1];
+                onb0 = tr[Q ^ 1] && ok0[Q ^ 1];
+                onb1 = tr[Q ^ 1] && ok1[Q ^ 1];
+                if (o2) {
+                    const int g = gA + (e == xoA ? 0 : gdB) + nk * (kr - 2);
+                    onb0 = onb0 && (__ldg(flags + g) & kInner);
+                    onb1 = onb1 && (__ldg(flags + g + 32) & kInner);
+                }
+                const double *pc = X + xm2 + e;
+                ob0 = pc[0];
+                ob1 = pc[32];
+                nb0 = cgs3_update<TURB>(c, X + xm3 + e, pc, X + xm1 + e, 0, B[eb], TURB ? E[eb] : 0.0, rb0);
+                nb1 = cgs3_update<TURB>(c, X + xm3 + e, pc, X + xm1 + e, 32, B[eb + 32], TURB ? E[eb + 32] : 0.0,
+                                        rb1);
+            }
+            if (R) {
+                double *pc = X + x00 + er[Q];
+                if (onr0) pc[0] = nr0;
+                if (onr1) pc[32] = nr1;
+                if (tr[Q] && kr >= ka && kr <= kb) acc += (onr0 ? rr0 : 0.0) + (onr1 ? rr1 : 0.0);
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(&reddone[Sg % kS3Bars]);
-            // black on plane ka - 3 + s (local plane s - 1), and the tile's two cells of that plane out
-            if (s >= 3 && !side) {
-                const int k = ka - 3 + s;
-                ok = mbar_wait(&reddone[(Sg - 2) % kS3Bars], (unsigned) ((Sg - 2) / kS3Bars) & 1u, kStPolls);
-                if (!ok) break;
-                const int q = P + s - 1;
-                const double *x0s = X + (q % kS3SlotsX) * kS3PlaneX;
-                const bool blkA = ((pA + k) & 1) != 0;
-                const int e = blkA ? xoffA : xoffB, eb = blkA ? boffA : boffB;
-                const bool tb = blkA ? tileA : tileB;
-                const int g = (blkA ? gA : gB) + nk * k;
-                double vb = x0s[e];
-                bool on = tb && (blkA ? okA : okB);
-                if (on && dirty_col && ob[k]) on = (__ldg(flags + g) & kInner) != 0;
-                if (on) {
-                    const int bo = (q % kS3SlotsB) * kS3PlaneB;
-                    double r2;
-                    vb = cgs3_update<TURB>(c, X + ((q - 1) % kS3SlotsX) * kS3PlaneX, x0s,
-                                           X + ((q + 1) % kS3SlotsX) * kS3PlaneX, e, B[bo + eb],
-                                           TURB ? E[bo + eb] : 0.0, r2);
-                    acc += r2;
-                }
-                if (tileA && okA) out[gA + nk * k] = blkA ? vb : x0s[xoffA];
-                if (tileB && okB) out[gB + nk * k] = blkA ? x0s[xoffB] : vb;
+            if (lane == 0) mbar_arrive(&reddone[(S + (kr - ka + 1)) & 7]);
+            if (K) {
+                acc += (onb0 ? rb0 : 0.0) + (onb1 ? rb1 : 0.0);
+                const double vb0 = onb0 ? nb0 : ob0, vb1 = onb1 ? nb1 : ob1;
+                const double *pr0 = X + xm2 + er[Q];  // the red cells of the same plane
+                const double vr0 = pr0[0], vr1 = pr0[32];
+                const bool aRed = er[Q] == xoA;
+                double *o = out + gA + nk * (kr - 2);
+                if (wA0) o[0] = aRed ? vr0 : vb0;
+                if (wB0) o[nj] = aRed ? vb0 : vr0;
+                if (wA1) o[32] = aRed ? vr1 : vb1;
+                if (wB1) o[nj + 32] = aRed ? vb1 : vr1;
             }
+        };
+
+        auto step = [&](int s, auto par) {
+            const int Sg = S + s;
+            const int kr = ka - 1 + s;
+            const int onext = (ob && kr + 1 < nzl) ? __ldg(ob + kr + 1) : 0;  // next step's, loaded early
+            if (side) {
+                if (lane == 31) issue_upto(P + min(s + 2, n + 3) + G3::AHEAD);
+                ok = __all_sync(0xffffffffu, ok);  // the side warp leaves together
+            }
+            if (ok) {
+                if (s == 0)
+                    ok = mbar_wait_s3(&full[P & 7], P) && mbar_wait_s3(&full[(P + 1) & 7], P + 1) &&
+                         mbar_wait_s3(&full[(P + 2) & 7], P + 2);
+                else if (s + 2 <= n + 3)
+                    ok = mbar_wait_s3(&full[(P + s + 2) & 7], P + s + 2);
+            }
+            const bool do_k = !side && s >= 3;  // black on plane kr - 2 (local plane s - 1)
+            if (ok && do_k) ok = mbar_wait_s3(&reddone[(Sg - 2) & 7], Sg - 2);
+            if (!ok) return;
+            const bool do_r = s <= n + 1 && kr >= bz0 && kr <= bz1;  // red on plane kr (local plane s + 1)
+            using T = S3Par<1>;
+            using F = S3Par<0>;
+            if (do_r && do_k) updates(par, T{}, T{}, kr);
+            else if (do_r) updates(par, T{}, F{}, kr);
+            else if (do_k) updates(par, F{}, T{}, kr);
+            else updates(par, F{}, F{}, kr);
             fence_proxy_async();  // this thread's shared-memory writes before slot refills
             __syncwarp();
-            if (lane == 0) mbar_arrive(&stepdone[Sg % kS3Bars]);
+            if (lane == 0) mbar_arrive(&stepdone[Sg & 7]);
+            // rotate the slot rings and the obstacle history to step s + 1
+            xm3 = xm2; xm2 = xm1; xm1 = x00; x00 = xp1;
+            xp1 = xp1 + G3::PlaneX == G3::NSX * G3::PlaneX ? 0 : xp1 + G3::PlaneX;
+            bm2 = bm1; bm1 = b00;
+            b00 = b00 + G3::PlaneB == G3::NSB * G3::PlaneB ? 0 : b00 + G3::PlaneB;
+            o2 = o1; o1 = o0; o0 = onext;
+        };
+        for (int s = 0; s <= n + 2 && ok; s += 2) {
+            step(s, S3Par<0>{});
+            if (s + 1 <= n + 2 && ok) step(s + 1, S3Par<1>{});
         }
         S += n + 3;
         P += n + 4;
@@ -1084,9 +1171,8 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
     if (!ok) {
         // a wait gave up: flag it, let the loads this block issued land, leave
         if (pred) *(volatile int *) &pred->pad = 1;
-        if (producer)
-            for (int g = max(0, issued - kS3Bars); g < issued; g++)
-                (void) mbar_wait(&full[g % kS3Bars], (unsigned) (g / kS3Bars) & 1u, kStPolls);
+        if (side && lane == 31)
+            for (int g = max(0, pr.issued - kS3Bars); g < pr.issued; g++) (void) mbar_wait_s3(&full[g & 7], g);
         return;
     }
     acc = artss_block_sum(acc, red_sm);
@@ -1313,82 +1399,89 @@ namespace {
 
 // TMA descriptors of one sweep: x (the array read), b, EV, for the kernel with
 // 72 x 12 windows and for the one-phase kernel (70 x 12 and 66 x 10)
-constexpr int kSweepRowPair = 6;  // variant number of k_cgs_sweep3
+constexpr int kSweepRowPair = 6;  // variant number of k_cgs_sweep3 with 64 x 8 tiles; + 1: 64 x 6 tiles
+constexpr int kSweepVariants = kSweepRowPair + 2;
 struct SweepMaps {
     const CUtensorMap *x = nullptr, *b = nullptr, *e = nullptr;
     const CUtensorMap *x2 = nullptr, *b2 = nullptr, *e2 = nullptr;
+    const CUtensorMap *x3 = nullptr, *b3 = nullptr, *e3 = nullptr;  // 72 x 10 and 66 x 8 windows
 };
 
-// Obstacle table of the row-pair sweep (k_cgs_sweep3): per tile column (64 x
-// kS3Ty cells, column-major over the inner box) and plane of level 0, 1 where
-// the tile or its 1-cell ring holds a box cell that is not inner (the kernel
-// reads cell flags there only).  *out = nullptr when every box cell is inner.
-// Built on the host from the inner-cell bitmap on first use.
-int sweep3_obst(artss_ctx *ctx, const Box3 &box, int ncx, int ncy, const uint8_t **out) {
-    if (ctx->sweep3_obst_state == 0) {
+// Obstacle table of the row-pair sweep (k_cgs_sweep3) with tiles of 64 x ty
+// cells (table t of the context): per tile column (column-major over the inner
+// box) and plane of level 0, 1 where the tile or its 1-cell ring holds a box
+// cell that is not inner (the kernel reads cell flags there only).
+// *out = nullptr when every box cell is inner.  Built on the host from the
+// inner-cell bitmap on first use.
+int sweep3_obst(artss_ctx *ctx, const Box3 &box, int t, int ty_rows, int ncx, int ncy, const uint8_t **out) {
+    if (ctx->sweep3_obst_state[t] == 0) {
         const Level &L = ctx->lvl[0];
         const std::vector<bool> &in = ctx->h_inner[0];
         if (!in.empty() && ctx->n_inner[0] == box.nx() * box.ny() * box.nz()) {
-            ctx->sweep3_obst_state = 2;
+            ctx->sweep3_obst_state[t] = 2;
         } else {
             // no lists uploaded: every cell goes through its flag
-            std::vector<uint8_t> t((size_t) ncx * ncy * L.Nz, in.empty() ? 1 : 0);
+            std::vector<uint8_t> tab((size_t) ncx * ncy * L.Nz, in.empty() ? 1 : 0);
             if (!in.empty()) {
                 for (int64_t k = box.z0; k <= box.z1; k++)
                     for (int64_t y = box.y0; y <= box.y1; y++)
                         for (int64_t x = box.x0; x <= box.x1; x++) {
                             if (in[(size_t) (x + L.Nx * y + L.nxy() * k)]) continue;
-                            const int64_t cx = (x - box.x0) / 64, cy = (y - box.y0) / kS3Ty;
+                            const int64_t cx = (x - box.x0) / 64, cy = (y - box.y0) / ty_rows;
                             for (int64_t ty = std::max<int64_t>(0, cy - 1); ty <= std::min<int64_t>(ncy - 1, cy + 1); ty++)
                                 for (int64_t tx = std::max<int64_t>(0, cx - 1); tx <= std::min<int64_t>(ncx - 1, cx + 1);
                                      tx++) {
-                                    const int64_t x0 = box.x0 + 64 * tx, y0 = box.y0 + kS3Ty * ty;
-                                    if (x >= x0 - 1 && x <= x0 + 64 && y >= y0 - 1 && y <= y0 + kS3Ty)
-                                        t[(size_t) ((tx + ncx * ty) * L.Nz + k)] = 1;
+                                    const int64_t x0 = box.x0 + 64 * tx, y0 = box.y0 + ty_rows * ty;
+                                    if (x >= x0 - 1 && x <= x0 + 64 && y >= y0 - 1 && y <= y0 + ty_rows)
+                                        tab[(size_t) ((tx + ncx * ty) * L.Nz + k)] = 1;
                                 }
                         }
             }
             if (ctx->capturing) { set_error("sweep obstacle table built inside a capture"); return ARTSS_ERR_STATE; }
-            ARTSS_CK(cudaMalloc(&ctx->d_sweep3_obst, t.size()));
-            ARTSS_CK(cudaMemcpy(ctx->d_sweep3_obst, t.data(), t.size(), cudaMemcpyHostToDevice));
-            ctx->sweep3_obst_state = 1;
+            ARTSS_CK(cudaMalloc(&ctx->d_sweep3_obst[t], tab.size()));
+            ARTSS_CK(cudaMemcpy(ctx->d_sweep3_obst[t], tab.data(), tab.size(), cudaMemcpyHostToDevice));
+            ctx->sweep3_obst_state[t] = 1;
         }
     }
-    *out = ctx->sweep3_obst_state == 1 ? ctx->d_sweep3_obst : nullptr;
+    *out = ctx->sweep3_obst_state[t] == 1 ? ctx->d_sweep3_obst[t] : nullptr;
     return ARTSS_OK;
 }
 
 // the row-pair sweep: persistent blocks, two per multiprocessor, at least
 // kS3MinPlanes (tile column, plane) units each
-int launch_sweep3(artss_ctx *ctx, bool turb, const Box3 &box, const SweepMaps &m, double *w, const Level &L,
-                  const DiffCoef &c, LoopState *pred, int *nb) {
-    const int ncx = (int) ((box.nx() + 63) / 64), ncy = (int) ((box.ny() + kS3Ty - 1) / kS3Ty);
+extern "C++" {  // a template inside the extern "C" block of this file
+template <class G3>
+int launch_sweep3(artss_ctx *ctx, bool turb, int t, const Box3 &box, const CUtensorMap *mx, const CUtensorMap *mb,
+                  const CUtensorMap *me, double *w, const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
+    const int ncx = (int) ((box.nx() + 63) / 64), ncy = (int) ((box.ny() + G3::TY - 1) / G3::TY);
     const int64_t units = (int64_t) ncx * ncy * box.nz();
     const int G = (int) std::min<int64_t>(std::min<int64_t>(2 * std::max(ctx->sm_count, 1), kMaxPartials / 2),
                                           std::max<int64_t>(1, units / kS3MinPlanes));
     const uint8_t *obst = nullptr;
-    int st = sweep3_obst(ctx, box, ncx, ncy, &obst);
+    int st = sweep3_obst(ctx, box, t, G3::TY, ncx, ncy, &obst);
     if (st) return st;
-    const size_t smem = sweep3_smem(turb);
+    const size_t smem = G3::smem(turb);
     if (turb)
-        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgs_sweep3<true>, dim3(G), kS3Threads, smem, *m.x, *m.b2, *m.e2, w,
+        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, (k_cgs_sweep3<true, G3>), dim3(G), G3::Threads, smem, *mx, *mb, *me, w,
                          (const uint8_t *) ctx->d_flags[0], obst, L, box, c, ncx, ncy, ctx->d_partials, pred);
     else
-        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgs_sweep3<false>, dim3(G), kS3Threads, smem, *m.x, *m.b2, *m.b2, w,
+        ARTSS_LAUNCH_PDL(ctx, FAM_CGS, (k_cgs_sweep3<false, G3>), dim3(G), G3::Threads, smem, *mx, *mb, *mb, w,
                          (const uint8_t *) ctx->d_flags[0], obst, L, box, c, ncx, ncy, ctx->d_partials, pred);
     ARTSS_LAUNCH_CK(ctx);
     *nb = G;
     return ARTSS_OK;
 }
+}  // extern "C++"
 
 // Variants of the TMA sweep: v < 3 the kernel with two barriers per plane step
 // and z-depth kStDepths[v]; 3 <= v < 6 the one-phase kernel with
-// kStDepths[v - 3]; v = 6 the row-pair kernel (kSweepRowPair); v >= 3 only
+// kStDepths[v - 3]; v = 6, 7 the row-pair kernel with 64 x 8 and 64 x 6 tiles; v >= 3 only
 // where the b / EV window starts at an even x.  Returns the number of blocks
 // (partials) in *nb.
 int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, const SweepMaps &m, double *w,
                      const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
-    if (v == kSweepRowPair) return launch_sweep3(ctx, turb, box, m, w, L, c, pred, nb);
+    if (v == kSweepRowPair) return launch_sweep3<S3Tall>(ctx, turb, 0, box, m.x, m.b2, m.e2, w, L, c, pred, nb);
+    if (v == kSweepRowPair + 1) return launch_sweep3<S3Flat>(ctx, turb, 1, box, m.x3, m.b3, m.e3, w, L, c, pred, nb);
     const int zb = kStDepths[v % 3];
     const dim3 g = sweep_tma_grid(box, zb);
     *nb = nblocks(g);
@@ -1420,9 +1513,10 @@ int set_sweep_smem(bool turb) {
     if (done[turb]) return ARTSS_OK;
     const int b1 = (int) sweep_tma_smem(turb), b2 = (int) sweep_tma2_smem(turb);
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    const int b3 = (int) sweep3_smem(turb);
+    const int b3 = (int) S3Tall::smem(turb), b4 = (int) S3Flat::smem(turb);
     if (turb) {
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true>, attr, b3));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true, S3Tall>, attr, b3));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true, S3Flat>, attr, b4));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, attr, b1));
@@ -1430,7 +1524,8 @@ int set_sweep_smem(bool turb) {
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 16>, attr, b2));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma2<true, 32>, attr, b2));
     } else {
-        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false>, attr, b3));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false, S3Tall>, attr, b3));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false, S3Flat>, attr, b4));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, attr, b1));
@@ -1466,7 +1561,7 @@ int tune_sweep(artss_ctx *ctx, bool turb, bool one_phase, const Box3 &box, const
     ARTSS_CK(cudaEventCreate(&e1));
     int best = fallback, st = ARTSS_OK, nb = 0;
     float best_ms = 1e30f;
-    for (int v = 0; v < (one_phase ? kSweepRowPair + 1 : 3) && !st; v++) {
+    for (int v = 0; v < (one_phase ? kSweepVariants : 3) && !st; v++) {
         if ((st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb))) break;  // warm
         cudaEventRecord(e0, ctx->stream);
         for (int r = 0; r < 3 && !st; r++) st = launch_sweep_tma(ctx, turb, v, box, m, w, L, c, pred, &nb);
@@ -1502,7 +1597,7 @@ int artss_ctx_pdl(artss_ctx *ctx, int enable) {
 
 int artss_ctx_sweep_variant(artss_ctx *ctx, int variant) {
     if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
-    if (variant < -1 || variant > kSweepRowPair) { set_error("sweep variant is -1 .. 6"); return ARTSS_ERR_ARG; }
+    if (variant < -1 || variant >= kSweepVariants) { set_error("sweep variant is -1 .. 7"); return ARTSS_ERR_ARG; }
     ctx->sweep_force = variant;
     return ARTSS_OK;
 }
@@ -1518,7 +1613,7 @@ int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent) {
     if (!ctx) return 0;
     const Level &L = ctx->lvl[0];
     auto it = ctx->tuned.find(TuneKey{0, L.Nx, L.Ny, L.Nz, turbulent ? 1 : 0});
-    return it == ctx->tuned.end() ? 0 : it->second == kSweepRowPair ? -1 : kStDepths[it->second % 3];
+    return it == ctx->tuned.end() ? 0 : it->second >= kSweepRowPair ? -1 : kStDepths[it->second % 3];
 }
 
 int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
@@ -1578,6 +1673,10 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
                 if ((st = tensor_map_3d(ctx, b, 0, &m.b2, kSt2BoxBX, kSt2BoxBY))) return st;
                 m.e2 = m.b2;
                 if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e2, kSt2BoxBX, kSt2BoxBY))) return st;
+                if ((st = tensor_map_3d(ctx, buf[r], 0, &m.x3, S3Flat::XW, S3Flat::XH))) return st;
+                if ((st = tensor_map_3d(ctx, b, 0, &m.b3, S3Flat::BW, S3Flat::BH))) return st;
+                m.e3 = m.b3;
+                if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e3, S3Flat::BW, S3Flat::BH))) return st;
             }
         }
     }
