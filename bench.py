@@ -46,6 +46,9 @@ def parse_args():
                     help="poisson: ms per pressure solve to a 1e-8 relative residual, plain FP64 VCycleMG "
                          "against the mixed-precision solve, on the 256^3 Neumann problem with box obstacles")
     ap.add_argument("--poisson-n", type=int, default=256)
+    ap.add_argument("--channel-nx", type=int, default=256,
+                    help="channel workload size nx x nx/2 x nx/2 (256: the benchmarked scene; smaller sizes for "
+                         "profiler captures)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
@@ -53,10 +56,11 @@ def parse_args():
     return ap.parse_args()
 
 
-def workload(name: str, steps: int):
+def workload(name: str, steps: int, nx: int = 256):
     from artss_b200 import scenes
     if name == "channel":
-        return "channel_256x128x128_cube_fp64", scenes.channel_with_cube(steps=steps)
+        return (f"channel_{nx}x{nx // 2}x{nx // 2}_cube_fp64",
+                scenes.channel_with_cube(nx=nx, ny=nx // 2, nz=nx // 2, steps=steps))
     return "box_64cubed_plume_fp64", scenes.plume_box(n=64, steps=steps, n_level=4)
 
 
@@ -205,7 +209,7 @@ def run_b200(args, dist):
 
     torch.cuda.set_device(dist.local)
     total_steps = args.warmup + 2 + 3 * args.steps + 2 * args.e2e_steps + 3 + 2
-    name, sc = workload(args.workload, total_steps)
+    name, sc = workload(args.workload, total_steps, args.channel_nx)
     tmp = tempfile.mkdtemp(prefix="artss_bench_")
     xml = scenes.write(sc, os.path.join(tmp, f"{name}_r{dist.rank}.xml"))
     sim = A.Simulation(xml, device=dist.local)
@@ -606,7 +610,7 @@ def cpu_baseline(args, inner):
     from tests import refdriver
     if not refdriver.available():
         return None
-    name, sc = workload(args.workload, args.cpu_steps)
+    name, sc = workload(args.workload, args.cpu_steps, args.channel_nx)
     tmp = tempfile.mkdtemp(prefix="artss_cpu_")
     from artss_b200 import scenes
     xml = scenes.write(sc, os.path.join(tmp, f"{name}_cpu.xml"))
@@ -622,7 +626,7 @@ def cpu_baseline(args, inner):
 def run_reference(args, dist):
     """--impl reference: the reference serial build, rank 0 only."""
     from tests import refdriver
-    name, sc = workload(args.workload, args.warmup + args.steps)
+    name, sc = workload(args.workload, args.warmup + args.steps, args.channel_nx)
     if not refdriver.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/artss_ref_driver is not built (make -C oracle ref)"}
     from artss_b200 import scenes
