@@ -149,6 +149,8 @@ def load_cuda() -> C.CDLL:
             "artss_projection": ([_P] + [_D] * 7, C.c_int),
             "artss_buoyancy_force": ([_P, _D, _D, _D, C.c_double, C.c_double], C.c_int),
             "artss_add_source": ([_P, _D, _D, C.c_double, C.c_int], C.c_int),
+            "artss_diffuse_explicit": ([_P, _D, _D, C.c_double, _D, C.c_double, C.c_int], C.c_int),
+            "artss_dissipate": ([_P, _D, _D, _D, _D, C.c_double, C.c_double, C.c_int], C.c_int),
             "artss_mg_create": ([_P, C.POINTER(MgCfg), C.POINTER(_P)], C.c_int),
             "artss_mg_destroy": ([_P], C.c_int),
             "artss_mg_pressure": ([_P, _D, _D, C.c_int, C.POINTER(MgStats)], C.c_int),
@@ -228,6 +230,12 @@ def load_host() -> C.CDLL:
             "artss_sim_finished": ([_P], C.c_int),
             "artss_sim_time": ([_P], C.c_double),
             "artss_sim_step_index": ([_P], C.c_int64),
+            "artss_sim_save": ([_P, C.c_char_p], C.c_int),
+            "artss_sim_write_dat": ([_P, C.c_char_p, C.c_char_p], C.c_int),
+            "artss_sim_write_vtk": ([_P, C.c_char_p], C.c_int),
+            "artss_sim_output_wait": ([_P], C.c_int),
+            "artss_sim_cfl": ([_P, C.POINTER(C.c_double)], C.c_int),
+            "artss_sim_restore": ([_P, C.c_char_p], C.c_int),
             "artss_sim_inner_cells": ([_P], C.c_int64),
             "artss_sim_get_field": ([_P, C.c_char_p, _D, C.c_int64], C.c_int),
             "artss_sim_set_field": ([_P, C.c_char_p, _D, C.c_int64], C.c_int),
@@ -344,6 +352,34 @@ class Simulation:
         done = C.c_int64()
         _host_check(self._lib.artss_sim_run(self._h, steps, C.byref(done)), "run")
         return done.value
+
+    def cfl(self) -> float:
+        """Analysis::calc_CFL of the current velocity (device max-reduction)."""
+        out = C.c_double()
+        _host_check(self._lib.artss_sim_cfl(self._h, C.byref(out)), "cfl")
+        return out.value
+
+    def write_dat(self, field: str, path: str) -> None:
+        """Queue Analysis::write_file of one field (written beside later steps)."""
+        _host_check(self._lib.artss_sim_write_dat(self._h, field.encode(), os.fsencode(path)), "write_dat")
+
+    def write_vtk(self, path: str) -> None:
+        """Queue VTKWriter::write_numerical (written beside later steps)."""
+        _host_check(self._lib.artss_sim_write_vtk(self._h, os.fsencode(path)), "write_vtk")
+
+    def output_wait(self) -> None:
+        """Every queued output file is written."""
+        _host_check(self._lib.artss_sim_output_wait(self._h), "output_wait")
+
+    def save(self, path: str) -> None:
+        """Checkpoint: every field, the step index and the time into one raw
+        file (artss_sim_save)."""
+        _host_check(self._lib.artss_sim_save(self._h, os.fsencode(path)), "save")
+
+    def restore(self, path: str) -> None:
+        """Rollback to a checkpoint of this scene (artss_sim_restore); the run
+        continues from the saved step."""
+        _host_check(self._lib.artss_sim_restore(self._h, os.fsencode(path)), "restore")
 
     def set_graphs(self, enable: bool = True) -> None:
         """Whole-step CUDA graphs: from the third step on each step is one

@@ -283,6 +283,13 @@ int artss_ctx_destroy(artss_ctx *ctx) {
         }
     }
     for (uint8_t *t : ctx->d_sweep3_obst) if (t) cudaFree(t);
+    if (ctx->rb_stream) cudaStreamSynchronize(ctx->rb_stream);
+    for (auto &r : ctx->rb) {
+        for (double *a : r.dev) cudaFree(a);
+        for (double *a : r.host) cudaFreeHost(a);
+        if (r.done) cudaEventDestroy(r.done);
+    }
+    if (ctx->rb_stream) cudaStreamDestroy(ctx->rb_stream);
     for (auto &m : ctx->prof.marks) cudaEventDestroy(m.first);
     for (auto &pe : ctx->prof.pending) cudaEventDestroy(pe.first);
     for (auto e : ctx->prof.events) cudaEventDestroy(e);
@@ -646,6 +653,87 @@ int artss_io_out(artss_ctx *ctx, int n_out, const double *const *fields, double 
         ARTSS_CK(cudaMemcpyAsync(host[k], ctx->io_stage_out[b][k], (size_t) n * sizeof(double), cudaMemcpyDeviceToHost,
                                  ctx->io_down));
     ARTSS_CK(cudaEventRecord(ctx->io_out_free[b], ctx->io_down));
+    return ARTSS_OK;
+}
+
+int artss_readback(artss_ctx *ctx, int n, const double *const *fields, int64_t count, int64_t *ticket) {
+    if (!ctx || n < 1 || count < 1 || !fields || !ticket) { set_error("bad readback arguments"); return ARTSS_ERR_ARG; }
+    for (int k = 0; k < n; k++)
+        if (!fields[k]) { set_error("null readback field"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("readback while a graph is captured"); return ARTSS_ERR_ARG; }
+    const int64_t t = ctx->rb_next;
+    artss_ctx::Readback &r = ctx->rb[t & 1];
+    {
+        // the slot's previous ticket (t - 2) must be released by its user
+        std::unique_lock<std::mutex> lock(ctx->rb_mutex);
+        ctx->rb_cv.wait(lock, [&] { return r.released; });
+    }
+    if (!ctx->rb_stream) ARTSS_CK(cudaStreamCreateWithFlags(&ctx->rb_stream, cudaStreamNonBlocking));
+    if (!r.done) ARTSS_CK(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+    ARTSS_CK(cudaEventSynchronize(r.done));  // the slot's previous copies are complete
+    if (r.count != count || (int) r.dev.size() < n) {
+        for (double *a : r.dev) cudaFree(a);
+        for (double *a : r.host) cudaFreeHost(a);
+        r.dev.clear();
+        r.host.clear();
+        r.count = count;
+    }
+    while ((int) r.dev.size() < n) {
+        double *d = nullptr, *h = nullptr;
+        ARTSS_CK(cudaMalloc(&d, (size_t) count * sizeof(double)));
+        ARTSS_CK(cudaMallocHost(&h, (size_t) count * sizeof(double)));
+        r.dev.push_back(d);
+        r.host.push_back(h);
+    }
+    // snapshot on the context stream (ordered after the work enqueued so far),
+    // device-to-host beside the context's later work
+    for (int k = 0; k < n; k++) {
+        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_copy, flat_blocks(count), 256, 0, r.dev[k], fields[k], count);
+        ARTSS_LAUNCH_CK(ctx);
+    }
+    cudaEvent_t snap = prof_event(ctx);
+    if (!snap) { set_error("cudaEventCreate failed"); return ARTSS_ERR_CUDA; }
+    ARTSS_CK(cudaEventRecord(snap, ctx->stream));
+    ARTSS_CK(cudaStreamWaitEvent(ctx->rb_stream, snap, 0));
+    ctx->prof.pool.push_back(snap);  // reusable once recorded and waited on
+    for (int k = 0; k < n; k++)
+        ARTSS_CK(cudaMemcpyAsync(r.host[k], r.dev[k], (size_t) count * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->rb_stream));
+    ARTSS_CK(cudaEventRecord(r.done, ctx->rb_stream));
+    {
+        std::lock_guard<std::mutex> lock(ctx->rb_mutex);
+        r.ticket = t;
+        r.released = false;
+    }
+    ctx->rb_next = t + 1;
+    *ticket = t;
+    return ARTSS_OK;
+}
+
+int artss_readback_wait(artss_ctx *ctx, int64_t ticket, const double **host, int n) {
+    if (!ctx || ticket < 0 || (n > 0 && !host)) { set_error("bad readback_wait arguments"); return ARTSS_ERR_ARG; }
+    artss_ctx::Readback &r = ctx->rb[ticket & 1];
+    cudaEvent_t done;
+    {
+        std::lock_guard<std::mutex> lock(ctx->rb_mutex);
+        if (r.ticket != ticket || r.released) { set_error("readback ticket not pending"); return ARTSS_ERR_STATE; }
+        if (n > (int) r.host.size()) { set_error("more arrays than the readback holds"); return ARTSS_ERR_ARG; }
+        done = r.done;
+        for (int k = 0; k < n; k++) host[k] = r.host[k];
+    }
+    ARTSS_CK(cudaEventSynchronize(done));
+    return ARTSS_OK;
+}
+
+int artss_readback_release(artss_ctx *ctx, int64_t ticket) {
+    if (!ctx || ticket < 0) { set_error("bad readback_release arguments"); return ARTSS_ERR_ARG; }
+    artss_ctx::Readback &r = ctx->rb[ticket & 1];
+    {
+        std::lock_guard<std::mutex> lock(ctx->rb_mutex);
+        if (r.ticket != ticket || r.released) { set_error("readback ticket not pending"); return ARTSS_ERR_STATE; }
+        r.released = true;
+    }
+    ctx->rb_cv.notify_all();
     return ARTSS_OK;
 }
 

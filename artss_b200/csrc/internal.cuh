@@ -7,7 +7,9 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <condition_variable>
 #include <map>
+#include <mutex>
 #include <utility>
 #include <string>
 #include <vector>
@@ -148,6 +150,20 @@ struct artss_ctx {
     // io_up, read-backs on io_down (one copy engine each), device staging
     cudaStream_t io_up = nullptr, io_down = nullptr;
     std::vector<double *> io_stage_in, io_stage_out[2];
+    // snapshot read-backs for output writers (artss_readback): per slot device
+    // staging, page-locked host copies, completion event; slot t % 2 of ticket t
+    struct Readback {
+        std::vector<double *> dev;
+        std::vector<double *> host;
+        int64_t count = 0;
+        cudaEvent_t done = nullptr;
+        int64_t ticket = -1;   // ticket occupying the slot
+        bool released = true;  // its user has finished with the host copies
+    } rb[2];
+    int64_t rb_next = 0;
+    cudaStream_t rb_stream = nullptr;
+    std::mutex rb_mutex;
+    std::condition_variable rb_cv;
     int64_t io_n = 0, io_calls = 0;
     cudaEvent_t io_in_ready = nullptr, io_in_free = nullptr, io_out_ready[2]{}, io_out_free[2]{};
     int64_t loop_hint[4][8] = {{1, 1, 1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1, 1, 1},

@@ -135,6 +135,91 @@ __global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict_
     }
 }
 
+// ExplicitDiffuse::ExplicitStep: laminar (ExplicitDiffuse.cpp:50-76, rd* = D / (d* d*)
+// on the host) and turbulent (:79-124: face viscosities 0.5 (EV_nb + EV) + D, no
+// division by the spacing, as the reference writes it); inner cells, same order
+template <bool TURB>
+__global__ void k_explicit_diffuse(double *__restrict__ out, const double *__restrict__ in,
+                                   const double *__restrict__ ev, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                                   double D, double dt, double rdx, double rdy, double rdz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int ni = 1, nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + nj * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        if (!TURB) {
+            out[q] = in[q] + dt * ((in[q + ni] - 2 * in[q] + in[q - ni]) * rdx + (in[q + nj] - 2 * in[q] + in[q - nj]) * rdy +
+                                   (in[q + nk] - 2 * in[q] + in[q - nk]) * rdz);
+        } else {
+            const double e0 = ev[q];
+            const double nu_x1 = 0.5 * (ev[q + ni] + e0) + D, nu_x2 = 0.5 * (ev[q - ni] + e0) + D;
+            const double nu_y1 = 0.5 * (ev[q + nj] + e0) + D, nu_y2 = 0.5 * (ev[q - nj] + e0) + D;
+            const double nu_z1 = 0.5 * (ev[q + nk] + e0) + D, nu_z2 = 0.5 * (ev[q - nk] + e0) + D;
+            const double c = in[q];
+            const double di0 = c - in[q - ni], di1 = in[q + ni] - c;
+            const double dj0 = c - in[q - nj], dj1 = in[q + nj] - c;
+            const double dk0 = c - in[q - nk], dk1 = in[q + nk] - c;
+            out[q] = c + dt * ((nu_x1 * di0 - nu_x2 * di1) + (nu_y1 * dj0 - nu_y2 * dj1) + (nu_z1 * dk0 - nu_z2 * dk1));
+        }
+    }
+}
+
+// ISource::dissipate (ISource.cpp:94-114): out += dt * nu * Phi on inner cells;
+// h* = 0.5 * (1 / d*) on the host (the reference's 0.5 * reciprocal_d*, the same
+// product), every sub-expression evaluated as the reference writes it
+__global__ void k_dissipate(double *__restrict__ out, const double *__restrict__ u, const double *__restrict__ v,
+                            const double *__restrict__ w, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                            double nu, double dt, double hx, double hy, double hz) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int ni = 1, nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + nj * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        const double ux = hx * (u[q + ni] - u[q - ni]), vy = hy * (v[q + nj] - v[q - nj]);
+        const double wz = hz * (w[q + nk] - w[q - nk]);
+        const double s12 = hx * (v[q + ni] - v[q - ni]) + hy * (u[q + nj] - u[q - nj]);
+        const double s23 = hy * (w[q + nj] - w[q - nj]) + hz * (v[q + nk] - v[q - nk]);
+        const double s31 = hz * (u[q + nk] - u[q - nk]) + hx * (w[q + ni] - w[q - ni]);
+        const double out_h = nu * (2 * ux * ux + 2 * vy * vy + 2 * wz * wz + s12 * s12 + s23 * s23 + s31 * s31);
+        out[q] += dt * out_h;
+    }
+}
+
+// Analysis::calc_CFL (Analysis.cpp:322-351): per block the largest
+// |u|/dx + |v|/dy + |w|/dz over inner cells; a maximum is exact in any order
+__global__ void k_cfl_max(const double *__restrict__ u, const double *__restrict__ v, const double *__restrict__ w,
+                          const uint8_t *__restrict__ flags, Level L, Box3 box, double dx, double dy, double dz,
+                          double *__restrict__ partials) {
+    __shared__ double sm[32];
+    double m = 0.0;  // C >= 0
+    const int i = (int) box.x0 + (int) (blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = (int) box.y0 + (int) (blockIdx.y * blockDim.y + threadIdx.y);
+    if (i <= (int) box.x1 && j <= (int) box.y1) {
+        const int nj = (int) L.Nx, nk = (int) L.nxy();
+        for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+            const int q = i + nj * j + nk * k;
+            if (!(flags[q] & kInner)) continue;
+            m = fmax(m, fabs(u[q]) / dx + fabs(v[q]) / dy + fabs(w[q]) / dz);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, lane = tid & 31, wid = tid >> 5;
+    if (lane == 0) sm[wid] = m;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+        m = lane < nw ? sm[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (lane == 0) partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = m;
+    }
+}
+
 // ------------------------------------------------------------ pressure coupling
 
 // IPressure.cpp:58-66; h* = 0.5 * (1/d*) (host)
@@ -1383,6 +1468,61 @@ int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const d
     ARTSS_LAUNCH_PDL(ctx, FAM_BUOYANCY, k_buoyancy, zgrid(box), box_block(), 0, force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
+}
+
+int artss_cfl(artss_ctx *ctx, const double *u, const double *v, const double *w, double dt, double *cfl) {
+    int st = check_field_args(ctx, {u, v, w, cfl});
+    if (st) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const dim3 g = zgrid(box);
+    if ((st = check_reduce_blocks(g))) return st;
+    const int nb = nblocks(g);
+    ARTSS_LAUNCH(ctx, FAM_REDUCE, k_cfl_max<<<g, box_block(), 0, ctx->stream>>>(
+                                      u, v, w, ctx->d_flags[0], L, box, ctx->grid.dx[0], ctx->grid.dy[0],
+                                      ctx->grid.dz[0], ctx->d_partials));
+    ARTSS_LAUNCH_CK(ctx);
+    std::vector<double> part((size_t) nb);
+    ARTSS_CK(cudaMemcpyAsync(part.data(), ctx->d_partials, (size_t) nb * sizeof(double), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    double m = 0.0;
+    for (double x : part) m = std::max(m, x);
+    *cfl = dt * m;
+    return ARTSS_OK;
+}
+
+int artss_diffuse_explicit(artss_ctx *ctx, double *out, const double *in, double D, const double *ev, double dt,
+                           int field_type) {
+    int st = check_field_args(ctx, {out, in});
+    if (st || (st = check_field_type(field_type))) return st;
+    if (out == in) { set_error("out and in must be distinct arrays"); return ARTSS_ERR_ARG; }
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
+    // ExplicitDiffuse.cpp:64-66 (laminar); the turbulent step uses D and EV only
+    const double rdx = D / (dx * dx), rdy = D / (dy * dy), rdz = D / (dz * dz);
+    if (ev)
+        ARTSS_LAUNCH_PDL(ctx, FAM_JACOBI, k_explicit_diffuse<true>, zgrid(box), box_block(), 0, out, in, ev,
+                         (const uint8_t *) ctx->d_flags[0], L, box, D, dt, rdx, rdy, rdz);
+    else
+        ARTSS_LAUNCH_PDL(ctx, FAM_JACOBI, k_explicit_diffuse<false>, zgrid(box), box_block(), 0, out, in,
+                         (const double *) nullptr, (const uint8_t *) ctx->d_flags[0], L, box, D, dt, rdx, rdy, rdz);
+    ARTSS_LAUNCH_CK(ctx);
+    return apply_bc(ctx, out, 0, field_type, nullptr);
+}
+
+int artss_dissipate(artss_ctx *ctx, double *out, const double *u, const double *v, const double *w, double nu,
+                    double dt, int field_type) {
+    int st = check_field_args(ctx, {out, u, v, w});
+    if (st || (st = check_field_type(field_type))) return st;
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const double hx = 0.5 * (1. / ctx->grid.dx[0]), hy = 0.5 * (1. / ctx->grid.dy[0]), hz = 0.5 * (1. / ctx->grid.dz[0]);
+    ARTSS_LAUNCH_PDL(ctx, FAM_ADD_SOURCE, k_dissipate, zgrid(box), box_block(), 0, out, u, v, w,
+                     (const uint8_t *) ctx->d_flags[0], L, box, nu, dt, hx, hy, hz);
+    ARTSS_LAUNCH_CK(ctx);
+    return apply_bc(ctx, out, 0, field_type, nullptr);
 }
 
 int artss_add_source(artss_ctx *ctx, double *out, const double *S, double dt, int field_type) {

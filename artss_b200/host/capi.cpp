@@ -1,10 +1,13 @@
 // extern "C" surface of the host runtime (include/artss_host.h).
+#include <cstring>
+#include <cstdio>
 #include "../../include/artss_host.h"
 
 #include <map>
 #include <memory>
 #include <string>
 
+#include "output.h"
 #include "solvers.h"
 
 using namespace artss;
@@ -19,6 +22,8 @@ struct artss_sim {
     std::unique_ptr<Runtime> rt;
     std::unique_ptr<SolverController> sc;
     std::unique_ptr<TimeIntegration> ti;
+    std::unique_ptr<OutputWriter> out;  // created by the first write
+    ~artss_sim() { out.reset(); }       // the writer's thread ends before the context goes
 };
 
 namespace {
@@ -254,6 +259,114 @@ int artss_sim_set_field(artss_sim *s, const char *name, const double *host, int6
         if (!f) throw std::invalid_argument(std::string("unknown field ") + name);
         if ((size_t) n != f->get_size()) throw std::invalid_argument("size mismatch");
         check(artss_upload(s->rt->ctx(), f->data, host, n), "set_field");
+        return ARTSS_OK;
+    });
+}
+
+// Checkpoint file: "ARTSSCKP", u32 version 1, u32 number of fields, i64 step,
+// f64 time, i64 Nx, Ny, Nz of level 0, then per field a 16-byte zero-padded
+// name, an i64 count and count little-endian doubles.
+static const char *const kCheckpointFields[] = {"u", "v", "w", "u0", "v0", "w0", "u_tmp", "v_tmp", "w_tmp", "nu_t",
+                                                "kappa_t", "p", "p0", "rhs", "T", "T0", "T_tmp", "T_a", "f_x", "f_y",
+                                                "f_z", "S_T"};
+
+int artss_sim_save(artss_sim *s, const char *path) {
+    return guarded([&] {
+        if (!s || !path) throw std::invalid_argument("null argument");
+        std::FILE *f = std::fopen(path, "wb");
+        if (!f) throw std::runtime_error(std::string("cannot write ") + path);
+        std::unique_ptr<std::FILE, int (*)(std::FILE *)> guard(f, std::fclose);
+        const GridLevel &L0 = s->rt->level(0);
+        const uint32_t version = 1, nf = (uint32_t) (sizeof(kCheckpointFields) / sizeof(*kCheckpointFields));
+        const int64_t step = s->ti->step_index(), dims[3] = {(int64_t) L0.N[0], (int64_t) L0.N[1], (int64_t) L0.N[2]};
+        const double t = s->ti->time();
+        bool ok = std::fwrite("ARTSSCKP", 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
+                  std::fwrite(&nf, 4, 1, f) == 1 && std::fwrite(&step, 8, 1, f) == 1 && std::fwrite(&t, 8, 1, f) == 1 &&
+                  std::fwrite(dims, 8, 3, f) == 3;
+        std::vector<double> host;
+        for (const char *name : kCheckpointFields) {
+            Field *fld = s->sc->fields().by_name(name);
+            const int64_t n = (int64_t) fld->get_size();
+            host.resize((size_t) n);
+            check(artss_download(s->rt->ctx(), host.data(), fld->data, n), "checkpoint");
+            char tag[16] = {};
+            std::strncpy(tag, name, sizeof(tag) - 1);
+            ok = ok && std::fwrite(tag, 1, 16, f) == 16 && std::fwrite(&n, 8, 1, f) == 1 &&
+                 std::fwrite(host.data(), 8, (size_t) n, f) == (size_t) n;
+        }
+        if (!ok) throw std::runtime_error(std::string("short write to ") + path);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_restore(artss_sim *s, const char *path) {
+    return guarded([&] {
+        if (!s || !path) throw std::invalid_argument("null argument");
+        std::FILE *f = std::fopen(path, "rb");
+        if (!f) throw std::runtime_error(std::string("cannot read ") + path);
+        std::unique_ptr<std::FILE, int (*)(std::FILE *)> guard(f, std::fclose);
+        char magic[8];
+        uint32_t version = 0, nf = 0;
+        int64_t step = 0, dims[3] = {};
+        double t = 0;
+        if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "ARTSSCKP", 8) != 0 || std::fread(&version, 4, 1, f) != 1 ||
+            version != 1 || std::fread(&nf, 4, 1, f) != 1 || std::fread(&step, 8, 1, f) != 1 ||
+            std::fread(&t, 8, 1, f) != 1 || std::fread(dims, 8, 3, f) != 3)
+            throw std::invalid_argument(std::string(path) + " is not an ARTSS checkpoint");
+        const GridLevel &L0 = s->rt->level(0);
+        if (dims[0] != (int64_t) L0.N[0] || dims[1] != (int64_t) L0.N[1] || dims[2] != (int64_t) L0.N[2])
+            throw std::invalid_argument("checkpoint grid differs from the scene's");
+        std::vector<double> host;
+        for (uint32_t q = 0; q < nf; q++) {
+            char tag[17] = {};
+            int64_t n = 0;
+            if (std::fread(tag, 1, 16, f) != 16 || std::fread(&n, 8, 1, f) != 1)
+                throw std::invalid_argument("truncated checkpoint");
+            Field *fld = s->sc->fields().by_name(tag);
+            if (!fld || (size_t) n != fld->get_size()) throw std::invalid_argument(std::string("checkpoint field ") + tag);
+            host.resize((size_t) n);
+            if (std::fread(host.data(), 8, (size_t) n, f) != (size_t) n) throw std::invalid_argument("truncated checkpoint");
+            check(artss_upload(s->rt->ctx(), fld->data, host.data(), n), "restore");
+        }
+        s->ti->set_step(step);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_write_dat(artss_sim *s, const char *field, const char *path) {
+    return guarded([&] {
+        if (!s || !field || !path) throw std::invalid_argument("null argument");
+        Field *f = s->sc->fields().by_name(field);
+        if (!f) throw std::invalid_argument(std::string("unknown field ") + field);
+        if (!s->out) s->out = std::make_unique<OutputWriter>(*s->rt);
+        s->out->write_dat(*f, path);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_write_vtk(artss_sim *s, const char *path) {
+    return guarded([&] {
+        if (!s || !path) throw std::invalid_argument("null argument");
+        FieldController &fc = s->sc->fields();
+        if (!s->out) s->out = std::make_unique<OutputWriter>(*s->rt);
+        s->out->write_vtk({&fc.u, &fc.v, &fc.w, &fc.p, &fc.rhs, &fc.T, &fc.nu_t, &fc.S_T}, path);
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_output_wait(artss_sim *s) {
+    return guarded([&] {
+        if (!s) throw std::invalid_argument("null simulation");
+        if (s->out) s->out->wait();
+        return ARTSS_OK;
+    });
+}
+
+int artss_sim_cfl(artss_sim *s, double *cfl) {
+    return guarded([&] {
+        if (!s || !cfl) throw std::invalid_argument("null argument");
+        FieldController &fc = s->sc->fields();
+        check(artss_cfl(s->rt->ctx(), fc.u.data, fc.v.data, fc.w.data, s->rt->dt(), cfl), "cfl");
         return ARTSS_OK;
     });
 }

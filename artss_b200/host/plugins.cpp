@@ -63,6 +63,18 @@ void ColoredGaussSeidelDiffuse::diffuse(Field &out, const Field &in, const Field
     run(out, in, b, D, &ev);
 }
 
+void ExplicitDiffuse::diffuse(Field &out, const Field &in, const Field &, real D, bool) {
+    check(artss_diffuse_explicit(m_rt.ctx(), out.data, in.data, D, nullptr, m_rt.dt(), out.get_type()),
+          "ExplicitDiffuse::diffuse");
+    last_iterations = 1;
+}
+
+void ExplicitDiffuse::diffuse(Field &out, const Field &in, const Field &, real D, const Field &ev, bool) {
+    check(artss_diffuse_explicit(m_rt.ctx(), out.data, in.data, D, ev.data, m_rt.dt(), out.get_type()),
+          "ExplicitDiffuse::diffuse");
+    last_iterations = 1;
+}
+
 void JacobiDiffuse::run(Field &out, const Field &in, const Field &b, real D, const Field *ev) {
     artss_iter_cfg cfg{(int64_t) m_settings.max_iter, m_settings.tol_res, m_settings.w};
     artss_iter_stats st{};
@@ -154,6 +166,13 @@ void ExplicitEulerSource::add_source(Field &out_x, Field &out_y, Field &out_z, c
         check(artss_add_source(m_rt.ctx(), outs[a]->data, srcs[a]->data, m_rt.dt(), outs[a]->get_type()),
               "ExplicitEulerSource::add_source");
     }
+}
+
+void ExplicitEulerSource::dissipate(Field &out, const Field &in_u, const Field &in_v, const Field &in_w, bool) {
+    const auto &phys = m_rt.settings().physical;
+    check(artss_dissipate(m_rt.ctx(), out.data, in_u.data, in_v.data, in_w.data, phys.nu.value(), m_rt.dt(),
+                          out.get_type()),
+          "ISource::dissipate");
 }
 
 void ExplicitEulerSource::add_source(Field &out, const Field &S, bool) {

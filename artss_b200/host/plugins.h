@@ -64,6 +64,8 @@ class ISource {
                             const Field &S_z, bool sync) = 0;
     virtual void add_source(Field &out, const Field &S, bool sync) = 0;
     static void buoyancy_force(Field &out, const Field &in, const Field &in_a, bool sync = true);
+    // viscous dissipation into out (ISource::dissipate, src/interfaces/ISource.cpp:63-123)
+    virtual void dissipate(Field &out, const Field &in_u, const Field &in_v, const Field &in_w, bool sync) = 0;
 };
 
 // ISourceFunction (src/interfaces/ISourceFunction.h:14-29)
@@ -99,6 +101,17 @@ class ColoredGaussSeidelDiffuse : public IDiffusion {
     void run(Field &out, const Field &in, const Field &b, real D, const Field *ev);
     Runtime &m_rt;
     settings::Diffusion m_settings;
+};
+
+// ExplicitDiffuse (src/diffusion/ExplicitDiffuse.cpp:27-127): one explicit step per call
+class ExplicitDiffuse : public IDiffusion {
+ public:
+    explicit ExplicitDiffuse(Runtime &rt) : m_rt(rt) {}
+    void diffuse(Field &out, const Field &in, const Field &b, real D, bool sync) override;
+    void diffuse(Field &out, const Field &in, const Field &b, real D, const Field &ev, bool sync) override;
+
+ private:
+    Runtime &m_rt;
 };
 
 class JacobiDiffuse : public IDiffusion {
@@ -158,6 +171,7 @@ class ExplicitEulerSource : public ISource {
     void add_source(Field &out_x, Field &out_y, Field &out_z, const Field &S_x, const Field &S_y, const Field &S_z,
                     bool sync) override;
     void add_source(Field &out, const Field &S, bool sync) override;
+    void dissipate(Field &out, const Field &in_u, const Field &in_v, const Field &in_w, bool sync) override;
 
  private:
     Runtime &m_rt;

@@ -15,6 +15,7 @@ std::unique_ptr<IAdvection> make_advection(Runtime &rt, const settings::Advectio
 std::unique_ptr<IDiffusion> make_diffusion(Runtime &rt, const settings::Diffusion &s) {
     if (s.type == "ColoredGaussSeidel") return std::make_unique<ColoredGaussSeidelDiffuse>(rt, s);
     if (s.type == "Jacobi") return std::make_unique<JacobiDiffuse>(rt, s);
+    if (s.type == "Explicit") return std::make_unique<ExplicitDiffuse>(rt);
     throw config_error("diffusion method '" + s.type + "' is not implemented");
 }
 
@@ -148,8 +149,7 @@ NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbul
         s.temperature.advection.fields != std::vector<int>{F_T} ||
         s.temperature.diffusion.fields != std::vector<int>{F_T} || s.pressure.field != F_P)
         throw config_error("Fields not specified correctly!");
-    if (s.temperature.source.dissipation)
-        throw config_error("temperature dissipation is not part of the fractional-step path implemented here");
+    m_dissipation = s.temperature.source.dissipation;
     // `in` of every diffuse() call below is re-coupled before it is read again,
     // and out and in are coupled from one field just before each call
     dif_vel->in_is_scratch = true;
@@ -239,6 +239,9 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
         dif_temp->diffuse(f.T, f.T0, f.T_tmp, kappa, sync);
         stats.diffusion_iterations[3] = dif_temp->last_iterations;
     }
+    // dissipation then the source (NSTempTurbSolver.cpp:220-240, NSTempSolver.cpp:168-190); the couple
+    // after each writes T0 and T_tmp, which update_data rewrites before anything reads them
+    if (m_dissipation) sou_temp->dissipate(f.T, f.u, f.v, f.w, sync);
     if (m_add_temp_source) sou_temp->add_source(f.T, f.S_T, sync);
 }
 
@@ -580,6 +583,12 @@ TimeIntegration::TimeIntegration(Runtime &rt, SolverController &sc)
     : m_rt(rt), m_sc(sc), m_dt(rt.settings().physical.dt), m_t_end(rt.settings().physical.t_end), m_t_cur(m_dt) {}
 
 bool TimeIntegration::finished() const { return !(m_t_cur < m_t_end + m_dt / 2); }
+
+void TimeIntegration::set_step(int64_t step) {
+    if (step < 1) throw std::invalid_argument("step index starts at 1");
+    m_step = step;
+    m_t_cur = (real) m_step * m_dt;  // as run() advances it
+}
 
 void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>> &in,
                               const std::vector<std::pair<Field *, real *>> &out) {

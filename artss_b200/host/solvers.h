@@ -74,7 +74,7 @@ class NSTempTurbSolver : public ISolver {
     std::unique_ptr<IPressure> pres;
     std::unique_ptr<ISource> sou_vel, sou_temp;
     std::unique_ptr<ISourceFunction> m_source_function_temperature;
-    bool m_add_source = false, m_add_temp_source = false;
+    bool m_add_source = false, m_add_temp_source = false, m_dissipation = false;
 };
 
 // NSSolver / NSTurbSolver (src/solver/NSSolver.cpp, NSTurbSolver.cpp)
@@ -173,6 +173,8 @@ class TimeIntegration {
     real time() const { return m_t_cur; }
     int64_t step_index() const { return m_step; }
     bool finished() const;
+    // continue from step `step` (its time is step * dt), e.g. after a rollback
+    void set_step(int64_t step);
 
  private:
     // the step as one graph (Runtime::graphs): captured at step kGraphStep,

@@ -81,6 +81,7 @@ class Scene:
     ic_params: dict = field(default_factory=dict)  # parameters of ExpSinusProd / GaussBubble / Hat / ...
     force: str = "Buoyancy"  # momentum source force_fct: Buoyancy, Uniform or Zero
     force_value: Tuple[float, float, float] = (0.0, 0.0, 0.0)  # Uniform: val_x, val_y, val_z
+    dissipation: bool = False  # temperature source: viscous dissipation (ISource::dissipate)
 
     @property
     def t_end(self) -> float:
@@ -265,6 +266,18 @@ def velocity_scene(solver: str, n: int = 32, steps: int = 5, diffusion: str = "J
     return Scene(**base)
 
 
+def pressure_scene(n: int = 32, n_level: int = 4, steps: int = 2, **kw) -> Scene:
+    """PressureSolver scene of the reference's tests/pressure family: a 2 m cube,
+    n^3 cells, Dirichlet p = 0 on every wall, rhs = sin(l pi x) sin(l pi y)
+    sin(l pi z) with l = 2 (SinSinSin), VCycleMG V(4,4) to 1e-7."""
+    base = dict(solver="PressureSolver", nx=n, ny=n, nz=n, X=(0.0, 2.0), Y=(0.0, 2.0), Z=(0.0, 2.0), dt=0.1,
+                steps=steps, n_level=n_level, max_cycle=100, mg_tol=1e-7, n_relax=4, smoother_max_iter=100,
+                smoother_tol=1e-7, boundaries=[("p", "front,back,left,right,bottom,top", "dirichlet", 0.0)],
+                noise=False, ic="SinSinSin", ic_params={"l": 2.0})
+    base.update(kw)
+    return Scene(**base)
+
+
 NS_SOLVERS = ("NSSolver", "NSTurbSolver")
 
 
@@ -412,7 +425,8 @@ def to_xml(s: Scene) -> str:
             a('      <turbulence include="Yes">')
             a(f"        <Pr_T> {_f(s.pr_t)} </Pr_T>")
             a("      </turbulence>")
-        a(f'      <source type="ExplicitEuler" dir="{s.buoyancy_dir}" temp_fct="Gauss" dissipation="No" random="No">')
+        a(f'      <source type="ExplicitEuler" dir="{s.buoyancy_dir}" temp_fct="Gauss" '
+          f'dissipation="{"Yes" if s.dissipation else "No"}" random="No">')
         a(f"        <HRR> {_f(s.hrr)} </HRR>")
         a(f"        <cp> {_f(s.cp)} </cp>")
         a(f"        <x0> {_f(s.source_pos[0])} </x0>")

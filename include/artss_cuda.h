@@ -211,6 +211,21 @@ int artss_copy_join(artss_ctx *ctx);
  * host beside later work.  The k-th artss_io_out returns once the (k-2)-th
  * has completed: host arrays given to call pair k-2 may then be reused.
  * artss_io_sync waits for every transfer and for the context's work. */
+/* Snapshot read-back for output writers (no counterpart in the reference,
+ * whose writers read host mirrors updated by OpenACC): the values of the n
+ * `fields` (count doubles each) as of the work enqueued so far are copied into
+ * device staging on the context stream and from there, on a copy stream, into
+ * page-locked host arrays of the library, beside the context's later work.
+ * *ticket identifies the read-back.  artss_readback_wait (callable from
+ * another thread) blocks until the copies are on the host and hands out the
+ * arrays; artss_readback_release gives them back.  Two read-backs can be in
+ * flight: the next call waits until the ticket two before it is released. */
+int artss_readback(artss_ctx *ctx, int n, const double *const *fields, int64_t count, int64_t *ticket);
+int artss_readback_wait(artss_ctx *ctx, int64_t ticket, const double **host, int n);
+int artss_readback_release(artss_ctx *ctx, int64_t ticket);
+/* Analysis::calc_CFL (src/analysis/Analysis.cpp:322-351): dt * max over inner
+ * cells of |u|/dx + |v|/dy + |w|/dz; synchronizes the stream. */
+int artss_cfl(artss_ctx *ctx, const double *u, const double *v, const double *w, double dt, double *cfl);
 int artss_io_in(artss_ctx *ctx, int n_in, double *const *fields, const double *const *host, int64_t n);
 int artss_io_out(artss_ctx *ctx, int n_out, const double *const *fields, double *const *host, int64_t n);
 int artss_io_sync(artss_ctx *ctx);
@@ -333,6 +348,18 @@ int artss_ctx_sweep_variant(artss_ctx *ctx, int variant);
 int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b,
                          double D, const double *ev, double dt, int field_type,
                          const artss_iter_cfg *cfg, artss_iter_stats *stats);
+
+/* IDiffusion::diffuse, ExplicitDiffuse (src/diffusion/ExplicitDiffuse.cpp:27-127):
+ * one explicit Euler step out = in + dt * (D Laplacian(in)) on inner cells
+ * (ev != NULL: the reference's turbulent form with face viscosities
+ * 0.5 (EV_nb + EV) + D), then the boundary program of field_type on out. */
+int artss_diffuse_explicit(artss_ctx *ctx, double *out, const double *in, double D, const double *ev, double dt,
+                           int field_type);
+/* ISource::dissipate (src/interfaces/ISource.cpp:63-123): out += dt * nu *
+ * Phi(u, v, w) (viscous dissipation) on inner cells, then the boundary
+ * program of field_type. */
+int artss_dissipate(artss_ctx *ctx, double *out, const double *u, const double *v, const double *w, double nu,
+                    double dt, int field_type);
 
 /* IPressure::divergence (src/interfaces/IPressure.cpp:20-110): rhs on inner
  * cells and zero on the computational domain's ghost ring. */

@@ -90,6 +90,29 @@ artss_ctx *artss_sim_context(artss_sim *s);
 /* per-step statistics of the last step: iterations of the u, v, w, T
  * diffusion solves, V-cycles and (first step) residual of the pressure solve */
 int artss_sim_last_stats(artss_sim *s, int64_t *diff_iters4, int64_t *mg_cycles, double *mg_residual);
+/* Checkpoint and rollback (the reference keeps data-assimilation checkpoints in
+ * HDF5, src/dataAssimilation/FieldIO.cpp:44-100, absent here): every field of
+ * the simulation, the step index and the time in one raw file (magic
+ * "ARTSSCKP", little-endian FP64 arrays).  After artss_sim_restore the run
+ * continues from the saved step and its fields equal those of the
+ * uninterrupted run. */
+int artss_sim_save(artss_sim *s, const char *path);
+int artss_sim_restore(artss_sim *s, const char *path);
+/* Output of the time loop (src/analysis/Analysis.cpp:360-390,
+ * src/visualisation/VTKWriter.cpp:60-106): the fields' values as of the steps
+ * run so far leave the device by a snapshot read-back beside the next steps,
+ * and a worker thread writes the file.  write_dat: one field, every level-0
+ * cell, one value per line in the default stream format (Analysis::write_file);
+ * write_vtk: the legacy binary VTK rectilinear grid of VTKWriter::write_numerical
+ * (u, v, w, p, rhs as divergence, T, concentration 0, sight, nu_t, S_T and the
+ * cell centres).  output_wait returns once every queued file is written (the
+ * first failure as its status). */
+int artss_sim_write_dat(artss_sim *s, const char *field, const char *path);
+int artss_sim_write_vtk(artss_sim *s, const char *path);
+int artss_sim_output_wait(artss_sim *s);
+/* Analysis::calc_CFL (src/analysis/Analysis.cpp:322-351) of the current
+ * velocity, reduced on the device */
+int artss_sim_cfl(artss_sim *s, double *cfl);
 /* one pressure solve of a PressureSolver scene with the current p and rhs */
 int artss_sim_pressure(artss_sim *s, int first_step, int64_t *cycles, double *residual);
 /* the multigrid solver of a PressureSolver scene, or NULL */

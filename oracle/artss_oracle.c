@@ -153,6 +153,52 @@ void oracle_add_source(const oracle_scene *s, double *out, const double *S, doub
     oracle_apply_bc(s, out, 0, ft);
 }
 
+/* ExplicitDiffuse::ExplicitStep (src/diffusion/ExplicitDiffuse.cpp:50-76, laminar;
+ * :79-124, turbulent: face viscosities from EV, no division by the spacing,
+ * as the reference writes it) + DomainController::apply_boundary (:28, :45) */
+void oracle_diffuse_explicit(const oracle_scene *s, double *out, const double *in, double D, const double *ev,
+                             double dt, int ft) {
+    const int64_t ni = 1, nj = s->Nx[0], nk = s->Nx[0] * s->Ny[0];
+    const double rdx = D / (s->dx[0] * s->dx[0]), rdy = D / (s->dy[0] * s->dy[0]), rdz = D / (s->dz[0] * s->dz[0]);
+    for (int64_t l = 0; l < s->n_inner[0]; l++) {
+        const int64_t q = s->inner[0][l];
+        if (!ev) {
+            out[q] = in[q] + dt * ((in[q + ni] - 2 * in[q] + in[q - ni]) * rdx + (in[q + nj] - 2 * in[q] + in[q - nj]) * rdy +
+                                   (in[q + nk] - 2 * in[q] + in[q - nk]) * rdz);
+        } else {
+            const double nu_x1 = 0.5 * (ev[q + ni] + ev[q]) + D, nu_x2 = 0.5 * (ev[q - ni] + ev[q]) + D;
+            const double nu_y1 = 0.5 * (ev[q + nj] + ev[q]) + D, nu_y2 = 0.5 * (ev[q - nj] + ev[q]) + D;
+            const double nu_z1 = 0.5 * (ev[q + nk] + ev[q]) + D, nu_z2 = 0.5 * (ev[q - nk] + ev[q]) + D;
+            const double di0 = in[q] - in[q - ni], di1 = in[q + ni] - in[q];
+            const double dj0 = in[q] - in[q - nj], dj1 = in[q + nj] - in[q];
+            const double dk0 = in[q] - in[q - nk], dk1 = in[q + nk] - in[q];
+            out[q] = in[q] + dt * ((nu_x1 * di0 - nu_x2 * di1) + (nu_y1 * dj0 - nu_y2 * dj1) + (nu_z1 * dk0 - nu_z2 * dk1));
+        }
+    }
+    oracle_apply_bc(s, out, 0, ft);
+}
+
+/* ISource::dissipate (src/interfaces/ISource.cpp:63-123) */
+void oracle_dissipate(const oracle_scene *s, double *out, const double *u, const double *v, const double *w,
+                      double nu, double dt, int ft) {
+    const int64_t ni = 1, nj = s->Nx[0], nk = s->Nx[0] * s->Ny[0];
+    const double rdx = 1. / s->dx[0], rdy = 1. / s->dy[0], rdz = 1. / s->dz[0];
+    for (int64_t l = 0; l < s->n_inner[0]; l++) {
+        const int64_t i = s->inner[0][l];
+        const double out_h = nu * (2 * (0.5 * rdx * (u[i + ni] - u[i - ni])) * (0.5 * rdx * (u[i + ni] - u[i - ni])) +
+                                   2 * (0.5 * rdy * (v[i + nj] - v[i - nj])) * (0.5 * rdy * (v[i + nj] - v[i - nj])) +
+                                   2 * (0.5 * rdz * (w[i + nk] - w[i - nk])) * (0.5 * rdz * (w[i + nk] - w[i - nk])) +
+                                   ((0.5 * rdx * (v[i + ni] - v[i - ni])) + (0.5 * rdy * (u[i + nj] - u[i - nj]))) *
+                                       ((0.5 * rdx * (v[i + ni] - v[i - ni])) + (0.5 * rdy * (u[i + nj] - u[i - nj]))) +
+                                   ((0.5 * rdy * (w[i + nj] - w[i - nj])) + (0.5 * rdz * (v[i + nk] - v[i - nk]))) *
+                                       ((0.5 * rdy * (w[i + nj] - w[i - nj])) + (0.5 * rdz * (v[i + nk] - v[i - nk]))) +
+                                   ((0.5 * rdz * (u[i + nk] - u[i - nk])) + (0.5 * rdx * (w[i + ni] - w[i - ni]))) *
+                                       ((0.5 * rdz * (u[i + nk] - u[i - nk])) + (0.5 * rdx * (w[i + ni] - w[i - ni]))));
+        out[i] += dt * out_h;
+    }
+    oracle_apply_bc(s, out, 0, ft);
+}
+
 /* ------------------------------------------------------------------ diffusion */
 
 static void parity(const oracle_scene *s, int level, int64_t idx, int *color) {

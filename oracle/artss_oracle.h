@@ -70,6 +70,16 @@ void oracle_projection(const oracle_scene *s, double *u, double *v, double *w, c
 void oracle_buoyancy(const oracle_scene *s, double *f, const double *T, const double *Ta, double beta, double g);
 void oracle_add_source(const oracle_scene *s, double *out, const double *S, double dt, int field_type);
 
+/* ExplicitDiffuse::diffuse (src/diffusion/ExplicitDiffuse.cpp:27-127): one
+ * explicit step out = in + dt * (...) on inner cells, then the boundary
+ * program; ev == NULL: laminar. */
+void oracle_diffuse_explicit(const oracle_scene *s, double *out, const double *in, double D, const double *ev,
+                             double dt, int field_type);
+/* ISource::dissipate (src/interfaces/ISource.cpp:63-123): out += dt * nu * Phi
+ * on inner cells, then the boundary program of field_type. */
+void oracle_dissipate(const oracle_scene *s, double *out, const double *u, const double *v, const double *w,
+                      double nu, double dt, int field_type);
+
 /* IDiffusion::diffuse; ev == NULL: laminar.  Returns iterations. */
 int64_t oracle_diffuse_cgs(const oracle_scene *s, double *out, double *in, const double *b, double D,
                            const double *ev, double dt, int field_type, int64_t max_iter, double tol, double w,

@@ -12,6 +12,9 @@
 //   artss_ref_driver <file.xml> [--steps N] [--dump DIR] [--every K]
 //                    [--lists] [--time] [--mg-rhs rhs.f64 --mg-rel-tol TOL]
 //                    [--fields u,v,w,...]   (dump only these fields)
+//                    [--vtk PREFIX] [--dat FIELD:PATH] [--cfl]
+//                    (after the steps: VTKWriter::write_numerical to PREFIX.vtk,
+//                     Analysis::write_file of one field, Analysis::calc_CFL printed)
 //
 // Dump layout (all little-endian, raw):
 //   DIR/meta.txt                       grid sizes per level, dt, steps
@@ -63,6 +66,9 @@
 #include "src/solver/SolverSelection.h"
 #include "src/solver/NSTempTurbSolver.h"
 #include "src/source/GaussFunction.h"
+#include "src/analysis/Analysis.h"
+#include "src/analysis/Solution.h"
+#include "src/visualisation/VTKWriter.h"
 #undef private
 #undef protected
 
@@ -218,7 +224,8 @@ int main(int argc, char **argv) {
     std::string dump_dir;
     long every = 1;
     bool lists = false, timing = false;
-    std::string mg_rhs;
+    std::string mg_rhs, vtk_prefix, dat_spec;
+    bool print_cfl = false;
     double mg_rel_tol = 1e-8;
     long mg_max_cycles = 1000;
     for (int a = 2; a < argc; a++) {
@@ -236,6 +243,9 @@ int main(int argc, char **argv) {
         else if (k == "--mg-rel-tol") mg_rel_tol = std::stod(next());
         else if (k == "--mg-max-cycles") mg_max_cycles = std::stol(next());
         else if (k == "--fields") g_dump_only = next();
+        else if (k == "--vtk") vtk_prefix = next();
+        else if (k == "--dat") dat_spec = next();
+        else if (k == "--cfl") print_cfl = true;
         else { std::fprintf(stderr, "unknown option %s\n", k.c_str()); return 1; }
     }
     if (!dump_dir.empty()) make_dir(dump_dir);
@@ -318,6 +328,20 @@ int main(int argc, char **argv) {
         }
         auto loop1 = std::chrono::steady_clock::now();
         const long steps_run = step - 1;
+        if (!vtk_prefix.empty()) VTKWriter::write_numerical(*fc, vtk_prefix);
+        if (!dat_spec.empty() || print_cfl) {
+            Solution solution(settings.initial_conditions_parameters, settings.solver_parameters.solution);
+            Analysis analysis(settings.solver_parameters.solution, settings.visualisation_parameters, solution);
+            if (!dat_spec.empty()) {
+                const size_t colon = dat_spec.find(':');
+                const std::string name = dat_spec.substr(0, colon), path = dat_spec.substr(colon + 1);
+                for (auto &nf : all_fields(fc))
+                    if (name == nf.name) analysis.write_file(*nf.f, path);  // appends ".dat"
+            }
+            if (print_cfl)
+                std::printf("{\"cfl\": %.17g}\n", analysis.calc_CFL(fc->get_field_u(), fc->get_field_v(),
+                                                                     fc->get_field_w(), dt));
+        }
         if (!dump_dir.empty()) write_meta(dump_dir, (size_t) steps_run);
         if (timing) {
             const size_t inner = DomainController::getInstance()->get_size_domain_inner_list_level_joined(0);

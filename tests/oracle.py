@@ -59,6 +59,8 @@ def lib():
             "oracle_projection": [S, _D, _D, _D, _D, _D, _D, _D],
             "oracle_buoyancy": [S, _D, _D, _D, C.c_double, C.c_double],
             "oracle_add_source": [S, _D, _D, C.c_double, C.c_int],
+            "oracle_diffuse_explicit": [S, _D, _D, C.c_double, _D, C.c_double, C.c_int],
+            "oracle_dissipate": [S, _D, _D, _D, _D, C.c_double, C.c_double, C.c_int],
         }
         for fn, a in sig.items():
             getattr(L, fn).argtypes = a

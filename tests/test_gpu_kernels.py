@@ -269,6 +269,35 @@ def test_cgs_odd_pitch(tmp_path, turbulent):
         ctx.close()
 
 
+@pytest.mark.parametrize("turbulent", [False, True])
+def test_explicit_diffusion(env, turbulent):
+    """ExplicitDiffuse (laminar and the reference's turbulent form) + the
+    boundary program, against the oracle, bit for bit."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    out0, in0, ev = rnd(111, n, 290, 300), rnd(112, n, 290, 300), rnd(113, n, 0, 1e-3)
+    dout, din, dev = ctx.field(out0), ctx.field(in0), ctx.field(ev)
+    A.cuda_check(ctx.lib.artss_diffuse_explicit(ctx.h, dout, din, 3.1e-5, dev if turbulent else None, sc.dt,
+                                                FT["v"]), "explicit")
+    ref = out0.copy()
+    oracle.lib().oracle_diffuse_explicit(osc.ptr, P(ref), P(in0), 3.1e-5, P(ev) if turbulent else None, sc.dt, FT["v"])
+    assert np.array_equal(ctx.download(dout), ref)
+    assert np.array_equal(ctx.download(din), in0)
+
+
+def test_dissipate(env):
+    """ISource::dissipate (viscous heating of T from u, v, w) + the boundary
+    program, against the oracle, bit for bit."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    T, u, v, w = rnd(121, n, 290, 300), rnd(122, n), rnd(123, n), rnd(124, n)
+    dT, du, dv, dw = ctx.field(T), ctx.field(u), ctx.field(v), ctx.field(w)
+    A.cuda_check(ctx.lib.artss_dissipate(ctx.h, dT, du, dv, dw, 3.1e-5, sc.dt, FT["T"]), "dissipate")
+    ref = T.copy()
+    oracle.lib().oracle_dissipate(osc.ptr, P(ref), P(u), P(v), P(w), 3.1e-5, sc.dt, FT["T"])
+    assert np.array_equal(ctx.download(dT), ref)
+
+
 def _sweep_scenes():
     """a channel with a cube (obstacle planes take the flag path of the
     row-pair sweep); odd sizes with a box that touches the x-y edges of the

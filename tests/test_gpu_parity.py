@@ -50,6 +50,15 @@ def _scenes():
         "ns_channel": scenes.ns_scene("channel", n=32, steps=4),
         "nsturb_vortex": scenes.ns_scene("vortex", "NSTurbSolver", n=32, steps=4),
         "nsturb_cavity_cgs": scenes.ns_scene("cavity", "NSTurbSolver", n=32, steps=3, diffusion="ColoredGaussSeidel"),
+        # ExplicitDiffuse (src/diffusion/ExplicitDiffuse.cpp) and the temperature's viscous
+        # dissipation (ISource::dissipate, src/interfaces/ISource.cpp:63-123)
+        "diffusion_explicit": scenes.velocity_scene("DiffusionSolver", n=32, steps=4, diffusion="Explicit"),
+        "diffusion_turb_explicit": scenes.velocity_scene("DiffusionTurbSolver", n=32, steps=4, diffusion="Explicit"),
+        "nstemp_dissipation": scenes.plume_box(n=32, steps=3, n_level=3, solver="NSTempSolver", dissipation=True),
+        "nstempturb_explicit_dissipation": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=3, n_level=3,
+                                                                    diffusion="Explicit", dissipation=True),
+        # PressureSolver (src/solver/PressureSolver.cpp:30-43) on the SinSinSin right-hand side
+        "pressure_sinsinsin": scenes.pressure_scene(n=32, n_level=4, steps=2),
     }
 
 
