@@ -109,7 +109,8 @@ void put_be(std::FILE *f, float v) {
 }  // namespace
 
 // The legacy VTK layout of a rectilinear grid with cell data: the first cell
-// scalar as SCALARS, the others as one FIELD block, big-endian floats.
+// scalar as SCALARS, the others as one FIELD block, big-endian floats, then an
+// empty point-data section.
 void OutputWriter::write_vtk_file(const Job &job, const double *const *host) {
     const GridLevel &g = m_rt.level(0);
     const auto &X1 = m_rt.geometry().grid().start_pd;
@@ -156,6 +157,8 @@ void OutputWriter::write_vtk_file(const Job &job, const double *const *host) {
         for (size_t q = 0; q < n; q++)
             put_be(f, src[v] >= 0 ? static_cast<float>(host[src[v]][q]) : src[v] == -2 ? m_sight[q] : 0.0f);
     }
+    // the (empty) point-data section that closes the file
+    std::fprintf(f, "POINT_DATA %d\n", (Nx + 1) * (Ny + 1) * (Nz + 1));
     if (std::ferror(f)) throw std::runtime_error("cannot write " + path);
 }
 
