@@ -145,6 +145,8 @@ def load_cuda() -> C.CDLL:
                                    C.POINTER(IterStats)], C.c_int),
             "artss_diffuse_jacobi": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg),
                                       C.POINTER(IterStats)], C.c_int),
+            "artss_diffuse_cgs_mixed": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg),
+                                         C.c_int, C.POINTER(IterStats)], C.c_int),
             "artss_divergence": ([_P, _D, _D, _D, _D], C.c_int),
             "artss_projection": ([_P] + [_D] * 7, C.c_int),
             "artss_buoyancy_force": ([_P, _D, _D, _D, C.c_double, C.c_double], C.c_int),

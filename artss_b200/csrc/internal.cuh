@@ -134,6 +134,8 @@ struct artss_ctx {
     // box cell that is not inner (k_cgs_sweep3); built on first use
     uint8_t *d_sweep3_obst[2] = {nullptr, nullptr};              // per tile height (64 x 8, 64 x 6)
     int sweep3_obst_state[2] = {0, 0};                           // 0 not built, 1 built, 2 every box cell inner
+    float *cgsm_w = nullptr;                                     // FP32 defect / correction of artss_diffuse_cgs_mixed
+    int64_t cgsm_n = 0;
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
     // host transfers overlapped with the step: a second stream, completion
     // events of its uploads by slot, a mark of the main stream, its tail

@@ -1264,6 +1264,83 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
     if (partials && tid == 0) partials[blockIdx.x] = acc;
 }
 
+// ---- colored Gauss-Seidel with FP32 sweeps inside FP64 defect correction ----
+//
+// One iteration of the reference's red-then-black sweep (stencil at
+// ColoredGaussSeidelDiffuse.cpp:316-341) written as a correction of x: with
+// the system rb x - sum(alpha x_nb) = dsign b and the defect r = dsign b -
+// (rb x - sum(alpha x_nb)) of the current x (FP64), the red update is
+// e = r / rb and the black update e = (r + sum(alpha e_red,nb)) / rb, then
+// x += e, which in exact arithmetic is the in-place sweep (w = 1).  The
+// defect and the correction are FP32 values in one scratch array (red cells:
+// e, black cells: r) and the black update is FP32 arithmetic; the defect and
+// x stay FP64.  The loop stops on the reference's measure ||rb (x_new - x)||_2
+// = ||rb e||_2.
+template <bool TURB>
+__device__ __forceinline__ void cgsm_coef(const DiffCoef &c, const double *__restrict__ ev, int q, double &ax,
+                                          double &ay, double &az, double &rb) {
+    ax = c.ax, ay = c.ay, az = c.az, rb = c.rbeta;
+    if (TURB) turb_alpha(c, ev[q], ax, ay, az, rb);
+}
+
+// red cells: w = (float) (r / rb); black cells: w = (float) r
+template <bool TURB>
+__global__ void k_cgsm_defect(float *__restrict__ wv, const double *__restrict__ x, const double *__restrict__ b,
+                              const double *__restrict__ ev, const uint8_t *__restrict__ flags, Level L, Box3 box,
+                              DiffCoef c, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    ARTSS_COLUMN(box);
+    if (!col) return;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+        const int q = i + nj * j + nk * k;
+        if (!(flags[q] & kInner)) continue;
+        double ax, ay, az, rb;
+        cgsm_coef<TURB>(c, ev, q, ax, ay, az, rb);
+        const double r = c.dsign * b[q] + ax * (x[q + 1] + x[q - 1]) + ay * (x[q + nj] + x[q - nj]) +
+                         az * (x[q + nk] + x[q - nk]) - rb * x[q];
+        wv[q] = ((i + j + k) & 1) == 0 ? (float) (r / rb) : (float) r;
+    }
+}
+
+// black cells: e = (r + sum(alpha e_red,nb)) / rb in FP32; every inner cell
+// x += e; block partial of sum (rb e)^2
+template <bool TURB>
+__global__ void k_cgsm_correct(double *__restrict__ x, const float *__restrict__ wv, const double *__restrict__ ev,
+                               const uint8_t *__restrict__ flags, Level L, Box3 box, DiffCoef c,
+                               double *__restrict__ partials, const LoopState *__restrict__ pred) {
+    __shared__ double smem[32];
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;  // iteration enqueued past convergence
+    ARTSS_COLUMN(box);
+    double acc = 0.0;
+    if (col) {
+        const int nj = (int) L.Nx, nk = (int) L.nxy();
+        for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
+            const int q = i + nj * j + nk * k;
+            if (!(flags[q] & kInner)) continue;
+            double ax, ay, az, rb;
+            cgsm_coef<TURB>(c, ev, q, ax, ay, az, rb);
+            float e = wv[q];
+            if (((i + j + k) & 1) != 0) {
+                // red neighbours that are not inner carry no correction
+                auto er = [&](int n) { return (flags[n] & kInner) ? wv[n] : 0.0f; };
+                e = (e + (float) ax * (er(q + 1) + er(q - 1)) + (float) ay * (er(q + nj) + er(q - nj)) +
+                     (float) az * (er(q + nk) + er(q - nk))) /
+                    (float) rb;
+            }
+            x[q] += (double) e;
+            const double rr = rb * (double) e;
+            acc += rr * rr;
+        }
+    }
+    acc = artss_block_sum(acc, smem);
+    if (partials && threadIdx.x == 0 && threadIdx.y == 0) partials[block_linear()] = acc;
+}
+
 // One Jacobi step of JacobiDiffuse (laminar: JacobiDiffuse.cpp:241-249, note
 // the division by reciprocal_beta; turbulent: :345-362) + residual partials
 // of sum (rbeta * (out - in))^2 (:72-79).
@@ -1897,6 +1974,69 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
         }
     }
     loop_hint(ctx, 0, field_type) = std::max<int64_t>(1, it);
+    if (stats) { stats->iterations = it; stats->residual = res; }
+    return ARTSS_OK;
+}
+
+int artss_diffuse_cgs_mixed(artss_ctx *ctx, double *out, double *in, const double *b, double D, const double *ev,
+                            double dt, int field_type, const artss_iter_cfg *cfg, int flags,
+                            artss_iter_stats *stats) {
+    int st = check_field_args(ctx, {out, in, b, cfg});
+    if (st || (st = check_field_type(field_type))) return st;
+    if (cfg->max_iter < 0) { set_error("max_iter < 0"); return ARTSS_ERR_ARG; }
+    if (cfg->w != 1.0) { set_error("the defect-correction sweep reproduces the relaxation weight 1 only"); return ARTSS_ERR_ARG; }
+    if (out == in || b == out || b == in) { set_error("out, in and b must be distinct arrays"); return ARTSS_ERR_ARG; }
+    if (ctx->capturing) { set_error("the mixed-precision diffusion is not captured into graphs"); return ARTSS_ERR_STATE; }
+    const Level &L = ctx->lvl[0];
+    const Box3 box = inner_box(L);
+    const dim3 g = zgrid(box);
+    if ((st = check_reduce_blocks(g))) return st;
+    const int nb = nblocks(g);
+    if (!ctx->cgsm_w || ctx->cgsm_n != L.size()) {
+        if (ctx->cgsm_w) cudaFree(ctx->cgsm_w);
+        ctx->cgsm_w = nullptr;
+        ARTSS_CK(cudaMalloc(&ctx->cgsm_w, (size_t) L.size() * sizeof(float)));
+        ctx->cgsm_n = L.size();
+    }
+    float *wv = ctx->cgsm_w;
+    const DiffCoef c = diff_coef(ctx, D, dt, cfg->w, 1.0);
+    // out.copy_data(in) (ColoredGaussSeidelDiffuse.cpp:41,114)
+    if (!(flags & ARTSS_DIFFUSE_OUT_HOLDS_IN) && (st = artss_copy(ctx, out, in, 0))) return st;
+    const int slot = 0;
+    long long it = 0;
+    double res = 1.;
+    bool cond = res > cfg->tol_res && it < cfg->max_iter;
+    if ((st = init_loop(ctx, slot, res, 0, cond ? 1 : 0))) return st;
+    LoopState ls{};
+    const LoopState *pred = ctx->d_loop + slot;
+    int64_t batch = std::max<int64_t>(1, std::min<int64_t>(loop_hint(ctx, 2, field_type), cfg->max_iter));
+    while (cond) {
+        for (int64_t r = 0; r < batch; r++) {
+            if (ev) {
+                ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgsm_defect<true>, g, box_block(), 0, wv, (const double *) out, b, ev,
+                                 (const uint8_t *) ctx->d_flags[0], L, box, c, pred);
+                ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgsm_correct<true>, g, box_block(), 0, out, (const float *) wv, ev,
+                                 (const uint8_t *) ctx->d_flags[0], L, box, c, ctx->d_partials, pred);
+            } else {
+                ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgsm_defect<false>, g, box_block(), 0, wv, (const double *) out, b,
+                                 (const double *) nullptr, (const uint8_t *) ctx->d_flags[0], L, box, c, pred);
+                ARTSS_LAUNCH_PDL(ctx, FAM_CGS, k_cgsm_correct<false>, g, box_block(), 0, out, (const float *) wv,
+                                 (const double *) nullptr, (const uint8_t *) ctx->d_flags[0], L, box, c,
+                                 ctx->d_partials, pred);
+            }
+            ARTSS_LAUNCH_CK(ctx);
+            if ((st = apply_bc(ctx, out, 0, field_type, pred))) return st;
+            if ((st = finalize_loop(ctx, slot, nb, cfg->tol_res, cfg->max_iter))) return st;
+        }
+        if ((st = read_loop(ctx, slot, &ls))) return st;
+        it = ls.it;
+        res = ls.residual;
+        cond = ls.cond != 0;
+        batch = std::min<int64_t>(2 * batch, std::max<int64_t>(1, cfg->max_iter - it));
+    }
+    loop_hint(ctx, 2, field_type) = std::max<int64_t>(1, it);
+    // the reference leaves in = out after every iteration (:79)
+    if (!(flags & ARTSS_DIFFUSE_IN_SCRATCH) && (st = artss_copy(ctx, in, out, 0))) return st;
     if (stats) { stats->iterations = it; stats->residual = res; }
     return ARTSS_OK;
 }

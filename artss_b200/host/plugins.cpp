@@ -46,11 +46,15 @@ void ColoredGaussSeidelDiffuse::run(Field &out, const Field &in, const Field &b,
     artss_iter_cfg cfg{(int64_t) m_settings.max_iter, m_settings.tol_res, m_settings.w};
     artss_iter_stats st{};
     // the reference overwrites its const `in` argument (ColoredGaussSeidelDiffuse.cpp:71)
-    check(artss_diffuse_cgs(m_rt.ctx(), out.data, in.data, b.data, D, ev ? ev->data : nullptr, m_rt.dt(),
-                            out.get_type(), &cfg,
-                            (in_is_scratch ? ARTSS_DIFFUSE_IN_SCRATCH : 0) | (out_holds_in ? ARTSS_DIFFUSE_OUT_HOLDS_IN : 0),
-                            &st),
-          "ColoredGaussSeidelDiffuse::diffuse");
+    const int flags = (in_is_scratch ? ARTSS_DIFFUSE_IN_SCRATCH : 0) | (out_holds_in ? ARTSS_DIFFUSE_OUT_HOLDS_IN : 0);
+    if (m_mixed)
+        check(artss_diffuse_cgs_mixed(m_rt.ctx(), out.data, in.data, b.data, D, ev ? ev->data : nullptr, m_rt.dt(),
+                                      out.get_type(), &cfg, flags, &st),
+              "ColoredGaussSeidelDiffuse::diffuse (mixed precision)");
+    else
+        check(artss_diffuse_cgs(m_rt.ctx(), out.data, in.data, b.data, D, ev ? ev->data : nullptr, m_rt.dt(),
+                                out.get_type(), &cfg, flags, &st),
+              "ColoredGaussSeidelDiffuse::diffuse");
     last_iterations = st.iterations;
     last_residual = st.residual;
 }
@@ -93,7 +97,8 @@ void JacobiDiffuse::diffuse(Field &out, const Field &in, const Field &b, real D,
 
 // ---------------------------------------------------------------- VCycleMG
 
-VCycleMG::VCycleMG(Runtime &rt, const settings::Pressure &s) : m_rt(rt), m_settings(s) {
+VCycleMG::VCycleMG(Runtime &rt, const settings::Pressure &s, bool to_rel_tol)
+    : m_rt(rt), m_settings(s), m_rel(to_rel_tol) {
     artss_mg_cfg c{};
     c.n_level = (int32_t) s.n_level;
     c.n_cycle = (int32_t) s.n_cycle;
@@ -112,6 +117,14 @@ VCycleMG::VCycleMG(Runtime &rt, const settings::Pressure &s) : m_rt(rt), m_setti
 VCycleMG::~VCycleMG() { artss_mg_destroy(m_mg); }
 
 void VCycleMG::pressure(Field &out, const Field &b, real t, bool) {
+    if (m_rel) {
+        artss_solve_stats st{};
+        check(artss_mg_solve_rel(m_mg, out.data, b.data, m_settings.tol_res, (int64_t) m_settings.max_cycle, &st),
+              "VCycleMGRel::pressure");
+        last_cycles = st.cycles;
+        last_residual = st.residual;
+        return;
+    }
     // VCycleMG::pressure (src/pressure/VCycleMG.cpp:142-207): Nt == 1 iterates to tolerance
     const auto Nt = static_cast<size_t>(std::round(t / m_rt.dt()));
     artss_mg_stats st{};

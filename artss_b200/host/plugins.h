@@ -93,7 +93,10 @@ class SLAdvect : public IAdvection {
 
 class ColoredGaussSeidelDiffuse : public IDiffusion {
  public:
-    ColoredGaussSeidelDiffuse(Runtime &rt, const settings::Diffusion &s) : m_rt(rt), m_settings(s) {}
+    // mixed: FP32 sweeps inside FP64 defect correction (artss_diffuse_cgs_mixed),
+    // the XML type ColoredGaussSeidelMixed (same keys)
+    ColoredGaussSeidelDiffuse(Runtime &rt, const settings::Diffusion &s, bool mixed = false)
+        : m_rt(rt), m_settings(s), m_mixed(mixed) {}
     void diffuse(Field &out, const Field &in, const Field &b, real D, bool sync) override;
     void diffuse(Field &out, const Field &in, const Field &b, real D, const Field &ev, bool sync) override;
 
@@ -101,6 +104,7 @@ class ColoredGaussSeidelDiffuse : public IDiffusion {
     void run(Field &out, const Field &in, const Field &b, real D, const Field *ev);
     Runtime &m_rt;
     settings::Diffusion m_settings;
+    bool m_mixed;
 };
 
 // ExplicitDiffuse (src/diffusion/ExplicitDiffuse.cpp:27-127): one explicit step per call
@@ -128,7 +132,10 @@ class JacobiDiffuse : public IDiffusion {
 
 class VCycleMG : public IPressure {
  public:
-    VCycleMG(Runtime &rt, const settings::Pressure &s);
+    // to_rel_tol: every call repeats the reference V-cycle until the relative
+    // residual ||b - A p|| / ||b|| <= tol_res (at most max_cycle cycles): the XML
+    // type VCycleMGRel, the FP64 counterpart of VCycleMGMixed
+    VCycleMG(Runtime &rt, const settings::Pressure &s, bool to_rel_tol = false);
     ~VCycleMG() override;
     void pressure(Field &out, const Field &b, real t, bool sync) override;
     artss_mg *handle() const { return m_mg; }
@@ -137,6 +144,7 @@ class VCycleMG : public IPressure {
     Runtime &m_rt;
     settings::Pressure m_settings;
     artss_mg *m_mg = nullptr;
+    bool m_rel = false;
 };
 
 // Mixed-precision pressure solve (no reference counterpart; artss_mixed_*):

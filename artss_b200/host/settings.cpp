@@ -189,7 +189,7 @@ Diffusion parse_diffusion(const XmlElement *head, const std::string &parent) {
     Section s = section(head, "diffusion");
     Diffusion d;
     d.type = req_str(s.values, "type", context);
-    if (d.type == "Jacobi" || d.type == "ColoredGaussSeidel") {
+    if (d.type == "Jacobi" || d.type == "ColoredGaussSeidel" || d.type == "ColoredGaussSeidelMixed") {
         const std::string c2 = ctx_join(context, d.type);
         d.has_iteration = true;
         d.w = req_real(s.values, "w", c2);
@@ -245,7 +245,7 @@ Pressure parse_pressure(const XmlElement *head, const std::string &parent) {
     p.field = match_field(req_str(s.values, "field", context));
     // VCycleMGMixed (no reference counterpart) reads the same keys; tol_res is
     // its relative tolerance and max_cycle its cycle limit per solve
-    if (p.type != "VCycleMG" && p.type != "VCycleMGMixed")
+    if (p.type != "VCycleMG" && p.type != "VCycleMGMixed" && p.type != "VCycleMGRel")
         throw config_error("pressure solver '" + p.type + "' has no parsing implementation.");
     const std::string c2 = ctx_join(context, "vcycle");
     p.n_level = req_size(s.values, "n_level", c2);

@@ -14,6 +14,7 @@ std::unique_ptr<IAdvection> make_advection(Runtime &rt, const settings::Advectio
 
 std::unique_ptr<IDiffusion> make_diffusion(Runtime &rt, const settings::Diffusion &s) {
     if (s.type == "ColoredGaussSeidel") return std::make_unique<ColoredGaussSeidelDiffuse>(rt, s);
+    if (s.type == "ColoredGaussSeidelMixed") return std::make_unique<ColoredGaussSeidelDiffuse>(rt, s, true);
     if (s.type == "Jacobi") return std::make_unique<JacobiDiffuse>(rt, s);
     if (s.type == "Explicit") return std::make_unique<ExplicitDiffuse>(rt);
     throw config_error("diffusion method '" + s.type + "' is not implemented");
@@ -26,6 +27,7 @@ std::unique_ptr<ITurbulence> make_turbulence(Runtime &rt, const settings::Turbul
 
 std::unique_ptr<IPressure> make_pressure(Runtime &rt, const settings::Pressure &s) {
     if (s.type == "VCycleMG") return std::make_unique<VCycleMG>(rt, s);
+    if (s.type == "VCycleMGRel") return std::make_unique<VCycleMG>(rt, s, true);
     if (s.type == "VCycleMGMixed") return std::make_unique<MixedVCycle>(rt, s);
     throw config_error("pressure method '" + s.type + "' is not implemented");
 }

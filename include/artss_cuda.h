@@ -344,6 +344,18 @@ int artss_cgs_sweep_variant(artss_ctx *ctx, int turbulent);
  * above; 3-7 need an inner box that starts at an odd x), -1 (default): the
  * autotuner's choice.  No counterpart in the reference. */
 int artss_ctx_sweep_variant(artss_ctx *ctx, int variant);
+/* IDiffusion::diffuse, ColoredGaussSeidelDiffuse with FP32 sweeps inside FP64
+ * defect correction (no counterpart in the reference; mirrors
+ * src/diffusion/ColoredGaussSeidelDiffuse.cpp:38-173): each iteration forms
+ * the FP64 defect of out, solves for the correction by one red-then-black
+ * sweep from zero with the correction in FP32, adds it in FP64 and applies the
+ * boundary program; the loop stops on the reference's measure ||rb (x_new -
+ * x)||_2 <= tol_res or max_iter.  In exact arithmetic each iteration is the
+ * reference's (w must be 1).  Same arguments and flags as artss_diffuse_cgs;
+ * not captured into graphs. */
+int artss_diffuse_cgs_mixed(artss_ctx *ctx, double *out, double *in, const double *b,
+                            double D, const double *ev, double dt, int field_type,
+                            const artss_iter_cfg *cfg, int flags, artss_iter_stats *stats);
 /* IDiffusion::diffuse, JacobiDiffuse (src/diffusion/JacobiDiffuse.cpp:31-203). */
 int artss_diffuse_jacobi(artss_ctx *ctx, double *out, double *in, const double *b,
                          double D, const double *ev, double dt, int field_type,
