@@ -298,6 +298,31 @@ def test_dissipate(env):
     assert np.array_equal(ctx.download(dT), ref)
 
 
+@pytest.mark.parametrize("turbulent", [False, True])
+def test_cgs_mixed_precision(env, turbulent):
+    """FP32 sweeps inside FP64 defect correction: the same iterations as the
+    reference's FP64 sweep (oracle), values within the FP32 rounding of the
+    corrections (1e-8 relative here)."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    out0, in0, b, ev = rnd(131, n, 290, 300), rnd(132, n, 290, 300), rnd(133, n, 290, 300), rnd(134, n, 0, 1e-3)
+    dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
+    cfg = A.IterCfg(5, 1e-300, 1.0)
+    stats = A.IterStats()
+    A.cuda_check(ctx.lib.artss_diffuse_cgs_mixed(ctx.h, dout, din, db, 4.2e-5, dev if turbulent else None, sc.dt,
+                                                 FT["u"], C.byref(cfg), 0, C.byref(stats)), "cgs mixed")
+    ro, ri = out0.copy(), in0.copy()
+    res = C.c_double()
+    its = oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev) if turbulent else None, sc.dt,
+                                          FT["u"], 5, 1e-300, 1.0, C.byref(res))
+    assert stats.iterations == its == 5
+    got = ctx.download(dout)
+    err = float(np.max(np.abs(got - ro)) / np.max(np.abs(ro)))
+    assert err <= 1e-8, err
+    assert np.array_equal(ctx.download(din), got)  # in = out as the reference leaves them
+    assert abs(stats.residual - res.value) <= 1e-5 * res.value
+
+
 def _sweep_scenes():
     """a channel with a cube (obstacle planes take the flag path of the
     row-pair sweep); odd sizes with a box that touches the x-y edges of the
