@@ -320,7 +320,16 @@ def test_cgs_mixed_precision(env, turbulent):
     err = float(np.max(np.abs(got - ro)) / np.max(np.abs(ro)))
     assert err <= 1e-8, err
     assert np.array_equal(ctx.download(din), got)  # in = out as the reference leaves them
-    assert abs(stats.residual - res.value) <= 1e-5 * res.value
+    # the stopping measure ||rb (x_new - x)||, taken while it is well above round-off
+    dout, din = ctx.field(out0), ctx.field(in0)
+    cfg2 = A.IterCfg(2, 1e-300, 1.0)
+    A.cuda_check(ctx.lib.artss_diffuse_cgs_mixed(ctx.h, dout, din, db, 4.2e-5, dev if turbulent else None, sc.dt,
+                                                 FT["u"], C.byref(cfg2), 0, C.byref(stats)), "cgs mixed")
+    ro, ri = out0.copy(), in0.copy()
+    oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev) if turbulent else None, sc.dt,
+                                    FT["u"], 2, 1e-300, 1.0, C.byref(res))
+    assert res.value > 1e-6
+    assert abs(stats.residual - res.value) <= 1e-6 * res.value, (stats.residual, res.value)
 
 
 def _sweep_scenes():

@@ -10,7 +10,12 @@
   same relative residual every step (VCycleMGRel): the reference's own
   pressure runs two cycles per step, which no converged solve matches.
 
-Bound: 1e-6 relative max-norm per field after every checked step."""
+Bound: 1e-6 relative max-norm per field over the inner cells after every
+checked step.  Where
+every wall is a Neumann wall for p (this box), p is fixed only up to a
+constant: the second comparison takes p relative to its mean over the inner
+cells (its gradient, which the projection uses, is what both runs share)."""
+import numpy as np
 import pytest
 
 import artss_b200 as A
@@ -22,14 +27,19 @@ TOL = 1e-6
 FIELDS = ["u", "v", "w", "p", "T", "nu_t"]
 
 
-def _run_pair(tmp_path, mixed: scenes.Scene, check):
+def _run_pair(tmp_path, mixed: scenes.Scene, check, p_modulo_mean=False):
     xml = scenes.write(mixed, str(tmp_path / "mixed.xml"))
+    inner = A.Geometry(xml).list("inner", 0)
     worst = {f: 0.0 for f in FIELDS}
+
+    def shift(f, a):
+        return a - np.mean(a[inner]) if (p_modulo_mean and f == "p") else a
+
     with A.Simulation(xml) as sim:
         for step in range(10, mixed.steps + 1, 10):
             assert sim.run(10) == 10
             for f in FIELDS:
-                err = refdriver.rel_max_err(sim.field(f), check(step, f))
+                err = refdriver.rel_max_err(shift(f, sim.field(f))[inner], shift(f, check(step, f))[inner])
                 worst[f] = max(worst[f], err)
                 assert err <= TOL, f"step {step} field {f}: relative max error {err:.3e}"
     return worst
@@ -55,6 +65,6 @@ def test_mixed_pressure_and_diffusion_200_steps(tmp_path):
             assert sim.run(10) == 10
             fields64[step] = {f: sim.field(f) for f in FIELDS}
     worst = _run_pair(tmp_path, scenes.plume_box(pressure="VCycleMGMixed", diffusion="ColoredGaussSeidelMixed"),
-                      lambda step, f: fields64[step][f])
+                      lambda step, f: fields64[step][f], p_modulo_mean=True)
     print("FP32 V-cycles + FP32 diffusion sweeps, 200 steps vs FP64 to the same tolerance, worst relative error: " +
           ", ".join(f"{f} {e:.3e}" for f, e in worst.items()))
