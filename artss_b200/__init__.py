@@ -81,6 +81,8 @@ class SolveStats(C.Structure):
 
 
 MIXED_REMOVE_MEAN = 1
+MIXED_RBGS = 2
+MIXED_BC_LAUNCH = 4
 
 
 class ConvDesc(C.Structure):

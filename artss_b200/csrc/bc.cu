@@ -224,6 +224,7 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
     });
     const int64_t n = (int64_t) folded.size();
     std::vector<int64_t> tgt(n), root(n);
+    std::vector<int8_t> sign(n);
     std::vector<uint8_t> depth(n), neg(n);
     std::vector<double> val((size_t) kBcMaxDepth * std::max<int64_t>(n, 1), 0.0);
     std::vector<int64_t> begin(waves + 1, 0);
@@ -232,6 +233,7 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
         root[q] = folded[q].root;
         depth[q] = (uint8_t) folded[q].depth;
         neg[q] = folded[q].neg;
+        sign[q] = (__builtin_popcount((unsigned) folded[q].neg & ((1u << folded[q].depth) - 1u)) & 1) ? -1 : 1;
         for (int s = 0; s < kBcMaxDepth; s++) val[s * n + q] = s < folded[q].depth ? folded[q].value[s] : 0.0;
         begin[folded[q].wave + 1] = q + 1;
     }
@@ -247,6 +249,8 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type, const 
     p.n = n;
     p.h_target = tgt;
     p.h_root = root;
+    p.h_sign = sign;
+    ctx->geom_version++;
     p.zero_values = true;
     for (double v : val) {
         uint64_t bits;

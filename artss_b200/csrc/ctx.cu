@@ -757,6 +757,7 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
     }
     const Level &L = ctx->lvl[level];
     ctx->n_inner[level] = n_inner;
+    ctx->geom_version++;
     if (level == 0) {
         // the sweep's obstacle table describes the old lists
         for (int t = 0; t < 2; t++) {

@@ -53,6 +53,7 @@ struct BcProgram {
     double *d_value = nullptr;         // [kBcMaxDepth][n]
     std::vector<int64_t> h_target;     // targets, host copy
     std::vector<int64_t> h_root;       // roots, host copy
+    std::vector<int8_t> h_sign;        // sign of x_t = +-x_r with every value zero, host copy
     bool zero_values = false;          // every value of the program is +0.0: x_t = +-x_r + 0
     // plan of the pipelined coarse solve: state -2 unknown, -1 not eligible, 1 planned
     int pipe_state = -2;
@@ -130,6 +131,7 @@ struct artss_ctx {
     bool autotune = true;                                        // time kernel variants on first use
     int sweep_force = -1;                                        // colored Gauss-Seidel sweep variant pinned (-1: tuned)
     int sm_count = 0;                                            // multiprocessors of the device
+    uint64_t geom_version = 0;                                   // bumped by every cell-list or boundary-program change
     // tile columns x planes of level 0 whose row-pair sweep tile (+ ring) holds a
     // box cell that is not inner (k_cgs_sweep3); built on first use
     uint8_t *d_sweep3_obst[2] = {nullptr, nullptr};              // per tile height (64 x 8, 64 x 6)
@@ -261,6 +263,86 @@ inline dim3 box_grid(const Box3 &b) {
 inline dim3 box_block() { return dim3(kBx, kBy, 1); }
 inline Box3 inner_box(const Level &L) { return {L.i1, L.i2, L.j1, L.j2, L.k1, L.k2}; }
 inline Box3 domain_box(const Level &L) { return {L.i1 - 1, L.i2 + 1, L.j1 - 1, L.j2 + 1, L.k1 - 1, L.k2 + 1}; }
+
+// Plane loop of one (i, j) column over planes k = z0 + blockIdx.z + t * gridDim.z,
+// U (default kColU) planes per round.  For every plane of a round `value(q, k)` runs first
+// (the cells of a column are independent, so their loads are in flight
+// together), then `put(q, k, v, flag)` for the planes whose cell carries kInner, in
+// ascending k, with the flag value already loaded.  A round's planes past z1 evaluate the round's first plane again
+// and store nothing.  Every cell of an inner box has its six neighbours inside
+// the level's array, so `value` reads them without a check.  32-bit indices:
+// artss_ctx_create rejects levels of 2^31 cells or more.
+constexpr int kColU = 4;
+template <int U = kColU, class FlagT, class V, class P>
+__device__ __forceinline__ void column_planes(int base, int nk, int z0, int z1, const FlagT *__restrict__ flags,
+                                              V value, P put) {
+    const int gz = (int) gridDim.z;
+    using T = decltype(value(0, 0));
+    for (int k0 = z0 + (int) blockIdx.z; k0 <= z1; k0 += U * gz) {
+        T v[U];
+        int q[U], kk[U];
+        FlagT fl[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + u * gz;
+            const bool in = k <= z1;
+            kk[u] = in ? k : k0;
+            q[u] = base + nk * kk[u];
+            fl[u] = flags[q[u]];
+            ok[u] = in && (fl[u] & kInner);
+            v[u] = value(q[u], kk[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (ok[u]) put(q[u], kk[u], v[u], fl[u]);
+    }
+}
+
+// z-marching variant for 7-point stencils of one array f: the block's planes
+// are the contiguous run [z0 + blockIdx.z * chunk, ...] of chunk =
+// ceil(nz / gridDim.z) planes, and the thread walks its column through them
+// kColU planes per round.  The centre values f[q] of planes k-1 .. k+kColU are
+// loaded once per round and handed to `value(q, k, f_km1, f_k, f_kp1)` as the
+// z-neighbours, so a cell costs one f load less than its stencil has z terms,
+// and each block streams through consecutive planes.  Planes past the run end
+// are clamped to the plane after it (a ghost or inner plane of the array) and
+// store nothing; `put` as in column_planes.
+template <class T, class FlagT, class V, class P>
+__device__ __forceinline__ void column_march(const T *__restrict__ f, int base, int nk, int z0, int z1,
+                                             const FlagT *__restrict__ flags, V value, P put) {
+    const int nz = z1 - z0 + 1, gz = (int) gridDim.z;
+    const int chunk = (nz + gz - 1) / gz;
+    const int kb = z0 + (int) blockIdx.z * chunk;
+    if (kb > z1) return;
+    const int ke = min(kb + chunk - 1, z1);
+    T c[kColU + 2];
+    c[0] = f[base + nk * (kb - 1)];
+    c[1] = f[base + nk * kb];
+    using R = decltype(value(0, 0, c[0], c[1], c[1]));
+    for (int k0 = kb; k0 <= ke; k0 += kColU) {
+#pragma unroll
+        for (int u = 0; u < kColU; u++) c[2 + u] = f[base + nk * min(k0 + 1 + u, ke + 1)];
+        R v[kColU];
+        int q[kColU];
+        FlagT fl[kColU];
+        bool ok[kColU];
+#pragma unroll
+        for (int u = 0; u < kColU; u++) {
+            const int k = k0 + u;
+            const bool in = k <= ke;
+            q[u] = base + nk * (in ? k : ke);
+            fl[u] = flags[q[u]];
+            ok[u] = in && (fl[u] & kInner);
+            v[u] = value(q[u], in ? k : ke, c[u], c[u + 1], c[u + 2]);
+        }
+#pragma unroll
+        for (int u = 0; u < kColU; u++)
+            if (ok[u]) put(q[u], k0 + u, v[u], fl[u]);
+        c[0] = c[kColU];
+        c[1] = c[kColU + 1];
+    }
+}
 
 // Grid-size helper for flat (1-D) loops over n elements.
 inline unsigned flat_blocks(int64_t n, int threads = 256) {

@@ -71,13 +71,13 @@ __global__ void k_mg_jacobi(double *__restrict__ out, const double *__restrict__
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + nk * k;
-        if (!(flags[q] & kInner)) continue;
-        const double out_h = c.beta * (c.dsign * b[q] + c.ax * (in[q + 1] + in[q - 1]) +
-                                       c.ay * (in[q + nj] + in[q - nj]) + c.az * (in[q + nk] + in[q - nk]));
-        out[q] = c.omw * in[q] + c.w * out_h;
-    }
+    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int q, int, double km, double c0, double kp) {
+            const double out_h = c.beta * (c.dsign * b[q] + c.ax * (in[q + 1] + in[q - 1]) +
+                                           c.ay * (in[q + nj] + in[q - nj]) + c.az * (kp + km));
+            return c.omw * c0 + c.w * out_h;
+        },
+        [&](int q, int, double v, auto) { out[q] = v; });
 }
 
 // colored Gauss-Seidel stencil with the multigrid coefficients
@@ -105,13 +105,14 @@ __global__ void k_mg_residuum(double *__restrict__ out, const double *__restrict
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + nk * k;
-        if (!(flags[q] & kInner)) continue;
-        const double weighted = (rx * (in[q - 1] - 2 * in[q] + in[q + 1]) + ry * (in[q - nj] - 2 * in[q] + in[q + nj]) +
-                                 rz * (in[q - nk] - 2 * in[q] + in[q + nk]));
-        out[q] = b[q] - weighted;
-    }
+    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int q, int, double km, double c0, double kp) {
+            const double weighted = (rx * (in[q - 1] - 2 * c0 + in[q + 1]) +
+                                     ry * (in[q - nj] - 2 * c0 + in[q + nj]) +
+                                     rz * (km - 2 * c0 + kp));
+            return b[q] - weighted;
+        },
+        [&](int q, int, double v, auto) { out[q] = v; });
 }
 
 // block partials of sum (b - A x)^2 over the level's inner cells
@@ -124,14 +125,18 @@ __global__ void k_mg_resnorm(const double *__restrict__ x, const double *__restr
     const int nj = (int) L.Nx, nk = (int) L.nxy();
     double acc = 0.0, accb = 0.0;
     if (col) {
-        for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-            const int q = i + (int) L.Nx * j + nk * k;
-            if (!(flags[q] & kInner)) continue;
-            const double r = b[q] - (rx * (x[q - 1] - 2 * x[q] + x[q + 1]) + ry * (x[q - nj] - 2 * x[q] + x[q + nj]) +
-                                     rz * (x[q - nk] - 2 * x[q] + x[q + nk]));
-            acc += r * r;
-            accb += b[q] * b[q];
-        }
+        struct RB { double r, b; };
+        column_march(x, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+            [&](int q, int, double km, double c0, double kp) {
+                const double r = b[q] - (rx * (x[q - 1] - 2 * c0 + x[q + 1]) +
+                                         ry * (x[q - nj] - 2 * c0 + x[q + nj]) +
+                                         rz * (km - 2 * c0 + kp));
+                return RB{r, b[q]};
+            },
+            [&](int, int, RB v, auto) {
+                acc += v.r * v.r;
+                accb += v.b * v.b;
+            });
     }
     const int bl = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     acc = artss_block_sum(acc, smem);
@@ -151,14 +156,14 @@ __global__ void k_mg_restrict(double *__restrict__ out, const double *__restrict
     MG_COLUMN(box);
     if (!col) return;
     const int fx = (int) F.Nx, fxy = (int) F.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) C.Nx * j + (int) C.nxy() * k;
-        if (!(flags[q] & kInner)) continue;
-        const int a = 2 * i - 1, bx = 2 * i, c = 2 * j - 1, d = 2 * j, e = 2 * k - 1, f = 2 * k;
-        out[q] = 0.125 * (in[a + fx * c + fxy * e] + in[bx + fx * c + fxy * e] + in[a + fx * d + fxy * e] +
-                          in[bx + fx * d + fxy * e] + in[a + fx * c + fxy * f] + in[bx + fx * c + fxy * f] +
-                          in[a + fx * d + fxy * f] + in[bx + fx * d + fxy * f]);
-    }
+    column_planes(i + (int) C.Nx * j, (int) C.nxy(), (int) box.z0, (int) box.z1, flags,
+        [&](int, int k) {
+            const int a = 2 * i - 1, bx = 2 * i, c = 2 * j - 1, d = 2 * j, e = 2 * k - 1, f = 2 * k;
+            return 0.125 * (in[a + fx * c + fxy * e] + in[bx + fx * c + fxy * e] + in[a + fx * d + fxy * e] +
+                            in[bx + fx * d + fxy * e] + in[a + fx * c + fxy * f] + in[bx + fx * c + fxy * f] +
+                            in[a + fx * d + fxy * f] + in[bx + fx * d + fxy * f]);
+        },
+        [&](int q, int, double v, auto) { out[q] = v; });
 }
 
 // VCycleMG::Prolongate (VCycleMG.cpp:464-546): 8 fine cells per coarse inner cell

@@ -28,6 +28,7 @@
 #include "internal.cuh"
 
 #include <algorithm>
+#include <unordered_map>
 
 struct artss_mixed {
     artss_ctx *ctx = nullptr;
@@ -37,6 +38,16 @@ struct artss_mixed {
     float *q[artss::kMaxLevel + 1]{};    // residual of level l
     float *e[artss::kMaxLevel + 1]{};    // correction of level l
     float *t[artss::kMaxLevel + 1]{};    // Jacobi ping-pong partner of e
+    // the level's homogeneous pressure program applied by the writers of the
+    // inner cells instead of by a launch after each sweep (levels 0 .. L-2, when
+    // fold[l]): nbm[l][x] bit 0 = inner, bits 1..7 = index of the cell's push
+    // pattern in push[l]; bits 2d .. 2d + 1 of a pattern = what the boundary cell
+    // x + off[d] (d: -x, +x, -y, +y, -z, +z) takes from inner cell x with value v:
+    // 0 nothing, 1 +v, 2 -v
+    uint8_t *nbm[artss::kMaxLevel + 1]{};
+    uint16_t *push[artss::kMaxLevel + 1]{};  // 128 patterns per level (pattern 0: none)
+    bool fold[artss::kMaxLevel + 1]{};
+    uint64_t geom_version = ~0ull;       // ctx->geom_version the tables describe
     int64_t n_inner0 = 0;
     int64_t hint = 1;                    // outer iterations of the last solve
 };
@@ -55,10 +66,11 @@ inline dim3 mx_grid(const Box3 &b) {
     return g;
 }
 
-#define MX_COLUMN(box)                                                            \
-    const int64_t i = (box).x0 + (int64_t) blockIdx.x * blockDim.x + threadIdx.x; \
-    const int64_t j = (box).y0 + (int64_t) blockIdx.y * blockDim.y + threadIdx.y; \
-    const bool col = (i <= (box).x1) && (j <= (box).y1)
+// 32-bit cell indices: artss_ctx_create rejects levels of 2^31 cells or more
+#define MX_COLUMN(box)                                                             \
+    const int i = (int) (box).x0 + (int) (blockIdx.x * blockDim.x + threadIdx.x); \
+    const int j = (int) (box).y0 + (int) (blockIdx.y * blockDim.y + threadIdx.y); \
+    const bool col = (i <= (int) (box).x1) && (j <= (int) (box).y1)
 
 struct CoefF {
     float ax, ay, az, beta, w, omw;
@@ -66,41 +78,83 @@ struct CoefF {
 
 // weighted Jacobi sweep of the pressure operator (the multigrid variant of
 // JacobiDiffuse::JacobiStep, dsign = -1), FP32
-__global__ void k_mx_jacobi(float *__restrict__ out, const float *__restrict__ in, const float *__restrict__ b,
-                            const uint8_t *__restrict__ flags, Level L, Box3 box, CoefF c,
-                            const LoopState *__restrict__ pred) {
+// store v at inner cell x and the boundary cells whose homogeneous program
+// value is +-x (push bits of the neighbour mask)
+__device__ __forceinline__ void mx_store(float *__restrict__ out, uint8_t mask, const uint16_t *__restrict__ push,
+                                         int x, float v, int nj, int nk) {
+    out[x] = v;
+    if (mask >> 1) {
+        const unsigned mm = __ldg(push + (mask >> 1));
+        const int off[6] = {-1, 1, -nj, nj, -nk, nk};
+#pragma unroll
+        for (int d = 0; d < 6; d++) {
+            const unsigned kind = (mm >> (2 * d)) & 3u;
+            if (kind) out[x + off[d]] = kind == 1u ? v : -v;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 8) k_mx_jacobi(float *__restrict__ out, const float *__restrict__ in, const float *__restrict__ b,
+                            const uint8_t *__restrict__ nbm, const uint16_t *__restrict__ push, Level L, Box3 box,
+                            CoefF c, const LoopState *__restrict__ pred) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + nj * j + nk * k;
-        if (!(flags[x] & kInner)) continue;
-        const float h = c.beta * (-b[x] + c.ax * (in[x + 1] + in[x - 1]) + c.ay * (in[x + nj] + in[x - nj]) +
-                                  c.az * (in[x + nk] + in[x - nk]));
-        out[x] = c.omw * in[x] + c.w * h;
-    }
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
+        [&](int x, int, float km, float c0, float kp) {
+            const float h = c.beta * (-b[x] + c.ax * (in[x + 1] + in[x - 1]) + c.ay * (in[x + nj] + in[x - nj]) +
+                                      c.az * (kp + km));
+            return c.omw * c0 + c.w * h;
+        },
+        [&](int x, int, float v, uint8_t fl) { mx_store(out, fl, push, x, v, nj, nk); });
+}
+
+// one colour of an in-place red-black Gauss-Seidel sweep of the same operator,
+// FP32: cells with (i + j + k) % 2 == color; first != 0: the sweep starts from a
+// zero correction, so the red cells get w * beta * (-b) and the black cells 0
+__global__ void k_mx_rbgs(float *__restrict__ e, const float *__restrict__ b, const uint8_t *__restrict__ flags,
+                          Level L, Box3 box, CoefF c, int color, int first, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;
+    MX_COLUMN(box);
+    if (!col) return;
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    // the cells of one colour read only cells of the other: no cell of the
+    // launch is both read and written
+    column_march((const float *) e, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int x, int, float km, float c0, float kp) {
+            if (first) return c.w * (c.beta * -b[x]);
+            const float h = c.beta * (-b[x] + c.ax * (e[x + 1] + e[x - 1]) + c.ay * (e[x + nj] + e[x - nj]) +
+                                      c.az * (kp + km));
+            return c.omw * c0 + c.w * h;
+        },
+        [&](int x, int k, float v, auto) {
+            if (((i + j + k) & 1) == color) e[x] = v;
+            else if (first) e[x] = 0.f;
+        });
 }
 
 // residual q = b - A e on inner cells, FP32 (VCycleMG::Residuum)
 __global__ void k_mx_residuum(float *__restrict__ out, const float *__restrict__ e, const float *__restrict__ b,
-                              const uint8_t *__restrict__ flags, Level L, Box3 box, float rx, float ry, float rz,
+                              const uint8_t *__restrict__ nbm, Level L, Box3 box, float rx, float ry, float rz,
                               const LoopState *__restrict__ pred) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + nj * j + nk * k;
-        if (!(flags[x] & kInner)) continue;
-        const float c2 = 2.f * e[x];
-        out[x] = b[x] - (rx * (e[x - 1] - c2 + e[x + 1]) + ry * (e[x - nj] - c2 + e[x + nj]) +
-                         rz * (e[x - nk] - c2 + e[x + nk]));
-    }
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    column_march(e, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
+        [&](int x, int, float km, float c0, float kp) {
+            const float c2 = 2.f * c0;
+            return b[x] - (rx * (e[x - 1] - c2 + e[x + 1]) + ry * (e[x - nj] - c2 + e[x + nj]) +
+                           rz * (km - c2 + kp));
+        },
+        [&](int x, int, float v, auto) { out[x] = v; });
 }
 
 // coarse inner cell = mean of its 8 children (VCycleMG::Restrict), FP32
@@ -112,60 +166,61 @@ __global__ void k_mx_restrict(float *__restrict__ out, const float *__restrict__
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
-    const int64_t fx = F.Nx, fxy = F.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + C.Nx * j + C.nxy() * k;
-        if (!(flags[x] & kInner)) continue;
-        const int64_t f = (2 * i - 1) + fx * (2 * j - 1) + fxy * (2 * k - 1);
-        out[x] = 0.125f * (in[f] + in[f + 1] + in[f + fx] + in[f + fx + 1] + in[f + fxy] + in[f + fxy + 1] +
-                           in[f + fxy + fx] + in[f + fxy + fx + 1]);
-    }
+    const int fx = (int) F.Nx, fxy = (int) F.nxy();
+    column_planes(i + (int) C.Nx * j, (int) C.nxy(), (int) box.z0, (int) box.z1, flags,
+        [&](int, int k) {
+            const int f = (2 * i - 1) + fx * (2 * j - 1) + fxy * (2 * k - 1);
+            return 0.125f * (in[f] + in[f + 1] + in[f + fx] + in[f + fx + 1] + in[f + fxy] + in[f + fxy + 1] +
+                             in[f + fxy + fx] + in[f + fxy + fx + 1]);
+        },
+        [&](int x, int, float v, auto) { out[x] = v; });
 }
 
 // first Jacobi sweep from a zero correction: every neighbour is zero, so
 // e = w * beta * (-b) on the inner cells
 __global__ void k_mx_jacobi0(float *__restrict__ out, const float *__restrict__ b, const uint8_t *__restrict__ flags,
-                             Level L, Box3 box, CoefF c, const LoopState *__restrict__ pred) {
+                             const uint16_t *__restrict__ push, Level L, Box3 box, CoefF c,
+                             const LoopState *__restrict__ pred) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + nj * j + nk * k;
-        if (!(flags[x] & kInner)) continue;
-        out[x] = c.w * (c.beta * -b[x]);
-    }
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    column_planes(i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int x, int) { return c.w * (c.beta * -b[x]); },
+        [&](int x, int, float v, uint8_t fl) { mx_store(out, fl, push, x, v, nj, nk); });
 }
 
 // fine correction += trilinear prolongation of the coarse correction
 // (weights 27/9/3/1 over 64 of VCycleMG::Prolongate), on the fine inner
 // children of each coarse inner cell, FP32
 __global__ void k_mx_prolong_add(float *__restrict__ fine, const float *__restrict__ in,
-                                 const uint8_t *__restrict__ cflags, const uint8_t *__restrict__ fflags, Level C,
-                                 Level F, Box3 box, const LoopState *__restrict__ pred) {
+                                 const uint8_t *__restrict__ cflags, const uint8_t *__restrict__ fflags,
+                                 const uint16_t *__restrict__ push, Level C, Level F, Box3 fbox,
+                                 const LoopState *__restrict__ pred) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;
-    MX_COLUMN(box);
+    MX_COLUMN(fbox);  // one thread per fine column: fine cell 2c (side +1) or 2c - 1 (side -1) of coarse cell c
     if (!col) return;
-    const int64_t nj = C.Nx, nk = C.nxy();
-    const int64_t fx = F.Nx, fxy = F.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + nj * j + nk * k;
-        if (!(cflags[x] & kInner)) continue;
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const int sx = (c & 1) ? 1 : -1, sy = (c & 2) ? 1 : -1, sz = (c & 4) ? 1 : -1;
-            const int64_t f = (2 * i - (sx < 0)) + fx * (2 * j - (sy < 0)) + fxy * (2 * k - (sz < 0));
-            if (!(fflags[f] & kInner)) continue;
+    const int nj = (int) C.Nx, nk = (int) C.nxy();
+    const int fx = (int) F.Nx, fxy = (int) F.nxy();
+    const int ci = (i + 1) >> 1, cj = (j + 1) >> 1;
+    const int sx = (i & 1) ? -1 : 1, sy = (j & 1) ? -1 : 1;
+    struct Out { float v; uint8_t cf; };
+    column_planes(i + fx * j, fxy, (int) fbox.z0, (int) fbox.z1, fflags,
+        [&](int f, int k) {
+            const int sz = (k & 1) ? -1 : 1;
+            const int x = ci + nj * cj + nk * ((k + 1) >> 1);
             const float v = 0.015625f * (27.f * in[x] + 9.f * in[x + sx] + 9.f * in[x + sy * nj] + 9.f * in[x + sz * nk] +
                                          3.f * in[x + sx + sy * nj] + 3.f * in[x + sx + sz * nk] +
                                          3.f * in[x + sy * nj + sz * nk] + in[x + sx + sy * nj + sz * nk]);
-            fine[f] += v;
-        }
-    }
+            return Out{fine[f] + v, cflags[x]};
+        },
+        [&](int f, int, Out o, uint8_t fl) {
+            if (o.cf & kInner) mx_store(fine, fl, push, f, o.v, fx, fxy);
+        });
 }
 
 // FP64 outer residual r = b - A p on level 0, stored as the FP32 right-hand
@@ -179,18 +234,19 @@ __global__ void k_mx_outer_residual(const double *__restrict__ p, const double *
     __shared__ double smem[32];
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
-    const int64_t nj = L.Nx, nk = L.nxy();
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
     double acc = 0.0;
     if (col) {
-        for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-            const int64_t x = i + nj * j + nk * k;
-            if (!(flags[x] & kInner)) continue;
-            const double c2 = 2 * p[x];
-            const double v = b[x] - (rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) +
-                                     rz * (p[x - nk] - c2 + p[x + nk]));
-            r[x] = (float) v;
-            acc += v * v;
-        }
+        column_march(p, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+            [&](int x, int, double km, double c0, double kp) {
+                const double c2 = 2 * c0;
+                return b[x] - (rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) +
+                               rz * (km - c2 + kp));
+            },
+            [&](int x, int, double v, auto) {
+                r[x] = (float) v;
+                acc += v * v;
+            });
     }
     acc = artss_block_sum(acc, smem);
     if (threadIdx.x == 0 && threadIdx.y == 0)
@@ -205,12 +261,10 @@ __global__ void k_mx_correct(double *__restrict__ p, const float *__restrict__ e
     if (pred && !pred->cond) return;
     MX_COLUMN(box);
     if (!col) return;
-    const int64_t nj = L.Nx, nk = L.nxy();
-    for (int64_t k = box.z0 + blockIdx.z; k <= box.z1; k += gridDim.z) {
-        const int64_t x = i + nj * j + nk * k;
-        if (!(flags[x] & kInner)) continue;
-        p[x] += (double) e[x];
-    }
+    const int nj = (int) L.Nx, nk = (int) L.nxy();
+    column_planes(i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int x, int) { return p[x] + (double) e[x]; },
+        [&](int x, int, double v, auto) { p[x] = v; });
 }
 
 // block partials of sum(x - shift) and sum((x - shift)^2) over the inner cells
@@ -281,42 +335,158 @@ int mx_bc(artss_mixed *m, float *f, int level, const LoopState *pred) {
     return apply_bc_f32(m->ctx, f, level, ARTSS_FIELD_P, pred);
 }
 
-// n_relax weighted-Jacobi sweeps from e = 0 on level l, each followed by the
-// boundary program; the result is left in m->e[l]
-int mx_smooth_from_zero(artss_mixed *m, int l, const LoopState *pred) {
-    artss_ctx *ctx = m->ctx;
-    const Level &L = ctx->lvl[l];
-    const Box3 box = inner_box(L);
-    const CoefF c = coef_f(ctx, l, m->cfg.w);
-    int st;
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi0, mx_grid(box), box_block(), 0, 
-                                         m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
-    ARTSS_LAUNCH_CK(ctx);
-    if ((st = mx_bc(m, m->e[l], l, pred))) return st;
-    for (int s = 1; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, 
-                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
-        ARTSS_LAUNCH_CK(ctx);
-        std::swap(m->e[l], m->t[l]);
-        if ((st = mx_bc(m, m->e[l], l, pred))) return st;
-    }
-    return ARTSS_OK;
+// the boundary program after a smoothing sweep, unless the level's stencils
+// read their boundary neighbours through the program (m->fold[l])
+int mx_bc_sweep(artss_mixed *m, float *f, int level, const LoopState *pred) {
+    return m->fold[level] ? ARTSS_OK : mx_bc(m, f, level, pred);
 }
 
-// n_relax weighted-Jacobi sweeps continuing from m->e[l]
-int mx_smooth(artss_mixed *m, int l, const LoopState *pred) {
+// n_relax red-black Gauss-Seidel sweeps (ARTSS_MIXED_RBGS), in place on
+// m->e[l], each colour followed by the level's boundary program
+int mx_smooth_rbgs(artss_mixed *m, int l, bool from_zero, const LoopState *pred) {
     artss_ctx *ctx = m->ctx;
     const Level &L = ctx->lvl[l];
     const Box3 box = inner_box(L);
     const CoefF c = coef_f(ctx, l, m->cfg.w);
     int st;
     for (int s = 0; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, 
-                                             m->t[l], m->e[l], m->r[l], ctx->d_flags[l], L, box, c, pred);
+        for (int color = 0; color < 2; color++) {
+            const int first = (from_zero && s == 0 && color == 0) ? 1 : 0;
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_rbgs, mx_grid(box), box_block(), 0, m->e[l],
+                             (const float *) m->r[l], ctx->d_flags[l], L, box, c, color, first, pred);
+            ARTSS_LAUNCH_CK(ctx);
+            if ((st = mx_bc(m, m->e[l], l, pred))) return st;
+        }
+    }
+    return ARTSS_OK;
+}
+
+// n_relax weighted-Jacobi sweeps from e = 0 on level l, each followed by the
+// boundary program; the result is left in m->e[l]
+int mx_smooth_from_zero(artss_mixed *m, int l, const LoopState *pred) {
+    if (m->cfg.flags & ARTSS_MIXED_RBGS) return mx_smooth_rbgs(m, l, true, pred);
+    artss_ctx *ctx = m->ctx;
+    const Level &L = ctx->lvl[l];
+    const Box3 box = inner_box(L);
+    const CoefF c = coef_f(ctx, l, m->cfg.w);
+    int st;
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi0, mx_grid(box), box_block(), 0,
+                     m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], L, box, c, pred);
+    ARTSS_LAUNCH_CK(ctx);
+    if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
+    for (int s = 1; s < m->cfg.n_relax; s++) {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, m->t[l],
+                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l],
+                         L, box, c, pred);
         ARTSS_LAUNCH_CK(ctx);
         std::swap(m->e[l], m->t[l]);
-        if ((st = mx_bc(m, m->e[l], l, pred))) return st;
+        if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
     }
+    return ARTSS_OK;
+}
+
+// n_relax weighted-Jacobi sweeps continuing from m->e[l]
+int mx_smooth(artss_mixed *m, int l, const LoopState *pred) {
+    if (m->cfg.flags & ARTSS_MIXED_RBGS) return mx_smooth_rbgs(m, l, false, pred);
+    artss_ctx *ctx = m->ctx;
+    const Level &L = ctx->lvl[l];
+    const Box3 box = inner_box(L);
+    const CoefF c = coef_f(ctx, l, m->cfg.w);
+    int st;
+    for (int s = 0; s < m->cfg.n_relax; s++) {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, m->t[l],
+                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l],
+                         L, box, c, pred);
+        ARTSS_LAUNCH_CK(ctx);
+        std::swap(m->e[l], m->t[l]);
+        if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
+    }
+    return ARTSS_OK;
+}
+
+// Push masks of levels 0 .. L-2 from the inner bitmaps and the pressure
+// boundary programs with every value zero (x_t = +-x_root after chain
+// folding).  Every boundary cell that a smoothing or residual stencil reads
+// (a face neighbour of an inner cell) must take its value from an inner face
+// neighbour, which then writes it with each of its own values.  A level where
+// that fails (a root that is not inner, not face-adjacent or itself written by
+// the program, an inner target) or a solver with ARTSS_MIXED_RBGS /
+// ARTSS_MIXED_BC_LAUNCH launches the program after each sweep instead, with a
+// mask of inner bits only.
+int mx_build_tables(artss_mixed *m) {
+    artss_ctx *ctx = m->ctx;
+    const bool allow = !(m->cfg.flags & (ARTSS_MIXED_RBGS | ARTSS_MIXED_BC_LAUNCH));
+    for (int l = 0; l + 1 < m->L; l++) {
+        const Level &L = ctx->lvl[l];
+        const int64_t n = L.size();
+        std::vector<uint16_t> pat((size_t) n, 0);  // 2 bits per direction, as a push pattern
+        const std::vector<bool> &inner = ctx->h_inner[l];
+        const bool have_inner = (int64_t) inner.size() == n;
+        bool fold = allow && have_inner;
+        const BcProgram &p = ctx->bc[l][ARTSS_FIELD_P];
+        if (fold && p.present && p.n) {
+            // final (root, sign) of every target, the program applied wave by wave
+            std::unordered_map<int64_t, std::pair<int64_t, int>> res;
+            res.reserve((size_t) p.n * 2);
+            for (int64_t a = 0; a < p.n; a++) {
+                int64_t r = p.h_root[(size_t) a];
+                int sg = p.h_sign[(size_t) a];
+                const auto it = res.find(r);
+                if (it != res.end()) {
+                    r = it->second.first;
+                    sg *= it->second.second;
+                }
+                res[p.h_target[(size_t) a]] = {r, sg};
+            }
+            const int64_t off[6] = {-1, 1, -L.Nx, L.Nx, -L.nxy(), L.nxy()};
+            for (const auto &kv : res) {
+                const int64_t t = kv.first, r = kv.second.first;
+                const int sg = kv.second.second;
+                if (inner[(size_t) t]) { fold = false; break; }
+                bool read = false;  // t is a face neighbour of an inner cell
+                for (int d = 0; d < 6 && !read; d++) {
+                    const int64_t x = t - off[d];
+                    read = x >= 0 && x < n && inner[(size_t) x];
+                }
+                if (!read) continue;
+                int dir = -1;  // t = r + off[dir]
+                for (int d = 0; d < 6; d++)
+                    if (r + off[d] == t) dir = d;
+                if (dir < 0 || r < 0 || r >= n || !inner[(size_t) r] || res.count(r)) { fold = false; break; }
+                pat[(size_t) r] = (uint16_t) (pat[(size_t) r] | ((sg > 0 ? 1u : 2u) << (2 * dir)));
+            }
+        }
+        // distinct patterns -> ids 1..127
+        std::vector<uint8_t> nbm((size_t) n, 0);
+        std::vector<uint16_t> push(128, 0);
+        std::unordered_map<uint16_t, int> ids;
+        for (int64_t x = 0; x < n && fold; x++) {
+            const uint16_t pv = pat[(size_t) x];
+            if (!pv) continue;
+            auto it = ids.find(pv);
+            if (it == ids.end()) {
+                if (ids.size() >= 127) { fold = false; break; }
+                it = ids.emplace(pv, (int) ids.size() + 1).first;
+                push[(size_t) it->second] = pv;
+            }
+            nbm[(size_t) x] = (uint8_t) (it->second << 1);
+        }
+        if (!fold) {
+            std::fill(push.begin(), push.end(), (uint16_t) 0);
+            std::fill(nbm.begin(), nbm.end(), (uint8_t) 0);
+        }
+        if (have_inner)
+            for (int64_t x = 0; x < n; x++)
+                if (inner[(size_t) x]) nbm[(size_t) x] = (uint8_t) (nbm[(size_t) x] | 1u);
+        m->fold[l] = fold;
+        if (!m->nbm[l]) ARTSS_CK(cudaMalloc(&m->nbm[l], (size_t) n));
+        if (!m->push[l]) ARTSS_CK(cudaMalloc(&m->push[l], 128 * sizeof(uint16_t)));
+        ARTSS_CK(cudaMemcpyAsync(m->push[l], push.data(), 128 * sizeof(uint16_t), cudaMemcpyHostToDevice, ctx->stream));
+        ARTSS_CK(cudaMemcpyAsync(m->nbm[l], nbm.data(), (size_t) n, cudaMemcpyHostToDevice, ctx->stream));
+        // the host vectors die with this iteration
+        ARTSS_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    m->geom_version = ctx->geom_version;
     return ARTSS_OK;
 }
 
@@ -330,10 +500,10 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
         if ((st = mx_smooth_from_zero(m, l, pred))) return st;
         const Level &L = ctx->lvl[l];
         const Box3 box = inner_box(L);
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_residuum, mx_grid(box), box_block(), 0, 
-                                               m->q[l], m->e[l], m->r[l], ctx->d_flags[l], L, box,
-                                               (float) (1. / (g.dx[l] * g.dx[l])), (float) (1. / (g.dy[l] * g.dy[l])),
-                                               (float) (1. / (g.dz[l] * g.dz[l])), pred);
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_residuum, mx_grid(box), box_block(), 0, m->q[l],
+                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], L, box,
+                         (float) (1. / (g.dx[l] * g.dx[l])),
+                         (float) (1. / (g.dy[l] * g.dy[l])), (float) (1. / (g.dz[l] * g.dz[l])), pred);
         ARTSS_LAUNCH_CK(ctx);
         if ((st = mx_bc(m, m->q[l], l, pred))) return st;
         const Level &C = ctx->lvl[l + 1];
@@ -359,13 +529,18 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
             return st;
     }
     for (int l = Lc - 1; l >= 0; l--) {
+        // the prolongation reads the coarse correction's boundary cells (edges
+        // and corners too): the level's program once, where the sweeps skipped it
+        if (l + 1 < Lc && m->fold[l + 1] && (st = mx_bc(m, m->e[l + 1], l + 1, pred))) return st;
         const Level &C = ctx->lvl[l + 1], &F = ctx->lvl[l];
-        const Box3 cbox = inner_box(C);
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add, mx_grid(cbox), box_block(), 0, 
-                                                 m->e[l], m->e[l + 1], ctx->d_flags[l + 1], ctx->d_flags[l], C, F,
-                                                 cbox, pred);
+        // the fine children 2c - 1, 2c of the coarse inner box, within the fine inner box
+        const Box3 fbox{std::max(F.i1, 2 * C.i1 - 1), std::min(F.i2, 2 * C.i2), std::max(F.j1, 2 * C.j1 - 1),
+                        std::min(F.j2, 2 * C.j2), std::max(F.k1, 2 * C.k1 - 1), std::min(F.k2, 2 * C.k2)};
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add, mx_grid(fbox), box_block(), 0,
+                         m->e[l], (const float *) m->e[l + 1], (const uint8_t *) ctx->d_flags[l + 1],
+                         (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], C, F, fbox, pred);
         ARTSS_LAUNCH_CK(ctx);
-        if ((st = mx_bc(m, m->e[l], l, pred))) return st;
+        if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
         if ((st = mx_smooth(m, l, pred))) return st;
     }
     return ARTSS_OK;
@@ -434,6 +609,7 @@ int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed *
         }
     }
     if (!st) st = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? ARTSS_OK : cuda_fail(cudaGetLastError(), "sync");
+    if (!st) st = mx_build_tables(m);
     if (st) { artss_mixed_destroy(m); return st; }
     *out = m;
     return ARTSS_OK;
@@ -442,9 +618,12 @@ int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed *
 int artss_mixed_destroy(artss_mixed *m) {
     if (!m) return ARTSS_OK;
     cudaStreamSynchronize(m->ctx->stream);
-    for (int l = 0; l <= kMaxLevel; l++)
+    for (int l = 0; l <= kMaxLevel; l++) {
         for (float *f : {m->r[l], m->q[l], m->e[l], m->t[l]})
             if (f) cudaFree(f);
+        if (m->nbm[l]) cudaFree(m->nbm[l]);
+        if (m->push[l]) cudaFree(m->push[l]);
+    }
     delete m;
     return ARTSS_OK;
 }
@@ -475,6 +654,11 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
     int st;
     const dim3 grid = mx_grid(box);
     if ((st = check_reduce_blocks(grid))) return st;
+    if (m->geom_version != ctx->geom_version) {
+        // cell lists or boundary programs changed since the tables were built
+        if (ctx->capturing) { set_error("the mixed solver's boundary tables are stale; solve once before capturing"); return ARTSS_ERR_ARG; }
+        if ((st = mx_build_tables(m))) return st;
+    }
     const int nb = (int) (grid.x * grid.y * grid.z);
     // ||b|| for the relative stopping rule: on the host, or (inside a capture)
     // kept in loop slot kSlotSum and applied by the loop step on the device

@@ -415,8 +415,30 @@ def train(net: UNet, samples, epochs: int, lr: float = 1e-3, seed: int = 0):
     return history
 
 
+def min_residual_step(lib, ctx, guess, p_prev, d, rhs, zero) -> float:
+    """guess = p_prev + alpha d with alpha minimising ||rhs - A guess||_2 over
+    the inner cells: alpha = (r . A d) / (A d . A d), r = rhs - A p_prev, the
+    dot product from three residual norms (polarisation identity; the pressure's
+    boundary values are zero, so A is linear on d).  The guess's residual is
+    never above the previous pressure's.  Returns alpha."""
+    _ck(lib.artss_apply_boundary(ctx, d, 0, 4), "bc")
+    ad, _ = _resnorm(lib, ctx, d, zero)             # ||A d||
+    r0, _ = _resnorm(lib, ctx, p_prev, rhs)         # ||r||
+    _ck(lib.artss_copy(ctx, guess, p_prev, 0), "copy")
+    _ck(lib.artss_add_field(ctx, guess, d, 0), "add")
+    _ck(lib.artss_apply_boundary(ctx, guess, 0, 4), "bc")
+    r1, _ = _resnorm(lib, ctx, guess, rhs)          # ||r - A d||
+    alpha = (r0 * r0 + ad * ad - r1 * r1) / (2.0 * ad * ad) if ad > 0 else 0.0
+    _ck(lib.artss_copy(ctx, guess, p_prev, 0), "copy")
+    if alpha != 0.0:
+        _ck(lib.artss_scale(ctx, d, alpha, 0), "scale")
+        _ck(lib.artss_add_field(ctx, guess, d, 0), "add")
+    _ck(lib.artss_apply_boundary(ctx, guess, 0, 4), "bc")
+    return alpha
+
+
 def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, device: int = 0, project: int = 2,
-             with_plain: bool = False):
+             with_plain: bool = False, min_residual: bool = True):
     """Per timestep of unseen scenes: the pressure equation solved to 1e-8 by
     the mixed-precision solver from (a) the previous pressure and (b) the
     network's guess p_prev + correction, the correction restricted `project`
@@ -488,9 +510,12 @@ def evaluate(net: UNet, seeds, steps: int, warmup: int, dims, tmpdir: str, devic
             _ck(lib.artss_nn_apply(ctx, 0, _p(out), 16, smp.zero, 1.0 / s_t, corr), "apply")
             if project:
                 _ck(lib.artss_coarse_project(ctx, corr, project), "project")
-            _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
-            _ck(lib.artss_add_field(ctx, guess, corr, 0), "add")
-            _ck(lib.artss_apply_boundary(ctx, guess, 0, 4), "bc")
+            if min_residual:
+                res.setdefault("alpha", []).append(min_residual_step(lib, ctx, guess, smp.p_prev, corr, rhs, smp.zero))
+            else:
+                _ck(lib.artss_copy(ctx, guess, smp.p_prev, 0), "copy")
+                _ck(lib.artss_add_field(ctx, guess, corr, 0), "add")
+                _ck(lib.artss_apply_boundary(ctx, guess, 0, 4), "bc")
             e2 = torch.cuda.Event(enable_timing=True)
             e2.record(stream)
             r_g, _ = _resnorm(lib, ctx, guess, rhs)

@@ -46,6 +46,7 @@ def parse_args():
                     help="poisson: ms per pressure solve to a 1e-8 relative residual, plain FP64 VCycleMG "
                          "against the mixed-precision solve, on the 256^3 Neumann problem with box obstacles")
     ap.add_argument("--poisson-n", type=int, default=256)
+    ap.add_argument("--poisson-levels", type=int, default=5)
     ap.add_argument("--channel-nx", type=int, default=256,
                     help="channel workload size nx x nx/2 x nx/2 (256: the benchmarked scene; smaller sizes for "
                          "profiler captures)")
@@ -395,7 +396,8 @@ def run_poisson(args, dist):
 
     torch.cuda.set_device(dist.local)
     n = args.poisson_n
-    sc = scenes.poisson_boxes(n=n, seed=args.seed, n_level=5)
+    nl = args.poisson_levels
+    sc = scenes.poisson_boxes(n=n, seed=args.seed, n_level=nl)
     xml = scenes.write(sc, os.path.join(tempfile.mkdtemp(prefix="artss_poisson_"), "poisson.xml"))
     geom = A.Geometry(xml)
     ctx = A.Context(geom, device=dist.local)
@@ -403,16 +405,23 @@ def run_poisson(args, dist):
     stream = torch.cuda.ExternalStream(cuda.artss_ctx_stream(ctx.h), device=torch.device("cuda", dist.local))
     inner = geom.list("inner", 0)
     b_raw = scenes.poisson_rhs(inner, ctx.size(), 1000 + args.seed)
-    db, b = A.consistent_rhs(ctx, b_raw, 5)
+    db, b = A.consistent_rhs(ctx, b_raw, nl)
     dp = ctx.field()
     mg = C.c_void_p()
-    mcfg = A.MgCfg(5, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
+    mcfg = A.MgCfg(nl, 2, 100, 2, 1e-8, 0, 0, 100, 1e-8, 0.6666666667)
     A.cuda_check(cuda.artss_mg_create(ctx.h, C.byref(mcfg), C.byref(mg)), "mg")
     mx = C.c_void_p()
     # Jacobi weight 6/7 (the smoothing-optimal weight of the 7-point operator);
     # coarse red-black SOR to 1e-2 relative, at most 20 sweeps
-    xcfg = A.MixedCfg(5, 2, 1, A.MIXED_REMOVE_MEAN, 6.0 / 7.0, 0.0, 1e-2, 20, 1e-8, 200)
+    xcfg = A.MixedCfg(nl, 2, 1, A.MIXED_REMOVE_MEAN, 6.0 / 7.0, 0.0, 1e-2, 20, 1e-8, 200)
     A.cuda_check(cuda.artss_mixed_create(ctx.h, C.byref(xcfg), C.byref(mx)), "mixed")
+    # red-black Gauss-Seidel smoothing (w = 1), one or two sweeps each side
+    mx_rb = {}
+    for nr in (1, 2):
+        h = C.c_void_p()
+        rcfg = A.MixedCfg(nl, nr, 1, A.MIXED_REMOVE_MEAN | A.MIXED_RBGS, 1.0, 0.0, 1e-2, 20, 1e-8, 200)
+        A.cuda_check(cuda.artss_mixed_create(ctx.h, C.byref(rcfg), C.byref(h)), "mixed rbgs")
+        mx_rb[nr] = h
 
     def plain(st):
         return cuda.artss_mg_solve_rel(mg, dp, db, 1e-8, 2000, C.byref(st))
@@ -420,8 +429,12 @@ def run_poisson(args, dist):
     def mixed(st):
         return cuda.artss_mixed_solve(mx, dp, db, C.byref(st))
 
+    def rbgs(nr):
+        return lambda st: cuda.artss_mixed_solve(mx_rb[nr], dp, db, C.byref(st))
+
     res = {}
-    for name, fn in (("plain_fp64", plain), ("mixed", mixed)):
+    for name, fn in (("plain_fp64", plain), ("mixed", mixed), ("mixed_rbgs_v11", rbgs(1)),
+                     ("mixed_rbgs_v22", rbgs(2))):
         st = A.SolveStats()
         for _ in range(args.warmup):
             A.cuda_check(cuda.artss_fill(ctx.h, dp, 0, 0.0), "fill")
@@ -451,6 +464,8 @@ def run_poisson(args, dist):
                      "cycles": int(st.cycles), "rel_residual": float(st.rel_residual),
                      "kernel_launches_ms": dict(sorted(fam.items(), key=lambda kv: -kv[1][1]))}
     cuda.artss_mixed_destroy(mx)
+    for h in mx_rb.values():
+        cuda.artss_mixed_destroy(h)
     cuda.artss_mg_destroy(mg)
     ctx.close()
     ms = dist.max(res["mixed"]["ms_per_solve"])
@@ -467,13 +482,17 @@ def run_poisson(args, dist):
         "vs_baseline": None,
         "dtype": "f32 V-cycles in f64 defect correction",
         "data": "synthetic",
-        "config": {"workload": f"poisson_{n}cubed_neumann_boxes", "cells": f"{n}x{n}x{n}",
+        "config": {"workload": f"poisson_{n}cubed_neumann_boxes_{nl}levels", "cells": f"{n}x{n}x{n}",
                    "inner_cells": int(len(inner)), "boxes": len(sc.obstacles), "seed": args.seed,
-                   "levels": 5, "rhs": "N(0,1) on fluid cells, zero mean, made consistent with the discrete operator (b = A p_inf, "
+                   "levels": nl, "rhs": "N(0,1) on fluid cells, zero mean, made consistent with the discrete operator (b = A p_inf, "
                           "relative change ~1e-4)", "start": "p = 0"},
         "plain_fp64": res["plain_fp64"],
         "mixed": res["mixed"],
+        "mixed_rbgs_v11": res["mixed_rbgs_v11"],
+        "mixed_rbgs_v22": res["mixed_rbgs_v22"],
         "speedup_vs_plain_fp64": res["plain_fp64"]["ms_per_solve"] / res["mixed"]["ms_per_solve"],
+        "speedup_rbgs_vs_plain_fp64": {k: res["plain_fp64"]["ms_per_solve"] / res[k]["ms_per_solve"]
+                                       for k in ("mixed_rbgs_v11", "mixed_rbgs_v22")},
     }
 
 

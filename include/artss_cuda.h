@@ -425,6 +425,13 @@ int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_to
  * mean-free b is not enough (the obstacle edge and corner cells make A
  * non-symmetric) -- artss_laplacian gives consistent right-hand sides. */
 #define ARTSS_MIXED_REMOVE_MEAN 1
+/* smoothing by red-black Gauss-Seidel (in place, w the over-relaxation
+ * weight, boundary program after each colour) instead of weighted Jacobi */
+#define ARTSS_MIXED_RBGS 2
+/* the FP32 levels launch the boundary program after every sweep; without it
+ * (and without ARTSS_MIXED_RBGS) their stencils read boundary neighbours
+ * through the program instead (same values, fewer launches) */
+#define ARTSS_MIXED_BC_LAUNCH 4
 typedef struct {
     int32_t n_level;          /* V-cycle levels 0 .. n_level-1; the coarse solve is on n_level-1 */
     int32_t n_relax;          /* weighted-Jacobi sweeps before and after each coarse correction */
