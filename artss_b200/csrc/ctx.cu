@@ -760,7 +760,7 @@ int artss_set_cell_lists(artss_ctx *ctx, int level, const int64_t *inner, int64_
     ctx->geom_version++;
     if (level == 0) {
         // the sweep's obstacle table describes the old lists
-        for (int t = 0; t < 2; t++) {
+        for (int t = 0; t < 3; t++) {
             if (ctx->d_sweep3_obst[t]) cudaFree(ctx->d_sweep3_obst[t]);
             ctx->d_sweep3_obst[t] = nullptr;
             ctx->sweep3_obst_state[t] = 0;

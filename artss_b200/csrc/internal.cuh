@@ -134,8 +134,8 @@ struct artss_ctx {
     uint64_t geom_version = 0;                                   // bumped by every cell-list or boundary-program change
     // tile columns x planes of level 0 whose row-pair sweep tile (+ ring) holds a
     // box cell that is not inner (k_cgs_sweep3); built on first use
-    uint8_t *d_sweep3_obst[2] = {nullptr, nullptr};              // per tile height (64 x 8, 64 x 6)
-    int sweep3_obst_state[2] = {0, 0};                           // 0 not built, 1 built, 2 every box cell inner
+    uint8_t *d_sweep3_obst[3] = {nullptr, nullptr, nullptr};     // per tile height (64 x 8, 64 x 6, 64 x 16)
+    int sweep3_obst_state[3] = {0, 0, 0};                        // 0 not built, 1 built, 2 every box cell inner
     float *cgsm_w = nullptr;                                     // FP32 defect / correction of artss_diffuse_cgs_mixed
     int64_t cgsm_n = 0;
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape
@@ -268,14 +268,15 @@ inline Box3 domain_box(const Level &L) { return {L.i1 - 1, L.i2 + 1, L.j1 - 1, L
 // U (default kColU) planes per round.  For every plane of a round `value(q, k)` runs first
 // (the cells of a column are independent, so their loads are in flight
 // together), then `put(q, k, v, flag)` for the planes whose cell carries kInner, in
-// ascending k, with the flag value already loaded.  A round's planes past z1 evaluate the round's first plane again
+// ascending k, with the flag value already loaded (`bit`: the flag bit that
+// selects the cells, kInner by default).  A round's planes past z1 evaluate the round's first plane again
 // and store nothing.  Every cell of an inner box has its six neighbours inside
 // the level's array, so `value` reads them without a check.  32-bit indices:
 // artss_ctx_create rejects levels of 2^31 cells or more.
 constexpr int kColU = 4;
 template <int U = kColU, class FlagT, class V, class P>
 __device__ __forceinline__ void column_planes(int base, int nk, int z0, int z1, const FlagT *__restrict__ flags,
-                                              V value, P put) {
+                                              V value, P put, unsigned bit = kInner) {
     const int gz = (int) gridDim.z;
     using T = decltype(value(0, 0));
     for (int k0 = z0 + (int) blockIdx.z; k0 <= z1; k0 += U * gz) {
@@ -290,7 +291,7 @@ __device__ __forceinline__ void column_planes(int base, int nk, int z0, int z1, 
             kk[u] = in ? k : k0;
             q[u] = base + nk * kk[u];
             fl[u] = flags[q[u]];
-            ok[u] = in && (fl[u] & kInner);
+            ok[u] = in && (fl[u] & bit);
             v[u] = value(q[u], kk[u]);
         }
 #pragma unroll

@@ -120,19 +120,19 @@ __global__ void k_smagorinsky(double *__restrict__ ev, const double *__restrict_
     ARTSS_COLUMN(box);
     if (!col) return;
     const int ni = 1, nj = (int) L.Nx, nk = (int) L.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + nk * k;
-        if (!(flags[q] & kInner)) continue;
-        const double S11 = (u[q + ni] - u[q - ni]) * 0.5 * rdx;
-        const double S22 = (v[q + nj] - v[q - nj]) * 0.5 * rdy;
-        const double S33 = (w[q + nk] - w[q - nk]) * 0.5 * rdz;
-        const double S12 = 0.5 * ((u[q + nj] - u[q - nj]) * 0.5 * rdy + (v[q + ni] - v[q - ni]) * 0.5 * rdx);
-        const double S13 = 0.5 * ((u[q + nk] - u[q - nk]) * 0.5 * rdz + (w[q + ni] - w[q - ni]) * 0.5 * rdx);
-        const double S23 = 0.5 * ((v[q + nk] - v[q - nk]) * 0.5 * rdz + (w[q + nj] - w[q - nj]) * 0.5 * rdy);
-        const double S_bar = sqrt(2. * (S11 * S11 + S22 * S22 + S33 * S33
-                                        + 2. * (S12 * S12) + 2. * (S13 * S13) + 2. * (S23 * S23)));
-        ev[q] = cs2d2 * S_bar;
-    }
+    column_planes<2>(i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int q, int) {
+            const double S11 = (u[q + ni] - u[q - ni]) * 0.5 * rdx;
+            const double S22 = (v[q + nj] - v[q - nj]) * 0.5 * rdy;
+            const double S33 = (w[q + nk] - w[q - nk]) * 0.5 * rdz;
+            const double S12 = 0.5 * ((u[q + nj] - u[q - nj]) * 0.5 * rdy + (v[q + ni] - v[q - ni]) * 0.5 * rdx);
+            const double S13 = 0.5 * ((u[q + nk] - u[q - nk]) * 0.5 * rdz + (w[q + ni] - w[q - ni]) * 0.5 * rdx);
+            const double S23 = 0.5 * ((v[q + nk] - v[q - nk]) * 0.5 * rdz + (w[q + nj] - w[q - nj]) * 0.5 * rdy);
+            const double S_bar = sqrt(2. * (S11 * S11 + S22 * S22 + S33 * S33
+                                            + 2. * (S12 * S12) + 2. * (S13 * S13) + 2. * (S23 * S23)));
+            return cs2d2 * S_bar;
+        },
+        [&](int q, int, double v_, uint8_t) { ev[q] = v_; });
 }
 
 // ExplicitDiffuse::ExplicitStep: laminar (ExplicitDiffuse.cpp:50-76, rd* = D / (d* d*)
@@ -231,14 +231,14 @@ __global__ void k_divergence(double *__restrict__ out, const double *__restrict_
     ARTSS_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + nk * k;
-        if (!(flags[q] & kInner)) continue;
-        const double a = hx * (u[q + 1] - u[q - 1]);
-        const double b = hy * (v[q + nj] - v[q - nj]);
-        const double c = hz * (w[q + nk] - w[q - nk]);
-        out[q] = a + b + c;
-    }
+    column_planes(i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int q, int) {
+            const double a = hx * (u[q + 1] - u[q - 1]);
+            const double b = hy * (v[q + nj] - v[q - nj]);
+            const double c = hz * (w[q + nk] - w[q - nk]);
+            return a + b + c;
+        },
+        [&](int q, int, double v_, uint8_t) { out[q] = v_; });
 }
 
 // zero the ghost ring of the computational domain (IPressure.cpp:69-104)
@@ -263,13 +263,17 @@ __global__ void k_projection(double *__restrict__ ou, double *__restrict__ ov, d
     ARTSS_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + nk * k;
-        if (!(flags[q] & kInner)) continue;
-        ou[q] = us[q] - hx * (p[q + 1] - p[q - 1]);
-        ov[q] = vs[q] - hy * (p[q + nj] - p[q - nj]);
-        ow[q] = ws[q] - hz * (p[q + nk] - p[q - nk]);
-    }
+    struct UVW { double u, v, w; };
+    column_planes<2>(i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        [&](int q, int) {
+            return UVW{us[q] - hx * (p[q + 1] - p[q - 1]), vs[q] - hy * (p[q + nj] - p[q - nj]),
+                       ws[q] - hz * (p[q + nk] - p[q - nk])};
+        },
+        [&](int q, int, UVW r, uint8_t) {
+            ou[q] = r.u;
+            ov[q] = r.v;
+            ow[q] = r.w;
+        });
 }
 
 // ------------------------------------------------------------ sources
@@ -281,11 +285,9 @@ __global__ void k_buoyancy(double *__restrict__ f, const double *__restrict__ T,
     pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + (int) L.nxy() * k;
-        if (!(flags[q] & kDomain)) continue;
-        f[q] = nbeta * (T[q] - Ta[q]) * g;
-    }
+    column_planes(i + (int) L.Nx * j, (int) L.nxy(), (int) box.z0, (int) box.z1, flags,
+        [&](int q, int) { return nbeta * (T[q] - Ta[q]) * g; },
+        [&](int q, int, double v_, uint8_t) { f[q] = v_; }, kDomain);
 }
 
 // ExplicitEulerSource.cpp:92-96
@@ -295,11 +297,9 @@ __global__ void k_add_source(double *__restrict__ out, const double *__restrict_
     pdl_trigger();
     ARTSS_COLUMN(box);
     if (!col) return;
-    for (int k = (int) box.z0 + (int) blockIdx.z; k <= (int) box.z1; k += (int) gridDim.z) {
-        const int q = i + (int) L.Nx * j + (int) L.nxy() * k;
-        if (!(flags[q] & kInner)) continue;
-        out[q] += dt * S[q];
-    }
+    column_planes(i + (int) L.Nx * j, (int) L.nxy(), (int) box.z0, (int) box.z1, flags,
+        [&](int q, int) { return out[q] + dt * S[q]; },
+        [&](int q, int, double v_, uint8_t) { out[q] = v_; });
 }
 
 // ------------------------------------------------------------ diffusion
@@ -935,9 +935,10 @@ k_cgs_sweep_tma2(const __grid_constant__ CUtensorMap tm_x, const __grid_constant
 // read its previous plane (I - NSX for x, I - NSB for b and EV); with
 // NSX >= AHEAD + 5 and NSB >= AHEAD + 4 that step lies before the producer's
 // current one, so the producer waits for warps at most one step behind it.
-template <int TY_, int NSX_, int NSB_, int AHEAD_>
+template <int TY_, int NSX_, int NSB_, int AHEAD_, int BPS_ = 2>
 struct S3Cfg {
     static constexpr int TY = TY_, NSX = NSX_, NSB = NSB_, AHEAD = AHEAD_;
+    static constexpr int BPS = BPS_;                // resident blocks per multiprocessor
     static constexpr int Pairs = (TY + 2) / 2;      // row pairs (tile + ring rows)
     static constexpr int Warps = Pairs + 1;         // row-pair warps (two x columns per lane) + side warp
     static constexpr int Threads = 32 * Warps;
@@ -948,14 +949,15 @@ struct S3Cfg {
     static constexpr unsigned BytesX = XW * XH * sizeof(double), BytesB = BW * BH * sizeof(double);
     static_assert(TY % 2 == 0 && TY + 2 <= 31, "row pairs; side lanes and the producer lane fit one warp");
     static_assert((PlaneX * 8) % 128 == 0 && (PlaneB * 8) % 128 == 0, "slots stay 128-byte aligned");
-    static_assert(NSX >= AHEAD + 5 && NSB >= AHEAD + 4 && NSX <= 8, "ring depths (barrier rings of 8)");
+    static_assert(NSX >= AHEAD + 5 && NSB >= AHEAD + 4 && NSX <= 16, "ring depths (barrier rings of 16)");
     static size_t smem(bool turb) {
         return (size_t) PlaneX * NSX * sizeof(double) + (size_t) PlaneB * NSB * (turb ? 2 : 1) * sizeof(double);
     }
 };
 using S3Tall = S3Cfg<8, 7, 6, 2>;   // 64 x 8 tiles, 192 threads, 112.9 KB (turbulent)
 using S3Flat = S3Cfg<6, 8, 7, 3>;   // 64 x 6 tiles, 160 threads, 105.2 KB, one step more lookahead
-constexpr int kS3Bars = 8;          // mbarriers per ring (full, step, red)
+using S3Wide = S3Cfg<16, 8, 7, 3, 1>;    // 64 x 16 tiles, 320 threads, one block per multiprocessor (226 KB)
+constexpr int kS3Bars = 16;         // mbarriers per ring (full, step, red)
 constexpr int kS3MinPlanes = 8;     // planes per block at least
 static_assert(S3Tall::XH == kTmaBoxY && S3Tall::BW == kSt2BoxBX && S3Tall::BH == kSt2BoxBY, "maps shared");
 
@@ -1004,7 +1006,7 @@ struct S3Par {
     static constexpr int value = V;
 };
 
-// Waits on phase (g >> 3) & 1 of a ring barrier (kS3Bars = 8 per ring): each
+// Waits on phase (g >> 4) & 1 of a ring barrier (kS3Bars = 16 per ring): each
 // try_wait may suspend the thread in hardware for up to kS3SuspendNs until the
 // phase completes, so a waiting warp does not spin on the issue slots; bounded
 // by kS3Polls tries.
@@ -1025,13 +1027,13 @@ __device__ __noinline__ bool mbar_wait_s3_slow(uint64_t *bar, unsigned parity) {
     return false;
 }
 __device__ __forceinline__ bool mbar_wait_s3(uint64_t *bar, int g) {
-    const unsigned parity = (unsigned) (g >> 3) & 1u;
+    const unsigned parity = (unsigned) (g >> 4) & 1u;
     return mbar_try_sleep(bar, parity) || mbar_wait_s3_slow(bar, parity);
 }
-static_assert(kS3Bars == 8, "barrier rings are indexed with & 7 and >> 3");
+static_assert(kS3Bars == 16, "barrier rings are indexed with & 15 and >> 4");
 
 template <bool TURB, class G3>
-__global__ void __launch_bounds__(G3::Threads, 2)
+__global__ void __launch_bounds__(G3::Threads, G3::BPS)
 k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_e, double *__restrict__ out, const uint8_t *__restrict__ flags,
              const uint8_t *__restrict__ obst, Level L, Box3 box, DiffCoef c, int ncx, int ncy,
@@ -1087,12 +1089,12 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
             // the slots of plane I held planes I-NSX (x) and I-NSB (b, EV): wait
             // until every warp has finished the last step that read them
             int d = -1;
-            if (I >= G3::NSX) d = deathx[(I - G3::NSX) & 7];
-            if (I >= G3::NSB) d = max(d, deathb[(I - G3::NSB) & 7]);
-            if (d >= 0 && !(ok = mbar_wait_s3(&stepdone[d & 7], d))) break;
+            if (I >= G3::NSX) d = deathx[(I - G3::NSX) & 15];
+            if (I >= G3::NSB) d = max(d, deathb[(I - G3::NSB) & 15]);
+            if (d >= 0 && !(ok = mbar_wait_s3(&stepdone[d & 15], d))) break;
             const int x0 = bx0 + 64 * (pr.col % ncx), y0 = by0 + TY * (pr.col / ncx);
             const int k = pr.ka - 2 + pr.q;
-            const int bar = I & 7;
+            const int bar = I & 15;
             // x of local plane q is read on steps q-2 .. q+2, b and EV on q-1 and q+1 (within 0 .. n+2)
             deathx[bar] = pr.S0 + min(pr.q + 2, n + 2);
             deathb[bar] = pr.S0 + min(pr.q + 1, n + 2);
@@ -1196,7 +1198,7 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
                 if (tr[Q] && kr >= ka && kr <= kb) acc += (onr0 ? rr0 : 0.0) + (onr1 ? rr1 : 0.0);
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(&reddone[(S + (kr - ka + 1)) & 7]);
+            if (lane == 0) mbar_arrive(&reddone[(S + (kr - ka + 1)) & 15]);
             if (K) {
                 acc += (onb0 ? rb0 : 0.0) + (onb1 ? rb1 : 0.0);
                 const double vb0 = onb0 ? nb0 : ob0, vb1 = onb1 ? nb1 : ob1;
@@ -1221,13 +1223,13 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
             }
             if (ok) {
                 if (s == 0)
-                    ok = mbar_wait_s3(&full[P & 7], P) && mbar_wait_s3(&full[(P + 1) & 7], P + 1) &&
-                         mbar_wait_s3(&full[(P + 2) & 7], P + 2);
+                    ok = mbar_wait_s3(&full[P & 15], P) && mbar_wait_s3(&full[(P + 1) & 15], P + 1) &&
+                         mbar_wait_s3(&full[(P + 2) & 15], P + 2);
                 else if (s + 2 <= n + 3)
-                    ok = mbar_wait_s3(&full[(P + s + 2) & 7], P + s + 2);
+                    ok = mbar_wait_s3(&full[(P + s + 2) & 15], P + s + 2);
             }
             const bool do_k = !side && s >= 3;  // black on plane kr - 2 (local plane s - 1)
-            if (ok && do_k) ok = mbar_wait_s3(&reddone[(Sg - 2) & 7], Sg - 2);
+            if (ok && do_k) ok = mbar_wait_s3(&reddone[(Sg - 2) & 15], Sg - 2);
             if (!ok) return;
             const bool do_r = s <= n + 1 && kr >= bz0 && kr <= bz1;  // red on plane kr (local plane s + 1)
             using T = S3Par<1>;
@@ -1238,7 +1240,7 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
             else updates(par, F{}, F{}, kr);
             fence_proxy_async();  // this thread's shared-memory writes before slot refills
             __syncwarp();
-            if (lane == 0) mbar_arrive(&stepdone[Sg & 7]);
+            if (lane == 0) mbar_arrive(&stepdone[Sg & 15]);
             // rotate the slot rings and the obstacle history to step s + 1
             xm3 = xm2; xm2 = xm1; xm1 = x00; x00 = xp1;
             xp1 = xp1 + G3::PlaneX == G3::NSX * G3::PlaneX ? 0 : xp1 + G3::PlaneX;
@@ -1257,7 +1259,7 @@ k_cgs_sweep3(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ C
         // a wait gave up: flag it, let the loads this block issued land, leave
         if (pred) *(volatile int *) &pred->pad = 1;
         if (side && lane == 31)
-            for (int g = max(0, pr.issued - kS3Bars); g < pr.issued; g++) (void) mbar_wait_s3(&full[g & 7], g);
+            for (int g = max(0, pr.issued - kS3Bars); g < pr.issued; g++) (void) mbar_wait_s3(&full[g & 15], g);
         return;
     }
     acc = artss_block_sum(acc, red_sm);
@@ -1420,7 +1422,7 @@ __global__ void k_swap(double *__restrict__ x, double *__restrict__ y, int64_t n
 // same call site needed last time (usually exact, one round trip), doubled
 // when a batch ends without convergence.
 inline int64_t& loop_hint(artss_ctx *ctx, int site, int field_type) {
-    return ctx->loop_hint[site][field_type & 7];
+    return ctx->loop_hint[site][field_type & 15];
 }
 
 int check_field_args(artss_ctx *ctx, std::initializer_list<const void *> ptrs) {
@@ -1616,12 +1618,15 @@ namespace {
 
 // TMA descriptors of one sweep: x (the array read), b, EV, for the kernel with
 // 72 x 12 windows and for the one-phase kernel (70 x 12 and 66 x 10)
-constexpr int kSweepRowPair = 6;  // variant number of k_cgs_sweep3 with 64 x 8 tiles; + 1: 64 x 6 tiles
-constexpr int kSweepVariants = kSweepRowPair + 2;
+// variant number of k_cgs_sweep3 with 64 x 8 tiles; + 1: 64 x 6 tiles; + 2: 64 x 16
+// tiles, one block per multiprocessor
+constexpr int kSweepRowPair = 6;
+constexpr int kSweepVariants = kSweepRowPair + 3;
 struct SweepMaps {
     const CUtensorMap *x = nullptr, *b = nullptr, *e = nullptr;
     const CUtensorMap *x2 = nullptr, *b2 = nullptr, *e2 = nullptr;
     const CUtensorMap *x3 = nullptr, *b3 = nullptr, *e3 = nullptr;  // 72 x 10 and 66 x 8 windows
+    const CUtensorMap *x4 = nullptr, *b4 = nullptr, *e4 = nullptr;  // 72 x 20 and 66 x 18 windows
 };
 
 // Obstacle table of the row-pair sweep (k_cgs_sweep3) with tiles of 64 x ty
@@ -1664,7 +1669,7 @@ int sweep3_obst(artss_ctx *ctx, const Box3 &box, int t, int ty_rows, int ncx, in
     return ARTSS_OK;
 }
 
-// the row-pair sweep: persistent blocks, two per multiprocessor, at least
+// the row-pair sweep: persistent blocks, G3::BPS per multiprocessor, at least
 // kS3MinPlanes (tile column, plane) units each
 extern "C++" {  // a template inside the extern "C" block of this file
 template <class G3>
@@ -1672,7 +1677,7 @@ int launch_sweep3(artss_ctx *ctx, bool turb, int t, const Box3 &box, const CUten
                   const CUtensorMap *me, double *w, const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
     const int ncx = (int) ((box.nx() + 63) / 64), ncy = (int) ((box.ny() + G3::TY - 1) / G3::TY);
     const int64_t units = (int64_t) ncx * ncy * box.nz();
-    const int G = (int) std::min<int64_t>(std::min<int64_t>(2 * std::max(ctx->sm_count, 1), kMaxPartials / 2),
+    const int G = (int) std::min<int64_t>(std::min<int64_t>(G3::BPS * std::max(ctx->sm_count, 1), kMaxPartials / 2),
                                           std::max<int64_t>(1, units / kS3MinPlanes));
     const uint8_t *obst = nullptr;
     int st = sweep3_obst(ctx, box, t, G3::TY, ncx, ncy, &obst);
@@ -1699,6 +1704,7 @@ int launch_sweep_tma(artss_ctx *ctx, bool turb, int v, const Box3 &box, const Sw
                      const Level &L, const DiffCoef &c, LoopState *pred, int *nb) {
     if (v == kSweepRowPair) return launch_sweep3<S3Tall>(ctx, turb, 0, box, m.x, m.b2, m.e2, w, L, c, pred, nb);
     if (v == kSweepRowPair + 1) return launch_sweep3<S3Flat>(ctx, turb, 1, box, m.x3, m.b3, m.e3, w, L, c, pred, nb);
+    if (v == kSweepRowPair + 2) return launch_sweep3<S3Wide>(ctx, turb, 2, box, m.x4, m.b4, m.e4, w, L, c, pred, nb);
     const int zb = kStDepths[v % 3];
     const dim3 g = sweep_tma_grid(box, zb);
     *nb = nblocks(g);
@@ -1731,9 +1737,11 @@ int set_sweep_smem(bool turb) {
     const int b1 = (int) sweep_tma_smem(turb), b2 = (int) sweep_tma2_smem(turb);
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     const int b3 = (int) S3Tall::smem(turb), b4 = (int) S3Flat::smem(turb);
+    const int b6 = (int) S3Wide::smem(turb);
     if (turb) {
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true, S3Tall>, attr, b3));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true, S3Flat>, attr, b4));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<true, S3Wide>, attr, b6));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<true, 32>, attr, b1));
@@ -1743,6 +1751,7 @@ int set_sweep_smem(bool turb) {
     } else {
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false, S3Tall>, attr, b3));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false, S3Flat>, attr, b4));
+        ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep3<false, S3Wide>, attr, b6));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 8>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 16>, attr, b1));
         ARTSS_CK(cudaFuncSetAttribute(k_cgs_sweep_tma<false, 32>, attr, b1));
@@ -1814,7 +1823,7 @@ int artss_ctx_pdl(artss_ctx *ctx, int enable) {
 
 int artss_ctx_sweep_variant(artss_ctx *ctx, int variant) {
     if (!ctx) { set_error("null argument"); return ARTSS_ERR_ARG; }
-    if (variant < -1 || variant >= kSweepVariants) { set_error("sweep variant is -1 .. 7"); return ARTSS_ERR_ARG; }
+    if (variant < -1 || variant >= kSweepVariants) { set_error("sweep variant is -1 .. 8"); return ARTSS_ERR_ARG; }
     ctx->sweep_force = variant;
     return ARTSS_OK;
 }
@@ -1894,6 +1903,10 @@ int artss_diffuse_cgs(artss_ctx *ctx, double *out, double *in, const double *b, 
                 if ((st = tensor_map_3d(ctx, b, 0, &m.b3, S3Flat::BW, S3Flat::BH))) return st;
                 m.e3 = m.b3;
                 if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e3, S3Flat::BW, S3Flat::BH))) return st;
+                if ((st = tensor_map_3d(ctx, buf[r], 0, &m.x4, S3Wide::XW, S3Wide::XH))) return st;
+                if ((st = tensor_map_3d(ctx, b, 0, &m.b4, S3Wide::BW, S3Wide::BH))) return st;
+                m.e4 = m.b4;
+                if (ev && (st = tensor_map_3d(ctx, ev, 0, &m.e4, S3Wide::BW, S3Wide::BH))) return st;
             }
         }
     }

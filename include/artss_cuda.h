@@ -336,12 +336,13 @@ int artss_ctx_autotune(artss_ctx *ctx, int enable);
 int artss_ctx_pdl(artss_ctx *ctx, int enable);
 int artss_cgs_sweep_depth(artss_ctx *ctx, int turbulent);
 /* the tuned sweep variant of level 0 (0-2: two-phase kernel of z-depth 8,
- * 16, 32; 3-5: one-phase kernel; 6, 7: row-pair kernel with persistent
- * blocks, 64 x 8 and 64 x 6 tiles), -1 before the first solve;
- * artss_cgs_sweep_depth returns -1 for variants 6 and 7 */
+ * 16, 32; 3-5: one-phase kernel; 6-8: row-pair kernel with persistent
+ * blocks: 64 x 8 and 64 x 6 tiles two blocks per multiprocessor, 64 x 16
+ * tiles one block), -1 before the first solve; artss_cgs_sweep_depth
+ * returns -1 for variants 6-8 */
 int artss_cgs_sweep_variant(artss_ctx *ctx, int turbulent);
-/* Pins the colored Gauss-Seidel sweep variant of artss_diffuse_cgs (0-7 as
- * above; 3-7 need an inner box that starts at an odd x), -1 (default): the
+/* Pins the colored Gauss-Seidel sweep variant of artss_diffuse_cgs (0-8 as
+ * above; 3-8 need an inner box that starts at an odd x), -1 (default): the
  * autotuner's choice.  No counterpart in the reference. */
 int artss_ctx_sweep_variant(artss_ctx *ctx, int variant);
 /* IDiffusion::diffuse, ColoredGaussSeidelDiffuse with FP32 sweeps inside FP64

@@ -350,8 +350,8 @@ def _sweep_scenes():
 @pytest.mark.parametrize("turbulent", [False, True])
 def test_cgs_every_sweep_variant(tmp_path, scene, turbulent):
     """Each sweep variant (two-phase and one-phase kernels at every z-depth,
-    the row-pair kernel with persistent blocks on 64 x 8 and 64 x 6 tiles),
-    pinned, gives the oracle's
+    the row-pair kernel with persistent blocks on 64 x 8, 64 x 6 and 64 x 16
+    tiles, two or one blocks per multiprocessor), pinned, gives the oracle's
     colored Gauss-Seidel iterations bit for bit."""
     sc = _sweep_scenes()[scene]
     geom = A.Geometry(scenes.write(sc, str(tmp_path / f"{scene}.xml")))
@@ -364,7 +364,7 @@ def test_cgs_every_sweep_variant(tmp_path, scene, turbulent):
         res = C.c_double()
         oracle.lib().oracle_diffuse_cgs(osc.ptr, P(ro), P(ri), P(b), 4.2e-5, P(ev) if turbulent else None, sc.dt,
                                         FT["u"], 5, 1e-300, 1.0, C.byref(res))
-        for v in range(8):
+        for v in range(9):
             A.cuda_check(ctx.lib.artss_ctx_sweep_variant(ctx.h, v), "variant")
             dout, din, db, dev = ctx.field(out0), ctx.field(in0), ctx.field(b), ctx.field(ev)
             cfg = A.IterCfg(5, 1e-300, 1.0)
