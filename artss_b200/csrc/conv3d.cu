@@ -16,9 +16,12 @@
 // the tap's weights, pre-packed as [C_in/8][C_out][8]; one thread issues the
 // C_in/16 MMAs of the tap and commits them to the stage's "empty" barrier.
 // After the 27th tap the accumulator (128 lanes x C_out FP32 columns) is read
-// by all 128 threads with tcgen05.ld: bias, optional ReLU, BF16, store.
-// Blocks are persistent over output tiles; loads run kConvStages taps ahead,
-// across tile boundaries.  Every wait is bounded and raises an error flag.
+// by warps 0-3 with tcgen05.ld: bias, optional ReLU, BF16, store.  Warp 4
+// loads and issues: two accumulators in tensor memory alternate between tiles,
+// so the MMAs of tile n+1 run while tile n is read out.  Blocks are persistent
+// over output tiles; loads run as many taps ahead as shared memory holds
+// stages (ConvShape::stages, at most kConvMaxStages), across tile boundaries.
+// Every wait is bounded and raises an error flag.
 #include "internal.cuh"
 #include "tc.cuh"
 
@@ -32,7 +35,8 @@ namespace artss {
 namespace {
 
 constexpr int kConvThreads = 128;
-constexpr int kConvStages = 4;
+constexpr int kConvFwdThreads = 160;  // warps 0-3: epilogue (tensor-memory lanes 0..127); warp 4: loads and MMAs
+constexpr int kConvMaxStages = 16;
 constexpr int kConvPolls = 1 << 20;
 constexpr size_t kConvGuard = 64 * 1024;           // shared memory past the last stage, never addressed by a correct descriptor
 constexpr size_t kConvSmemMax = 227 * 1024 - 2048;  // dynamic limit minus the kernels' static shared memory
@@ -42,29 +46,34 @@ struct ConvShape {
     int tw, th, tz;           // tile: tw x th x tz voxels, tw * th * tz = 128 (x fastest)
     int tiles_x, tiles_y, tiles_z, tiles;
     unsigned a_bytes, b_bytes, stage_bytes;
+    int stages;               // ring depth (taps in flight)
 };
 
-__global__ void __launch_bounds__(kConvThreads, 1)
+__global__ void __launch_bounds__(kConvFwdThreads, 1)
 k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__restrict__ wp,
              const float *__restrict__ bias, __nv_bfloat16 *__restrict__ y, ConvShape s, int relu,
              int *__restrict__ err) {
     extern __shared__ __align__(1024) uint8_t cv_sm[];
-    __shared__ __align__(8) uint64_t full[kConvStages], empty[kConvStages], accb;
+    // full / empty: the stage ring; accf[a]: accumulator a holds a finished tile;
+    // acce[a]: the four epilogue warps have read accumulator a out
+    __shared__ __align__(8) uint64_t full[kConvMaxStages], empty[kConvMaxStages], accf[2], acce[2];
     __shared__ uint32_t tmem_base;
-    __shared__ int s_fail;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int S = s.stages;
     const unsigned tcols = s.cout <= 32 ? 32u : (s.cout <= 64 ? 64u : (s.cout <= 128 ? 128u : 256u));
     if (tid == 0) {
-        for (int i = 0; i < kConvStages; i++) {
+        for (int i = 0; i < S; i++) {
             tc::mbar_init(&full[i], 1);
             tc::mbar_init(&empty[i], 1);
         }
-        tc::mbar_init(&accb, 1);
+        for (int i = 0; i < 2; i++) {
+            tc::mbar_init(&accf[i], 1);
+            tc::mbar_init(&acce[i], 4);
+        }
         tc::fence_barrier_init();
-        s_fail = 0;
     }
     if (warp == 0) {
-        tc::tmem_alloc(&tmem_base, tcols);
+        tc::tmem_alloc(&tmem_base, 2 * tcols);
         tc::tmem_relinquish();
     }
     tc::tc_fence_before();
@@ -73,83 +82,100 @@ k_conv3d_fwd(const __grid_constant__ CUtensorMap tm_x, const __nv_bfloat16 *__re
     const uint32_t tmem = tmem_base;
     const int my_tiles = (s.tiles - (int) blockIdx.x + (int) gridDim.x - 1) / (int) gridDim.x;
     const int nsteps = my_tiles * 27;
-    const int kk_n = s.cin / 16;
-    const uint32_t idesc = tc::idesc_bf16(128, s.cout, 0, 0);
-    const unsigned lbo_a = 128 * 16, lbo_b = (unsigned) s.cout * 16;
 
-    // thread 0: issue the loads of step p
-    auto produce = [&](int p) {
-        const int st = p % kConvStages;
-        if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
-            return false;
-        const int tile = (int) blockIdx.x + (p / 27) * (int) gridDim.x, tap = p % 27;
-        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
-        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
-        tc::mbar_expect_tx(&full[st], s.a_bytes + s.b_bytes);
-        tc::tma_load_5d(a, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, tzi * s.tz + dz, 0, &full[st]);
-        tc::bulk_load(a + s.a_bytes, wp + (size_t) tap * s.cout * s.cin, s.b_bytes, &full[st]);
-        return true;
-    };
-
-    int step = 0;
-    bool ok = true;
-    if (tid == 0)
-        for (int p = 0; p < kConvStages - 1 && p < nsteps && ok; p++) ok = produce(p);
-    for (int it = 0; it < my_tiles; it++) {
-        const int tile = (int) blockIdx.x + it * (int) gridDim.x;
-        if (tid == 0 && ok) {
-            for (int tap = 0; tap < 27 && ok; tap++, step++) {
-                if (step + kConvStages - 1 < nsteps) ok = produce(step + kConvStages - 1);
-                const int st = step % kConvStages;
-                if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / kConvStages) & 1), kConvPolls);
-                if (!ok) break;
+    if (warp == 4) {
+        if (lane == 0) {
+            const int kk_n = s.cin / 16;
+            const uint32_t idesc = tc::idesc_bf16(128, s.cout, 0, 0);
+            const unsigned lbo_a = 128 * 16, lbo_b = (unsigned) s.cout * 16;
+            // the loads of step p (tile p / 27, tap p % 27)
+            auto produce = [&](int p) {
+                const int st = p % S;
+                if (p >= S && !tc::mbar_wait(&empty[st], (unsigned) ((p / S - 1) & 1), kConvPolls)) return false;
+                const int tile = (int) blockIdx.x + (p / 27) * (int) gridDim.x, tap = p % 27;
+                const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
+                const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+                uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+                tc::mbar_expect_tx(&full[st], s.a_bytes + s.b_bytes);
+                tc::tma_load_5d(a, &tm_x, 0, tx * s.tw + dx, ty * s.th + dy, tzi * s.tz + dz, 0, &full[st]);
+                tc::bulk_load(a + s.a_bytes, wp + (size_t) tap * s.cout * s.cin, s.b_bytes, &full[st]);
+                return true;
+            };
+            bool ok = true;
+            int issued = 0;  // steps whose loads were issued
+            for (int p = 0; p < S - 1 && p < nsteps && ok; p++)
+                if ((ok = produce(p))) issued = p + 1;
+            int step = 0;
+            for (int it = 0; it < my_tiles && ok; it++) {
+                const int acc = it & 1;
+                const uint32_t d = tmem + (uint32_t) acc * tcols;
+                // accumulator acc last held tile it - 2: wait until it was read out
+                if (it >= 2) ok = tc::mbar_wait(&acce[acc], (unsigned) (((it >> 1) - 1) & 1), kConvPolls);
                 tc::tc_fence_after();
-                const uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
-                const uint8_t *b = a + s.a_bytes;
-                for (int kk = 0; kk < kk_n; kk++) {
-                    const uint64_t da = tc::smem_desc(a + 2 * kk * lbo_a, lbo_a, 128);
-                    const uint64_t db = tc::smem_desc(b + 2 * kk * lbo_b, lbo_b, 128);
-                    tc::mma_bf16(tmem, da, db, idesc, (tap | kk) != 0);
+                for (int tap = 0; tap < 27 && ok; tap++, step++) {
+                    if (step + S - 1 < nsteps && (ok = produce(step + S - 1))) issued = step + S;
+                    const int st = step % S;
+                    if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / S) & 1), kConvPolls);
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
+                    const uint8_t *b = a + s.a_bytes;
+                    for (int kk = 0; kk < kk_n; kk++) {
+                        const uint64_t da = tc::smem_desc(a + 2 * kk * lbo_a, lbo_a, 128);
+                        const uint64_t db = tc::smem_desc(b + 2 * kk * lbo_b, lbo_b, 128);
+                        tc::mma_bf16(d, da, db, idesc, (tap | kk) != 0);
+                    }
+                    tc::mma_commit(&empty[st]);
                 }
-                tc::mma_commit(&empty[st]);
-                if (tap == 26) tc::mma_commit(&accb);
+                if (ok) tc::mma_commit(&accf[acc]);
             }
-            if (!ok) s_fail = 1;
+            if (!ok) {
+                if (err) atomicExch(err, 1);
+                // let this block's loads and MMAs in flight finish before it leaves
+                for (int p = step; p < issued; p++)
+                    (void) tc::mbar_wait(&full[p % S], (unsigned) ((p / S) & 1), kConvPolls);
+                if (step > 0)
+                    (void) tc::mbar_wait(&empty[(step - 1) % S], (unsigned) (((step - 1) / S) & 1), kConvPolls);
+            }
         }
-        // epilogue: lane = voxel of the tile, columns = output channels.  Only
-        // the issuing thread polls the accumulator barrier; the others wait at
-        // the block barrier (polling threads of its own warp would compete with
-        // it for the warp's issue slots)
-        bool acc_ok = true;
-        if (tid == 0) acc_ok = ok && tc::mbar_wait(&accb, (unsigned) (it & 1), kConvPolls);
-        if (__syncthreads_or(!acc_ok || s_fail)) {
-            if (tid == 0 && err) atomicExch(err, 1);
-            break;
-        }
-        tc::tc_fence_after();
-        const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
-        const int vx = tx * s.tw + tid % s.tw, vy = ty * s.th + (tid / s.tw) % s.th, vz = tzi * s.tz + tid / (s.tw * s.th);
-        __nv_bfloat16 *yo = y + (((size_t) vz * s.H + vy) * s.W + vx) * s.cout;
-        for (int c0 = 0; c0 < s.cout; c0 += 16) {
-            float v[16];
-            tc::tmem_ld16(tmem + ((uint32_t) (32 * warp) << 16) + (uint32_t) c0, v);
-            __align__(16) __nv_bfloat16 o[16];
+    } else {
+        // epilogue: lane = voxel of the tile, columns = output channels
+        for (int it = 0; it < my_tiles; it++) {
+            const int acc = it & 1;
+            if (!tc::mbar_wait(&accf[acc], (unsigned) ((it >> 1) & 1), kConvPolls)) {
+                if (lane == 0 && err) atomicExch(err, 1);
+                break;
+            }
+            tc::tc_fence_after();
+            const int tile = (int) blockIdx.x + it * (int) gridDim.x;
+            const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
+            const int vx = tx * s.tw + tid % s.tw, vy = ty * s.th + (tid / s.tw) % s.th,
+                      vz = tzi * s.tz + tid / (s.tw * s.th);
+            __nv_bfloat16 *yo = y + (((size_t) vz * s.H + vy) * s.W + vx) * s.cout;
+            const uint32_t src = tmem + (uint32_t) acc * tcols + ((uint32_t) (32 * warp) << 16);
+            for (int c0 = 0; c0 < s.cout; c0 += 16) {
+                float v[16];
+                tc::tmem_ld16(src + (uint32_t) c0, v);
+                __align__(16) __nv_bfloat16 o[16];
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                float r = v[i] + (bias ? bias[c0 + i] : 0.f);
-                if (relu) r = fmaxf(r, 0.f);
-                o[i] = __float2bfloat16_rn(r);
+                for (int i = 0; i < 16; i++) {
+                    float r = v[i] + (bias ? bias[c0 + i] : 0.f);
+                    if (relu) r = fmaxf(r, 0.f);
+                    o[i] = __float2bfloat16_rn(r);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(yo + c0);
+                dst[0] = reinterpret_cast<const uint4 *>(o)[0];
+                dst[1] = reinterpret_cast<const uint4 *>(o)[1];
             }
-            uint4 *dst = reinterpret_cast<uint4 *>(yo + c0);
-            dst[0] = reinterpret_cast<const uint4 *>(o)[0];
-            dst[1] = reinterpret_cast<const uint4 *>(o)[1];
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&acce[acc]);
         }
-        tc::tc_fence_before();
-        __syncthreads();
     }
+    tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, tcols);
+    tc::tc_fence_after();
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * tcols);
 }
 
 // Weight gradient dW[t][co][ci] += sum_v dY[v][co] x[v + off_t][ci] as a GEMM
@@ -167,17 +193,18 @@ __global__ void __launch_bounds__(kConvThreads, 1)
 k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__ CUtensorMap tm_dy,
                float *__restrict__ dw, ConvShape s, int tiles_per_block, int *__restrict__ err) {
     extern __shared__ __align__(1024) uint8_t cv_sm[];
-    __shared__ __align__(8) uint64_t full[kConvStages], empty[kConvStages], accb;
+    __shared__ __align__(8) uint64_t full[kConvMaxStages], empty[kConvMaxStages], accb;
     __shared__ uint32_t tmem_base;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int S = s.stages;
     const unsigned tcols = s.cin <= 32 ? 32u : (s.cin <= 64 ? 64u : (s.cin <= 128 ? 128u : 256u));
     const int t_begin = (int) blockIdx.x * tiles_per_block;
     const int t_end = min(s.tiles, t_begin + tiles_per_block);
     const int ntile = t_end - t_begin;
     if (ntile <= 0) return;
     if (tid == 0) {
-        for (int i = 0; i < kConvStages; i++) {
+        for (int i = 0; i < S; i++) {
             tc::mbar_init(&full[i], 1);
             tc::mbar_init(&empty[i], 1);
         }
@@ -199,9 +226,8 @@ k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__
     const unsigned b_bytes = s.a_bytes;                            // x tile, C_in/8 channel groups
 
     auto produce = [&](int p) {
-        const int st = p % kConvStages;
-        if (p >= kConvStages && !tc::mbar_wait(&empty[st], (unsigned) ((p / kConvStages - 1) & 1), kConvPolls))
-            return false;
+        const int st = p % S;
+        if (p >= S && !tc::mbar_wait(&empty[st], (unsigned) ((p / S - 1) & 1), kConvPolls)) return false;
         const int tap = p / ntile, tile = t_begin + p % ntile;
         const int tx = tile % s.tiles_x, ty = (tile / s.tiles_x) % s.tiles_y, tzi = tile / (s.tiles_x * s.tiles_y);
         const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
@@ -215,13 +241,13 @@ k_conv3d_wgrad(const __grid_constant__ CUtensorMap tm_x, const __grid_constant__
     bool ok = true;
     int step = 0;
     if (tid == 0)
-        for (int p = 0; p < kConvStages - 1 && p < nsteps && ok; p++) ok = produce(p);
+        for (int p = 0; p < S - 1 && p < nsteps && ok; p++) ok = produce(p);
     for (int tap = 0; tap < 27; tap++) {
         if (tid == 0 && ok) {
             for (int i = 0; i < ntile && ok; i++, step++) {
-                if (step + kConvStages - 1 < nsteps) ok = produce(step + kConvStages - 1);
-                const int st = step % kConvStages;
-                if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / kConvStages) & 1), kConvPolls);
+                if (step + S - 1 < nsteps) ok = produce(step + S - 1);
+                const int st = step % S;
+                if (ok) ok = tc::mbar_wait(&full[st], (unsigned) ((step / S) & 1), kConvPolls);
                 if (!ok) break;
                 tc::tc_fence_after();
                 const uint8_t *a = cv_sm + (size_t) st * s.stage_bytes;
@@ -293,6 +319,13 @@ int encode_act_map(const __nv_bfloat16 *x, const ConvShape &s, int c, int box_ch
     return ARTSS_OK;
 }
 
+// stages of `bytes` each that fit the dynamic shared memory with kConvGuardMin
+// left over, at most kConvMaxStages
+constexpr size_t kConvGuardMin = 16 * 1024;
+int conv_stages(size_t bytes) {
+    return (int) std::min<size_t>(kConvMaxStages, (kConvSmemMax - kConvGuardMin) / bytes);
+}
+
 int conv_shape(const artss_conv_desc *d, ConvShape *s) {
     if (d->D < 1 || d->H < 1 || d->W < 1 || d->cin < 16 || d->cin % 16 || d->cin > 256 ||
         d->cout < 16 || d->cout % 16 || d->cout > 256) {
@@ -317,9 +350,8 @@ int conv_shape(const artss_conv_desc *d, ConvShape *s) {
     s->a_bytes = 128u * (unsigned) d->cin * 2u;
     s->b_bytes = (unsigned) d->cout * (unsigned) d->cin * 2u;
     s->stage_bytes = (s->a_bytes + s->b_bytes + 1023u) & ~1023u;
-    if ((size_t) s->stage_bytes * kConvStages > kConvSmemMax) {
-        set_error("conv3d: stages too large"); return ARTSS_ERR_LIMIT;
-    }
+    s->stages = conv_stages(s->stage_bytes);
+    if (s->stages < 2) { set_error("conv3d: stages too large"); return ARTSS_ERR_LIMIT; }
     return ARTSS_OK;
 }
 
@@ -337,8 +369,9 @@ int conv3d_wgrad(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const 
     // stage: dY tile (128 voxels x 128 padded channels) + x tile
     const unsigned stage = ((unsigned) kWgradMRows * 128u * 2u + s.a_bytes + 1023u) & ~1023u;
     s.stage_bytes = stage;
-    const size_t stages = (size_t) stage * kConvStages;
-    if (stages > kConvSmemMax) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    s.stages = conv_stages(stage);
+    if (s.stages < 2) { set_error("conv3d wgrad: stages too large"); return ARTSS_ERR_LIMIT; }
+    const size_t stages = (size_t) stage * s.stages;
     const size_t smem = stages + std::min<size_t>(kConvGuard, kConvSmemMax - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
@@ -361,13 +394,13 @@ int conv3d_fwd(artss_ctx *ctx, const artss_conv_desc *d, const void *x, const vo
     }
     CUtensorMap m;
     if ((st = encode_x_map((const __nv_bfloat16 *) x, s, &m))) return st;
-    const size_t stages = (size_t) s.stage_bytes * kConvStages;
+    const size_t stages = (size_t) s.stage_bytes * s.stages;
     const size_t smem = stages + std::min<size_t>(kConvGuard, kConvSmemMax - stages);
     ARTSS_CK(cudaFuncSetAttribute(k_conv3d_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     const int grid = std::min(s.tiles, sms);
-    ARTSS_LAUNCH(ctx, FAM_CONV, k_conv3d_fwd<<<grid, kConvThreads, smem, ctx->stream>>>(
+    ARTSS_LAUNCH(ctx, FAM_CONV, k_conv3d_fwd<<<grid, kConvFwdThreads, smem, ctx->stream>>>(
                                     m, (const __nv_bfloat16 *) wp, bias, (__nv_bfloat16 *) y, s, d->relu,
                                     &ctx->d_loop[kNnErrSlot].pad));
     ARTSS_LAUNCH_CK(ctx);
