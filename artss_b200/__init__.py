@@ -143,6 +143,7 @@ def load_cuda() -> C.CDLL:
             "artss_advect_sl": ([_P, _D, _D, _D, _D, _D, C.c_double, C.c_int], C.c_int),
             "artss_advect_sl_uvw": ([_P] + [_D] * 9 + [C.c_double], C.c_int),
             "artss_turb_const_smagorinsky": ([_P, _D, _D, _D, _D, C.c_double], C.c_int),
+            "artss_turb_dynamic_smagorinsky": ([_P, _D, _D, _D, _D, C.c_double], C.c_int),
             "artss_diffuse_cgs": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg), C.c_int,
                                    C.POINTER(IterStats)], C.c_int),
             "artss_diffuse_jacobi": ([_P, _D, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.POINTER(IterCfg),

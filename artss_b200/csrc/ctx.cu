@@ -284,6 +284,7 @@ int artss_ctx_destroy(artss_ctx *ctx) {
     }
     for (uint8_t *t : ctx->d_sweep3_obst) if (t) cudaFree(t);
     if (ctx->cgsm_w) cudaFree(ctx->cgsm_w);
+    if (ctx->dsmag) cudaFree(ctx->dsmag);
     if (ctx->rb_stream) cudaStreamSynchronize(ctx->rb_stream);
     for (auto &r : ctx->rb) {
         for (double *a : r.dev) cudaFree(a);

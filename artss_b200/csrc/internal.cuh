@@ -136,6 +136,8 @@ struct artss_ctx {
     // box cell that is not inner (k_cgs_sweep3); built on first use
     uint8_t *d_sweep3_obst[3] = {nullptr, nullptr, nullptr};     // per tile height (64 x 8, 64 x 6, 64 x 16)
     int sweep3_obst_state[3] = {0, 0, 0};                        // 0 not built, 1 built, 2 every box cell inner
+    double *dsmag = nullptr;                                     // work arrays of artss_turb_dynamic_smagorinsky
+    uint64_t dsmag_version = 0;                                  // geom_version they were zeroed for
     float *cgsm_w = nullptr;                                     // FP32 defect / correction of artss_diffuse_cgs_mixed
     int64_t cgsm_n = 0;
     std::map<artss::TuneKey, int> tuned;                         // autotuned variant per kernel and shape

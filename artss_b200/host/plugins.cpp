@@ -167,6 +167,13 @@ void ConstSmagorinsky::calc_turbulent_viscosity(Field &ev, const Field &in_u, co
           "ConstSmagorinsky");
 }
 
+void DynamicSmagorinsky::calc_turbulent_viscosity(Field &ev, const Field &in_u, const Field &in_v, const Field &in_w,
+                                                  bool) {
+    check(artss_turb_dynamic_smagorinsky(m_rt.ctx(), ev.data, in_u.data, in_v.data, in_w.data,
+                                         m_rt.settings().physical.nu.value()),
+          "DynamicSmagorinsky");
+}
+
 void ExplicitEulerSource::add_source(Field &out_x, Field &out_y, Field &out_z, const Field &S_x, const Field &S_y,
                                      const Field &S_z, bool) {
     // ExplicitEulerSource.cpp:40-96: only the axes listed in `dir`, in x, y, z order

@@ -173,6 +173,18 @@ class ConstSmagorinsky : public ITurbulence {
     real m_cs;
 };
 
+// DynamicSmagorinsky (src/turbulence/DynamicSmagorinsky.cpp:172-427); nu from the settings
+class DynamicSmagorinsky : public ITurbulence {
+ public:
+    explicit DynamicSmagorinsky(Runtime &rt) : m_rt(rt) {}
+    void calc_turbulent_viscosity(Field &ev, const Field &in_u, const Field &in_v, const Field &in_w,
+                                  bool sync) override;
+    void explicit_filtering(Field &, const Field &, bool) override {}
+
+ private:
+    Runtime &m_rt;
+};
+
 class ExplicitEulerSource : public ISource {
  public:
     ExplicitEulerSource(Runtime &rt, std::vector<int> dir) : m_rt(rt), m_dir(std::move(dir)) {}

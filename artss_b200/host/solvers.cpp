@@ -22,6 +22,7 @@ std::unique_ptr<IDiffusion> make_diffusion(Runtime &rt, const settings::Diffusio
 
 std::unique_ptr<ITurbulence> make_turbulence(Runtime &rt, const settings::Turbulence &s) {
     if (s.type == "ConstSmagorinsky") return std::make_unique<ConstSmagorinsky>(rt, s.cs);
+    if (s.type == "DynamicSmagorinsky") return std::make_unique<DynamicSmagorinsky>(rt);
     throw config_error("turbulence method '" + s.type + "' is not implemented");
 }
 

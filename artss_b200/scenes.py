@@ -51,6 +51,7 @@ class Scene:
     diff_max_iter: int = 100
     diff_tol: float = 1e-7
     cs: float = 0.2
+    turbulence: str = "ConstSmagorinsky"  # or "DynamicSmagorinsky" (no parameters)
     buoyancy_dir: str = "z"
     t_ambient: float = 299.15
     n_level: int = 4
@@ -372,6 +373,14 @@ def to_xml(s: Scene) -> str:
     a("  </physical_parameters>")
     a(f'  <solver description="{s.solver}" >')
 
+    def turbulence_block():
+        if s.turbulence == "DynamicSmagorinsky":
+            a('    <turbulence type="DynamicSmagorinsky">')
+        else:
+            a('    <turbulence type="ConstSmagorinsky">')
+            a(f"      <Cs> {_f(s.cs)} </Cs>")
+        a("    </turbulence>")
+
     def diffusion_block(tag_field: str, indent: str, typ: str, max_iter: int, tol: float, w: float):
         a(f'{indent}<diffusion type="{typ}" field="{tag_field}">')
         a(f"{indent}  <max_iter> {max_iter} </max_iter>")
@@ -386,17 +395,13 @@ def to_xml(s: Scene) -> str:
         if s.solver != "AdvectionSolver":
             diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
         if s.solver == "DiffusionTurbSolver":
-            a('    <turbulence type="ConstSmagorinsky">')
-            a(f"      <Cs> {_f(s.cs)} </Cs>")
-            a("    </turbulence>")
+            turbulence_block()
     elif s.solver != "PressureSolver":
         a('    <advection type="SemiLagrangian" field="u,v,w">')
         a("    </advection>")
         diffusion_block("u,v,w", "    ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
         if turbulent:
-            a('    <turbulence type="ConstSmagorinsky">')
-            a(f"      <Cs> {_f(s.cs)} </Cs>")
-            a("    </turbulence>")
+            turbulence_block()
         if s.force == "Buoyancy":
             a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
             a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")

@@ -309,6 +309,16 @@ int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *ou
  * (src/turbulence/ConstSmagorinsky.cpp:30-87), including apply_boundary(ev). */
 int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t,
                                  const double *u, const double *v, const double *w, double cs);
+/* ITurbulence::calc_turbulent_viscosity, DynamicSmagorinsky
+ * (src/turbulence/DynamicSmagorinsky.cpp:172-427): the dynamic
+ * Smagorinsky-Lilly eddy viscosity on the inner cells of level 0, with the
+ * reference's filters, its in-place 27-cell averaging of the coefficient in
+ * list order and ev = 0 where ev + nu < 0; no boundary program (the reference
+ * applies none).  The first call (or the first after the cell lists or
+ * boundary programs changed) sets up 40 level-0 work arrays and must not be
+ * inside a stream capture. */
+int artss_turb_dynamic_smagorinsky(artss_ctx *ctx, double *nu_t, const double *u, const double *v,
+                                   const double *w, double nu);
 
 /* IDiffusion::diffuse, ColoredGaussSeidelDiffuse (src/diffusion/ColoredGaussSeidelDiffuse.cpp:38-173).
  * ev == NULL selects the laminar variant.  `in` is overwritten as in the

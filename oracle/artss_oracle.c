@@ -579,3 +579,118 @@ int64_t oracle_mg_pressure(oracle_mg *mg, double *p, const double *rhs, int firs
 }
 
 int64_t oracle_mg_last_coarse_iterations(const oracle_mg *mg) { return mg->last_coarse_it; }
+
+/* DynamicSmagorinsky::explicit_filtering (src/turbulence/DynamicSmagorinsky.cpp:384-427):
+ * trapezoidal 3x3x3 weights, x offset outermost, z innermost */
+static void ds_filter(const oracle_scene *s, double *out, const double *in) {
+    const int64_t Nx = s->Nx[0], Ny = s->Ny[0];
+    const double a[3] = {1. / 4., 1. / 2., 1. / 4.};
+    for (int64_t j = 0; j < s->n_inner[0]; j++) {
+        const int64_t i = s->inner[0][j];
+        double sum = 0;
+        for (int64_t l = 0; l < 3; l++)
+            for (int64_t m = 0; m < 3; m++)
+                for (int64_t n = 0; n < 3; n++)
+                    sum = sum + a[l] * a[m] * a[n] * in[i - 1 + l + Nx * (m - 1) + Nx * Ny * (n - 1)];
+        out[i] = sum;
+    }
+}
+
+void oracle_dynamic_smagorinsky(const oracle_scene *s, double *ev, const double *u, const double *v, const double *w,
+                                double nu) {
+    enum { UF, VF, WF, UU, VV, WW, UV, UW, VW, UUF, VVF, WWF, UVF, UWF, VWF, UFUF, VFVF, WFWF, UFVF, UFWF, VFWF,
+           L11, L22, L33, L12, L13, L23, S11, S22, S33, S12, S13, S23, S11F, S22F, S33F, S12F, S13F, S23F,
+           P11, P22, P33, P12, P13, P23, P11F, P22F, P33F, P12F, P13F, P23F, M11, M22, M33, M12, M13, M23,
+           SBAR, SBARF, CS, NARR };
+    const int64_t Nx = s->Nx[0], Ny = s->Ny[0], N = Nx * Ny * s->Nz[0];
+    double *f[NARR];
+    for (int a = 0; a < NARR; a++) f[a] = (double *) calloc((size_t) N, sizeof(double));
+    const double dx = s->dx[0], dy = s->dy[0], dz = s->dz[0];
+    const double rdx = 1. / dx, rdy = 1. / dy, rdz = 1. / dz;
+    const double alpha = 2.0;
+    const double delta_s = cbrt(dx * dy * dz);
+    const int64_t n_in = s->n_inner[0];
+    const int64_t *lst = s->inner[0];
+    ds_filter(s, f[UF], u);
+    ds_filter(s, f[VF], v);
+    ds_filter(s, f[WF], w);
+    for (int64_t j = 0; j < n_in; j++) {
+        const int64_t i = lst[j];
+        f[UU][i] = f[UF][i] * f[UF][i];
+        f[VV][i] = f[VF][i] * f[VF][i];
+        f[WW][i] = f[WF][i] * f[WF][i];
+        f[UV][i] = f[UF][i] * f[VF][i];
+        f[UW][i] = f[UF][i] * f[WF][i];
+        f[VW][i] = f[VF][i] * f[WF][i];
+        f[UFUF][i] = f[UF][i] * f[UF][i];
+        f[VFVF][i] = f[VF][i] * f[VF][i];
+        f[WFWF][i] = f[WF][i] * f[WF][i];
+        f[UFVF][i] = f[UF][i] * f[VF][i];
+        f[UFWF][i] = f[UF][i] * f[WF][i];
+        f[VFWF][i] = f[VF][i] * f[WF][i];
+    }
+    /* the reference filters ww twice and never uw (uw_f keeps its zeros) */
+    ds_filter(s, f[UUF], f[UU]);
+    ds_filter(s, f[VVF], f[VV]);
+    ds_filter(s, f[WWF], f[WW]);
+    ds_filter(s, f[UVF], f[UV]);
+    ds_filter(s, f[VWF], f[VW]);
+    ds_filter(s, f[WWF], f[WW]);
+    const double *uf = f[UF], *vf = f[VF], *wf = f[WF];
+    for (int64_t j = 0; j < n_in; j++) {
+        const int64_t i = lst[j];
+        f[L11][i] = f[UUF][i] - f[UFUF][i];
+        f[L22][i] = f[VVF][i] - f[VFVF][i];
+        f[L33][i] = f[WWF][i] - f[WFWF][i];
+        f[L12][i] = f[UVF][i] - f[UFVF][i];
+        f[L13][i] = f[UWF][i] - f[UFWF][i];
+        f[L23][i] = f[VWF][i] - f[VFWF][i];
+        f[S11][i] = (uf[i + 1] - uf[i - 1]) * 0.5 * rdx;
+        f[S22][i] = (vf[i + Nx] - vf[i - Nx]) * 0.5 * rdy;
+        f[S33][i] = (wf[i + Nx * Ny] - wf[i - Nx * Ny]) * 0.5 * rdz;
+        f[S12][i] = 0.5 * ((uf[i + Nx] - uf[i - Nx]) * 0.5 * rdy + (vf[i + 1] - vf[i - 1]) * 0.5 * rdx);
+        f[S13][i] = 0.5 * ((uf[i + Nx * Ny] - uf[i - Nx * Ny]) * 0.5 * rdz + (wf[i + 1] - wf[i - 1]) * 0.5 * rdx);
+        f[S23][i] = 0.5 * ((vf[i + Nx * Ny] - vf[i - Nx * Ny]) * 0.5 * rdz + (wf[i + Nx] - wf[i - Nx]) * 0.5 * rdy);
+        f[SBAR][i] = sqrt(2. * (f[S11][i] * f[S11][i] + f[S22][i] * f[S22][i] + f[S33][i] * f[S33][i] +
+                                2. * (f[S12][i] * f[S12][i]) + 2. * (f[S13][i] * f[S13][i]) +
+                                2. * (f[S23][i] * f[S23][i])));
+        f[P11][i] = f[SBAR][i] * f[S11][i];
+        f[P22][i] = f[SBAR][i] * f[S22][i];
+        f[P33][i] = f[SBAR][i] * f[S33][i];
+        f[P12][i] = f[SBAR][i] * f[S12][i];
+        f[P13][i] = f[SBAR][i] * f[S13][i];
+        f[P23][i] = f[SBAR][i] * f[S23][i];
+    }
+    for (int a = 0; a < 6; a++) ds_filter(s, f[S11F + a], f[S11 + a]);
+    for (int a = 0; a < 6; a++) ds_filter(s, f[P11F + a], f[P11 + a]);
+    double *Cs = f[CS];
+    for (int64_t j = 0; j < n_in; j++) {
+        const int64_t i = lst[j];
+        f[SBARF][i] = sqrt(2. * (f[S11F][i] * f[S11F][i] + f[S22F][i] * f[S22F][i] + f[S33F][i] * f[S33F][i] +
+                                 2. * (f[S12F][i] * f[S12F][i]) + 2. * (f[S13F][i] * f[S13F][i]) +
+                                 2. * (f[S23F][i] * f[S23F][i])));
+        for (int a = 0; a < 6; a++)
+            f[M11 + a][i] = 2.0 * delta_s * delta_s * (f[P11F + a][i] - alpha * alpha * f[SBARF][i] * f[S11F + a][i]);
+        /* the reference's products (not sums) of the 22 and 33 terms, kept */
+        const double num = f[L11][i] * f[M11][i] + f[L22][i] * f[M22][i] * f[L33][i] * f[M33][i] +
+                           2.0 * f[L12][i] * f[M12][i] + 2.0 * f[L13][i] * f[M13][i] + 2.0 * f[L23][i] * f[M23][i];
+        const double den = f[M11][i] * f[M11][i] + f[M22][i] * f[M22][i] * f[M33][i] * f[M33][i] +
+                           2.0 * f[M12][i] * f[M12][i] + 2.0 * f[M13][i] * f[M13][i] + 2.0 * f[M23][i] * f[M23][i];
+        Cs[i] = num / den;
+    }
+    /* local averaging in place, in list order (earlier cells already averaged) */
+    for (int64_t j = 0; j < n_in; j++) {
+        const int64_t i = lst[j];
+        double sum = 0;
+        for (int64_t l = 0; l < 3; l++)
+            for (int64_t m = 0; m < 3; m++)
+                for (int64_t n = 0; n < 3; n++) sum = sum + Cs[i - 1 + l + Nx * (m - 1) + Nx * Ny * (n - 1)];
+        Cs[i] = sum / 27.0;
+        ev[i] = 2.0 * Cs[i] * delta_s * delta_s * f[SBAR][i];
+    }
+    for (int64_t j = 0; j < n_in; j++) {
+        const int64_t i = lst[j];
+        if ((ev[i] + nu) < 0) ev[i] = 0;
+    }
+    for (int a = 0; a < NARR; a++) free(f[a]);
+}

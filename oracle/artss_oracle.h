@@ -75,6 +75,14 @@ void oracle_add_source(const oracle_scene *s, double *out, const double *S, doub
  * program; ev == NULL: laminar. */
 void oracle_diffuse_explicit(const oracle_scene *s, double *out, const double *in, double D, const double *ev,
                              double dt, int field_type);
+/* DynamicSmagorinsky::calc_turbulent_viscosity (src/turbulence/DynamicSmagorinsky.cpp:172-376)
+ * with its explicit_filtering (:384-427), loop by loop: ev on the inner cells
+ * (no boundary program).  The reference's work fields start as zero and only
+ * their inner cells are written; this restatement allocates them zeroed per
+ * call, which gives the same values (every inner cell is written before it is
+ * read in a call). */
+void oracle_dynamic_smagorinsky(const oracle_scene *s, double *ev, const double *u, const double *v, const double *w,
+                                double nu);
 /* ISource::dissipate (src/interfaces/ISource.cpp:63-123): out += dt * nu * Phi
  * on inner cells, then the boundary program of field_type. */
 void oracle_dissipate(const oracle_scene *s, double *out, const double *u, const double *v, const double *w,

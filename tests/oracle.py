@@ -61,6 +61,7 @@ def lib():
             "oracle_add_source": [S, _D, _D, C.c_double, C.c_int],
             "oracle_diffuse_explicit": [S, _D, _D, C.c_double, _D, C.c_double, C.c_int],
             "oracle_dissipate": [S, _D, _D, _D, _D, C.c_double, C.c_double, C.c_int],
+            "oracle_dynamic_smagorinsky": [S, _D, _D, _D, _D, C.c_double],
         }
         for fn, a in sig.items():
             getattr(L, fn).argtypes = a

@@ -57,10 +57,17 @@ def ref_list(out_dir: str, name: str, level: int) -> np.ndarray:
 
 
 def rel_max_err(a: np.ndarray, b: np.ndarray, mask: Optional[np.ndarray] = None) -> float:
-    """max|a-b| / max(max|b|, tiny) over the masked cells."""
+    """max|a-b| / max(max|b|, tiny) over the masked cells.  NaNs must sit on
+    the same cells in both (the reference produces them in some scenes, e.g.
+    DynamicSmagorinsky's 0/0 coefficient where the filtered strain vanishes);
+    otherwise the error is infinite.  The other cells are compared as usual."""
     if mask is not None:
         a = a[mask]
         b = b[mask]
+    na, nb = np.isnan(a), np.isnan(b)
+    if not np.array_equal(na, nb):
+        return float("inf")
+    a, b = a[~na], b[~nb]
     if a.size == 0:
         return 0.0
     scale = max(float(np.max(np.abs(b))), 1e-300)

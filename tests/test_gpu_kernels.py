@@ -74,6 +74,29 @@ def test_advect(env):
         assert np.array_equal(ctx.download(o), ref)
 
 
+def test_dynamic_smagorinsky(env):
+    """DynamicSmagorinsky (filters, Leonard stress, dynamic coefficient, the
+    in-place list-order averaging run as hyperplanes, the clamp) against the
+    oracle's loop-by-loop restatement, bit for bit, twice in a row (the work
+    fields persist in the context)."""
+    sc, geom, ctx, osc = env
+    n = ctx.size()
+    for seed in (41, 42):
+        u, v, w = rnd(seed, n), rnd(seed + 10, n), rnd(seed + 20, n)
+        du, dv, dw = (ctx.field(a) for a in (u, v, w))
+        ev0 = rnd(seed + 30, n)
+        dev = ctx.field(ev0)
+        # nu large enough that some cells take the clamp
+        nu = 1e-3
+        A.cuda_check(ctx.lib.artss_turb_dynamic_smagorinsky(ctx.h, dev, du, dv, dw, nu), "dynamic smagorinsky")
+        ref = ev0.copy()
+        oracle.lib().oracle_dynamic_smagorinsky(osc.ptr, P(ref), P(u), P(v), P(w), nu)
+        got = ctx.download(dev)
+        assert np.array_equal(got, ref)
+        inner = geom.list("inner", 0)
+        assert (got[inner] == 0).any() and (got[inner] != 0).any()
+
+
 def test_smagorinsky_divergence_projection_sources(env):
     sc, geom, ctx, osc = env
     L = oracle.lib()

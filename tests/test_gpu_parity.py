@@ -57,6 +57,11 @@ def _scenes():
         "nstemp_dissipation": scenes.plume_box(n=32, steps=3, n_level=3, solver="NSTempSolver", dissipation=True),
         "nstempturb_explicit_dissipation": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=3, n_level=3,
                                                                     diffusion="Explicit", dissipation=True),
+        # DynamicSmagorinsky (src/turbulence/DynamicSmagorinsky.cpp:172-427) in the turbulent timestep
+        "nstempturb_dynamic_smagorinsky": scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=3, n_level=3,
+                                                                   turbulence="DynamicSmagorinsky"),
+        "diffusion_turb_dynamic": scenes.velocity_scene("DiffusionTurbSolver", n=32, steps=3,
+                                                        turbulence="DynamicSmagorinsky"),
         # PressureSolver (src/solver/PressureSolver.cpp:30-43) on the SinSinSin right-hand side
         "pressure_sinsinsin": scenes.pressure_scene(n=32, n_level=4, steps=2),
     }
