@@ -317,6 +317,34 @@ Temperature parse_temperature(const XmlElement *head, const std::string &parent,
     return t;
 }
 
+// Settings.cpp:840-889
+Concentration parse_concentration(const XmlElement *head, const std::string &parent, bool turbulence) {
+    const std::string context = ctx_join(parent, "concentration");
+    Section s = section(head, "concentration");
+    const XmlElement *sub = need(s, context);
+    Concentration c;
+    c.advection = parse_advection(sub, context);
+    c.diffusion = parse_diffusion(sub, context);
+    if (turbulence) {
+        Section ts = section(sub, "turbulence");
+        const std::string c2 = ctx_join(context, "turbulence");
+        c.has_turbulence = req_bool(ts.values, "include", c2);
+        if (c.has_turbulence) c.turbulent_schmidt_number = req_real(ts.values, "Sc_T", c2);
+    }
+    Section ss = section(sub, "source");
+    const std::string cs = "source";
+    c.source.type = req_str(ss.values, "type", cs);
+    c.source.dir = axes_of(req_str(ss.values, "dir", cs));
+    c.source.random = req_bool(ss.values, "random", cs);
+    if (c.source.random) c.source.random_parameters = parse_random(need(ss, ctx_join(context, cs)), ctx_join(context, cs));
+    c.source.con_fct = req_str(ss.values, "con_fct", cs);
+    if (c.source.con_fct == "Gauss") c.source.gauss = parse_gauss(ss.values, cs);
+    else if (c.source.con_fct == "Cube") c.source.cube = parse_cube(ss.values, cs);
+    else
+        throw config_error("concentration source function '" + c.source.con_fct + "' has no parsing implementation.");
+    return c;
+}
+
 Solver parse_solver(const XmlElement *root) {
     const std::string context = "solver";
     Section s = section(root, context);
@@ -351,6 +379,21 @@ Solver parse_solver(const XmlElement *root) {
         sp.pressure = parse_pressure(sub, context);
         sp.temperature = parse_temperature(sub, context, true);
         sp.turbulence = parse_turbulence(sub, context);
+        sp.source = parse_source(sub, context);
+    } else if (d == "NSTempConSolver") {
+        sp.advection = parse_advection(sub, context);
+        sp.diffusion = parse_diffusion(sub, context);
+        sp.pressure = parse_pressure(sub, context);
+        sp.temperature = parse_temperature(sub, context, false);
+        sp.concentration = parse_concentration(sub, context, false);
+        sp.source = parse_source(sub, context);
+    } else if (d == "NSTempTurbConSolver") {
+        sp.advection = parse_advection(sub, context);
+        sp.diffusion = parse_diffusion(sub, context);
+        sp.pressure = parse_pressure(sub, context);
+        sp.temperature = parse_temperature(sub, context, true);
+        sp.turbulence = parse_turbulence(sub, context);
+        sp.concentration = parse_concentration(sub, context, true);
         sp.source = parse_source(sub, context);
     } else if (d == "NSTurbSolver") {
         sp.advection = parse_advection(sub, context);

@@ -128,6 +128,26 @@ struct Temperature {
     TemperatureSource source;
 };
 
+// concentration block of NSTempConSolver / NSTempTurbConSolver
+// (Settings.cpp:840-889): the source's con_fct is Gauss or Cube
+struct ConcentrationSource {
+    std::string type;
+    std::vector<int> dir;
+    std::string con_fct;
+    bool random = false;
+    Random random_parameters;
+    Gauss gauss;
+    Cube cube;
+};
+
+struct Concentration {
+    Advection advection;
+    Diffusion diffusion;
+    bool has_turbulence = false;
+    std::optional<double> turbulent_schmidt_number;
+    ConcentrationSource source;
+};
+
 struct Solver {
     std::string description;
     Advection advection;
@@ -136,6 +156,7 @@ struct Solver {
     Source source;
     Pressure pressure;
     Temperature temperature;
+    Concentration concentration;
     bool analytical_solution = false;
 };
 

@@ -55,6 +55,17 @@ static std::unique_ptr<ISourceFunction> make_temperature_source_function(Runtime
     throw config_error("temperature source function '" + s.temp_fct + "' is not implemented");
 }
 
+// SolverSelection::set_concentration_source_function (src/solver/SolverSelection.cpp:165-190):
+// the Gauss function of the concentration settings
+static std::unique_ptr<ISourceFunction> make_concentration_source_function(Runtime &rt,
+                                                                            const settings::ConcentrationSource &s) {
+    if (s.con_fct == "Gauss") {
+        if (s.random) throw config_error("a concentration-source noise is not implemented");
+        return std::make_unique<GaussFunction>(rt, s.gauss);
+    }
+    throw config_error("concentration source function '" + s.con_fct + "' is not implemented");
+}
+
 // ---------------------------------------------------------------- fields
 
 FieldController::FieldController(Runtime &rt)
@@ -63,14 +74,24 @@ FieldController::FieldController(Runtime &rt)
       T0(rt, F_T), T_tmp(rt, F_T), T_ambient(rt, F_T), f_x(rt, F_U), f_y(rt, F_V), f_z(rt, F_W), S_T(rt, F_T),
       m_rt(rt) {}
 
+void FieldController::enable_concentration() {
+    if (C) return;
+    C = std::make_unique<Field>(m_rt, F_RHO);
+    C0 = std::make_unique<Field>(m_rt, F_RHO);
+    C_tmp = std::make_unique<Field>(m_rt, F_RHO);
+    S_C = std::make_unique<Field>(m_rt, F_RHO);
+    gamma_t = std::make_unique<Field>(m_rt, F_RHO);
+}
+
 void FieldController::set_up_boundary() {
-    // FieldController::set_up_boundary (src/field/FieldController.cpp:102-112); the
-    // concentration field is all zero on this path and carries no boundary data
+    // FieldController::set_up_boundary (src/field/FieldController.cpp:102-112); without a
+    // concentration solver the concentration field is all zero and unused here
     m_rt.apply_boundary(u);
     m_rt.apply_boundary(v);
     m_rt.apply_boundary(w);
     m_rt.apply_boundary(p);
     m_rt.apply_boundary(T);
+    if (C) m_rt.apply_boundary(*C);
     m_rt.apply_boundary(T_ambient);
 }
 
@@ -79,6 +100,7 @@ void FieldController::update_data() {
     couple_vector(u, u0, u_tmp, v, v0, v_tmp, w, w0, w_tmp);
     p0.copy_data(p);
     couple_scalar(T, T0, T_tmp);
+    if (C) couple_scalar(*C, *C0, *C_tmp);
 }
 
 void FieldController::couple_vector(const Field &a, Field &a0, Field &a_tmp, const Field &b, Field &b0, Field &b_tmp,
@@ -124,13 +146,18 @@ Field *FieldController::by_name(const std::string &n) {
     if (n == "f_y") return &f_y;
     if (n == "f_z") return &f_z;
     if (n == "S_T") return &S_T;
+    if (n == "C") return C.get();
+    if (n == "C0") return C0.get();
+    if (n == "C_tmp") return C_tmp.get();
+    if (n == "S_C") return S_C.get();
+    if (n == "gamma_t") return gamma_t.get();
     return nullptr;
 }
 
 // ---------------------------------------------------------------- NSTempTurbSolver
 
-NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent)
-    : m_rt(rt), m_fc(fc), m_turb(turbulent) {
+NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent, bool concentration)
+    : m_rt(rt), m_fc(fc), m_turb(turbulent), m_con(concentration) {
     // NSTempSolver (src/solver/NSTempSolver.cpp:19-48) is the same composition
     // without the turbulence model
     const settings::Solver &s = rt.settings().solver;
@@ -159,6 +186,21 @@ NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbul
     dif_temp->in_is_scratch = true;
     dif_vel->out_holds_in = true;
     dif_temp->out_holds_in = true;
+    if (m_con) {
+        // NSTempTurbConSolver.cpp:28-53 / NSTempConSolver.cpp:29-51, with the concentration's
+        // advection held in its own slot (the reference stores it in adv_temp a second time
+        // and never sets adv_con, so its do_step cannot run; this is the evident intent)
+        m_fc.enable_concentration();
+        adv_con = make_advection(rt, s.concentration.advection);
+        dif_con = make_diffusion(rt, s.diffusion);  // the velocity settings, as for the temperature
+        sou_con = make_source(rt, s.concentration.source.type, s.concentration.source.dir);
+        m_source_function_concentration = make_concentration_source_function(rt, s.concentration.source);
+        m_add_con_source = s.concentration.source.con_fct != "Zero";
+        if (s.concentration.advection.fields != std::vector<int>{F_RHO} ||
+            s.concentration.diffusion.fields != std::vector<int>{F_RHO})
+            throw config_error("Fields not specified correctly!");
+        if (!m_rt.settings().physical.gamma) throw config_error("physical_parameters: gamma missing");
+    }
 }
 
 void NSTempTurbSolver::do_step(real t, bool sync) {
@@ -246,6 +288,29 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     // after each writes T0 and T_tmp, which update_data rewrites before anything reads them
     if (m_dissipation) sou_temp->dissipate(f.T, f.u, f.v, f.w, sync);
     if (m_add_temp_source) sou_temp->add_source(f.T, f.S_T, sync);
+
+    // 6. concentration (NSTempTurbConSolver.cpp:243-286, NSTempConSolver.cpp:203-232)
+    if (!m_con) return;
+    Field &C = *f.C, &C0 = *f.C0, &C_tmp = *f.C_tmp;
+    const real gamma = phys.gamma.value();
+    const auto &cs = m_rt.settings().solver.concentration;
+    adv_con->advect(C, C0, f.u, f.v, f.w, sync);
+    FieldController::couple_scalar(C, C0, C_tmp);
+    if (m_turb && cs.has_turbulence) {
+        const real rSc_T = 1. / cs.turbulent_schmidt_number.value();
+        check(artss_scale_copy(m_rt.ctx(), f.gamma_t->data, f.nu_t.data, rSc_T, 0), "gamma_t");
+        dif_con->diffuse(C, C0, C_tmp, gamma, *f.gamma_t, sync);
+        FieldController::couple_scalar(C, C0, C_tmp);
+    } else if (gamma != 0.) {
+        dif_con->diffuse(C, C0, C_tmp, gamma, sync);
+        FieldController::couple_scalar(C, C0, C_tmp);
+    }
+    // the turbulent solver adds the source when the concentration has turbulence
+    // (NSTempTurbConSolver.cpp:278), the laminar one when a source function is set
+    if (m_turb ? cs.has_turbulence : m_add_con_source) {
+        sou_con->add_source(C, *f.S_C, sync);
+        FieldController::couple_scalar(C, C0, C_tmp);
+    }
 }
 
 // couple_vector after the velocity diffusion (:152): with a momentum source
@@ -257,9 +322,15 @@ void NSTempTurbSolver::couple_after_diffusion() {
     if (!m_add_source) FieldController::couple_tmp(f.u, f.u_tmp, f.v, f.v_tmp, f.w, f.w_tmp);
 }
 
-void NSTempTurbSolver::update_source(real t_cur) { m_source_function_temperature->update_source(m_fc.S_T, t_cur); }
+void NSTempTurbSolver::update_source(real t_cur) {
+    m_source_function_temperature->update_source(m_fc.S_T, t_cur);
+    if (m_con) m_source_function_concentration->update_source(*m_fc.S_C, t_cur);
+}
 
-void NSTempTurbSolver::update_obstacle_change() { m_source_function_temperature->update_obstacle_change(); }
+void NSTempTurbSolver::update_obstacle_change() {
+    m_source_function_temperature->update_obstacle_change();
+    if (m_con) m_source_function_concentration->update_obstacle_change();
+}
 
 // ---------------------------------------------------------------- NSSolver / NSTurbSolver
 
@@ -371,8 +442,9 @@ void PressureSolver::do_step(real t, bool sync) { pres->pressure(m_fc.p, m_fc.rh
 SolverController::SolverController(Runtime &rt) : m_rt(rt) {
     m_fc = std::make_unique<FieldController>(rt);
     const std::string &d = rt.settings().solver.description;
-    if (d == "NSTempTurbSolver" || d == "NSTempSolver") {
-        m_solver = std::make_unique<NSTempTurbSolver>(rt, *m_fc, d == "NSTempTurbSolver");
+    if (d == "NSTempTurbSolver" || d == "NSTempSolver" || d == "NSTempTurbConSolver" || d == "NSTempConSolver") {
+        m_solver = std::make_unique<NSTempTurbSolver>(rt, *m_fc, d == "NSTempTurbSolver" || d == "NSTempTurbConSolver",
+                                                      d == "NSTempTurbConSolver" || d == "NSTempConSolver");
         m_has_momentum_source = true;
     } else if (d == "NSSolver" || d == "NSTurbSolver") {
         m_solver = std::make_unique<NSSolver>(rt, *m_fc, d == "NSTurbSolver");
@@ -545,7 +617,8 @@ void SolverController::set_up_fields() {
                            "Vortex, Zero (the initial conditions of the solvers this library runs)");
     }
     const std::string &d = m_rt.settings().solver.description;
-    if (d == "NSTempTurbSolver" || d == "NSTempSolver") force_source();
+    if (d == "NSTempTurbSolver" || d == "NSTempSolver" || d == "NSTempTurbConSolver" || d == "NSTempConSolver")
+        force_source();
 }
 
 void SolverController::force_source() {

@@ -24,7 +24,11 @@ class FieldController {
     Field T, T0, T_tmp, T_ambient;
     Field f_x, f_y, f_z;
     Field S_T;
+    // concentration, its copies, source and eddy diffusivity (field type rho);
+    // allocated by enable_concentration for NSTempConSolver / NSTempTurbConSolver
+    std::unique_ptr<Field> C, C0, C_tmp, S_C, gamma_t;
 
+    void enable_concentration();
     void set_up_boundary();
     void update_data();
     static void couple_vector(const Field &a, Field &a0, Field &a_tmp, const Field &b, Field &b0, Field &b_tmp,
@@ -55,9 +59,12 @@ struct StepStats {
 };
 
 // NSTempTurbSolver (src/solver/NSTempTurbSolver.cpp:94-248)
+// NSTempTurbSolver (src/solver/NSTempTurbSolver.cpp); turbulent = false:
+// NSTempSolver; concentration = true: NSTempTurbConSolver / NSTempConSolver
+// (src/solver/NSTempTurbConSolver.cpp, NSTempConSolver.cpp)
 class NSTempTurbSolver : public ISolver {
  public:
-    NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent = true);
+    NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent = true, bool concentration = false);
     void do_step(real t, bool sync) override;
     void update_source(real t_cur) override;
     void update_obstacle_change() override;
@@ -75,6 +82,11 @@ class NSTempTurbSolver : public ISolver {
     std::unique_ptr<ISource> sou_vel, sou_temp;
     std::unique_ptr<ISourceFunction> m_source_function_temperature;
     bool m_add_source = false, m_add_temp_source = false, m_dissipation = false;
+    bool m_con = false, m_add_con_source = false;
+    std::unique_ptr<IAdvection> adv_con;
+    std::unique_ptr<IDiffusion> dif_con;
+    std::unique_ptr<ISource> sou_con;
+    std::unique_ptr<ISourceFunction> m_source_function_concentration;
 };
 
 // NSSolver / NSTurbSolver (src/solver/NSSolver.cpp, NSTurbSolver.cpp)

@@ -52,6 +52,11 @@ class Scene:
     diff_tol: float = 1e-7
     cs: float = 0.2
     turbulence: str = "ConstSmagorinsky"  # or "DynamicSmagorinsky" (no parameters)
+    # NSTempTurbSolver / NSTempSolver scenes written as NSTempTurbConSolver /
+    # NSTempConSolver with a concentration set up exactly like the temperature
+    # (gamma = kappa, Sc_T = Pr_T, the same Gauss source, the T boundary
+    # conditions for rho)
+    concentration: bool = False
     buoyancy_dir: str = "z"
     t_ambient: float = 299.15
     n_level: int = 4
@@ -370,8 +375,15 @@ def to_xml(s: Scene) -> str:
         a("    <rhoa> 1 </rhoa>")
         if temperature:
             a(f"    <kappa> {_f(s.kappa)} </kappa>")
+        if s.concentration:
+            a(f"    <gamma> {_f(s.kappa)} </gamma>")
     a("  </physical_parameters>")
-    a(f'  <solver description="{s.solver}" >')
+    description = s.solver
+    if s.concentration:
+        if s.solver not in ("NSTempTurbSolver", "NSTempSolver"):
+            raise ValueError("concentration needs NSTempTurbSolver or NSTempSolver")
+        description = "NSTempTurbConSolver" if s.solver == "NSTempTurbSolver" else "NSTempConSolver"
+    a(f'  <solver description="{description}" >')
 
     def turbulence_block():
         if s.turbulence == "DynamicSmagorinsky":
@@ -443,6 +455,27 @@ def to_xml(s: Scene) -> str:
         a(f"        <tau> {_f(s.tau)} </tau>")
         a("      </source>")
         a("    </temperature>")
+        if s.concentration:
+            a("    <concentration>")
+            a('      <advection type="SemiLagrangian" field="rho">')
+            a("      </advection>")
+            diffusion_block("rho", "      ", s.diffusion, s.diff_max_iter, s.diff_tol, 1.0)
+            if turbulent:
+                a('      <turbulence include="Yes">')
+                a(f"        <Sc_T> {_f(s.pr_t)} </Sc_T>")
+                a("      </turbulence>")
+            a(f'      <source type="ExplicitEuler" dir="{s.buoyancy_dir}" con_fct="Gauss" random="No">')
+            a(f"        <HRR> {_f(s.hrr)} </HRR>")
+            a(f"        <cp> {_f(s.cp)} </cp>")
+            a(f"        <x0> {_f(s.source_pos[0])} </x0>")
+            a(f"        <y0> {_f(s.source_pos[1])} </y0>")
+            a(f"        <z0> {_f(s.source_pos[2])} </z0>")
+            a(f"        <sigma_x> {_f(s.sigma[0])} </sigma_x>")
+            a(f"        <sigma_y> {_f(s.sigma[1])} </sigma_y>")
+            a(f"        <sigma_z> {_f(s.sigma[2])} </sigma_z>")
+            a(f"        <tau> {_f(s.tau)} </tau>")
+            a("      </source>")
+            a("    </concentration>")
     a('    <solution available="No">')
     a("    </solution>")
     a("  </solver>")
@@ -456,8 +489,14 @@ def to_xml(s: Scene) -> str:
     a("  </domain_parameters>")
     a('  <adaption dynamic="No" data_extraction="No"> </adaption>')
     a('  <data_assimilation enabled="No" />')
+    def with_rho(bcs):
+        out = list(bcs)
+        if s.concentration:
+            out += [("rho", patch, typ, val) for fld, patch, typ, val in bcs if "T" in fld.split(",")]
+        return out
+
     a("  <boundaries>")
-    for fld, patch, typ, val in s.boundaries:
+    for fld, patch, typ, val in with_rho(s.boundaries):
         a(f'    <boundary field="{fld}" patch="{patch}" type="{typ}" value="{_f(val)}" />')
     a("  </boundaries>")
     if s.obstacles:
@@ -466,7 +505,7 @@ def to_xml(s: Scene) -> str:
             a(f'    <obstacle name="{b.name}">')
             a(f'      <geometry ox1="{_f(b.x1)}" ox2="{_f(b.x2)}" oy1="{_f(b.y1)}" oy2="{_f(b.y2)}"'
               f' oz1="{_f(b.z1)}" oz2="{_f(b.z2)}"/>')
-            for fld, patch, typ, val in (s.obstacle_bcs or solid_obstacle_bcs()):
+            for fld, patch, typ, val in with_rho(s.obstacle_bcs or solid_obstacle_bcs()):
                 a(f'      <boundary field="{fld}" patch="{patch}" type="{typ}" value="{_f(val)}"/>')
             a("    </obstacle>")
         a("  </obstacles>")
