@@ -347,6 +347,73 @@ __device__ __forceinline__ void column_march(const T *__restrict__ f, int base, 
     }
 }
 
+// Launch shapes the autotuner tries for column kernels: threads of a block in
+// x and y, and the cap on the number of blocks (the z extent of the grid is
+// the box's planes, capped so that x * y * z blocks stay within it).  Shape 0
+// is the untuned default.
+struct ColShape {
+    unsigned bx, by, cap;
+};
+constexpr ColShape kColShapes[] = {{64, 4, 2048}, {32, 8, 2048}, {128, 2, 2048}, {32, 4, 4096},
+                                   {64, 4, 4096}, {64, 4, 1024}, {128, 4, 1024}, {256, 1, 2048}};
+constexpr int kColShapeCount = (int) (sizeof(kColShapes) / sizeof(kColShapes[0]));
+inline dim3 col_grid(const Box3 &b, const ColShape &s) {
+    const int64_t gx = (b.nx() + s.bx - 1) / s.bx, gy = (b.ny() + s.by - 1) / s.by;
+    const int64_t cap = std::max<int64_t>(1, (int64_t) s.cap / std::max<int64_t>(gx * gy, 1));
+    return dim3((unsigned) gx, (unsigned) gy, (unsigned) std::max<int64_t>(1, std::min<int64_t>(b.nz(), cap)));
+}
+// Kernel ids of the launch-shape tuner (TuneKey::kernel; 0 is the sweep variant)
+enum ColKernel : int {
+    kTuneAdvect1 = 101, kTuneAdvect3, kTuneSmagorinsky, kTuneDivergence, kTuneProjection, kTuneBuoyancy,
+    kTuneMgJacobi, kTuneMgResiduum, kTuneMgRestrict, kTuneMgProlongate
+};
+
+// Launches a column kernel, `launch(grid, block)` returning a status, with the
+// tuned shape of (kernel, level shape).  The first eager call of a key times
+// every shape (one warm launch, then three) and keeps the fastest in the
+// context; the kernel must write the same values when it runs again with the
+// same arguments (its output is not its input) and must not reduce (a
+// reduction's order would follow the choice; a call whose output aliases an
+// input passes may_tune = false).  Inside a capture, with the autotuner off or
+// without may_tune, an untuned key launches shape 0.
+template <class F>
+int tuned_column_launch(artss_ctx *ctx, int kernel, int level, const Box3 &box, bool may_tune, F launch) {
+    const Level &L = ctx->lvl[level];
+    const TuneKey key{kernel, L.Nx, L.Ny, L.Nz, level};
+    auto it = ctx->tuned.find(key);
+    if (it != ctx->tuned.end()) {
+        const ColShape &s = kColShapes[it->second];
+        return launch(col_grid(box, s), dim3(s.bx, s.by, 1));
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    // captures that other code opened on the stream count too
+    if (!ctx->autotune || ctx->capturing || !may_tune || cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+        return launch(col_grid(box, kColShapes[0]), dim3(kBx, kBy, 1));
+    cudaEvent_t e0, e1;
+    ARTSS_CK(cudaEventCreate(&e0));
+    ARTSS_CK(cudaEventCreate(&e1));
+    int best = 0, st = ARTSS_OK;
+    float best_ms = 1e30f;
+    for (int v = 0; v < kColShapeCount && !st; v++) {
+        const ColShape &s = kColShapes[v];
+        const dim3 g = col_grid(box, s), b(s.bx, s.by, 1);
+        if ((st = launch(g, b))) break;
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < 3 && !st; r++) st = launch(g, b);
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) { st = cuda_fail(cudaGetLastError(), "launch-shape tuning"); break; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    ctx->tuned[key] = best;
+    return ARTSS_OK;
+}
+
 // Grid-size helper for flat (1-D) loops over n elements.
 inline unsigned flat_blocks(int64_t n, int threads = 256) {
     int64_t b = (n + threads - 1) / threads;

@@ -216,10 +216,12 @@ int mg_jacobi_step(artss_mg *mg, double *out, const double *in, const double *b,
     artss_ctx *ctx = mg->ctx;
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mg_jacobi, mg_grid(box), box_block(), 0, out, in, b, ctx->d_flags[level], L, box,
-                                                               mg_coef(mg, level));
-    ARTSS_LAUNCH_CK(ctx);
-    return ARTSS_OK;
+    const MgCoef c = mg_coef(mg, level);
+    return tuned_column_launch(ctx, kTuneMgJacobi, level, box, out != in && out != b, [&](dim3 g, dim3 bl) -> int {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mg_jacobi, g, bl, 0, out, in, b, ctx->d_flags[level], L, box, c);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    });
 }
 
 int mg_cgs_step(artss_mg *mg, double *out, const double *b, int level) {
@@ -1370,20 +1372,24 @@ int mg_restrict(artss_mg *mg, double *coarse, const double *fine, int coarse_lev
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mg_restrict, mg_grid(box), box_block(), 0, coarse, fine, ctx->d_flags[coarse_level], C,
-                                                                 ctx->lvl[coarse_level - 1], box);
-    ARTSS_LAUNCH_CK(ctx);
-    return ARTSS_OK;
+    return tuned_column_launch(ctx, kTuneMgRestrict, coarse_level, box, true, [&](dim3 g, dim3 b) -> int {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mg_restrict, g, b, 0, coarse, fine, ctx->d_flags[coarse_level], C,
+                         ctx->lvl[coarse_level - 1], box);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    });
 }
 
 int mg_prolongate(artss_mg *mg, double *fine, const double *coarse, int coarse_level) {
     artss_ctx *ctx = mg->ctx;
     const Level &C = ctx->lvl[coarse_level];
     const Box3 box = inner_box(C);
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mg_prolongate, mg_grid(box), box_block(), 0, fine, coarse, ctx->d_flags[coarse_level], C,
-                                                                   ctx->lvl[coarse_level - 1], box);
-    ARTSS_LAUNCH_CK(ctx);
-    return ARTSS_OK;
+    return tuned_column_launch(ctx, kTuneMgProlongate, coarse_level, box, true, [&](dim3 g, dim3 b) -> int {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mg_prolongate, g, b, 0, fine, coarse, ctx->d_flags[coarse_level], C,
+                         ctx->lvl[coarse_level - 1], box);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    });
 }
 
 int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, int level) {
@@ -1391,12 +1397,14 @@ int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, in
     const Level &L = ctx->lvl[level];
     const Box3 box = inner_box(L);
     const artss_grid_desc &g = ctx->grid;
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mg_residuum, mg_grid(box), box_block(), 0, out, in, b, ctx->d_flags[level], L, box,
-                                                                 1. / (g.dx[level] * g.dx[level]),
-                                                                 1. / (g.dy[level] * g.dy[level]),
-                                                                 1. / (g.dz[level] * g.dz[level]));
-    ARTSS_LAUNCH_CK(ctx);
-    return ARTSS_OK;
+    const double rx = 1. / (g.dx[level] * g.dx[level]), ry = 1. / (g.dy[level] * g.dy[level]),
+                 rz = 1. / (g.dz[level] * g.dz[level]);
+    return tuned_column_launch(ctx, kTuneMgResiduum, level, box, out != in && out != b, [&](dim3 gr, dim3 bl) -> int {
+        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mg_residuum, gr, bl, 0, out, in, b, ctx->d_flags[level], L, box, rx,
+                         ry, rz);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    });
 }
 
 // VCycleMG::VCycleMultigrid (VCycleMG.cpp:215-288).  The reference copies out

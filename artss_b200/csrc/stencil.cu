@@ -1466,10 +1466,14 @@ int artss_advect_sl(artss_ctx *ctx, double *out, const double *in, const double 
     if (L.size() >= ((int64_t) 1 << 31)) { set_error("advection: level of 2^31 cells or more"); return ARTSS_ERR_LIMIT; }
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
-    const dim3 g = zgrid(box);
-    ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<1>), g, box_block(), 0, out, nullptr, nullptr, in, nullptr, nullptr, u, v, w,
-                                                    ctx->d_flags[0], L, box, c);
-    ARTSS_LAUNCH_CK(ctx);
+    const bool fresh = out != in && out != u && out != v && out != w;
+    if ((st = tuned_column_launch(ctx, kTuneAdvect1, 0, box, fresh, [&](dim3 g, dim3 b) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<1>), g, b, 0, out, nullptr, nullptr, in, nullptr, nullptr, u,
+                              v, w, ctx->d_flags[0], L, box, c);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     return apply_bc(ctx, out, 0, out_field_type);
 }
 
@@ -1482,10 +1486,16 @@ int artss_advect_sl_uvw(artss_ctx *ctx, double *out_u, double *out_v, double *ou
     if (L.size() >= ((int64_t) 1 << 31)) { set_error("advection: level of 2^31 cells or more"); return ARTSS_ERR_LIMIT; }
     const Box3 box = inner_box(L);
     AdvCoef c{dt / ctx->grid.dx[0], dt / ctx->grid.dy[0], dt / ctx->grid.dz[0], L.i1, L.i2, L.j1, L.j2, L.k1, L.k2};
-    const dim3 g = zgrid(box);
-    ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<3>), g, box_block(), 0, out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
-                                                    ctx->d_flags[0], L, box, c);
-    ARTSS_LAUNCH_CK(ctx);
+    bool fresh = true;
+    for (const double *o : {(const double *) out_u, (const double *) out_v, (const double *) out_w})
+        for (const double *x : {in_u, in_v, in_w, u, v, w}) fresh = fresh && o != x;
+    if ((st = tuned_column_launch(ctx, kTuneAdvect3, 0, box, fresh, [&](dim3 g, dim3 b) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_ADVECT, (k_advect<3>), g, b, 0, out_u, out_v, out_w, in_u, in_v, in_w, u, v, w,
+                              ctx->d_flags[0], L, box, c);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     if ((st = apply_bc(ctx, out_u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, out_v, 0, ARTSS_FIELD_V))) return st;
     return apply_bc(ctx, out_w, 0, ARTSS_FIELD_W);
@@ -1500,9 +1510,14 @@ int artss_turb_const_smagorinsky(artss_ctx *ctx, double *nu_t, const double *u, 
     const double dx = ctx->grid.dx[0], dy = ctx->grid.dy[0], dz = ctx->grid.dz[0];
     const double delta_s = cbrt(dx * dy * dz);
     const double cs2d2 = cs * cs * delta_s * delta_s;
-    ARTSS_LAUNCH_PDL(ctx, FAM_SMAGORINSKY, k_smagorinsky, zgrid(box), box_block(), 0, nu_t, u, v, w, ctx->d_flags[0], L, box, 1. / dx,
-                                                               1. / dy, 1. / dz, cs2d2);
-    ARTSS_LAUNCH_CK(ctx);
+    const bool fresh = nu_t != u && nu_t != v && nu_t != w;
+    if ((st = tuned_column_launch(ctx, kTuneSmagorinsky, 0, box, fresh, [&](dim3 g, dim3 b) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_SMAGORINSKY, k_smagorinsky, g, b, 0, nu_t, u, v, w, ctx->d_flags[0], L, box,
+                              1. / dx, 1. / dy, 1. / dz, cs2d2);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     return apply_bc(ctx, nu_t, 0, ARTSS_FIELD_NU);
 }
 
@@ -1514,8 +1529,14 @@ int artss_divergence(artss_ctx *ctx, double *rhs, const double *u, const double 
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    ARTSS_LAUNCH_PDL(ctx, FAM_DIVERGENCE, k_divergence, zgrid(box), box_block(), 0, rhs, u, v, w, ctx->d_flags[0], L, box, hx, hy, hz);
-    ARTSS_LAUNCH_CK(ctx);
+    const bool fresh = rhs != u && rhs != v && rhs != w;
+    if ((st = tuned_column_launch(ctx, kTuneDivergence, 0, box, fresh, [&](dim3 g, dim3 b) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_DIVERGENCE, k_divergence, g, b, 0, rhs, u, v, w, ctx->d_flags[0], L, box, hx,
+                              hy, hz);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     const Box3 ring = domain_box(L);
     ARTSS_LAUNCH_PDL(ctx, FAM_DIVERGENCE, k_ghost_ring_zero, zgrid(ring), box_block(), 0, rhs, L, ring);
     ARTSS_LAUNCH_CK(ctx);
@@ -1531,9 +1552,16 @@ int artss_projection(artss_ctx *ctx, double *u, double *v, double *w, const doub
     const double hx = 0.5 * (1. / ctx->grid.dx[0]);
     const double hy = 0.5 * (1. / ctx->grid.dy[0]);
     const double hz = 0.5 * (1. / ctx->grid.dz[0]);
-    ARTSS_LAUNCH_PDL(ctx, FAM_PROJECTION, k_projection, zgrid(box), box_block(), 0, u, v, w, us, vs, ws, p, ctx->d_flags[0], L, box, hx,
-                                                              hy, hz);
-    ARTSS_LAUNCH_CK(ctx);
+    bool fresh = true;
+    for (const double *o : {(const double *) u, (const double *) v, (const double *) w})
+        for (const double *x : {us, vs, ws, p}) fresh = fresh && o != x;
+    if ((st = tuned_column_launch(ctx, kTuneProjection, 0, box, fresh, [&](dim3 g, dim3 b) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_PROJECTION, k_projection, g, b, 0, u, v, w, us, vs, ws, p, ctx->d_flags[0], L,
+                              box, hx, hy, hz);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     if ((st = apply_bc(ctx, u, 0, ARTSS_FIELD_U))) return st;
     if ((st = apply_bc(ctx, v, 0, ARTSS_FIELD_V))) return st;
     return apply_bc(ctx, w, 0, ARTSS_FIELD_W);
@@ -1544,9 +1572,12 @@ int artss_buoyancy_force(artss_ctx *ctx, double *force, const double *T, const d
     if (st) return st;
     const Level &L = ctx->lvl[0];
     const Box3 box = domain_box(L);
-    ARTSS_LAUNCH_PDL(ctx, FAM_BUOYANCY, k_buoyancy, zgrid(box), box_block(), 0, force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
-    ARTSS_LAUNCH_CK(ctx);
-    return ARTSS_OK;
+    const bool fresh = force != T && force != Ta;
+    return tuned_column_launch(ctx, kTuneBuoyancy, 0, box, fresh, [&](dim3 gr, dim3 b) -> int {
+        ARTSS_LAUNCH_PDL(ctx, FAM_BUOYANCY, k_buoyancy, gr, b, 0, force, T, Ta, ctx->d_flags[0], L, box, -beta, g);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    });
 }
 
 int artss_cfl(artss_ctx *ctx, const double *u, const double *v, const double *w, double dt, double *cfl) {
