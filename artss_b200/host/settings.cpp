@@ -479,6 +479,18 @@ InitialConditions parse_ic(const XmlElement *root) {
     for (const auto &k : it->second) req_str(s.values, k, c2);
     if (ic.usr_fct == "Uniform") ic.uniform_value = req_real(s.values, "val", c2);
     else if (ic.usr_fct == "SinSinSin") ic.sin_l = req_real(s.values, "l", c2);
+    else if (ic.usr_fct == "LayersT") {
+        // parse_layers_parameters (src/utility/settings/Settings.cpp:302-321)
+        const size_t n = req_size(s.values, "n_layers", c2);
+        if (n == 0)
+            throw config_error("Numbers of layers has to be at least 1. Current value: " + std::to_string(n));
+        ic.layers_dir = match_axis(req_str(s.values, "dir", c2));
+        for (size_t i = 1; i < n; i++) {
+            ic.layers_values.push_back(req_real(s.values, "value_" + std::to_string(i), c2));
+            ic.layers_borders.push_back(req_real(s.values, "border_" + std::to_string(i), c2));
+        }
+        ic.layers_values.push_back(req_real(s.values, "value_" + std::to_string(n), c2));
+    }
     return ic;
 }
 
@@ -540,9 +552,20 @@ Settings parse_settings(const std::string &content, const std::string &filename)
             throw config_error("surfaces are not supported by this library (no reference configuration uses them)");
     }
     {
-        Section da = section(root, "data_assimilation");
-        if (req_bool(da.values, "enabled", "data_assimilation"))
-            throw config_error("data assimilation is not part of this library");
+        // parse_assimilation_parameters (src/utility/settings/Settings.cpp:971-989).  The
+        // reference acts on the section only in builds with ASSIMILATION defined (MPI
+        // ranks, src/TimeIntegration.cpp:124-133 and :158-186, src/main.cpp:63-110); its serial and single-GPU
+        // builds parse it and run the plain time loop.  This library does the same.
+        const std::string context = "data_assimilation";
+        Section da = section(root, context);
+        st.assimilation.enabled = req_bool(da.values, "enabled", context);
+        if (st.assimilation.enabled) {
+            st.assimilation.class_name = req_str(da.values, "class_name", context);
+            if (opt_bool(da.values, "load_data", false)) {
+                req_str(da.values, "file", context);
+                req_real(da.values, "time", context);
+            }
+        }
     }
     st.ic = parse_ic(root);
     {

@@ -166,7 +166,17 @@ struct InitialConditions {
     Random random_parameters;
     double uniform_value = 0;   // Uniform: val
     double sin_l = 0;           // SinSinSin: l
+    int layers_dir = -1;                  // LayersT: axis across the layers
+    std::vector<double> layers_values;    // LayersT: value_1 .. value_n
+    std::vector<double> layers_borders;   // LayersT: border_1 .. border_{n-1}
     std::map<std::string, std::string> values;  // all parameters of the section
+};
+
+// data_assimilation section: parsed, without effect on the time loop (as in the
+// reference's builds without ASSIMILATION)
+struct Assimilation {
+    bool enabled = false;
+    std::string class_name;
 };
 
 struct Settings {
@@ -175,6 +185,7 @@ struct Settings {
     Solver solver;
     Domain domain;
     bool adaption = false;
+    Assimilation assimilation;
     std::vector<Boundary> boundaries;
     bool obstacles_enabled = false;
     std::vector<Obstacle> obstacles;

@@ -480,24 +480,85 @@ void SolverController::set_up_fields() {
     const auto &ic = m_rt.settings().ic;
     const Geometry &geo = m_rt.geometry();
     const IdxList &inner = geo.inner(0);
+    auto add_random = [&](std::vector<real> &T) {
+        // Functions::random (src/Functions.cpp:738-774); the draws cover
+        // all Nx*Ny*Nz cells in linear order, applied to inner cells
+        if (!ic.random) return;
+        const auto &r = ic.random_parameters;
+        if (!r.custom_seed) throw config_error("initial noise without custom_seed is not reproducible");
+        if (!r.absolute && (r.range > 1 || r.range < 0))
+            throw config_error("range for relative noise has to be between [0:1]");
+        UniformRandom noise(r.range, r.step_size, r.seed);
+        std::vector<real> n = noise.random_field(T.size());
+        for (Idx idx : inner) {
+            if (r.absolute) T[(size_t) idx] += n[(size_t) idx];
+            else T[(size_t) idx] *= (1 + n[(size_t) idx]);
+        }
+    };
     if (ic.usr_fct == "Uniform") {
         std::vector<real> T = m_fc->T.to_host();
         for (Idx idx : inner) T[(size_t) idx] = ic.uniform_value;
-        if (ic.random) {
-            // Functions::random (src/Functions.cpp:738-774); the draws cover
-            // all Nx*Ny*Nz cells in linear order, applied to inner cells
-            const auto &r = ic.random_parameters;
-            if (!r.custom_seed) throw config_error("initial noise without custom_seed is not reproducible");
-            if (!r.absolute && (r.range > 1 || r.range < 0))
-                throw config_error("range for relative noise has to be between [0:1]");
-            UniformRandom noise(r.range, r.step_size, r.seed);
-            std::vector<real> n = noise.random_field(T.size());
-            for (Idx idx : inner) {
-                if (r.absolute) T[(size_t) idx] += n[(size_t) idx];
-                else T[(size_t) idx] *= (1 + n[(size_t) idx]);
+        add_random(T);
+        m_fc->T.from_host(T);
+    } else if (ic.usr_fct == "LayersT") {
+        // Functions::layers (src/Functions.cpp:521-594): layer l covers the cells whose
+        // lower face lies in [border_l, border_{l+1}], the outer borders being the
+        // computational domain's; layers are written in order, so a cell whose face
+        // sits on a border takes the upper layer's value
+        std::vector<real> T = m_fc->T.to_host();
+        const int dir = ic.layers_dir;
+        if (dir >= 0) {
+            const Grid &grid = geo.grid();
+            const GridLevel &g = grid.level(0);
+            const size_t n = ic.layers_values.size();
+            std::vector<real> borders(n + 1);
+            for (size_t l = 1; l < n; l++) borders[l] = ic.layers_borders[l - 1];
+            borders[0] = grid.start_cd[dir];
+            borders[n] = grid.end_cd[dir];
+            const size_t Nx = g.N[0], Nxy = g.N[0] * g.N[1];
+            const real X1 = grid.start_pd[dir], h = g.spacing[dir];
+            for (size_t l = 0; l < n; l++)
+                for (Idx idx : inner) {
+                    const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx;
+                    const size_t i = (size_t) idx - k * Nxy - j * Nx;
+                    const size_t c = dir == 0 ? i : dir == 1 ? j : k;
+                    const real x = (X1 + ((real) c - 0.5) * h) - 0.5 * h;
+                    if (borders[l] <= x && x <= borders[l + 1]) T[(size_t) idx] = ic.layers_values[l];
+                }
+        }
+        add_random(T);
+        m_fc->T.from_host(T);
+    } else if (ic.usr_fct == "ExpSinusSum") {
+        // Functions::exp_sinus_sum (src/Functions.cpp:369-420) at t = 0: the Burgers
+        // test state on the inner cells of u, v and w, 3D when Nz > 3
+        const GridLevel &g = geo.grid().level(0);
+        const auto &X1 = geo.grid().start_pd;
+        const size_t Nx = g.N[0], Nxy = g.N[0] * g.N[1];
+        const real nu = m_rt.settings().physical.nu.value_or(0.0), t = 0.;
+        const bool three_d = g.N[2] > 3;
+        const real d = three_d ? 3. : 2.;
+        std::vector<real> u = m_fc->u.to_host(), v = m_fc->v.to_host(), w = m_fc->w.to_host();
+        for (Idx idx : inner) {
+            const size_t k = (size_t) idx / Nxy, j = ((size_t) idx - k * Nxy) / Nx, i = (size_t) idx - k * Nxy - j * Nx;
+            const real xi = X1[0] + ((real) i - 0.5) * g.spacing[0];
+            const real yj = X1[1] + ((real) j - 0.5) * g.spacing[1];
+            const real e = std::exp(-d * nu * t);
+            if (three_d) {
+                const real zk = X1[2] + ((real) k - 0.5) * g.spacing[2];
+                const real s = std::sin(xi + yj + zk);
+                u[(size_t) idx] = e * s;
+                v[(size_t) idx] = -0.5 * e * s;
+                w[(size_t) idx] = -0.5 * e * s;
+            } else {
+                const real s = std::sin(xi + yj);
+                u[(size_t) idx] = e * s;
+                v[(size_t) idx] = -e * s;
+                w[(size_t) idx] = 0.;
             }
         }
-        m_fc->T.from_host(T);
+        m_fc->u.from_host(u);
+        m_fc->v.from_host(v);
+        m_fc->w.from_host(w);
     } else if (ic.usr_fct == "SinSinSin") {
         // Functions::sin_sin_sin (src/Functions.cpp:782-812)
         m_fc->p.set_value(0.);
@@ -612,9 +673,13 @@ void SolverController::set_up_fields() {
         m_fc->p.from_host(p);
         if (ic.usr_fct != "Drift") m_fc->p.set_value(0.);
     } else if (ic.usr_fct != "Zero") {
+        // Jet (Functions::jet, src/Functions.cpp:658-688) measures its end indices from the
+        // END of the physical domain, so every end coordinate inside the domain gives a
+        // negative index converted to size_t, and its axis loops run to number_of_axes
+        // inclusive; no reference configuration uses it
         throw config_error("initial condition '" + ic.usr_fct +
-                           "' is not one of Uniform, SinSinSin, ExpSinusProd, GaussBubble, Hat, Drift, McDermott, "
-                           "Vortex, Zero (the initial conditions of the solvers this library runs)");
+                           "' is not one of Uniform, LayersT, SinSinSin, ExpSinusProd, ExpSinusSum, GaussBubble, Hat, "
+                           "Drift, McDermott, Vortex, Zero (the initial conditions of the solvers this library runs)");
     }
     const std::string &d = m_rt.settings().solver.description;
     if (d == "NSTempTurbSolver" || d == "NSTempSolver" || d == "NSTempTurbConSolver" || d == "NSTempConSolver")

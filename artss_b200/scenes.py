@@ -88,6 +88,14 @@ class Scene:
     force: str = "Buoyancy"  # momentum source force_fct: Buoyancy, Uniform or Zero
     force_value: Tuple[float, float, float] = (0.0, 0.0, 0.0)  # Uniform: val_x, val_y, val_z
     dissipation: bool = False  # temperature source: viscous dissipation (ISource::dissipate)
+    # computational domain inside the physical one (X, Y, Z): ((x1, x2), (y1, y2), (z1, z2));
+    # nx, ny, nz then count the computational domain's cells
+    cd: Optional[Tuple[Tuple[float, float], Tuple[float, float], Tuple[float, float]]] = None
+    use_init_values: bool = False  # Buoyancy: use_init_values="Yes" (no ambient temperature value)
+    ic_attrs: dict = field(default_factory=dict)  # attributes of <initial_conditions> (LayersT: dir)
+    # <adaption dynamic="Yes"> with a Layers class of these parameters (buffer,
+    # check_value, timestep, expansion_size); both ARTSS and this library reject it
+    adaption: Optional[dict] = None
 
     @property
     def t_end(self) -> float:
@@ -284,6 +292,62 @@ def pressure_scene(n: int = 32, n_level: int = 4, steps: int = 2, **kw) -> Scene
     return Scene(**base)
 
 
+def layered_channel(nx: int = 64, ny: int = 16, nz: int = 32, steps: int = 4, n_level: int = 4,
+                    use_init_values: bool = False, **kw) -> Scene:
+    """A computational domain inside a longer physical one: the channel runs
+    0..48 m in x, the solver works on x in 16..24 m (nx cells, so the physical
+    domain holds 6 nx cells plus ghosts); y in -2..2 m, z in -3..3 m.  The
+    temperature starts in four horizontal layers (LayersT across y), a Gauss
+    source near the floor heats it, buoyancy acts along y.  No-slip floor,
+    ceiling and side walls, open ends (Neumann velocity, p = 0)."""
+    base = dict(solver="NSTempTurbSolver", nx=nx, ny=ny, nz=nz, X=(0.0, 48.0), Y=(-2.0, 2.0), Z=(-3.0, 3.0),
+                cd=((16.0, 24.0), (-2.0, 2.0), (-3.0, 3.0)), dt=0.05, steps=steps, nu=2.5e-5, kappa=3.3e-5,
+                beta=3.28e-3, diffusion="Jacobi", diff_tol=1e-7, n_level=n_level, n_cycle=2, max_cycle=100,
+                mg_tol=1e-7, n_relax=4, smoother="Jacobi", smoother_tol=1e-7, buoyancy_dir="y",
+                use_init_values=use_init_values, t_ambient=300.0, hrr=5000.0, cp=1.0,
+                source_pos=(20.0, -2.0, 0.0), sigma=(0.75, 1.0, 0.75), tau=5.0, noise=False, ic="LayersT",
+                ic_attrs={"dir": "y"},
+                ic_params={"n_layers": 4, "border_1": -1.0, "border_2": 0.0, "border_3": 1.0,
+                           "value_1": 300.5, "value_2": 301.0, "value_3": 302.5, "value_4": 304.0},
+                boundaries=[("u,v,w", "front,back,bottom,top", "dirichlet", 0.0),
+                            ("u,v,w", "left,right", "neumann", 0.0),
+                            ("p", "front,back,bottom,top", "neumann", 0.0),
+                            ("p", "left,right", "dirichlet", 0.0),
+                            ("T", "front,back,bottom,top,left,right", "neumann", 0.0)])
+    base.update(kw)
+    return Scene(**base)
+
+
+def inset_box(n: int = 32, steps: int = 4, n_level: int = 3, **kw) -> Scene:
+    """A computational domain strictly inside the physical domain on every
+    axis (x 4..8 of 0..12, y 1..5 of 0..6, z 2..4 of 0..6 m; n x n x n/2 cells
+    of 4/n m) with a solid block inside it, colored Gauss-Seidel diffusion and
+    the plume source: every boundary condition acts on faces interior to the
+    physical arrays."""
+    h = 4.0 / n
+    block = Box(5.5, 5.5 + 8 * h, 1.0, 1.0 + 6 * h, 2.5, 2.5 + 4 * h, "block")
+    base = dict(nx=n, ny=n, nz=n // 2, X=(0.0, 12.0), Y=(0.0, 6.0), Z=(0.0, 6.0),
+                cd=((4.0, 8.0), (1.0, 5.0), (2.0, 4.0)), steps=steps, n_level=n_level, dt=0.01,
+                source_pos=(6.0, 2.0, 3.0), sigma=(0.4, 0.4, 0.4), hrr=50.0, buoyancy_dir="y",
+                boundaries=closed_box_bcs(), obstacles=[block], obstacle_bcs=solid_obstacle_bcs())
+    base.update(kw)
+    return Scene(**base)
+
+
+def burgers_scene(n: int = 32, nz: int = 1, steps: int = 4, **kw) -> Scene:
+    """AdvectionDiffusionSolver on the ExpSinusSum state (the reference's Burgers
+    test family, tests/burgers): a periodic 2 pi box, n x n x nz cells; nz = 1
+    is the 2-D form (u = -v = sin(x + y), w = 0), larger nz the 3-D one
+    (u = sin(x + y + z), v = w = -u / 2)."""
+    L = 2.0 * math.pi
+    base = dict(solver="AdvectionDiffusionSolver", nx=n, ny=n, nz=nz, X=(0.0, L), Y=(0.0, L),
+                Z=(0.0, L if nz > 1 else L / n), dt=0.01, steps=steps, nu=0.05, diffusion="Jacobi", diff_tol=1e-7,
+                diff_max_iter=100, noise=False, ic="ExpSinusSum",
+                boundaries=[("u,v,w", "front,back,left,right,bottom,top", "periodic", 0.0)])
+    base.update(kw)
+    return Scene(**base)
+
+
 NS_SOLVERS = ("NSSolver", "NSTurbSolver")
 
 
@@ -415,8 +479,10 @@ def to_xml(s: Scene) -> str:
         if turbulent:
             turbulence_block()
         if s.force == "Buoyancy":
-            a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" use_init_values="No">')
-            a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
+            a(f'    <source type="ExplicitEuler" force_fct="Buoyancy" dir="{s.buoyancy_dir}" '
+              f'use_init_values="{"Yes" if s.use_init_values else "No"}">')
+            if not s.use_init_values:
+                a(f"      <ambient_temperature_value> {_f(s.t_ambient)} </ambient_temperature_value>")
         elif s.force == "Uniform":
             a(f'    <source type="ExplicitEuler" force_fct="Uniform" dir="{s.buoyancy_dir}">')
             for ax, val in zip("xyz", s.force_value):
@@ -479,15 +545,27 @@ def to_xml(s: Scene) -> str:
     a('    <solution available="No">')
     a("    </solution>")
     a("  </solver>")
-    a('  <domain_parameters enable_computational_domain="No">')
+    a(f'  <domain_parameters enable_computational_domain="{"Yes" if s.cd else "No"}">')
     for ax, (lo, hi) in zip("XYZ", (s.X, s.Y, s.Z)):
         a(f"    <{ax}1> {_f(lo)} </{ax}1>")
         a(f"    <{ax}2> {_f(hi)} </{ax}2>")
+    if s.cd:
+        for ax, (lo, hi) in zip("xyz", s.cd):
+            a(f"    <{ax}1> {_f(lo)} </{ax}1>")
+            a(f"    <{ax}2> {_f(hi)} </{ax}2>")
     a(f"    <nx> {s.nx} </nx>")
     a(f"    <ny> {s.ny} </ny>")
     a(f"    <nz> {s.nz} </nz>")
     a("  </domain_parameters>")
-    a('  <adaption dynamic="No" data_extraction="No"> </adaption>')
+    if s.adaption:
+        a('  <adaption dynamic="Yes" data_extraction="No">')
+        a('    <class name="Layers">')
+        for k, v in s.adaption.items():
+            a(f"      <{k}> {_f(v)} </{k}>")
+        a("    </class>")
+        a("  </adaption>")
+    else:
+        a('  <adaption dynamic="No" data_extraction="No"> </adaption>')
     a('  <data_assimilation enabled="No" />')
     def with_rho(bcs):
         out = list(bcs)
@@ -512,21 +590,21 @@ def to_xml(s: Scene) -> str:
     else:
         a('  <obstacles enabled="No"/>')
     a('  <surfaces enabled="No"/>')
+    # Uniform and LayersT take the seeded noise on T (SolverController.cpp:167-180)
+    noisy = s.noise and s.ic in ("Uniform", "LayersT")
+    attrs = "".join(f' {k}="{v}"' for k, v in s.ic_attrs.items())
+    a(f'  <initial_conditions usr_fct="{s.ic}"{attrs} random="{"Yes" if noisy else "No"}">')
     if s.ic == "Uniform":
-        a(f'  <initial_conditions usr_fct="Uniform" random="{"Yes" if s.noise else "No"}">')
         a(f"    <val> {_f(s.T0)} </val>")
-        if s.noise:
-            a('    <random absolute="Yes" custom_seed="Yes" custom_steps="Yes">')
-            a(f"      <seed> {s.seed} </seed>")
-            a(f"      <step_size> {_f(s.noise_step)} </step_size>")
-            a(f"      <range> {_f(s.noise_range)} </range>")
-            a("    </random>")
-        a("  </initial_conditions>")
-    else:
-        a(f'  <initial_conditions usr_fct="{s.ic}" random="No">')
-        for k, v in s.ic_params.items():
-            a(f"    <{k}> {_f(v)} </{k}>")
-        a("  </initial_conditions>")
+    for k, v in s.ic_params.items():
+        a(f"    <{k}> {_f(v)} </{k}>")
+    if noisy:
+        a('    <random absolute="Yes" custom_seed="Yes" custom_steps="Yes">')
+        a(f"      <seed> {s.seed} </seed>")
+        a(f"      <step_size> {_f(s.noise_step)} </step_size>")
+        a(f"      <range> {_f(s.noise_range)} </range>")
+        a("    </random>")
+    a("  </initial_conditions>")
     a('  <visualisation save_vtk="No" save_csv="No">')
     a("  </visualisation>")
     a('  <logging file="artss.log" level="info">')

@@ -64,6 +64,15 @@ def _scenes():
                                                         turbulence="DynamicSmagorinsky"),
         # PressureSolver (src/solver/PressureSolver.cpp:30-43) on the SinSinSin right-hand side
         "pressure_sinsinsin": scenes.pressure_scene(n=32, n_level=4, steps=2),
+        # a computational domain inside the physical one (DomainData x1..z2), the LayersT
+        # initial state (Functions::layers) with and without noise, buoyancy with
+        # use_init_values (T_ambient never set: zero, as in the reference)
+        "cd_layered_channel": scenes.layered_channel(steps=4),
+        "cd_layered_channel_init_values": scenes.layered_channel(steps=3, use_init_values=True, noise=True),
+        "cd_inset_box_obstacle": scenes.inset_box(steps=4),
+        # AdvectionDiffusionSolver on ExpSinusSum (Functions::exp_sinus_sum), 2-D and 3-D
+        "burgers_2d": scenes.burgers_scene(n=32, nz=1, steps=4),
+        "burgers_3d": scenes.burgers_scene(n=32, nz=16, steps=4),
     }
 
 
