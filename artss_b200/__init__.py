@@ -83,6 +83,7 @@ class SolveStats(C.Structure):
 MIXED_REMOVE_MEAN = 1
 MIXED_RBGS = 2
 MIXED_BC_LAUNCH = 4
+MIXED_CLUSTER_COARSE = 8
 
 
 class ConvDesc(C.Structure):

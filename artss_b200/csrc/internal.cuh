@@ -437,11 +437,13 @@ int apply_bc(artss_ctx *ctx, double *f, int level, int field_type, const LoopSta
 
 // Homogeneous boundary program (values zero) on FP32 storage (bc.cu).
 int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const LoopState *pred = nullptr);
-// FP64 cluster solve of a level's pressure equation on FP32 storage, zero
-// boundary values, tolerance relative to the initial residual (mg.cu).
+// FP64 cluster (block: one-block where the level fits) solve of a level's
+// pressure equation on FP32 storage, zero boundary values, tolerance relative
+// to the initial residual (mg.cu).
 bool cluster_fits(const artss_ctx *ctx, int level, int buffers, int *plane_cap, int64_t *smem);
+bool block_fits(const artss_ctx *ctx, int level, int buffers, int64_t *smem);
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
-                       long long max_it, const LoopState *pred);
+                       long long max_it, const LoopState *pred, bool block);
 
 // TMA descriptor of a level array for kTmaBoxX x kTmaBoxY plane windows (tma.cu);
 // tma_level_ok: the level's row pitch allows TMA (Nx even).

@@ -620,6 +620,219 @@ k_mg_coarse_cluster(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__rest
     cl.sync();
 }
 
+// ---------------------------------------------------------------- one-block coarse solve
+//
+// The loop of k_mg_coarse_cluster on ONE block for a level that fits its
+// shared memory (a few thousand inner cells, the coarsest grid of a deep
+// V-cycle): the whole level array (and tmp's for Jacobi) lives in shared
+// memory, each thread keeps its cells' offsets and right-hand side and its
+// boundary assignments (target, root, chain) in registers, and the barriers
+// are block barriers.  Cell slots 0 .. kBlkCells/2 - 1 of a thread hold cells
+// of colour 0, the others colour 1, numbered so that the 32 lanes of a warp
+// hold cells of one colour: a colour pass runs without divergence.  The
+// residual's warp sums are added by every warp in the same butterfly order,
+// and the loop test compares the squared sum with tol^2 outside a guard band
+// (the square root only inside it).  Same iterates as the cluster kernel; only
+// the order of the residual sums differs.  The set-up that reads no result of
+// the previous kernel (cell slots, boundary slots) runs before the
+// programmatic-launch wait.
+
+constexpr int kBlkThreads = 1024;
+constexpr int kBlkCells = 4;     // cell slots per thread, half per colour: at most 2048 cells per colour
+constexpr int kBlkTargets = 4;   // boundary assignments per thread, all waves together
+
+// box cells of colour col ((i + j + k) % 2) in slot order: slot s = (k, j, t)
+// row-major over ceil(nx / 2) pairs per row, x = x0 + 2 t + the row's offset
+__host__ __device__ inline int64_t blk_slots(const Box3 &box) {
+    return ((box.nx() + 1) / 2) * box.ny() * box.nz();
+}
+
+template <bool CGS, typename TS>
+__global__ void __launch_bounds__(kBlkThreads, 1)
+k_mg_coarse_block(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restrict__ b,
+                  const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
+                  const __grid_constant__ BcView bc, double tol, int rel, long long max_it, LoopState *__restrict__ st,
+                  const LoopState *__restrict__ pred) {
+    extern __shared__ double sm[];
+    __shared__ double red[kBlkThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int nj = (int) L.Nx, nk = (int) (L.Nx * L.Ny), ntot = (int) (L.Nx * L.Ny * L.Nz);
+    constexpr int H = kBlkCells / 2;
+    // this thread's cells (static: the level's flags): offsets and colour masks
+    int co[kBlkCells];
+    unsigned m0 = 0, m1 = 0;
+    {
+        const int np = (int) ((box.nx() + 1) / 2), nrow = np * (int) box.ny(), nslot = nrow * (int) box.nz();
+#pragma unroll
+        for (int m = 0; m < kBlkCells; m++) {
+            const int col = m < H ? 0 : 1;
+            const int s = tid + (m % H) * kBlkThreads;
+            co[m] = 0;
+            if (s < nslot) {
+                const int k = (int) box.z0 + s / nrow, r = s % nrow, j = (int) box.y0 + r / np;
+                const int x0 = (int) box.x0;
+                const int i = x0 + 2 * (r % np) + ((x0 + j + k + col) & 1);
+                if (i <= (int) box.x1) {
+                    const int q = i + nj * j + nk * k;
+                    if (__ldg(flags + q) & kInner) {
+                        co[m] = q;
+                        if (!CGS || col == 0) m0 |= 1u << m;
+                        else m1 |= 1u << m;
+                    }
+                }
+            }
+        }
+    }
+    // this thread's boundary assignments, in wave order: slot u is its u-th
+    // assignment begin[w] + tid + v * threads over the waves w (a slot index known
+    // at compile time, so the slots stay in registers); bdn = depth | neg << 8 |
+    // (wave + 1) << 16, 0 for an empty slot
+    int bt[kBlkTargets], br[kBlkTargets], bq[kBlkTargets];
+    uint32_t bdn[kBlkTargets];
+    {
+        // slot -> assignment first (no loads), then all slots' loads at once
+        int wv[kBlkTargets];
+#pragma unroll
+        for (int u = 0; u < kBlkTargets; u++) {
+            bq[u] = -1;
+            wv[u] = 0;
+            int before = 0;
+            for (int w = 0; w < bc.waves; w++) {
+                const int64_t n_w = bc.begin[w + 1] - bc.begin[w] - tid;
+                const int cnt = n_w > 0 ? (int) ((n_w + kBlkThreads - 1) / kBlkThreads) : 0;
+                if (bq[u] < 0 && u < before + cnt) {
+                    bq[u] = (int) (bc.begin[w] + tid + (int64_t) (u - before) * kBlkThreads);
+                    wv[u] = w + 1;
+                }
+                before += cnt;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBlkTargets; u++) {
+            bt[u] = br[u] = 0;
+            bdn[u] = 0;
+            if (bq[u] >= 0) {
+                bt[u] = (int) __ldg(bc.target + bq[u]);
+                br[u] = (int) __ldg(bc.root + bq[u]);
+                bdn[u] = (uint32_t) __ldg(bc.depth + bq[u]) | (uint32_t) __ldg(bc.neg + bq[u]) << 8 |
+                         (uint32_t) wv[u] << 16;
+            }
+        }
+    }
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes (b, out, pred) are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;
+    double cb[kBlkCells];
+#pragma unroll
+    for (int m = 0; m < kBlkCells; m++) cb[m] = ((m0 | m1) >> m & 1) ? (double) b[co[m]] : 0.0;
+    for (int q = tid; q < ntot; q += kBlkThreads) sm[q] = (double) out[q];
+#define BLK_APPLY_BC(base)                                                                                     \
+    for (int w = 0; w < bc.waves; w++) {                                                                       \
+        _Pragma("unroll") for (int u = 0; u < kBlkTargets; u++) {                                              \
+            if ((int) (bdn[u] >> 16) != w + 1) continue;                                                       \
+            double x = sm[(base) + br[u]];                                                                     \
+            const int d = (int) (bdn[u] & 0xffu);                                                              \
+            const uint32_t mneg = (bdn[u] >> 8) & 0xffu;                                                       \
+            _Pragma("unroll") for (int e = 0; e < kBcMaxDepth; e++) if (e < d) x =                             \
+                ((mneg >> e) & 1 ? -x : x) + (bc.value ? __ldg(bc.value + e * bc.n + bq[u]) : 0.0);            \
+            sm[(base) + bt[u]] = x;                                                                            \
+        }                                                                                                      \
+        __syncthreads();                                                                                       \
+    }
+    // sum of ||b - A x||^2 over the inner cells (x at sm[base ..]), the same in
+    // every thread
+    auto ressum = [&](int base) {
+        double acc = 0.0;
+#pragma unroll
+        for (int m = 0; m < kBlkCells; m++) {
+            if (!((m0 | m1) >> m & 1)) continue;
+            const int o = base + co[m];
+            const double c0 = sm[o];
+            const double rr = cb[m] - (rx * (sm[o - 1] - 2 * c0 + sm[o + 1]) + ry * (sm[o - nj] - 2 * c0 + sm[o + nj]) +
+                                       rz * (sm[o - nk] - 2 * c0 + sm[o + nk]));
+            acc += rr * rr;
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        double v = red[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    };
+    __syncthreads();
+    BLK_APPLY_BC(0);
+    if (!CGS) {
+        for (int q = tid; q < ntot; q += kBlkThreads) sm[ntot + q] = sm[q];
+        __syncthreads();
+    }
+    int A = 0, B = ntot;  // offsets of the two arrays (Field::swap of the reference)
+    double res = 10000.;
+    long long it = 0;
+    if (rel) {
+        tol *= sqrt(ressum(A));
+        __syncthreads();  // red is rewritten by the next reduction
+    }
+    // res > tol decided on the squared sum s where that is exact: outside +-16
+    // units of roundoff around tol^2 sqrt(s) lies on the same side of tol
+    const double tol2 = tol * tol;
+    const bool fast = tol2 > 1e-280 && tol2 < 1e280;
+    bool above = res > tol;
+    double s_last = -1.0;
+    while (above && it < max_it) {
+        if (CGS) {
+#pragma unroll
+            for (int color = 0; color < 2; color++) {
+#pragma unroll
+                for (int m = color * H; m < (color + 1) * H; m++) {
+                    if (!((color ? m1 : m0) >> m & 1)) continue;
+                    const int o = co[m];
+                    const double out_h = c.beta * (c.dsign * cb[m] + c.ax * (sm[o + 1] + sm[o - 1]) +
+                                                   c.ay * (sm[o + nj] + sm[o - nj]) + c.az * (sm[o + nk] + sm[o - nk]));
+                    sm[o] = c.omw * sm[o] + c.w * out_h;
+                }
+                __syncthreads();
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < kBlkCells; m++) {
+                if (!(m0 >> m & 1)) continue;
+                const int o = co[m];
+                const double out_h = c.beta * (c.dsign * cb[m] + c.ax * (sm[B + o + 1] + sm[B + o - 1]) +
+                                               c.ay * (sm[B + o + nj] + sm[B + o - nj]) +
+                                               c.az * (sm[B + o + nk] + sm[B + o - nk]));
+                sm[A + o] = c.omw * sm[B + o] + c.w * out_h;
+            }
+            __syncthreads();
+        }
+        BLK_APPLY_BC(A);
+        const double s = ressum(A);
+        s_last = s;
+        if (fast && s > tol2 * (1.0 + 0x1p-49)) above = true;
+        else if (fast && s < tol2 * (1.0 - 0x1p-49)) above = false;
+        else above = sqrt(s) > tol;
+        if (!CGS) {
+            const int t = A;
+            A = B;
+            B = t;
+        }
+        it++;
+    }
+#undef BLK_APPLY_BC
+    if (s_last >= 0) res = sqrt(s_last);
+    __syncthreads();
+    // sm[0 ..) is out's storage and sm[ntot ..) tmp's, whatever the swaps did
+    for (int q = tid; q < ntot; q += kBlkThreads) {
+        out[q] = (TS) sm[q];
+        if (!CGS && tmp) tmp[q] = (TS) sm[ntot + q];
+    }
+    if (tid == 0 && st) {
+        st->it = it;
+        st->residual = res;
+        st->cond = 0;
+    }
+}
+
 // ---------------------------------------------------------------- pipelined Jacobi coarse solve
 //
 // VCycleMG::call_solve_jacobi (src/pressure/VCycleMG.cpp:727-800) on the
@@ -1224,18 +1437,58 @@ BcView bc_view(const artss_ctx *ctx, int level) {
     return v;
 }
 
+// true when the level fits k_mg_coarse_block: its inner box in the threads'
+// cell slots, its array (and tmp's) in shared memory, its boundary program in
+// the threads' assignment slots
+bool block_fits(const artss_ctx *ctx, int level, int buffers, int64_t *smem) {
+    const Level &L = ctx->lvl[level];
+    const BcProgram &p = ctx->bc[level][ARTSS_FIELD_P];
+    if (p.present && p.waves > kCoarseMaxWaves) return false;
+    const Box3 box = inner_box(L);
+    if (blk_slots(box) > (int64_t) kBlkThreads * (kBlkCells / 2)) return false;
+    const int64_t bytes = buffers * L.size() * (int64_t) sizeof(double);
+    if (bytes > kCoarseSmemBytes) return false;
+    if (p.present && p.n > 0) {
+        int64_t per_thread = 0;
+        for (int w = 0; w < p.waves; w++)
+            per_thread += (p.wave_begin[w + 1] - p.wave_begin[w] + kBlkThreads - 1) / kBlkThreads;
+        if (per_thread > kBlkTargets) return false;
+    }
+    *smem = bytes;
+    return true;
+}
+
+template <bool CGS, typename TS>
+int launch_coarse_block(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level, const MgCoef &c, double rx,
+                        double ry, double rz, const BcView &v, double tol, int rel, long long mi, int64_t smem,
+                        LoopState *st, const LoopState *pred) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_block<CGS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) kCoarseSmemBytes));
+        attr_set = true;
+    }
+    const Level &L = ctx->lvl[level];
+    ARTSS_LAUNCH_PDL(ctx, FAM_MG_COARSE, (k_mg_coarse_block<CGS, TS>), 1, kBlkThreads, smem, out, tmp, b,
+                     (const uint8_t *) ctx->d_flags[level], L, inner_box(L), c, rx, ry, rz, v, tol, rel, mi, st, pred);
+    ARTSS_LAUNCH_CK(ctx);
+    return ARTSS_OK;
+}
+
 // FP64 solve of one level's pressure system by the cluster kernel on FP32
 // storage (the coarsest-grid solve of the mixed-precision V-cycle); the
 // level's boundary values are taken as zero, tol is relative to the initial
-// residual.
+// residual.  block: by k_mg_coarse_block where the level fits one block.
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
-                       long long max_it, const LoopState *pred) {
+                       long long max_it, const LoopState *pred, bool block) {
     const bool cgs = smoother == ARTSS_SMOOTHER_CGS;
     int cap = 0;
     int64_t smem = 0;
     PipeLaunch pl{};
     const bool pipe = !cgs && coarse_pipe_plan(ctx, level, &pl);
-    if (!pipe && !cluster_fits(ctx, level, cgs ? 1 : 2, &cap, &smem)) {
+    int64_t bs = 0;
+    if (!pipe && !cluster_fits(ctx, level, cgs ? 1 : 2, &cap, &smem) &&
+        !(block && block_fits(ctx, level, cgs ? 1 : 2, &bs))) {
         set_error("the coarsest level does not fit the cluster coarse solve");
         return ARTSS_ERR_LIMIT;
     }
@@ -1250,6 +1503,14 @@ int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, in
     c.omw = 1 - w;
     BcView v = bc_view(ctx, level);
     v.value = nullptr;  // homogeneous: the correction equation has zero boundary values
+    int64_t bsmem = 0;
+    if (block && block_fits(ctx, level, cgs ? 1 : 2, &bsmem)) {
+        if (cgs)
+            return launch_coarse_block<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
+                                                    bsmem, nullptr, pred);
+        return launch_coarse_block<false, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
+                                                 bsmem, nullptr, pred);
+    }
     if (cgs)
         return launch_coarse_cluster<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
                                                   cap, smem, nullptr, pred);

@@ -525,7 +525,7 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
             w = m->cfg.coarse_smoother == ARTSS_SMOOTHER_CGS ? 2. / (1. + sin(M_PI / (n + 1.))) : 0.6666666667;
         }
         if ((st = coarse_cluster_f32(ctx, m->e[Lc], m->r[Lc], Lc, m->cfg.coarse_smoother, w, m->cfg.coarse_rel_tol,
-                                     m->cfg.coarse_max_iter, pred)))
+                                     m->cfg.coarse_max_iter, pred, !(m->cfg.flags & ARTSS_MIXED_CLUSTER_COARSE))))
             return st;
     }
     for (int l = Lc - 1; l >= 0; l--) {
@@ -603,7 +603,9 @@ int artss_mixed_create(artss_ctx *ctx, const artss_mixed_cfg *cfg, artss_mixed *
     if (!st) {
         int cap = 0;
         int64_t smem = 0;
-        if (!cluster_fits(ctx, m->L - 1, cfg->coarse_smoother == ARTSS_SMOOTHER_CGS ? 1 : 2, &cap, &smem)) {
+        const int buffers = cfg->coarse_smoother == ARTSS_SMOOTHER_CGS ? 1 : 2;
+        if (!cluster_fits(ctx, m->L - 1, buffers, &cap, &smem) &&
+            ((cfg->flags & ARTSS_MIXED_CLUSTER_COARSE) || !block_fits(ctx, m->L - 1, buffers, &smem))) {
             set_error("the coarsest level is too large for the cluster coarse solve; use more levels");
             st = ARTSS_ERR_LIMIT;
         }

@@ -443,11 +443,15 @@ int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_to
  * (and without ARTSS_MIXED_RBGS) their stencils read boundary neighbours
  * through the program instead (same values, fewer launches) */
 #define ARTSS_MIXED_BC_LAUNCH 4
+/* solve the coarsest level on a thread-block cluster even where it fits one
+ * block (shared memory, register-resident cells and boundary assignments,
+ * block barriers only); same iterates, up to the order of the residual sums */
+#define ARTSS_MIXED_CLUSTER_COARSE 8
 typedef struct {
     int32_t n_level;          /* V-cycle levels 0 .. n_level-1; the coarse solve is on n_level-1 */
     int32_t n_relax;          /* weighted-Jacobi sweeps before and after each coarse correction */
-    int32_t coarse_smoother;  /* ARTSS_SMOOTHER_JACOBI or ARTSS_SMOOTHER_CGS (FP64, one cluster kernel) */
-    int32_t flags;            /* ARTSS_MIXED_REMOVE_MEAN */
+    int32_t coarse_smoother;  /* ARTSS_SMOOTHER_JACOBI or ARTSS_SMOOTHER_CGS (FP64, one kernel) */
+    int32_t flags;            /* ARTSS_MIXED_* */
     double w;                 /* Jacobi weight of the FP32 sweeps */
     double coarse_w;          /* relaxation weight of the coarse solve; <= 0: red-black SOR with the
                                * model problem's optimal weight 2 / (1 + sin(pi / (n + 1))) for CGS,

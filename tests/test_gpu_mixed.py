@@ -142,3 +142,21 @@ def test_mixed_boundary_writes_match_launched_programs(case):
     launched = solve_pair(sc, seed, flags | A.MIXED_BC_LAUNCH)
     assert folded[7].cycles == launched[7].cycles
     assert np.array_equal(folded[4], launched[4])
+
+
+@pytest.mark.parametrize("case", ["neumann_boxes", "dirichlet_channel"])
+def test_mixed_block_coarse_matches_cluster(case):
+    """The coarsest level solved by one block (shared memory, block barriers;
+    the default where the level fits) and by the thread-block cluster
+    (MIXED_CLUSTER_COARSE) compute the same iterates; only the order of the
+    residual sums that stop the coarse loop differs."""
+    if case == "neumann_boxes":
+        sc, seed, flags = scenes.poisson_boxes(n=32, seed=8, n_level=3), 8, A.MIXED_REMOVE_MEAN
+    else:
+        sc, seed, flags = scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=1, n_level=3), 7, 0
+    block = solve_pair(sc, seed, flags)
+    cluster = solve_pair(sc, seed, flags | A.MIXED_CLUSTER_COARSE)
+    inner = block[3]
+    assert block[7].cycles == cluster[7].cycles and block[7].rel_residual <= 1e-8
+    p_b, p_c = block[4][inner], cluster[4][inner]
+    assert np.abs(p_b - p_c).max() <= 1e-9 * np.abs(p_c).max()
