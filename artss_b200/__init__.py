@@ -84,6 +84,7 @@ MIXED_REMOVE_MEAN = 1
 MIXED_RBGS = 2
 MIXED_BC_LAUNCH = 4
 MIXED_CLUSTER_COARSE = 8
+MIXED_FINE_PROLONG = 16
 
 
 class ConvDesc(C.Structure):

@@ -365,7 +365,8 @@ inline dim3 col_grid(const Box3 &b, const ColShape &s) {
 // Kernel ids of the launch-shape tuner (TuneKey::kernel; 0 is the sweep variant)
 enum ColKernel : int {
     kTuneAdvect1 = 101, kTuneAdvect3, kTuneSmagorinsky, kTuneDivergence, kTuneProjection, kTuneBuoyancy,
-    kTuneMgJacobi, kTuneMgResiduum, kTuneMgRestrict, kTuneMgProlongate
+    kTuneMgJacobi, kTuneMgResiduum, kTuneMgRestrict, kTuneMgProlongate,
+    kTuneMxJacobi0, kTuneMxJacobi, kTuneMxResiduum, kTuneMxRestrict
 };
 
 // Launches a column kernel, `launch(grid, block)` returning a status, with the
@@ -375,9 +376,11 @@ enum ColKernel : int {
 // same arguments (its output is not its input) and must not reduce (a
 // reduction's order would follow the choice; a call whose output aliases an
 // input passes may_tune = false).  Inside a capture, with the autotuner off or
-// without may_tune, an untuned key launches shape 0.
+// without may_tune, an untuned key launches shape 0.  max_threads: the
+// kernel's __launch_bounds__ (shapes with larger blocks are not tried).
 template <class F>
-int tuned_column_launch(artss_ctx *ctx, int kernel, int level, const Box3 &box, bool may_tune, F launch) {
+int tuned_column_launch(artss_ctx *ctx, int kernel, int level, const Box3 &box, bool may_tune, F launch,
+                        unsigned max_threads = 1024) {
     const Level &L = ctx->lvl[level];
     const TuneKey key{kernel, L.Nx, L.Ny, L.Nz, level};
     auto it = ctx->tuned.find(key);
@@ -397,6 +400,7 @@ int tuned_column_launch(artss_ctx *ctx, int kernel, int level, const Box3 &box, 
     float best_ms = 1e30f;
     for (int v = 0; v < kColShapeCount && !st; v++) {
         const ColShape &s = kColShapes[v];
+        if (s.bx * s.by > max_threads) continue;
         const dim3 g = col_grid(box, s), b(s.bx, s.by, 1);
         if ((st = launch(g, b))) break;
         cudaEventRecord(e0, ctx->stream);

@@ -94,9 +94,13 @@ __device__ __forceinline__ void mx_store(float *__restrict__ out, uint8_t mask, 
     }
 }
 
+// CORRECT (the last sweep of level 0 in a V-cycle): instead of storing the
+// sweep's value v, add it to the FP64 iterate, p[x] += (double) v, which is
+// k_mx_correct's update of the same value (out and push unused)
+template <bool CORRECT>
 __global__ void __launch_bounds__(256, 8) k_mx_jacobi(float *__restrict__ out, const float *__restrict__ in, const float *__restrict__ b,
                             const uint8_t *__restrict__ nbm, const uint16_t *__restrict__ push, Level L, Box3 box,
-                            CoefF c, const LoopState *__restrict__ pred) {
+                            CoefF c, const LoopState *__restrict__ pred, double *__restrict__ p) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     if (pred && !pred->cond) return;
@@ -109,7 +113,10 @@ __global__ void __launch_bounds__(256, 8) k_mx_jacobi(float *__restrict__ out, c
                                       c.az * (kp + km));
             return c.omw * c0 + c.w * h;
         },
-        [&](int x, int, float v, uint8_t fl) { mx_store(out, fl, push, x, v, nj, nk); });
+        [&](int x, int, float v, uint8_t fl) {
+            if (CORRECT) p[x] = p[x] + (double) v;
+            else mx_store(out, fl, push, x, v, nj, nk);
+        });
 }
 
 // one colour of an in-place red-black Gauss-Seidel sweep of the same operator,
@@ -221,6 +228,82 @@ __global__ void k_mx_prolong_add(float *__restrict__ fine, const float *__restri
         [&](int f, int, Out o, uint8_t fl) {
             if (o.cf & kInner) mx_store(fine, fl, push, f, o.v, fx, fxy);
         });
+}
+
+// The same prolongation, one thread per coarse column: the thread marches up
+// its contiguous run of coarse planes keeping the 3 x 3 x 3 coarse
+// neighbourhood in registers (one new 3 x 3 plane per step) and updates the 8
+// fine children of each coarse inner cell, each with k_mx_prolong_add's
+// expression, so every fine value is the same bit for bit.  The fine x pairs
+// of a warp's 32 coarse columns are 64 consecutive cells.
+__global__ void __launch_bounds__(256) k_mx_prolong_add8(float *__restrict__ fine, const float *__restrict__ in,
+                                                         const uint8_t *__restrict__ cflags,
+                                                         const uint8_t *__restrict__ fflags,
+                                                         const uint16_t *__restrict__ push, Level C, Level F,
+                                                         Box3 cbox, Box3 fbox, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;
+    MX_COLUMN(cbox);  // (i, j): the coarse column
+    if (!col) return;
+    const int nj = (int) C.Nx, nk = (int) C.nxy();
+    const int fx = (int) F.Nx, fxy = (int) F.nxy();
+    const int nzc = (int) cbox.nz();
+    const int chunk = (nzc + (int) gridDim.z - 1) / (int) gridDim.z;
+    const int k0 = (int) cbox.z0 + (int) blockIdx.z * chunk;
+    const int k1 = min((int) cbox.z1, k0 + chunk - 1);
+    if (k0 > k1) return;
+    // w[p][b][a]: coarse value at (i + a - 1, j + b - 1, k + p - 1) for the current plane k
+    float w[3][3][3];
+    auto load_plane = [&](int k, float (&pl)[3][3]) {
+        const int x = i + nj * j + nk * k;
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int a = 0; a < 3; a++) pl[b][a] = in[x + (a - 1) + nj * (b - 1)];
+    };
+    load_plane(k0 - 1, w[0]);
+    load_plane(k0, w[1]);
+    // fine children of this column that lie in the fine box
+    const int fi0 = 2 * i - 1, fj0 = 2 * j - 1;
+    const bool xa = fi0 >= (int) fbox.x0 && fi0 <= (int) fbox.x1, xb = fi0 + 1 >= (int) fbox.x0 && fi0 + 1 <= (int) fbox.x1;
+    const bool ya = fj0 >= (int) fbox.y0 && fj0 <= (int) fbox.y1, yb = fj0 + 1 >= (int) fbox.y0 && fj0 + 1 <= (int) fbox.y1;
+    for (int k = k0; k <= k1; k++) {
+        // every load of the step first (the children lie in the fine array: 2 c <=
+        // the fine inner box's end + 1), then the arithmetic and the stores
+        const bool cin = (cflags[i + nj * j + nk * k] & kInner) != 0;
+        uint8_t fl[8];
+        float fv[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int f = fi0 + (c & 1) + fx * (fj0 + ((c >> 1) & 1)) + fxy * (2 * k - 1 + (c >> 2));
+            fl[c] = fflags[f];
+            fv[c] = fine[f];
+        }
+        load_plane(k + 1, w[2]);
+        if (cin) {
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                const int fk = 2 * k - 1 + dz;
+                if (fk < (int) fbox.z0 || fk > (int) fbox.z1 || !(dy ? yb : ya) || !(dx ? xb : xa) || !(fl[c] & kInner))
+                    continue;
+                const int px = dx ? 2 : 0, py = dy ? 2 : 0, pz = dz ? 2 : 0;  // s = +1 for the even child
+                const int f = fi0 + dx + fx * (fj0 + dy) + fxy * fk;
+                const float v = 0.015625f * (27.f * w[1][1][1] + 9.f * w[1][1][px] + 9.f * w[1][py][1] +
+                                             9.f * w[pz][1][1] + 3.f * w[1][py][px] + 3.f * w[pz][1][px] +
+                                             3.f * w[pz][py][1] + w[pz][py][px]);
+                mx_store(fine, fl[c], push, f, fv[c] + v, fx, fxy);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                w[0][b][a] = w[1][b][a];
+                w[1][b][a] = w[2][b][a];
+            }
+    }
 }
 
 // FP64 outer residual r = b - A p on level 0, stored as the FP32 right-hand
@@ -361,6 +444,27 @@ int mx_smooth_rbgs(artss_mixed *m, int l, bool from_zero, const LoopState *pred)
     return ARTSS_OK;
 }
 
+// one weighted-Jacobi sweep m->t[l] <- m->e[l] (p: added to p instead, see
+// k_mx_jacobi), in the launch shape tuned for the level (the p form repeats
+// no launch, so it takes the shape the plain form was tuned to)
+int mx_jacobi(artss_mixed *m, int l, const CoefF &c, const LoopState *pred, double *p) {
+    artss_ctx *ctx = m->ctx;
+    const Level &L = ctx->lvl[l];
+    const Box3 box = inner_box(L);
+    return tuned_column_launch(ctx, kTuneMxJacobi, l, box, p == nullptr, [&](dim3 g, dim3 bl) -> int {
+        if (p)
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi<true>, g, bl, 0, m->t[l], (const float *) m->e[l],
+                             (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], L,
+                             box, c, pred, p);
+        else
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi<false>, g, bl, 0, m->t[l], (const float *) m->e[l],
+                             (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], L,
+                             box, c, pred, (double *) nullptr);
+        ARTSS_LAUNCH_CK(ctx);
+        return ARTSS_OK;
+    }, 256);
+}
+
 // n_relax weighted-Jacobi sweeps from e = 0 on level l, each followed by the
 // boundary program; the result is left in m->e[l]
 int mx_smooth_from_zero(artss_mixed *m, int l, const LoopState *pred) {
@@ -370,23 +474,27 @@ int mx_smooth_from_zero(artss_mixed *m, int l, const LoopState *pred) {
     const Box3 box = inner_box(L);
     const CoefF c = coef_f(ctx, l, m->cfg.w);
     int st;
-    ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi0, mx_grid(box), box_block(), 0,
-                     m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], L, box, c, pred);
-    ARTSS_LAUNCH_CK(ctx);
+    if ((st = tuned_column_launch(ctx, kTuneMxJacobi0, l, box, true, [&](dim3 g, dim3 bl) -> int {
+             ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi0, g, bl, 0, m->e[l], (const float *) m->r[l],
+                              (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], L, box, c, pred);
+             ARTSS_LAUNCH_CK(ctx);
+             return ARTSS_OK;
+         })))
+        return st;
     if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
     for (int s = 1; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, m->t[l],
-                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l],
-                         L, box, c, pred);
-        ARTSS_LAUNCH_CK(ctx);
+        if ((st = mx_jacobi(m, l, c, pred, nullptr))) return st;
         std::swap(m->e[l], m->t[l]);
         if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
     }
     return ARTSS_OK;
 }
 
-// n_relax weighted-Jacobi sweeps continuing from m->e[l]
-int mx_smooth(artss_mixed *m, int l, const LoopState *pred) {
+// n_relax weighted-Jacobi sweeps continuing from m->e[l]; p: the last sweep
+// adds its values to p (FP64) instead of storing them (the correction p += e
+// of the outer loop, whose e is not read again); *corrected tells whether it did
+int mx_smooth(artss_mixed *m, int l, const LoopState *pred, double *p = nullptr, bool *corrected = nullptr) {
+    if (corrected) *corrected = false;
     if (m->cfg.flags & ARTSS_MIXED_RBGS) return mx_smooth_rbgs(m, l, false, pred);
     artss_ctx *ctx = m->ctx;
     const Level &L = ctx->lvl[l];
@@ -394,10 +502,12 @@ int mx_smooth(artss_mixed *m, int l, const LoopState *pred) {
     const CoefF c = coef_f(ctx, l, m->cfg.w);
     int st;
     for (int s = 0; s < m->cfg.n_relax; s++) {
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mx_jacobi, mx_grid(box), box_block(), 0, m->t[l],
-                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l],
-                         L, box, c, pred);
-        ARTSS_LAUNCH_CK(ctx);
+        if (p && s + 1 == m->cfg.n_relax) {
+            if ((st = mx_jacobi(m, l, c, pred, p))) return st;
+            if (corrected) *corrected = true;
+            break;
+        }
+        if ((st = mx_jacobi(m, l, c, pred, nullptr))) return st;
         std::swap(m->e[l], m->t[l]);
         if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
     }
@@ -490,8 +600,9 @@ int mx_build_tables(artss_mixed *m) {
     return ARTSS_OK;
 }
 
-// FP32 V-cycle on A e = r[0] with e = 0 at start; result in m->e[0]
-int mx_vcycle(artss_mixed *m, const LoopState *pred) {
+// FP32 V-cycle on A e = r[0] with e = 0 at start; result in m->e[0], or, with p,
+// added to p by the last smoothing sweep where *corrected says so
+int mx_vcycle(artss_mixed *m, const LoopState *pred, double *p = nullptr, bool *corrected = nullptr) {
     artss_ctx *ctx = m->ctx;
     const int Lc = m->L - 1;  // coarsest level
     const artss_grid_desc &g = ctx->grid;
@@ -500,17 +611,25 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
         if ((st = mx_smooth_from_zero(m, l, pred))) return st;
         const Level &L = ctx->lvl[l];
         const Box3 box = inner_box(L);
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_residuum, mx_grid(box), box_block(), 0, m->q[l],
-                         (const float *) m->e[l], (const float *) m->r[l], (const uint8_t *) m->nbm[l], L, box,
-                         (float) (1. / (g.dx[l] * g.dx[l])),
-                         (float) (1. / (g.dy[l] * g.dy[l])), (float) (1. / (g.dz[l] * g.dz[l])), pred);
-        ARTSS_LAUNCH_CK(ctx);
+        if ((st = tuned_column_launch(ctx, kTuneMxResiduum, l, box, true, [&](dim3 gr, dim3 bl) -> int {
+                 ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESIDUUM, k_mx_residuum, gr, bl, 0, m->q[l], (const float *) m->e[l],
+                                  (const float *) m->r[l], (const uint8_t *) m->nbm[l], L, box,
+                                  (float) (1. / (g.dx[l] * g.dx[l])), (float) (1. / (g.dy[l] * g.dy[l])),
+                                  (float) (1. / (g.dz[l] * g.dz[l])), pred);
+                 ARTSS_LAUNCH_CK(ctx);
+                 return ARTSS_OK;
+             })))
+            return st;
         if ((st = mx_bc(m, m->q[l], l, pred))) return st;
         const Level &C = ctx->lvl[l + 1];
         const Box3 cbox = inner_box(C);
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mx_restrict, mx_grid(cbox), box_block(), 0, 
-                                               m->r[l + 1], m->q[l], ctx->d_flags[l + 1], C, L, cbox, pred);
-        ARTSS_LAUNCH_CK(ctx);
+        if ((st = tuned_column_launch(ctx, kTuneMxRestrict, l + 1, cbox, true, [&](dim3 gr, dim3 bl) -> int {
+                 ARTSS_LAUNCH_PDL(ctx, FAM_MG_RESTRICT, k_mx_restrict, gr, bl, 0, m->r[l + 1], m->q[l],
+                                  ctx->d_flags[l + 1], C, L, cbox, pred);
+                 ARTSS_LAUNCH_CK(ctx);
+                 return ARTSS_OK;
+             })))
+            return st;
     }
     // coarsest level: FP64 solve from zero
     {
@@ -536,12 +655,19 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred) {
         // the fine children 2c - 1, 2c of the coarse inner box, within the fine inner box
         const Box3 fbox{std::max(F.i1, 2 * C.i1 - 1), std::min(F.i2, 2 * C.i2), std::max(F.j1, 2 * C.j1 - 1),
                         std::min(F.j2, 2 * C.j2), std::max(F.k1, 2 * C.k1 - 1), std::min(F.k2, 2 * C.k2)};
-        ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add, mx_grid(fbox), box_block(), 0,
-                         m->e[l], (const float *) m->e[l + 1], (const uint8_t *) ctx->d_flags[l + 1],
-                         (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], C, F, fbox, pred);
+        const Box3 cbox = inner_box(C);
+        if (m->cfg.flags & ARTSS_MIXED_FINE_PROLONG) {
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add, mx_grid(fbox), box_block(), 0,
+                             m->e[l], (const float *) m->e[l + 1], (const uint8_t *) ctx->d_flags[l + 1],
+                             (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], C, F, fbox, pred);
+        } else {
+            ARTSS_LAUNCH_PDL(ctx, FAM_MG_PROLONGATE, k_mx_prolong_add8, mx_grid(cbox), box_block(), 0,
+                             m->e[l], (const float *) m->e[l + 1], (const uint8_t *) ctx->d_flags[l + 1],
+                             (const uint8_t *) m->nbm[l], (const uint16_t *) m->push[l], C, F, cbox, fbox, pred);
+        }
         ARTSS_LAUNCH_CK(ctx);
         if ((st = mx_bc_sweep(m, m->e[l], l, pred))) return st;
-        if ((st = mx_smooth(m, l, pred))) return st;
+        if ((st = mx_smooth(m, l, pred, l == 0 ? p : nullptr, l == 0 ? corrected : nullptr))) return st;
     }
     return ARTSS_OK;
 }
@@ -703,10 +829,13 @@ int artss_mixed_solve(artss_mixed *m, double *p, const double *b, artss_solve_st
             if (ctx->capturing) st = finalize_loop_rel(ctx, kSlotOuter, nb, m->cfg.rel_tol, kSlotSum, max_eval);
             else st = finalize_loop(ctx, kSlotOuter, nb, tol, max_eval);
             if (st) return st;
-            if ((st = mx_vcycle(m, pred))) return st;
-            ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_mx_correct, grid, box_block(), 0, 
-                                                p, m->e[0], ctx->d_flags[0], L, box, pred);
-            ARTSS_LAUNCH_CK(ctx);
+            bool corrected = false;
+            if ((st = mx_vcycle(m, pred, p, &corrected))) return st;
+            if (!corrected) {
+                ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_mx_correct, grid, box_block(), 0,
+                                                    p, m->e[0], ctx->d_flags[0], L, box, pred);
+                ARTSS_LAUNCH_CK(ctx);
+            }
             if ((st = apply_bc(ctx, p, 0, ARTSS_FIELD_P, pred))) return st;
         }
         if (ctx->capturing) {

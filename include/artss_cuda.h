@@ -447,6 +447,10 @@ int artss_mg_solve_rel(artss_mg *mg, double *p, const double *rhs, double rel_to
  * block (shared memory, register-resident cells and boundary assignments,
  * block barriers only); same iterates, up to the order of the residual sums */
 #define ARTSS_MIXED_CLUSTER_COARSE 8
+/* prolongate one fine cell per thread (8 coarse loads each) instead of one
+ * coarse column per thread updating its 8 children from a register window;
+ * same values */
+#define ARTSS_MIXED_FINE_PROLONG 16
 typedef struct {
     int32_t n_level;          /* V-cycle levels 0 .. n_level-1; the coarse solve is on n_level-1 */
     int32_t n_relax;          /* weighted-Jacobi sweeps before and after each coarse correction */

@@ -160,3 +160,19 @@ def test_mixed_block_coarse_matches_cluster(case):
     assert block[7].cycles == cluster[7].cycles and block[7].rel_residual <= 1e-8
     p_b, p_c = block[4][inner], cluster[4][inner]
     assert np.abs(p_b - p_c).max() <= 1e-9 * np.abs(p_c).max()
+
+
+@pytest.mark.parametrize("case", ["neumann_boxes", "dirichlet_channel"])
+def test_mixed_coarse_column_prolongation_matches_fine(case):
+    """The prolongation by coarse columns (a register window of 27 coarse
+    values, 8 children per coarse cell; the default) and by fine cells
+    (MIXED_FINE_PROLONG) evaluate the same expression for every fine cell: the
+    solves are bit-identical, cycle for cycle."""
+    if case == "neumann_boxes":
+        sc, seed, flags = scenes.poisson_boxes(n=32, seed=9, n_level=4), 9, A.MIXED_REMOVE_MEAN
+    else:
+        sc, seed, flags = scenes.channel_with_cube(nx=64, ny=32, nz=32, steps=1, n_level=3), 7, 0
+    column = solve_pair(sc, seed, flags)
+    fine = solve_pair(sc, seed, flags | A.MIXED_FINE_PROLONG)
+    assert column[7].cycles == fine[7].cycles
+    assert np.array_equal(column[4], fine[4])
