@@ -305,13 +305,13 @@ __device__ __forceinline__ void column_planes(int base, int nk, int z0, int z1, 
 // z-marching variant for 7-point stencils of one array f: the block's planes
 // are the contiguous run [z0 + blockIdx.z * chunk, ...] of chunk =
 // ceil(nz / gridDim.z) planes, and the thread walks its column through them
-// kColU planes per round.  The centre values f[q] of planes k-1 .. k+kColU are
+// U (default kColU) planes per round.  The centre values f[q] of planes k-1 .. k+U are
 // loaded once per round and handed to `value(q, k, f_km1, f_k, f_kp1)` as the
 // z-neighbours, so a cell costs one f load less than its stencil has z terms,
 // and each block streams through consecutive planes.  Planes past the run end
 // are clamped to the plane after it (a ghost or inner plane of the array) and
 // store nothing; `put` as in column_planes.
-template <class T, class FlagT, class V, class P>
+template <int U = kColU, class T, class FlagT, class V, class P>
 __device__ __forceinline__ void column_march(const T *__restrict__ f, int base, int nk, int z0, int z1,
                                              const FlagT *__restrict__ flags, V value, P put) {
     const int nz = z1 - z0 + 1, gz = (int) gridDim.z;
@@ -319,19 +319,19 @@ __device__ __forceinline__ void column_march(const T *__restrict__ f, int base, 
     const int kb = z0 + (int) blockIdx.z * chunk;
     if (kb > z1) return;
     const int ke = min(kb + chunk - 1, z1);
-    T c[kColU + 2];
+    T c[U + 2];
     c[0] = f[base + nk * (kb - 1)];
     c[1] = f[base + nk * kb];
     using R = decltype(value(0, 0, c[0], c[1], c[1]));
-    for (int k0 = kb; k0 <= ke; k0 += kColU) {
+    for (int k0 = kb; k0 <= ke; k0 += U) {
 #pragma unroll
-        for (int u = 0; u < kColU; u++) c[2 + u] = f[base + nk * min(k0 + 1 + u, ke + 1)];
-        R v[kColU];
-        int q[kColU];
-        FlagT fl[kColU];
-        bool ok[kColU];
+        for (int u = 0; u < U; u++) c[2 + u] = f[base + nk * min(k0 + 1 + u, ke + 1)];
+        R v[U];
+        int q[U];
+        FlagT fl[U];
+        bool ok[U];
 #pragma unroll
-        for (int u = 0; u < kColU; u++) {
+        for (int u = 0; u < U; u++) {
             const int k = k0 + u;
             const bool in = k <= ke;
             q[u] = base + nk * (in ? k : ke);
@@ -340,10 +340,10 @@ __device__ __forceinline__ void column_march(const T *__restrict__ f, int base, 
             v[u] = value(q[u], in ? k : ke, c[u], c[u + 1], c[u + 2]);
         }
 #pragma unroll
-        for (int u = 0; u < kColU; u++)
+        for (int u = 0; u < U; u++)
             if (ok[u]) put(q[u], k0 + u, v[u], fl[u]);
-        c[0] = c[kColU];
-        c[1] = c[kColU + 1];
+        c[0] = c[U];
+        c[1] = c[U + 1];
     }
 }
 
@@ -447,7 +447,7 @@ int apply_bc_f32(artss_ctx *ctx, float *f, int level, int field_type, const Loop
 bool cluster_fits(const artss_ctx *ctx, int level, int buffers, int *plane_cap, int64_t *smem);
 bool block_fits(const artss_ctx *ctx, int level, int buffers, int64_t *smem);
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
-                       long long max_it, const LoopState *pred, bool block);
+                       long long max_it, const LoopState *pred, bool block, bool zero_start);
 
 // TMA descriptor of a level array for kTmaBoxX x kTmaBoxY plane windows (tma.cu);
 // tma_level_ok: the level's row pitch allows TMA (Nx even).

@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
 k_mg_coarse_block(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restrict__ b,
                   const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c, double rx, double ry, double rz,
                   const __grid_constant__ BcView bc, double tol, int rel, long long max_it, LoopState *__restrict__ st,
-                  const LoopState *__restrict__ pred) {
+                  const LoopState *__restrict__ pred, int zero_start) {
     extern __shared__ double sm[];
     __shared__ double red[kBlkThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31;
@@ -725,7 +725,8 @@ k_mg_coarse_block(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restri
     double cb[kBlkCells];
 #pragma unroll
     for (int m = 0; m < kBlkCells; m++) cb[m] = ((m0 | m1) >> m & 1) ? (double) b[co[m]] : 0.0;
-    for (int q = tid; q < ntot; q += kBlkThreads) sm[q] = (double) out[q];
+    // zero_start: the iterate starts at zero (out is not read)
+    for (int q = tid; q < ntot; q += kBlkThreads) sm[q] = zero_start ? 0.0 : (double) out[q];
 #define BLK_APPLY_BC(base)                                                                                     \
     for (int w = 0; w < bc.waves; w++) {                                                                       \
         _Pragma("unroll") for (int u = 0; u < kBlkTargets; u++) {                                              \
@@ -1437,6 +1438,15 @@ BcView bc_view(const artss_ctx *ctx, int level) {
     return v;
 }
 
+// out = 0 (the coarse solve's start on the cluster path)
+__global__ void k_fill_f32(float *__restrict__ f, int64_t n, const LoopState *__restrict__ pred) {
+    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
+    pdl_trigger();
+    if (pred && !pred->cond) return;
+    for (int64_t q = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < n; q += (int64_t) gridDim.x * blockDim.x)
+        f[q] = 0.f;
+}
+
 // true when the level fits k_mg_coarse_block: its inner box in the threads'
 // cell slots, its array (and tmp's) in shared memory, its boundary program in
 // the threads' assignment slots
@@ -1461,7 +1471,7 @@ bool block_fits(const artss_ctx *ctx, int level, int buffers, int64_t *smem) {
 template <bool CGS, typename TS>
 int launch_coarse_block(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level, const MgCoef &c, double rx,
                         double ry, double rz, const BcView &v, double tol, int rel, long long mi, int64_t smem,
-                        LoopState *st, const LoopState *pred) {
+                        LoopState *st, const LoopState *pred, bool zero_start) {
     static bool attr_set = false;
     if (!attr_set) {
         ARTSS_CK(cudaFuncSetAttribute(k_mg_coarse_block<CGS, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1470,7 +1480,7 @@ int launch_coarse_block(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level
     }
     const Level &L = ctx->lvl[level];
     ARTSS_LAUNCH_PDL(ctx, FAM_MG_COARSE, (k_mg_coarse_block<CGS, TS>), 1, kBlkThreads, smem, out, tmp, b,
-                     (const uint8_t *) ctx->d_flags[level], L, inner_box(L), c, rx, ry, rz, v, tol, rel, mi, st, pred);
+                     (const uint8_t *) ctx->d_flags[level], L, inner_box(L), c, rx, ry, rz, v, tol, rel, mi, st, pred, zero_start ? 1 : 0);
     ARTSS_LAUNCH_CK(ctx);
     return ARTSS_OK;
 }
@@ -1478,9 +1488,10 @@ int launch_coarse_block(artss_ctx *ctx, TS *out, TS *tmp, const TS *b, int level
 // FP64 solve of one level's pressure system by the cluster kernel on FP32
 // storage (the coarsest-grid solve of the mixed-precision V-cycle); the
 // level's boundary values are taken as zero, tol is relative to the initial
-// residual.  block: by k_mg_coarse_block where the level fits one block.
+// residual.  block: by k_mg_coarse_block where the level fits one block;
+// zero_start: the solve starts from zero (out's contents are not read).
 int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, int smoother, double w, double tol,
-                       long long max_it, const LoopState *pred, bool block) {
+                       long long max_it, const LoopState *pred, bool block, bool zero_start) {
     const bool cgs = smoother == ARTSS_SMOOTHER_CGS;
     int cap = 0;
     int64_t smem = 0;
@@ -1507,9 +1518,14 @@ int coarse_cluster_f32(artss_ctx *ctx, float *out, const float *b, int level, in
     if (block && block_fits(ctx, level, cgs ? 1 : 2, &bsmem)) {
         if (cgs)
             return launch_coarse_block<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
-                                                    bsmem, nullptr, pred);
+                                                    bsmem, nullptr, pred, zero_start);
         return launch_coarse_block<false, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,
-                                                 bsmem, nullptr, pred);
+                                                 bsmem, nullptr, pred, zero_start);
+    }
+    if (zero_start) {
+        const int64_t n = ctx->lvl[level].size();
+        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_fill_f32, flat_blocks(n), 256, 0, out, n, pred);
+        ARTSS_LAUNCH_CK(ctx);
     }
     if (cgs)
         return launch_coarse_cluster<true, float>(ctx, out, nullptr, b, level, c, c.ax, c.ay, c.az, v, tol, 1, max_it,

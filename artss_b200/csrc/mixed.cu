@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_mx_prolong_add8(float *__restrict__ fin
 
 // FP64 outer residual r = b - A p on level 0, stored as the FP32 right-hand
 // side of the correction equation; block partials of ||r||^2
-__global__ void k_mx_outer_residual(const double *__restrict__ p, const double *__restrict__ b,
+__global__ void __launch_bounds__(256, 8) k_mx_outer_residual(const double *__restrict__ p, const double *__restrict__ b,
                                     float *__restrict__ r, const uint8_t *__restrict__ flags, Level L, Box3 box,
                                     double rx, double ry, double rz, double *__restrict__ partials,
                                     const LoopState *__restrict__ pred) {
@@ -320,7 +320,7 @@ __global__ void k_mx_outer_residual(const double *__restrict__ p, const double *
     const int nj = (int) L.Nx, nk = (int) L.nxy();
     double acc = 0.0;
     if (col) {
-        column_march(p, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        column_march<2>(p, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
             [&](int x, int, double km, double c0, double kp) {
                 const double c2 = 2 * c0;
                 return b[x] - (rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) +
@@ -390,14 +390,6 @@ __global__ void k_mx_laplacian(double *__restrict__ out, const double *__restric
         const double c2 = 2 * p[x];
         out[x] = rx * (p[x - 1] - c2 + p[x + 1]) + ry * (p[x - nj] - c2 + p[x + nj]) + rz * (p[x - nk] - c2 + p[x + nk]);
     }
-}
-
-__global__ void k_mx_fill(float *__restrict__ f, int64_t n, const LoopState *__restrict__ pred) {
-    pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
-    pdl_trigger();
-    if (pred && !pred->cond) return;
-    for (int64_t q = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; q < n; q += (int64_t) gridDim.x * blockDim.x)
-        f[q] = 0.f;
 }
 
 }  // namespace
@@ -633,9 +625,6 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred, double *p = nullptr, bool *
     }
     // coarsest level: FP64 solve from zero
     {
-        const int64_t n = ctx->lvl[Lc].size();
-        ARTSS_LAUNCH_PDL(ctx, FAM_FIELD_OP, k_mx_fill, flat_blocks(n), 256, 0, m->e[Lc], n, pred);
-        ARTSS_LAUNCH_CK(ctx);
         double w = m->cfg.coarse_w;
         if (w <= 0) {
             // red-black SOR with the optimal weight of the model problem on this grid
@@ -644,7 +633,8 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred, double *p = nullptr, bool *
             w = m->cfg.coarse_smoother == ARTSS_SMOOTHER_CGS ? 2. / (1. + sin(M_PI / (n + 1.))) : 0.6666666667;
         }
         if ((st = coarse_cluster_f32(ctx, m->e[Lc], m->r[Lc], Lc, m->cfg.coarse_smoother, w, m->cfg.coarse_rel_tol,
-                                     m->cfg.coarse_max_iter, pred, !(m->cfg.flags & ARTSS_MIXED_CLUSTER_COARSE))))
+                                     m->cfg.coarse_max_iter, pred, !(m->cfg.flags & ARTSS_MIXED_CLUSTER_COARSE),
+                                     true)))
             return st;
     }
     for (int l = Lc - 1; l >= 0; l--) {
