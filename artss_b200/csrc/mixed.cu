@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256, 8) k_mx_jacobi(float *__restrict__ out, c
     MX_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
+    column_march<2>(in, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
         [&](int x, int, float km, float c0, float kp) {
             const float h = c.beta * (-b[x] + c.ax * (in[x + 1] + in[x - 1]) + c.ay * (in[x + nj] + in[x - nj]) +
                                       c.az * (kp + km));
@@ -146,7 +146,7 @@ __global__ void k_mx_rbgs(float *__restrict__ e, const float *__restrict__ b, co
 }
 
 // residual q = b - A e on inner cells, FP32 (VCycleMG::Residuum)
-__global__ void k_mx_residuum(float *__restrict__ out, const float *__restrict__ e, const float *__restrict__ b,
+__global__ void __launch_bounds__(256, 8) k_mx_residuum(float *__restrict__ out, const float *__restrict__ e, const float *__restrict__ b,
                               const uint8_t *__restrict__ nbm, Level L, Box3 box, float rx, float ry, float rz,
                               const LoopState *__restrict__ pred) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
@@ -155,7 +155,7 @@ __global__ void k_mx_residuum(float *__restrict__ out, const float *__restrict__
     MX_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    column_march(e, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
+    column_march<2>(e, i + nj * j, nk, (int) box.z0, (int) box.z1, nbm,
         [&](int x, int, float km, float c0, float kp) {
             const float c2 = 2.f * c0;
             return b[x] - (rx * (e[x - 1] - c2 + e[x + 1]) + ry * (e[x - nj] - c2 + e[x + nj]) +
@@ -610,7 +610,7 @@ int mx_vcycle(artss_mixed *m, const LoopState *pred, double *p = nullptr, bool *
                                   (float) (1. / (g.dz[l] * g.dz[l])), pred);
                  ARTSS_LAUNCH_CK(ctx);
                  return ARTSS_OK;
-             })))
+             }, 256)))
             return st;
         if ((st = mx_bc(m, m->q[l], l, pred))) return st;
         const Level &C = ctx->lvl[l + 1];
