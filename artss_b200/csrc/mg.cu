@@ -64,14 +64,14 @@ struct MgCoef {
 };
 
 // JacobiDiffuse::JacobiStep, multigrid variant (JacobiDiffuse.cpp:274-305)
-__global__ void k_mg_jacobi(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
+__global__ void __launch_bounds__(256, 8) k_mg_jacobi(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
                             const uint8_t *__restrict__ flags, Level L, Box3 box, MgCoef c) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+    column_march<2>(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
         [&](int q, int, double km, double c0, double kp) {
             const double out_h = c.beta * (c.dsign * b[q] + c.ax * (in[q + 1] + in[q - 1]) +
                                            c.ay * (in[q + nj] + in[q - nj]) + c.az * (kp + km));
@@ -98,14 +98,14 @@ __global__ void k_mg_cgs_color(double *__restrict__ out, const double *__restric
 }
 
 // VCycleMG::Residuum (VCycleMG.cpp:346-354)
-__global__ void k_mg_residuum(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
+__global__ void __launch_bounds__(256, 8) k_mg_residuum(double *__restrict__ out, const double *__restrict__ in, const double *__restrict__ b,
                               const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz) {
     pdl_wait();  // launched by launch_pdl: the predecessor's writes are visible after this
     pdl_trigger();
     MG_COLUMN(box);
     if (!col) return;
     const int nj = (int) L.Nx, nk = (int) L.nxy();
-    column_march(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+    column_march<2>(in, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
         [&](int q, int, double km, double c0, double kp) {
             const double weighted = (rx * (in[q - 1] - 2 * c0 + in[q + 1]) +
                                      ry * (in[q - nj] - 2 * c0 + in[q + nj]) +
@@ -117,7 +117,7 @@ __global__ void k_mg_residuum(double *__restrict__ out, const double *__restrict
 
 // block partials of sum (b - A x)^2 over the level's inner cells
 // (VCycleMG.cpp:186-194, :668-679, :777-788)
-__global__ void k_mg_resnorm(const double *__restrict__ x, const double *__restrict__ b,
+__global__ void __launch_bounds__(256, 8) k_mg_resnorm(const double *__restrict__ x, const double *__restrict__ b,
                              const uint8_t *__restrict__ flags, Level L, Box3 box, double rx, double ry, double rz,
                              double *__restrict__ partials, double *__restrict__ partials_b) {
     __shared__ double smem[32];
@@ -126,7 +126,7 @@ __global__ void k_mg_resnorm(const double *__restrict__ x, const double *__restr
     double acc = 0.0, accb = 0.0;
     if (col) {
         struct RB { double r, b; };
-        column_march(x, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
+        column_march<2>(x, i + nj * j, nk, (int) box.z0, (int) box.z1, flags,
             [&](int q, int, double km, double c0, double kp) {
                 const double r = b[q] - (rx * (x[q - 1] - 2 * c0 + x[q + 1]) +
                                          ry * (x[q - nj] - 2 * c0 + x[q + nj]) +
@@ -221,7 +221,7 @@ int mg_jacobi_step(artss_mg *mg, double *out, const double *in, const double *b,
         ARTSS_LAUNCH_PDL(ctx, FAM_MG_JACOBI, k_mg_jacobi, g, bl, 0, out, in, b, ctx->d_flags[level], L, box, c);
         ARTSS_LAUNCH_CK(ctx);
         return ARTSS_OK;
-    });
+    }, 256);
 }
 
 int mg_cgs_step(artss_mg *mg, double *out, const double *b, int level) {
@@ -1681,7 +1681,7 @@ int mg_residuum(artss_mg *mg, double *out, const double *in, const double *b, in
                          ry, rz);
         ARTSS_LAUNCH_CK(ctx);
         return ARTSS_OK;
-    });
+    }, 256);
 }
 
 // VCycleMG::VCycleMultigrid (VCycleMG.cpp:215-288).  The reference copies out
