@@ -125,3 +125,65 @@ def test_computational_domain_lists_match_reference(tmp_path, name):
         for n in all_names(g):
             np.testing.assert_array_equal(g.list(n, level), refdriver.ref_list(d, n, level),
                                           err_msg=f"{name}: {n} level {level}")
+
+
+@pytest.mark.parametrize("case", ["no_layers", "missing_border", "missing_value"])
+def test_malformed_layers_rejected_like_the_reference(tmp_path, case):
+    """LayersT parameters are read as in parse_layers_parameters
+    (Settings.cpp:302-321): at least one layer, value_1 .. value_n and
+    border_1 .. border_{n-1}; a malformed set is refused with the reference's
+    message."""
+    params = dict(scenes.layered_channel(steps=0).ic_params)
+    if case == "no_layers":
+        params["n_layers"] = 0
+        msg = "Numbers of layers has to be at least 1. Current value: 0"
+    elif case == "missing_border":
+        del params["border_2"]
+        msg = "Value border_2 is for initial_conditions/LayersT required."
+    else:
+        del params["value_4"]
+        msg = "Value value_4 is for initial_conditions/LayersT required."
+    sc = scenes.layered_channel(steps=0, ic_params=params)
+    xml = scenes.write(sc, str(tmp_path / f"{case}.xml"))
+    with pytest.raises(A.ArtssError) as e:
+        A.Geometry(xml)
+    assert msg in str(e.value)
+    if refdriver.available():
+        import subprocess
+        r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
+        assert r.returncode != 0 and msg in r.stderr, r.stderr
+
+
+@pytest.mark.parametrize("section,accepted", [
+    ('<data_assimilation enabled="Yes" class_name="TemperatureSourceChanger" />', True),
+    ('<data_assimilation enabled="Yes" />', False),
+    ('<data_assimilation enabled="Yes" class_name="ObstacleChanger" load_data="Yes" file="x" />', False),
+])
+def test_data_assimilation_section_read_like_the_reference(tmp_path, section, accepted):
+    """The data-assimilation section is parsed as in parse_assimilation_parameters
+    (Settings.cpp:971-989): class_name is required when enabled, file and time
+    when load_data is set; an accepted section leaves the scene as it is."""
+    sc = scenes.plume_box(n=16, steps=0, n_level=2)
+    text = scenes.to_xml(sc)
+    assert '<data_assimilation enabled="No" />' in text
+    xml = str(tmp_path / "da.xml")
+    with open(xml, "w") as f:
+        f.write(text.replace('<data_assimilation enabled="No" />', section))
+    ref_rc = None
+    if refdriver.available():
+        import subprocess
+        r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
+        ref_rc, ref_err = r.returncode, r.stderr
+    if accepted:
+        g = A.Geometry(xml)
+        assert g.levels == 2
+        if ref_rc is not None:
+            assert ref_rc == 0, ref_err
+    else:
+        msg = ("Value class_name is for data_assimilation required." if "class_name" not in section
+               else "Value time is for data_assimilation required.")
+        with pytest.raises(A.ArtssError) as e:
+            A.Geometry(xml)
+        assert msg in str(e.value)
+        if ref_rc is not None:
+            assert ref_rc != 0 and msg in ref_err, ref_err
