@@ -538,8 +538,10 @@ Settings parse_settings(const std::string &content, const std::string &filename)
                         ob.start[a] = req_real(g.values, std::string("o") + lo[a] + "1", context);
                         ob.end[a] = req_real(g.values, std::string("o") + lo[a] + "2", context);
                     }
+                    // parse_obstacle (Settings.cpp:424-429): boundaries under "boundaries (<name>)"
+                    const std::string cb = ctx_join(context, "boundaries (" + ob.name + ")");
                     for (const auto &bc : c->children)
-                        if (bc->name == "boundary") ob.boundaries.push_back(parse_boundary(bc.get(), context));
+                        if (bc->name == "boundary") ob.boundaries.push_back(parse_boundary(bc.get(), cb));
                 }
                 st.obstacles.push_back(ob);
             }

@@ -187,3 +187,26 @@ def test_data_assimilation_section_read_like_the_reference(tmp_path, section, ac
         assert msg in str(e.value)
         if ref_rc is not None:
             assert ref_rc != 0 and msg in ref_err, ref_err
+
+
+def test_obstacle_boundary_error_names_the_obstacle(tmp_path):
+    """A missing boundary attribute inside an obstacle is reported under the
+    reference's context, obstacles/obstacle/boundaries (<name>)/boundary
+    (Settings.cpp:424-429)."""
+    text = scenes.to_xml(scenes.room_with_door(n=16, steps=0, n_level=2))
+    i = text.index('<obstacle name="')
+    name = text[i + len('<obstacle name="'):text.index('"', i + len('<obstacle name="'))]
+    j = text.index("<boundary ", i)
+    k = text.index(' type="', j)
+    end = text.index('"', k + len(' type="'))
+    xml = str(tmp_path / "room.xml")
+    with open(xml, "w") as f:
+        f.write(text[:k] + text[end + 1:])
+    msg = f"Value type is for obstacles/obstacle/boundaries ({name})/boundary required."
+    with pytest.raises(A.ArtssError) as e:
+        A.Geometry(xml)
+    assert msg in str(e.value)
+    if refdriver.available():
+        import subprocess
+        r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
+        assert r.returncode != 0 and msg in r.stderr, r.stderr
