@@ -476,7 +476,12 @@ InitialConditions parse_ic(const XmlElement *root) {
     };
     auto it = required.find(ic.usr_fct);
     if (it == required.end()) throw config_error(ic.usr_fct + " has no parsing implementation.");
-    for (const auto &k : it->second) req_str(s.values, k, c2);
+    // the reference reads every parameter but an axis name as a number, and a
+    // value that is not one counts as missing (get_required_real, Settings.cpp:81-88)
+    for (const auto &k : it->second) {
+        if (k == "dir") req_str(s.values, k, c2);
+        else req_real(s.values, k, c2);
+    }
     if (ic.usr_fct == "Uniform") ic.uniform_value = req_real(s.values, "val", c2);
     else if (ic.usr_fct == "SinSinSin") ic.sin_l = req_real(s.values, "l", c2);
     else if (ic.usr_fct == "LayersT") {

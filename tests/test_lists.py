@@ -210,3 +210,24 @@ def test_obstacle_boundary_error_names_the_obstacle(tmp_path):
         import subprocess
         r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
         assert r.returncode != 0 and msg in r.stderr, r.stderr
+
+
+def test_non_numeric_initial_condition_parameter_rejected_like_the_reference(tmp_path):
+    """An initial-condition parameter that is not a number counts as missing
+    (get_required_real, Settings.cpp:81-88): the file is refused while it is
+    read, with the reference's message."""
+    sc = scenes.ns_scene("channel", n=16, steps=0)
+    text = scenes.to_xml(sc)
+    i = text.index("<u_lin>")
+    j = text.index("</u_lin>", i)
+    xml = str(tmp_path / "drift.xml")
+    with open(xml, "w") as f:
+        f.write(text[:i] + "<u_lin> fast " + text[j:])
+    msg = "Value u_lin is for initial_conditions/Drift required."
+    with pytest.raises(A.ArtssError) as e:
+        A.Geometry(xml)
+    assert msg in str(e.value)
+    if refdriver.available():
+        import subprocess
+        r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
+        assert r.returncode != 0 and msg in r.stderr, r.stderr
