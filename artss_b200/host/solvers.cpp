@@ -507,7 +507,10 @@ void SolverController::set_up_fields() {
         // sits on a border takes the upper layer's value
         std::vector<real> T = m_fc->T.to_host();
         const int dir = ic.layers_dir;
-        if (dir >= 0) {
+        // an axis name the reference does not know fails its first coordinate
+        // lookup (Coordinate::operator[], src/domain/Coordinate.h:53)
+        if (dir < 0) throw config_error("unknown axis");
+        {
             const Grid &grid = geo.grid();
             const GridLevel &g = grid.level(0);
             const size_t n = ic.layers_values.size();
