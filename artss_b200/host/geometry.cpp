@@ -64,6 +64,17 @@ Grid::Grid(const settings::Domain &d, size_t levels) : levels_(levels), lv_(leve
             g.N[a] = (size_t) (std::round(length_pd[a] / g.spacing[a]) + 2);
             g.cd_start[a] = (size_t) std::round((start_cd[a] - start_pd[a]) / g.spacing[a]) + 1;
             g.cd_end[a] = (size_t) std::round((end_cd[a] - start_pd[a]) / g.spacing[a]);
+            // The reference sizes its inner and boundary lists by the level's cell
+            // count (Domain::init, src/domain/Domain.cpp:40-54) but fills them over
+            // the index range above (Domain::inner_cells, Domain.cpp:191-203).  When a
+            // computational domain's bounds fall between a coarse level's cells the
+            // rounding makes the two differ by one: the reference then writes past
+            // its lists or leaves zero entries in them.  Such a domain is refused.
+            if (g.cd_end[a] + 1 < g.cd_start[a] || g.cd_end[a] + 1 - g.cd_start[a] != g.n[a])
+                throw config_error("computational domain bounds fall between the cells of multigrid level " +
+                                   std::to_string(l) + " on axis " + std::string(1, "xyz"[a]) + " (" +
+                                   std::to_string(g.n[a]) + " cells, index range " + std::to_string(g.cd_start[a]) +
+                                   ".." + std::to_string(g.cd_end[a]) + ")");
         }
     }
 }

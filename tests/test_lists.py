@@ -127,6 +127,56 @@ def test_computational_domain_lists_match_reference(tmp_path, name):
                                           err_msg=f"{name}: {n} level {level}")
 
 
+def _inset(n, before, after, levels, h=0.1):
+    """A computational domain of n cells of h per axis with `before` and
+    `after` physical cells on either side of it."""
+    ext = [(0.0, (before[a] + n[a] + after[a]) * h) for a in range(3)]
+    cd = tuple((before[a] * h, (before[a] + n[a]) * h) for a in range(3))
+    return scenes.Scene(steps=0, n_level=levels, boundaries=scenes.closed_box_bcs(), nx=n[0], ny=n[1], nz=n[2],
+                        X=ext[0], Y=ext[1], Z=ext[2], cd=cd, noise=False,
+                        source_pos=tuple((cd[a][0] + cd[a][1]) / 2 for a in range(3)))
+
+
+@pytest.mark.parametrize("shape,axis,coarse,overrun", [
+    (((12, 8, 8), (5, 0, 0), (1, 0, 0)), "x", "6 cells, index range 3..9", True),
+    (((8, 24, 8), (0, 3, 0), (0, 0, 0)), "y", "12 cells, index range 3..13", False),
+])
+def test_computational_domain_between_coarse_cells_refused(tmp_path, shape, axis, coarse, overrun):
+    """A computational domain whose bounds fall between the cells of a coarse
+    level: the level's index range and its cell count differ by one.  The
+    reference sizes its lists by the count and fills them over the range
+    (Domain.cpp:40-54, 191-203) -- it writes past its inner list (glibc aborts)
+    or leaves zero entries in it; this library refuses the file."""
+    xml = scenes.write(_inset(*shape, levels=1), str(tmp_path / "cd.xml"))
+    with pytest.raises(A.ArtssError, match=f"fall between the cells of multigrid level 1 on axis {axis} \\({coarse}\\)"):
+        A.Geometry(xml)
+    if refdriver.available():
+        import subprocess
+        r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0", "--dump", str(tmp_path), "--lists"],
+                           capture_output=True, text=True, timeout=300)
+        if overrun:
+            assert r.returncode != 0 and "reference error" not in r.stderr, r.stderr
+        else:
+            assert r.returncode == 0, r.stderr
+            assert (refdriver.ref_list(str(tmp_path), "inner", 1) == 0).sum() == 16
+
+
+def test_computational_domain_off_coarse_cells_lists_match_reference(tmp_path):
+    """Odd margins whose coarse-level rounding still gives the level's cell
+    count are accepted, with the reference's lists on every level."""
+    if not refdriver.available():
+        pytest.skip("reference oracle not built")
+    for i, shape in enumerate([((12, 8, 8), (3, 0, 0), (3, 0, 0)), ((16, 8, 8), (3, 2, 2), (1, 2, 2)),
+                               ((12, 12, 8), (2, 3, 2), (2, 1, 2))]):
+        xml = scenes.write(_inset(*shape, levels=1), str(tmp_path / f"cd{i}.xml"))
+        d = refdriver.run(xml, str(tmp_path / f"ref{i}"), steps=0, lists=True)
+        g = A.Geometry(xml)
+        for level in range(g.levels + 1):
+            for n in all_names(g):
+                np.testing.assert_array_equal(g.list(n, level), refdriver.ref_list(d, n, level),
+                                              err_msg=f"{shape}: {n} level {level}")
+
+
 @pytest.mark.parametrize("case", ["no_layers", "missing_border", "missing_value"])
 def test_malformed_layers_rejected_like_the_reference(tmp_path, case):
     """LayersT parameters are read as in parse_layers_parameters
