@@ -836,7 +836,7 @@ k_mg_coarse_block(TS *__restrict__ out, TS *__restrict__ tmp, const TS *__restri
 
 // ---------------------------------------------------------------- pipelined Jacobi coarse solve
 //
-// VCycleMG::call_solve_jacobi (src/pressure/VCycleMG.cpp:727-800) on the
+// VCycleMG::call_solve_jacobi (src/pressure/VCycleMG.cpp:725-798) on the
 // cluster with every access to the rank's own shared memory and one cluster
 // barrier per sweep, for boundary programs of a single wave (every
 // configuration of the reference's tests):

@@ -295,7 +295,7 @@ Geometry::Geometry(const settings::Settings &s)
             check_bc(t, o.boundaries, "obstacle '" + o.name + "'");
             obstacle_bc_.push_back(t);
         }
-        // DomainController::detect_neighbouring_obstacles (src/domain/DomainController.cpp:148-169)
+        // DomainController::detect_neighbouring_obstacles (src/domain/DomainController.cpp:154-173)
         for (size_t a = 0; a < lvl0.size(); a++)
             for (size_t b = a + 1; b < lvl0.size(); b++)
                 for (int axis = 0; axis < 3; axis++) {
@@ -364,7 +364,7 @@ Geometry::Geometry(const settings::Settings &s)
                            (g.cd_end[2] - g.cd_start[2] + 1);
         if (inner.size() + obst.size() != box)
             throw config_error("obstacles overlap on multigrid level " + std::to_string(l) +
-                               "; the reference list construction (src/domain/Domain.cpp:224-233) is undefined there");
+                               "; the reference list construction (src/domain/Domain.cpp:50-54, 191-203) is undefined there");
         IdxList all = boundary_[l][0];
         for (int p = 1; p < 6; p++) all = merge_unique(all, boundary_[l][p]);
         domain_[l] = merge_keep(inner, all);

@@ -122,7 +122,7 @@ int match_bc(const std::string &s) {
     return match_name(s, names, 3, "boundary condition");
 }
 
-// Mapping::match_axis (src/utility/Mapping.cpp:5-11): an unknown name maps to
+// Mapping::match_axis (src/utility/Mapping.cpp:17-23): an unknown name maps to
 // UNKNOWN_AXIS (-1), which the solvers then ignore
 int match_axis(std::string s) {
     std::transform(s.begin(), s.end(), s.begin(), [](unsigned char c) { return (char) std::toupper(c); });

@@ -40,7 +40,7 @@ std::unique_ptr<ISource> make_source(Runtime &rt, const std::string &type, const
 
 static std::unique_ptr<ISourceFunction> make_temperature_source_function(Runtime &rt,
                                                                           const settings::TemperatureSource &s) {
-    // SolverSelection::set_temperature_source_function (src/solver/SolverSelection.cpp:165-212)
+    // SolverSelection::set_temperature_source_function (src/solver/SolverSelection.cpp:138-163)
     if (s.temp_fct == "Gauss") {
         auto g = std::make_unique<GaussFunction>(rt, s.gauss);
         if (s.random) {

@@ -270,7 +270,7 @@ int artss_set_boundary_program(artss_ctx *ctx, int level, int field_type,
 /* Number of kernel waves the compiled program of (level, field_type) needs. */
 int artss_boundary_program_waves(artss_ctx *ctx, int level, int field_type);
 
-/* DomainController::apply_boundary (src/domain/DomainController.cpp:139-141). */
+/* DomainController::apply_boundary (src/domain/DomainController.cpp:145-147). */
 int artss_apply_boundary(artss_ctx *ctx, double *field, int level, int field_type);
 
 /* ------------------------------------------------------------------ */
