@@ -305,14 +305,14 @@ __global__ void k_add_source(double *__restrict__ out, const double *__restrict_
 // ------------------------------------------------------------ diffusion
 
 struct DiffCoef {
-    double ax, ay, az;         // laminar alphas  D*dt/dx^2 ... (ColoredGaussSeidelDiffuse.cpp:56-58)
+    double ax, ay, az;         // laminar alphas  D*dt/dx^2 ... (ColoredGaussSeidelDiffuse.cpp:58-60)
     double beta;               // 1/(1 + 2 sum alpha)
     double rbeta;              // 1 + 2 sum alpha
     double dsign, w, omw;      // sign of b, relaxation weight, (1 - w)
     double D, dt, rdx, rdy, rdz;  // turbulent variant: alphas from D + EV per cell
 };
 
-// alpha / beta of the turbulent variant (ColoredGaussSeidelDiffuse.cpp:248-253)
+// alpha / beta of the turbulent variant (ColoredGaussSeidelDiffuse.cpp:273-278)
 __device__ __forceinline__ void turb_alpha(const DiffCoef &c, double ev, double &ax, double &ay, double &az,
                                            double &rb) {
     ax = (c.D + ev) * c.dt * c.rdx * c.rdx;

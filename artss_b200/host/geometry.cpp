@@ -9,7 +9,7 @@ namespace artss {
 // ------------------------------------------------------------------ merges
 
 IdxList merge_keep(const IdxList &a, const IdxList &b) {
-    // Algorithm::merge_sort (src/utility/Algorithm.cpp:16-48): ties take b
+    // Algorithm::merge_sort (src/utility/Algorithm.cpp:22-54): ties take b
     IdxList out;
     out.reserve(a.size() + b.size());
     size_t p = 0, q = 0;
@@ -20,7 +20,7 @@ IdxList merge_keep(const IdxList &a, const IdxList &b) {
 }
 
 IdxList merge_unique(const IdxList &a, const IdxList &b) {
-    // Algorithm::merge_sort_with_duplicates (src/utility/Algorithm.cpp:50-103)
+    // Algorithm::merge_sort_with_duplicates (src/utility/Algorithm.cpp:65-113)
     if (a.empty()) return b;
     if (b.empty()) return a;
     IdxList out;
@@ -125,7 +125,7 @@ namespace {
 
 ObstacleBox make_box(const std::string &name, std::array<size_t, 3> start, std::array<size_t, 3> end,
                      const GridLevel &g) {
-    // Obstacle::init / create_obstacle / remove_cells_at_boundary (src/domain/Obstacle.cpp:49-190, :459-477)
+    // Obstacle::init / create_obstacle / remove_cells_at_boundary (src/domain/Obstacle.cpp:51-191, :458-478)
     ObstacleBox b;
     b.name = name;
     b.start = start;
@@ -170,7 +170,7 @@ ObstacleBox make_box(const std::string &name, std::array<size_t, 3> start, std::
 
 bool overlap_1d(size_t a1, size_t a2, size_t b1, size_t b2) { return a1 <= b2 && a2 >= b1; }
 
-// Obstacle::calculate_area_index (src/domain/Obstacle.cpp:504-533)
+// Obstacle::calculate_area_index (src/domain/Obstacle.cpp:513-544)
 void area_index(const ObstacleBox &o1, const ObstacleBox &o2, size_t &c1, size_t &c2, int axis, bool start) {
     if (start) {
         c1 = o1.start[axis];
@@ -217,7 +217,7 @@ IdxList remove_rect(const IdxList &list, const std::array<size_t, 3> &rs, const 
     return out;
 }
 
-// Obstacle::circular_constraints (src/domain/Obstacle.cpp:578-858): o1 lies
+// Obstacle::circular_constraints (src/domain/Obstacle.cpp:597-859): o1 lies
 // directly after o2 along `axis`
 void circular_constraints(ObstacleBox &o1, ObstacleBox &o2, int axis, const GridLevel &g) {
     if (o1.start[axis] - 1 != o2.end[axis]) return;

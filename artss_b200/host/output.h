@@ -2,7 +2,7 @@
 // (artss_readback): the values leave the device beside the following steps
 // and a worker thread formats and writes the files, so the steps do not wait
 // for the file system.
-//  * write_dat: Analysis::write_file (src/analysis/Analysis.cpp:378-387), one
+//  * write_dat: Analysis::write_file (src/analysis/Analysis.cpp:381-390), one
 //    value per line in the default stream format, every cell of level 0;
 //  * write_vtk: VTKWriter::write_numerical (src/visualisation/VTKWriter.cpp:60-
 //    106): a legacy binary VTK rectilinear grid (big-endian floats) of the

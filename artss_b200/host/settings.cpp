@@ -20,7 +20,7 @@ using Map = std::map<std::string, std::string>;
 const char *const kYes = "Yes";
 
 // Section `name` among the children of `head`: its attributes plus the text
-// of its children (Settings.cpp:26-54, map_parameter_section).
+// of its children (Settings.cpp:23-55, map_parameter_section).
 struct Section {
     const XmlElement *el = nullptr;
     Map values;
@@ -459,7 +459,7 @@ InitialConditions parse_ic(const XmlElement *root) {
     ic.usr_fct = req_str(s.values, "usr_fct", context);
     ic.values = s.values;
     const std::string c2 = ctx_join(context, ic.usr_fct);
-    // required keys per initial condition (Settings.cpp:183-330)
+    // required keys per initial condition (Settings.cpp:189-331)
     static const std::map<std::string, std::vector<std::string>> required = {
         {"Uniform", {"val"}},
         {"SinSinSin", {"l"}},

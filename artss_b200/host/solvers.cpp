@@ -158,14 +158,14 @@ Field *FieldController::by_name(const std::string &n) {
 
 NSTempTurbSolver::NSTempTurbSolver(Runtime &rt, FieldController &fc, bool turbulent, bool concentration)
     : m_rt(rt), m_fc(fc), m_turb(turbulent), m_con(concentration) {
-    // NSTempSolver (src/solver/NSTempSolver.cpp:19-48) is the same composition
+    // NSTempSolver (src/solver/NSTempSolver.cpp:16-49) is the same composition
     // without the turbulence model
     const settings::Solver &s = rt.settings().solver;
     adv_vel = make_advection(rt, s.advection);
     adv_temp = make_advection(rt, s.temperature.advection);
     dif_vel = make_diffusion(rt, s.diffusion);
     if (turbulent) mu_tub = make_turbulence(rt, s.turbulence);
-    dif_temp = make_diffusion(rt, s.diffusion);  // NSTempTurbSolver.cpp:45: the velocity settings
+    dif_temp = make_diffusion(rt, s.diffusion);  // NSTempTurbSolver.cpp:50: the velocity settings
     pres = make_pressure(rt, s.pressure);
     sou_vel = make_source(rt, s.source.type, s.source.dir);
     sou_temp = make_source(rt, s.temperature.source.type, s.temperature.source.dir);
@@ -222,7 +222,7 @@ void NSTempTurbSolver::do_step(real t, bool sync) {
     FieldController::couple_vector(f.u, f.u0, f.u_tmp, f.v, f.v0, f.v_tmp, f.w, f.w0, f.w_tmp);
 
     // 2. turbulent viscosity and diffusion (:140-152); NSTempSolver: laminar
-    //    diffusion when nu != 0 (NSTempSolver.cpp:99-108)
+    //    diffusion when nu != 0 (NSTempSolver.cpp:109-119)
     artss_ctx_stage_mark(ctx, ARTSS_STAGE_DIFFUSION);
     if (m_turb) {
         mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
@@ -398,12 +398,12 @@ void VelocitySolver::do_step(real, bool sync) {
     FieldController &f = m_fc;
     const real nu = m_rt.settings().physical.nu.value_or(0.0);
     switch (m_kind) {
-        case ADVECTION:  // AdvectionSolver.cpp:47-66
+        case ADVECTION:  // AdvectionSolver.cpp:57-79
             adv->advect(f.u, f.u0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
             adv->advect(f.v, f.v0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
             adv->advect(f.w, f.w0, *m_u_lin, *m_v_lin, *m_w_lin, sync);
             break;
-        case ADVECTION_DIFFUSION:  // AdvectionDiffusionSolver.cpp:45-95
+        case ADVECTION_DIFFUSION:  // AdvectionDiffusionSolver.cpp:42-84
             adv->advect(f.u, f.u0, f.u0, f.v0, f.w0, sync);
             adv->advect(f.v, f.v0, f.u0, f.v0, f.w0, sync);
             adv->advect(f.w, f.w0, f.u0, f.v0, f.w0, sync);
@@ -414,12 +414,12 @@ void VelocitySolver::do_step(real, bool sync) {
                 dif->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
             }
             break;
-        case DIFFUSION:  // DiffusionSolver.cpp:40-62
+        case DIFFUSION:  // DiffusionSolver.cpp:39-65
             dif->diffuse(f.u, f.u0, f.u_tmp, nu, sync);
             dif->diffuse(f.v, f.v0, f.v_tmp, nu, sync);
             dif->diffuse(f.w, f.w0, f.w_tmp, nu, sync);
             break;
-        case DIFFUSION_TURB:  // DiffusionTurbSolver.cpp:44-77
+        case DIFFUSION_TURB:  // DiffusionTurbSolver.cpp:38-68
             mu_tub->calc_turbulent_viscosity(f.nu_t, f.u, f.v, f.w, true);
             dif->diffuse(f.u, f.u0, f.u_tmp, nu, f.nu_t, sync);
             dif->diffuse(f.v, f.v0, f.v_tmp, nu, f.nu_t, sync);
@@ -475,7 +475,7 @@ SolverController::SolverController(Runtime &rt) : m_rt(rt) {
 }
 
 void SolverController::set_up_fields() {
-    // SolverController::set_up_fields (src/solver/SolverController.cpp:84-218), the
+    // SolverController::set_up_fields (src/solver/SolverController.cpp:95-205), the
     // initial conditions of the fractional-step path
     const auto &ic = m_rt.settings().ic;
     const Geometry &geo = m_rt.geometry();
@@ -690,7 +690,7 @@ void SolverController::set_up_fields() {
 }
 
 void SolverController::force_source() {
-    // SolverController::force_source (src/solver/SolverController.cpp:228-258)
+    // SolverController::force_source (src/solver/SolverController.cpp:229-257)
     const auto &src = m_rt.settings().solver.source;
     if (src.force_fct == "Buoyancy") {
         if (!src.use_init_values) m_fc->T_ambient.set_value(src.ambient_temperature.value());

@@ -163,7 +163,7 @@ class SolverController {
     bool m_has_momentum_source = false;
 };
 
-// TimeIntegration (src/TimeIntegration.cpp:46-186), benchmark branch.
+// TimeIntegration (src/TimeIntegration.cpp:45-186), benchmark branch.
 class TimeIntegration {
  public:
     TimeIntegration(Runtime &rt, SolverController &sc);

@@ -155,7 +155,7 @@ def room_with_door(n: int = 32, steps: int = 10, n_level: int = 2, diffusion: st
     """A closed room built from seven touching wall obstacles with a door in
     one wall, heated at the floor centre: the obstacle layout of the
     reference's Steckler test (touching walls exercise the neighbouring-obstacle
-    handling of src/domain/Obstacle.cpp:539-858), on a 3.2 m cube of n^3 cells."""
+    handling of src/domain/Obstacle.cpp:513-859), on a 3.2 m cube of n^3 cells."""
     h = 3.2 / n
     c = lambda k: round(k * h, 12)  # noqa: E731  cell-aligned coordinate
     q = n // 16  # wall thickness in cells

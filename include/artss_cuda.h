@@ -11,7 +11,7 @@
  *  - Arrays use the reference layout IX(i,j,k) = i + Nx*j + Nx*Ny*k with one
  *    ghost layer (ARTSS src/utility/GlobalMacrosTypes.h:70), FP64 unless noted.
  *  - "level" is the multigrid level (0 = finest), "field_type" the reference
- *    FieldType (ARTSS src/utility/Mapping.h:55-58) that selects boundary
+ *    FieldType (ARTSS src/utility/Mapping.h:52-54) that selects boundary
  *    conditions.
  *  - Iterative solvers never hang: each loop is bounded by its max_iter and
  *    reports the iterations it took.
@@ -39,7 +39,7 @@ enum artss_status {
     ARTSS_ERR_LIMIT = -6      /* a size exceeds a documented maximum */
 };
 
-/* ARTSS FieldType (src/utility/Mapping.h:55-58) */
+/* ARTSS FieldType (src/utility/Mapping.h:52-54) */
 enum artss_field_type {
     ARTSS_FIELD_RHO = 0, ARTSS_FIELD_U = 1, ARTSS_FIELD_V = 2, ARTSS_FIELD_W = 3,
     ARTSS_FIELD_P = 4, ARTSS_FIELD_T = 5, ARTSS_FIELD_NU = 6, ARTSS_NUM_FIELD_TYPES = 7
@@ -48,7 +48,7 @@ enum artss_field_type {
 typedef struct artss_ctx artss_ctx;
 
 /* Per-level grid geometry, as DomainData computes it
- * (ARTSS src/domain/DomainData.cpp:12-56, DomainData.h:181-190). */
+ * (ARTSS src/domain/DomainData.cpp:12-56, DomainData.h:144-171). */
 typedef struct {
     int32_t n_levels;                    /* coarse levels (reference n_level); levels 0..n_levels */
     int32_t reserved;
@@ -147,7 +147,7 @@ int64_t artss_ctx_kernel_launches(artss_ctx *ctx);
  * of the profiled ones. */
 #define ARTSS_KERNEL_FAMILIES 22
 /* Stage timing (no counterpart in the reference, whose benchmark build only
- * prints a wall clock per step, src/TimeIntegration.cpp:59,183).  With
+ * prints one wall-clock time for the run, src/TimeIntegration.cpp:59,183).  With
  * enable != 0 the host solvers record one CUDA event on the context stream
  * at each stage boundary of a timestep (not inside graph capture);
  * artss_ctx_stage_read synchronizes the stream and returns the device time
@@ -179,7 +179,7 @@ const char *artss_kernel_family_name(int family);
 int artss_field_alloc(artss_ctx *ctx, int level, double **out);
 int artss_field_free(artss_ctx *ctx, double *field);
 int64_t artss_field_size(artss_ctx *ctx, int level);
-/* Field::update_dev / update_host (src/field/Field.h:41-49). */
+/* Field::update_dev / update_host (src/field/Field.h:45-52). */
 int artss_upload(artss_ctx *ctx, double *dst, const double *host, int64_t n);
 int artss_download(artss_ctx *ctx, double *host, const double *src, int64_t n);
 /* The same copies ordered on the context's stream without waiting for them:

@@ -580,7 +580,7 @@ int64_t oracle_mg_pressure(oracle_mg *mg, double *p, const double *rhs, int firs
 
 int64_t oracle_mg_last_coarse_iterations(const oracle_mg *mg) { return mg->last_coarse_it; }
 
-/* DynamicSmagorinsky::explicit_filtering (src/turbulence/DynamicSmagorinsky.cpp:384-427):
+/* DynamicSmagorinsky::explicit_filtering (src/turbulence/DynamicSmagorinsky.cpp:393-427):
  * trapezoidal 3x3x3 weights, x offset outermost, z innermost */
 static void ds_filter(const oracle_scene *s, double *out, const double *in) {
     const int64_t Nx = s->Nx[0], Ny = s->Ny[0];

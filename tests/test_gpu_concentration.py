@@ -5,7 +5,7 @@ Sc_T, the source, couples).
 
 The reference cannot run either solver: both constructors store the
 concentration's advection in adv_temp a second time and never set adv_con
-(NSTempTurbConSolver.cpp:30, NSTempConSolver.cpp:30), so do_step calls through
+(NSTempTurbConSolver.cpp:29, NSTempConSolver.cpp:30), so do_step calls through
 an unset pointer.  Parity is anchored instead on
 * u, v, w, p, T: the concentration is passive, so the Con solver's velocity,
   pressure and temperature equal the reference build's NSTempTurbSolver /
