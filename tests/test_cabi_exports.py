@@ -44,3 +44,16 @@ def test_pipelined_transfer_entry_points_declared():
         assert n in cuda, n
     for n in ("artss_sim_step_io", "artss_sim_step_io_async", "artss_sim_io_sync", "artss_sim_set_graphs"):
         assert n in host, n
+
+
+def test_integration_index_lists_every_entry_point():
+    """The entry-point index of INTEGRATION.md names every declared function
+    (the network kernels by their artss_nn_ prefix)."""
+    with open(os.path.join(os.path.dirname(HERE), "INTEGRATION.md")) as f:
+        text = f.read()
+    assert "## 7. Entry-point index" in text
+    index = text.split("## 7. Entry-point index", 1)[1]
+    listed = set(re.findall(r"`(artss_\w+)`", index))
+    missing = [n for h in ("artss_cuda.h", "artss_host.h") for n in declared(h)
+               if n not in listed and not (n.startswith("artss_nn_") and "artss_nn_*" in index)]
+    assert not missing, missing
