@@ -185,36 +185,69 @@ void area_index(const ObstacleBox &o1, const ObstacleBox &o2, size_t &c1, size_t
     }
 }
 
-// Removes the cells of the rectangle [rs, re] (fixed on `axis`) from a
-// sorted patch list by walking it with a cursor over the rectangle in
-// ascending order.  The cursor only advances on a match, exactly like the
-// removal loops of Obstacle::circular_constraints
-// (src/domain/Obstacle.cpp:657-782).
-IdxList remove_rect(const IdxList &list, const std::array<size_t, 3> &rs, const std::array<size_t, 3> &re, int axis,
-                    int o0, int o1, const GridLevel &g) {
-    IdxList out;
-    out.reserve(list.size());
-    std::array<size_t, 3> c = rs;
-    Idx target = g.index(c[0], c[1], c[2]);
-    size_t a0 = rs[o0], a1 = rs[o1];
+// One obstacle's side of the cell removal of Obstacle::circular_constraints
+// (src/domain/Obstacle.cpp:700-808): the cells of the rectangle [rs, re]
+// (fixed on `axis`) are removed from a sorted patch list by a cursor that
+// moves over the rectangle in ascending order, and only on a match.  Cells
+// below the rectangle's first cell are kept as they are; where every cell of
+// the list lies below it, the reference reads on past the end of the list
+// (Obstacle.cpp:704-723) and its result depends on the memory behind it, and
+// this walk stops at the end.
+struct PatchWalk {
+    const IdxList &in;
+    const GridLevel &g;
+    std::array<size_t, 3> cur, re;
+    size_t reset0;  // the cursor's first coordinate on the inner axis
+    int o0, o1;
+    size_t pos = 0;
     bool ended = false;
-    for (Idx e : list) {
-        if (!ended && e == target) {
-            a0++;
-            if (a0 > re[o0]) {
-                a0 = rs[o0];
-                a1++;
-                if (a1 > re[o1]) ended = true;
-            }
-            c[o0] = a0;
-            c[o1] = a1;
-            c[axis] = rs[axis];
-            target = g.index(c[0], c[1], c[2]);
-        } else {
-            out.push_back(e);
-        }
+    Idx target;
+    IdxList out;
+
+    PatchWalk(const IdxList &list, const std::array<size_t, 3> &rs, const std::array<size_t, 3> &re_, int inner,
+              int outer, const GridLevel &gl)
+        : in(list), g(gl), cur(rs), re(re_), reset0(rs[inner]), o0(inner), o1(outer) {
+        target = g.index(cur[0], cur[1], cur[2]);
+        out.reserve(in.size());
+        while (pos < in.size() && in[pos] < target) out.push_back(in[pos++]);
     }
-    return out;
+    bool more() const { return pos < in.size(); }
+    bool in_rows() const { return cur[o1] <= re[o1]; }
+    void step() {
+        const Idx e = in[pos++];
+        if (e != target) {
+            out.push_back(e);
+            return;
+        }
+        if (++cur[o0] > re[o0]) {
+            cur[o0] = reset0;
+            if (++cur[o1] > re[o1]) ended = true;
+        }
+        target = g.index(cur[0], cur[1], cur[2]);
+    }
+};
+
+// Both walks run in one loop (Obstacle.cpp:734-771) while both lists have
+// cells and neither rectangle is exhausted; the walk left over then continues only while its
+// cursor row lies inside its rectangle.  The coupling matters where
+// calculate_area_index makes a rectangle empty on the outer axis (two
+// obstacles side by side but offset): its first matching cell is removed
+// only if the joint loop reaches it.
+void remove_rects(IdxList &l1, IdxList &l2, const std::array<size_t, 3> &r1s, const std::array<size_t, 3> &r1e,
+                  const std::array<size_t, 3> &r2s, const std::array<size_t, 3> &r2e, int inner, int outer,
+                  const GridLevel &g) {
+    PatchWalk w1(l1, r1s, r1e, inner, outer, g), w2(l2, r2s, r2e, inner, outer, g);
+    while (w1.more() && w2.more() && !w1.ended && !w2.ended) {
+        w1.step();
+        w2.step();
+    }
+    for (PatchWalk *w : {&w1, &w2}) {
+        if (!w->ended)
+            while (w->more() && w->in_rows()) w->step();
+        while (w->more()) w->out.push_back(w->in[w->pos++]);
+    }
+    l1 = std::move(w1.out);
+    l2 = std::move(w2.out);
 }
 
 // Obstacle::circular_constraints (src/domain/Obstacle.cpp:597-859): o1 lies
@@ -235,8 +268,7 @@ void circular_constraints(ObstacleBox &o1, ObstacleBox &o2, int axis, const Grid
     area_index(o1, o2, r1e[ax0], r2e[ax0], ax0, false);
     area_index(o1, o2, r1s[ax1], r2s[ax1], ax1, true);
     area_index(o1, o2, r1e[ax1], r2e[ax1], ax1, false);
-    o1.patch[p1] = remove_rect(o1.patch[p1], r1s, r1e, axis, ax0, ax1, g);
-    o2.patch[p2] = remove_rect(o2.patch[p2], r2s, r2e, axis, ax0, ax1, g);
+    remove_rects(o1.patch[p1], o2.patch[p2], r1s, r1e, r2s, r2e, ax0, ax1, g);
 }
 
 void fill_bc(BcTable &t, const std::vector<settings::Boundary> &bs) {

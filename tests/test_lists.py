@@ -177,6 +177,49 @@ def test_computational_domain_off_coarse_cells_lists_match_reference(tmp_path):
                                               err_msg=f"{shape}: {n} level {level}")
 
 
+_OFFSET_NEIGHBOURS = [  # two obstacles side by side, offset across the shared face (cell index ranges)
+    [((7, 7), (9, 10), (2, 3)), ((8, 9), (9, 11), (2, 2))],
+    [((4, 6), (4, 5), (7, 8)), ((3, 6), (6, 8), (7, 7))],
+    [((7, 10), (7, 7), (9, 9)), ((8, 10), (7, 9), (10, 10))],
+    [((4, 5), (8, 9), (6, 7)), ((6, 7), (8, 10), (6, 6))],
+    [((7, 9), (7, 8), (8, 10)), ((10, 11), (7, 9), (8, 8))],
+]
+
+
+def _offset_scene(cells, levels):
+    h = 0.1
+    boxes = [scenes.Box(round((c[0][0] - 1) * h, 10), round(c[0][1] * h, 10), round((c[1][0] - 1) * h, 10),
+                        round(c[1][1] * h, 10), round((c[2][0] - 1) * h, 10), round(c[2][1] * h, 10), f"b{i}")
+             for i, c in enumerate(cells)]
+    return scenes.Scene(steps=0, n_level=levels, nx=12, ny=12, nz=12, X=(0.0, 1.2), Y=(0.0, 1.2), Z=(0.0, 1.2),
+                        obstacles=boxes, obstacle_bcs=scenes.solid_obstacle_bcs(), boundaries=scenes.closed_box_bcs(),
+                        noise=False, source_pos=(0.3, 0.3, 0.9))
+
+
+def test_offset_neighbour_removal_known_answer(tmp_path):
+    """Obstacle::circular_constraints walks both obstacles' facing patches in
+    one loop (Obstacle.cpp:734-771); a removal rectangle that is empty on the
+    outer axis gives up its first matching cell only while that joint loop
+    runs.  Here obstacle 0's right patch keeps (7,10,2): the reference build
+    gives [539, 721, 735] (two independent walks would also drop 539)."""
+    xml = scenes.write(_offset_scene(_OFFSET_NEIGHBOURS[0], 1), str(tmp_path / "n.xml"))
+    g = A.Geometry(xml)
+    np.testing.assert_array_equal(g.list("obst0_right", 0), [539, 721, 735])
+
+
+@pytest.mark.parametrize("case", range(len(_OFFSET_NEIGHBOURS)))
+def test_offset_neighbour_lists_match_reference(tmp_path, case):
+    if not refdriver.available():
+        pytest.skip("reference oracle not built")
+    xml = scenes.write(_offset_scene(_OFFSET_NEIGHBOURS[case], 2), str(tmp_path / "n.xml"))
+    d = refdriver.run(xml, str(tmp_path / "ref"), steps=0, lists=True)
+    g = A.Geometry(xml)
+    for level in range(g.levels + 1):
+        for n in all_names(g):
+            np.testing.assert_array_equal(g.list(n, level), refdriver.ref_list(d, n, level),
+                                          err_msg=f"case {case}: {n} level {level}")
+
+
 @pytest.mark.parametrize("case", ["no_layers", "missing_border", "missing_value"])
 def test_malformed_layers_rejected_like_the_reference(tmp_path, case):
     """LayersT parameters are read as in parse_layers_parameters
