@@ -75,7 +75,7 @@ void oracle_add_source(const oracle_scene *s, double *out, const double *S, doub
  * program; ev == NULL: laminar. */
 void oracle_diffuse_explicit(const oracle_scene *s, double *out, const double *in, double D, const double *ev,
                              double dt, int field_type);
-/* DynamicSmagorinsky::calc_turbulent_viscosity (src/turbulence/DynamicSmagorinsky.cpp:172-376)
+/* DynamicSmagorinsky::calc_turbulent_viscosity (src/turbulence/DynamicSmagorinsky.cpp:172-384)
  * with its explicit_filtering (:384-427), loop by loop: ev on the inner cells
  * (no boundary program).  The reference's work fields start as zero and only
  * their inner cells are written; this restatement allocates them zeroed per

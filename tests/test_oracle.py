@@ -198,8 +198,9 @@ def _random_boundaries(rng):
 
 def test_random_boundary_conditions_oracle_matches_reference(tmp_path):
     """Random per-patch domain and obstacle boundary conditions on random
-    obstacle scenes: the oracle with this library's boundary programs equals
-    the reference build after each of three steps."""
+    obstacle scenes, with either multigrid smoother and 1-3 sweeps: the
+    oracle with this library's boundary programs equals the reference build
+    after each of three steps."""
     import random
     if not refdriver.available():
         pytest.skip("reference oracle build not present")
@@ -208,6 +209,8 @@ def test_random_boundary_conditions_oracle_matches_reference(tmp_path):
     for case in range(24):
         sc = _random_obstacle_scene(rng)
         sc.boundaries, sc.obstacle_bcs = _random_boundaries(rng)
+        sc.smoother = rng.choice(["Jacobi", "ColoredGaussSeidel"])  # multigrid smoother and sweeps
+        sc.n_relax = rng.choice([1, 2, 3])
         xml = scenes.write(sc, str(tmp_path / f"b{case}.xml"))
         try:
             A.Geometry(xml)
