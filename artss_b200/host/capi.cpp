@@ -40,7 +40,10 @@ int guarded(F &&f) {
     } catch (const cuda_error &e) {
         g_err = e.what();
         return ARTSS_ERR_CUDA;
-    } catch (const std::exception &e) {
+    } catch (const std::invalid_argument &e) {  // a pointer, name, size or file the call cannot use
+        g_err = e.what();
+        return ARTSS_ERR_ARG;
+    } catch (const std::exception &e) {  // a call the simulation's state or kind does not allow
         g_err = e.what();
         return ARTSS_ERR_STATE;
     }
@@ -375,7 +378,7 @@ int artss_sim_last_stats(artss_sim *s, int64_t *diff_iters4, int64_t *mg_cycles,
     return guarded([&] {
         if (!s) throw std::invalid_argument("null simulation");
         auto *ns = dynamic_cast<NSTempTurbSolver *>(&s->sc->solver());
-        if (!ns) throw std::invalid_argument("statistics are kept by NSTempTurbSolver scenes");
+        if (!ns) throw std::logic_error("statistics are kept by NSTempTurbSolver scenes");
         if (diff_iters4)
             for (int k = 0; k < 4; k++) diff_iters4[k] = ns->stats.diffusion_iterations[k];
         if (mg_cycles) *mg_cycles = ns->stats.pressure_cycles;
@@ -388,7 +391,7 @@ int artss_sim_pressure(artss_sim *s, int first_step, int64_t *cycles, double *re
     return guarded([&] {
         if (!s) throw std::invalid_argument("null simulation");
         auto *ps = dynamic_cast<PressureSolver *>(&s->sc->solver());
-        if (!ps) throw std::invalid_argument("not a PressureSolver scene");
+        if (!ps) throw std::logic_error("not a PressureSolver scene");
         const real dt = s->rt->dt();
         ps->pressure().pressure(s->sc->fields().p, s->sc->fields().rhs, first_step ? dt : 2 * dt, false);
         check(artss_ctx_sync(s->rt->ctx()), "pressure");

@@ -736,7 +736,7 @@ void TimeIntegration::set_step(int64_t step) {
 
 void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>> &in,
                               const std::vector<std::pair<Field *, real *>> &out) {
-    if (finished()) throw std::invalid_argument("the simulation has reached t_end");
+    if (finished()) throw std::logic_error("the simulation has reached t_end");
     StepIO io(m_rt.ctx());
     // NSTempTurbSolver / NSTempSolver read p and T late: those arrive on the
     // second stream during the step; the rest before it
@@ -769,7 +769,7 @@ void TimeIntegration::step_io(const std::vector<std::pair<Field *, const real *>
 
 void TimeIntegration::step_io_async(const std::vector<std::pair<Field *, const real *>> &in,
                                     const std::vector<std::pair<Field *, real *>> &out) {
-    if (finished()) throw std::invalid_argument("the simulation has reached t_end");
+    if (finished()) throw std::logic_error("the simulation has reached t_end");
     artss_ctx *ctx = m_rt.ctx();
     FieldController &fc = m_sc.fields();
     const int64_t n = (int64_t) fc.u.get_size();

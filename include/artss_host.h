@@ -23,7 +23,12 @@ extern "C" {
 typedef struct artss_geom artss_geom;
 typedef struct artss_sim artss_sim;
 
-/* last error of the calling thread (config errors, CUDA errors) */
+/* Status of the int-returning functions: ARTSS_OK; ARTSS_ERR_ARG for a
+ * pointer, name, level, size or file the call cannot use (an XML file the
+ * settings reader refuses included); ARTSS_ERR_STATE for a call the scene's
+ * solver or the simulation's state does not allow (a step after t_end);
+ * ARTSS_ERR_CUDA for a device error.  The message of the last failure on the
+ * calling thread: */
 const char *artss_host_last_error(void);
 
 /* ---- geometry (CPU only) ---- */

@@ -57,3 +57,40 @@ def test_integration_index_lists_every_entry_point():
     missing = [n for h in ("artss_cuda.h", "artss_host.h") for n in declared(h)
                if n not in listed and not (n.startswith("artss_nn_") and "artss_nn_*" in index)]
     assert not missing, missing
+
+
+def test_geometry_entry_points_report_bad_arguments(tmp_path):
+    """The CPU-only geometry functions of the host library return
+    ARTSS_ERR_ARG (-1) with a message for unusable arguments and a file the
+    settings reader refuses, and ARTSS_OK for a valid call."""
+    import ctypes as C
+    from artss_b200 import scenes
+    lib = C.CDLL(library_path("libartss_host.so"))
+    lib.artss_host_last_error.restype = C.c_char_p
+    lib.artss_geom_create.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+    lib.artss_geom_list.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.POINTER(C.c_int64)),
+                                    C.POINTER(C.c_int64)]
+    lib.artss_geom_boundary_program.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p),
+                                                C.POINTER(C.c_int64)]
+    lib.artss_geom_destroy.argtypes = [C.c_void_p]
+    err = lambda: lib.artss_host_last_error().decode()  # noqa: E731
+
+    h = C.c_void_p()
+    assert lib.artss_geom_create(str(tmp_path / "absent.xml").encode(), C.byref(h)) == -1
+    assert lib.artss_geom_create(None, C.byref(h)) == -1 and "null" in err()
+    xml = scenes.write(scenes.plume_box(n=16, steps=1, n_level=2), str(tmp_path / "box.xml"))
+    assert lib.artss_geom_create(xml.encode(), C.byref(h)) == 0
+    try:
+        data, n = C.POINTER(C.c_int64)(), C.c_int64()
+        assert lib.artss_geom_list(h, b"inner", 0, C.byref(data), C.byref(n)) == 0 and n.value == 16 ** 3
+        assert lib.artss_geom_list(h, b"nonsense", 0, C.byref(data), C.byref(n)) == -1
+        assert "unknown list 'nonsense'" in err()
+        assert lib.artss_geom_list(h, b"inner", 3, C.byref(data), C.byref(n)) == -1 and "level" in err()
+        assert lib.artss_geom_list(h, b"inner", -1, C.byref(data), C.byref(n)) == -1
+        assert lib.artss_geom_list(h, None, 0, C.byref(data), C.byref(n)) == -1
+        ops, m = C.c_void_p(), C.c_int64()
+        assert lib.artss_geom_boundary_program(h, 0, 4, C.byref(ops), C.byref(m)) == 0 and m.value > 0
+        assert lib.artss_geom_boundary_program(h, 0, 7, C.byref(ops), C.byref(m)) == -1
+        assert lib.artss_geom_boundary_program(h, 9, 4, C.byref(ops), C.byref(m)) == -1
+    finally:
+        lib.artss_geom_destroy(h)
