@@ -324,3 +324,56 @@ def test_non_numeric_initial_condition_parameter_rejected_like_the_reference(tmp
         import subprocess
         r = subprocess.run([refdriver.DRIVER, xml, "--steps", "0"], capture_output=True, text=True, timeout=300)
         assert r.returncode != 0 and msg in r.stderr, r.stderr
+
+
+def _gtest_scene(tmp_path, pd, cd, n, levels=1, boxes=()):
+    """A scene with the domain parameters of a reference gtest (physical
+    domain pd, computational domain cd, n inner cells)."""
+    sc = scenes.Scene(solver="PressureSolver", nx=n[0], ny=n[1], nz=n[2], X=pd[0], Y=pd[1], Z=pd[2],
+                      cd=None if cd == pd else cd, n_level=levels, ic="Zero", noise=False, steps=1,
+                      boundaries=[("p", "front,back,bottom,top,left,right", "dirichlet", 0.0)],
+                      obstacles=list(boxes), obstacle_bcs=[("p", "front,back,bottom,top,left,right", "neumann", 0.0)])
+    return A.Geometry(scenes.write(sc, str(tmp_path / "gtest.xml")))
+
+
+def _sizes(g, level):
+    return {p: len(g.list("bnd_" + p, level)) for p in PATCHES}, len(g.list("domain", level)), len(g.list("inner", level))
+
+
+_GT_PD = ((0.0, 5.0), (0.0, 10.0), (0.0, 15.0))
+
+
+def test_domain_sizes_known_answers(tmp_path):
+    """ARTSS gtests/domain/Domain.cpp:13-129: patch, domain-list and inner-list
+    sizes without and with a computational domain, on level 1, and with a
+    3x3x1 obstacle in the corner (cells 162-178)."""
+    full = {"left": 12 * 22, "right": 12 * 22, "front": 7 * 22, "back": 7 * 22, "bottom": 7 * 12, "top": 7 * 12}
+    assert _sizes(_gtest_scene(tmp_path, _GT_PD, _GT_PD, (5, 20, 10)), 0) == (full, 1848, 1000)
+    g = _gtest_scene(tmp_path, ((0.0, 10.0), (0.0, 11.0), (0.0, 15.0)), _GT_PD, (5, 20, 10))
+    assert _sizes(g, 0) == (full, 1848, 1000)
+    g = _gtest_scene(tmp_path, _GT_PD, _GT_PD, (8, 12, 4))
+    assert _sizes(g, 1) == ({"left": 32, "right": 32, "bottom": 24, "top": 24, "front": 48, "back": 48}, 192, 48)
+    g = _gtest_scene(tmp_path, _GT_PD, _GT_PD, (5, 20, 10), boxes=[scenes.Box(0.0, 3.0, 0.0, 1.5, 0.0, 1.5, "corner")])
+    np.testing.assert_array_equal(g.list("obst", 0), [162, 163, 164, 169, 170, 171, 176, 177, 178])
+    assert _sizes(g, 0) == (full, 1839, 991)
+
+
+def test_domain_indices_known_answers(tmp_path):
+    """ARTSS gtests/domain/Domain.cpp:215-390: sorted lists, and the first and
+    last index of the inner list and of every boundary patch, for a
+    computational domain inside a physical one (z from -1.5) and without."""
+    def ends(g, name):
+        L = g.list(name, 0)
+        assert np.all(np.diff(L) > 0), name
+        return int(L[0]), int(L[-1])
+    g = _gtest_scene(tmp_path, ((0.0, 7.0), (0.0, 15.0), (-1.5, 30.0)), _GT_PD, (5, 20, 10))
+    assert ends(g, "inner") == (586, 3353)
+    assert ends(g, "bnd_left") == (288, 3645) and ends(g, "bnd_right") == (294, 3651)
+    assert ends(g, "bnd_bottom") == (288, 3462) and ends(g, "bnd_top") == (477, 3651)
+    assert ends(g, "bnd_front") == (288, 483) and ends(g, "bnd_back") == (3456, 3651)
+    g = _gtest_scene(tmp_path, _GT_PD, _GT_PD, (5, 20, 10))
+    assert ends(g, "inner") == (162, 1685)
+    assert ends(g, "bnd_left") == (0, 1841) and ends(g, "bnd_right") == (6, 1847)
+    assert ends(g, "bnd_bottom") == (0, 1700) and ends(g, "bnd_top") == (147, 1847)
+    assert ends(g, "bnd_front") == (0, 153) and ends(g, "bnd_back") == (1694, 1847)
+    assert ends(g, "domain") == (0, 1847)
