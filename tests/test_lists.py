@@ -377,3 +377,26 @@ def test_domain_indices_known_answers(tmp_path):
     assert ends(g, "bnd_bottom") == (0, 1700) and ends(g, "bnd_top") == (147, 1847)
     assert ends(g, "bnd_front") == (0, 153) and ends(g, "bnd_back") == (1694, 1847)
     assert ends(g, "domain") == (0, 1847)
+
+
+def test_domain_data_known_answers(tmp_path):
+    """ARTSS gtests/domain/DomainData.cpp:23-310: cells per level (with and
+    without ghost layer), spacings and the computational domain's index range,
+    without and with a computational domain inside the physical one."""
+    pd = ((0.0, 1.0), (-1.0, 1.2), (-0.3, 0.3))
+    d = _gtest_scene(tmp_path, pd, pd, (10, 11, 12)).grid_desc()
+    assert (d.Nx[0], d.Ny[0], d.Nz[0]) == (12, 13, 14) and d.Nx[0] * d.Ny[0] * d.Nz[0] == 2184
+    assert (d.dx[0], d.dy[0], d.dz[0]) == pytest.approx((0.1, 0.2, 0.05), rel=1e-15)
+    assert (d.i1[0], d.j1[0], d.k1[0], d.i2[0], d.j2[0], d.k2[0]) == (1, 1, 1, 10, 11, 12)
+
+    pd = ((0.0, 1.2), (-1.0, -0.2), (-0.3, 0.3))
+    d = _gtest_scene(tmp_path, pd, pd, (24, 4, 1), levels=2).grid_desc()
+    assert [(d.i2[l] - d.i1[l] + 1, d.j2[l] - d.j1[l] + 1, d.k2[l] - d.k1[l] + 1) for l in range(3)] == \
+        [(24, 4, 1), (12, 2, 1), (6, 1, 1)]
+    assert [(d.Nx[l], d.Ny[l], d.Nz[l]) for l in range(3)] == [(26, 6, 3), (14, 4, 3), (8, 3, 3)]
+    for l, h in enumerate([(0.05, 0.2, 0.6), (0.1, 0.4, 0.6), (0.2, 0.8, 0.6)]):
+        assert (d.dx[l], d.dy[l], d.dz[l]) == pytest.approx(h, rel=1e-15), l
+
+    cd = ((0.0, 1.0), (-1.0, 1.2), (-0.3, 0.3))
+    d = _gtest_scene(tmp_path, ((0.0, 1.0), (-1.2, 1.4), (-0.4, 0.4)), cd, (10, 11, 12), levels=2).grid_desc()
+    assert (d.i1[0], d.j1[0], d.k1[0], d.i2[0], d.j2[0], d.k2[0]) == (1, 2, 3, 10, 12, 14)
