@@ -47,8 +47,8 @@ def test_pipelined_transfer_entry_points_declared():
 
 
 def test_integration_index_lists_every_entry_point():
-    """The entry-point index of INTEGRATION.md names every declared function
-    (the network kernels by their artss_nn_ prefix)."""
+    """The integration guide's entry-point index names every declared
+    function (the network kernels by their artss_nn_ prefix)."""
     with open(os.path.join(os.path.dirname(HERE), "INTEGRATION.md")) as f:
         text = f.read()
     assert "## 7. Entry-point index" in text
